@@ -1,0 +1,230 @@
+/*
+ * vipe_b200 — C ABI of the B200 (sm_100a) implementation of ViPE's DROID-style
+ * SLAM backend hot path: dense bundle adjustment (slam_ext), correlation
+ * build/lookup (droid_net_ext) and the lietorch group kernels (lietorch_ext).
+ *
+ * Conventions for every entry point:
+ *   - all tensor arguments are raw DEVICE pointers to contiguous row-major
+ *     buffers in the layouts of the reference extension (shapes given per
+ *     function); integer index tensors are int64 like the reference's `long`;
+ *   - work is enqueued on `stream` (a cudaStream_t passed as void*); nothing
+ *     synchronises the stream unless the comment says so;
+ *   - the return value is a vipe_status (0 = success).  Host-side argument
+ *     errors are detected before any launch; device-side findings (bad
+ *     indices, solver failure) are written to the optional `dev_status` word
+ *     (int32 in device memory) and read by the caller when it wants them;
+ *   - buffers named *_out are written completely; buffers named *_io are
+ *     updated in place (as the reference mutates poses/disps/intrinsics).
+ *
+ * The library holds no torch types: the Python package vipe_b200.ext mirrors
+ * the reference's pybind modules on top of this ABI.
+ */
+#ifndef VIPE_B200_H
+#define VIPE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum vipe_status {
+    VIPE_OK = 0,
+    VIPE_ERR_ARG = 1,          /* bad shape / size / null pointer             */
+    VIPE_ERR_INDEX = 2,        /* edge index outside [0, num_frames)          */
+    VIPE_ERR_RANGE = 3,        /* empty or invalid optimisation window t0..t1 */
+    VIPE_ERR_KX_MISMATCH = 4,  /* eta rows != |unique(cat(arange(t0,t1),ii))| */
+    VIPE_ERR_WORKSPACE = 5,    /* workspace smaller than required             */
+    VIPE_ERR_CAPACITY = 6,     /* graph exceeds a documented kernel limit     */
+    VIPE_ERR_CUDA = 7,         /* a CUDA runtime call failed                  */
+    VIPE_ERR_DTYPE = 8,        /* unsupported element type                    */
+    VIPE_ERR_GROUP = 9,        /* unsupported Lie group id                    */
+    VIPE_WARN_SOLVER = 16      /* (dev_status only) Cholesky failed: dx = 0   */
+};
+
+/* element types for dtype-generic entry points */
+enum vipe_dtype { VIPE_F32 = 0, VIPE_F64 = 1, VIPE_F16 = 2, VIPE_BF16 = 3 };
+
+/* Human-readable message for a status code (static storage). */
+const char* vipe_status_string(int status);
+
+/* Last CUDA error text seen by the library on this thread ("" if none). */
+const char* vipe_last_error(void);
+
+/* =====================================================================
+ * slam_ext — dense bundle adjustment and geometry helpers
+ * ===================================================================== */
+
+/* Bytes of device workspace needed by vipe_slam_ba_extended for a graph of
+ * `num_edges` edges over `num_frames` frames of ht x wd depth maps, depth-row
+ * count `num_kx` (= eta.shape[0]) and window [t0, t1). */
+size_t vipe_slam_ba_workspace_size(int num_frames, int ht, int wd, int num_edges, int num_kx, int t0, int t1);
+
+/* Replaces slam_ext.ba_extended (reference: csrc/slam_ext/slam.cpp:46-51,
+ * implementation csrc/slam_ext/geom_kernels.cu:1626-1847).
+ *   poses_io      (num_frames, 7) f32  [tx ty tz qx qy qz qw], updated in place
+ *   disps_io      (num_frames, ht, wd) f32, updated in place
+ *   intrinsics_io (4,) f32 [fx fy cx cy], fx/fy updated when optimize_intrinsics
+ *   disps_sens    (num_frames, ht, wd) f32
+ *   targets, weights (num_edges, 2, ht, wd) f32
+ *   eta           (num_kx, ht, wd) f32
+ *   ii, jj        (num_edges,) int64
+ *   depth_active  (num_frames,) f32
+ * Outputs (last LM iteration, as the reference returns them):
+ *   dx_out     (t1-t0, 6) f32
+ *   dz_out     (num_kx, ht*wd) f32, untouched when motion_only
+ *   energy_out (iterations,) f32 when compute_energy, else may be NULL
+ * workspace: device buffer of vipe_slam_ba_workspace_size() bytes.
+ * dev_status: optional device int32; receives VIPE_ERR_INDEX /
+ *   VIPE_ERR_KX_MISMATCH / VIPE_ERR_CAPACITY found on the device (the call then
+ *   leaves poses/disps untouched) or VIPE_WARN_SOLVER (dx = 0, as the reference
+ *   does on Cholesky failure). */
+int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* intrinsics_io, const float* disps_sens,
+                          const float* targets, const float* weights, const float* eta, const int64_t* ii,
+                          const int64_t* jj, const float* depth_active, int num_frames, int ht, int wd,
+                          int num_edges, int num_kx, int t0, int t1, int iterations, float lm, float ep,
+                          int motion_only, float alpha, int optimize_intrinsics, float intrinsics_lm,
+                          float intrinsics_ep, float intrinsics_scale, int compute_energy, float* dx_out,
+                          float* dz_out, float* energy_out, void* workspace, size_t workspace_bytes,
+                          int32_t* dev_status, void* stream);
+
+/* Replaces slam_ext.ba (reference: csrc/slam_ext/slam.cpp:42-45,
+ * geom_kernels.cu:1826-1834): ba_extended with depth_active = 1, no focal
+ * optimisation and no energy.  depth_active_scratch: device f32 buffer of
+ * num_frames entries that the call fills with ones. */
+int vipe_slam_ba(float* poses_io, float* disps_io, float* intrinsics_io, const float* disps_sens, const float* targets,
+                 const float* weights, const float* eta, const int64_t* ii, const int64_t* jj, int num_frames, int ht,
+                 int wd, int num_edges, int num_kx, int t0, int t1, int iterations, float lm, float ep,
+                 int motion_only, float alpha, float* depth_active_scratch, float* dx_out, float* dz_out,
+                 void* workspace, size_t workspace_bytes, int32_t* dev_status, void* stream);
+
+/* Debug view of the device-built graph index (bit-exact tests).  Runs only the
+ * index construction of vipe_slam_ba_extended into `workspace` and copies:
+ *   kx_out (num_kx) int64 — sorted unique depth frames
+ *   kk_out (t1-t0+num_edges) int64 — inverse map of cat(arange(t0,t1), ii)
+ *   pair_out: up to pair_cap (a, b) pose pairs (int32, local ids) that receive
+ *   a Schur block, sorted; *num_pairs gets the count.
+ * Synchronises `stream`. */
+int vipe_slam_ba_index_debug(const int64_t* ii, const int64_t* jj, int num_frames, int num_edges, int num_kx, int t0,
+                             int t1, int64_t* kx_out, int64_t* kk_out, int32_t* pair_out, int pair_cap,
+                             int* num_pairs, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Replaces slam_ext.frame_distance (reference: geom_kernels.cu:613-768,
+ * 1849-1877).  poses (NV,7), disps (ND,ht,wd), intrinsics (V,4), pi,pj,qi,qj,di
+ * (num,) int64 -> dist_out (num,) f32. */
+int vipe_slam_frame_distance(const float* poses, const float* disps, const float* intrinsics, const int64_t* pi,
+                             const int64_t* pj, const int64_t* qi, const int64_t* qj, const int64_t* di, int num,
+                             int ht, int wd, float beta, float* dist_out, void* stream);
+
+/* Replaces slam_ext.projmap (reference: geom_kernels.cu:526-611, 1879-1903).
+ * -> coords_out (num,ht,wd,3) f32 (third channel 0), valid_out (num,ht,wd,1). */
+int vipe_slam_projmap(const float* poses, const float* disps, const float* intrinsics, const int64_t* ii,
+                      const int64_t* jj, int num, int ht, int wd, float* coords_out, float* valid_out, void* stream);
+
+/* Replaces slam_ext.depth_filter (reference: geom_kernels.cu:770-885,
+ * 1905-1929).  ix (num,) int64, thresh (num,) f32 -> counter_out (num,ht,wd). */
+int vipe_slam_depth_filter(const float* poses, const float* disps, const float* intrinsics, const int64_t* ix,
+                           const float* thresh, int num_frames, int num, int ht, int wd, float* counter_out,
+                           void* stream);
+
+/* Replaces slam_ext.iproj (reference: geom_kernels.cu:887-953, 1931-1950).
+ * -> points_out (num_frames,ht,wd,3) f32. */
+int vipe_slam_iproj(const float* poses, const float* disps, const float* intrinsics, int num_frames, int ht, int wd,
+                    float* points_out, void* stream);
+
+/* =====================================================================
+ * lietorch_ext — group kernels.  group_id: 1 SO3, 2 RxSO3, 3 SE3, 4 Sim3
+ * (reference dispatch: csrc/lietorch_ext/dispatch.h:17-50).  dtype VIPE_F32 or
+ * VIPE_F64.  `batch` group elements; embedding size N, tangent size K per group
+ * (SO3 4/3, RxSO3 5/4, SE3 7/6, Sim3 8/7).  Gradients with respect to group
+ * elements are stored with row stride N (first K entries used), as in the
+ * reference (csrc/lietorch_ext/lietorch_gpu.cu:85-98).
+ * Bindings replaced: csrc/lietorch_ext/lietorch.cpp:306-336.
+ * ===================================================================== */
+int vipe_lie_expm(int group_id, int dtype, int64_t batch, const void* a, void* X_out, void* stream);
+int vipe_lie_expm_backward(int group_id, int dtype, int64_t batch, const void* grad, const void* a, void* da_out,
+                           void* stream);
+int vipe_lie_logm(int group_id, int dtype, int64_t batch, const void* X, void* a_out, void* stream);
+int vipe_lie_logm_backward(int group_id, int dtype, int64_t batch, const void* grad, const void* X, void* dX_out,
+                           void* stream);
+int vipe_lie_inv(int group_id, int dtype, int64_t batch, const void* X, void* Y_out, void* stream);
+int vipe_lie_inv_backward(int group_id, int dtype, int64_t batch, const void* grad, const void* X, void* dX_out,
+                          void* stream);
+int vipe_lie_mul(int group_id, int dtype, int64_t batch, const void* X, const void* Y, void* Z_out, void* stream);
+int vipe_lie_mul_backward(int group_id, int dtype, int64_t batch, const void* grad, const void* X, const void* Y,
+                          void* dX_out, void* dY_out, void* stream);
+int vipe_lie_adj(int group_id, int dtype, int64_t batch, const void* X, const void* a, void* b_out, void* stream);
+int vipe_lie_adj_backward(int group_id, int dtype, int64_t batch, const void* grad, const void* X, const void* a,
+                          void* dX_out, void* da_out, void* stream);
+int vipe_lie_adjT(int group_id, int dtype, int64_t batch, const void* X, const void* a, void* b_out, void* stream);
+int vipe_lie_adjT_backward(int group_id, int dtype, int64_t batch, const void* grad, const void* X, const void* a,
+                           void* dX_out, void* da_out, void* stream);
+int vipe_lie_act(int group_id, int dtype, int64_t batch, const void* X, const void* p, void* q_out, void* stream);
+int vipe_lie_act_backward(int group_id, int dtype, int64_t batch, const void* grad, const void* X, const void* p,
+                          void* dX_out, void* dp_out, void* stream);
+int vipe_lie_act4(int group_id, int dtype, int64_t batch, const void* X, const void* p, void* q_out, void* stream);
+int vipe_lie_act4_backward(int group_id, int dtype, int64_t batch, const void* grad, const void* X, const void* p,
+                           void* dX_out, void* dp_out, void* stream);
+int vipe_lie_as_matrix(int group_id, int dtype, int64_t batch, const void* X, void* T_out, void* stream);
+int vipe_lie_projector(int group_id, int dtype, int64_t batch, const void* X, void* P_out, void* stream);
+int vipe_lie_Jinv(int group_id, int dtype, int64_t batch, const void* X, const void* a, void* b_out, void* stream);
+
+/* =====================================================================
+ * droid_net_ext — correlation lookup and build
+ * Bindings replaced: csrc/droid_net_ext/droid.cpp:75-81.
+ * ===================================================================== */
+
+/* corr_index_forward (correlation_kernels.cu:22-66,115-136).
+ * volume (B, h1, w1, h2, w2) dtype, coords (B, 2, h1, w1) f32
+ * -> corr_out (B, 2r+1, 2r+1, h1, w1) dtype (x-offset major). */
+int vipe_corr_index_forward(int dtype, const void* volume, const float* coords, int B, int h1, int w1, int h2, int w2,
+                            int radius, void* corr_out, void* stream);
+
+/* corr_index_backward (correlation_kernels.cu:68-113,138-158).
+ * -> volume_grad_out (B, h1, w1, h2, w2) dtype (written completely). */
+int vipe_corr_index_backward(int dtype, const float* coords, const void* corr_grad, int B, int h1, int w1, int h2,
+                             int w2, int radius, void* volume_grad_out, void* stream);
+
+/* altcorr_forward (altcorr_kernel.cu:26-138,368-392).
+ * fmap1 (B,H1,W1,C), fmap2 (B,H2,W2,C) dtype, coords (B,S,H1,W1,2) f32
+ * -> corr_out (B,S,(2r+1)^2,H1,W1) dtype. */
+int vipe_altcorr_forward(int dtype, const void* fmap1, const void* fmap2, const float* coords, int B, int S, int H1,
+                         int W1, int H2, int W2, int C, int radius, void* corr_out, void* stream);
+
+/* altcorr_backward (altcorr_kernel.cu:242-366,426-455), f32 only.
+ * -> fmap1_grad_out, fmap2_grad_out (shapes of the fmaps), coords_grad_out
+ * (B,S,H1,W1,2): the reference returns zeros there; this library writes the
+ * exact derivative of the bilinear lookup when `exact_coords_grad` is 1 and
+ * zeros otherwise. */
+int vipe_altcorr_backward(const float* fmap1, const float* fmap2, const float* coords, const float* corr_grad, int B,
+                          int S, int H1, int W1, int H2, int W2, int C, int radius, int exact_coords_grad,
+                          float* fmap1_grad_out, float* fmap2_grad_out, float* coords_grad_out, void* stream);
+
+/* altcorr_index_forward (altcorr_kernel.cu:140-240,394-424).
+ * fmap1 (B,Nf,H,W,C) dtype (level 0), fmap2 levels l=0..L-1 each
+ * (B,Nf,H>>l... floor sizes H2[l],W2[l],C), coords (B,M,H,W,2) f32,
+ * ii, jj (M,) int64 -> corr_out (B,M,L*(2r+1)^2,H,W) f32. */
+int vipe_altcorr_index_forward(int dtype, const void* fmap1, const void* const* fmap2_levels, const int* H2,
+                               const int* W2, int num_levels, const float* coords, const int64_t* ii,
+                               const int64_t* jj, int B, int Nf, int M, int H, int W, int C, int radius,
+                               float* corr_out, void* stream);
+
+/* All-pairs correlation volume with its average-pooled pyramid — the build of
+ * CorrBlock (vipe/slam/networks/droid_net.py:56-69,94-102): for each of the
+ * `num` pairs, level l holds avg_pool^l((fmap1/4)^T (fmap2/4)) over the target
+ * (h2, w2) axes.  fmap1, fmap2 (num, C, ht, wd) in `in_dtype` (VIPE_F16 or
+ * VIPE_BF16), C % 16 == 0.  level_out[l] (num, ht, wd, ht>>l, wd>>l) in
+ * `out_dtype` (VIPE_F32, VIPE_F16 or VIPE_BF16).  ht, wd divisible by
+ * 2^(num_levels-1).  Uses tcgen05 tensor cores with TMEM accumulators. */
+size_t vipe_corr_volume_workspace_size(int num, int C, int ht, int wd);
+int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* fmap1, const void* fmap2, int num, int C, int ht,
+                           int wd, int num_levels, void* const* level_out, void* workspace, size_t workspace_bytes,
+                           void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VIPE_B200_H */
