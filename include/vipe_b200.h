@@ -53,6 +53,14 @@ const char* vipe_status_string(int status);
 /* Last CUDA error text seen by the library on this thread ("" if none). */
 const char* vipe_last_error(void);
 
+/* Launch profiler (no counterpart in the reference).  While enabled, each
+ * kernel launch of the library is bracketed by CUDA events on its stream.
+ * vipe_profile_collect synchronises those events, writes per-kernel-name total
+ * milliseconds and launch counts (names: NUL-terminated, `name_stride` bytes
+ * apart) and clears the record; returns the number of kernel names. */
+void vipe_profile_enable(int on);
+int vipe_profile_collect(char* names, int name_stride, float* total_ms, int* launches, int max_kernels);
+
 /* =====================================================================
  * slam_ext — dense bundle adjustment and geometry helpers
  * ===================================================================== */

@@ -49,7 +49,7 @@ namespace vipe {
 namespace ba {
 
 constexpr int kMaxSlots = 32;          // window poses coupled to one depth frame
-constexpr int kMaxPoses = 1024;        // t1 - t0 (dense reduced system)
+constexpr int kMaxPoses = 127;         // t1 - t0: 6P+1 unknowns fit the staged Cholesky panel
 constexpr int kNT = 105;               // per-edge terms, see term layout below
 constexpr int kEdgeThreads = 256;
 constexpr int kFrameThreads = 256;
@@ -97,6 +97,7 @@ struct Work {
     double* Hm;      // dim * dim
     double* bv;      // dim
     double* df;      // 1
+    double* linv;    // inverse diagonal blocks of the Cholesky factor
 };
 
 __host__ __device__ inline int npt_of(int m) {
@@ -153,7 +154,7 @@ void carve(C& c, const Dims& d, Work* w) {
     take_i(w ? w->pe_list : dummy, 2 * E + 1);
     take_i(w ? w->pf_ptr : dummy, P + 1);
     take_i(w ? w->pf_list : dummy, E + K + 1);
-    auto pf = c.template take<float>((size_t)std::max<size_t>(1, E) * d.CHe * kNT);
+    auto pf = c.template take<float>((size_t)std::max<size_t>(1, E) * d.CHe * 36);
     auto pd = c.template take<double>((size_t)std::max<size_t>(1, E) * kNT);
     auto ps = c.template take<float>((size_t)d.tile_cap * d.CF * 16);
     auto pen = c.template take<float>(K * d.CF + 1);
@@ -161,6 +162,7 @@ void carve(C& c, const Dims& d, Work* w) {
     auto pH = c.template take<double>((size_t)d.dim * d.dim);
     auto pb = c.template take<double>((size_t)d.dim);
     auto pdf = c.template take<double>(4);
+    auto pli = c.template take<double>((size_t)((d.dim + 31) / 32) * 32 * 32);
     if (w) {
         w->epart = (float*)pf;
         w->eterm = (double*)pd;
@@ -170,6 +172,7 @@ void carve(C& c, const Dims& d, Work* w) {
         w->Hm = (double*)pH;
         w->bv = (double*)pb;
         w->df = (double*)pdf;
+        w->linv = (double*)pli;
     }
 }
 
@@ -468,10 +471,20 @@ struct EdgeArgs {
     float iscale;
 };
 
+// Per-pixel accumulation needs only the target-pose block: the source-pose
+// Jacobian of every pixel is Ji = -M Jj with M = Ad^T(Tij) constant per edge
+// (the adjoint pull-back used by the reference, geom_kernels.cu:88-102), so
+//   Hii = M Hjj M^T,  Hij = -M Hjj,  vi = -M vj,  fi = -M fj.
+// Chunk partial layout (kNE floats): [0,21) Hjj upper triangle (n >= m),
+// [21,27) vj, [27,33) fj, 33 hf, 34 vf, 35 flow energy.
+constexpr int kNE = 36;
+
+__host__ __device__ inline int tri6(int r, int c) { return r >= c ? r * (r + 1) / 2 + c : c * (c + 1) / 2 + r; }
+
 template <bool kIntr>
 __global__ void __launch_bounds__(kEdgeThreads) ba_edge_kernel(EdgeArgs A, Dims d, Work w) {
     if (w.status[0]) return;
-    __shared__ float red[kEdgeThreads / 32][kNT];
+    __shared__ float red[kEdgeThreads / 32][kNE];
     const int e = blockIdx.x, c = blockIdx.y;
     const int a = (int)A.ii[e], b = (int)A.jj[e];
     const bool stereo = a == b;
@@ -479,16 +492,14 @@ __global__ void __launch_bounds__(kEdgeThreads) ba_edge_kernel(EdgeArgs A, Dims 
     edge_pose(A.poses, a, b, tij, qij);
     const float fx = A.intr[0], fy = A.intr[1], cx = A.intr[2], cy = A.intr[3];
 
-    float H[78];
-    float vv[12];
-    float F[12];
+    float H[21], vj[6], fj[6];
     float hf = 0.f, vf = 0.f, en = 0.f;
 #pragma unroll
-    for (int n = 0; n < 78; n++) H[n] = 0.f;
+    for (int n = 0; n < 21; n++) H[n] = 0.f;
 #pragma unroll
-    for (int n = 0; n < 12; n++) {
-        vv[n] = 0.f;
-        F[n] = 0.f;
+    for (int n = 0; n < 6; n++) {
+        vj[n] = 0.f;
+        fj[n] = 0.f;
     }
     const int HW = d.HW, W = d.W;
     const int p0 = c * d.chunk_e, p1 = min(HW, p0 + d.chunk_e);
@@ -503,77 +514,113 @@ __global__ void __launch_bounds__(kEdgeThreads) ba_edge_kernel(EdgeArgs A, Dims 
         en += L.we[0] * L.r[0] * L.r[0] + L.we[1] * L.r[1] * L.r[1];
 #pragma unroll
         for (int ch = 0; ch < 2; ch++) {
-            float J[12];
-#pragma unroll
-            for (int n = 0; n < 6; n++) {
-                J[n] = L.Ji[ch][n];
-                J[6 + n] = L.Jj[ch][n];
-            }
             const float wt = L.w[ch];
             int l = 0;
 #pragma unroll
-            for (int n = 0; n < 12; n++) {
-                const float wj = wt * J[n];
+            for (int n = 0; n < 6; n++) {
+                const float wjn = wt * L.Jj[ch][n];
 #pragma unroll
-                for (int m = 0; m <= n; m++) H[l++] += wj * J[m];
+                for (int m = 0; m <= n; m++) H[l++] += wjn * L.Jj[ch][m];
             }
             const float wr = wt * L.r[ch];
 #pragma unroll
-            for (int n = 0; n < 12; n++) vv[n] += wr * J[n];
+            for (int n = 0; n < 6; n++) vj[n] += wr * L.Jj[ch][n];
             if (kIntr) {
                 const float wf = wt * L.Jf[ch];
 #pragma unroll
-                for (int n = 0; n < 12; n++) F[n] += wf * J[n];
+                for (int n = 0; n < 6; n++) fj[n] += wf * L.Jj[ch][n];
                 hf += wf * L.Jf[ch];
                 vf += wr * L.Jf[ch];
             }
         }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float vals[kNE];
 #pragma unroll
-    for (int n = 0; n < 78; n++) {
-        const float s = warp_sum(H[n]);
-        if (lane == 0) red[warp][n] = s;
-    }
+    for (int n = 0; n < 21; n++) vals[n] = H[n];
 #pragma unroll
-    for (int n = 0; n < 12; n++) {
-        const float s = warp_sum(vv[n]);
-        if (lane == 0) red[warp][kTV + n] = s;
+    for (int n = 0; n < 6; n++) {
+        vals[21 + n] = vj[n];
+        vals[27 + n] = fj[n];
     }
-    if (kIntr) {
+    vals[33] = hf;
+    vals[34] = vf;
+    vals[35] = en;
 #pragma unroll
-        for (int n = 0; n < 12; n++) {
-            const float s = warp_sum(F[n]);
-            if (lane == 0) red[warp][kTF + n] = s;
-        }
-        const float s1 = warp_sum(hf), s2 = warp_sum(vf);
-        if (lane == 0) {
-            red[warp][kTHF] = s1;
-            red[warp][kTVF] = s2;
-        }
-    } else if (lane == 0) {
-        for (int n = kTF; n < kTEN; n++) red[warp][n] = 0.f;
-    }
-    {
-        const float s = warp_sum(en);
-        if (lane == 0) red[warp][kTEN] = s;
+    for (int n = 0; n < kNE; n++) {
+        if (!kIntr && n >= 27 && n < 35) continue;
+        const float sv = warp_sum(vals[n]);
+        if (lane == 0) red[warp][n] = sv;
     }
     __syncthreads();
-    for (int n = threadIdx.x; n < kNT; n += kEdgeThreads) {
-        float s = 0.f;
+    for (int n = threadIdx.x; n < kNE; n += kEdgeThreads) {
+        float sv = 0.f;
+        if (kIntr || n < 27 || n == 35) {
 #pragma unroll
-        for (int q = 0; q < kEdgeThreads / 32; q++) s += red[q][n];
-        w.epart[((size_t)e * d.CHe + c) * kNT + n] = s;
+            for (int q = 0; q < kEdgeThreads / 32; q++) sv += red[q][n];
+        }
+        w.epart[((size_t)e * d.CHe + c) * kNE + n] = sv;
     }
 }
 
-__global__ void ba_edge_reduce(Dims d, Work w) {
+// Chunk partials -> FP64 per-edge terms in the 12x12 layout (kNT values).
+__global__ void ba_edge_reduce(EdgeArgs A, Dims d, Work w) {
     if (w.status[0]) return;
-    const int e = blockIdx.x;
-    for (int n = threadIdx.x; n < kNT; n += blockDim.x) {
-        double s = 0.0;
-        for (int c = 0; c < d.CHe; c++) s += (double)w.epart[((size_t)e * d.CHe + c) * kNT + n];
-        w.eterm[(size_t)e * kNT + n] = s;
+    __shared__ double t[kNE];
+    __shared__ double M[6][6];
+    const int e = blockIdx.x, tid = threadIdx.x;
+    for (int n = tid; n < kNE; n += blockDim.x) {
+        double sv = 0.0;
+        for (int c = 0; c < d.CHe; c++) sv += (double)w.epart[((size_t)e * d.CHe + c) * kNE + n];
+        t[n] = sv;
+    }
+    if (tid < 6) {
+        float tij[3], qij[4];
+        edge_pose(A.poses, (int)A.ii[e], (int)A.jj[e], tij, qij);
+        float ek[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, col[6];
+        ek[tid] = 1.f;
+        adj_t(tij, qij, ek, col);
+        for (int r = 0; r < 6; r++) M[r][tid] = (double)col[r];
+    }
+    __syncthreads();
+    double* out = w.eterm + (size_t)e * kNT;
+    // full 12x12 over J = [Ji, Jj]: thread per (row, col) of the lower triangle
+    for (int q = tid; q < 78; q += blockDim.x) {
+        int r = 0;
+        while ((r + 1) * (r + 2) / 2 <= q) r++;
+        const int c = q - r * (r + 1) / 2;  // c <= r
+        double v;
+        if (r >= 6 && c >= 6) {
+            v = t[tri6(r - 6, c - 6)];  // Hjj
+        } else if (r >= 6) {
+            // entry (Jj_{r-6}, Ji_c) = sum w Jj Ji = -(Hjj M^T)[r-6][c]
+            double sacc = 0.0;
+            for (int k = 0; k < 6; k++) sacc += t[tri6(r - 6, k)] * M[c][k];
+            v = -sacc;
+        } else {
+            // Hii = M Hjj M^T
+            double sacc = 0.0;
+            for (int k = 0; k < 6; k++)
+                for (int l = 0; l < 6; l++) sacc += M[r][k] * t[tri6(k, l)] * M[c][l];
+            v = sacc;
+        }
+        out[q] = v;
+    }
+    if (tid < 6) {
+        double vi = 0.0, fi = 0.0;
+        for (int k = 0; k < 6; k++) {
+            vi -= M[tid][k] * t[21 + k];
+            fi -= M[tid][k] * t[27 + k];
+        }
+        out[kTV + tid] = vi;
+        out[kTV + 6 + tid] = t[21 + tid];
+        out[kTF + tid] = fi;
+        out[kTF + 6 + tid] = t[27 + tid];
+    }
+    if (tid == 0) {
+        out[kTHF] = t[33];
+        out[kTVF] = t[34];
+        out[kTEN] = t[35];
     }
 }
 
@@ -895,170 +942,227 @@ __global__ void ba_assemble_rhs(Dims d, Work w, int with_frames, int with_intr) 
 
 // ---------------------------------------------------------------- dense FP64 Cholesky
 
-constexpr int kCholThreads = 1024;
+constexpr int kCholThreads = 512;
 constexpr int kNB = 32;
+constexpr int kPanelRows = 768;  // systems up to 768 unknowns stage their panel in shared memory
 
-// Damped LL^T of H (dim x dim, row-major, lower triangle used) and solve
-// H x = b.  diag += ep + lm*diag for pose rows, iep + ilm*diag for the focal row
-// (geom_kernels.cu:1269-1288, :1389-1417).  On a non-positive pivot x = 0 and
-// VIPE_WARN_SOLVER is raised, as the reference falls back to dx = 0.
-__global__ void __launch_bounds__(kCholThreads)
+__device__ __forceinline__ double damped(double dg, bool scalar, float lm, float ep, float ilm, float iep) {
+    return dg + (scalar ? ((double)iep + (double)ilm * dg) : ((double)ep + (double)lm * dg));
+}
+
+// Damped LL^T of H (n x n, row-major, lower triangle used) and solve H x = b,
+// one CTA.  diag += ep + lm*diag for pose rows, iep + ilm*diag for the focal
+// row (geom_kernels.cu:1269-1288, :1389-1417).  Right-looking over 32-column
+// panels staged TRANSPOSED in shared memory (pT[c][r], rows contiguous, so a
+// thread reads the 4 rows of its tile as two 16-byte vectors without bank
+// conflicts):
+//   * the 32x32 diagonal block is factored by one warp in registers (lane i owns
+//     row i; identity padding past n) and inverted (lane j solves column j);
+//   * the panel below is X = A L_kk^-T, an independent-accumulator product;
+//   * the forward substitution rides along (y_k = L_kk^-1 b_k, b -= X y_k);
+//   * the trailing update uses 4x4 register tiles fed from the staged panel.
+// The inverse diagonal blocks are kept (Linv) for the backward substitution.
+// On a non-positive pivot x = 0 and VIPE_WARN_SOLVER is raised, as the
+// reference falls back to dx = 0 (geom_kernels.cu:1283-1285).
+__host__ __device__ inline int chol_ldr(int dim) {
+    // transposed panel row length: >= max(dim, 32) + 4 (tiles read up to 3 rows
+    // past the last panel row, which are zero-filled), == 2 (mod 4) doubles so
+    // that 16-byte row-pair loads stay aligned
+    int r = (dim < kNB ? kNB : dim) + 4;
+    r = (r + 3) & ~3;
+    return r + 2;
+}
+
+__global__ void __launch_bounds__(kCholThreads, 1)
     ba_cholesky_kernel(Dims d, Work w, float lm, float ep, float ilm, float iep, int with_intr, float* dx_out,
                        int32_t* warn) {
     if (w.status[0]) return;
-    __shared__ double Lkk[kNB][kNB + 1];
+    extern __shared__ double pT[];  // kNB columns x LDR rows (transposed panel)
+    __shared__ double Li[kNB][kNB + 1];  // inverse of the diagonal block, Li[row][col]
     __shared__ double ysh[kNB];
     __shared__ int fail;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = with_intr ? d.dim : d.dim - 1;
     const int ld = d.dim;
+    const int np = 6 * d.P;
+    const int LDR = chol_ldr(d.dim);
     double* A = w.Hm;
     double* x = w.bv;
+    double* Linv = w.linv;  // nblk x kNB x kNB
     if (tid == 0) fail = 0;
-    for (int i = tid; i < n; i += kCholThreads) {
-        const double dg = A[(size_t)i * ld + i];
-        const bool sc = i >= 6 * d.P;
-        A[(size_t)i * ld + i] = dg + (sc ? ((double)iep + (double)ilm * dg) : ((double)ep + (double)lm * dg));
-    }
+    for (int i = tid; i < n; i += kCholThreads)
+        A[(size_t)i * ld + i] = damped(A[(size_t)i * ld + i], i >= np, lm, ep, ilm, iep);
     __syncthreads();
     const int nblk = (n + kNB - 1) / kNB;
     for (int kb = 0; kb < nblk; kb++) {
-        const int k0 = kb * kNB, kn = min(kNB, n - k0);
-        for (int q = tid; q < kNB * kNB; q += kCholThreads) {
-            const int r = q / kNB, cc = q % kNB;
-            Lkk[r][cc] = (r < kn && cc < kn) ? A[(size_t)(k0 + r) * ld + k0 + cc] : 0.0;
+        const int k0 = kb * kNB, kn = min(kNB, n - k0), nr = n - k0;
+        for (int q = tid; q < nr * kNB; q += kCholThreads) {
+            const int r = q / kNB, c = q % kNB;
+            pT[c * LDR + r] = c < kn ? A[(size_t)(k0 + r) * ld + k0 + c] : 0.0;
         }
         __syncthreads();
         if (warp == 0) {
-            for (int j = 0; j < kn; j++) {
-                const double djj = Lkk[j][j];
-                const bool bad = !(djj > 0.0);
-                const double l = bad ? 1.0 : sqrt(djj);
-                if (bad && lane == 0) fail = 1;
-                __syncwarp();
-                if (lane == j) Lkk[j][j] = l;
-                if (lane > j && lane < kn) Lkk[lane][j] /= l;
-                __syncwarp();
-                if (lane > j && lane < kn) {
-                    const double lij = Lkk[lane][j];
-                    for (int cc = j + 1; cc <= lane; cc++) Lkk[lane][cc] -= lij * Lkk[cc][j];
+            // register Cholesky of the (identity-padded) diagonal block; lane = row
+            double rv[kNB];
+#pragma unroll
+            for (int c = 0; c < kNB; c++)
+                rv[c] = (lane < kn && c < kn) ? pT[c * LDR + lane] : (lane == c ? 1.0 : 0.0);
+            bool bad = false;
+#pragma unroll
+            for (int j = 0; j < kNB; j++) {
+                const double piv = __shfl_sync(0xffffffffu, rv[j], j);
+                bad |= !(piv > 0.0);
+                const double l = piv > 0.0 ? sqrt(piv) : 1.0;
+                rv[j] = (lane == j) ? l : (lane > j ? rv[j] / l : rv[j]);
+#pragma unroll
+                for (int c = j + 1; c < kNB; c++) {
+                    const double lcj = __shfl_sync(0xffffffffu, rv[j], c);
+                    if (lane >= c) rv[c] -= rv[j] * lcj;
                 }
-                __syncwarp();
             }
+            if (bad && lane == 0) fail = 1;
+            // the factor goes to Li's shared buffer first (row-major), then is inverted in place by columns
+#pragma unroll
+            for (int c = 0; c < kNB; c++) {
+                const double v = (c <= lane) ? rv[c] : 0.0;
+                if (lane < kn) pT[c * LDR + lane] = v;
+                Li[lane][c] = v;  // L (padded) row-major, temporarily
+            }
+            __syncwarp();
+            // inverse: lane j solves L z = e_j; coefficients L[t][q] are warp broadcasts
+            double z[kNB];
+#pragma unroll
+            for (int t = 0; t < kNB; t++) {
+                double sacc = (t == lane) ? 1.0 : 0.0;
+#pragma unroll
+                for (int q = 0; q < t; q++) sacc -= Li[t][q] * z[q];
+                z[t] = (t < lane) ? 0.0 : sacc / Li[t][t];
+            }
+            __syncwarp();
+#pragma unroll
+            for (int t = 0; t < kNB; t++) Li[t][lane] = z[t];
         }
         __syncthreads();
         if (fail) break;
-        for (int q = tid; q < kn * kn; q += kCholThreads) {
-            const int r = q / kn, cc = q % kn;
-            if (cc <= r) A[(size_t)(k0 + r) * ld + k0 + cc] = Lkk[r][cc];
-        }
-        // panel: rows below solve X Lkk^T = A
-        const int r0 = k0 + kn;
-        for (int i = r0 + tid; i < n; i += kCholThreads) {
-            double* row = A + (size_t)i * ld + k0;
-            for (int cc = 0; cc < kn; cc++) {
-                double s = row[cc];
-                for (int t = 0; t < cc; t++) s -= row[t] * Lkk[cc][t];
-                row[cc] = s / Lkk[cc][cc];
+        for (int q = tid; q < kNB * kNB; q += kCholThreads)
+            Linv[(size_t)kb * kNB * kNB + q] = Li[q / kNB][q % kNB];
+        // panel below the diagonal block: X = A L_kk^-T  (X[r][c] = sum_{t<=c} A[r][t] Li[c][t])
+        // (Li is read through a volatile pointer so the compiler does not hoist
+        // all 528 coefficients out of the row loop into registers)
+        const volatile double* Lv = &Li[0][0];
+        for (int r = kn + tid; r < nr; r += kCholThreads) {
+            double a[kNB];
+#pragma unroll
+            for (int t = 0; t < kNB; t++) a[t] = pT[t * LDR + r];
+#pragma unroll
+            for (int c0 = 0; c0 < kNB; c0 += 4) {
+                double o0 = 0.0, o1 = 0.0, o2 = 0.0, o3 = 0.0;
+#pragma unroll
+                for (int t = 0; t < c0 + 4; t++) {
+                    const double at = a[t];
+                    if (t <= c0) o0 += at * Lv[c0 * (kNB + 1) + t];
+                    if (t <= c0 + 1) o1 += at * Lv[(c0 + 1) * (kNB + 1) + t];
+                    if (t <= c0 + 2) o2 += at * Lv[(c0 + 2) * (kNB + 1) + t];
+                    o3 += at * Lv[(c0 + 3) * (kNB + 1) + t];
+                }
+                pT[c0 * LDR + r] = (c0 < kn) ? o0 : 0.0;
+                pT[(c0 + 1) * LDR + r] = (c0 + 1 < kn) ? o1 : 0.0;
+                pT[(c0 + 2) * LDR + r] = (c0 + 2 < kn) ? o2 : 0.0;
+                pT[(c0 + 3) * LDR + r] = (c0 + 3 < kn) ? o3 : 0.0;
             }
         }
+        // forward substitution of this block: y_k = L_kk^-1 b_k
+        if (tid < kNB) {
+            double yv = 0.0;
+            for (int t = 0; t <= tid; t++) yv += Li[tid][t] * (t < kn ? x[k0 + t] : 0.0);
+            ysh[tid] = tid < kn ? yv : 0.0;
+        }
         __syncthreads();
-        // trailing update (lower triangle), 4x4 tiles
-        const int nr = n - r0;
-        if (nr > 0) {
-            const int n4 = (nr + 3) / 4;
-            const long ntile = (long)n4 * (n4 + 1) / 2;
-            for (long t = tid; t < ntile; t += kCholThreads) {
-                // decode t -> (bi, bj), bj <= bi, row-major lower triangle
+        if (tid < kn) x[k0 + tid] = ysh[tid];
+        for (int q = tid; q < nr * kNB; q += kCholThreads) {
+            const int r = q / kNB, c = q % kNB;
+            if (c < kn && (r >= kn || c <= r)) A[(size_t)(k0 + r) * ld + k0 + c] = pT[c * LDR + r];
+        }
+        for (int r = kn + tid; r < nr; r += kCholThreads) {
+            double sacc = 0.0;
+#pragma unroll 8
+            for (int t = 0; t < kNB; t++) sacc += pT[t * LDR + r] * ysh[t];
+            x[k0 + r] -= sacc;
+        }
+        // trailing update of the lower triangle, 4x4 register tiles from the staged panel
+        // (panel rows past nr are zero-filled below, so tiles need no row predicates)
+        const int nt2 = nr - kn;
+        if (nt2 > 0) {
+            const int n4 = (nt2 + 3) / 4;
+            for (int q = tid; q < kNB * 4; q += kCholThreads) {
+                const int c = q >> 2, r = nr + (q & 3);
+                if (r < LDR) pT[c * LDR + r] = 0.0;
+            }
+            __syncthreads();
+            const int ntile = n4 * (n4 + 1) / 2;
+            for (int t = tid; t < ntile; t += kCholThreads) {
                 int bi = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-                while ((long)bi * (bi + 1) / 2 > t) bi--;
-                while ((long)(bi + 1) * (bi + 2) / 2 <= t) bi++;
-                const int bj = (int)(t - (long)bi * (bi + 1) / 2);
+                while (bi * (bi + 1) / 2 > t) bi--;
+                while ((bi + 1) * (bi + 2) / 2 <= t) bi++;
+                const int bj = t - bi * (bi + 1) / 2;
+                const int ri = kn + 4 * bi, rj = kn + 4 * bj;  // panel rows (multiples of 2)
                 double c4[4][4];
 #pragma unroll
                 for (int r = 0; r < 4; r++)
 #pragma unroll
-                    for (int cc = 0; cc < 4; cc++) c4[r][cc] = 0.0;
-                const int ib = r0 + 4 * bi, jb = r0 + 4 * bj;
-                for (int t2 = 0; t2 < kn; t2++) {
-                    double li[4], lj[4];
-#pragma unroll
-                    for (int r = 0; r < 4; r++) {
-                        li[r] = (ib + r < n) ? A[(size_t)(ib + r) * ld + k0 + t2] : 0.0;
-                        lj[r] = (jb + r < n) ? A[(size_t)(jb + r) * ld + k0 + t2] : 0.0;
-                    }
+                    for (int c = 0; c < 4; c++) c4[r][c] = 0.0;
+#pragma unroll 4
+                for (int t2 = 0; t2 < kNB; t2++) {
+                    const double2* ci = reinterpret_cast<const double2*>(pT + t2 * LDR + ri);
+                    const double2* cj = reinterpret_cast<const double2*>(pT + t2 * LDR + rj);
+                    const double2 i01 = ci[0], i23 = ci[1], j01 = cj[0], j23 = cj[1];
+                    const double li[4] = {i01.x, i01.y, i23.x, i23.y};
+                    const double lj[4] = {j01.x, j01.y, j23.x, j23.y};
 #pragma unroll
                     for (int r = 0; r < 4; r++)
 #pragma unroll
-                        for (int cc = 0; cc < 4; cc++) c4[r][cc] += li[r] * lj[cc];
+                        for (int c = 0; c < 4; c++) c4[r][c] += li[r] * lj[c];
                 }
 #pragma unroll
                 for (int r = 0; r < 4; r++)
 #pragma unroll
-                    for (int cc = 0; cc < 4; cc++) {
-                        const int gi = ib + r, gj = jb + cc;
-                        if (gi < n && gj < n && gj <= gi) A[(size_t)gi * ld + gj] -= c4[r][cc];
+                    for (int c = 0; c < 4; c++) {
+                        const int gi = k0 + ri + r, gj = k0 + rj + c;
+                        if (gi < n && gj <= gi) A[(size_t)gi * ld + gj] -= c4[r][c];
                     }
             }
         }
         __syncthreads();
     }
     if (!fail) {
-        // forward: L y = b (blocked by kNB)
-        for (int kb = 0; kb < nblk; kb++) {
-            const int k0 = kb * kNB, kn = min(kNB, n - k0);
-            if (warp == 0) {
-                double yv = lane < kn ? x[k0 + lane] : 0.0;
-                for (int j = 0; j < kn; j++) {
-                    const double lj = lane < kn ? A[(size_t)(k0 + lane) * ld + k0 + j] : 0.0;
-                    double yj = __shfl_sync(0xffffffffu, yv, j);
-                    yj /= A[(size_t)(k0 + j) * ld + k0 + j];
-                    if (lane == j) yv = yj;
-                    if (lane > j) yv -= lj * yj;
-                }
-                if (lane < kn) {
-                    x[k0 + lane] = yv;
-                    ysh[lane] = yv;
-                }
-            }
-            __syncthreads();
-            for (int i = k0 + kn + tid; i < n; i += kCholThreads) {
-                double s = 0.0;
-                for (int t = 0; t < kn; t++) s += A[(size_t)i * ld + k0 + t] * ysh[t];
-                x[i] -= s;
-            }
-            __syncthreads();
-        }
-        // backward: L^T x = y
+        // backward substitution L^T x = y: x_k = L_kk^-T y_k, then y_i -= L_ki^T x_k for i < k0
         for (int kb = nblk - 1; kb >= 0; kb--) {
             const int k0 = kb * kNB, kn = min(kNB, n - k0);
-            if (warp == 0) {
-                double yv = lane < kn ? x[k0 + lane] : 0.0;
-                for (int j = kn - 1; j >= 0; j--) {
-                    const double lj = lane < kn ? A[(size_t)(k0 + j) * ld + k0 + lane] : 0.0;  // L[j][lane]
-                    double xj = __shfl_sync(0xffffffffu, yv, j);
-                    xj /= A[(size_t)(k0 + j) * ld + k0 + j];
-                    if (lane == j) yv = xj;
-                    if (lane < j) yv -= lj * xj;
-                }
-                if (lane < kn) {
-                    x[k0 + lane] = yv;
-                    ysh[lane] = yv;
-                }
+            for (int q = tid; q < kNB * kNB; q += kCholThreads)
+                Li[q / kNB][q % kNB] = Linv[(size_t)kb * kNB * kNB + q];
+            if (tid < kNB) ysh[tid] = tid < kn ? x[k0 + tid] : 0.0;
+            __syncthreads();
+            double xv = 0.0;
+            if (tid < kNB)
+                for (int t = tid; t < kNB; t++) xv += Li[t][tid] * ysh[t];  // (L^-T)[tid][t] = Li[t][tid]
+            __syncthreads();
+            if (tid < kNB) {
+                ysh[tid] = tid < kn ? xv : 0.0;
+                if (tid < kn) x[k0 + tid] = xv;
             }
             __syncthreads();
-            // x[i] -= sum_t L[k0+t][i] * x[k0+t] for i < k0
             for (int i = tid; i < k0; i += kCholThreads) {
-                double s = 0.0;
-                for (int t = 0; t < kn; t++) s += A[(size_t)(k0 + t) * ld + i] * ysh[t];
-                x[i] -= s;
+                double sacc = 0.0;
+#pragma unroll 8
+                for (int t = 0; t < kn; t++) sacc += A[(size_t)(k0 + t) * ld + i] * ysh[t];
+                x[i] -= sacc;
             }
             __syncthreads();
         }
     }
-    for (int i = tid; i < 6 * d.P; i += kCholThreads) dx_out[i] = fail ? 0.f : (float)x[i];
+    for (int i = tid; i < np; i += kCholThreads) dx_out[i] = fail ? 0.f : (float)x[i];
     if (tid == 0) {
-        w.df[0] = (fail || !with_intr) ? 0.0 : x[6 * d.P];
+        w.df[0] = (fail || !with_intr) ? 0.0 : x[np];
         if (fail && warn) atomicOr(warn, VIPE_WARN_SOLVER);
     }
 }
@@ -1177,7 +1281,10 @@ int check_dims(int num_frames, int ht, int wd, int num_edges, int num_kx, int t0
 bool g_smem_set[64] = {false};
 
 int launch_index(const int64_t* ii, const int64_t* jj, const Dims& d, const Work& w, cudaStream_t st) {
-    ba_index_kernel<<<1, kIndexThreads, 0, st>>>(ii, jj, d, w);
+    {
+        VIPE_PROF("ba_index", st);
+        ba_index_kernel<<<1, kIndexThreads, 0, st>>>(ii, jj, d, w);
+    }
     VIPE_LAUNCH_CHECK();
     return VIPE_OK;
 }
@@ -1225,6 +1332,8 @@ extern "C" int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* in
                                            kStageFloats * 4));
         VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            kStageFloats * 4));
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_cholesky_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           chol_ldr(kPanelRows) * kNB * (int)sizeof(double)));
         g_smem_set[dev] = true;
     }
     if ((rc = launch_index(ii, jj, d, w, st)) != VIPE_OK) return rc;
@@ -1234,46 +1343,65 @@ extern "C" int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* in
     FrameArgs fa{poses_io, disps_io, disps_sens, intrinsics_io, targets, weights, eta, depth_active, jj, alpha,
                  intrinsics_scale};
     const long npairs = (long)d.P * (d.P + 1) / 2;
+    const size_t chol_smem = (size_t)chol_ldr(d.dim) * kNB * sizeof(double);
     for (int itr = 0; itr < iterations; itr++) {
         if (d.E > 0) {
             dim3 ge(d.E, d.CHe);
+            {
+            VIPE_PROF("ba_edge", st);
             if (intr)
                 ba_edge_kernel<true><<<ge, kEdgeThreads, 0, st>>>(ea, d, w);
             else
                 ba_edge_kernel<false><<<ge, kEdgeThreads, 0, st>>>(ea, d, w);
+            }
             VIPE_LAUNCH_CHECK();
-            ba_edge_reduce<<<d.E, 128, 0, st>>>(d, w);
+            {
+                VIPE_PROF("ba_edge_reduce", st);
+                ba_edge_reduce<<<d.E, 128, 0, st>>>(ea, d, w);
+            }
             VIPE_LAUNCH_CHECK();
         }
         if (!motion_only) {
             dim3 gf(d.K, d.CF);
+            VIPE_PROF("ba_frame", st);
             if (intr)
                 ba_frame_kernel<true><<<gf, kFrameThreads, kStageFloats * 4, st>>>(fa, d, w);
             else
                 ba_frame_kernel<false><<<gf, kFrameThreads, kStageFloats * 4, st>>>(fa, d, w);
             VIPE_LAUNCH_CHECK();
         }
-        ba_assemble_blocks<<<ceil_div(npairs, 8), 256, 0, st>>>(ii, jj, d, w, motion_only ? 0 : 1);
+        {
+            VIPE_PROF("ba_assemble", st);
+            ba_assemble_blocks<<<ceil_div(npairs, 8), 256, 0, st>>>(ii, jj, d, w, motion_only ? 0 : 1);
         VIPE_LAUNCH_CHECK();
-        ba_assemble_rhs<<<ceil_div(d.P + 1, 8), 256, 0, st>>>(d, w, motion_only ? 0 : 1, intr ? 1 : 0);
+            ba_assemble_rhs<<<ceil_div(d.P + 1, 8), 256, 0, st>>>(d, w, motion_only ? 0 : 1, intr ? 1 : 0);
+        }
         VIPE_LAUNCH_CHECK();
         if (compute_energy) {
+            VIPE_PROF("ba_energy", st);
             ba_energy_kernel<<<1, 256, 0, st>>>(d, w, motion_only ? 0 : 1, energy_out, itr);
             VIPE_LAUNCH_CHECK();
         }
-        ba_cholesky_kernel<<<1, kCholThreads, 0, st>>>(d, w, lm, ep, intrinsics_lm, intrinsics_ep, intr ? 1 : 0,
-                                                       dx_out, dev_status);
+        {
+        VIPE_PROF("ba_cholesky", st);
+        ba_cholesky_kernel<<<1, kCholThreads, chol_smem, st>>>(d, w, lm, ep, intrinsics_lm, intrinsics_ep,
+                                                               intr ? 1 : 0, dx_out, dev_status);
+        }
         VIPE_LAUNCH_CHECK();
         if (!motion_only) {
             dim3 gb(d.K, d.CF);
+            VIPE_PROF("ba_backsub", st);
             if (intr)
                 ba_backsub_kernel<true><<<gb, 256, 0, st>>>(fa, d, w, dx_out, disps_io, dz_out);
             else
                 ba_backsub_kernel<false><<<gb, 256, 0, st>>>(fa, d, w, dx_out, disps_io, dz_out);
             VIPE_LAUNCH_CHECK();
         }
-        ba_retract_kernel<<<ceil_div(d.P, 128), 128, 0, st>>>(d, w, dx_out, poses_io, intrinsics_io, intr ? 1 : 0,
-                                                              intrinsics_scale);
+        {
+            VIPE_PROF("ba_retract", st);
+            ba_retract_kernel<<<ceil_div(d.P, 128), 128, 0, st>>>(d, w, dx_out, poses_io, intrinsics_io,
+                                                                  intr ? 1 : 0, intrinsics_scale);
+        }
         VIPE_LAUNCH_CHECK();
     }
     if (dev_status) {

@@ -16,6 +16,22 @@ namespace vipe {
 // Records the last CUDA error string for vipe_last_error().
 void set_last_error(const char* msg);
 
+// Launch profiler (vipe_profile_enable / vipe_profile_collect).
+bool prof_enabled();
+int prof_begin(const char* name, cudaStream_t st);
+void prof_end(int id, cudaStream_t st);
+
+// RAII bracket of one launch: VIPE_PROF("kernel", stream) before the launch.
+struct ProfScope {
+    int id;
+    cudaStream_t st;
+    ProfScope(const char* n, cudaStream_t s) : id(prof_enabled() ? prof_begin(n, s) : -1), st(s) {}
+    ~ProfScope() {
+        if (id >= 0) prof_end(id, st);
+    }
+};
+#define VIPE_PROF(name, st) ::vipe::ProfScope _vipe_prof_scope_##__LINE__(name, st)
+
 #define VIPE_CUDA_TRY(expr)                                  \
     do {                                                     \
         cudaError_t _e = (expr);                             \
