@@ -225,7 +225,9 @@ int vipe_altcorr_index_forward(int dtype, const void* fmap1, const void* const* 
  * (h2, w2) axes.  fmap1, fmap2 (num, C, ht, wd) in `in_dtype` (VIPE_F16 or
  * VIPE_BF16), C % 16 == 0.  level_out[l] (num, ht, wd, ht>>l, wd>>l) in
  * `out_dtype` (VIPE_F32, VIPE_F16 or VIPE_BF16).  ht, wd divisible by
- * 2^(num_levels-1).  Uses tcgen05 tensor cores with TMEM accumulators. */
+ * 2^(num_levels-1).  Uses tcgen05 tensor cores with TMEM accumulators.
+ * The first int32 of `workspace` becomes nonzero if a bounded wait inside the
+ * kernel expired (the output is then incomplete). */
 size_t vipe_corr_volume_workspace_size(int num, int C, int ht, int wd);
 int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* fmap1, const void* fmap2, int num, int C, int ht,
                            int wd, int num_levels, void* const* level_out, void* workspace, size_t workspace_bytes,

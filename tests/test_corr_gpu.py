@@ -1,0 +1,141 @@
+"""Correlation ops on the GPU against the FP64 oracle (oracle/corr.py).
+
+* lookups (corr_index fwd/bwd, altcorr fwd/bwd, altcorr_index fwd) in f32
+  (atol 1e-4), f16 inputs (atol 2e-3 on O(1) outputs), f64 (atol 1e-10);
+  out-of-map coordinates exercise the zero padding;
+* the reference's own check (tests/test_altcorr_indexed.py): 7 fp16 frames,
+  128 channels, 48x64, 5 edges, coords = grid + 0.4 N(0,1), seed 2028 —
+  indexed vs per-level lookup at atol 2e-4, rtol 1e-4;
+* the tcgen05 volume build + fused pyramid vs the FP64 oracle evaluated on the
+  same BF16 / FP16-rounded inputs: |err| <= 1e-4 * max|V| (FP32 accumulation).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import oracle.corr as oc
+
+pytestmark = pytest.mark.gpu
+
+
+def _dne():
+    from vipe_b200.ext import droid_net_ext
+
+    return droid_net_ext
+
+
+def _grid_coords(B, H, W, gen, sigma, spill=0.0):
+    yy, xx = torch.meshgrid(torch.arange(H), torch.arange(W), indexing="ij")
+    c = torch.stack([xx, yy], 0).float()[None].repeat(B, 1, 1, 1)
+    c = c + sigma * torch.randn(c.shape, generator=gen)
+    if spill:
+        c[:, :, :2] -= spill  # push some lookups off the map
+    return c
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float16, torch.float64])
+def test_corr_index_forward_backward(dtype):
+    g = torch.Generator().manual_seed(11)
+    B, h1, w1, h2, w2 = 2, 6, 8, 6, 8
+    vol = torch.randn(B, h1, w1, h2, w2, generator=g)
+    coords = _grid_coords(B, h1, w1, g, 1.5, spill=5.0)
+    out = _dne().corr_index_forward(vol.to(dtype).cuda(), coords.cuda(), 3)[0]
+    want = oc.corr_index_forward(vol.to(dtype).double().numpy(), coords.numpy(), 3)
+    tol = {torch.float32: 1e-5, torch.float16: 4e-3, torch.float64: 1e-12}[dtype]
+    np.testing.assert_allclose(out.double().cpu().numpy(), want, atol=tol)
+    grad = torch.randn(B, 7, 7, h1, w1, generator=g)
+    vg = _dne().corr_index_backward(vol.to(dtype).cuda(), coords.cuda(), grad.to(dtype).cuda(), 3)[0]
+    wv = oc.corr_index_backward(vol.shape, coords.numpy(), grad.to(dtype).double().numpy(), 3)
+    np.testing.assert_allclose(vg.double().cpu().numpy(), wv, atol=tol * 4)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float16])
+def test_altcorr_forward(dtype):
+    g = torch.Generator().manual_seed(12)
+    B, S, H, W, C = 2, 2, 8, 16, 64
+    f1 = torch.randn(B, H, W, C, generator=g) / 8
+    f2 = torch.randn(B, H, W, C, generator=g) / 8
+    coords = torch.stack([_grid_coords(B, H, W, g, 1.5, spill=4.0).permute(0, 2, 3, 1) for _ in range(S)], 1)
+    out = _dne().altcorr_forward(f1.to(dtype).cuda(), f2.to(dtype).cuda(), coords.contiguous().cuda(), 3)[0]
+    want = oc.altcorr_forward(f1.to(dtype).double().numpy(), f2.to(dtype).double().numpy(), coords.numpy(), 3)
+    tol = 1e-5 if dtype == torch.float32 else 3e-3
+    np.testing.assert_allclose(out.double().cpu().numpy(), want, atol=tol)
+
+
+@pytest.mark.parametrize("exact", [False, True])
+def test_altcorr_backward(exact):
+    g = torch.Generator().manual_seed(13)
+    B, S, H, W, C = 1, 2, 6, 8, 32
+    f1 = torch.randn(B, H, W, C, generator=g) / 4
+    f2 = torch.randn(B, H, W, C, generator=g) / 4
+    coords = torch.stack([_grid_coords(B, H, W, g, 1.2).permute(0, 2, 3, 1) for _ in range(S)], 1).contiguous()
+    grad = torch.randn(B, S, 49, H, W, generator=g)
+    g1, g2, gc = _dne().altcorr_backward(f1.cuda(), f2.cuda(), coords.cuda(), grad.cuda(), 3, exact)
+    w1, w2, wc = oc.altcorr_backward(f1.numpy(), f2.numpy(), coords.numpy(), grad.numpy(), 3, exact_coords=exact)
+    np.testing.assert_allclose(g1.cpu().numpy(), w1, atol=1e-4)
+    np.testing.assert_allclose(g2.cpu().numpy(), w2, atol=1e-4)
+    np.testing.assert_allclose(gc.cpu().numpy(), wc, atol=1e-4)
+    if not exact:
+        assert float(gc.abs().max()) == 0.0  # reference returns zeros (altcorr_kernel.cu:440)
+
+
+def test_altcorr_index_matches_oracle_and_reference_property():
+    # reference tests/test_altcorr_indexed.py:23-48
+    from vipe_b200.droid_corr import AltCorrBlock
+
+    torch.manual_seed(2028)
+    batch, n_frames, channels, height, width, n_edges = 1, 7, 128, 48, 64, 5
+    fmaps = torch.randn(batch, n_frames, channels, height, width, device="cuda", dtype=torch.float16)
+    yy, xx = torch.meshgrid(torch.arange(height, device="cuda"), torch.arange(width, device="cuda"), indexing="ij")
+    coords = torch.stack([xx, yy], dim=-1).float()[None].repeat(batch, n_edges, 1, 1, 1)
+    coords = coords + 0.4 * torch.randn_like(coords)
+    ii = torch.tensor([0, 1, 2, 3, 4], device="cuda", dtype=torch.long)
+    jj = torch.tensor([1, 2, 3, 4, 5], device="cuda", dtype=torch.long)
+    corr = AltCorrBlock(fmaps)
+    cs = coords.unsqueeze(dim=-2)
+    reference = corr.corr_fn_reference(cs, ii, jj)
+    indexed = corr.corr_fn_indexed(cs, ii, jj)
+    torch.testing.assert_close(indexed, reference, atol=2e-4, rtol=1e-4)
+    default = corr(coords, ii, jj)
+    torch.testing.assert_close(default, reference.squeeze(dim=-1), atol=2e-4, rtol=1e-4)
+    # against the FP64 oracle on the same fp16 pyramid (edges 0..1 to keep the CPU side quick)
+    levels = [p.double().cpu().numpy() for p in corr.pyramid]
+    want = oc.altcorr_index_forward(levels[0], levels, coords[:, :2].cpu().numpy(), [0, 1], [1, 2], 3)
+    np.testing.assert_allclose(indexed[:, :2, ..., 0].double().cpu().numpy(), want, atol=5e-4)
+
+
+@pytest.mark.parametrize("in_dtype,tol", [(torch.bfloat16, 1e-4), (torch.float16, 1e-4)])
+def test_volume_build_pyramid(in_dtype, tol):
+    from vipe_b200.corr_build import corr_volume_pyramid
+
+    g = torch.Generator().manual_seed(14)
+    num, C, H, W = 3, 128, 16, 32
+    f1 = torch.randn(num, C, H, W, generator=g) / np.sqrt(C) * 4
+    f2 = torch.randn(num, C, H, W, generator=g) / np.sqrt(C) * 4
+    levels = corr_volume_pyramid(f1.to(in_dtype).cuda(), f2.to(in_dtype).cuda(), 4, out_dtype=torch.float32)
+    want = oc.corr_pyramid(f1.to(in_dtype).double().numpy(), f2.to(in_dtype).double().numpy(), 4)
+    for l, (got, w) in enumerate(zip(levels, want)):
+        got = got.cpu().double().numpy().reshape(w.shape)
+        scale = np.abs(w).max()
+        err = np.abs(got - w).max()
+        assert err <= tol * scale, (l, err, scale)
+
+
+def test_volume_build_shapes_and_corrblock():
+    from vipe_b200.droid_corr import CorrBlock
+
+    g = torch.Generator().manual_seed(15)
+    B, N, C, H, W = 1, 2, 128, 8, 16
+    f1 = (torch.randn(B, N, C, H, W, generator=g) / 4).half().cuda()
+    f2 = (torch.randn(B, N, C, H, W, generator=g) / 4).half().cuda()
+    cb = CorrBlock(f1, f2, num_levels=4, radius=3)
+    assert [tuple(p.shape) for p in cb.corr_pyramid] == [(2, 8, 16, 8, 16), (2, 8, 16, 4, 8), (2, 8, 16, 2, 4),
+                                                          (2, 8, 16, 1, 2)]
+    coords = _grid_coords(B * N, H, W, g, 1.0).permute(0, 2, 3, 1).reshape(B, N, H, W, 2).cuda()
+    out = cb(coords)
+    assert out.shape == (B, N, 4 * 49, H, W)
+    pyr = oc.corr_pyramid(f1[0].double().cpu().numpy(), f2[0].double().cpu().numpy(), 4)
+    c4 = coords[0].permute(0, 3, 1, 2).cpu().numpy()
+    want = np.concatenate([oc.corr_index_forward(pyr[l], c4 / 2**l, 3).reshape(N, 49, H, W) for l in range(4)], 1)
+    np.testing.assert_allclose(out[0].double().cpu().numpy(), want, atol=1e-2)

@@ -980,6 +980,8 @@ __global__ void __launch_bounds__(kCholThreads, 1)
     extern __shared__ double pT[];  // kNB columns x LDR rows (transposed panel)
     __shared__ double Li[kNB][kNB + 1];  // inverse of the diagonal block, Li[row][col]
     __shared__ double ysh[kNB];
+    __shared__ double bsh[kNB];
+    __shared__ double dinv[kNB];
     __shared__ int fail;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = with_intr ? d.dim : d.dim - 1;
@@ -996,9 +998,23 @@ __global__ void __launch_bounds__(kCholThreads, 1)
     const int nblk = (n + kNB - 1) / kNB;
     for (int kb = 0; kb < nblk; kb++) {
         const int k0 = kb * kNB, kn = min(kNB, n - k0), nr = n - k0;
-        for (int q = tid; q < nr * kNB; q += kCholThreads) {
-            const int r = q / kNB, c = q % kNB;
-            pT[c * LDR + r] = c < kn ? A[(size_t)(k0 + r) * ld + k0 + c] : 0.0;
+        {
+            const int tot = nr * kNB;
+            for (int q0 = tid; q0 < tot; q0 += 4 * kCholThreads) {
+                double v[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int q = q0 + u * kCholThreads;
+                    const int r = q / kNB, c = q % kNB;
+                    v[u] = (q < tot && c < kn) ? A[(size_t)(k0 + r) * ld + k0 + c] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int q = q0 + u * kCholThreads;
+                    if (q < tot) pT[(q % kNB) * LDR + q / kNB] = v[u];
+                }
+            }
+            if (tid < kNB) bsh[tid] = tid < kn ? x[k0 + tid] : 0.0;
         }
         __syncthreads();
         if (warp == 0) {
@@ -1008,12 +1024,15 @@ __global__ void __launch_bounds__(kCholThreads, 1)
             for (int c = 0; c < kNB; c++)
                 rv[c] = (lane < kn && c < kn) ? pT[c * LDR + lane] : (lane == c ? 1.0 : 0.0);
             bool bad = false;
+            double my_dinv = 1.0;
 #pragma unroll
             for (int j = 0; j < kNB; j++) {
                 const double piv = __shfl_sync(0xffffffffu, rv[j], j);
                 bad |= !(piv > 0.0);
                 const double l = piv > 0.0 ? sqrt(piv) : 1.0;
-                rv[j] = (lane == j) ? l : (lane > j ? rv[j] / l : rv[j]);
+                const double il = 1.0 / l;
+                if (lane == j) my_dinv = il;
+                rv[j] = (lane == j) ? l : (lane > j ? rv[j] * il : rv[j]);
 #pragma unroll
                 for (int c = j + 1; c < kNB; c++) {
                     const double lcj = __shfl_sync(0xffffffffu, rv[j], c);
@@ -1021,6 +1040,7 @@ __global__ void __launch_bounds__(kCholThreads, 1)
                 }
             }
             if (bad && lane == 0) fail = 1;
+            dinv[lane] = my_dinv;
             // the factor goes to Li's shared buffer first (row-major), then is inverted in place by columns
 #pragma unroll
             for (int c = 0; c < kNB; c++) {
@@ -1033,10 +1053,14 @@ __global__ void __launch_bounds__(kCholThreads, 1)
             double z[kNB];
 #pragma unroll
             for (int t = 0; t < kNB; t++) {
-                double sacc = (t == lane) ? 1.0 : 0.0;
+                double s0 = (t == lane) ? 1.0 : 0.0, s1 = 0.0;
 #pragma unroll
-                for (int q = 0; q < t; q++) sacc -= Li[t][q] * z[q];
-                z[t] = (t < lane) ? 0.0 : sacc / Li[t][t];
+                for (int q = 0; q + 1 < t; q += 2) {
+                    s0 -= Li[t][q] * z[q];
+                    s1 -= Li[t][q + 1] * z[q + 1];
+                }
+                if (t & 1) s0 -= Li[t][t - 1] * z[t - 1];
+                z[t] = (t < lane) ? 0.0 : (s0 + s1) * dinv[t];
             }
             __syncwarp();
 #pragma unroll
@@ -1073,9 +1097,12 @@ __global__ void __launch_bounds__(kCholThreads, 1)
         }
         // forward substitution of this block: y_k = L_kk^-1 b_k
         if (tid < kNB) {
-            double yv = 0.0;
-            for (int t = 0; t <= tid; t++) yv += Li[tid][t] * (t < kn ? x[k0 + t] : 0.0);
-            ysh[tid] = tid < kn ? yv : 0.0;
+            double y0 = 0.0, y1 = 0.0;
+            for (int t = 0; t <= tid; t += 2) {
+                y0 += Li[tid][t] * bsh[t];
+                if (t + 1 <= tid) y1 += Li[tid][t + 1] * bsh[t + 1];
+            }
+            ysh[tid] = tid < kn ? y0 + y1 : 0.0;
         }
         __syncthreads();
         if (tid < kn) x[k0 + tid] = ysh[tid];

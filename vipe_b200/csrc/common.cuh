@@ -37,7 +37,7 @@ struct ProfScope {
         cudaError_t _e = (expr);                             \
         if (_e != cudaSuccess) {                             \
             ::vipe::set_last_error(cudaGetErrorString(_e));  \
-            return VIPE_ERR_CUDA;                            \
+            return (int)VIPE_ERR_CUDA;                       \
         }                                                    \
     } while (0)
 

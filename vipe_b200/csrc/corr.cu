@@ -1,0 +1,576 @@
+// Correlation lookups of the DROID update operator — drop-in for the
+// reference's droid_net_ext (vipe csrc/droid_net_ext/droid.cpp:75-81):
+//
+//   corr_index_forward / backward   bilinear radius-r lookup in a materialised
+//       volume (correlation_kernels.cu:22-158)
+//   altcorr_forward / backward      the same lookup computed on the fly from
+//       feature maps (altcorr_kernel.cu:26-138, 242-366)
+//   altcorr_index_forward           indexed, multi-level on-the-fly lookup
+//       (altcorr_kernel.cu:140-240, 394-424)
+//
+// Conventions kept from the reference: taps at floor(x) - r + i, floor(y) - r
+// + j for i, j in [0, 2r+1]; output channel = i * (2r+1) + j (x-offset major);
+// bilinear weights from the fractional parts; zeros outside the map; pyramid
+// level l looks up at coords / 2^l.  Accumulation is in FP32 (FP64 for double
+// inputs) and each output is written once.
+//
+// On-the-fly kernels: one warp per (pixel, sample), one tap per lane (a window
+// of (2r+2)^2 = 64 taps for r = 3 is two taps per lane); each lane computes the
+// full C-channel dot product of its tap against the pixel's feature vector
+// (staged once in shared memory and reused for every pyramid level), then the
+// bilinear combination is done with warp shuffles.  Output tiles of 32 pixels
+// are staged in shared memory and written as coalesced rows.
+
+#include "common.cuh"
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+namespace vipe {
+namespace corr {
+
+template <typename T>
+__device__ __forceinline__ float to_f(T v) {
+    return static_cast<float>(v);
+}
+template <>
+__device__ __forceinline__ float to_f<__half>(__half v) {
+    return __half2float(v);
+}
+template <>
+__device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 v) {
+    return __bfloat162float(v);
+}
+
+template <typename T>
+__device__ __forceinline__ T from_f(float v) {
+    return static_cast<T>(v);
+}
+template <>
+__device__ __forceinline__ __half from_f<__half>(float v) {
+    return __float2half_rn(v);
+}
+template <>
+__device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float v) {
+    return __float2bfloat16_rn(v);
+}
+
+template <typename T>
+struct Acc {
+    using type = float;
+};
+template <>
+struct Acc<double> {
+    using type = double;
+};
+
+__device__ __forceinline__ bool inb(int h, int w, int H, int W) { return h >= 0 && h < H && w >= 0 && w < W; }
+
+// ---------------------------------------------------------------- materialised-volume lookup
+
+template <typename T>
+__global__ void corr_index_fwd_kernel(const T* __restrict__ vol, const float* __restrict__ coords, T* __restrict__ out,
+                                      int B, int h1, int w1, int h2, int w2, int r) {
+    using A = typename Acc<T>::type;
+    const int64_t HW1 = (int64_t)h1 * w1;
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= B * HW1) return;
+    const int n = (int)(idx / HW1);
+    const int64_t pix = idx % HW1;
+    const float x0 = coords[((int64_t)n * 2 + 0) * HW1 + pix];
+    const float y0 = coords[((int64_t)n * 2 + 1) * HW1 + pix];
+    const float fx0 = floorf(x0), fy0 = floorf(y0);
+    const A dx = (A)(x0 - fx0), dy = (A)(y0 - fy0);
+    const int bx = (int)fx0 - r, by = (int)fy0 - r;
+    const int rd = 2 * r + 1;
+    const T* plane = vol + ((int64_t)n * HW1 + pix) * ((int64_t)h2 * w2);
+    T* o = out + (int64_t)n * rd * rd * HW1 + pix;
+    for (int i = 0; i < rd; i++) {
+        for (int j = 0; j < rd; j++) {
+            // out[i][j] = bilinear at (bx + i + dx, by + j + dy)
+            A v = 0;
+            const int xa = bx + i, ya = by + j;
+            if (inb(ya, xa, h2, w2)) v += (1 - dx) * (1 - dy) * (A)to_f(plane[(int64_t)ya * w2 + xa]);
+            if (inb(ya, xa + 1, h2, w2)) v += dx * (1 - dy) * (A)to_f(plane[(int64_t)ya * w2 + xa + 1]);
+            if (inb(ya + 1, xa, h2, w2)) v += (1 - dx) * dy * (A)to_f(plane[(int64_t)(ya + 1) * w2 + xa]);
+            if (inb(ya + 1, xa + 1, h2, w2)) v += dx * dy * (A)to_f(plane[(int64_t)(ya + 1) * w2 + xa + 1]);
+            o[(int64_t)(i * rd + j) * HW1] = from_f<T>((float)v);
+        }
+    }
+}
+
+template <>
+__global__ void corr_index_fwd_kernel<double>(const double* __restrict__ vol, const float* __restrict__ coords,
+                                              double* __restrict__ out, int B, int h1, int w1, int h2, int w2, int r) {
+    const int64_t HW1 = (int64_t)h1 * w1;
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= B * HW1) return;
+    const int n = (int)(idx / HW1);
+    const int64_t pix = idx % HW1;
+    const float x0 = coords[((int64_t)n * 2 + 0) * HW1 + pix];
+    const float y0 = coords[((int64_t)n * 2 + 1) * HW1 + pix];
+    const float fx0 = floorf(x0), fy0 = floorf(y0);
+    const double dx = (double)(x0 - fx0), dy = (double)(y0 - fy0);
+    const int bx = (int)fx0 - r, by = (int)fy0 - r;
+    const int rd = 2 * r + 1;
+    const double* plane = vol + ((int64_t)n * HW1 + pix) * ((int64_t)h2 * w2);
+    double* o = out + (int64_t)n * rd * rd * HW1 + pix;
+    for (int i = 0; i < rd; i++)
+        for (int j = 0; j < rd; j++) {
+            double v = 0;
+            const int xa = bx + i, ya = by + j;
+            if (inb(ya, xa, h2, w2)) v += (1 - dx) * (1 - dy) * plane[(int64_t)ya * w2 + xa];
+            if (inb(ya, xa + 1, h2, w2)) v += dx * (1 - dy) * plane[(int64_t)ya * w2 + xa + 1];
+            if (inb(ya + 1, xa, h2, w2)) v += (1 - dx) * dy * plane[(int64_t)(ya + 1) * w2 + xa];
+            if (inb(ya + 1, xa + 1, h2, w2)) v += dx * dy * plane[(int64_t)(ya + 1) * w2 + xa + 1];
+            o[(int64_t)(i * rd + j) * HW1] = v;
+        }
+}
+
+// volume_grad must be zero on entry; each pixel owns its (h2, w2) plane, so the
+// scatter has no conflicts and is deterministic
+template <typename T>
+__global__ void corr_index_bwd_kernel(const float* __restrict__ coords, const T* __restrict__ g,
+                                      T* __restrict__ vgrad, int B, int h1, int w1, int h2, int w2, int r) {
+    using A = typename Acc<T>::type;
+    const int64_t HW1 = (int64_t)h1 * w1;
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= B * HW1) return;
+    const int n = (int)(idx / HW1);
+    const int64_t pix = idx % HW1;
+    const float x0 = coords[((int64_t)n * 2 + 0) * HW1 + pix];
+    const float y0 = coords[((int64_t)n * 2 + 1) * HW1 + pix];
+    const float fx0 = floorf(x0), fy0 = floorf(y0);
+    const A dx = (A)(x0 - fx0), dy = (A)(y0 - fy0);
+    const int bx = (int)fx0 - r, by = (int)fy0 - r;
+    const int rd = 2 * r + 1;
+    T* plane = vgrad + ((int64_t)n * HW1 + pix) * ((int64_t)h2 * w2);
+    const T* go = g + (int64_t)n * rd * rd * HW1 + pix;
+    for (int i = 0; i <= rd; i++)
+        for (int j = 0; j <= rd; j++) {
+            const int x1 = bx + i, y1 = by + j;
+            if (!inb(y1, x1, h2, w2)) continue;
+            A s = 0;
+            if (i > 0 && j > 0) s += (A)to_f(go[(int64_t)((i - 1) * rd + (j - 1)) * HW1]) * dx * dy;
+            if (i > 0 && j < rd) s += (A)to_f(go[(int64_t)((i - 1) * rd + j) * HW1]) * dx * (1 - dy);
+            if (i < rd && j > 0) s += (A)to_f(go[(int64_t)(i * rd + (j - 1)) * HW1]) * (1 - dx) * dy;
+            if (i < rd && j < rd) s += (A)to_f(go[(int64_t)(i * rd + j) * HW1]) * (1 - dx) * (1 - dy);
+            plane[(int64_t)y1 * w2 + x1] = from_f<T>((float)s);
+        }
+}
+
+template <>
+__global__ void corr_index_bwd_kernel<double>(const float* __restrict__ coords, const double* __restrict__ g,
+                                              double* __restrict__ vgrad, int B, int h1, int w1, int h2, int w2,
+                                              int r) {
+    const int64_t HW1 = (int64_t)h1 * w1;
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= B * HW1) return;
+    const int n = (int)(idx / HW1);
+    const int64_t pix = idx % HW1;
+    const float x0 = coords[((int64_t)n * 2 + 0) * HW1 + pix];
+    const float y0 = coords[((int64_t)n * 2 + 1) * HW1 + pix];
+    const float fx0 = floorf(x0), fy0 = floorf(y0);
+    const double dx = x0 - fx0, dy = y0 - fy0;
+    const int bx = (int)fx0 - r, by = (int)fy0 - r;
+    const int rd = 2 * r + 1;
+    double* plane = vgrad + ((int64_t)n * HW1 + pix) * ((int64_t)h2 * w2);
+    const double* go = g + (int64_t)n * rd * rd * HW1 + pix;
+    for (int i = 0; i <= rd; i++)
+        for (int j = 0; j <= rd; j++) {
+            const int x1 = bx + i, y1 = by + j;
+            if (!inb(y1, x1, h2, w2)) continue;
+            double s = 0;
+            if (i > 0 && j > 0) s += go[(int64_t)((i - 1) * rd + (j - 1)) * HW1] * dx * dy;
+            if (i > 0 && j < rd) s += go[(int64_t)((i - 1) * rd + j) * HW1] * dx * (1 - dy);
+            if (i < rd && j > 0) s += go[(int64_t)(i * rd + (j - 1)) * HW1] * (1 - dx) * dy;
+            if (i < rd && j < rd) s += go[(int64_t)(i * rd + j) * HW1] * (1 - dx) * (1 - dy);
+            plane[(int64_t)y1 * w2 + x1] = s;
+        }
+}
+
+// ---------------------------------------------------------------- on-the-fly lookup (warp per pixel)
+
+constexpr int kWarps = 8;        // warps per CTA
+constexpr int kTile = 32;        // pixels per CTA tile (one row segment)
+constexpr int kMaxC = 256;       // channels staged per pixel
+constexpr int kMaxR = 3;         // radius supported by the warp kernels
+constexpr int kMaxOut = (2 * kMaxR + 1) * (2 * kMaxR + 1);
+
+// Dot product of C channels of a tap row (global, dtype T) with f1 (shared, A);
+// 16-byte vector loads when C allows.
+template <typename T, typename A>
+__device__ __forceinline__ A row_dot(const T* __restrict__ f2, const A* f1s, int C) {
+    constexpr int V = 16 / (int)sizeof(T);
+    A s = 0;
+    if (C % V == 0) {
+        for (int c = 0; c < C; c += V) {
+            const uint4 raw = __ldg(reinterpret_cast<const uint4*>(f2 + c));
+            const T* e = reinterpret_cast<const T*>(&raw);
+#pragma unroll
+            for (int k = 0; k < V; k++) s += f1s[c + k] * (A)to_f(e[k]);
+        }
+    } else {
+        for (int c = 0; c < C; c++) s += f1s[c] * (A)to_f(f2[c]);
+    }
+    return s;
+}
+
+// Dot products of the (2r+2)^2 window taps against f1 (shared memory) for one
+// pixel; lane owns taps `lane` and `lane + 32`.  Returns them in t0, t1.
+template <typename T, typename A>
+__device__ __forceinline__ void window_dots(const T* __restrict__ fmap2, int H2, int W2, int C, const A* f1s, float xc,
+                                            float yc, int r, A& t0, A& t1) {
+    const int lane = threadIdx.x & 31;
+    const int ne = 2 * r + 2;
+    const int nt = ne * ne;
+    const int bx = (int)floorf(xc) - r, by = (int)floorf(yc) - r;
+    t0 = 0;
+    t1 = 0;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int tap = lane + 32 * h;
+        if (tap >= nt) continue;
+        const int ix = tap / ne, iy = tap % ne;
+        const int x2 = bx + ix, y2 = by + iy;
+        A sacc = 0;
+        if (inb(y2, x2, H2, W2)) sacc = row_dot<T, A>(fmap2 + ((int64_t)y2 * W2 + x2) * C, f1s, C);
+        if (h == 0) t0 = sacc; else t1 = sacc;
+    }
+}
+
+// value of tap (ix, iy) held by lane (ix*ne+iy) mod 32 in t0/t1
+template <typename A>
+__device__ __forceinline__ A tap_value(A t0, A t1, int ne, int ix, int iy) {
+    const int tap = ix * ne + iy;
+    const A a = __shfl_sync(0xffffffffu, t0, tap & 31);
+    const A b = __shfl_sync(0xffffffffu, t1, tap & 31);
+    return tap < 32 ? a : b;
+}
+
+// bilinear combination of the window taps into (2r+1)^2 outputs; lane writes
+// outputs lane and lane+32 into out_s[ch * stride]
+template <typename A>
+__device__ __forceinline__ void combine(A t0, A t1, int r, float xc, float yc, float* out_s, int stride) {
+    const int lane = threadIdx.x & 31;
+    const int rd = 2 * r + 1, ne = rd + 1;
+    const A dx = (A)(xc - floorf(xc)), dy = (A)(yc - floorf(yc));
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int ch = lane + 32 * h;
+        // shuffles must be executed by all lanes: compute indices clamped
+        const int chc = ch < rd * rd ? ch : 0;
+        const int i = chc / rd, j = chc % rd;
+        const A a00 = tap_value(t0, t1, ne, i, j);
+        const A a10 = tap_value(t0, t1, ne, i + 1, j);
+        const A a01 = tap_value(t0, t1, ne, i, j + 1);
+        const A a11 = tap_value(t0, t1, ne, i + 1, j + 1);
+        const A v = (1 - dx) * (1 - dy) * a00 + dx * (1 - dy) * a10 + (1 - dx) * dy * a01 + dx * dy * a11;
+        if (ch < rd * rd) out_s[ch * stride] = (float)v;
+    }
+}
+
+// altcorr_forward: fmap1 (B,H1,W1,C), fmap2 (B,H2,W2,C), coords (B,S,H1,W1,2)
+// -> out (B,S,rd^2,H1,W1).  grid: (ceil(W1/32), H1, B*S)
+template <typename T>
+__global__ void __launch_bounds__(kWarps * 32)
+    altcorr_fwd_kernel(const T* __restrict__ fmap1, const T* __restrict__ fmap2, const float* __restrict__ coords,
+                       T* __restrict__ out, int B, int S, int H1, int W1, int H2, int W2, int C, int r) {
+    using A = typename Acc<T>::type;
+    __shared__ A f1s[kWarps][kMaxC];
+    __shared__ float os[kMaxOut][kTile];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bs = blockIdx.z, b = bs / S;
+    const int h1 = blockIdx.y, w0 = blockIdx.x * kTile;
+    const int rd = 2 * r + 1;
+    const int64_t HW1 = (int64_t)H1 * W1;
+    for (int pp = warp; pp < kTile; pp += kWarps) {
+        const int w1 = w0 + pp;
+        if (w1 >= W1) break;
+        const T* f1 = fmap1 + (((int64_t)b * H1 + h1) * W1 + w1) * C;
+        for (int c = lane; c < C; c += 32) f1s[warp][c] = (A)to_f(f1[c]);
+        __syncwarp();
+        const float* cp = coords + (((int64_t)bs * H1 + h1) * W1 + w1) * 2;
+        const float xc = cp[0], yc = cp[1];
+        A t0, t1;
+        window_dots<T, A>(fmap2 + (int64_t)b * H2 * W2 * C, H2, W2, C, f1s[warp], xc, yc, r, t0, t1);
+        combine<A>(t0, t1, r, xc, yc, &os[0][pp], kTile);
+        __syncwarp();
+    }
+    __syncthreads();
+    const int nw = min(kTile, W1 - w0);
+    for (int q = threadIdx.x; q < rd * rd * kTile; q += blockDim.x) {
+        const int ch = q / kTile, pp = q % kTile;
+        if (pp < nw) out[((int64_t)bs * rd * rd + ch) * HW1 + (int64_t)h1 * W1 + w0 + pp] = from_f<T>(os[ch][pp]);
+    }
+}
+
+// altcorr_index_forward: fmap1 (B,Nf,H,W,C) level 0, levels[l] (B,Nf,H2[l],W2[l],C),
+// coords (B,M,H,W,2), ii/jj (M) -> out (B,M,L*rd^2,H,W) f32.  grid (ceil(W/32), H, B*M)
+struct LevelPtrs {
+    const void* p[8];
+    int H2[8];
+    int W2[8];
+};
+
+constexpr int kMaxL = 4;  // pyramid levels kept in the shared output tile
+
+template <typename T>
+__global__ void __launch_bounds__(kWarps * 32)
+    altcorr_index_fwd_kernel(const T* __restrict__ fmap1, LevelPtrs lv, int L, const float* __restrict__ coords,
+                             const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, float* __restrict__ out,
+                             int B, int Nf, int M, int H, int W, int C, int r) {
+    using A = typename Acc<T>::type;
+    __shared__ A f1s[kWarps][kMaxC];
+    __shared__ float os[kMaxL * kMaxOut][kTile];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bm = blockIdx.z, b = bm / M, m = bm % M;
+    const int h = blockIdx.y, w0 = blockIdx.x * kTile;
+    const int src = (int)ii[m], dst = (int)jj[m];
+    const int rd = 2 * r + 1, nch = rd * rd;
+    const int64_t HW = (int64_t)H * W;
+    const int nw = min(kTile, W - w0);
+    for (int pp = warp; pp < nw; pp += kWarps) {
+        const int w = w0 + pp;
+        const T* f1 = fmap1 + ((((int64_t)b * Nf + src) * H + h) * W + w) * C;
+        for (int c = lane; c < C; c += 32) f1s[warp][c] = (A)to_f(f1[c]);
+        __syncwarp();
+        const float* cp = coords + (((int64_t)bm * H + h) * W + w) * 2;
+        for (int l = 0; l < L; l++) {
+            // reference: coords / 2^l at level l (droid_net.py:78, altcorr_kernel.cu:182-183)
+            const float scale = (float)(1 << l);
+            const float xc = cp[0] / scale, yc = cp[1] / scale;
+            const int H2 = lv.H2[l], W2 = lv.W2[l];
+            const T* f2base = static_cast<const T*>(lv.p[l]) + ((int64_t)b * Nf + dst) * H2 * W2 * C;
+            A t0, t1;
+            window_dots<T, A>(f2base, H2, W2, C, f1s[warp], xc, yc, r, t0, t1);
+            combine<A>(t0, t1, r, xc, yc, &os[l * nch][pp], kTile);
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < L * nch * kTile; q += blockDim.x) {
+        const int ch = q / kTile, pp = q % kTile;
+        if (pp < nw) out[((int64_t)bm * L * nch + ch) * HW + (int64_t)h * W + w0 + pp] = os[ch][pp];
+    }
+}
+
+// altcorr_backward (f32): fmap1_grad (B,H1,W1,C) and fmap2_grad (B,H2,W2,C) must
+// be zero on entry.  Per (pixel, sample) warp: tap gradients from the bilinear
+// adjoint; fmap1_grad gathered per pixel (owned by the warp across samples);
+// fmap2_grad scattered with atomic adds (windows of neighbouring pixels overlap),
+// as the reference does.  With exact_coords the derivative of the bilinear
+// weights is written to coords_grad (B,S,H1,W1,2); otherwise zeros.
+__global__ void __launch_bounds__(kWarps * 32)
+    altcorr_bwd_kernel(const float* __restrict__ fmap1, const float* __restrict__ fmap2,
+                       const float* __restrict__ coords, const float* __restrict__ g, float* __restrict__ g1,
+                       float* __restrict__ g2, float* __restrict__ gc, int B, int S, int H1, int W1, int H2, int W2,
+                       int C, int r, int exact_coords) {
+    __shared__ float f1s[kWarps][kMaxC];
+    __shared__ float acc1[kWarps][kMaxC];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.z;
+    const int h1 = blockIdx.y;
+    const int w1 = blockIdx.x * kWarps + warp;
+    if (w1 >= W1) return;
+    const int rd = 2 * r + 1, ne = rd + 1, nt = ne * ne;
+    const int64_t HW1 = (int64_t)H1 * W1;
+    const float* f1 = fmap1 + (((int64_t)b * H1 + h1) * W1 + w1) * C;
+    for (int c = lane; c < C; c += 32) {
+        f1s[warp][c] = f1[c];
+        acc1[warp][c] = 0.f;
+    }
+    __syncwarp();
+    const float* f2base = fmap2 + (int64_t)b * H2 * W2 * C;
+    float* g2base = g2 + (int64_t)b * H2 * W2 * C;
+    for (int s = 0; s < S; s++) {
+        const int64_t bs = (int64_t)b * S + s;
+        const float* cp = coords + ((bs * H1 + h1) * W1 + w1) * 2;
+        const float xc = cp[0], yc = cp[1];
+        const float dx = xc - floorf(xc), dy = yc - floorf(yc);
+        const int bx = (int)floorf(xc) - r, by = (int)floorf(yc) - r;
+        const float* gp = g + bs * rd * rd * HW1 + (int64_t)h1 * W1 + w1;
+        float gt[2];
+#pragma unroll
+        for (int hh = 0; hh < 2; hh++) {
+            const int tap = lane + 32 * hh;
+            float v = 0.f;
+            if (tap < nt) {
+                const int i = tap / ne, j = tap % ne;
+                if (i > 0 && j > 0) v += gp[(int64_t)((i - 1) * rd + (j - 1)) * HW1] * dx * dy;
+                if (i > 0 && j < rd) v += gp[(int64_t)((i - 1) * rd + j) * HW1] * dx * (1.f - dy);
+                if (i < rd && j > 0) v += gp[(int64_t)(i * rd + (j - 1)) * HW1] * (1.f - dx) * dy;
+                if (i < rd && j < rd) v += gp[(int64_t)(i * rd + j) * HW1] * (1.f - dx) * (1.f - dy);
+            }
+            gt[hh] = v;
+        }
+        float t0 = 0.f, t1 = 0.f;
+        if (exact_coords) window_dots<float, float>(f2base, H2, W2, C, f1s[warp], xc, yc, r, t0, t1);
+        // taps: fmap1 grad gather (lanes over channels) and fmap2 grad scatter
+        for (int tap = 0; tap < nt; tap++) {
+            const float gv = __shfl_sync(0xffffffffu, gt[tap >> 5], tap & 31);
+            const int ix = tap / ne, iy = tap % ne;
+            const int x2 = bx + ix, y2 = by + iy;
+            if (gv == 0.f || !inb(y2, x2, H2, W2)) continue;
+            const float* f2 = f2base + ((int64_t)y2 * W2 + x2) * C;
+            float* q2 = g2base + ((int64_t)y2 * W2 + x2) * C;
+            for (int c = lane; c < C; c += 32) {
+                acc1[warp][c] += gv * f2[c];
+                atomicAdd(q2 + c, gv * f1s[warp][c]);
+            }
+        }
+        if (gc) {
+            float cx = 0.f, cy = 0.f;
+            if (exact_coords) {
+                // d out[i][j] / d dx = (1-dy)(a10 - a00) + dy (a11 - a01), similarly for dy
+#pragma unroll
+                for (int hh = 0; hh < 2; hh++) {
+                    const int ch = lane + 32 * hh;
+                    const int chc = ch < rd * rd ? ch : 0;
+                    const int i = chc / rd, j = chc % rd;
+                    const float a00 = tap_value(t0, t1, ne, i, j);
+                    const float a10 = tap_value(t0, t1, ne, i + 1, j);
+                    const float a01 = tap_value(t0, t1, ne, i, j + 1);
+                    const float a11 = tap_value(t0, t1, ne, i + 1, j + 1);
+                    if (ch < rd * rd) {
+                        const float go = gp[(int64_t)ch * HW1];
+                        cx += go * ((1.f - dy) * (a10 - a00) + dy * (a11 - a01));
+                        cy += go * ((1.f - dx) * (a01 - a00) + dx * (a11 - a10));
+                    }
+                }
+                cx = warp_sum(cx);
+                cy = warp_sum(cy);
+            }
+            if (lane == 0) {
+                float* o = gc + ((bs * H1 + h1) * W1 + w1) * 2;
+                o[0] = cx;
+                o[1] = cy;
+            }
+        }
+    }
+    __syncwarp();
+    float* q1 = g1 + (((int64_t)b * H1 + h1) * W1 + w1) * C;
+    for (int c = lane; c < C; c += 32) q1[c] = acc1[warp][c];
+}
+
+template <typename F>
+int dispatch(int dtype, F&& f) {
+    switch (dtype) {
+        case VIPE_F32: return f(float());
+        case VIPE_F64: return f(double());
+        case VIPE_F16: return f(__half());
+        case VIPE_BF16: return f(__nv_bfloat16());
+        default: return VIPE_ERR_DTYPE;
+    }
+}
+
+}  // namespace corr
+}  // namespace vipe
+
+using namespace vipe;
+using namespace vipe::corr;
+
+extern "C" int vipe_corr_index_forward(int dtype, const void* volume, const float* coords, int B, int h1, int w1,
+                                       int h2, int w2, int radius, void* corr_out, void* stream) {
+    if (B < 0 || h1 < 0 || w1 < 0 || h2 <= 0 || w2 <= 0 || radius < 0) return VIPE_ERR_ARG;
+    const int64_t n = (int64_t)B * h1 * w1;
+    if (n == 0) return VIPE_OK;
+    cudaStream_t st = as_stream(stream);
+    return dispatch(dtype, [&](auto tag) {
+        using T = decltype(tag);
+        VIPE_PROF("corr_index_fwd", st);
+        corr_index_fwd_kernel<T><<<ceil_div(n, 256), 256, 0, st>>>(static_cast<const T*>(volume), coords,
+                                                                   static_cast<T*>(corr_out), B, h1, w1, h2, w2,
+                                                                   radius);
+        VIPE_LAUNCH_CHECK();
+        return (int)VIPE_OK;
+    });
+}
+
+extern "C" int vipe_corr_index_backward(int dtype, const float* coords, const void* corr_grad, int B, int h1, int w1,
+                                        int h2, int w2, int radius, void* volume_grad_out, void* stream) {
+    if (B < 0 || h1 < 0 || w1 < 0 || h2 <= 0 || w2 <= 0 || radius < 0) return VIPE_ERR_ARG;
+    const int64_t n = (int64_t)B * h1 * w1;
+    cudaStream_t st = as_stream(stream);
+    return dispatch(dtype, [&](auto tag) {
+        using T = decltype(tag);
+        VIPE_CUDA_TRY(cudaMemsetAsync(volume_grad_out, 0, (size_t)n * h2 * w2 * sizeof(T), st));
+        if (n == 0) return (int)VIPE_OK;
+        VIPE_PROF("corr_index_bwd", st);
+        corr_index_bwd_kernel<T><<<ceil_div(n, 256), 256, 0, st>>>(coords, static_cast<const T*>(corr_grad),
+                                                                   static_cast<T*>(volume_grad_out), B, h1, w1, h2,
+                                                                   w2, radius);
+        VIPE_LAUNCH_CHECK();
+        return (int)VIPE_OK;
+    });
+}
+
+extern "C" int vipe_altcorr_forward(int dtype, const void* fmap1, const void* fmap2, const float* coords, int B, int S,
+                                    int H1, int W1, int H2, int W2, int C, int radius, void* corr_out, void* stream) {
+    if (B < 0 || S < 0 || H1 < 0 || W1 < 0 || H2 <= 0 || W2 <= 0 || C <= 0) return VIPE_ERR_ARG;
+    if (C > kMaxC || radius < 0 || radius > kMaxR) return VIPE_ERR_CAPACITY;
+    if ((int64_t)B * S * H1 * W1 == 0) return VIPE_OK;
+    if (B * S > 65535 || H1 > 65535) return VIPE_ERR_CAPACITY;
+    cudaStream_t st = as_stream(stream);
+    dim3 grid(ceil_div(W1, kTile), H1, B * S);
+    return dispatch(dtype, [&](auto tag) {
+        using T = decltype(tag);
+        VIPE_PROF("altcorr_fwd", st);
+        altcorr_fwd_kernel<T><<<grid, kWarps * 32, 0, st>>>(static_cast<const T*>(fmap1),
+                                                             static_cast<const T*>(fmap2), coords,
+                                                             static_cast<T*>(corr_out), B, S, H1, W1, H2, W2, C,
+                                                             radius);
+        VIPE_LAUNCH_CHECK();
+        return (int)VIPE_OK;
+    });
+}
+
+extern "C" int vipe_altcorr_backward(const float* fmap1, const float* fmap2, const float* coords,
+                                     const float* corr_grad, int B, int S, int H1, int W1, int H2, int W2, int C,
+                                     int radius, int exact_coords_grad, float* fmap1_grad_out, float* fmap2_grad_out,
+                                     float* coords_grad_out, void* stream) {
+    if (B < 0 || S < 0 || H1 < 0 || W1 < 0 || H2 <= 0 || W2 <= 0 || C <= 0) return VIPE_ERR_ARG;
+    if (C > kMaxC || radius < 0 || radius > kMaxR) return VIPE_ERR_CAPACITY;
+    cudaStream_t st = as_stream(stream);
+    VIPE_CUDA_TRY(cudaMemsetAsync(fmap1_grad_out, 0, (size_t)B * H1 * W1 * C * sizeof(float), st));
+    VIPE_CUDA_TRY(cudaMemsetAsync(fmap2_grad_out, 0, (size_t)B * H2 * W2 * C * sizeof(float), st));
+    if (coords_grad_out)
+        VIPE_CUDA_TRY(cudaMemsetAsync(coords_grad_out, 0, (size_t)B * S * H1 * W1 * 2 * sizeof(float), st));
+    if ((int64_t)B * H1 * W1 == 0 || S == 0) return VIPE_OK;
+    if (B > 65535 || H1 > 65535) return VIPE_ERR_CAPACITY;
+    dim3 grid(ceil_div(W1, kWarps), H1, B);
+    VIPE_PROF("altcorr_bwd", st);
+    altcorr_bwd_kernel<<<grid, kWarps * 32, 0, st>>>(fmap1, fmap2, coords, corr_grad, fmap1_grad_out, fmap2_grad_out,
+                                                     coords_grad_out, B, S, H1, W1, H2, W2, C, radius,
+                                                     exact_coords_grad);
+    VIPE_LAUNCH_CHECK();
+    return VIPE_OK;
+}
+
+extern "C" int vipe_altcorr_index_forward(int dtype, const void* fmap1, const void* const* fmap2_levels,
+                                          const int* H2, const int* W2, int num_levels, const float* coords,
+                                          const int64_t* ii, const int64_t* jj, int B, int Nf, int M, int H, int W,
+                                          int C, int radius, float* corr_out, void* stream) {
+    if (B < 0 || Nf <= 0 || M < 0 || H < 0 || W < 0 || C <= 0 || num_levels <= 0) return VIPE_ERR_ARG;
+    if (num_levels > kMaxL || C > kMaxC || radius < 0 || radius > kMaxR) return VIPE_ERR_CAPACITY;
+    if ((int64_t)B * M * H * W == 0) return VIPE_OK;
+    if (B * M > 65535 || H > 65535) return VIPE_ERR_CAPACITY;
+    LevelPtrs lv;
+    for (int l = 0; l < num_levels; l++) {
+        if (H2[l] <= 0 || W2[l] <= 0 || !fmap2_levels[l]) return VIPE_ERR_ARG;
+        lv.p[l] = fmap2_levels[l];
+        lv.H2[l] = H2[l];
+        lv.W2[l] = W2[l];
+    }
+    cudaStream_t st = as_stream(stream);
+    dim3 grid(ceil_div(W, kTile), H, B * M);
+    return dispatch(dtype, [&](auto tag) {
+        using T = decltype(tag);
+        VIPE_PROF("altcorr_index_fwd", st);
+        altcorr_index_fwd_kernel<T><<<grid, kWarps * 32, 0, st>>>(static_cast<const T*>(fmap1), lv, num_levels,
+                                                                   coords, ii, jj, corr_out, B, Nf, M, H, W, C,
+                                                                   radius);
+        VIPE_LAUNCH_CHECK();
+        return (int)VIPE_OK;
+    });
+}

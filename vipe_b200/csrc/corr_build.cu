@@ -1,0 +1,542 @@
+// All-pairs correlation volume + average-pooled pyramid on tcgen05 tensor cores.
+//
+// Replaces CorrBlock.corr and its pyramid (vipe/slam/networks/droid_net.py:56-69,
+// 94-102): for every edge e, V_e = (F1_e / 4)^T (F2_e / 4) over C channels
+// (source pixel x target pixel), and level l = avg_pool2d^l(V_e) over the target
+// axes (2x2 windows, floor sizes).
+//
+// Data path (one persistent launch, one CTA per SM):
+//   * pack pass: F1, F2 (num, C, H, W) -> K-major BF16/FP16 rows (num, H*W, Kp)
+//     scaled by 1/4 (exact), F2's pixels reordered so that 256 consecutive rows
+//     are an 8 x TW block of the target image (TW = 32, 16 or 8 | W);
+//   * warp 0 lane 0: TMA loads (SWIZZLE_128B, 64-channel boxes) of the A tile
+//     (128 source pixels x Kp, reused for all N tiles of the work item) and of
+//     the B tiles (8 x TW target pixels x Kp, double-buffered);
+//   * warp 1 lane 0: tcgen05.mma.cta_group::1.kind::f16, M = 128, N = 8*TW,
+//     K = 16 per instruction, FP32 accumulator in tensor memory, two TMEM
+//     accumulator buffers (2 x 256 columns) so the MMA of tile t+1 overlaps the
+//     epilogue of tile t;
+//   * warps 4-7: epilogue.  tcgen05.ld puts one source pixel's row (the whole
+//     8 x TW target block) in each thread's registers, so the 2x2 / 4x4 / 8x8
+//     average pools of levels 1-3 close inside the thread; every level is
+//     converted and stored straight from registers.
+// The output write (sum over levels of num*HW*HW/4^l elements) is the HBM
+// roofline of this kernel.
+//
+// Every mbarrier wait is bounded: on expiry the CTA records an error, stops
+// issuing work, drains its in-flight copies (bounded) and frees tensor memory.
+
+#include "common.cuh"
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <mutex>
+
+namespace vipe {
+namespace cbuild {
+
+constexpr int kBM = 128;       // source pixels per tile (TMEM lanes)
+constexpr int kTH = 8;         // target rows per N tile
+constexpr int kKC = 64;        // channels per TMA box / swizzle row (128 B of 16-bit)
+constexpr int kMaxKC = 2;      // up to 128 channels (A + two B stages fit in shared memory)
+constexpr int kThreads = 256;  // 8 warps
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s bound on any mbarrier wait
+
+struct Params {
+    int num, C, Kp, H, W, HW, TW, N, levels;
+    int mtiles, ntiles;
+    long items;  // num * mtiles
+    int out_dtype;
+    void* out[4];
+    int* err;
+};
+
+// ---------------------------------------------------------------- PTX helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t gtimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// bounded wait; returns false (and flags the CTA) when 2 s pass or another
+// role already failed
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* fail) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = gtimer();
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (*fail) return false;
+        if (gtimer() - t0 > kWaitNs) break;
+    }
+    *fail = 1;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major, 128-byte swizzled operand: 8-row x 128 B atoms, atoms 1024 B apart
+__device__ __forceinline__ uint64_t smem_desc(const void* base) {
+    const uint64_t addr = smem_u32(base);
+    uint64_t d = 0;
+    d |= (addr >> 4) & 0x3FFFull;          // start address
+    d |= (uint64_t)1 << 16;                // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;      // stride byte offset: 8 rows x 128 B
+    d |= (uint64_t)1 << 46;                // descriptor version (sm100)
+    d |= (uint64_t)2 << 61;                // SWIZZLE_128B
+    return d;
+}
+
+// kind::f16 instruction descriptor: D f32, A/B bf16 (1) or f16 (0), both K-major
+__host__ __device__ constexpr uint32_t instr_desc(int ab_format, int M, int N) {
+    return (1u << 4) | ((uint32_t)ab_format << 7) | ((uint32_t)ab_format << 10) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accum) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(idesc), "r"(accum));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
+    uint32_t r[8];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// ---------------------------------------------------------------- output stores
+
+template <typename T>
+__device__ __forceinline__ T cvt(float v);
+template <>
+__device__ __forceinline__ float cvt<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ __half cvt<__half>(float v) { return __float2half_rn(v); }
+template <>
+__device__ __forceinline__ __nv_bfloat16 cvt<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+
+template <typename T, int N>
+__device__ __forceinline__ void store_row(T* dst, const float* v) {
+    // N contiguous elements; 16-byte aligned whenever N * sizeof(T) is a multiple of 16
+    if constexpr ((N * sizeof(T)) % 16 == 0) {
+#pragma unroll
+        for (int i = 0; i < N; i += 16 / (int)sizeof(T)) {
+            alignas(16) T tmp[16 / sizeof(T)];
+#pragma unroll
+            for (int k = 0; k < (int)(16 / sizeof(T)); k++) tmp[k] = cvt<T>(v[i + k]);
+            *reinterpret_cast<uint4*>(dst + i) = *reinterpret_cast<const uint4*>(tmp);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; i++) dst[i] = cvt<T>(v[i]);
+    }
+}
+
+// one 8x8 target block of one source row: level 0 plus pools
+template <typename T>
+__device__ __forceinline__ void emit_block(const Params& p, long row, int h0, int w0, const float (&blk)[8][8]) {
+    const int H = p.H, W = p.W;
+#pragma unroll
+    for (int r = 0; r < 8; r++) store_row<T, 8>(static_cast<T*>(p.out[0]) + (row * H + h0 + r) * W + w0, blk[r]);
+    if (p.levels > 1) {
+        float l1[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                l1[r][c] = 0.25f * (blk[2 * r][2 * c] + blk[2 * r][2 * c + 1] + blk[2 * r + 1][2 * c] +
+                                    blk[2 * r + 1][2 * c + 1]);
+        const int H1 = H >> 1, W1 = W >> 1;
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+            store_row<T, 4>(static_cast<T*>(p.out[1]) + (row * H1 + (h0 >> 1) + r) * W1 + (w0 >> 1), l1[r]);
+        if (p.levels > 2) {
+            float l2[2][2];
+#pragma unroll
+            for (int r = 0; r < 2; r++)
+#pragma unroll
+                for (int c = 0; c < 2; c++)
+                    l2[r][c] = 0.25f * (l1[2 * r][2 * c] + l1[2 * r][2 * c + 1] + l1[2 * r + 1][2 * c] +
+                                        l1[2 * r + 1][2 * c + 1]);
+            const int H2 = H >> 2, W2 = W >> 2;
+#pragma unroll
+            for (int r = 0; r < 2; r++)
+                store_row<T, 2>(static_cast<T*>(p.out[2]) + (row * H2 + (h0 >> 2) + r) * W2 + (w0 >> 2), l2[r]);
+            if (p.levels > 3) {
+                const float l3 = 0.25f * (l2[0][0] + l2[0][1] + l2[1][0] + l2[1][1]);
+                const int H3 = H >> 3, W3 = W >> 3;
+                static_cast<T*>(p.out[3])[(row * H3 + (h0 >> 3)) * W3 + (w0 >> 3)] = cvt<T>(l3);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- main kernel
+
+// dynamic shared memory: A tile (KC boxes of 128 rows x 128 B) then two B
+// stages (KC boxes of N rows x 128 B each); every box starts 1024-B aligned
+__host__ __device__ inline size_t a_region(int KC) { return (size_t)KC * kBM * 128; }
+__host__ __device__ inline size_t b_box(int N) { return (size_t)N * 128; }
+
+template <typename TOut>
+__global__ void __launch_bounds__(kThreads, 1)
+    corr_build_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, Params p,
+                      int ab_format) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* sbase = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ uint64_t barA_full, barA_empty;
+    __shared__ uint64_t barB_full[2], barB_empty[2];
+    __shared__ uint64_t barAcc_full[2], barAcc_empty[2];
+    __shared__ uint32_t tmem_base;
+    __shared__ volatile int fail;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int KC = p.Kp / kKC;
+    const int N = p.N;
+    auto sa = [&](int kc) { return sbase + (size_t)kc * kBM * 128; };
+    auto sb = [&](int st, int kc) { return sbase + a_region(KC) + ((size_t)st * KC + kc) * b_box(N); };
+
+    if (tid == 0) {
+        fail = 0;
+        mbar_init(&barA_full, 1);
+        mbar_init(&barA_empty, 1);
+        for (int s = 0; s < 2; s++) {
+            mbar_init(&barB_full[s], 1);
+            mbar_init(&barB_empty[s], 1);
+            mbar_init(&barAcc_full[s], 1);
+            mbar_init(&barAcc_empty[s], 4);  // one arrive per epilogue warp
+        }
+        fence_barrier_init();
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tmem_base)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base;
+
+    const uint32_t a_bytes = (uint32_t)kBM * 128u * KC;
+    const uint32_t b_bytes = (uint32_t)N * 128u * KC;
+
+    if (warp == 0 && lane == 0) {
+        // ------------------------------------------------ TMA producer
+        uint32_t t = 0, it = 0;
+        for (long item = blockIdx.x; item < p.items && !fail; item += gridDim.x, it++) {
+            const int e = (int)(item / p.mtiles), mt = (int)(item % p.mtiles);
+            if (it > 0 && !mbar_wait(&barA_empty, (it - 1) & 1, &fail)) break;
+            mbar_expect_tx(&barA_full, a_bytes);
+            for (int kc = 0; kc < KC; kc++)
+                tma_load_2d(sa(kc), &mapA, &barA_full, kc * kKC, e * p.HW + mt * kBM);
+            for (int nt = 0; nt < p.ntiles; nt++, t++) {
+                const int s = t & 1;
+                if (t >= 2 && !mbar_wait(&barB_empty[s], ((t >> 1) - 1) & 1, &fail)) break;
+                mbar_expect_tx(&barB_full[s], b_bytes);
+                for (int kc = 0; kc < KC; kc++)
+                    tma_load_2d(sb(s, kc), &mapB, &barB_full[s], kc * kKC, e * p.HW + nt * N);
+            }
+        }
+        // drain: the last loads issued must land before the CTA exits
+        if (fail && t > 0) {
+            mbar_wait(&barB_full[(t - 1) & 1], ((t - 1) >> 1) & 1, &fail);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ------------------------------------------------ MMA issuer
+        const uint32_t idesc = instr_desc(ab_format, kBM, N);
+        uint32_t t = 0, it = 0;
+        for (long item = blockIdx.x; item < p.items && !fail; item += gridDim.x, it++) {
+            if (!mbar_wait(&barA_full, it & 1, &fail)) break;
+            tc_fence_after();
+            for (int nt = 0; nt < p.ntiles; nt++, t++) {
+                const int s = t & 1, acc = t & 1;
+                if (!mbar_wait(&barB_full[s], (t >> 1) & 1, &fail)) break;
+                if (t >= 2 && !mbar_wait(&barAcc_empty[acc], ((t >> 1) - 1) & 1, &fail)) break;
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(acc * 256);
+                for (int kc = 0; kc < KC; kc++) {
+                    const uint64_t da = smem_desc(sa(kc));
+                    const uint64_t db = smem_desc(sb(s, kc));
+#pragma unroll
+                    for (int k = 0; k < kKC / 16; k++) {
+                        // advance 16 channels = 32 bytes inside the swizzled row
+                        mma_f16(d, da + (uint64_t)(k * 2), db + (uint64_t)(k * 2), idesc, (kc | k) ? 1u : 0u);
+                    }
+                }
+                mma_commit(&barB_empty[s]);
+                mma_commit(&barAcc_full[acc]);
+            }
+            mma_commit(&barA_empty);
+        }
+    } else if (warp >= 4) {
+        // ------------------------------------------------ epilogue
+        const int q = warp - 4;                 // TMEM lane quarter
+        const int mrow = q * 32 + lane;          // row of the 128-row tile
+        const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
+        const int TW = p.TW, blocks_w = p.W / TW;
+        uint32_t t = 0;
+        for (long item = blockIdx.x; item < p.items && !fail; item += gridDim.x) {
+            const int e = (int)(item / p.mtiles), mt = (int)(item % p.mtiles);
+            const int m = mt * kBM + mrow;
+            for (int nt = 0; nt < p.ntiles; nt++, t++) {
+                const int acc = t & 1;
+                if (!mbar_wait(&barAcc_full[acc], (t >> 1) & 1, &fail)) break;
+                tc_fence_after();
+                const int hb = nt / blocks_w, wb = nt % blocks_w;
+                const long row = (long)e * p.HW + m;
+                for (int c0 = 0; c0 < TW; c0 += 8) {
+                    float blk[8][8];
+#pragma unroll
+                    for (int r = 0; r < 8; r++)
+                        tmem_ld8(tmem + lane_addr + (uint32_t)(acc * 256 + r * TW + c0), blk[r]);
+                    tmem_wait_ld();
+                    if (m < p.HW) emit_block<TOut>(p, row, hb * kTH, wb * TW + c0, blk);
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&barAcc_empty[acc]);
+            }
+        }
+    }
+    __syncthreads();
+    if (fail && tid == 0) atomicExch(p.err, 1);
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+    }
+}
+
+// ---------------------------------------------------------------- pack pass
+
+// F (num, C, H, W) -> rows (num, HW, Kp) of 16-bit type, scaled by 1/4;
+// permute: target-block pixel order (8 x TW blocks) for the B operand.
+template <typename TIn, typename TOp>
+__global__ void pack_kernel(const TIn* __restrict__ f, TOp* __restrict__ out, int C, int Kp, int H, int W, int TW,
+                            int permute) {
+    __shared__ float tile[32][65];
+    const int e = blockIdx.z;
+    const int HW = H * W;
+    const int p0 = blockIdx.x * 32;          // 32 pixels
+    const int c0 = blockIdx.y * 64;          // 64 channels
+    const TIn* src = f + (size_t)e * C * HW;
+    for (int i = threadIdx.x; i < 32 * 64; i += blockDim.x) {
+        const int cc = i / 32, pp = i % 32;
+        const int c = c0 + cc, px = p0 + pp;
+        float v = 0.f;
+        if (c < C && px < HW) v = static_cast<float>(src[(size_t)c * HW + px]);
+        tile[pp][cc] = v * 0.25f;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 32 * 64; i += blockDim.x) {
+        const int pp = i / 64, cc = i % 64;
+        const int px = p0 + pp;
+        if (px >= HW || c0 + cc >= Kp) continue;
+        int row = px;
+        if (permute) {
+            const int h = px / W, w = px % W;
+            const int hb = h / kTH, r = h % kTH, wb = w / TW, c = w % TW;
+            row = ((hb * (W / TW) + wb) * kTH + r) * TW + c;
+        }
+        out[((size_t)e * HW + row) * Kp + c0 + cc] = static_cast<TOp>(tile[pp][cc]);
+    }
+}
+
+
+// ---------------------------------------------------------------- host side
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled get_encode() {
+    static EncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    });
+    return fn;
+}
+
+int make_map(CUtensorMap* map, void* base, CUtensorMapDataType dt, uint64_t rows, int Kp, int box_rows) {
+    EncodeTiled enc = get_encode();
+    if (!enc) return VIPE_ERR_CUDA;
+    const cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)Kp * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)kKC, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, dt, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? VIPE_OK : VIPE_ERR_CUDA;
+}
+
+int pick_tw(int W) {
+    if (W % 32 == 0) return 32;
+    if (W % 16 == 0) return 16;
+    if (W % 8 == 0) return 8;
+    return 0;
+}
+
+size_t smem_bytes(int KC, int N) { return a_region(KC) + 2 * KC * b_box(N) + 1024; }
+
+bool g_attr_set[64] = {false};
+
+}  // namespace cbuild
+}  // namespace vipe
+
+using namespace vipe;
+using namespace vipe::cbuild;
+
+extern "C" size_t vipe_corr_volume_workspace_size(int num, int C, int ht, int wd) {
+    if (num <= 0 || C <= 0 || ht <= 0 || wd <= 0) return 0;
+    const size_t Kp = (size_t)((C + kKC - 1) / kKC) * kKC;
+    const size_t rows = (size_t)num * ht * wd;
+    // error word + two packed operands (16-bit)
+    return 256 + 2 * (((rows * Kp * 2) + 255) & ~size_t(255));
+}
+
+extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* fmap1, const void* fmap2, int num,
+                                      int C, int ht, int wd, int num_levels, void* const* level_out, void* workspace,
+                                      size_t workspace_bytes, void* stream) {
+    if (num <= 0 || C <= 0 || ht <= 0 || wd <= 0 || num_levels < 1 || num_levels > 4) return VIPE_ERR_ARG;
+    if (!fmap1 || !fmap2 || !level_out || !workspace) return VIPE_ERR_ARG;
+    for (int l = 0; l < num_levels; l++)
+        if (!level_out[l]) return VIPE_ERR_ARG;
+    const int TW = pick_tw(wd);
+    if (TW == 0 || ht % kTH != 0) return VIPE_ERR_CAPACITY;  // fused pooling needs 8 x 8 closable blocks
+    const int Kp = ((C + kKC - 1) / kKC) * kKC;
+    if (Kp / kKC > kMaxKC) return VIPE_ERR_CAPACITY;
+    if (in_dtype != VIPE_F16 && in_dtype != VIPE_BF16 && in_dtype != VIPE_F32) return VIPE_ERR_DTYPE;
+    if (out_dtype != VIPE_F32 && out_dtype != VIPE_F16 && out_dtype != VIPE_BF16) return VIPE_ERR_DTYPE;
+    if (workspace_bytes < vipe_corr_volume_workspace_size(num, C, ht, wd)) return VIPE_ERR_WORKSPACE;
+    cudaStream_t st = as_stream(stream);
+    const int HW = ht * wd;
+    const size_t rows = (size_t)num * HW;
+    const size_t op_bytes = ((rows * Kp * 2) + 255) & ~size_t(255);
+    // workspace: [error word, 256 B][packed F1][packed F2]
+    char* ws = static_cast<char*>(workspace);
+    int* err = reinterpret_cast<int*>(ws);
+    void* pa = ws + 256;
+    void* pb = ws + 256 + op_bytes;
+    VIPE_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
+
+    // operand type: FP16 inputs stay FP16, others go to BF16
+    const int op_fmt = (in_dtype == VIPE_F16) ? 0 : 1;
+    dim3 pg(ceil_div(HW, 32), Kp / kKC, num);
+    {
+        VIPE_PROF("corr_pack", st);
+        for (int side = 0; side < 2; side++) {
+            const void* src = side == 0 ? fmap1 : fmap2;
+            void* dst = side == 0 ? pa : pb;
+            const int perm = side;
+            if (in_dtype == VIPE_F16)
+                pack_kernel<__half, __half><<<pg, 256, 0, st>>>(static_cast<const __half*>(src),
+                                                                static_cast<__half*>(dst), C, Kp, ht, wd, TW, perm);
+            else if (in_dtype == VIPE_BF16)
+                pack_kernel<__nv_bfloat16, __nv_bfloat16><<<pg, 256, 0, st>>>(
+                    static_cast<const __nv_bfloat16*>(src), static_cast<__nv_bfloat16*>(dst), C, Kp, ht, wd, TW, perm);
+            else
+                pack_kernel<float, __nv_bfloat16><<<pg, 256, 0, st>>>(static_cast<const float*>(src),
+                                                                      static_cast<__nv_bfloat16*>(dst), C, Kp, ht,
+                                                                      wd, TW, perm);
+            VIPE_LAUNCH_CHECK();
+        }
+    }
+    const int N = kTH * TW;
+    CUtensorMap mA, mB;
+    const CUtensorMapDataType dt = op_fmt == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    int rc;
+    if ((rc = make_map(&mA, pa, dt, rows, Kp, kBM)) != VIPE_OK) return rc;
+    if ((rc = make_map(&mB, pb, dt, rows, Kp, N)) != VIPE_OK) return rc;
+
+    Params p;
+    p.num = num; p.C = C; p.Kp = Kp; p.H = ht; p.W = wd; p.HW = HW; p.TW = TW; p.N = N; p.levels = num_levels;
+    p.mtiles = (HW + kBM - 1) / kBM;
+    p.ntiles = HW / N;
+    p.items = (long)num * p.mtiles;
+    p.out_dtype = out_dtype;
+    for (int l = 0; l < 4; l++) p.out[l] = l < num_levels ? level_out[l] : nullptr;
+    p.err = err;
+
+    int dev = 0, sms = 148;
+    VIPE_CUDA_TRY(cudaGetDevice(&dev));
+    VIPE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const size_t smem = smem_bytes(Kp / kKC, N);
+    const int smem_max = (int)smem_bytes(kMaxKC, 256);
+    if (dev < 64 && !g_attr_set[dev]) {
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(corr_build_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(corr_build_kernel<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(corr_build_kernel<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           smem_max));
+        g_attr_set[dev] = true;
+    }
+    const int grid = (int)std::min<long>(p.items, (long)sms);
+    VIPE_PROF("corr_build", st);
+    if (out_dtype == VIPE_F32)
+        corr_build_kernel<float><<<grid, kThreads, smem, st>>>(mA, mB, p, op_fmt);
+    else if (out_dtype == VIPE_F16)
+        corr_build_kernel<__half><<<grid, kThreads, smem, st>>>(mA, mB, p, op_fmt);
+    else
+        corr_build_kernel<__nv_bfloat16><<<grid, kThreads, smem, st>>>(mA, mB, p, op_fmt);
+    VIPE_LAUNCH_CHECK();
+    return VIPE_OK;
+}

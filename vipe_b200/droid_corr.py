@@ -1,0 +1,162 @@
+"""Correlation blocks of the DROID update operator on vipe_b200 kernels.
+
+Mirrors the API of the reference's vipe/slam/networks/droid_net.py:32-196
+(CorrSampler, CorrBlock, CorrLayer, AltCorrBlock) so FactorGraph-style callers
+can switch by import.  Differences from the reference:
+
+  * CorrBlock builds the all-pairs volume and its average-pooled pyramid in one
+    tcgen05 kernel per edge batch (vipe_corr_volume_build: BF16/FP16 operands,
+    FP32 accumulation in tensor memory, pooling fused into the epilogue) instead
+    of torch.matmul followed by three avg_pool2d passes;
+  * CorrSampler / CorrLayer backward return the exact coordinate gradient of the
+    bilinear lookup when ``exact_coords_grad`` is set (the reference returns no
+    or zero coordinate gradient).
+"""
+
+from __future__ import annotations
+
+import torch
+import torch.nn.functional as F
+
+from .ext import droid_net_ext
+
+
+class CorrSampler(torch.autograd.Function):
+    """Lookup in a materialised volume (reference droid_net.py:32-45)."""
+
+    @staticmethod
+    def forward(ctx, volume, coords, radius):
+        ctx.save_for_backward(volume, coords)
+        ctx.radius = radius
+        (corr,) = droid_net_ext.corr_index_forward(volume, coords, radius)
+        return corr
+
+    @staticmethod
+    def backward(ctx, grad_output):
+        volume, coords = ctx.saved_tensors
+        (grad_volume,) = droid_net_ext.corr_index_backward(volume, coords, grad_output.contiguous(), ctx.radius)
+        return grad_volume, None, None
+
+
+class CorrBlock:
+    """All-pairs correlation volume pyramid + radius lookup (reference droid_net.py:48-102).
+
+    fmap1, fmap2: (batch, num, C, H, W).  ``out_dtype`` selects the stored
+    volume type (the reference keeps the autocast type, fp16, under
+    FactorGraph); ``compute_dtype`` the tensor-core operand type.
+    """
+
+    def __init__(self, fmap1, fmap2, num_levels=4, radius=3, out_dtype=None, compute_dtype=None):
+        self.num_levels = num_levels
+        self.radius = radius
+        batch, num, dim, ht, wd = fmap1.shape
+        if out_dtype is None:
+            out_dtype = fmap1.dtype if fmap1.dtype in (torch.float16, torch.bfloat16) else torch.float32
+        from .corr_build import corr_volume_pyramid
+
+        levels = corr_volume_pyramid(fmap1.reshape(batch * num, dim, ht, wd), fmap2.reshape(batch * num, dim, ht, wd),
+                                     num_levels, out_dtype=out_dtype, compute_dtype=compute_dtype)
+        self.corr_pyramid = [lv.view(batch * num, ht, wd, lv.shape[-2], lv.shape[-1]) for lv in levels]
+
+    def __call__(self, coords):
+        out_pyramid = []
+        batch, num, ht, wd, _ = coords.shape
+        coords = coords.permute(0, 1, 4, 2, 3).contiguous().view(batch * num, 2, ht, wd)
+        for i in range(self.num_levels):
+            corr = CorrSampler.apply(self.corr_pyramid[i], (coords / 2**i).contiguous(), self.radius)
+            out_pyramid.append(corr.view(batch, num, -1, ht, wd))
+        return torch.cat(out_pyramid, dim=2)
+
+    def cat(self, other):
+        for i in range(self.num_levels):
+            self.corr_pyramid[i] = torch.cat([self.corr_pyramid[i], other.corr_pyramid[i]], 0)
+        return self
+
+    def __getitem__(self, index):
+        for i in range(self.num_levels):
+            self.corr_pyramid[i] = self.corr_pyramid[i][index]
+        return self
+
+    @staticmethod
+    def corr(fmap1, fmap2):
+        """All-pairs correlation (batch, num, H, W, H, W) of (fmap1/4)^T (fmap2/4)."""
+        from .corr_build import corr_volume_pyramid
+
+        batch, num, dim, ht, wd = fmap1.shape
+        (v,) = corr_volume_pyramid(fmap1.reshape(batch * num, dim, ht, wd), fmap2.reshape(batch * num, dim, ht, wd),
+                                   1, out_dtype=torch.float32)
+        return v.view(batch, num, ht, wd, ht, wd)
+
+
+class CorrLayer(torch.autograd.Function):
+    """On-the-fly lookup (reference droid_net.py:105-118)."""
+
+    exact_coords_grad = False
+
+    @staticmethod
+    def forward(ctx, fmap1, fmap2, coords, r):
+        ctx.r = r
+        ctx.save_for_backward(fmap1, fmap2, coords)
+        (corr,) = droid_net_ext.altcorr_forward(fmap1, fmap2, coords, ctx.r)
+        return corr
+
+    @staticmethod
+    def backward(ctx, grad_corr):
+        fmap1, fmap2, coords = ctx.saved_tensors
+        g1, g2, gc = droid_net_ext.altcorr_backward(fmap1, fmap2, coords, grad_corr.contiguous(), ctx.r,
+                                                    CorrLayer.exact_coords_grad)
+        return g1, g2, gc, None
+
+
+class AltCorrBlock:
+    """Lookup without a materialised volume (reference droid_net.py:121-196).
+
+    fmaps: (B, N, C, H, W).  The pyramid is fmaps / 4 average-pooled per level
+    and stored channels-last (B, N, H_l, W_l, C), floor sizes.
+    """
+
+    def __init__(self, fmaps, num_levels=4, radius=3):
+        self.num_levels = num_levels
+        self.radius = radius
+        B, N, C, H, W = fmaps.shape
+        f = fmaps.view(B * N, C, H, W) / 4.0
+        self.pyramid = []
+        for i in range(num_levels):
+            self.pyramid.append(f.permute(0, 2, 3, 1).contiguous().view(B, N, H // 2**i, W // 2**i, C))
+            f = F.avg_pool2d(f, 2, stride=2)
+
+    def corr_fn_reference(self, coords, ii, jj):
+        """Per-level on-the-fly lookup in fp32 (the reference's checking route)."""
+        B, N, H, W, S, _ = coords.shape
+        coords = coords.permute(0, 1, 4, 2, 3, 5)
+        out = []
+        for i in range(self.num_levels):
+            f1 = self.pyramid[0][:, ii]
+            f2 = self.pyramid[i][:, jj]
+            ci = (coords / 2**i).reshape(B * N, S, H, W, 2).contiguous()
+            f1 = f1.reshape((B * N,) + f1.shape[2:])
+            f2 = f2.reshape((B * N,) + f2.shape[2:])
+            corr = CorrLayer.apply(f1.float().contiguous(), f2.float().contiguous(), ci, self.radius)
+            out.append(corr.view(B, N, S, -1, H, W).permute(0, 1, 3, 4, 5, 2))
+        return torch.cat(out, dim=2)
+
+    def corr_fn_indexed(self, coords, ii, jj):
+        if coords.shape[-2] != 1:
+            return self.corr_fn_reference(coords, ii, jj)
+        coords = coords.squeeze(dim=-2).contiguous()
+        (corr,) = droid_net_ext.altcorr_index_forward(self.pyramid[0], self.pyramid, coords, ii.contiguous(),
+                                                      jj.contiguous(), self.radius)
+        return corr.unsqueeze(dim=-1)
+
+    def corr_fn(self, coords, ii, jj):
+        return self.corr_fn_indexed(coords, ii, jj)
+
+    def __call__(self, coords, ii, jj):
+        squeeze = False
+        if coords.dim() == 5:
+            coords = coords.unsqueeze(dim=-2)
+            squeeze = True
+        corr = self.corr_fn(coords, ii, jj)
+        if squeeze:
+            corr = corr.squeeze(dim=-1)
+        return corr.contiguous()
