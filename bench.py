@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-s", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-corr", action="store_true")
     return ap.parse_args()
 
 
@@ -174,6 +175,79 @@ def profile_kernels(lib, run_once, n):
         nm = names.raw[k * stride:(k + 1) * stride].split(b"\0")[0].decode()
         out[nm] = (ms[k], cnt[k])
     return out
+
+
+def corr_build_bench(dev, steps, hbm_peak, peak_src, bf16_peak):
+    """Correlation volume + 4-level pyramid at 640 edges, 128 ch, 48x64 (BF16 operands).
+
+    Algorithmic bytes = BF16 inputs read (2 x 640 x 128 x 3072 x 2 B) + FP16
+    pyramid written (640 x 3072 x 3072 x (1 + 1/4 + 1/16 + 1/64) x 2 B).
+    Also times the reference's GPU path for the same product: torch.matmul
+    (cuBLAS, fp16) of the /4-scaled maps and three avg_pool2d passes.
+    """
+    import torch
+    import torch.nn.functional as F
+
+    from vipe_b200.corr_build import corr_volume_pyramid
+
+    E, C, H, W = 640, 128, 48, 64
+    HW = H * W
+    g = torch.Generator(device=dev).manual_seed(1002)
+    f1 = (torch.randn(E, C, H, W, generator=g, device=dev) / C**0.5).to(torch.bfloat16)
+    f2 = (torch.randn(E, C, H, W, generator=g, device=dev) / C**0.5).to(torch.bfloat16)
+    for _ in range(2):
+        lv = corr_volume_pyramid(f1, f2, 4, out_dtype=torch.float16, check=True)
+    del lv
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    outs = None
+    for k in range(steps):
+        evs[k][0].record(stream)
+        outs = corr_volume_pyramid(f1, f2, 4, out_dtype=torch.float16, check=False)
+        evs[k][1].record(stream)
+        torch.cuda.synchronize(dev)
+        del outs
+    ms = sorted(a.elapsed_time(b) for a, b in evs)[len(evs) // 2]
+    out_bytes = E * HW * HW * (1 + 1 / 4 + 1 / 16 + 1 / 64) * 2
+    in_bytes = 2 * E * C * HW * 2
+    flops = 2.0 * E * HW * HW * C
+    ach = (out_bytes + in_bytes) / (ms / 1e3) / 1e9
+    # reference GPU path (cuBLAS matmul + avg_pool2d), fp16 as under the reference's autocast
+    a = (f1.to(torch.float16) / 4.0).reshape(E, C, HW)
+    b = (f2.to(torch.float16) / 4.0).reshape(E, C, HW)
+    chunk = 160
+
+    def ref_path():
+        for s0 in range(0, E, chunk):
+            corr = torch.matmul(a[s0:s0 + chunk].transpose(1, 2), b[s0:s0 + chunk])
+            corr = corr.reshape(-1, 1, H, W)
+            for _ in range(3):
+                corr = F.avg_pool2d(corr, 2, stride=2)
+    ref_path()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ref_path()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ref_ms = e0.elapsed_time(e1)
+    return {
+        "workload": "correlation volume + 4-level avg-pool pyramid, 640 edges, 128 ch, 48x64, BF16 operands, "
+        "FP32 accumulate, FP16 volume",
+        "ms_per_build": ms,
+        "achieved": ach,
+        "peak": hbm_peak,
+        "unit": "GB/s",
+        "bound": "hbm",
+        "frac": ach / hbm_peak,
+        "peak_source": peak_src,
+        "bytes_per_build": out_bytes + in_bytes,
+        "tflops": flops / (ms / 1e3) / 1e12,
+        "tensor_frac_of_bf16_peak": flops / (ms / 1e3) / 1e12 / bf16_peak,
+        "reference_cublas_matmul_avgpool_ms": ref_ms,
+        "speedup_vs_reference_gpu_path": ref_ms / ms,
+    }
 
 
 def cpu_baseline(p, sample_s):
@@ -374,6 +448,11 @@ def run_ours(args):
     breakdown = {k: {"ms_per_solve": v[0] / len(prof_states), "share": v[0] / total_prof} for k, v in prof.items()}
 
     launches_per_solve = sum(v[1] for v in prof.values()) / len(prof_states)
+    corr = None
+    if not args.no_corr:
+        del states, prof_states
+        torch.cuda.empty_cache()
+        corr = corr_build_bench(dev, 5, hbm, src, bf16)
 
     line = None
     if rank == 0:
@@ -410,6 +489,7 @@ def run_ours(args):
             "kernel_breakdown": breakdown,
             "gpu_launches": int(launches_per_solve * args.steps),
             "clocks": clk.summary(),
+            "corr": corr,
         }
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(p, args.cpu_sample_s)

@@ -120,16 +120,22 @@ int vipe_slam_ba_index_debug(const int64_t* ii, const int64_t* jj, int num_frame
                              int* num_pairs, void* workspace, size_t workspace_bytes, void* stream);
 
 /* Replaces slam_ext.frame_distance (reference: geom_kernels.cu:613-768,
- * 1849-1877).  poses (NV,7), disps (ND,ht,wd), intrinsics (V,4), pi,pj,qi,qj,di
- * (num,) int64 -> dist_out (num,) f32. */
+ * 1849-1877).  poses (num_poses,7), disps (num_disps,ht,wd), intrinsics
+ * (num_views,4), pi,pj (pose rows), qi,qj (intrinsics rows), di (disp rows)
+ * (num,) int64 -> dist_out (num,) f32.  A pair with an index outside its
+ * tensor gets NaN (the reference reads out of bounds). */
 int vipe_slam_frame_distance(const float* poses, const float* disps, const float* intrinsics, const int64_t* pi,
                              const int64_t* pj, const int64_t* qi, const int64_t* qj, const int64_t* di, int num,
-                             int ht, int wd, float beta, float* dist_out, void* stream);
+                             int num_poses, int num_disps, int num_views, int ht, int wd, float beta, float* dist_out,
+                             void* stream);
 
 /* Replaces slam_ext.projmap (reference: geom_kernels.cu:526-611, 1879-1903).
- * -> coords_out (num,ht,wd,3) f32 (third channel 0), valid_out (num,ht,wd,1). */
+ * poses (num_frames,7), disps (num_frames,ht,wd), ii,jj (num,) int64
+ * -> coords_out (num,ht,wd,3) f32 (third channel 0), valid_out (num,ht,wd,1);
+ * NaN for an edge with an index outside [0, num_frames). */
 int vipe_slam_projmap(const float* poses, const float* disps, const float* intrinsics, const int64_t* ii,
-                      const int64_t* jj, int num, int ht, int wd, float* coords_out, float* valid_out, void* stream);
+                      const int64_t* jj, int num, int num_frames, int ht, int wd, float* coords_out, float* valid_out,
+                      void* stream);
 
 /* Replaces slam_ext.depth_filter (reference: geom_kernels.cu:770-885,
  * 1905-1929).  ix (num,) int64, thresh (num,) f32 -> counter_out (num,ht,wd). */

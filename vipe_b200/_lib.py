@@ -36,8 +36,8 @@ _SIGS: dict[str, tuple] = {
     ),
     "vipe_slam_ba": (I, [P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, F, I, F, P, P, P, P, SZ, P, P]),
     "vipe_slam_ba_index_debug": (I, [P, P, I, I, I, I, I, P, P, P, I, P, P, SZ, P]),
-    "vipe_slam_frame_distance": (I, [P, P, P, P, P, P, P, P, I, I, I, F, P, P]),
-    "vipe_slam_projmap": (I, [P, P, P, P, P, I, I, I, P, P, P]),
+    "vipe_slam_frame_distance": (I, [P, P, P, P, P, P, P, P, I, I, I, I, I, I, F, P, P]),
+    "vipe_slam_projmap": (I, [P, P, P, P, P, I, I, I, I, P, P, P]),
     "vipe_slam_depth_filter": (I, [P, P, P, P, P, I, I, I, I, P, P]),
     "vipe_slam_iproj": (I, [P, P, P, I, I, I, P, P]),
     "vipe_corr_index_forward": (I, [I, P, P, I, I, I, I, I, I, P, P]),

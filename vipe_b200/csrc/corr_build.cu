@@ -171,58 +171,97 @@ __device__ __forceinline__ __half cvt<__half>(float v) { return __float2half_rn(
 template <>
 __device__ __forceinline__ __nv_bfloat16 cvt<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
 
-template <typename T, int N>
-__device__ __forceinline__ void store_row(T* dst, const float* v) {
-    // N contiguous elements; 16-byte aligned whenever N * sizeof(T) is a multiple of 16
-    if constexpr ((N * sizeof(T)) % 16 == 0) {
-#pragma unroll
-        for (int i = 0; i < N; i += 16 / (int)sizeof(T)) {
+// Epilogue staging.  Each epilogue warp owns 32 source rows; a pass covers 16
+// target columns (two 8x8 blocks) of all 8 target rows.  Per row the staged
+// bytes are: level 0 8 x 16, level 1 4 x 8, level 2 2 x 4, level 3 1 x 2
+// elements; row strides are padded to 16 (mod 128) bytes so that each
+// quarter-warp's 16-byte accesses hit distinct bank groups.
+constexpr int kPassW = 16;
+
+template <typename T>
+struct Stage {
+    static constexpr int sz = (int)sizeof(T);
+    static constexpr int r0 = 8 * kPassW * sz + 16;        // level 0 row stride (bytes)
+    static constexpr int r1 = 4 * (kPassW / 2) * sz + 16;  // level 1
+    static constexpr int r2 = 2 * (kPassW / 4) * sz + 16;  // level 2
+    static constexpr int r3 = 16;                          // level 3 (2 values)
+    static constexpr int per_warp = 32 * (r0 + r1 + r2 + r3);
+};
+
+template <typename T>
+__device__ __forceinline__ void sts_vals(uint8_t* dst, const float* v, int n) {
+    // n values -> packed type T at dst (16-byte aligned when n * sizeof(T) >= 16)
+    if ((n * (int)sizeof(T)) % 16 == 0) {
+        for (int i = 0; i < n; i += 16 / (int)sizeof(T)) {
             alignas(16) T tmp[16 / sizeof(T)];
 #pragma unroll
             for (int k = 0; k < (int)(16 / sizeof(T)); k++) tmp[k] = cvt<T>(v[i + k]);
-            *reinterpret_cast<uint4*>(dst + i) = *reinterpret_cast<const uint4*>(tmp);
+            *reinterpret_cast<uint4*>(dst + i * sizeof(T)) = *reinterpret_cast<const uint4*>(tmp);
         }
     } else {
-#pragma unroll
-        for (int i = 0; i < N; i++) dst[i] = cvt<T>(v[i]);
+        T* d = reinterpret_cast<T*>(dst);
+        for (int i = 0; i < n; i++) d[i] = cvt<T>(v[i]);
     }
 }
 
-// one 8x8 target block of one source row: level 0 plus pools
+// pools one 8x8 block (rows r, cols c) and stages all levels at column block cb (0/1 of the pass)
 template <typename T>
-__device__ __forceinline__ void emit_block(const Params& p, long row, int h0, int w0, const float (&blk)[8][8]) {
-    const int H = p.H, W = p.W;
+__device__ __forceinline__ void stage_block(uint8_t* st, int lane, int cb, const float (&blk)[8][8]) {
+    using S = Stage<T>;
+    uint8_t* s0 = st;
+    uint8_t* s1 = s0 + 32 * S::r0;
+    uint8_t* s2 = s1 + 32 * S::r1;
+    uint8_t* s3 = s2 + 32 * S::r2;
 #pragma unroll
-    for (int r = 0; r < 8; r++) store_row<T, 8>(static_cast<T*>(p.out[0]) + (row * H + h0 + r) * W + w0, blk[r]);
-    if (p.levels > 1) {
-        float l1[4][4];
+    for (int r = 0; r < 8; r++) sts_vals<T>(s0 + lane * S::r0 + (r * kPassW + cb * 8) * S::sz, blk[r], 8);
+    float l1[4][4];
 #pragma unroll
-        for (int r = 0; r < 4; r++)
+    for (int r = 0; r < 4; r++)
 #pragma unroll
-            for (int c = 0; c < 4; c++)
-                l1[r][c] = 0.25f * (blk[2 * r][2 * c] + blk[2 * r][2 * c + 1] + blk[2 * r + 1][2 * c] +
-                                    blk[2 * r + 1][2 * c + 1]);
-        const int H1 = H >> 1, W1 = W >> 1;
+        for (int c = 0; c < 4; c++)
+            l1[r][c] = 0.25f * (blk[2 * r][2 * c] + blk[2 * r][2 * c + 1] + blk[2 * r + 1][2 * c] + blk[2 * r + 1][2 * c + 1]);
 #pragma unroll
-        for (int r = 0; r < 4; r++)
-            store_row<T, 4>(static_cast<T*>(p.out[1]) + (row * H1 + (h0 >> 1) + r) * W1 + (w0 >> 1), l1[r]);
-        if (p.levels > 2) {
-            float l2[2][2];
+    for (int r = 0; r < 4; r++) sts_vals<T>(s1 + lane * S::r1 + (r * (kPassW / 2) + cb * 4) * S::sz, l1[r], 4);
+    float l2[2][2];
 #pragma unroll
-            for (int r = 0; r < 2; r++)
+    for (int r = 0; r < 2; r++)
 #pragma unroll
-                for (int c = 0; c < 2; c++)
-                    l2[r][c] = 0.25f * (l1[2 * r][2 * c] + l1[2 * r][2 * c + 1] + l1[2 * r + 1][2 * c] +
-                                        l1[2 * r + 1][2 * c + 1]);
-            const int H2 = H >> 2, W2 = W >> 2;
+        for (int c = 0; c < 2; c++)
+            l2[r][c] = 0.25f * (l1[2 * r][2 * c] + l1[2 * r][2 * c + 1] + l1[2 * r + 1][2 * c] + l1[2 * r + 1][2 * c + 1]);
 #pragma unroll
-            for (int r = 0; r < 2; r++)
-                store_row<T, 2>(static_cast<T*>(p.out[2]) + (row * H2 + (h0 >> 2) + r) * W2 + (w0 >> 2), l2[r]);
-            if (p.levels > 3) {
-                const float l3 = 0.25f * (l2[0][0] + l2[0][1] + l2[1][0] + l2[1][1]);
-                const int H3 = H >> 3, W3 = W >> 3;
-                static_cast<T*>(p.out[3])[(row * H3 + (h0 >> 3)) * W3 + (w0 >> 3)] = cvt<T>(l3);
-            }
+    for (int r = 0; r < 2; r++) sts_vals<T>(s2 + lane * S::r2 + (r * (kPassW / 4) + cb * 2) * S::sz, l2[r], 2);
+    const float l3 = 0.25f * (l2[0][0] + l2[0][1] + l2[1][0] + l2[1][1]);
+    sts_vals<T>(s3 + lane * S::r3 + cb * S::sz, &l3, 1);
+}
+
+// copies a staged level of the warp's 32 rows to global: `nseg` segments of
+// `seg` bytes per row, `sstride` bytes apart in shared memory; segment j of
+// row i goes to gbase + (row0 + i) * grow_stride + j * gseg_stride
+template <typename T>
+__device__ __forceinline__ void flush_level(const uint8_t* st, int rstride, int nseg, int seg, int sstride, long row0,
+                                            int nrows, uint8_t* gbase, long grow_stride, long gseg_stride, int lane) {
+    if (seg >= 16) {
+        const int cps = seg / 16;  // 16-byte chunks per segment
+        const int total = 32 * nseg * cps;
+        for (int j = lane; j < total; j += 32) {
+            const int k = j % cps, sg = (j / cps) % nseg, i = j / (cps * nseg);
+            if (i >= nrows) continue;
+            const uint4 v = *reinterpret_cast<const uint4*>(st + i * rstride + sg * sstride + k * 16);
+            *reinterpret_cast<uint4*>(gbase + (row0 + i) * grow_stride + sg * gseg_stride + k * 16) = v;
+        }
+    } else {
+        const int total = 32 * nseg;
+        for (int j = lane; j < total; j += 32) {
+            const int sg = j % nseg, i = j / nseg;
+            if (i >= nrows) continue;
+            const uint8_t* src = st + i * rstride + sg * sstride;
+            uint8_t* dst = gbase + (row0 + i) * grow_stride + sg * gseg_stride;
+            if (seg == 8)
+                *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(src);
+            else if (seg == 4)
+                *reinterpret_cast<uint32_t*>(dst) = *reinterpret_cast<const uint32_t*>(src);
+            else
+                *reinterpret_cast<uint16_t*>(dst) = *reinterpret_cast<const uint16_t*>(src);
         }
     }
 }
@@ -251,6 +290,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int N = p.N;
     auto sa = [&](int kc) { return sbase + (size_t)kc * kBM * 128; };
     auto sb = [&](int st, int kc) { return sbase + a_region(KC) + ((size_t)st * KC + kc) * b_box(N); };
+    const int NBS = (int)sizeof(TOut) == 4 ? 1 : 2;  // B stages (FP32 staging needs the room of one)
+    const size_t stage_off = a_region(KC) + (size_t)NBS * KC * b_box(N);
 
     if (tid == 0) {
         fail = 0;
@@ -286,8 +327,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int kc = 0; kc < KC; kc++)
                 tma_load_2d(sa(kc), &mapA, &barA_full, kc * kKC, e * p.HW + mt * kBM);
             for (int nt = 0; nt < p.ntiles; nt++, t++) {
-                const int s = t & 1;
-                if (t >= 2 && !mbar_wait(&barB_empty[s], ((t >> 1) - 1) & 1, &fail)) break;
+                const int s = (int)(t % NBS);
+                const uint32_t use = t / NBS;
+                if (use >= 1 && !mbar_wait(&barB_empty[s], (use - 1) & 1, &fail)) break;
                 mbar_expect_tx(&barB_full[s], b_bytes);
                 for (int kc = 0; kc < KC; kc++)
                     tma_load_2d(sb(s, kc), &mapB, &barB_full[s], kc * kKC, e * p.HW + nt * N);
@@ -295,7 +337,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         // drain: the last loads issued must land before the CTA exits
         if (fail && t > 0) {
-            mbar_wait(&barB_full[(t - 1) & 1], ((t - 1) >> 1) & 1, &fail);
+            // bounded; returns at once if the last stage already completed
+            const uint32_t last = t - 1;
+            const uint64_t t0 = gtimer();
+            while (!mbar_try_wait(&barB_full[last % NBS], (last / NBS) & 1) && gtimer() - t0 < kWaitNs) {
+            }
         }
     } else if (warp == 1 && lane == 0) {
         // ------------------------------------------------ MMA issuer
@@ -305,8 +351,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (!mbar_wait(&barA_full, it & 1, &fail)) break;
             tc_fence_after();
             for (int nt = 0; nt < p.ntiles; nt++, t++) {
-                const int s = t & 1, acc = t & 1;
-                if (!mbar_wait(&barB_full[s], (t >> 1) & 1, &fail)) break;
+                const int s = (int)(t % NBS), acc = t & 1;
+                if (!mbar_wait(&barB_full[s], (t / NBS) & 1, &fail)) break;
                 if (t >= 2 && !mbar_wait(&barAcc_empty[acc], ((t >> 1) - 1) & 1, &fail)) break;
                 tc_fence_after();
                 const uint32_t d = tmem + (uint32_t)(acc * 256);
@@ -327,30 +373,65 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (warp >= 4) {
         // ------------------------------------------------ epilogue
         const int q = warp - 4;                 // TMEM lane quarter
-        const int mrow = q * 32 + lane;          // row of the 128-row tile
         const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
         const int TW = p.TW, blocks_w = p.W / TW;
+        using St = Stage<TOut>;
+        uint8_t* st = sbase + stage_off + (size_t)q * St::per_warp;
+        const int sz = (int)sizeof(TOut);
         uint32_t t = 0;
         for (long item = blockIdx.x; item < p.items && !fail; item += gridDim.x) {
             const int e = (int)(item / p.mtiles), mt = (int)(item % p.mtiles);
-            const int m = mt * kBM + mrow;
+            const int m0 = mt * kBM + q * 32;               // first source row of this warp
+            const int nrows = max(0, min(32, p.HW - m0));
+            const long row0 = (long)e * p.HW + m0;
             for (int nt = 0; nt < p.ntiles; nt++, t++) {
                 const int acc = t & 1;
                 if (!mbar_wait(&barAcc_full[acc], (t >> 1) & 1, &fail)) break;
                 tc_fence_after();
                 const int hb = nt / blocks_w, wb = nt % blocks_w;
-                const long row = (long)e * p.HW + m;
-                for (int c0 = 0; c0 < TW; c0 += 8) {
-                    float blk[8][8];
+                const int passes = (TW + kPassW - 1) / kPassW;
+                for (int ps = 0; ps < passes; ps++) {
+                    const int pw = min(kPassW, TW - ps * kPassW);  // 16 or 8 columns in this pass
+                    for (int cb = 0; cb < pw / 8; cb++) {
+                        float blk[8][8];
+                        const int c0 = ps * kPassW + cb * 8;
 #pragma unroll
-                    for (int r = 0; r < 8; r++)
-                        tmem_ld8(tmem + lane_addr + (uint32_t)(acc * 256 + r * TW + c0), blk[r]);
-                    tmem_wait_ld();
-                    if (m < p.HW) emit_block<TOut>(p, row, hb * kTH, wb * TW + c0, blk);
+                        for (int r = 0; r < 8; r++)
+                            tmem_ld8(tmem + lane_addr + (uint32_t)(acc * 256 + r * TW + c0), blk[r]);
+                        tmem_wait_ld();
+                        stage_block<TOut>(st, lane, cb, blk);
+                    }
+                    if (ps == passes - 1) {
+                        // all of this accumulator is in registers / staging: release TMEM early
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&barAcc_empty[acc]);
+                    }
+                    __syncwarp();
+                    const int h0 = hb * kTH, w0 = wb * TW + ps * kPassW;
+                    uint8_t* s0 = st;
+                    uint8_t* s1 = s0 + 32 * St::r0;
+                    uint8_t* s2 = s1 + 32 * St::r1;
+                    uint8_t* s3 = s2 + 32 * St::r2;
+                    // level l row of the output volume: (row, H_l, W_l)
+                    const int H = p.H, W = p.W;
+                    flush_level<TOut>(s0, St::r0, 8, pw * sz, kPassW * sz, row0, nrows,
+                                      static_cast<uint8_t*>(p.out[0]) + ((long)h0 * W + w0) * sz, (long)H * W * sz,
+                                      (long)W * sz, lane);
+                    if (p.levels > 1)
+                        flush_level<TOut>(s1, St::r1, 4, (pw / 2) * sz, (kPassW / 2) * sz, row0, nrows,
+                                          static_cast<uint8_t*>(p.out[1]) + ((long)(h0 >> 1) * (W >> 1) + (w0 >> 1)) * sz,
+                                          (long)(H >> 1) * (W >> 1) * sz, (long)(W >> 1) * sz, lane);
+                    if (p.levels > 2)
+                        flush_level<TOut>(s2, St::r2, 2, (pw / 4) * sz, (kPassW / 4) * sz, row0, nrows,
+                                          static_cast<uint8_t*>(p.out[2]) + ((long)(h0 >> 2) * (W >> 2) + (w0 >> 2)) * sz,
+                                          (long)(H >> 2) * (W >> 2) * sz, (long)(W >> 2) * sz, lane);
+                    if (p.levels > 3)
+                        flush_level<TOut>(s3, St::r3, 1, (pw / 8) * sz, (kPassW / 8) * sz, row0, nrows,
+                                          static_cast<uint8_t*>(p.out[3]) + ((long)(h0 >> 3) * (W >> 3) + (w0 >> 3)) * sz,
+                                          (long)(H >> 3) * (W >> 3) * sz, (long)(W >> 3) * sz, lane);
+                    __syncwarp();
                 }
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&barAcc_empty[acc]);
             }
         }
     }
@@ -436,7 +517,11 @@ int pick_tw(int W) {
     return 0;
 }
 
-size_t smem_bytes(int KC, int N) { return a_region(KC) + 2 * KC * b_box(N) + 1024; }
+template <typename T>
+size_t smem_bytes(int KC, int N) {
+    const int nbs = sizeof(T) == 4 ? 1 : 2;
+    return a_region(KC) + (size_t)nbs * KC * b_box(N) + 4 * (size_t)Stage<T>::per_warp + 1024;
+}
 
 bool g_attr_set[64] = {false};
 
@@ -520,13 +605,18 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
     int dev = 0, sms = 148;
     VIPE_CUDA_TRY(cudaGetDevice(&dev));
     VIPE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const size_t smem = smem_bytes(Kp / kKC, N);
-    const int smem_max = (int)smem_bytes(kMaxKC, 256);
+    size_t smem;
+    if (out_dtype == VIPE_F32)
+        smem = smem_bytes<float>(Kp / kKC, N);
+    else
+        smem = smem_bytes<__half>(Kp / kKC, N);
     if (dev < 64 && !g_attr_set[dev]) {
-        VIPE_CUDA_TRY(cudaFuncSetAttribute(corr_build_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
-        VIPE_CUDA_TRY(cudaFuncSetAttribute(corr_build_kernel<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(corr_build_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem_bytes<float>(kMaxKC, 256)));
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(corr_build_kernel<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem_bytes<__half>(kMaxKC, 256)));
         VIPE_CUDA_TRY(cudaFuncSetAttribute(corr_build_kernel<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           smem_max));
+                                           (int)smem_bytes<__nv_bfloat16>(kMaxKC, 256)));
         g_attr_set[dev] = true;
     }
     const int grid = (int)std::min<long>(p.items, (long)sms);

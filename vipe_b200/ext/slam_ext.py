@@ -8,8 +8,10 @@ library on the tensors' current stream.
 Differences, all on inputs the reference does not define:
   * edge indices outside [0, num_frames) raise RuntimeError (the reference reads
     out of bounds);
-  * a window with more than 1024 poses, or a depth frame coupled to more than 32
-    window poses, raises RuntimeError (documented kernel limits).
+  * a window with more than 127 poses (6*127+1 unknowns fill the shared-memory
+    panel of the on-device Cholesky), or a depth frame coupled to more than 32
+    window poses, raises RuntimeError (documented kernel limits);
+  * frame_distance / projmap entries with out-of-range indices are NaN.
 A Cholesky failure leaves dx = 0 silently, as in the reference
 (geom_kernels.cu:1283-1285); ``last_solver_failed()`` reports it.
 """
@@ -229,7 +231,8 @@ def frame_distance(poses, disps, intrinsics, pi, pj, qi, qj, di, beta):
     if num > 0:
         rc = _lib.load().vipe_slam_frame_distance(
             poses.data_ptr(), disps.data_ptr(), intrinsics.data_ptr(), pi.data_ptr(), pj.data_ptr(),
-            qi.data_ptr(), qj.data_ptr(), di.data_ptr(), num, ht, wd, float(beta), dist.data_ptr(),
+            qi.data_ptr(), qj.data_ptr(), di.data_ptr(), num, poses.shape[0], disps.shape[0],
+            intrinsics.numel() // 4, ht, wd, float(beta), dist.data_ptr(),
             _lib.stream_of(poses),
         )
         _lib.check(rc, "slam_ext.frame_distance")
@@ -252,8 +255,8 @@ def projmap(poses, disps, intrinsics, ii, jj):
     valid = torch.zeros(num, ht, wd, 1, dtype=torch.float32, device=poses.device)
     if num > 0:
         rc = _lib.load().vipe_slam_projmap(
-            poses.data_ptr(), disps.data_ptr(), intrinsics.data_ptr(), ii.data_ptr(), jj.data_ptr(), num, ht, wd,
-            coords.data_ptr(), valid.data_ptr(), _lib.stream_of(poses),
+            poses.data_ptr(), disps.data_ptr(), intrinsics.data_ptr(), ii.data_ptr(), jj.data_ptr(), num,
+            min(poses.shape[0], disps.shape[0]), ht, wd, coords.data_ptr(), valid.data_ptr(), _lib.stream_of(poses),
         )
         _lib.check(rc, "slam_ext.projmap")
     return [coords, valid]
@@ -270,6 +273,7 @@ def depth_filter(poses, disps, intrinsics, ix, thresh):
     _lib.require_dtype("ix", ix, torch.int64)
     num = ix.shape[0]
     nf, ht, wd = disps.shape
+    nf = min(nf, poses.shape[0])
     counter = torch.zeros(num, ht, wd, dtype=torch.float32, device=disps.device)
     if num > 0:
         rc = _lib.load().vipe_slam_depth_filter(
@@ -287,6 +291,8 @@ def iproj(poses, disps, intrinsics):
         _lib.require_contiguous(name, t)
         _lib.require_dtype(name, t, torch.float32)
     nf, ht, wd = disps.shape
+    if poses.shape[0] < nf:
+        raise RuntimeError("iproj: poses has fewer rows than disps")
     points = torch.zeros(nf, ht, wd, 3, dtype=torch.float32, device=disps.device)
     rc = _lib.load().vipe_slam_iproj(
         poses.data_ptr(), disps.data_ptr(), intrinsics.data_ptr(), nf, ht, wd, points.data_ptr(),
