@@ -41,7 +41,9 @@ constexpr int kBM = 128;       // source pixels per tile (TMEM lanes)
 constexpr int kTH = 8;         // target rows per N tile
 constexpr int kKC = 64;        // channels per TMA box / swizzle row (128 B of 16-bit)
 constexpr int kMaxKC = 2;      // up to 128 channels (A + two B stages fit in shared memory)
-constexpr int kThreads = 256;  // 8 warps
+constexpr int kThreads = 320;  // 8 epilogue warps, 1 TMA warp, 1 MMA warp
+constexpr int kEpiWarps = 8;
+constexpr int kTmaWarp = 8, kMmaWarp = 9;
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s bound on any mbarrier wait
 
 struct Params {
@@ -171,99 +173,141 @@ __device__ __forceinline__ __half cvt<__half>(float v) { return __float2half_rn(
 template <>
 __device__ __forceinline__ __nv_bfloat16 cvt<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
 
-// Epilogue staging.  Each epilogue warp owns 32 source rows; a pass covers 16
-// target columns (two 8x8 blocks) of all 8 target rows.  Per row the staged
-// bytes are: level 0 8 x 16, level 1 4 x 8, level 2 2 x 4, level 3 1 x 2
-// elements; row strides are padded to 16 (mod 128) bytes so that each
-// quarter-warp's 16-byte accesses hit distinct bank groups.
-constexpr int kPassW = 16;
-
+// Epilogue staging.  Eight epilogue warps: warp w owns TMEM lane quarter
+// w % 4 (32 source rows) and half w / 4 of the tile's TW target columns, taken
+// in passes of PW columns (16 for 16-bit output, 8 for FP32).  A pass stages,
+// per source row: level 0 8 x PW, level 1 4 x PW/2, level 2 2 x PW/4, level 3
+// 1 x PW/8 elements; row strides are 16 (mod 128) bytes or odd multiples of 16,
+// so each quarter-warp's accesses hit distinct bank groups.  The staged pass is
+// then written with 16-byte (level 0/1), 8-byte and 4-byte stores in which
+// consecutive lanes cover consecutive bytes of one output row segment.
 template <typename T>
 struct Stage {
     static constexpr int sz = (int)sizeof(T);
-    static constexpr int r0 = 8 * kPassW * sz + 16;        // level 0 row stride (bytes)
-    static constexpr int r1 = 4 * (kPassW / 2) * sz + 16;  // level 1
-    static constexpr int r2 = 2 * (kPassW / 4) * sz + 16;  // level 2
-    static constexpr int r3 = 16;                          // level 3 (2 values)
+    static constexpr int PW = sz == 4 ? 8 : 16;
+    static constexpr int r0 = 8 * PW * sz + 16;         // level 0 row stride (bytes)
+    static constexpr int r1 = 4 * (PW / 2) * sz + 16;   // level 1
+    static constexpr int r2 = 2 * (PW / 4) * sz + 16;   // level 2
+    static constexpr int r3 = 16;                       // level 3
     static constexpr int per_warp = 32 * (r0 + r1 + r2 + r3);
 };
 
 template <typename T>
-__device__ __forceinline__ void sts_vals(uint8_t* dst, const float* v, int n) {
-    // n values -> packed type T at dst (16-byte aligned when n * sizeof(T) >= 16)
-    if ((n * (int)sizeof(T)) % 16 == 0) {
-        for (int i = 0; i < n; i += 16 / (int)sizeof(T)) {
-            alignas(16) T tmp[16 / sizeof(T)];
-#pragma unroll
-            for (int k = 0; k < (int)(16 / sizeof(T)); k++) tmp[k] = cvt<T>(v[i + k]);
-            *reinterpret_cast<uint4*>(dst + i * sizeof(T)) = *reinterpret_cast<const uint4*>(tmp);
+__device__ __forceinline__ uint32_t pack2(float a, float b);
+template <>
+__device__ __forceinline__ uint32_t pack2<__half>(float a, float b) {
+    const __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+template <>
+__device__ __forceinline__ uint32_t pack2<__nv_bfloat16>(float a, float b) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// store n (= 8, 4, 2 or 1) values of type T at dst with the widest aligned access
+template <typename T, int n>
+__device__ __forceinline__ void sts_n(uint8_t* dst, const float* v) {
+    if constexpr (sizeof(T) == 4) {
+        if constexpr (n == 8) {
+            reinterpret_cast<float4*>(dst)[0] = make_float4(v[0], v[1], v[2], v[3]);
+            reinterpret_cast<float4*>(dst)[1] = make_float4(v[4], v[5], v[6], v[7]);
+        } else if constexpr (n == 4) {
+            *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+        } else if constexpr (n == 2) {
+            *reinterpret_cast<float2*>(dst) = make_float2(v[0], v[1]);
+        } else {
+            *reinterpret_cast<float*>(dst) = v[0];
         }
     } else {
-        T* d = reinterpret_cast<T*>(dst);
-        for (int i = 0; i < n; i++) d[i] = cvt<T>(v[i]);
+        if constexpr (n == 8) {
+            *reinterpret_cast<uint4*>(dst) =
+                make_uint4(pack2<T>(v[0], v[1]), pack2<T>(v[2], v[3]), pack2<T>(v[4], v[5]), pack2<T>(v[6], v[7]));
+        } else if constexpr (n == 4) {
+            *reinterpret_cast<uint2*>(dst) = make_uint2(pack2<T>(v[0], v[1]), pack2<T>(v[2], v[3]));
+        } else if constexpr (n == 2) {
+            *reinterpret_cast<uint32_t*>(dst) = pack2<T>(v[0], v[1]);
+        } else {
+            *reinterpret_cast<T*>(dst) = cvt<T>(v[0]);
+        }
     }
 }
 
-// pools one 8x8 block (rows r, cols c) and stages all levels at column block cb (0/1 of the pass)
+// pools one 8x8 block and stages all levels at column block cb of the pass
 template <typename T>
 __device__ __forceinline__ void stage_block(uint8_t* st, int lane, int cb, const float (&blk)[8][8]) {
     using S = Stage<T>;
-    uint8_t* s0 = st;
-    uint8_t* s1 = s0 + 32 * S::r0;
-    uint8_t* s2 = s1 + 32 * S::r1;
-    uint8_t* s3 = s2 + 32 * S::r2;
+    uint8_t* s0 = st + lane * S::r0;
+    uint8_t* s1 = st + 32 * S::r0 + lane * S::r1;
+    uint8_t* s2 = st + 32 * (S::r0 + S::r1) + lane * S::r2;
+    uint8_t* s3 = st + 32 * (S::r0 + S::r1 + S::r2) + lane * S::r3;
 #pragma unroll
-    for (int r = 0; r < 8; r++) sts_vals<T>(s0 + lane * S::r0 + (r * kPassW + cb * 8) * S::sz, blk[r], 8);
+    for (int r = 0; r < 8; r++) sts_n<T, 8>(s0 + (r * S::PW + cb * 8) * S::sz, blk[r]);
     float l1[4][4];
 #pragma unroll
     for (int r = 0; r < 4; r++)
 #pragma unroll
         for (int c = 0; c < 4; c++)
-            l1[r][c] = 0.25f * (blk[2 * r][2 * c] + blk[2 * r][2 * c + 1] + blk[2 * r + 1][2 * c] + blk[2 * r + 1][2 * c + 1]);
+            l1[r][c] = 0.25f * ((blk[2 * r][2 * c] + blk[2 * r][2 * c + 1]) + (blk[2 * r + 1][2 * c] + blk[2 * r + 1][2 * c + 1]));
 #pragma unroll
-    for (int r = 0; r < 4; r++) sts_vals<T>(s1 + lane * S::r1 + (r * (kPassW / 2) + cb * 4) * S::sz, l1[r], 4);
+    for (int r = 0; r < 4; r++) sts_n<T, 4>(s1 + (r * (S::PW / 2) + cb * 4) * S::sz, l1[r]);
     float l2[2][2];
 #pragma unroll
     for (int r = 0; r < 2; r++)
 #pragma unroll
         for (int c = 0; c < 2; c++)
-            l2[r][c] = 0.25f * (l1[2 * r][2 * c] + l1[2 * r][2 * c + 1] + l1[2 * r + 1][2 * c] + l1[2 * r + 1][2 * c + 1]);
+            l2[r][c] = 0.25f * ((l1[2 * r][2 * c] + l1[2 * r][2 * c + 1]) + (l1[2 * r + 1][2 * c] + l1[2 * r + 1][2 * c + 1]));
 #pragma unroll
-    for (int r = 0; r < 2; r++) sts_vals<T>(s2 + lane * S::r2 + (r * (kPassW / 4) + cb * 2) * S::sz, l2[r], 2);
-    const float l3 = 0.25f * (l2[0][0] + l2[0][1] + l2[1][0] + l2[1][1]);
-    sts_vals<T>(s3 + lane * S::r3 + cb * S::sz, &l3, 1);
+    for (int r = 0; r < 2; r++) sts_n<T, 2>(s2 + (r * (S::PW / 4) + cb * 2) * S::sz, l2[r]);
+    const float l3 = 0.25f * ((l2[0][0] + l2[0][1]) + (l2[1][0] + l2[1][1]));
+    sts_n<T, 1>(s3 + cb * S::sz, &l3);
 }
 
-// copies a staged level of the warp's 32 rows to global: `nseg` segments of
-// `seg` bytes per row, `sstride` bytes apart in shared memory; segment j of
-// row i goes to gbase + (row0 + i) * grow_stride + j * gseg_stride
-template <typename T>
-__device__ __forceinline__ void flush_level(const uint8_t* st, int rstride, int nseg, int seg, int sstride, long row0,
-                                            int nrows, uint8_t* gbase, long grow_stride, long gseg_stride, int lane) {
-    if (seg >= 16) {
-        const int cps = seg / 16;  // 16-byte chunks per segment
-        const int total = 32 * nseg * cps;
-        for (int j = lane; j < total; j += 32) {
-            const int k = j % cps, sg = (j / cps) % nseg, i = j / (cps * nseg);
-            if (i >= nrows) continue;
-            const uint4 v = *reinterpret_cast<const uint4*>(st + i * rstride + sg * sstride + k * 16);
-            *reinterpret_cast<uint4*>(gbase + (row0 + i) * grow_stride + sg * gseg_stride + k * 16) = v;
-        }
-    } else {
-        const int total = 32 * nseg;
-        for (int j = lane; j < total; j += 32) {
-            const int sg = j % nseg, i = j / nseg;
-            if (i >= nrows) continue;
-            const uint8_t* src = st + i * rstride + sg * sstride;
-            uint8_t* dst = gbase + (row0 + i) * grow_stride + sg * gseg_stride;
-            if (seg == 8)
-                *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(src);
-            else if (seg == 4)
-                *reinterpret_cast<uint32_t*>(dst) = *reinterpret_cast<const uint32_t*>(src);
-            else
-                *reinterpret_cast<uint16_t*>(dst) = *reinterpret_cast<const uint16_t*>(src);
-        }
+// writes one staged level: per row NSEG segments of SEG bytes (SSTR apart in
+// shared memory), copied in CHUNK-byte pieces; lanes walk chunks of one row
+// segment consecutively
+template <int NSEG, int SEG, int SSTR, int CHUNK>
+__device__ __forceinline__ void flush_fixed(const uint8_t* st, int rstride, int nrows, uint8_t* gbase,
+                                            uint32_t grow_stride, uint32_t gseg_stride, int lane) {
+    constexpr int CPS = SEG / CHUNK;         // chunks per segment
+    constexpr int CPR = NSEG * CPS;          // chunks per row
+    constexpr int TOTAL = 32 * CPR;
+#pragma unroll 4
+    for (int j = lane; j < TOTAL; j += 32) {
+        const int i = j / CPR;               // compile-time power-of-two divisors
+        const int sg = (j / CPS) % NSEG;
+        const int k = j % CPS;
+        if (i >= nrows) continue;
+        const uint8_t* src = st + i * rstride + sg * SSTR + k * CHUNK;
+        uint8_t* dst = gbase + (size_t)i * grow_stride + (size_t)sg * gseg_stride + k * CHUNK;
+        if constexpr (CHUNK == 16)
+            *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(src);
+        else if constexpr (CHUNK == 8)
+            *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(src);
+        else if constexpr (CHUNK == 4)
+            *reinterpret_cast<uint32_t*>(dst) = *reinterpret_cast<const uint32_t*>(src);
+        else
+            *reinterpret_cast<uint16_t*>(dst) = *reinterpret_cast<const uint16_t*>(src);
     }
+}
+
+// flush a full pass (PW columns) or a half pass (8 columns, only when TW = 8 and PW = 16)
+template <typename T, int COLS>
+__device__ __forceinline__ void flush_pass(const uint8_t* st, int nrows, uint8_t* const* lvl, const uint32_t* rs,
+                                           const uint32_t* ss, int levels, int lane) {
+    using S = Stage<T>;
+    constexpr int sz = S::sz;
+    constexpr int s0 = COLS * sz, s1 = (COLS / 2) * sz, s2 = (COLS / 4) * sz, s3 = (COLS / 8) * sz;
+    flush_fixed<8, s0, S::PW * sz, (s0 >= 16 ? 16 : s0)>(st, S::r0, nrows, lvl[0], rs[0], ss[0], lane);
+    if (levels > 1)
+        flush_fixed<4, s1, (S::PW / 2) * sz, (s1 >= 16 ? 16 : s1)>(st + 32 * S::r0, S::r1, nrows, lvl[1], rs[1], ss[1],
+                                                                   lane);
+    if (levels > 2)
+        flush_fixed<2, s2, (S::PW / 4) * sz, (s2 >= 16 ? 16 : s2)>(st + 32 * (S::r0 + S::r1), S::r2, nrows, lvl[2],
+                                                                   rs[2], ss[2], lane);
+    if (levels > 3)
+        flush_fixed<1, s3, (S::PW / 8) * sz, (s3 >= 16 ? 16 : s3)>(st + 32 * (S::r0 + S::r1 + S::r2), S::r3, nrows,
+                                                                   lvl[3], rs[3], ss[3], lane);
 }
 
 // ---------------------------------------------------------------- main kernel
@@ -290,7 +334,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int N = p.N;
     auto sa = [&](int kc) { return sbase + (size_t)kc * kBM * 128; };
     auto sb = [&](int st, int kc) { return sbase + a_region(KC) + ((size_t)st * KC + kc) * b_box(N); };
-    const int NBS = (int)sizeof(TOut) == 4 ? 1 : 2;  // B stages (FP32 staging needs the room of one)
+    const int NBS = 1;  // one B stage: the MMA + load of tile t+1 hide under the epilogue of tile t
     const size_t stage_off = a_region(KC) + (size_t)NBS * KC * b_box(N);
 
     if (tid == 0) {
@@ -301,11 +345,11 @@ __global__ void __launch_bounds__(kThreads, 1)
             mbar_init(&barB_full[s], 1);
             mbar_init(&barB_empty[s], 1);
             mbar_init(&barAcc_full[s], 1);
-            mbar_init(&barAcc_empty[s], 4);  // one arrive per epilogue warp
+            mbar_init(&barAcc_empty[s], kEpiWarps);  // one arrive per epilogue warp
         }
         fence_barrier_init();
     }
-    if (warp == 1) {
+    if (warp == kMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tmem_base)));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
@@ -317,7 +361,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t a_bytes = (uint32_t)kBM * 128u * KC;
     const uint32_t b_bytes = (uint32_t)N * 128u * KC;
 
-    if (warp == 0 && lane == 0) {
+    if (warp == kTmaWarp && lane == 0) {
         // ------------------------------------------------ TMA producer
         uint32_t t = 0, it = 0;
         for (long item = blockIdx.x; item < p.items && !fail; item += gridDim.x, it++) {
@@ -343,7 +387,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             while (!mbar_try_wait(&barB_full[last % NBS], (last / NBS) & 1) && gtimer() - t0 < kWaitNs) {
             }
         }
-    } else if (warp == 1 && lane == 0) {
+    } else if (warp == kMmaWarp && lane == 0) {
         // ------------------------------------------------ MMA issuer
         const uint32_t idesc = instr_desc(ab_format, kBM, N);
         uint32_t t = 0, it = 0;
@@ -370,14 +414,23 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             mma_commit(&barA_empty);
         }
-    } else if (warp >= 4) {
+    } else if (warp < kEpiWarps) {
         // ------------------------------------------------ epilogue
-        const int q = warp - 4;                 // TMEM lane quarter
+        using St = Stage<TOut>;
+        constexpr int PW = St::PW;
+        const int q = warp & 3, half = warp >> 2;   // TMEM lane quarter, column half
         const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
         const int TW = p.TW, blocks_w = p.W / TW;
-        using St = Stage<TOut>;
-        uint8_t* st = sbase + stage_off + (size_t)q * St::per_warp;
-        const int sz = (int)sizeof(TOut);
+        const int col_lo = TW >= 16 ? half * (TW / 2) : 0;
+        const int col_hi = TW >= 16 ? col_lo + TW / 2 : (half == 0 ? TW : 0);
+        uint8_t* st = sbase + stage_off + (size_t)warp * St::per_warp;
+        constexpr int sz = (int)sizeof(TOut);
+        const int H = p.H, W = p.W;
+        uint32_t rs[4], ss[4];
+        for (int l = 0; l < 4; l++) {
+            rs[l] = (uint32_t)((H >> l) * (W >> l) * sz);  // one source row of level l
+            ss[l] = (uint32_t)((W >> l) * sz);             // one target row of level l
+        }
         uint32_t t = 0;
         for (long item = blockIdx.x; item < p.items && !fail; item += gridDim.x) {
             const int e = (int)(item / p.mtiles), mt = (int)(item % p.mtiles);
@@ -389,47 +442,40 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (!mbar_wait(&barAcc_full[acc], (t >> 1) & 1, &fail)) break;
                 tc_fence_after();
                 const int hb = nt / blocks_w, wb = nt % blocks_w;
-                const int passes = (TW + kPassW - 1) / kPassW;
-                for (int ps = 0; ps < passes; ps++) {
-                    const int pw = min(kPassW, TW - ps * kPassW);  // 16 or 8 columns in this pass
+                if (col_lo >= col_hi) {
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&barAcc_empty[acc]);
+                    continue;
+                }
+                for (int c = col_lo; c < col_hi; c += PW) {
+                    const int pw = min(PW, col_hi - c);  // PW, or 8 when TW = 8
                     for (int cb = 0; cb < pw / 8; cb++) {
                         float blk[8][8];
-                        const int c0 = ps * kPassW + cb * 8;
 #pragma unroll
                         for (int r = 0; r < 8; r++)
-                            tmem_ld8(tmem + lane_addr + (uint32_t)(acc * 256 + r * TW + c0), blk[r]);
+                            tmem_ld8(tmem + lane_addr + (uint32_t)(acc * 256 + r * TW + c + cb * 8), blk[r]);
                         tmem_wait_ld();
                         stage_block<TOut>(st, lane, cb, blk);
                     }
-                    if (ps == passes - 1) {
-                        // all of this accumulator is in registers / staging: release TMEM early
+                    if (c + PW >= col_hi) {
+                        // the whole accumulator slice of this warp is read: release TMEM
                         tc_fence_before();
                         __syncwarp();
                         if (lane == 0) mbar_arrive(&barAcc_empty[acc]);
                     }
                     __syncwarp();
-                    const int h0 = hb * kTH, w0 = wb * TW + ps * kPassW;
-                    uint8_t* s0 = st;
-                    uint8_t* s1 = s0 + 32 * St::r0;
-                    uint8_t* s2 = s1 + 32 * St::r1;
-                    uint8_t* s3 = s2 + 32 * St::r2;
-                    // level l row of the output volume: (row, H_l, W_l)
-                    const int H = p.H, W = p.W;
-                    flush_level<TOut>(s0, St::r0, 8, pw * sz, kPassW * sz, row0, nrows,
-                                      static_cast<uint8_t*>(p.out[0]) + ((long)h0 * W + w0) * sz, (long)H * W * sz,
-                                      (long)W * sz, lane);
-                    if (p.levels > 1)
-                        flush_level<TOut>(s1, St::r1, 4, (pw / 2) * sz, (kPassW / 2) * sz, row0, nrows,
-                                          static_cast<uint8_t*>(p.out[1]) + ((long)(h0 >> 1) * (W >> 1) + (w0 >> 1)) * sz,
-                                          (long)(H >> 1) * (W >> 1) * sz, (long)(W >> 1) * sz, lane);
-                    if (p.levels > 2)
-                        flush_level<TOut>(s2, St::r2, 2, (pw / 4) * sz, (kPassW / 4) * sz, row0, nrows,
-                                          static_cast<uint8_t*>(p.out[2]) + ((long)(h0 >> 2) * (W >> 2) + (w0 >> 2)) * sz,
-                                          (long)(H >> 2) * (W >> 2) * sz, (long)(W >> 2) * sz, lane);
-                    if (p.levels > 3)
-                        flush_level<TOut>(s3, St::r3, 1, (pw / 8) * sz, (kPassW / 8) * sz, row0, nrows,
-                                          static_cast<uint8_t*>(p.out[3]) + ((long)(h0 >> 3) * (W >> 3) + (w0 >> 3)) * sz,
-                                          (long)(H >> 3) * (W >> 3) * sz, (long)(W >> 3) * sz, lane);
+                    const int h0 = hb * kTH, w0 = wb * TW + c;
+                    uint8_t* lvl[4];
+                    for (int l = 0; l < 4; l++)
+                        lvl[l] = l < p.levels
+                                     ? static_cast<uint8_t*>(p.out[l]) + (size_t)row0 * rs[l] +
+                                           ((size_t)(h0 >> l) * (W >> l) + (w0 >> l)) * sz
+                                     : nullptr;
+                    if (pw == PW)
+                        flush_pass<TOut, PW>(st, nrows, lvl, rs, ss, p.levels, lane);
+                    else
+                        flush_pass<TOut, 8>(st, nrows, lvl, rs, ss, p.levels, lane);
                     __syncwarp();
                 }
             }
@@ -437,7 +483,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     __syncthreads();
     if (fail && tid == 0) atomicExch(p.err, 1);
-    if (warp == 1) {
+    if (warp == kMmaWarp) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
     }
@@ -519,8 +565,7 @@ int pick_tw(int W) {
 
 template <typename T>
 size_t smem_bytes(int KC, int N) {
-    const int nbs = sizeof(T) == 4 ? 1 : 2;
-    return a_region(KC) + (size_t)nbs * KC * b_box(N) + 4 * (size_t)Stage<T>::per_warp + 1024;
+    return a_region(KC) + (size_t)KC * b_box(N) + kEpiWarps * (size_t)Stage<T>::per_warp + 1024;
 }
 
 bool g_attr_set[64] = {false};
