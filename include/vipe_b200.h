@@ -108,6 +108,34 @@ int vipe_slam_ba(float* poses_io, float* disps_io, float* intrinsics_io, const f
                  int motion_only, float alpha, float* depth_active_scratch, float* dx_out, float* dz_out,
                  void* workspace, size_t workspace_bytes, int32_t* dev_status, void* stream);
 
+/* Bundle adjustment for callers that cannot allocate device memory.  No
+ * counterpart in the reference (its ba_cuda_impl allocates through ATen).
+ * Hosts that forbid allocation after start-up, or bindings (cgo, JNI, plain C)
+ * whose runtime has no CUDA allocator, cannot provide the workspace that
+ * vipe_slam_ba_extended takes.  This entry point runs the same solve, with the
+ * same arguments minus workspace/workspace_bytes, on a scratch array compiled
+ * into the library: VIPE_BA_NOALLOC_SCRATCH_BYTES (16 MiB) of device memory on
+ * every GPU that loads the library, held until the process exits.  It calls no
+ * cudaMalloc/cudaFree.
+ *   - Graphs whose vipe_slam_ba_workspace_size() exceeds the scratch are
+ *     rejected with VIPE_ERR_CAPACITY before any launch (vipe_last_error()
+ *     names both sizes).  A 64-keyframe 48x64 graph with 628 edges needs
+ *     about 12 MiB.
+ *   - The first call on a device looks up the scratch's device address there
+ *     (cudaGetSymbolAddress, which loads the library's module on that device);
+ *     make that first call before any stream capture.
+ *   - Every call on a device shares the one array and the next call overwrites
+ *     it: calls whose work overlaps on the GPU (different streams, or
+ *     concurrent host threads) race and must be serialised by the caller. */
+#define VIPE_BA_NOALLOC_SCRATCH_BYTES (16u << 20)
+int vipe_slam_ba_extended_noalloc(float* poses_io, float* disps_io, float* intrinsics_io, const float* disps_sens,
+                                  const float* targets, const float* weights, const float* eta, const int64_t* ii,
+                                  const int64_t* jj, const float* depth_active, int num_frames, int ht, int wd,
+                                  int num_edges, int num_kx, int t0, int t1, int iterations, float lm, float ep,
+                                  int motion_only, float alpha, int optimize_intrinsics, float intrinsics_lm,
+                                  float intrinsics_ep, float intrinsics_scale, int compute_energy, float* dx_out,
+                                  float* dz_out, float* energy_out, int32_t* dev_status, void* stream);
+
 /* Debug view of the device-built graph index (bit-exact tests).  Runs only the
  * index construction of vipe_slam_ba_extended into `workspace` and copies:
  *   kx_out (num_kx) int64 — sorted unique depth frames

@@ -29,12 +29,18 @@ SZ = ctypes.c_size_t
 _SIGS: dict[str, tuple] = {
     "vipe_status_string": (ctypes.c_char_p, [I]),
     "vipe_last_error": (ctypes.c_char_p, []),
+    "vipe_profile_enable": (None, [I]),
+    "vipe_profile_collect": (I, [ctypes.c_char_p, I, P, P, I]),
     "vipe_slam_ba_workspace_size": (SZ, [I, I, I, I, I, I, I]),
     "vipe_slam_ba_extended": (
         I,
         [P, P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, F, I, F, I, F, F, F, I, P, P, P, P, SZ, P, P],
     ),
     "vipe_slam_ba": (I, [P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, F, I, F, P, P, P, P, SZ, P, P]),
+    "vipe_slam_ba_extended_noalloc": (
+        I,
+        [P, P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, F, I, F, I, F, F, F, I, P, P, P, P, P],
+    ),
     "vipe_slam_ba_index_debug": (I, [P, P, I, I, I, I, I, P, P, P, I, P, P, SZ, P]),
     "vipe_slam_frame_distance": (I, [P, P, P, P, P, P, P, P, I, I, I, I, I, I, F, P, P]),
     "vipe_slam_projmap": (I, [P, P, P, P, P, I, I, I, I, P, P, P]),
