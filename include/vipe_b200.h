@@ -136,6 +136,42 @@ int vipe_slam_ba_extended_noalloc(float* poses_io, float* disps_io, float* intri
                                   float intrinsics_ep, float intrinsics_scale, int compute_energy, float* dx_out,
                                   float* dz_out, float* energy_out, int32_t* dev_status, void* stream);
 
+/* Batched bundle adjustment: many clips' graphs solved together, each phase of
+ * the LM step one launch over all graphs.  No counterpart in the reference,
+ * whose ba_cuda_impl (csrc/slam_ext/geom_kernels.cu:1626-1824) solves one graph
+ * per call; per graph the arithmetic is that of vipe_slam_ba_extended.
+ *
+ * Layout: graph g has num_frames[g] frames, num_edges[g] edges, num_kx[g]
+ * depth rows and window [t0[g], t1[g]); every tensor of the single-graph call
+ * is concatenated over the graphs along its leading axis, in graph order:
+ *   poses (sum frames, 7), disps / disps_sens (sum frames, ht, wd),
+ *   depth_active (sum frames), targets / weights (sum edges, 2, ht, wd),
+ *   ii / jj (sum edges) int64 holding frame indices LOCAL to their graph,
+ *   eta (sum kx, ht, wd), intrinsics (num_graphs, 4),
+ *   dx_out (sum (t1-t0), 6), dz_out (sum kx, ht*wd),
+ *   energy_out (num_graphs, iterations), dev_status (num_graphs) int32.
+ * The plan is host-side; bind uploads its graph table into a device workspace
+ * of vipe_slam_ba_batch_workspace_size() bytes (synchronises `stream`).
+ * vipe_slam_ba_batch_solve then only enqueues kernels (no allocation, copy or
+ * synchronisation), so it may be captured into a CUDA graph.
+ * edge_chunks / frame_chunks: pixel chunks per edge / per depth frame for the
+ * linearisation kernels (0 = chosen from the batch size). */
+typedef struct vipe_ba_batch_plan vipe_ba_batch_plan;
+int vipe_slam_ba_batch_plan_create(int num_graphs, const int* num_frames, const int* num_edges, const int* num_kx,
+                                   const int* t0, const int* t1, int ht, int wd, int edge_chunks, int frame_chunks,
+                                   vipe_ba_batch_plan** plan_out);
+size_t vipe_slam_ba_batch_workspace_size(const vipe_ba_batch_plan* plan);
+/* totals_out[4] = {sum frames, sum edges, sum kx, sum (t1-t0)} */
+int vipe_slam_ba_batch_totals(const vipe_ba_batch_plan* plan, int64_t* totals_out);
+int vipe_slam_ba_batch_bind(vipe_ba_batch_plan* plan, void* workspace, size_t workspace_bytes, void* stream);
+int vipe_slam_ba_batch_solve(const vipe_ba_batch_plan* plan, float* poses_io, float* disps_io, float* intrinsics_io,
+                             const float* disps_sens, const float* targets, const float* weights, const float* eta,
+                             const int64_t* ii, const int64_t* jj, const float* depth_active, int iterations,
+                             float lm, float ep, int motion_only, float alpha, int optimize_intrinsics,
+                             float intrinsics_lm, float intrinsics_ep, float intrinsics_scale, int compute_energy,
+                             float* dx_out, float* dz_out, float* energy_out, int32_t* dev_status, void* stream);
+void vipe_slam_ba_batch_plan_destroy(vipe_ba_batch_plan* plan);
+
 /* Debug view of the device-built graph index (bit-exact tests).  Runs only the
  * index construction of vipe_slam_ba_extended into `workspace` and copies:
  *   kx_out (num_kx) int64 — sorted unique depth frames

@@ -105,17 +105,19 @@ __host__ __device__ inline int npt_of(int m) {
     return nt * (nt + 1) / 2;
 }
 
-Dims make_dims(int N, int H, int W, int E, int K, int t0, int t1) {
+// che / cf: pixel-chunk counts of the per-edge and per-frame kernels; 0 picks
+// them so that one graph alone launches about two CTAs per SM.
+Dims make_dims(int N, int H, int W, int E, int K, int t0, int t1, int che = 0, int cf = 0) {
     Dims d;
     d.N = N; d.H = H; d.W = W; d.HW = H * W; d.E = E; d.K = K; d.t0 = t0; d.t1 = t1;
     d.P = t1 - t0;
     d.dim = 6 * d.P + 1;
     const int target = 2 * 148;
-    int che = E > 0 ? (target + E - 1) / E : 1;
+    if (che <= 0) che = E > 0 ? (target + E - 1) / E : 1;
     che = std::max(1, std::min(che, std::max(1, d.HW / 1024)));
     d.chunk_e = (d.HW + che - 1) / che;
     d.CHe = (d.HW + d.chunk_e - 1) / d.chunk_e;
-    int cf = K > 0 ? (target + K - 1) / K : 1;
+    if (cf <= 0) cf = K > 0 ? (target + K - 1) / K : 1;
     cf = std::max(1, std::min(cf, 8));
     int chunk = (d.HW + cf - 1) / cf;
     chunk = ((chunk + 255) / 256) * 256;
@@ -175,6 +177,102 @@ void carve(C& c, const Dims& d, Work* w) {
         w->linv = (double*)pli;
     }
 }
+
+// ---------------------------------------------------------------- graph table
+//
+// Every kernel runs over a table of graphs.  A single solve is a table of one;
+// a batch places many clips' graphs side by side: inputs are concatenated
+// along their leading axis (frames, edges, depth rows, window poses) and each
+// graph's descriptor holds its sizes, its carve of the workspace and its
+// offsets into the concatenated tensors.  Edge indices stay local to their
+// graph.  A launch over the batch is one flat grid: per kernel, boff[g] is the
+// first block of graph g (boff[G] = total), found by binary search.
+
+struct BAPtrs {
+    float* poses;              // (frames, 7)
+    float* disps;              // (frames, H, W)
+    float* intr;               // (graphs, 4)
+    const float* disps_sens;   // (frames, H, W)
+    const float* targets;      // (edges, 2, H, W)
+    const float* weights;      // (edges, 2, H, W)
+    const float* eta;          // (depth rows, H, W)
+    const int64_t* ii;         // (edges,) local frame index
+    const int64_t* jj;
+    const float* depth_active; // (frames,)
+    float* dx;                 // (window poses, 6)
+    float* dz;                 // (depth rows, H*W)
+    float* energy;             // (graphs, energy_stride)
+    int32_t* status;           // device status word(s): graph g uses status[g * status_stride]
+    int energy_stride;
+    int status_stride;
+};
+
+struct GraphDesc {
+    Dims d;
+    Work w;
+    long frame_off, edge_off, kx_off, pose_off;
+    int g;
+};
+
+struct Batch {
+    const GraphDesc* gds;  // device table
+    const int* boff;       // per-kernel block offsets, or nullptr (see locate)
+    int G;
+};
+
+// Graph of this block.  With boff: flat grid over all graphs.  Without: a
+// single graph (G == 1, local = blockIdx.x) or one block per graph (g = blockIdx.x).
+__device__ __forceinline__ int locate(const Batch& B, int& local) {
+    if (B.boff == nullptr) {
+        if (B.G == 1) {
+            local = blockIdx.x;
+            return 0;
+        }
+        local = 0;
+        return blockIdx.x;
+    }
+    const int x = blockIdx.x;
+    int lo = 0, hi = B.G;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(B.boff + mid) <= x) lo = mid; else hi = mid;
+    }
+    local = x - __ldg(B.boff + lo);
+    return lo;
+}
+
+__device__ __forceinline__ BAPtrs rebase(const BAPtrs& b, const GraphDesc& g) {
+    const long HW = g.d.HW;
+    BAPtrs p;
+    p.poses = b.poses + g.frame_off * 7;
+    p.disps = b.disps + g.frame_off * HW;
+    p.intr = b.intr + (long)g.g * 4;
+    p.disps_sens = b.disps_sens + g.frame_off * HW;
+    p.targets = b.targets ? b.targets + g.edge_off * 2 * HW : nullptr;
+    p.weights = b.weights ? b.weights + g.edge_off * 2 * HW : nullptr;
+    p.eta = b.eta + g.kx_off * HW;
+    p.ii = b.ii ? b.ii + g.edge_off : nullptr;
+    p.jj = b.jj ? b.jj + g.edge_off : nullptr;
+    p.depth_active = b.depth_active + g.frame_off;
+    p.dx = b.dx + g.pose_off * 6;
+    p.dz = b.dz ? b.dz + g.kx_off * HW : nullptr;
+    p.energy = b.energy ? b.energy + (long)g.g * b.energy_stride : nullptr;
+    p.status = b.status ? b.status + (long)g.g * b.status_stride : nullptr;
+    p.energy_stride = b.energy_stride;
+    p.status_stride = b.status_stride;
+    return p;
+}
+
+// binds d, w, P (rebased pointers) and local_ (block index within the graph)
+#define BA_BIND(B, base)                                \
+    int local_;                                         \
+    const int g_ = locate(B, local_);                   \
+    const GraphDesc* __restrict__ gd_ = (B).gds + g_;   \
+    const Dims d = gd_->d;                              \
+    const Work w = gd_->w;                              \
+    const BAPtrs io = rebase(base, *gd_);                \
+    (void)io;                                           \
+    (void)d;
 
 // ---------------------------------------------------------------- index build
 
@@ -264,11 +362,22 @@ __device__ __forceinline__ int bit_rank(unsigned word, int q) {
     return base + __popc(wv & ((1u << (q & 31)) - 1u));
 }
 
+// use_init: single-graph call; `init` is the graph's descriptor, which thread 0
+// also stores at B.gds[0] for the kernels that follow.
 __global__ void __launch_bounds__(kIndexThreads)
-    ba_index_kernel(const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, Dims d, Work w) {
+    ba_index_kernel(BAPtrs base, Batch B, GraphDesc init, int use_init) {
     __shared__ int sh_warp[32];
     __shared__ unsigned sh_bm[32][32];
     __shared__ int sh_flag;
+    int local_;
+    const int g_ = use_init ? 0 : locate(B, local_);
+    const GraphDesc gd = use_init ? init : B.gds[g_];
+    if (use_init && threadIdx.x == 0) *const_cast<GraphDesc*>(B.gds) = init;
+    const Dims d = gd.d;
+    const Work w = gd.w;
+    const BAPtrs io = rebase(base, gd);
+    const int64_t* __restrict__ ii = io.ii;
+    const int64_t* __restrict__ jj = io.jj;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int N = d.N, E = d.E, t0 = d.t0, t1 = d.t1, P = d.P;
 
@@ -482,10 +591,12 @@ constexpr int kNE = 36;
 __host__ __device__ inline int tri6(int r, int c) { return r >= c ? r * (r + 1) / 2 + c : c * (c + 1) / 2 + r; }
 
 template <bool kIntr>
-__global__ void __launch_bounds__(kEdgeThreads) ba_edge_kernel(EdgeArgs A, Dims d, Work w) {
+__global__ void __launch_bounds__(kEdgeThreads) ba_edge_kernel(BAPtrs base, Batch B, float iscale) {
+    BA_BIND(B, base);
     if (w.status[0]) return;
+    const EdgeArgs A{io.poses, io.disps, io.intr, io.targets, io.weights, io.ii, io.jj, iscale};
     __shared__ float red[kEdgeThreads / 32][kNE];
-    const int e = blockIdx.x, c = blockIdx.y;
+    const int e = local_ % d.E, c = local_ / d.E;
     const int a = (int)A.ii[e], b = (int)A.jj[e];
     const bool stereo = a == b;
     float tij[3], qij[4];
@@ -564,11 +675,13 @@ __global__ void __launch_bounds__(kEdgeThreads) ba_edge_kernel(EdgeArgs A, Dims 
 }
 
 // Chunk partials -> FP64 per-edge terms in the 12x12 layout (kNT values).
-__global__ void ba_edge_reduce(EdgeArgs A, Dims d, Work w) {
+__global__ void ba_edge_reduce(BAPtrs base, Batch B) {
+    BA_BIND(B, base);
     if (w.status[0]) return;
+    const EdgeArgs A{io.poses, io.disps, io.intr, io.targets, io.weights, io.ii, io.jj, 1.f};
     __shared__ double t[kNE];
     __shared__ double M[6][6];
-    const int e = blockIdx.x, tid = threadIdx.x;
+    const int e = local_, tid = threadIdx.x;
     for (int n = tid; n < kNE; n += blockDim.x) {
         double sv = 0.0;
         for (int c = 0; c < d.CHe; c++) sv += (double)w.epart[((size_t)e * d.CHe + c) * kNE + n];
@@ -651,12 +764,15 @@ __device__ __forceinline__ void decode_tile(int tau, int nt, int& ti, int& tj) {
 }
 
 template <bool kIntr>
-__global__ void __launch_bounds__(kFrameThreads) ba_frame_kernel(FrameArgs A, Dims d, Work w) {
+__global__ void __launch_bounds__(kFrameThreads) ba_frame_kernel(BAPtrs base, Batch B, float alpha, float iscale) {
+    BA_BIND(B, base);
     if (w.status[0]) return;
+    const FrameArgs A{io.poses, io.disps, io.disps_sens, io.intr, io.targets, io.weights, io.eta, io.depth_active, io.jj,
+                      alpha, iscale};
     extern __shared__ float4 stage4[];
     float* stage = reinterpret_cast<float*>(stage4);
     __shared__ float red[kFrameThreads / 32];
-    const int s = blockIdx.x, c = blockIdx.y, tid = threadIdx.x;
+    const int s = local_ % d.K, c = local_ / d.K, tid = threadIdx.x;
     const int HW = d.HW, W = d.W;
     const int k = w.kx[s];
     const float act = A.depth_active[k];
@@ -823,11 +939,13 @@ __device__ __forceinline__ int find_slot(const Work& w, int s, int a) {
 }
 
 // one warp per pose pair (a <= b): H[6a.., 6b..] and its mirror
-__global__ void ba_assemble_blocks(const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, Dims d, Work w,
-                                   int with_frames) {
+__global__ void ba_assemble_blocks(BAPtrs base, Batch B, int with_frames) {
+    BA_BIND(B, base);
     if (w.status[0]) return;
+    const int64_t* __restrict__ ii = io.ii;
+    const int64_t* __restrict__ jj = io.jj;
     const int lane = threadIdx.x & 31;
-    const long pair = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const long pair = (long)local_ * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int P = d.P;
     if (pair >= (long)P * (P + 1) / 2) return;
     // decode pair -> (a, b), a <= b, row-major upper triangle
@@ -884,10 +1002,11 @@ __global__ void ba_assemble_blocks(const int64_t* __restrict__ ii, const int64_t
 }
 
 // one warp per pose: rhs rows and the focal column; block P (last) does the corner
-__global__ void ba_assemble_rhs(Dims d, Work w, int with_frames, int with_intr) {
+__global__ void ba_assemble_rhs(BAPtrs base, Batch B, int with_frames, int with_intr) {
+    BA_BIND(B, base);
     if (w.status[0]) return;
     const int lane = threadIdx.x & 31;
-    const int a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int a = local_ * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int P = d.P, dim = d.dim;
     if (a < P) {
         // lanes 0..5: rhs entries; lanes 8..13: focal column entries
@@ -974,9 +1093,10 @@ __host__ __device__ inline int chol_ldr(int dim) {
 }
 
 __global__ void __launch_bounds__(kCholThreads, 1)
-    ba_cholesky_kernel(Dims d, Work w, float lm, float ep, float ilm, float iep, int with_intr, float* dx_out,
-                       int32_t* warn) {
+    ba_cholesky_kernel(BAPtrs base, Batch B, float lm, float ep, float ilm, float iep, int with_intr) {
+    BA_BIND(B, base);
     if (w.status[0]) return;
+    float* dx_out = io.dx;
     extern __shared__ double pT[];  // kNB columns x LDR rows (transposed panel)
     __shared__ double Li[kNB][kNB + 1];  // inverse of the diagonal block, Li[row][col]
     __shared__ double ysh[kNB];
@@ -1190,17 +1310,22 @@ __global__ void __launch_bounds__(kCholThreads, 1)
     for (int i = tid; i < np; i += kCholThreads) dx_out[i] = fail ? 0.f : (float)x[i];
     if (tid == 0) {
         w.df[0] = (fail || !with_intr) ? 0.0 : x[np];
-        if (fail && warn) atomicOr(warn, VIPE_WARN_SOLVER);
+        if (fail && io.status) atomicOr(io.status, VIPE_WARN_SOLVER);
     }
 }
 
 // ---------------------------------------------------------------- back substitution
 
 template <bool kIntr>
-__global__ void __launch_bounds__(256) ba_backsub_kernel(FrameArgs A, Dims d, Work w, const float* __restrict__ dx,
-                                                          float* disps_io, float* dz_out) {
+__global__ void __launch_bounds__(256) ba_backsub_kernel(BAPtrs base, Batch B) {
+    BA_BIND(B, base);
     if (w.status[0]) return;
-    const int s = blockIdx.x, c = blockIdx.y;
+    const FrameArgs A{io.poses, io.disps, io.disps_sens, io.intr, io.targets, io.weights, io.eta, io.depth_active, io.jj,
+                      0.f, 1.f};
+    const float* __restrict__ dx = io.dx;
+    float* disps_io = io.disps;
+    float* dz_out = io.dz;
+    const int s = local_ % d.K, c = local_ / d.K;
     const int HW = d.HW, W = d.W, P = d.P;
     const int k = w.kx[s];
     const float act = A.depth_active[k];
@@ -1252,10 +1377,13 @@ __global__ void __launch_bounds__(256) ba_backsub_kernel(FrameArgs A, Dims d, Wo
     }
 }
 
-__global__ void ba_retract_kernel(Dims d, Work w, const float* __restrict__ dx, float* poses_io, float* intr_io,
-                                  int with_intr, float iscale) {
+__global__ void ba_retract_kernel(BAPtrs base, Batch B, int with_intr, float iscale) {
+    BA_BIND(B, base);
     if (w.status[0]) return;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const float* __restrict__ dx = io.dx;
+    float* poses_io = io.poses;
+    float* intr_io = io.intr;
+    const int t = local_ * blockDim.x + threadIdx.x;
     if (t < d.P) {
         float xi[6], T[7];
         for (int n = 0; n < 6; n++) xi[n] = dx[6 * t + n];
@@ -1264,15 +1392,17 @@ __global__ void ba_retract_kernel(Dims d, Work w, const float* __restrict__ dx, 
         retract_pose(xi, T);
         for (int n = 0; n < 7; n++) pz[n] = T[n];
     }
-    if (with_intr && blockIdx.x == 0 && threadIdx.x == 0) {
+    if (with_intr && local_ == 0 && threadIdx.x == 0) {
         const float dfs = (float)(w.df[0] * (double)iscale);
         intr_io[0] += dfs;
         intr_io[1] += dfs;
     }
 }
 
-__global__ void ba_energy_kernel(Dims d, Work w, int with_frames, float* energy_out, int itr) {
+__global__ void ba_energy_kernel(BAPtrs base, Batch B, int with_frames, int itr) {
+    BA_BIND(B, base);
     if (w.status[0]) return;
+    float* energy_out = io.energy;
     __shared__ double red[32];
     double s = 0.0;
     for (int e = threadIdx.x; e < d.E; e += blockDim.x) s += w.eterm[(size_t)e * kNT + kTEN];
@@ -1288,8 +1418,9 @@ __global__ void ba_energy_kernel(Dims d, Work w, int with_frames, float* energy_
     }
 }
 
-__global__ void ba_status_kernel(Work w, int32_t* dev_status) {
-    if (w.status[0]) atomicOr(dev_status, w.status[0]);
+__global__ void ba_status_kernel(BAPtrs base, Batch B) {
+    BA_BIND(B, base);
+    if (w.status[0]) atomicOr(io.status, w.status[0]);
 }
 
 __global__ void fill_ones(float* p, int n) {
@@ -1307,13 +1438,153 @@ int check_dims(int num_frames, int ht, int wd, int num_edges, int num_kx, int t0
 
 bool g_smem_set[64] = {false};
 
-int launch_index(const int64_t* ii, const int64_t* jj, const Dims& d, const Work& w, cudaStream_t st) {
+int ensure_attributes() {
+    int dev = 0;
+    VIPE_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 64 && !g_smem_set[dev]) {
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kStageFloats * 4));
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kStageFloats * 4));
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_cholesky_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           chol_ldr(kPanelRows) * kNB * (int)sizeof(double)));
+        g_smem_set[dev] = true;
+    }
+    return VIPE_OK;
+}
+
+// Launch geometry of a table of graphs: per kernel, the flat block count of
+// each graph and their running offsets (uploaded as Batch::boff for batches).
+enum { kOffEdge = 0, kOffEdgeRed, kOffFrame, kOffPairs, kOffRhs, kOffRetr, kNumOff };
+
+struct Geometry {
+    int G = 0;
+    std::vector<int> off[kNumOff];  // G + 1 entries each
+    size_t chol_smem = 0;
+    bool any_edges = false;
+};
+
+void fill_geometry(const std::vector<Dims>& dims, Geometry& geo) {
+    geo.G = (int)dims.size();
+    for (int k = 0; k < kNumOff; k++) geo.off[k].assign(geo.G + 1, 0);
+    for (int g = 0; g < geo.G; g++) {
+        const Dims& d = dims[g];
+        const long npairs = (long)d.P * (d.P + 1) / 2;
+        const int cnt[kNumOff] = {d.E * d.CHe, d.E, d.K * d.CF, (int)ceil_div(npairs, 8), (int)ceil_div(d.P + 1, 8),
+                                  (int)ceil_div(d.P, 128)};
+        for (int k = 0; k < kNumOff; k++) geo.off[k][g + 1] = geo.off[k][g] + cnt[k];
+        geo.chol_smem = std::max(geo.chol_smem, (size_t)chol_ldr(d.dim) * kNB * sizeof(double));
+        geo.any_edges |= d.E > 0;
+    }
+}
+
+struct SolveArgs {
+    int iterations;
+    float lm, ep, alpha;
+    int motion_only, intr;
+    float ilm, iep, iscale;
+    int compute_energy;
+};
+
+// Enqueues the index build and `iterations` LM steps for every graph of the
+// table.  single: one graph whose descriptor `init` the index kernel stores;
+// otherwise the table and the offsets are already on the device.  Launches
+// only: no allocation, copy or synchronisation, so the sequence can be
+// captured into a CUDA graph.
+int run_solve(const Geometry& geo, const GraphDesc* d_table, const int* d_off, const BAPtrs& base,
+              const GraphDesc* init, const SolveArgs& a, cudaStream_t st) {
+    const bool single = init != nullptr;
+    const int G = geo.G;
+    auto batch = [&](int k) { return Batch{d_table, single ? nullptr : d_off + (size_t)k * (G + 1), G}; };
+    const Batch per_graph{d_table, nullptr, G};
+    auto grid = [&](int k) { return (unsigned)geo.off[k][G]; };
     {
         VIPE_PROF("ba_index", st);
-        ba_index_kernel<<<1, kIndexThreads, 0, st>>>(ii, jj, d, w);
+        ba_index_kernel<<<G, kIndexThreads, 0, st>>>(base, per_graph, single ? *init : GraphDesc{}, single ? 1 : 0);
     }
     VIPE_LAUNCH_CHECK();
+    const bool intr = a.intr != 0;
+    const int with_frames = a.motion_only ? 0 : 1;
+    for (int itr = 0; itr < a.iterations; itr++) {
+        if (geo.any_edges) {
+            {
+                VIPE_PROF("ba_edge", st);
+                if (intr)
+                    ba_edge_kernel<true><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(base, batch(kOffEdge), a.iscale);
+                else
+                    ba_edge_kernel<false><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(base, batch(kOffEdge), a.iscale);
+            }
+            VIPE_LAUNCH_CHECK();
+            {
+                VIPE_PROF("ba_edge_reduce", st);
+                ba_edge_reduce<<<grid(kOffEdgeRed), 128, 0, st>>>(base, batch(kOffEdgeRed));
+            }
+            VIPE_LAUNCH_CHECK();
+        }
+        if (with_frames && grid(kOffFrame) > 0) {
+            VIPE_PROF("ba_frame", st);
+            if (intr)
+                ba_frame_kernel<true><<<grid(kOffFrame), kFrameThreads, kStageFloats * 4, st>>>(
+                    base, batch(kOffFrame), a.alpha, a.iscale);
+            else
+                ba_frame_kernel<false><<<grid(kOffFrame), kFrameThreads, kStageFloats * 4, st>>>(
+                    base, batch(kOffFrame), a.alpha, a.iscale);
+            VIPE_LAUNCH_CHECK();
+        }
+        {
+            VIPE_PROF("ba_assemble", st);
+            ba_assemble_blocks<<<grid(kOffPairs), 256, 0, st>>>(base, batch(kOffPairs), with_frames);
+            VIPE_LAUNCH_CHECK();
+            ba_assemble_rhs<<<grid(kOffRhs), 256, 0, st>>>(base, batch(kOffRhs), with_frames, intr ? 1 : 0);
+        }
+        VIPE_LAUNCH_CHECK();
+        if (a.compute_energy) {
+            VIPE_PROF("ba_energy", st);
+            ba_energy_kernel<<<G, 256, 0, st>>>(base, per_graph, with_frames, itr);
+            VIPE_LAUNCH_CHECK();
+        }
+        {
+            VIPE_PROF("ba_cholesky", st);
+            ba_cholesky_kernel<<<G, kCholThreads, geo.chol_smem, st>>>(base, per_graph, a.lm, a.ep, a.ilm, a.iep,
+                                                                       intr ? 1 : 0);
+        }
+        VIPE_LAUNCH_CHECK();
+        if (with_frames && grid(kOffFrame) > 0) {
+            VIPE_PROF("ba_backsub", st);
+            if (intr)
+                ba_backsub_kernel<true><<<grid(kOffFrame), 256, 0, st>>>(base, batch(kOffFrame));
+            else
+                ba_backsub_kernel<false><<<grid(kOffFrame), 256, 0, st>>>(base, batch(kOffFrame));
+            VIPE_LAUNCH_CHECK();
+        }
+        {
+            VIPE_PROF("ba_retract", st);
+            ba_retract_kernel<<<grid(kOffRetr), 128, 0, st>>>(base, batch(kOffRetr), intr ? 1 : 0, a.iscale);
+        }
+        VIPE_LAUNCH_CHECK();
+    }
+    if (base.status) {
+        ba_status_kernel<<<G, 1, 0, st>>>(base, per_graph);
+        VIPE_LAUNCH_CHECK();
+    }
     return VIPE_OK;
+}
+
+// carve of a single-graph workspace: [descriptor][graph work]
+template <typename C>
+GraphDesc* carve_single(C& c, const Dims& d, Work* w) {
+    GraphDesc* t = c.template take<GraphDesc>(1);
+    carve(c, d, w);
+    return t;
+}
+
+// carve of a batch workspace: [descriptor table][block offsets][work of graph 0][work of graph 1]...
+template <typename C>
+void carve_batch(C& c, std::vector<GraphDesc>& gds, GraphDesc** table, int** off) {
+    const int G = (int)gds.size();
+    *table = c.template take<GraphDesc>(G);
+    *off = c.template take<int>((size_t)kNumOff * (G + 1));
+    for (int g = 0; g < G; g++) carve(c, gds[g].d, &gds[g].w);
 }
 
 }  // namespace ba
@@ -1322,13 +1593,39 @@ int launch_index(const int64_t* ii, const int64_t* jj, const Dims& d, const Work
 using namespace vipe;
 using namespace vipe::ba;
 
+// Host-side plan of a batch of graphs (opaque to C callers).
+struct vipe_ba_batch_plan {
+    int G = 0;
+    std::vector<GraphDesc> gds;  // Work pointers valid once bound
+    Geometry geo;
+    size_t bytes = 0;
+    long frames = 0, edges = 0, kx = 0, poses = 0;
+    void* ws = nullptr;  // workspace the table was uploaded to
+    GraphDesc* d_table = nullptr;
+    int* d_off = nullptr;
+    std::vector<int> off_host;  // kNumOff x (G + 1), the image of d_off
+};
+
 extern "C" size_t vipe_slam_ba_workspace_size(int num_frames, int ht, int wd, int num_edges, int num_kx, int t0,
                                               int t1) {
     if (check_dims(num_frames, ht, wd, num_edges, num_kx, t0, t1) != VIPE_OK) return 0;
     Dims d = make_dims(num_frames, ht, wd, num_edges, num_kx, t0, t1);
     Sizer s;
-    carve(s, d, nullptr);
+    carve_single(s, d, nullptr);
     return s.used + 256;
+}
+
+static int check_ba_args(const float* poses_io, const float* disps_io, const float* intrinsics_io,
+                         const float* disps_sens, const float* targets, const float* weights, const float* eta,
+                         const int64_t* ii, const int64_t* jj, const float* depth_active, long num_edges,
+                         int iterations, int motion_only, int compute_energy, const float* dx_out,
+                         const float* dz_out, const float* energy_out) {
+    if (!poses_io || !disps_io || !intrinsics_io || !disps_sens || !eta || !depth_active || !dx_out) return VIPE_ERR_ARG;
+    if (num_edges > 0 && (!targets || !weights || !ii || !jj)) return VIPE_ERR_ARG;
+    if (!motion_only && !dz_out) return VIPE_ERR_ARG;
+    if (compute_energy && iterations > 0 && !energy_out) return VIPE_ERR_ARG;
+    if (iterations < 0) return VIPE_ERR_ARG;
+    return VIPE_OK;
 }
 
 extern "C" int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* intrinsics_io, const float* disps_sens,
@@ -1341,102 +1638,148 @@ extern "C" int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* in
                                      int32_t* dev_status, void* stream) {
     int rc = check_dims(num_frames, ht, wd, num_edges, num_kx, t0, t1);
     if (rc != VIPE_OK) return rc;
-    if (!poses_io || !disps_io || !intrinsics_io || !disps_sens || !eta || !depth_active || !dx_out) return VIPE_ERR_ARG;
-    if (num_edges > 0 && (!targets || !weights || !ii || !jj)) return VIPE_ERR_ARG;
-    if (!motion_only && !dz_out) return VIPE_ERR_ARG;
-    if (compute_energy && iterations > 0 && !energy_out) return VIPE_ERR_ARG;
-    if (iterations < 0) return VIPE_ERR_ARG;
+    rc = check_ba_args(poses_io, disps_io, intrinsics_io, disps_sens, targets, weights, eta, ii, jj, depth_active,
+                       num_edges, iterations, motion_only, compute_energy, dx_out, dz_out, energy_out);
+    if (rc != VIPE_OK) return rc;
     cudaStream_t st = as_stream(stream);
-    Dims d = make_dims(num_frames, ht, wd, num_edges, num_kx, t0, t1);
+    GraphDesc gd{};
+    gd.d = make_dims(num_frames, ht, wd, num_edges, num_kx, t0, t1);
     Carver cv(workspace, workspace_bytes);
-    Work w;
-    carve(cv, d, &w);
+    GraphDesc* table = carve_single(cv, gd.d, &gd.w);
     if (!cv.ok) return VIPE_ERR_WORKSPACE;
-    int dev = 0;
-    VIPE_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 64 && !g_smem_set[dev]) {
-        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           kStageFloats * 4));
-        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           kStageFloats * 4));
-        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_cholesky_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           chol_ldr(kPanelRows) * kNB * (int)sizeof(double)));
-        g_smem_set[dev] = true;
-    }
-    if ((rc = launch_index(ii, jj, d, w, st)) != VIPE_OK) return rc;
+    if ((rc = ensure_attributes()) != VIPE_OK) return rc;
+    Geometry geo;
+    fill_geometry({gd.d}, geo);
+    BAPtrs base{poses_io, disps_io, intrinsics_io, disps_sens, targets, weights, eta, ii, jj, depth_active,
+                dx_out, motion_only ? nullptr : dz_out, compute_energy ? energy_out : nullptr, dev_status,
+                iterations, 0};
+    SolveArgs a{iterations, lm, ep, alpha, motion_only, optimize_intrinsics, intrinsics_lm, intrinsics_ep,
+                intrinsics_scale, compute_energy};
+    return run_solve(geo, table, nullptr, base, &gd, a, st);
+}
 
-    const bool intr = optimize_intrinsics != 0;
-    EdgeArgs ea{poses_io, disps_io, intrinsics_io, targets, weights, ii, jj, intrinsics_scale};
-    FrameArgs fa{poses_io, disps_io, disps_sens, intrinsics_io, targets, weights, eta, depth_active, jj, alpha,
-                 intrinsics_scale};
-    const long npairs = (long)d.P * (d.P + 1) / 2;
-    const size_t chol_smem = (size_t)chol_ldr(d.dim) * kNB * sizeof(double);
-    for (int itr = 0; itr < iterations; itr++) {
-        if (d.E > 0) {
-            dim3 ge(d.E, d.CHe);
-            {
-            VIPE_PROF("ba_edge", st);
-            if (intr)
-                ba_edge_kernel<true><<<ge, kEdgeThreads, 0, st>>>(ea, d, w);
-            else
-                ba_edge_kernel<false><<<ge, kEdgeThreads, 0, st>>>(ea, d, w);
-            }
-            VIPE_LAUNCH_CHECK();
-            {
-                VIPE_PROF("ba_edge_reduce", st);
-                ba_edge_reduce<<<d.E, 128, 0, st>>>(ea, d, w);
-            }
-            VIPE_LAUNCH_CHECK();
+// ---------------------------------------------------------------- batched solve
+
+extern "C" int vipe_slam_ba_batch_plan_create(int num_graphs, const int* num_frames, const int* num_edges,
+                                              const int* num_kx, const int* t0, const int* t1, int ht, int wd,
+                                              int edge_chunks, int frame_chunks, vipe_ba_batch_plan** plan_out) {
+    if (!plan_out) return VIPE_ERR_ARG;
+    *plan_out = nullptr;
+    if (num_graphs <= 0 || !num_frames || !num_edges || !num_kx || !t0 || !t1) return VIPE_ERR_ARG;
+    if (edge_chunks < 0 || frame_chunks < 0) return VIPE_ERR_ARG;
+    long sumE = 0, sumK = 0;
+    for (int g = 0; g < num_graphs; g++) {
+        const int rc = check_dims(num_frames[g], ht, wd, num_edges[g], num_kx[g], t0[g], t1[g]);
+        if (rc != VIPE_OK) {
+            char msg[96];
+            snprintf(msg, sizeof(msg), "graph %d of the batch has invalid sizes", g);
+            set_last_error(msg);
+            return rc;
         }
-        if (!motion_only) {
-            dim3 gf(d.K, d.CF);
-            VIPE_PROF("ba_frame", st);
-            if (intr)
-                ba_frame_kernel<true><<<gf, kFrameThreads, kStageFloats * 4, st>>>(fa, d, w);
-            else
-                ba_frame_kernel<false><<<gf, kFrameThreads, kStageFloats * 4, st>>>(fa, d, w);
-            VIPE_LAUNCH_CHECK();
-        }
-        {
-            VIPE_PROF("ba_assemble", st);
-            ba_assemble_blocks<<<ceil_div(npairs, 8), 256, 0, st>>>(ii, jj, d, w, motion_only ? 0 : 1);
-        VIPE_LAUNCH_CHECK();
-            ba_assemble_rhs<<<ceil_div(d.P + 1, 8), 256, 0, st>>>(d, w, motion_only ? 0 : 1, intr ? 1 : 0);
-        }
-        VIPE_LAUNCH_CHECK();
-        if (compute_energy) {
-            VIPE_PROF("ba_energy", st);
-            ba_energy_kernel<<<1, 256, 0, st>>>(d, w, motion_only ? 0 : 1, energy_out, itr);
-            VIPE_LAUNCH_CHECK();
-        }
-        {
-        VIPE_PROF("ba_cholesky", st);
-        ba_cholesky_kernel<<<1, kCholThreads, chol_smem, st>>>(d, w, lm, ep, intrinsics_lm, intrinsics_ep,
-                                                               intr ? 1 : 0, dx_out, dev_status);
-        }
-        VIPE_LAUNCH_CHECK();
-        if (!motion_only) {
-            dim3 gb(d.K, d.CF);
-            VIPE_PROF("ba_backsub", st);
-            if (intr)
-                ba_backsub_kernel<true><<<gb, 256, 0, st>>>(fa, d, w, dx_out, disps_io, dz_out);
-            else
-                ba_backsub_kernel<false><<<gb, 256, 0, st>>>(fa, d, w, dx_out, disps_io, dz_out);
-            VIPE_LAUNCH_CHECK();
-        }
-        {
-            VIPE_PROF("ba_retract", st);
-            ba_retract_kernel<<<ceil_div(d.P, 128), 128, 0, st>>>(d, w, dx_out, poses_io, intrinsics_io,
-                                                                  intr ? 1 : 0, intrinsics_scale);
-        }
-        VIPE_LAUNCH_CHECK();
+        sumE += num_edges[g];
+        sumK += num_kx[g];
     }
-    if (dev_status) {
-        ba_status_kernel<<<1, 1, 0, st>>>(w, dev_status);
-        VIPE_LAUNCH_CHECK();
+    // Batch-wide pixel chunking: the whole batch, not each graph, should give
+    // about two CTAs per SM; large batches therefore run unchunked.
+    const int target = 2 * 148;
+    const int che = edge_chunks > 0 ? edge_chunks : (sumE > 0 ? (int)std::max<long>(1, (target + sumE - 1) / sumE) : 1);
+    const int cf = frame_chunks > 0 ? frame_chunks : (int)std::max<long>(1, (target + sumK - 1) / sumK);
+    auto* plan = new vipe_ba_batch_plan();
+    plan->G = num_graphs;
+    plan->gds.resize(num_graphs);
+    std::vector<Dims> dims(num_graphs);
+    for (int g = 0; g < num_graphs; g++) {
+        GraphDesc& gd = plan->gds[g];
+        gd = GraphDesc{};
+        gd.d = make_dims(num_frames[g], ht, wd, num_edges[g], num_kx[g], t0[g], t1[g], che, cf);
+        gd.frame_off = plan->frames;
+        gd.edge_off = plan->edges;
+        gd.kx_off = plan->kx;
+        gd.pose_off = plan->poses;
+        gd.g = g;
+        plan->frames += num_frames[g];
+        plan->edges += num_edges[g];
+        plan->kx += num_kx[g];
+        plan->poses += t1[g] - t0[g];
+        dims[g] = gd.d;
     }
+    fill_geometry(dims, plan->geo);
+    for (int k = 0; k < kNumOff; k++)
+        if ((long)plan->geo.off[k][num_graphs] > 0x7fffffffL) {
+            delete plan;
+            return VIPE_ERR_CAPACITY;
+        }
+    plan->off_host.resize((size_t)kNumOff * (num_graphs + 1));
+    for (int k = 0; k < kNumOff; k++)
+        std::copy(plan->geo.off[k].begin(), plan->geo.off[k].end(), plan->off_host.begin() + (size_t)k * (num_graphs + 1));
+    Sizer sz;
+    GraphDesc* t;
+    int* o;
+    std::vector<GraphDesc> tmp = plan->gds;
+    carve_batch(sz, tmp, &t, &o);
+    plan->bytes = sz.used + 256;
+    *plan_out = plan;
     return VIPE_OK;
 }
+
+extern "C" size_t vipe_slam_ba_batch_workspace_size(const vipe_ba_batch_plan* plan) { return plan ? plan->bytes : 0; }
+
+extern "C" int vipe_slam_ba_batch_totals(const vipe_ba_batch_plan* plan, int64_t* totals_out) {
+    if (!plan || !totals_out) return VIPE_ERR_ARG;
+    totals_out[0] = plan->frames;
+    totals_out[1] = plan->edges;
+    totals_out[2] = plan->kx;
+    totals_out[3] = plan->poses;
+    return VIPE_OK;
+}
+
+extern "C" int vipe_slam_ba_batch_bind(vipe_ba_batch_plan* plan, void* workspace, size_t workspace_bytes,
+                                       void* stream) {
+    if (!plan || !workspace) return VIPE_ERR_ARG;
+    Carver cv(workspace, workspace_bytes);
+    GraphDesc* table;
+    int* off;
+    carve_batch(cv, plan->gds, &table, &off);
+    if (!cv.ok) return VIPE_ERR_WORKSPACE;
+    int rc = ensure_attributes();
+    if (rc != VIPE_OK) return rc;
+    cudaStream_t st = as_stream(stream);
+    VIPE_CUDA_TRY(cudaMemcpyAsync(table, plan->gds.data(), plan->gds.size() * sizeof(GraphDesc),
+                                  cudaMemcpyHostToDevice, st));
+    VIPE_CUDA_TRY(cudaMemcpyAsync(off, plan->off_host.data(), plan->off_host.size() * sizeof(int),
+                                  cudaMemcpyHostToDevice, st));
+    VIPE_CUDA_TRY(cudaStreamSynchronize(st));
+    plan->ws = workspace;
+    plan->d_table = table;
+    plan->d_off = off;
+    return VIPE_OK;
+}
+
+extern "C" int vipe_slam_ba_batch_solve(const vipe_ba_batch_plan* plan, float* poses_io, float* disps_io,
+                                        float* intrinsics_io, const float* disps_sens, const float* targets,
+                                        const float* weights, const float* eta, const int64_t* ii, const int64_t* jj,
+                                        const float* depth_active, int iterations, float lm, float ep,
+                                        int motion_only, float alpha, int optimize_intrinsics, float intrinsics_lm,
+                                        float intrinsics_ep, float intrinsics_scale, int compute_energy,
+                                        float* dx_out, float* dz_out, float* energy_out, int32_t* dev_status,
+                                        void* stream) {
+    if (!plan) return VIPE_ERR_ARG;
+    if (!plan->d_table) {
+        set_last_error("vipe_slam_ba_batch_solve: plan is not bound to a workspace");
+        return VIPE_ERR_WORKSPACE;
+    }
+    int rc = check_ba_args(poses_io, disps_io, intrinsics_io, disps_sens, targets, weights, eta, ii, jj, depth_active,
+                           plan->edges, iterations, motion_only, compute_energy, dx_out, dz_out, energy_out);
+    if (rc != VIPE_OK) return rc;
+    BAPtrs base{poses_io, disps_io, intrinsics_io, disps_sens, targets, weights, eta, ii, jj, depth_active,
+                dx_out, motion_only ? nullptr : dz_out, compute_energy ? energy_out : nullptr, dev_status,
+                iterations, 1};
+    SolveArgs a{iterations, lm, ep, alpha, motion_only, optimize_intrinsics, intrinsics_lm, intrinsics_ep,
+                intrinsics_scale, compute_energy};
+    return run_solve(plan->geo, plan->d_table, plan->d_off, base, nullptr, a, as_stream(stream));
+}
+
+extern "C" void vipe_slam_ba_batch_plan_destroy(vipe_ba_batch_plan* plan) { delete plan; }
 
 extern "C" int vipe_slam_ba(float* poses_io, float* disps_io, float* intrinsics_io, const float* disps_sens,
                             const float* targets, const float* weights, const float* eta, const int64_t* ii,
@@ -1461,12 +1804,18 @@ extern "C" int vipe_slam_ba_index_debug(const int64_t* ii, const int64_t* jj, in
     int rc = check_dims(num_frames, 1, 1, num_edges, num_kx, t0, t1);
     if (rc != VIPE_OK) return rc;
     cudaStream_t st = as_stream(stream);
-    Dims d = make_dims(num_frames, 1, 1, num_edges, num_kx, t0, t1);
+    GraphDesc gd{};
+    gd.d = make_dims(num_frames, 1, 1, num_edges, num_kx, t0, t1);
+    const Dims& d = gd.d;
+    const Work& w = gd.w;
     Carver cv(workspace, workspace_bytes);
-    Work w;
-    carve(cv, d, &w);
+    GraphDesc* table = carve_single(cv, gd.d, &gd.w);
     if (!cv.ok) return VIPE_ERR_WORKSPACE;
-    if ((rc = launch_index(ii, jj, d, w, st)) != VIPE_OK) return rc;
+    BAPtrs base{};
+    base.ii = ii;
+    base.jj = jj;
+    ba_index_kernel<<<1, kIndexThreads, 0, st>>>(base, Batch{table, nullptr, 1}, gd, 1);
+    VIPE_LAUNCH_CHECK();
     int status = 0;
     VIPE_CUDA_TRY(cudaMemcpyAsync(&status, w.status, sizeof(int), cudaMemcpyDeviceToHost, st));
     VIPE_CUDA_TRY(cudaStreamSynchronize(st));

@@ -256,3 +256,159 @@ def ba_small(n_frames: int = 6, ht: int = 12, wd: int = 16, radius: int = 2, see
     """A reduced-size problem with the same generative model (fast CPU oracle cases)."""
     return make_ba_problem(n_frames, band_edges(n_frames, radius), seed=seed, ht=ht, wd=wd, t0=t0,
                            iterations=iterations, intrinsics=(15.0, 15.0, wd / 2.0, ht / 2.0))
+
+
+# ---------------------------------------------------------------- batched workload (many uneven clips)
+
+def _torch_quat_rot(q, x):
+    v, w = q[..., :3], q[..., 3:4]
+    uv = 2.0 * torch.cross(v, x, dim=-1)
+    return x + w * uv + torch.cross(v, uv, dim=-1)
+
+
+def _torch_quat_mul(a, b):
+    ax, ay, az, aw = a.unbind(-1)
+    bx, by, bz, bw = b.unbind(-1)
+    return torch.stack([aw * bx + ax * bw + ay * bz - az * by, aw * by - ax * bz + ay * bw + az * bx,
+                        aw * bz + ax * by - ay * bx + az * bw, aw * bw - ax * bx - ay * by - az * bz], -1)
+
+
+def _torch_relative(Ti, Tj):
+    """Tij = Tj * Ti^-1 for (..., 7) SE3 poses."""
+    qi_inv = Ti[..., 3:] * Ti.new_tensor([-1.0, -1.0, -1.0, 1.0])
+    ti_inv = -_torch_quat_rot(qi_inv, Ti[..., :3])
+    q = _torch_quat_mul(Tj[..., 3:], qi_inv)
+    t = Tj[..., :3] + _torch_quat_rot(Tj[..., 3:], ti_inv)
+    return torch.cat([t, q], -1)
+
+
+@dataclass
+class BABatch:
+    """Concatenated inputs of many clips (the BatchPlan layout) plus per-clip sizes."""
+
+    tensors: dict  # BATCH_KEYS -> tensor on `device`
+    num_frames: list
+    num_edges: list
+    num_kx: list
+    t0: list
+    t1: list
+    ht: int
+    wd: int
+    poses_gt: torch.Tensor
+    disps_gt: torch.Tensor
+
+    @property
+    def sizes(self):
+        return (self.num_frames, self.num_edges, self.num_kx, self.t0, self.t1)
+
+    @property
+    def G(self) -> int:
+        return len(self.num_frames)
+
+    def clip(self, g: int) -> BAProblem:
+        """Clip g as a standalone BAProblem (CPU tensors), for per-graph reference solves."""
+        fo, eo, ko = (sum(x[:g]) for x in (self.num_frames, self.num_edges, self.num_kx))
+        n, e, k = self.num_frames[g], self.num_edges[g], self.num_kx[g]
+        t = {key: v.cpu() for key, v in self.tensors.items()}
+        return BAProblem(poses=t["poses"][fo:fo + n].clone(), disps=t["disps"][fo:fo + n].clone(),
+                         intrinsics=t["intrinsics"][g].clone(), disps_sens=t["disps_sens"][fo:fo + n].clone(),
+                         targets=t["targets"][eo:eo + e].clone(), weights=t["weights"][eo:eo + e].clone(),
+                         eta=t["eta"][ko:ko + k].clone(), ii=t["ii"][eo:eo + e].clone(), jj=t["jj"][eo:eo + e].clone(),
+                         depth_active=t["depth_active"][fo:fo + n].clone(), t0=self.t0[g], t1=self.t1[g],
+                         iterations=4, poses_gt=self.poses_gt[fo:fo + n].cpu(), disps_gt=self.disps_gt[fo:fo + n].cpu())
+
+
+def make_ba_batch(num_clips: int, seed: int, frames_range=(8, 96), radius: int = 3, loops_mean: float = 4.0,
+                  loop_gap: int = 8, outlier_frac: float = 0.01, ht: int = 48, wd: int = 64, t0: int = 2,
+                  intrinsics=(60.0, 60.0, 32.0, 24.0), device="cpu") -> BABatch:
+    """Many clips of the BA generative model with uneven sizes.
+
+    Keyframe counts ~ U{frames_range}; edges |i-j| <= radius plus Poisson(loops_mean)
+    random loop pairs with |i-j| > loop_gap (both directions); a fraction
+    `outlier_frac` of target entries is replaced by U(-20, 20) px with weight
+    0.05.  Structure comes from numpy (seeded), the bulk noise from a seeded
+    torch generator on `device` (generation runs on the GPU for large batches).
+    """
+    rng = np.random.default_rng(seed)
+    dev = torch.device(device)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    nf = rng.integers(frames_range[0], frames_range[1] + 1, size=num_clips).tolist()
+    ii_l, jj_l, ne, nk = [], [], [], []
+    T_all = []
+    for g in range(num_clips):
+        n = nf[g]
+        edges = band_edges(n, radius)
+        nl = int(rng.poisson(loops_mean))
+        if n - 1 > loop_gap and nl > 0:
+            edges += random_long_edges(n, nl, loop_gap, rng)
+        ii_l += [e[0] for e in edges]
+        jj_l += [e[1] for e in edges]
+        ne.append(len(edges))
+        kx = np.unique(np.concatenate([np.arange(t0, n), np.array([e[0] for e in edges], dtype=np.int64)]))
+        nk.append(len(kx))
+        T = np.zeros((n, 7))
+        T[0] = [0, 0, 0, 0, 0, 0, 1]
+        steps = np.concatenate([rng.normal(0, 0.05, (n, 3)), rng.normal(0, 0.02, (n, 3))], 1)
+        for i in range(1, n):
+            T[i] = se3_mul(se3_exp(steps[i]), T[i - 1])
+        T_all.append(T)
+    Nt, Et, Kt = sum(nf), sum(ne), sum(nk)
+    T_gt = torch.from_numpy(np.concatenate(T_all)).to(dev)
+    frame_off = np.concatenate([[0], np.cumsum(nf)[:-1]])
+    clip_of_edge = np.repeat(np.arange(num_clips), ne)
+    ii = torch.tensor(ii_l, dtype=torch.int64, device=dev)
+    jj = torch.tensor(jj_l, dtype=torch.int64, device=dev)
+    gi = ii + torch.from_numpy(frame_off[clip_of_edge]).to(dev)
+    gj = jj + torch.from_numpy(frame_off[clip_of_edge]).to(dev)
+    # ground-truth inverse depth: blurred noise mapped to [0.1, 1]
+    noise = torch.randn(Nt, 1, ht, wd, generator=gen, device=dev, dtype=torch.float64)
+    r = 12
+    k1 = torch.exp(-0.5 * (torch.arange(-r, r + 1, device=dev, dtype=torch.float64) / 4.0) ** 2)
+    k1 = k1 / k1.sum()
+    sm = torch.nn.functional.conv2d(torch.nn.functional.pad(noise, (r, r, 0, 0), mode="replicate"), k1.view(1, 1, 1, -1))
+    sm = torch.nn.functional.conv2d(torch.nn.functional.pad(sm, (0, 0, r, r), mode="replicate"), k1.view(1, 1, -1, 1))
+    sm = sm[:, 0]
+    lo = sm.flatten(1).min(1).values.view(-1, 1, 1)
+    hi = sm.flatten(1).max(1).values.view(-1, 1, 1)
+    d_gt = 0.1 + 0.9 * (sm - lo) / (hi - lo).clamp_min(1e-12)
+    fx, fy, cx, cy = intrinsics
+    vv, uu = torch.meshgrid(torch.arange(ht, device=dev, dtype=torch.float64),
+                            torch.arange(wd, device=dev, dtype=torch.float64), indexing="ij")
+    X = torch.stack([(uu - cx) / fx, (vv - cy) / fy, torch.ones_like(uu)], -1)  # (H, W, 3)
+    targets = torch.empty(Et, 2, ht, wd, device=dev, dtype=torch.float32)
+    weights = torch.empty(Et, 2, ht, wd, device=dev, dtype=torch.float32)
+    chunk = 4096
+    for e0 in range(0, Et, chunk):
+        e1 = min(Et, e0 + chunk)
+        Tij = _torch_relative(T_gt[gi[e0:e1]], T_gt[gj[e0:e1]])  # (c, 7)
+        Xj = _torch_quat_rot(Tij[:, None, None, 3:], X[None]) + d_gt[gi[e0:e1]][..., None] * Tij[:, None, None, :3]
+        z = Xj[..., 2]
+        tg = torch.stack([fx * Xj[..., 0] / z + cx, fy * Xj[..., 1] / z + cy], 1)
+        tg = tg + 0.5 * torch.randn(tg.shape, generator=gen, device=dev, dtype=torch.float64)
+        wt = torch.rand(tg.shape, generator=gen, device=dev, dtype=torch.float64) * 0.9 + 0.1
+        if outlier_frac > 0:
+            out = torch.rand(tg.shape, generator=gen, device=dev, dtype=torch.float64) < outlier_frac
+            tg = torch.where(out, torch.rand(tg.shape, generator=gen, device=dev, dtype=torch.float64) * 40 - 20, tg)
+            wt = torch.where(out, torch.full_like(wt, 0.05), wt)
+        targets[e0:e1] = tg.float()
+        weights[e0:e1] = wt.float()
+    # initial state
+    delta = torch.cat([torch.randn(Nt, 3, generator=gen, device=dev, dtype=torch.float64) * (0.02 / math.sqrt(3)),
+                       torch.randn(Nt, 3, generator=gen, device=dev, dtype=torch.float64) * (0.01 / math.sqrt(3))], 1)
+    P0 = torch.from_numpy(se3_mul(se3_exp(delta.cpu().numpy()), T_gt.cpu().numpy())).to(dev)
+    d0 = d_gt * (1 + 0.05 * torch.randn(d_gt.shape, generator=gen, device=dev, dtype=torch.float64))
+    eta = 0.2 * (torch.rand(Kt, ht, wd, generator=gen, device=dev, dtype=torch.float64) * (1e-2 - 1e-4) + 1e-4) + 1e-7
+    tensors = dict(
+        poses=P0.float().contiguous(), disps=d0.float().contiguous(),
+        intrinsics=torch.tensor(intrinsics, dtype=torch.float32, device=dev).repeat(num_clips, 1).contiguous(),
+        disps_sens=torch.zeros(Nt, ht, wd, device=dev), targets=targets, weights=weights,
+        eta=eta.float().contiguous(), ii=ii, jj=jj, depth_active=torch.ones(Nt, device=dev),
+    )
+    return BABatch(tensors=tensors, num_frames=nf, num_edges=ne, num_kx=nk, t0=[t0] * num_clips, t1=nf, ht=ht, wd=wd,
+                   poses_gt=T_gt.float(), disps_gt=d_gt.float())
+
+
+def ba_config4_se3(device="cpu", num_clips: int = 256) -> BABatch:
+    """256 clips, keyframes ~ U{8..96}, |i-j| <= 3 + Poisson(4) loops, 1% outliers (SE3 form)."""
+    return make_ba_batch(num_clips, seed=1004, device=device)
