@@ -40,10 +40,10 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "BA solves/s"
+METRIC = "batched BA solves/s"
 WORKLOAD = (
-    "plain FP32 drop-in slam_ext.ba_extended: 64 keyframes 48x64 SE3, 628 edges "
-    "(|i-j|<=3 + 128 random long-range pairs x2), 4 LM iterations, t0=2"
+    "batched BA: 256 clips, keyframes ~U{8..96} at 48x64, SE3, edges |i-j|<=3 + Poisson(4) loop pairs "
+    "(|i-j|>8, both directions), 1% outlier flow (U(-20,20) px, weight 0.05), 4 LM iterations, t0=2"
 )
 
 
@@ -250,25 +250,33 @@ def corr_build_bench(dev, steps, hbm_peak, peak_src, bf16_peak):
     }
 
 
-def cpu_baseline(p, sample_s):
+def _cpu_clip_solves(sample_s, max_clips=256):
+    """Solves clips of the 256-clip batch one after another on the CPU oracle until
+    `sample_s` seconds have passed; returns (solves, seconds, threads)."""
     import oracle.ba as ob
+    from vipe_b200 import workloads as Wk
 
     threads = os.cpu_count() or 1
     ob.set_threads(threads)
-    ob.ba(p, fp64=False)  # warm (builds the oracle if needed)
+    b = Wk.ba_config4_se3(device="cpu", num_clips=24)  # the batch's first clips (same sizes and model)
+    ob.ba(b.clip(0), fp64=False, iterations=1)  # warm (builds the oracle if needed)
     n, t0 = 0, time.perf_counter()
-    while True:
-        ob.ba(p, fp64=False)
+    while n < max_clips:
+        ob.ba(b.clip(n % b.G), fp64=False, iterations=4)
         n += 1
-        el = time.perf_counter() - t0
-        if el >= sample_s or n >= 200:
+        if time.perf_counter() - t0 >= sample_s:
             break
+    return n, time.perf_counter() - t0, threads
+
+
+def cpu_baseline(sample_s):
+    n, el, threads = _cpu_clip_solves(sample_s)
     return {
         "value": n / el,
         "unit": "solves/s",
         "cores": threads,
         "kind": "port",
-        "sample": f"{n} solves of the same 64-keyframe / 628-edge / 4-iteration graph in {el:.1f} s "
+        "sample": f"{n} clip solves cycling over the first 24 clips of the 256-clip batch, 4 LM iterations each, in {el:.1f} s "
         f"(oracle/ba_oracle.cpp, FP32 per-edge math on {threads} threads, dense FP64 Cholesky)",
     }
 
@@ -279,19 +287,15 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    from vipe_b200 import workloads as Wk
-    import oracle.ba as ob
-
-    p = Wk.ba_config1()
+    per_step = 10.0
+    solves, secs = 0, 0.0
     threads = os.cpu_count() or 1
-    ob.set_threads(threads)
-    for _ in range(max(0, args.warmup)):
-        ob.ba(p, fp64=False)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        ob.ba(p, fp64=False)
-    el = time.perf_counter() - t0
-    v = args.steps / el
+    for k in range(max(0, args.warmup) + args.steps):
+        n, el, threads = _cpu_clip_solves(per_step if k >= args.warmup else 2.0, max_clips=64)
+        if k >= args.warmup:
+            solves += n
+            secs += el
+    v = solves / secs
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -300,20 +304,21 @@ def run_reference(args):
         "n_gpus": args.gpus,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": 1e3 * el / args.steps,
+        "ms_per_step": 1e3 * secs / max(1, args.steps),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "global_batch": 1, "parallelism": "host threads"},
+        "config": {"workload": WORKLOAD, "global_batch": 256, "parallelism": "host threads"},
         "cpu_baseline": {
             "value": v,
             "unit": "solves/s",
             "cores": threads,
             "kind": "port",
-            "sample": f"{args.steps} full solves of the workload graph (oracle/ba_oracle.cpp: the reference's "
-            f"ba_cuda_impl restated on the CPU; the reference extension needs Eigen and CUDA and is not built here)",
+            "sample": f"{solves} clip solves of the 256-clip batch (each step solves clips for about {per_step:.0f} s; "
+            f"oracle/ba_oracle.cpp, the reference's ba_cuda_impl restated on the CPU; the reference extension "
+            f"needs Eigen and CUDA and is not built here)",
         },
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -322,6 +327,226 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- our arm
+
+def batch_kernel_bytes(b, name):
+    """Algorithmic DRAM bytes of one launch of a BA kernel over the whole batch (fp32 = 4 B)."""
+    HW = b.ht * b.wd
+    E, K = sum(b.num_edges), sum(b.num_kx)
+    if name == "ba_edge":
+        return E * HW * 16 + K * HW * 4
+    if name == "ba_frame":
+        return E * HW * 16 + K * HW * 24
+    if name == "ba_backsub":
+        return E * HW * 8 + K * HW * 24
+    return None
+
+
+def batched_leg(dev, args, world, dist, flush, stream):
+    """The chosen batched form on the 256-clip uneven batch; returns (value, e2e, extras)."""
+    import torch
+
+    from vipe_b200 import _lib, ba_batch as BB, workloads as Wk
+
+    b = Wk.ba_config4_se3(device=dev)
+    iters, lm, ep = 4, 1e-4, 0.1
+    tune = BB.autotune(b.sizes, b.ht, b.wd, b.tensors, iters, lm, ep, dev, reps=1)
+    plan = BB.BatchPlan(*b.sizes, b.ht, b.wd, dev, edge_chunks=tune.edge_chunks, frame_chunks=tune.frame_chunks)
+    static = {k: v.clone() for k, v in b.tensors.items()}
+    cap = plan.capture(static, iterations=iters, lm=lm, ep=ep)
+    mutable = ("poses", "disps", "intrinsics")
+
+    def reset():
+        for k in mutable:
+            static[k].copy_(b.tensors[k])
+
+    for _ in range(max(3, args.warmup)):
+        reset()
+        cap.replay()
+    torch.cuda.synchronize(dev)
+    n = max(3, args.steps // 2)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+    if world > 1:
+        dist.barrier()
+    for k in range(n):
+        reset()
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        cap.replay()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    dev_ms = sum(a.elapsed_time(c) for a, c in ev)
+    t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    batch_ms = float(t.item()) / n
+    value = world * b.G / (batch_ms / 1e3)
+    status = cap.out[3].cpu().tolist()
+
+    # accuracy of the batch against the FP64 oracle on a few clips
+    acc = []
+    import oracle.ba as ob
+
+    fo = 0
+    for g in range(b.G):
+        if g in (0, b.G // 2, b.G - 1):
+            p = b.clip(g)
+            want = ob.ba(p, fp64=True)
+            gp = static["poses"][fo:fo + b.num_frames[g]].double().cpu().numpy()
+            acc.append(float(abs(gp - want["poses"]).max()))
+        fo += b.num_frames[g]
+
+    # end to end through the public API: pinned host inputs -> device, solve, results -> host
+    host = {k: v.cpu().pin_memory() for k, v in b.tensors.items()}
+    h2d = sum(v.numel() * v.element_size() for v in host.values())
+    out_host = None
+    e2e = []
+    for k in range(4):
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.fill_(float(k))
+        a.record(stream)
+        for key, v in host.items():
+            static[key].copy_(v, non_blocking=True)
+        dx, dz, _, st = plan.solve(**static, iterations=iters, lm=lm, ep=ep, out=cap.out, check=False)
+        outs = [static["poses"], static["disps"], dx, st]
+        if out_host is None:
+            out_host = [torch.empty_like(o, device="cpu").pin_memory() for o in outs]
+        for o, h in zip(outs, out_host):
+            h.copy_(o, non_blocking=True)
+        c.record(stream)
+        torch.cuda.synchronize(dev)
+        if k >= 1:
+            e2e.append(a.elapsed_time(c))
+    d2h = sum(h.numel() * h.element_size() for h in out_host)
+    te = torch.tensor([sum(e2e)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * b.G * len(e2e) / (float(te.item()) / 1e3)
+
+    # live per-kernel profile of one eager batched solve
+    lib = _lib.load()
+
+    def once():
+        reset()
+        flush.fill_(1.0)
+        plan.solve(**static, iterations=iters, lm=lm, ep=ep, out=cap.out, check=False)
+
+    prof = profile_kernels(lib, once, 2)
+    launches = sum(v[1] for v in prof.values()) / 2
+    hbm, bf16, src = measured_peaks()
+    total = sum(v[0] for v in prof.values())
+    breakdown = {k: {"ms_per_batch": v[0] / 2, "share": v[0] / total} for k, v in prof.items()}
+    roof = None
+    for name, (ms, cnt) in sorted(prof.items(), key=lambda kv: -kv[1][0]):
+        nbytes = batch_kernel_bytes(b, name)
+        if nbytes is None:
+            continue
+        avg_s = ms / cnt / 1e3
+        ach = nbytes / avg_s / 1e9
+        roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "traffic": None, "peak_source": src, "bytes_per_launch": nbytes, "avg_launch_ms": avg_s * 1e3}
+        break
+
+    # the plain drop-in on the same batch, clip by clip, same GPU (the 5x comparison)
+    from vipe_b200.ext import slam_ext as S
+
+    S.CHECK_DEVICE_STATUS = False
+    fo = eo = ko = 0
+    clips = []
+    for g in range(b.G):
+        n_, e_, k_ = b.num_frames[g], b.num_edges[g], b.num_kx[g]
+        clips.append({key: (b.tensors[key][fo:fo + n_] if key in ("poses", "disps", "disps_sens", "depth_active")
+                            else b.tensors[key][eo:eo + e_] if key in ("targets", "weights", "ii", "jj")
+                            else b.tensors[key][ko:ko + k_] if key == "eta" else b.tensors[key][g])
+                      for key in b.tensors})
+        fo, eo, ko = fo + n_, eo + e_, ko + k_
+    work = [{k: (v.clone() if k in mutable else v) for k, v in c.items()} for c in clips]
+
+    def plain_pass():
+        for g, c in enumerate(work):
+            S.ba_extended(c["poses"], c["disps"], c["intrinsics"], c["disps_sens"], c["targets"], c["weights"],
+                          c["eta"], c["ii"], c["jj"], c["depth_active"], b.t0[g], b.t1[g], iters, lm, ep, False,
+                          0.001, False, 1e-6, 1e-6, 1.0, False)
+
+    plain_pass()
+    for g, c in enumerate(work):
+        for k in mutable:
+            c[k].copy_(clips[g][k])
+    torch.cuda.synchronize(dev)
+    a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    plain_pass()
+    c.record(stream)
+    torch.cuda.synchronize(dev)
+    plain_ms = a.elapsed_time(c)
+    extras = {
+        "batch": {"clips": b.G, "frames": sum(b.num_frames), "edges": sum(b.num_edges), "depth_rows": sum(b.num_kx),
+                  "input_bytes": h2d},
+        "batch_ms": batch_ms,
+        "status_nonzero": sum(1 for x in status if x),
+        "autotune": {"edge_chunks": tune.edge_chunks, "frame_chunks": tune.frame_chunks,
+                     "table_ms": [[ec, fc, ms] for ec, fc, ms in tune.table]},
+        "plain_same_gpu": {"value": b.G / (plain_ms / 1e3), "unit": "solves/s", "ms_per_batch": plain_ms,
+                           "api": "vipe_b200.ext.slam_ext.ba_extended, one clip per call"},
+        "speedup_vs_plain_same_gpu": (b.G / (batch_ms / 1e3)) / (b.G / (plain_ms / 1e3)),
+        "max_pose_err_vs_fp64_oracle": max(acc),
+        "kernel_breakdown": breakdown,
+        "roofline": roof,
+        "gpu_launches_per_batch": launches,
+    }
+    e2e_line = {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "api": "vipe_b200.ba_batch.BatchPlan.solve (pinned host tensors copied in and out each step)"}
+    del plan, cap, static, work, clips
+    return value, e2e_line, extras, b.G, n
+
+
+def plain_cfg1_leg(dev, args, flush, stream):
+    """The plain FP32 drop-in on the 64-keyframe / 628-edge graph (one graph per call)."""
+    import torch
+
+    from vipe_b200 import _lib, workloads as Wk
+    from vipe_b200.ext import slam_ext as S
+
+    lib = _lib.load()
+    p = Wk.ba_config1()
+    g0 = p.to(dev)
+    S.CHECK_DEVICE_STATUS = False
+    for _ in range(3):
+        ba_call(S, g0.clone())
+    states = [g0.clone() for _ in range(args.steps)]
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize(dev)
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        ba_call(S, states[k])
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    prof_states = [g0.clone() for _ in range(3)]
+    it = iter(prof_states)
+
+    def once():
+        flush.fill_(1.0)
+        ba_call(S, next(it))
+
+    prof = profile_kernels(lib, once, len(prof_states))
+    total = sum(v[0] for v in prof.values())
+    hbm, _, src = measured_peaks()
+    fr = prof.get("ba_frame")
+    roof = None
+    if fr:
+        nbytes = kernel_bytes(p, "ba_frame")
+        avg_s = fr[0] / fr[1] / 1e3
+        roof = {"kernel": "ba_frame", "achieved": nbytes / avg_s / 1e9, "peak": hbm, "unit": "GB/s",
+                "frac": nbytes / avg_s / 1e9 / hbm, "peak_source": src}
+    return {
+        "workload": "plain FP32 drop-in slam_ext.ba_extended: 64 keyframes 48x64 SE3, 628 edges "
+        "(|i-j|<=3 + 128 random long-range pairs x2), 4 LM iterations, t0=2",
+        "value": 1e3 / ms, "unit": "solves/s", "ms_per_solve": ms,
+        "kernel_breakdown": {k: {"ms_per_solve": v[0] / 3, "share": v[0] / total} for k, v in prof.items()},
+        "roofline_ba_frame": roof,
+    }
+
 
 def run_ours(args):
     import torch
@@ -334,136 +559,28 @@ def run_ours(args):
         from datetime import timedelta
 
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
-
-    from vipe_b200 import _lib, workloads as Wk
-    from vipe_b200.ext import slam_ext as S
-
-    lib = _lib.load()
-    p = Wk.ba_config1()
-    g0 = p.to(dev)
-    S.CHECK_DEVICE_STATUS = False  # the status word is read once after the timed region
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
-    def fresh():
-        q = g0.clone()
-        return q
-
-    # warmup
-    for _ in range(max(3, args.warmup)):
-        ba_call(S, fresh())
-    torch.cuda.synchronize(dev)
-
-    # device-timed region: fresh mutable state per step, L2 flushed between steps
-    states = [fresh() for _ in range(args.steps)]
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
     with ClockSampler(local) as clk:
-        for k in range(args.steps):
-            flush.fill_(float(k))
-            ev[k][0].record(stream)
-            ba_call(S, states[k])
-            ev[k][1].record(stream)
-        torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
-    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
-    t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = world * args.steps / (max_ms / 1e3)
-
-    # sanity: the status word of a checked solve
-    S.CHECK_DEVICE_STATUS = True
-    chk = fresh()
-    ba_call(S, chk)
-    S.CHECK_DEVICE_STATUS = False
-
-    # end-to-end through the public API from pinned host memory
-    host_in = {k: getattr(p, k).pin_memory() for k in
-               ("poses", "disps", "intrinsics", "disps_sens", "targets", "weights", "eta", "ii", "jj", "depth_active")}
-    h2d = sum(v.numel() * v.element_size() for v in host_in.values())
-    out_host = None
-    e2e_ev = []
-    S.CHECK_DEVICE_STATUS = True  # the public API default: one status read per call
-    for k in range(max(1, args.steps // 2) + 2):
-        flush.fill_(float(k))
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        q = Wk.BAProblem(**{**{kk: vv for kk, vv in p.__dict__.items()},
-                            **{kk: vv.to(dev, non_blocking=True) for kk, vv in host_in.items()}})
-        dx, dz, _ = ba_call(S, q)
-        outs = [q.poses, q.disps, q.intrinsics, dx, dz]
-        if out_host is None:
-            out_host = [torch.empty_like(o, device="cpu").pin_memory() for o in outs]
-        for o, h in zip(outs, out_host):
-            h.copy_(o, non_blocking=True)
-        b.record(stream)
-        torch.cuda.synchronize(dev)
-        if k >= 2:
-            e2e_ev.append(a.elapsed_time(b))
-    d2h = sum(h.numel() * h.element_size() for h in out_host)
-    e2e_ms = sum(e2e_ev)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * len(e2e_ev) / (float(te.item()) / 1e3)
-    S.CHECK_DEVICE_STATUS = False
-
-    # dominant kernel, timed live (events around each launch on this stream)
-    prof_states = [fresh() for _ in range(5)]
-    it = iter(prof_states)
-
-    def once():
-        flush.fill_(1.0)
-        ba_call(S, next(it))
-
-    prof = profile_kernels(lib, once, len(prof_states))
-    dom = max(prof.items(), key=lambda kv: kv[1][0])
+        value, e2e, extras, G, n = batched_leg(dev, args, world, dist, flush, stream)
+    torch.cuda.empty_cache()
+    plain = plain_cfg1_leg(dev, args, flush, stream)
     hbm, bf16, src = measured_peaks()
-    roof = None
-    for name, (ms, n) in sorted(prof.items(), key=lambda kv: -kv[1][0]):
-        nbytes = kernel_bytes(p, name)
-        if nbytes is None:
-            continue
-        avg_s = ms / n / 1e3
-        ach = nbytes / avg_s / 1e9
-        roof = {
-            "kernel": name,
-            "bound": "hbm",
-            "achieved": ach,
-            "peak": hbm,
-            "unit": "GB/s",
-            "frac": ach / hbm,
-            "traffic": None,
-            "peak_source": src,
-            "bytes_per_launch": nbytes,
-            "avg_launch_ms": avg_s * 1e3,
-        }
-        break
-    total_prof = sum(v[0] for v in prof.values())
-    breakdown = {k: {"ms_per_solve": v[0] / len(prof_states), "share": v[0] / total_prof} for k, v in prof.items()}
-
-    launches_per_solve = sum(v[1] for v in prof.values()) / len(prof_states)
     corr = None
     if not args.no_corr:
-        del states, prof_states
         torch.cuda.empty_cache()
         corr = corr_build_bench(dev, 5, hbm, src, bf16)
 
-    line = None
     if rank == 0:
         line = {
             "metric": METRIC,
             "value": value,
             "unit": "solves/s",
             "n_gpus": world,
-            "steps": args.steps,
-            "warmup": args.warmup,
-            "ms_per_step": max_ms / args.steps,
+            "steps": n,
+            "warmup": max(3, args.warmup),
+            "ms_per_step": extras["batch_ms"],
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
@@ -471,28 +588,23 @@ def run_ours(args):
             "data": "synthetic",
             "config": {
                 "workload": WORKLOAD,
-                "global_batch": world,
-                "per_gpu_batch": 1,
+                "global_batch": G * world,
+                "per_gpu_batch": G,
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                "l2": "flushed (256 MiB write) between timed steps",
-                "form": "plain FP32 drop-in (FP64 block sums and Cholesky on the GPU)",
+                "l2": "inputs (about 4 GB) larger than L2; 256 MiB flush write between steps",
+                "form": "batched, CUDA-graph captured LM loop, autotuned pixel chunking; FP32 linearisation, "
+                "FP64 block sums and Cholesky",
             },
-            "e2e": {
-                "value": e2e_value,
-                "unit": "solves/s",
-                "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h,
-                "api": "vipe_b200.ext.slam_ext.ba_extended (status word checked, one sync per call)",
-            },
-            "roofline": roof,
-            "dominant_kernel": dom[0],
-            "kernel_breakdown": breakdown,
-            "gpu_launches": int(launches_per_solve * args.steps),
+            "e2e": e2e,
+            "roofline": extras.pop("roofline"),
+            "gpu_launches": int(extras["gpu_launches_per_batch"] * n),
             "clocks": clk.summary(),
+            "batched": extras,
+            "plain_cfg1": plain,
             "corr": corr,
         }
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(p, args.cpu_sample_s)
+            line["cpu_baseline"] = cpu_baseline(args.cpu_sample_s)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
