@@ -10,9 +10,9 @@ reduced system is solved densely (torch.linalg.solve) instead of by Cholesky.
 
 Written with torch ops only, so torch.autograd differentiates the whole solve,
 including the second derivatives of the reprojection that the Jacobian formulas
-carry.  ``detach_damping`` treats the LM damping ep + lm*diag(S) as a constant
-(the convention of the CUDA adjoint); with it False the damping's dependence on
-diag(S) is differentiated as well.
+carry.  ``detach_damping`` treats the LM damping ep + lm*diag(S) as a constant;
+with it False (as the CUDA adjoint does) the damping's dependence on diag(S) is
+differentiated as well.
 
 Poses use lietorch's SE3 layout [tx ty tz qx qy qz qw] (world-to-camera), and
 tangent vectors [tau, phi]; gradients with respect to poses are taken as left

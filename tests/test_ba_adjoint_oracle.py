@@ -5,8 +5,8 @@ autograd of the torch BA against FP64 central finite differences of the C++
 oracle (h = 1e-6) on random entries of targets, weights, initial poses (left
 tangent perturbations) and initial depths, for a random-weighted loss of pose
 log-errors and depth errors.  With the damping differentiated the two agree to
-about 1e-6 relative; with the damping held constant (the CUDA adjoint's
-convention) within 1e-3.
+about 1e-6 relative; with the damping held constant within 1e-3 (the size of
+the term the CUDA adjoint therefore includes).
 """
 
 import numpy as np

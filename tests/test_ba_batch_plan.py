@@ -16,7 +16,7 @@ def _plan(nf, ne, nk, t0, t1, ht=48, wd=64, ec=0, fc=0):
     lib = _lib.load()
     h = ctypes.c_void_p()
     rc = lib.vipe_slam_ba_batch_plan_create(len(nf), _ints(nf), _ints(ne), _ints(nk), _ints(t0), _ints(t1), ht, wd,
-                                            ec, fc, ctypes.byref(h))
+                                            ec, fc, 0, ctypes.byref(h))
     return rc, h
 
 

@@ -36,7 +36,7 @@ class BatchPlan:
     """A bound plan: graph table uploaded into a device workspace on `device`."""
 
     def __init__(self, num_frames, num_edges, num_kx, t0, t1, ht: int, wd: int, device, edge_chunks: int = 0,
-                 frame_chunks: int = 0):
+                 frame_chunks: int = 0, adjoint: bool = False):
         lib = _lib.load()
         self.G = len(num_frames)
         if not (len(num_edges) == len(num_kx) == len(t0) == len(t1) == self.G) or self.G == 0:
@@ -48,10 +48,11 @@ class BatchPlan:
         self.sizes = (tuple(map(int, num_frames)), tuple(map(int, num_edges)), tuple(map(int, num_kx)),
                       tuple(map(int, t0)), tuple(map(int, t1)))
         self.edge_chunks, self.frame_chunks = int(edge_chunks), int(frame_chunks)
+        self.adjoint = bool(adjoint)
         h = ctypes.c_void_p()
         rc = lib.vipe_slam_ba_batch_plan_create(self.G, _ints(num_frames), _ints(num_edges), _ints(num_kx), _ints(t0),
                                                 _ints(t1), self.ht, self.wd, self.edge_chunks, self.frame_chunks,
-                                                ctypes.byref(h))
+                                                int(self.adjoint), ctypes.byref(h))
         _lib.check(rc, "BatchPlan")
         self._h = h
         tot = (ctypes.c_int64 * 4)()
@@ -112,14 +113,16 @@ class BatchPlan:
 
     def solve(self, poses, disps, intrinsics, disps_sens, targets, weights, eta, ii, jj, depth_active, iterations,
               lm, ep, motion_only=False, alpha=0.001, optimize_intrinsics=False, intrinsics_lm=1e-6,
-              intrinsics_ep=1e-6, intrinsics_scale=1.0, compute_energy=False, out=None, check=True):
+              intrinsics_ep=1e-6, intrinsics_scale=1.0, compute_energy=False, out=None, check=True, tape=None):
         """LM iterations on every graph; poses/disps/intrinsics are updated in place.
 
         Returns (dx, dz, energy, status): dx (sum P, 6), dz (sum K, H*W) or None,
         energy (G, iterations) or (G, 0), status (G,) int32 device words
         (0, a vipe_status error, or VIPE_WARN_SOLVER when that graph's Cholesky
         failed and its dx is 0).  ``out`` reuses preallocated outputs (for
-        CUDA-graph capture); ``check`` validates shapes on the host.
+        CUDA-graph capture); ``check`` validates shapes on the host; ``tape``
+        = (tape_poses (iterations, frames, 7), tape_disps (iterations, frames,
+        H, W)) receives the state entering each iteration (the backward's input).
         """
         if check:
             self._check(poses, disps, intrinsics, disps_sens, targets, weights, eta, ii, jj, depth_active)
@@ -133,7 +136,8 @@ class BatchPlan:
             depth_active.data_ptr(), iterations, float(lm), float(ep), int(bool(motion_only)), float(alpha),
             int(bool(optimize_intrinsics)), float(intrinsics_lm), float(intrinsics_ep), float(intrinsics_scale),
             int(bool(compute_energy)), dx.data_ptr(), _lib.ptr(dz), energy.data_ptr() if compute_energy else None,
-            status.data_ptr(), torch.cuda.current_stream(self.device).cuda_stream,
+            status.data_ptr(), None if tape is None else tape[0].data_ptr(),
+            None if tape is None else tape[1].data_ptr(), torch.cuda.current_stream(self.device).cuda_stream,
         )
         _lib.check(rc, "BatchPlan.solve")
         return dx, dz, energy, status

@@ -37,7 +37,7 @@
 // diag += ep + lm*diag, dx = 0 on Cholesky failure, the back-substitution that
 // skips rows whose pose is t0 (geom_kernels.cu:1186), retraction order.
 
-#include "common.cuh"
+#include "ba_internal.cuh"
 #include "se3_device.cuh"
 
 #include <algorithm>
@@ -47,232 +47,6 @@
 
 namespace vipe {
 namespace ba {
-
-constexpr int kMaxSlots = 32;          // window poses coupled to one depth frame
-constexpr int kMaxPoses = 127;         // t1 - t0: 6P+1 unknowns fit the staged Cholesky panel
-constexpr int kNT = 105;               // per-edge terms, see term layout below
-constexpr int kEdgeThreads = 256;
-constexpr int kFrameThreads = 256;
-constexpr int kTilesPerThread = 5;     // 4x4 SYRK tiles held in registers per thread
-constexpr int kStageFloats = 25872;    // e' staging: Dp rows x (T + 4) pixels, <= 101 KiB
-constexpr int kIndexThreads = 1024;
-
-// per-edge term layout
-//   [0,78)   upper triangle (row-major, n >= m) of the 12x12 block [Ji Jj]^T W [Ji Jj]
-//   [78,84)  vi     [84,90) vj     [90,96) fi    [96,102) fj
-//   102 hf   103 vf   104 flow energy
-constexpr int kTV = 78, kTF = 90, kTHF = 102, kTVF = 103, kTEN = 104;
-
-__host__ __device__ inline int tri12(int r, int c) { return r >= c ? r * (r + 1) / 2 + c : c * (c + 1) / 2 + r; }
-
-struct Dims {
-    int N, H, W, HW, E, K, t0, t1, P, dim;
-    int CHe, chunk_e;  // edge kernel pixel chunks
-    int CF, chunk_f;   // frame kernel pixel chunks
-    long tile_cap;     // capacity of frame SYRK tiles
-};
-
-struct Work {
-    int* status;   // [0] error code
-    int* meta;     // [0] nkx [1] sum_m [2] sum_tiles [3] max_m
-    int* flag;
-    int* rank;
-    int* kx;
-    int* fe_ptr;
-    int* fe_list;
-    int* edge_slot;
-    int* fp_ptr;
-    int* fp_list;
-    int* self_slot;
-    int* ftile_off;
-    int* pe_ptr;
-    int* pe_list;
-    int* pf_ptr;
-    int* pf_list;
-    float* epart;    // E * CHe * kNT
-    double* eterm;   // E * kNT
-    float* spart;    // tile_cap * CF * 16
-    float* fen;      // K * CF
-    float* qwf;      // K * HW * 3
-    double* Hm;      // dim * dim
-    double* bv;      // dim
-    double* df;      // 1
-    double* linv;    // inverse diagonal blocks of the Cholesky factor
-};
-
-__host__ __device__ inline int npt_of(int m) {
-    int nt = (6 * m + 2 + 3) / 4;
-    return nt * (nt + 1) / 2;
-}
-
-// che / cf: pixel-chunk counts of the per-edge and per-frame kernels; 0 picks
-// them so that one graph alone launches about two CTAs per SM.
-Dims make_dims(int N, int H, int W, int E, int K, int t0, int t1, int che = 0, int cf = 0) {
-    Dims d;
-    d.N = N; d.H = H; d.W = W; d.HW = H * W; d.E = E; d.K = K; d.t0 = t0; d.t1 = t1;
-    d.P = t1 - t0;
-    d.dim = 6 * d.P + 1;
-    const int target = 2 * 148;
-    if (che <= 0) che = E > 0 ? (target + E - 1) / E : 1;
-    che = std::max(1, std::min(che, std::max(1, d.HW / 1024)));
-    d.chunk_e = (d.HW + che - 1) / che;
-    d.CHe = (d.HW + d.chunk_e - 1) / d.chunk_e;
-    if (cf <= 0) cf = K > 0 ? (target + K - 1) / K : 1;
-    cf = std::max(1, std::min(cf, 8));
-    int chunk = (d.HW + cf - 1) / cf;
-    chunk = ((chunk + 255) / 256) * 256;
-    d.chunk_f = chunk;
-    d.CF = (d.HW + chunk - 1) / chunk;
-    // Upper bound of sum over frames of npt(m_s): slots are <= kMaxSlots per
-    // frame and sum_s m_s <= E + K.  npt(m) <= (1.5 m + 3.25)^2 / 2.
-    const int M = std::max(1, std::min(kMaxSlots, d.P));
-    double b1 = (double)K * npt_of(M);
-    double b2 = (1.5 * M + 3.25) / 2.0 * (1.5 * (double)(E + K) + 3.25 * K);
-    d.tile_cap = (long)std::min(b1, b2) + K + 1;
-    return d;
-}
-
-template <typename C>
-void carve(C& c, const Dims& d, Work* w) {
-    const size_t N = d.N, E = d.E, K = d.K, P = d.P;
-    auto take_i = [&](int*& dst, size_t n) {
-        auto p = c.template take<int>(n);
-        if (w) dst = (int*)p;
-    };
-    int* dummy;
-    take_i(w ? w->status : dummy, 4);
-    take_i(w ? w->meta : dummy, 8);
-    take_i(w ? w->flag : dummy, N);
-    take_i(w ? w->rank : dummy, N);
-    take_i(w ? w->kx : dummy, N);
-    take_i(w ? w->fe_ptr : dummy, K + 1);
-    take_i(w ? w->fe_list : dummy, E + 1);
-    take_i(w ? w->edge_slot : dummy, E + 1);
-    take_i(w ? w->fp_ptr : dummy, K + 1);
-    take_i(w ? w->fp_list : dummy, E + K + 1);
-    take_i(w ? w->self_slot : dummy, K + 1);
-    take_i(w ? w->ftile_off : dummy, K + 1);
-    take_i(w ? w->pe_ptr : dummy, P + 1);
-    take_i(w ? w->pe_list : dummy, 2 * E + 1);
-    take_i(w ? w->pf_ptr : dummy, P + 1);
-    take_i(w ? w->pf_list : dummy, E + K + 1);
-    auto pf = c.template take<float>((size_t)std::max<size_t>(1, E) * d.CHe * 36);
-    auto pd = c.template take<double>((size_t)std::max<size_t>(1, E) * kNT);
-    auto ps = c.template take<float>((size_t)d.tile_cap * d.CF * 16);
-    auto pen = c.template take<float>(K * d.CF + 1);
-    auto pq = c.template take<float>(K * (size_t)d.HW * 3);
-    auto pH = c.template take<double>((size_t)d.dim * d.dim);
-    auto pb = c.template take<double>((size_t)d.dim);
-    auto pdf = c.template take<double>(4);
-    auto pli = c.template take<double>((size_t)((d.dim + 31) / 32) * 32 * 32);
-    if (w) {
-        w->epart = (float*)pf;
-        w->eterm = (double*)pd;
-        w->spart = (float*)ps;
-        w->fen = (float*)pen;
-        w->qwf = (float*)pq;
-        w->Hm = (double*)pH;
-        w->bv = (double*)pb;
-        w->df = (double*)pdf;
-        w->linv = (double*)pli;
-    }
-}
-
-// ---------------------------------------------------------------- graph table
-//
-// Every kernel runs over a table of graphs.  A single solve is a table of one;
-// a batch places many clips' graphs side by side: inputs are concatenated
-// along their leading axis (frames, edges, depth rows, window poses) and each
-// graph's descriptor holds its sizes, its carve of the workspace and its
-// offsets into the concatenated tensors.  Edge indices stay local to their
-// graph.  A launch over the batch is one flat grid: per kernel, boff[g] is the
-// first block of graph g (boff[G] = total), found by binary search.
-
-struct BAPtrs {
-    float* poses;              // (frames, 7)
-    float* disps;              // (frames, H, W)
-    float* intr;               // (graphs, 4)
-    const float* disps_sens;   // (frames, H, W)
-    const float* targets;      // (edges, 2, H, W)
-    const float* weights;      // (edges, 2, H, W)
-    const float* eta;          // (depth rows, H, W)
-    const int64_t* ii;         // (edges,) local frame index
-    const int64_t* jj;
-    const float* depth_active; // (frames,)
-    float* dx;                 // (window poses, 6)
-    float* dz;                 // (depth rows, H*W)
-    float* energy;             // (graphs, energy_stride)
-    int32_t* status;           // device status word(s): graph g uses status[g * status_stride]
-    int energy_stride;
-    int status_stride;
-};
-
-struct GraphDesc {
-    Dims d;
-    Work w;
-    long frame_off, edge_off, kx_off, pose_off;
-    int g;
-};
-
-struct Batch {
-    const GraphDesc* gds;  // device table
-    const int* boff;       // per-kernel block offsets, or nullptr (see locate)
-    int G;
-};
-
-// Graph of this block.  With boff: flat grid over all graphs.  Without: a
-// single graph (G == 1, local = blockIdx.x) or one block per graph (g = blockIdx.x).
-__device__ __forceinline__ int locate(const Batch& B, int& local) {
-    if (B.boff == nullptr) {
-        if (B.G == 1) {
-            local = blockIdx.x;
-            return 0;
-        }
-        local = 0;
-        return blockIdx.x;
-    }
-    const int x = blockIdx.x;
-    int lo = 0, hi = B.G;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(B.boff + mid) <= x) lo = mid; else hi = mid;
-    }
-    local = x - __ldg(B.boff + lo);
-    return lo;
-}
-
-__device__ __forceinline__ BAPtrs rebase(const BAPtrs& b, const GraphDesc& g) {
-    const long HW = g.d.HW;
-    BAPtrs p;
-    p.poses = b.poses + g.frame_off * 7;
-    p.disps = b.disps + g.frame_off * HW;
-    p.intr = b.intr + (long)g.g * 4;
-    p.disps_sens = b.disps_sens + g.frame_off * HW;
-    p.targets = b.targets ? b.targets + g.edge_off * 2 * HW : nullptr;
-    p.weights = b.weights ? b.weights + g.edge_off * 2 * HW : nullptr;
-    p.eta = b.eta + g.kx_off * HW;
-    p.ii = b.ii ? b.ii + g.edge_off : nullptr;
-    p.jj = b.jj ? b.jj + g.edge_off : nullptr;
-    p.depth_active = b.depth_active + g.frame_off;
-    p.dx = b.dx + g.pose_off * 6;
-    p.dz = b.dz ? b.dz + g.kx_off * HW : nullptr;
-    p.energy = b.energy ? b.energy + (long)g.g * b.energy_stride : nullptr;
-    p.status = b.status ? b.status + (long)g.g * b.status_stride : nullptr;
-    p.energy_stride = b.energy_stride;
-    p.status_stride = b.status_stride;
-    return p;
-}
-
-// binds d, w, P (rebased pointers) and local_ (block index within the graph)
-#define BA_BIND(B, base)                                \
-    int local_;                                         \
-    const int g_ = locate(B, local_);                   \
-    const GraphDesc* __restrict__ gd_ = (B).gds + g_;   \
-    const Dims d = gd_->d;                              \
-    const Work w = gd_->w;                              \
-    const BAPtrs io = rebase(base, *gd_);                \
-    (void)io;                                           \
-    (void)d;
 
 // ---------------------------------------------------------------- index build
 
@@ -569,27 +343,6 @@ __global__ void __launch_bounds__(kIndexThreads)
 
 // ---------------------------------------------------------------- per-edge terms
 
-struct EdgeArgs {
-    const float* poses;
-    const float* disps;
-    const float* intr;
-    const float* targets;
-    const float* weights;
-    const int64_t* ii;
-    const int64_t* jj;
-    float iscale;
-};
-
-// Per-pixel accumulation needs only the target-pose block: the source-pose
-// Jacobian of every pixel is Ji = -M Jj with M = Ad^T(Tij) constant per edge
-// (the adjoint pull-back used by the reference, geom_kernels.cu:88-102), so
-//   Hii = M Hjj M^T,  Hij = -M Hjj,  vi = -M vj,  fi = -M fj.
-// Chunk partial layout (kNE floats): [0,21) Hjj upper triangle (n >= m),
-// [21,27) vj, [27,33) fj, 33 hf, 34 vf, 35 flow energy.
-constexpr int kNE = 36;
-
-__host__ __device__ inline int tri6(int r, int c) { return r >= c ? r * (r + 1) / 2 + c : c * (c + 1) / 2 + r; }
-
 template <bool kIntr>
 __global__ void __launch_bounds__(kEdgeThreads) ba_edge_kernel(BAPtrs base, Batch B, float iscale) {
     BA_BIND(B, base);
@@ -738,20 +491,6 @@ __global__ void ba_edge_reduce(BAPtrs base, Batch B) {
 }
 
 // ---------------------------------------------------------------- per-frame Schur
-
-struct FrameArgs {
-    const float* poses;
-    const float* disps;
-    const float* disps_sens;
-    const float* intr;
-    const float* targets;
-    const float* weights;
-    const float* eta;
-    const float* depth_active;
-    const int64_t* jj;
-    float alpha;
-    float iscale;
-};
 
 __device__ __forceinline__ void decode_tile(int tau, int nt, int& ti, int& tj) {
     int r = 0, rem = tau;
@@ -1061,10 +800,6 @@ __global__ void ba_assemble_rhs(BAPtrs base, Batch B, int with_frames, int with_
 
 // ---------------------------------------------------------------- dense FP64 Cholesky
 
-constexpr int kCholThreads = 512;
-constexpr int kNB = 32;
-constexpr int kPanelRows = 768;  // systems up to 768 unknowns stage their panel in shared memory
-
 __device__ __forceinline__ double damped(double dg, bool scalar, float lm, float ep, float ilm, float iep) {
     return dg + (scalar ? ((double)iep + (double)ilm * dg) : ((double)ep + (double)lm * dg));
 }
@@ -1083,15 +818,6 @@ __device__ __forceinline__ double damped(double dg, bool scalar, float lm, float
 // The inverse diagonal blocks are kept (Linv) for the backward substitution.
 // On a non-positive pivot x = 0 and VIPE_WARN_SOLVER is raised, as the
 // reference falls back to dx = 0 (geom_kernels.cu:1283-1285).
-__host__ __device__ inline int chol_ldr(int dim) {
-    // transposed panel row length: >= max(dim, 32) + 4 (tiles read up to 3 rows
-    // past the last panel row, which are zero-filled), == 2 (mod 4) doubles so
-    // that 16-byte row-pair loads stay aligned
-    int r = (dim < kNB ? kNB : dim) + 4;
-    r = (r + 3) & ~3;
-    return r + 2;
-}
-
 __global__ void __launch_bounds__(kCholThreads, 1)
     ba_cholesky_kernel(BAPtrs base, Batch B, float lm, float ep, float ilm, float iep, int with_intr) {
     BA_BIND(B, base);
@@ -1310,8 +1036,65 @@ __global__ void __launch_bounds__(kCholThreads, 1)
     for (int i = tid; i < np; i += kCholThreads) dx_out[i] = fail ? 0.f : (float)x[i];
     if (tid == 0) {
         w.df[0] = (fail || !with_intr) ? 0.0 : x[np];
+        w.meta[4] = fail;
         if (fail && io.status) atomicOr(io.status, VIPE_WARN_SOLVER);
     }
+}
+
+// Second solve with the factor the Cholesky kernel left in Hm (L in the lower
+// triangle) and linv (inverse diagonal blocks): adj_lam = S'^-1 adj_rhs over the
+// 6P pose unknowns; zero when the factorisation failed (the forward step was
+// dx = 0 then).  One CTA per graph.
+__global__ void __launch_bounds__(kCholThreads) ba_chol_resolve_kernel(BAPtrs base, Batch B) {
+    BA_BIND(B, base);
+    if (w.status[0]) return;
+    __shared__ double xs[kPanelRows];
+    __shared__ double ysh[kNB];
+    const int tid = threadIdx.x;
+    const int n = 6 * d.P, ld = d.dim;
+    const double* A = w.Hm;
+    const double* Linv = w.linv;
+    const bool fail = w.meta[4] != 0;
+    for (int i = tid; i < n; i += kCholThreads) xs[i] = fail ? 0.0 : w.adj_rhs[i];
+    __syncthreads();
+    if (!fail) {
+        const int nblk = (n + kNB - 1) / kNB;
+        for (int kb = 0; kb < nblk; kb++) {  // L y = b
+            const int k0 = kb * kNB, kn = min(kNB, n - k0);
+            if (tid < kNB) {
+                double acc = 0.0;
+                if (tid < kn)
+                    for (int t = 0; t <= tid; t++) acc += Linv[(size_t)kb * kNB * kNB + tid * kNB + t] * xs[k0 + t];
+                ysh[tid] = acc;
+            }
+            __syncthreads();
+            if (tid < kn) xs[k0 + tid] = ysh[tid];
+            for (int r = k0 + kn + tid; r < n; r += kCholThreads) {
+                double acc = 0.0;
+                for (int t = 0; t < kn; t++) acc += A[(size_t)r * ld + k0 + t] * ysh[t];
+                xs[r] -= acc;
+            }
+            __syncthreads();
+        }
+        for (int kb = nblk - 1; kb >= 0; kb--) {  // L^T x = y
+            const int k0 = kb * kNB, kn = min(kNB, n - k0);
+            if (tid < kNB) {
+                double acc = 0.0;
+                if (tid < kn)
+                    for (int t = tid; t < kn; t++) acc += Linv[(size_t)kb * kNB * kNB + t * kNB + tid] * xs[k0 + t];
+                ysh[tid] = acc;
+            }
+            __syncthreads();
+            if (tid < kn) xs[k0 + tid] = ysh[tid];
+            for (int i = tid; i < k0; i += kCholThreads) {
+                double acc = 0.0;
+                for (int t = 0; t < kn; t++) acc += A[(size_t)(k0 + t) * ld + i] * ysh[t];
+                xs[i] -= acc;
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = tid; i < n; i += kCholThreads) w.adj_lam[i] = xs[i];
 }
 
 // ---------------------------------------------------------------- back substitution
@@ -1453,118 +1236,134 @@ int ensure_attributes() {
     return VIPE_OK;
 }
 
-// Launch geometry of a table of graphs: per kernel, the flat block count of
-// each graph and their running offsets (uploaded as Batch::boff for batches).
-enum { kOffEdge = 0, kOffEdgeRed, kOffFrame, kOffPairs, kOffRhs, kOffRetr, kNumOff };
-
-struct Geometry {
-    int G = 0;
-    std::vector<int> off[kNumOff];  // G + 1 entries each
-    size_t chol_smem = 0;
-    bool any_edges = false;
-};
-
-void fill_geometry(const std::vector<Dims>& dims, Geometry& geo) {
-    geo.G = (int)dims.size();
-    for (int k = 0; k < kNumOff; k++) geo.off[k].assign(geo.G + 1, 0);
-    for (int g = 0; g < geo.G; g++) {
-        const Dims& d = dims[g];
-        const long npairs = (long)d.P * (d.P + 1) / 2;
-        const int cnt[kNumOff] = {d.E * d.CHe, d.E, d.K * d.CF, (int)ceil_div(npairs, 8), (int)ceil_div(d.P + 1, 8),
-                                  (int)ceil_div(d.P, 128)};
-        for (int k = 0; k < kNumOff; k++) geo.off[k][g + 1] = geo.off[k][g] + cnt[k];
-        geo.chol_smem = std::max(geo.chol_smem, (size_t)chol_ldr(d.dim) * kNB * sizeof(double));
-        geo.any_edges |= d.E > 0;
-    }
+// Launch helpers.  `d_off` == nullptr: a single graph whose descriptor the
+// index kernel stores from `init` (later kernels read it back from d_table[0]).
+// Each helper only enqueues kernels: no allocation, copy or synchronisation,
+// so a whole solve can be captured into a CUDA graph.
+static Batch batch_of(const Geometry& geo, const GraphDesc* d_table, const int* d_off, int k) {
+    return Batch{d_table, d_off ? d_off + (size_t)k * (geo.G + 1) : nullptr, geo.G};
 }
 
-struct SolveArgs {
-    int iterations;
-    float lm, ep, alpha;
-    int motion_only, intr;
-    float ilm, iep, iscale;
-    int compute_energy;
-};
-
-// Enqueues the index build and `iterations` LM steps for every graph of the
-// table.  single: one graph whose descriptor `init` the index kernel stores;
-// otherwise the table and the offsets are already on the device.  Launches
-// only: no allocation, copy or synchronisation, so the sequence can be
-// captured into a CUDA graph.
-int run_solve(const Geometry& geo, const GraphDesc* d_table, const int* d_off, const BAPtrs& base,
-              const GraphDesc* init, const SolveArgs& a, cudaStream_t st) {
-    const bool single = init != nullptr;
-    const int G = geo.G;
-    auto batch = [&](int k) { return Batch{d_table, single ? nullptr : d_off + (size_t)k * (G + 1), G}; };
-    const Batch per_graph{d_table, nullptr, G};
-    auto grid = [&](int k) { return (unsigned)geo.off[k][G]; };
+int launch_index(const Geometry& geo, const GraphDesc* d_table, const BAPtrs& base, const GraphDesc* init,
+                 cudaStream_t st) {
+    const Batch per_graph{d_table, nullptr, geo.G};
     {
         VIPE_PROF("ba_index", st);
-        ba_index_kernel<<<G, kIndexThreads, 0, st>>>(base, per_graph, single ? *init : GraphDesc{}, single ? 1 : 0);
+        ba_index_kernel<<<geo.G, kIndexThreads, 0, st>>>(base, per_graph, init ? *init : GraphDesc{}, init ? 1 : 0);
     }
     VIPE_LAUNCH_CHECK();
+    return VIPE_OK;
+}
+
+int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const int* d_off, const BAPtrs& base,
+                           const SolveArgs& a, int itr, cudaStream_t st) {
+    const int G = geo.G;
+    const Batch per_graph{d_table, nullptr, G};
+    auto grid = [&](int k) { return (unsigned)geo.off[k][G]; };
     const bool intr = a.intr != 0;
     const int with_frames = a.motion_only ? 0 : 1;
-    for (int itr = 0; itr < a.iterations; itr++) {
-        if (geo.any_edges) {
-            {
-                VIPE_PROF("ba_edge", st);
-                if (intr)
-                    ba_edge_kernel<true><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(base, batch(kOffEdge), a.iscale);
-                else
-                    ba_edge_kernel<false><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(base, batch(kOffEdge), a.iscale);
-            }
-            VIPE_LAUNCH_CHECK();
-            {
-                VIPE_PROF("ba_edge_reduce", st);
-                ba_edge_reduce<<<grid(kOffEdgeRed), 128, 0, st>>>(base, batch(kOffEdgeRed));
-            }
-            VIPE_LAUNCH_CHECK();
-        }
-        if (with_frames && grid(kOffFrame) > 0) {
-            VIPE_PROF("ba_frame", st);
-            if (intr)
-                ba_frame_kernel<true><<<grid(kOffFrame), kFrameThreads, kStageFloats * 4, st>>>(
-                    base, batch(kOffFrame), a.alpha, a.iscale);
-            else
-                ba_frame_kernel<false><<<grid(kOffFrame), kFrameThreads, kStageFloats * 4, st>>>(
-                    base, batch(kOffFrame), a.alpha, a.iscale);
-            VIPE_LAUNCH_CHECK();
-        }
+    if (geo.any_edges) {
         {
-            VIPE_PROF("ba_assemble", st);
-            ba_assemble_blocks<<<grid(kOffPairs), 256, 0, st>>>(base, batch(kOffPairs), with_frames);
-            VIPE_LAUNCH_CHECK();
-            ba_assemble_rhs<<<grid(kOffRhs), 256, 0, st>>>(base, batch(kOffRhs), with_frames, intr ? 1 : 0);
+            VIPE_PROF("ba_edge", st);
+            if (intr)
+                ba_edge_kernel<true><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(
+                    base, batch_of(geo, d_table, d_off, kOffEdge), a.iscale);
+            else
+                ba_edge_kernel<false><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(
+                    base, batch_of(geo, d_table, d_off, kOffEdge), a.iscale);
         }
         VIPE_LAUNCH_CHECK();
-        if (a.compute_energy) {
-            VIPE_PROF("ba_energy", st);
-            ba_energy_kernel<<<G, 256, 0, st>>>(base, per_graph, with_frames, itr);
-            VIPE_LAUNCH_CHECK();
-        }
         {
-            VIPE_PROF("ba_cholesky", st);
-            ba_cholesky_kernel<<<G, kCholThreads, geo.chol_smem, st>>>(base, per_graph, a.lm, a.ep, a.ilm, a.iep,
-                                                                       intr ? 1 : 0);
-        }
-        VIPE_LAUNCH_CHECK();
-        if (with_frames && grid(kOffFrame) > 0) {
-            VIPE_PROF("ba_backsub", st);
-            if (intr)
-                ba_backsub_kernel<true><<<grid(kOffFrame), 256, 0, st>>>(base, batch(kOffFrame));
-            else
-                ba_backsub_kernel<false><<<grid(kOffFrame), 256, 0, st>>>(base, batch(kOffFrame));
-            VIPE_LAUNCH_CHECK();
-        }
-        {
-            VIPE_PROF("ba_retract", st);
-            ba_retract_kernel<<<grid(kOffRetr), 128, 0, st>>>(base, batch(kOffRetr), intr ? 1 : 0, a.iscale);
+            VIPE_PROF("ba_edge_reduce", st);
+            ba_edge_reduce<<<grid(kOffEdgeRed), 128, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffEdgeRed));
         }
         VIPE_LAUNCH_CHECK();
     }
+    if (with_frames && grid(kOffFrame) > 0) {
+        VIPE_PROF("ba_frame", st);
+        if (intr)
+            ba_frame_kernel<true><<<grid(kOffFrame), kFrameThreads, kStageFloats * 4, st>>>(
+                base, batch_of(geo, d_table, d_off, kOffFrame), a.alpha, a.iscale);
+        else
+            ba_frame_kernel<false><<<grid(kOffFrame), kFrameThreads, kStageFloats * 4, st>>>(
+                base, batch_of(geo, d_table, d_off, kOffFrame), a.alpha, a.iscale);
+        VIPE_LAUNCH_CHECK();
+    }
+    {
+        VIPE_PROF("ba_assemble", st);
+        ba_assemble_blocks<<<grid(kOffPairs), 256, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffPairs),
+                                                             with_frames);
+        VIPE_LAUNCH_CHECK();
+        ba_assemble_rhs<<<grid(kOffRhs), 256, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffRhs), with_frames,
+                                                       intr ? 1 : 0);
+    }
+    VIPE_LAUNCH_CHECK();
+    if (a.compute_energy) {
+        VIPE_PROF("ba_energy", st);
+        ba_energy_kernel<<<G, 256, 0, st>>>(base, per_graph, with_frames, itr);
+        VIPE_LAUNCH_CHECK();
+    }
+    {
+        VIPE_PROF("ba_cholesky", st);
+        ba_cholesky_kernel<<<G, kCholThreads, geo.chol_smem, st>>>(base, per_graph, a.lm, a.ep, a.ilm, a.iep,
+                                                                   intr ? 1 : 0);
+    }
+    VIPE_LAUNCH_CHECK();
+    return VIPE_OK;
+}
+
+int launch_chol_resolve(const Geometry& geo, const GraphDesc* d_table, const BAPtrs& base, cudaStream_t st) {
+    {
+        VIPE_PROF("ba_chol_resolve", st);
+        ba_chol_resolve_kernel<<<geo.G, kCholThreads, 0, st>>>(base, Batch{d_table, nullptr, geo.G});
+    }
+    VIPE_LAUNCH_CHECK();
+    return VIPE_OK;
+}
+
+static int launch_update(const Geometry& geo, const GraphDesc* d_table, const int* d_off, const BAPtrs& base,
+                         const SolveArgs& a, cudaStream_t st) {
+    const int G = geo.G;
+    auto grid = [&](int k) { return (unsigned)geo.off[k][G]; };
+    const bool intr = a.intr != 0;
+    if (!a.motion_only && grid(kOffFrame) > 0) {
+        VIPE_PROF("ba_backsub", st);
+        if (intr)
+            ba_backsub_kernel<true><<<grid(kOffFrame), 256, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffFrame));
+        else
+            ba_backsub_kernel<false><<<grid(kOffFrame), 256, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffFrame));
+        VIPE_LAUNCH_CHECK();
+    }
+    {
+        VIPE_PROF("ba_retract", st);
+        ba_retract_kernel<<<grid(kOffRetr), 128, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffRetr),
+                                                         intr ? 1 : 0, a.iscale);
+    }
+    VIPE_LAUNCH_CHECK();
+    return VIPE_OK;
+}
+
+// Enqueues the index build and `iterations` LM steps for every graph of the
+// table.  With a tape, the state (poses, disps) entering iteration k is first
+// copied to tape_poses + k * frames * 7 and tape_disps + k * frames * H * W
+// (device-to-device copies, capturable like the kernels).
+int run_solve(const Geometry& geo, const GraphDesc* d_table, const int* d_off, const BAPtrs& base,
+              const GraphDesc* init, const SolveArgs& a, cudaStream_t st, float* tape_poses = nullptr,
+              float* tape_disps = nullptr, long tape_frames = 0, long hw = 0) {
+    int rc = launch_index(geo, d_table, base, init, st);
+    if (rc != VIPE_OK) return rc;
+    for (int itr = 0; itr < a.iterations; itr++) {
+        if (tape_poses) {
+            VIPE_CUDA_TRY(cudaMemcpyAsync(tape_poses + (size_t)itr * tape_frames * 7, base.poses,
+                                          sizeof(float) * tape_frames * 7, cudaMemcpyDeviceToDevice, st));
+            VIPE_CUDA_TRY(cudaMemcpyAsync(tape_disps + (size_t)itr * tape_frames * hw, base.disps,
+                                          sizeof(float) * tape_frames * hw, cudaMemcpyDeviceToDevice, st));
+        }
+        if ((rc = launch_linearize_solve(geo, d_table, d_off, base, a, itr, st)) != VIPE_OK) return rc;
+        if ((rc = launch_update(geo, d_table, d_off, base, a, st)) != VIPE_OK) return rc;
+    }
     if (base.status) {
-        ba_status_kernel<<<G, 1, 0, st>>>(base, per_graph);
+        ba_status_kernel<<<geo.G, 1, 0, st>>>(base, Batch{d_table, nullptr, geo.G});
         VIPE_LAUNCH_CHECK();
     }
     return VIPE_OK;
@@ -1593,18 +1392,6 @@ void carve_batch(C& c, std::vector<GraphDesc>& gds, GraphDesc** table, int** off
 using namespace vipe;
 using namespace vipe::ba;
 
-// Host-side plan of a batch of graphs (opaque to C callers).
-struct vipe_ba_batch_plan {
-    int G = 0;
-    std::vector<GraphDesc> gds;  // Work pointers valid once bound
-    Geometry geo;
-    size_t bytes = 0;
-    long frames = 0, edges = 0, kx = 0, poses = 0;
-    void* ws = nullptr;  // workspace the table was uploaded to
-    GraphDesc* d_table = nullptr;
-    int* d_off = nullptr;
-    std::vector<int> off_host;  // kNumOff x (G + 1), the image of d_off
-};
 
 extern "C" size_t vipe_slam_ba_workspace_size(int num_frames, int ht, int wd, int num_edges, int num_kx, int t0,
                                               int t1) {
@@ -1662,7 +1449,8 @@ extern "C" int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* in
 
 extern "C" int vipe_slam_ba_batch_plan_create(int num_graphs, const int* num_frames, const int* num_edges,
                                               const int* num_kx, const int* t0, const int* t1, int ht, int wd,
-                                              int edge_chunks, int frame_chunks, vipe_ba_batch_plan** plan_out) {
+                                              int edge_chunks, int frame_chunks, int with_adjoint,
+                                              vipe_ba_batch_plan** plan_out) {
     if (!plan_out) return VIPE_ERR_ARG;
     *plan_out = nullptr;
     if (num_graphs <= 0 || !num_frames || !num_edges || !num_kx || !t0 || !t1) return VIPE_ERR_ARG;
@@ -1683,15 +1471,22 @@ extern "C" int vipe_slam_ba_batch_plan_create(int num_graphs, const int* num_fra
     // about two CTAs per SM; large batches therefore run unchunked.
     const int target = 2 * 148;
     const int che = edge_chunks > 0 ? edge_chunks : (sumE > 0 ? (int)std::max<long>(1, (target + sumE - 1) / sumE) : 1);
-    const int cf = frame_chunks > 0 ? frame_chunks : (int)std::max<long>(1, (target + sumK - 1) / sumK);
+    int cf = frame_chunks > 0 ? frame_chunks : (int)std::max<long>(1, (target + sumK - 1) / sumK);
+    // the adjoint keeps a few floats per pixel of a (frame, chunk) block in
+    // shared memory: at most 3072 pixels per chunk
+    if (with_adjoint) cf = std::max(cf, (ht * wd + 3071) / 3072);
     auto* plan = new vipe_ba_batch_plan();
     plan->G = num_graphs;
+    plan->adjoint = with_adjoint ? 1 : 0;
+    plan->ht = ht;
+    plan->wd = wd;
     plan->gds.resize(num_graphs);
     std::vector<Dims> dims(num_graphs);
     for (int g = 0; g < num_graphs; g++) {
         GraphDesc& gd = plan->gds[g];
         gd = GraphDesc{};
         gd.d = make_dims(num_frames[g], ht, wd, num_edges[g], num_kx[g], t0[g], t1[g], che, cf);
+        gd.d.adj = plan->adjoint;
         gd.frame_off = plan->frames;
         gd.edge_off = plan->edges;
         gd.kx_off = plan->kx;
@@ -1762,8 +1557,9 @@ extern "C" int vipe_slam_ba_batch_solve(const vipe_ba_batch_plan* plan, float* p
                                         int motion_only, float alpha, int optimize_intrinsics, float intrinsics_lm,
                                         float intrinsics_ep, float intrinsics_scale, int compute_energy,
                                         float* dx_out, float* dz_out, float* energy_out, int32_t* dev_status,
-                                        void* stream) {
+                                        float* tape_poses, float* tape_disps, void* stream) {
     if (!plan) return VIPE_ERR_ARG;
+    if ((tape_poses == nullptr) != (tape_disps == nullptr)) return VIPE_ERR_ARG;
     if (!plan->d_table) {
         set_last_error("vipe_slam_ba_batch_solve: plan is not bound to a workspace");
         return VIPE_ERR_WORKSPACE;
@@ -1776,7 +1572,8 @@ extern "C" int vipe_slam_ba_batch_solve(const vipe_ba_batch_plan* plan, float* p
                 iterations, 1};
     SolveArgs a{iterations, lm, ep, alpha, motion_only, optimize_intrinsics, intrinsics_lm, intrinsics_ep,
                 intrinsics_scale, compute_energy};
-    return run_solve(plan->geo, plan->d_table, plan->d_off, base, nullptr, a, as_stream(stream));
+    return run_solve(plan->geo, plan->d_table, plan->d_off, base, nullptr, a, as_stream(stream), tape_poses,
+                     tape_disps, plan->frames, (long)plan->ht * plan->wd);
 }
 
 extern "C" void vipe_slam_ba_batch_plan_destroy(vipe_ba_batch_plan* plan) { delete plan; }

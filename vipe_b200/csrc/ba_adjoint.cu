@@ -1,0 +1,894 @@
+// Hand-written adjoint of the dense bundle adjustment (no counterpart in the
+// reference, which has no BA backward: vipe csrc/slam_ext/slam.cpp binds only
+// forward entry points).
+//
+// The forward LM step at state x_k = (poses T, inverse depths d) is
+//   y   = v - E Q w_z,      S' = B - E Q E^T + D,     S' dxi = y,
+//   dz  = Q (w_z - E~^T dxi)                 (E~: E without pose t0's rows,
+//                                             the reference's back-substitution,
+//                                             geom_kernels.cu:1186)
+//   T  <- Exp(dxi) T,   d <- d + dz,
+// with B, v, E, C = 1/Q, w_z sums over edge pixels of the reprojection
+// Jacobians (geom_kernels.cu:178-524) and D = ep + lm diag(S) the LM damping.
+// Going backwards through the iterations (states re-read from the forward's
+// tape, Jacobians recomputed, never stored):
+//
+//   g_dxi = J_l(dxi)^T g_T,   g_T <- Ad(Exp dxi)^T g_T          (retraction)
+//   a     = Q g_dz                                               (g_dz = g_d)
+//   lam   = S'^-1 (g_dxi - E~ a)          (the same reduced system, re-solved)
+//   mu    = Q E^T lam,  dzf = Q (w_z - E^T dxi),  L = lm lam o dxi (damping)
+//   g_wz  = a - mu,     g_C = mu dzf - a dz - Q^2 sum_a L_a E_a^2,
+//   g_E   = -dzf lam + mu dxi - a dxi~ + 2 Q L o E,
+//   g_v   = lam,        g_B = -lam dxi^T - diag(L)
+//
+// Every remaining dependence is a sum over (edge, pixel) of a scalar phi of the
+// Jacobian rows J_c, the depth Jacobian Jz_c and the residual r_c, with the
+// adjoint quantities held fixed; its gradient gives the targets and weights
+// directly, and with respect to the two poses and the pixel's depth it needs the
+// derivatives of Jacobian-vector products J.v.  Those are taken exactly: the
+// transformed point is X' = Tij X with X = (x, y, 1, d); a left perturbation
+// s A of the target pose (s B of the source pose) moves it by Ps = A X'
+// (-Tij B X), and J.v along a tangent v = (v_i, v_j) is grad f . (v_j X' -
+// Tij v_i X).  Their mixed derivative splits, for every direction v, into
+//   Ps . (h_v + grad f x v_j,phi) + e_phi . [target: -(Y_v x grad f); source: R^T (Y_v x grad f)]
+// with Y_v = R (v_i,tau d + v_i,phi x X3) and h_v from the projection's second
+// derivative.  So per edge the pixels only accumulate G0 = sum g X^T (3x4) and
+// one 3-vector for the rotation dofs, contracted with Ps per pose direction
+// once per edge; the per-pixel directions of the damping terms fit the same form.
+
+// Precision: the per-pixel work is FP32 like the forward; the re-solve and every
+// pose-level sum are FP64.
+
+#include "ba_internal.cuh"
+#include "se3_device.cuh"
+
+namespace vipe {
+namespace ba {
+
+constexpr int kAdjThreads = 256;
+constexpr int kAdjMaxDeg = 64;       // edges leaving one depth frame
+constexpr int kAdjMaxChunk = 3072;   // pixels of one (frame, chunk) block
+
+// ---------------------------------------------------------------- small helpers
+
+__device__ __forceinline__ void cross3(const double* a, const double* b, double* c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// v <- ad(xi)^T v for xi = (tau, phi): (-phi x v_tau, -tau x v_tau - phi x v_phi)
+__device__ __forceinline__ void adT_apply(const double* xi, double* v) {
+    double a[3], b[3], c[3];
+    cross3(xi + 3, v, a);
+    cross3(xi, v, b);
+    cross3(xi + 3, v + 3, c);
+    for (int n = 0; n < 3; n++) {
+        v[n] = -a[n];
+        v[3 + n] = -b[n] - c[n];
+    }
+}
+
+// 4x4 homogeneous matrices (row-major, double)
+struct M4 {
+    double m[16];
+};
+
+__device__ __forceinline__ M4 mzero() {
+    M4 z;
+    for (int q = 0; q < 16; q++) z.m[q] = 0.0;
+    return z;
+}
+
+__device__ __forceinline__ M4 mmul(const M4& a, const M4& b) {
+    M4 c;
+    for (int r = 0; r < 4; r++)
+        for (int k = 0; k < 4; k++) {
+            double s = 0.0;
+            for (int j = 0; j < 4; j++) s += a.m[4 * r + j] * b.m[4 * j + k];
+            c.m[4 * r + k] = s;
+        }
+    return c;
+}
+
+__device__ __forceinline__ M4 madd(const M4& a, const M4& b, double sb) {
+    M4 c;
+    for (int q = 0; q < 16; q++) c.m[q] = a.m[q] + sb * b.m[q];
+    return c;
+}
+
+// se3 generator of xi = (tau, phi): [[phi x, tau], [0, 0]]
+__device__ __forceinline__ M4 hat(const double* xi) {
+    M4 h = mzero();
+    h.m[1] = -xi[5];
+    h.m[2] = xi[4];
+    h.m[4] = xi[5];
+    h.m[6] = -xi[3];
+    h.m[8] = -xi[4];
+    h.m[9] = xi[3];
+    h.m[3] = xi[0];
+    h.m[7] = xi[1];
+    h.m[11] = xi[2];
+    return h;
+}
+
+__device__ __forceinline__ void quat_to_rot(const double* q, double* R) {
+    const double x = q[0], y = q[1], z = q[2], w = q[3];
+    R[0] = 1 - 2 * (y * y + z * z);
+    R[1] = 2 * (x * y - w * z);
+    R[2] = 2 * (x * z + w * y);
+    R[3] = 2 * (x * y + w * z);
+    R[4] = 1 - 2 * (x * x + z * z);
+    R[5] = 2 * (y * z - w * x);
+    R[6] = 2 * (x * z - w * y);
+    R[7] = 2 * (y * z + w * x);
+    R[8] = 1 - 2 * (x * x + y * y);
+}
+
+// Tij = Tj Ti^-1 as a 4x4 (stereo edges: the fixed baseline (-0.1, 0, 0))
+__device__ M4 edge_matrix(const float* poses, int a, int b) {
+    float tij[3], qij[4];
+    edge_pose(poses, a, b, tij, qij);
+    const double q[4] = {qij[0], qij[1], qij[2], qij[3]};
+    double R[9];
+    quat_to_rot(q, R);
+    M4 T;
+    for (int r = 0; r < 3; r++) {
+        for (int c = 0; c < 3; c++) T.m[4 * r + c] = R[3 * r + c];
+        T.m[4 * r + 3] = tij[r];
+    }
+    T.m[12] = T.m[13] = T.m[14] = 0.0;
+    T.m[15] = 1.0;
+    return T;
+}
+
+// the edge's 12-vector [source pose, target pose] of a window-pose field (zero
+// for poses outside the window; drop_t0 also zeroes pose t0)
+template <typename Tin>
+__device__ __forceinline__ void edge_dir(const Tin* field, int ia, int ib, int t0, int P, bool drop_t0, double* v) {
+    for (int n = 0; n < 12; n++) v[n] = 0.0;
+    const int la = ia - t0, lb = ib - t0;
+    if (la >= 0 && la < P && !(drop_t0 && la == 0))
+        for (int n = 0; n < 6; n++) v[n] = (double)field[6 * la + n];
+    if (lb >= 0 && lb < P && !(drop_t0 && lb == 0))
+        for (int n = 0; n < 6; n++) v[6 + n] = (double)field[6 * lb + n];
+}
+
+// row r of the 3x4 matrix M times X = (x, y, 1, d)
+__device__ __forceinline__ float mrow(const float* M, int r, const float* X) {
+    return M[4 * r] * X[0] + M[4 * r + 1] * X[1] + M[4 * r + 2] + M[4 * r + 3] * X[3];
+}
+
+// ---------------------------------------------------------------- kernels
+
+// gT <- incoming pose gradients (left tangent, lietorch layout (N, 7), [6] unused)
+__global__ void ba_adj_init_kernel(BAPtrs base, Batch B) {
+    BA_BIND(B, base);
+    for (int q = threadIdx.x; q < d.N * 6; q += blockDim.x) w.adj_gT[q] = (double)io.g_poses[(q / 6) * 7 + q % 6];
+}
+
+// retraction T' = Exp(dxi) T:  g_dxi = J_l(dxi)^T g_T',  g_T = Ad(Exp dxi)^T g_T'
+// with J_l = sum ad^n/(n+1)!, Ad(Exp) = sum ad^n/n! (series in FP64).
+__global__ void ba_adj_prep_kernel(BAPtrs base, Batch B) {
+    BA_BIND(B, base);
+    if (w.status[0]) return;
+    for (int a = threadIdx.x; a < d.P; a += blockDim.x) {
+        double xi[6], term[6], adacc[6], jl[6];
+        for (int n = 0; n < 6; n++) xi[n] = (double)io.dx[6 * a + n];
+        double* g = w.adj_gT + (size_t)(d.t0 + a) * 6;
+        for (int n = 0; n < 6; n++) {
+            term[n] = g[n];
+            adacc[n] = g[n];
+            jl[n] = g[n];
+        }
+        double c = 1.0;  // 1/k!
+        for (int k = 1; k <= 30; k++) {
+            adT_apply(xi, term);
+            c /= k;
+            double mx = 0.0;
+            for (int n = 0; n < 6; n++) {
+                adacc[n] += c * term[n];
+                jl[n] += c / (k + 1) * term[n];
+                mx = fmax(mx, fabs(term[n]));
+            }
+            if (mx * c < 1e-30) break;
+        }
+        for (int n = 0; n < 6; n++) {
+            w.adj_rhs[6 * a + n] = jl[n];
+            g[n] = adacc[n];
+        }
+    }
+}
+
+// per (depth frame, pixel chunk): for each edge leaving the frame, the 12 sums
+//   sum_p a_p act wd_c Jz_c [Ji_c, Jj_c],  a_p = Q_p g_d(p)
+__global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_a_kernel(BAPtrs base, Batch B) {
+    BA_BIND(B, base);
+    if (w.status[0]) return;
+    __shared__ float red[kAdjThreads / 32][12];
+    const int s = local_ % d.K, c = local_ / d.K, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int HW = d.HW, W = d.W;
+    const int k = w.kx[s];
+    const float act = io.depth_active[k];
+    const float fx = io.intr[0], fy = io.intr[1], cx = io.intr[2], cy = io.intr[3];
+    const int p0 = c * d.chunk_f, p1 = min(HW, p0 + d.chunk_f);
+    for (int q = w.fe_ptr[s]; q < w.fe_ptr[s + 1]; q++) {
+        const int e = w.fe_list[q];
+        const int b = (int)io.jj[e];
+        float tij[3], qij[4];
+        edge_pose(io.poses, k, b, tij, qij);
+        float acc[12];
+#pragma unroll
+        for (int n = 0; n < 12; n++) acc[n] = 0.f;
+        if (act != 0.f) {
+            const float* wp = io.weights + (size_t)e * 2 * HW;
+            for (int p = p0 + tid; p < p1; p += kAdjThreads) {
+                const float u = (float)(p % W), v = (float)(p / W);
+                const float disp = io.disps[(size_t)k * HW + p];
+                const float a = w.qwf[((size_t)s * HW + p) * 3] * io.g_disps[(size_t)k * HW + p];
+                PixelLin L;
+                linearize<false, false>(tij, qij, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p),
+                                        __ldg(wp + HW + p), 0.f, 0.f, act, 1.f, L);
+#pragma unroll
+                for (int ch = 0; ch < 2; ch++) {
+                    const float g = a * act * L.wd[ch] * L.Jz[ch];
+#pragma unroll
+                    for (int n = 0; n < 6; n++) {
+                        acc[n] += g * L.Ji[ch][n];
+                        acc[6 + n] += g * L.Jj[ch][n];
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int n = 0; n < 12; n++) {
+            const float sv = warp_sum(acc[n]);
+            if (lane == 0) red[warp][n] = sv;
+        }
+        __syncthreads();
+        if (tid < 12) {
+            float sv = 0.f;
+            for (int r = 0; r < kAdjThreads / 32; r++) sv += red[r][tid];
+            w.adj_aslot[((size_t)e * d.CF + c) * 12 + tid] = sv;
+        }
+        __syncthreads();
+    }
+}
+
+// rhs = g_dxi - E~ a per window pose (pose t0 keeps g_dxi: E~ has no rows for it)
+__global__ void ba_adj_rhs_kernel(BAPtrs base, Batch B) {
+    BA_BIND(B, base);
+    if (w.status[0]) return;
+    for (int q = threadIdx.x; q < 6 * d.P; q += blockDim.x) {
+        const int a = q / 6, n = q % 6;
+        if (a == 0) continue;
+        double sub = 0.0;
+        for (int r = w.pe_ptr[a]; r < w.pe_ptr[a + 1]; r++) {
+            const int ent = w.pe_list[r];
+            const int e = ent >> 2, fl = ent & 3;
+            for (int c = 0; c < d.CF; c++) {
+                const float* src = w.adj_aslot + ((size_t)e * d.CF + c) * 12;
+                if (fl & 1) sub += (double)src[n];
+                if (fl & 2) sub += (double)src[6 + n];
+            }
+        }
+        w.adj_rhs[q] -= sub;
+    }
+}
+
+// Jacobian rows of one pixel of one edge from the edge's 3x4 transform M0 =
+// [R | t] (same values as the reference formulas, geom_kernels.cu:338-350):
+//   target pose:  tau_n: grad f . e_n W        phi_n: e_n . (P x grad f)
+//   source pose:  tau_n: -W (R^T grad f)_n     phi_n: -e_n . (X3 x R^T grad f)
+// with P = M0 X, W = d, grad f the projection gradient on P.
+struct PixJ {
+    float P[3];
+    float iz;
+    float gf[2][3];
+    float J[2][12];  // [source 6 | target 6] per channel
+    float jz[2];
+};
+
+__device__ __forceinline__ bool pix_jac(const float* M0, const float* X, float fx, float fy, PixJ& o) {
+#pragma unroll
+    for (int r = 0; r < 3; r++) o.P[r] = mrow(M0, r, X);
+    if (o.P[2] < 0.25f) return false;  // the forward's MIN_DEPTH mask
+    const float iz = 1.f / o.P[2];
+    o.iz = iz;
+    o.gf[0][0] = fx * iz; o.gf[0][1] = 0.f; o.gf[0][2] = -fx * o.P[0] * iz * iz;
+    o.gf[1][0] = 0.f; o.gf[1][1] = fy * iz; o.gf[1][2] = -fy * o.P[1] * iz * iz;
+    const float W = X[3];
+#pragma unroll
+    for (int ch = 0; ch < 2; ch++) {
+        const float* g = o.gf[ch];
+        float rg[3];  // R^T grad f
+#pragma unroll
+        for (int n = 0; n < 3; n++) rg[n] = M0[n] * g[0] + M0[4 + n] * g[1] + M0[8 + n] * g[2];
+        o.J[ch][0] = -W * rg[0];
+        o.J[ch][1] = -W * rg[1];
+        o.J[ch][2] = -W * rg[2];
+        o.J[ch][3] = -(X[1] * rg[2] - 1.f * rg[1]);
+        o.J[ch][4] = -(1.f * rg[0] - X[0] * rg[2]);
+        o.J[ch][5] = -(X[0] * rg[1] - X[1] * rg[0]);
+        o.J[ch][6] = g[0] * W;
+        o.J[ch][7] = g[1] * W;
+        o.J[ch][8] = g[2] * W;
+        o.J[ch][9] = o.P[1] * g[2] - o.P[2] * g[1];
+        o.J[ch][10] = o.P[2] * g[0] - o.P[0] * g[2];
+        o.J[ch][11] = o.P[0] * g[1] - o.P[1] * g[0];
+        o.jz[ch] = g[0] * M0[3] + g[1] * M0[7] + g[2] * M0[11];
+    }
+    return true;
+}
+
+__device__ __forceinline__ void cross3f(const float* a, const float* b, float* c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// One tangent direction v = [v_i | v_j] (12) at one pixel: Y = R (v_i,tau W + v_i,phi x X3),
+// Pt = M^t_v X = v_j,tau W + v_j,phi x P - Y, and dPt/dW.
+struct DirPix {
+    float Y[3], Pt[3], dPt[3];
+};
+
+__device__ __forceinline__ void dir_pix(const float* M0, const float* X, const float* P, const float* v, DirPix& o) {
+    const float W = X[3];
+    float z[3], c[3];
+    const float X3[3] = {X[0], X[1], 1.f};
+    cross3f(v + 3, X3, c);
+#pragma unroll
+    for (int n = 0; n < 3; n++) z[n] = v[n] * W + c[n];
+#pragma unroll
+    for (int r = 0; r < 3; r++) o.Y[r] = M0[4 * r] * z[0] + M0[4 * r + 1] * z[1] + M0[4 * r + 2] * z[2];
+    float cp[3];
+    cross3f(v + 9, P, cp);
+#pragma unroll
+    for (int r = 0; r < 3; r++) o.Pt[r] = v[6 + r] * W + cp[r] - o.Y[r];
+    // d/dW: v_j,tau + v_j,phi x t - R v_i,tau
+    const float t[3] = {M0[3], M0[7], M0[11]};
+    float ct[3];
+    cross3f(v + 9, t, ct);
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+        o.dPt[r] = v[6 + r] + ct[r] - (M0[4 * r] * v[0] + M0[4 * r + 1] * v[1] + M0[4 * r + 2] * v[2]);
+}
+
+// Mixed second derivative along direction v with coefficient cd, channel ch:
+//   f^{s v}_c = grad f . (M^{sv}_k X) + Ps_k . h,  h = (-f iz^2 Zt, 0, f iz^2 Xt - 2 iz f^v)  (u; v: rows 1, 2)
+// and, for pose directions k, grad f . (M^{sv}_k X) = Ps_k . (grad f x v_j,phi)
+// + e_k,phi . [target: -(Y x grad f); source: R^T (Y x grad f)].
+// Adds to g0h (Ps coefficient valid for every s-direction), g0x (pose-only Ps
+// coefficient), om (rotation-dof vector) and returns the depth s-direction value
+// grad f . dPt/dW (the h part for depth is g0h . t, added by the caller).
+__device__ __forceinline__ float mixed(const PixJ& J, int ch, float fxy, const float* v, const DirPix& D, float fv,
+                                       float cd, float* g0h, float* g0x, float* om) {
+    const float* g = J.gf[ch];
+    const float iz = J.iz, iz2 = iz * iz;
+    g0h[ch] += cd * (-fxy * iz2 * D.Pt[2]);
+    g0h[2] += cd * (fxy * iz2 * D.Pt[ch] - 2.f * iz * fv);
+    float gx[3];
+    cross3f(g, v + 9, gx);
+    float yg[3];
+    cross3f(D.Y, g, yg);
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        g0x[r] += cd * gx[r];
+        om[r] += cd * yg[r];
+    }
+    return cd * (g[0] * D.dPt[0] + g[1] * D.dPt[1] + g[2] * D.dPt[2]);
+}
+
+constexpr int kPixF = 14;   // per-pixel floats kept in shared memory by ba_adj_frame_b_kernel
+constexpr int kEdgeF = 96;  // per-edge floats: M0, Mt x3, directions x3, damping weights
+
+// per (depth frame, pixel chunk): the per-pixel adjoint quantities, then the
+// gradient of phi (with the exact derivative of the LM damping) for every edge
+// leaving the frame.  Dynamic shared memory: kPixF floats per pixel.
+__global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_b_kernel(BAPtrs base, Batch B, float alpha, float lm) {
+    BA_BIND(B, base);
+    if (w.status[0]) return;
+    extern __shared__ float pix[];  // [kPixF][chunk]: a, dzf, mu, gwz, gC, gd, disp, Q, Es[6]
+    __shared__ float Esh[kAdjMaxDeg][kEdgeF];
+    __shared__ int grp[kAdjMaxDeg];  // -1: unique target; else index of the first edge with the same target
+    __shared__ float red[kAdjThreads / 32][16];
+    __shared__ int any_dup;
+    const int s = local_ % d.K, c = local_ / d.K, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int HW = d.HW, W = d.W, t0 = d.t0, P = d.P;
+    const int k = w.kx[s];
+    const float act = io.depth_active[k];
+    const float fx = io.intr[0], fy = io.intr[1], cx = io.intr[2], cy = io.intr[3];
+    const int p0 = c * d.chunk_f, p1 = min(HW, p0 + d.chunk_f), np_ = p1 - p0;
+    const int eb = w.fe_ptr[s], ee = w.fe_ptr[s + 1];
+    const int deg = ee - eb;
+    if (deg > kAdjMaxDeg || d.chunk_f > kAdjMaxChunk) {
+        if (tid == 0) atomicOr(w.status, VIPE_ERR_CAPACITY);
+        return;
+    }
+    const int CH = d.chunk_f;
+    float* pa = pix;
+    float* pdzf = pix + CH;
+    float* pmu = pix + 2 * CH;
+    float* pgwz = pix + 3 * CH;
+    float* pgC = pix + 4 * CH;
+    float* pgd = pix + 5 * CH;
+    float* pdisp = pix + 6 * CH;
+    float* pQ = pix + 7 * CH;
+    float* pEs = pix + 8 * CH;  // 6 x CH: the frame's own-pose slot of E at each pixel
+    const bool self_in = k >= t0 && k < t0 + P;
+
+    // per-edge data: [0,12) M0, [12,48) Mt for lam, dxi, dxi~, [48,84) the directions, [84,96) damping lm*lam*dxi
+    if (tid == 0) any_dup = 0;
+    __syncthreads();
+    for (int q = warp; q < deg; q += kAdjThreads / 32) {
+        const int e = w.fe_list[eb + q];
+        const int b = (int)io.jj[e];
+        float* Eq = Esh[q];
+        if (lane < 16) {
+            const int dir = lane >> 2;
+            const int row = lane & 3;
+            if (row < 3) {
+                const M4 T = edge_matrix(io.poses, k, b);
+                double out[4];
+                if (dir == 0) {
+                    for (int col = 0; col < 4; col++) out[col] = T.m[4 * row + col];
+                } else {
+                    double v[12];
+                    if (dir == 1)
+                        edge_dir(w.adj_lam, k, b, t0, P, false, v);
+                    else
+                        edge_dir(io.dx, k, b, t0, P, dir == 3, v);
+                    const M4 Vi = hat(v), Vj = hat(v + 6);
+                    const M4 Mt = madd(mmul(Vj, T), mmul(T, Vi), -1.0);
+                    for (int col = 0; col < 4; col++) out[col] = Mt.m[4 * row + col];
+                }
+                for (int col = 0; col < 4; col++) Eq[12 * dir + 4 * row + col] = (float)out[col];
+            }
+        } else if (lane < 19) {
+            const int dir = lane - 16;
+            double v[12];
+            if (dir == 0)
+                edge_dir(w.adj_lam, k, b, t0, P, false, v);
+            else
+                edge_dir(io.dx, k, b, t0, P, dir == 2, v);
+            for (int n = 0; n < 12; n++) Eq[48 + 12 * dir + n] = (float)v[n];
+        } else if (lane == 19) {
+            double vl[12], vd[12];
+            edge_dir(w.adj_lam, k, b, t0, P, false, vl);
+            edge_dir(io.dx, k, b, t0, P, false, vd);
+            for (int n = 0; n < 12; n++) Eq[84 + n] = (float)((double)lm * vl[n] * vd[n]);
+        } else if (lane == 20) {
+            int g = -1;
+            if (b != k)
+                for (int q2 = 0; q2 < deg; q2++) {
+                    if (q2 == q) continue;
+                    if ((int)io.jj[w.fe_list[eb + q2]] == b) {
+                        g = q2 < q ? q2 : q;
+                        for (int q3 = 0; q3 < q2 && q3 < q; q3++)
+                            if ((int)io.jj[w.fe_list[eb + q3]] == b) g = min(g, q3);
+                        break;
+                    }
+                }
+            grp[q] = g;
+            if (g >= 0) atomicOr(&any_dup, 1);
+        }
+    }
+    __syncthreads();
+    const bool dup = any_dup != 0;
+
+    // target-slot E contribution of edge q at a pixel (sum over channels)
+    auto tvec = [&](int q, const float* X, int p, float* out) {
+        const int e = w.fe_list[eb + q];
+        PixJ J;
+#pragma unroll
+        for (int n = 0; n < 6; n++) out[n] = 0.f;
+        if (!pix_jac(Esh[q], X, fx, fy, J)) return;
+        const float* wp = io.weights + (size_t)e * 2 * HW;
+        const float wc[2] = {0.001f * __ldg(wp + p), 0.001f * __ldg(wp + HW + p)};
+#pragma unroll
+        for (int ch = 0; ch < 2; ch++) {
+            const float g = act * act * wc[ch] * J.jz[ch];
+#pragma unroll
+            for (int n = 0; n < 6; n++) out[n] += g * J.J[ch][6 + n];
+        }
+    };
+
+    // ---- per-pixel adjoint quantities
+    for (int i = tid; i < np_; i += kAdjThreads) {
+        const int p = p0 + i;
+        const float u = (float)(p % W), v = (float)(p / W);
+        const float disp = io.disps[(size_t)k * HW + p];
+        const float X[4] = {(u - cx) / fx, (v - cy) / fy, 1.f, disp};
+        float eD = 0.f, eDt = 0.f, eL = 0.f, dampC = 0.f;
+        float Es[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (act != 0.f) {
+            for (int q = 0; q < deg; q++) {
+                const int e = w.fe_list[eb + q];
+                const bool stereo = (int)io.jj[e] == k;
+                const float* Eq = Esh[q];
+                PixJ J;
+                if (!pix_jac(Eq, X, fx, fy, J)) continue;
+                const float* wp = io.weights + (size_t)e * 2 * HW;
+                const float wc[2] = {0.001f * __ldg(wp + p), 0.001f * __ldg(wp + HW + p)};
+                float tv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int ch = 0; ch < 2; ch++) {
+                    const float g = act * act * wc[ch] * J.jz[ch];
+                    float jl = 0.f, jd = 0.f, jdt = 0.f;
+#pragma unroll
+                    for (int n = 0; n < 12; n++) {
+                        jl += J.J[ch][n] * Eq[48 + n];
+                        jd += J.J[ch][n] * Eq[60 + n];
+                        jdt += J.J[ch][n] * Eq[72 + n];
+                    }
+                    eL += g * jl;
+                    eD += g * jd;
+                    eDt += g * jdt;
+#pragma unroll
+                    for (int n = 0; n < 6; n++) {
+                        Es[n] += g * J.J[ch][n];
+                        if (stereo) Es[n] += g * J.J[ch][6 + n];
+                        else tv[n] += g * J.J[ch][6 + n];
+                    }
+                }
+                if (!stereo && grp[q] < 0)
+#pragma unroll
+                    for (int n = 0; n < 6; n++) dampC += Eq[90 + n] * tv[n] * tv[n];
+            }
+            if (dup) {  // targets shared by several edges: the slot holds their sum
+                for (int q = 0; q < deg; q++) {
+                    if (grp[q] != q) continue;
+                    float sum[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, tv[6];
+                    for (int q2 = q; q2 < deg; q2++)
+                        if (grp[q2] == q) {
+                            tvec(q2, X, p, tv);
+                            for (int n = 0; n < 6; n++) sum[n] += tv[n];
+                        }
+                    for (int n = 0; n < 6; n++) dampC += Esh[q][90 + n] * sum[n] * sum[n];
+                }
+            }
+            if (self_in && deg > 0) {
+                // lm lam dxi of the frame's own pose: the source half of any edge's damping weights
+#pragma unroll
+                for (int n = 0; n < 6; n++) dampC += Esh[0][84 + n] * Es[n] * Es[n];
+            }
+        }
+        const float* qw = w.qwf + ((size_t)s * HW + p) * 3;
+        const float Q = qw[0], wz = qw[1];
+        const float a = Q * io.g_disps[(size_t)k * HW + p];
+        const float dzf = Q * (wz - eD);
+        const float dz = Q * (wz - eDt);
+        const float mu = Q * eL;
+        const float gwz = a - mu;
+        const float gC = mu * dzf - a * dz - Q * Q * dampC;
+        const float dsens = io.disps_sens[(size_t)k * HW + p];
+        const float msk = (dsens > 0.f ? 1.f : 0.f) * act;
+        io.g_eta[(size_t)s * HW + p] += act * gC;
+        io.g_dsens[(size_t)k * HW + p] += act * msk * alpha * gwz;
+        pa[i] = a;
+        pdzf[i] = dzf;
+        pmu[i] = mu;
+        pgwz[i] = gwz;
+        pgC[i] = gC;
+        pgd[i] = -act * msk * alpha * gwz;
+        pdisp[i] = disp;
+        pQ[i] = Q;
+#pragma unroll
+        for (int n = 0; n < 6; n++) pEs[n * CH + i] = Es[n];
+    }
+    __syncthreads();
+
+    // ---- per edge: phi gradients
+    for (int q = 0; q < deg; q++) {
+        const int e = w.fe_list[eb + q];
+        const int b = (int)io.jj[e];
+        const bool stereo = k == b;
+        const float* Eq = Esh[q];
+        const float* tp = io.targets + (size_t)e * 2 * HW;
+        const float* wp = io.weights + (size_t)e * 2 * HW;
+        float* gtp = io.g_targets + (size_t)e * 2 * HW;
+        float* gwp = io.g_weights + (size_t)e * 2 * HW;
+        float mom[15];  // G0 (3x4) and the rotation-dof vector
+#pragma unroll
+        for (int m = 0; m < 15; m++) mom[m] = 0.f;
+        for (int i = tid; i < np_; i += kAdjThreads) {
+            const int p = p0 + i;
+            const float u = (float)(p % W), v = (float)(p / W);
+            const float X[4] = {(u - cx) / fx, (v - cy) / fy, 1.f, pdisp[i]};
+            PixJ J;
+            if (!pix_jac(Eq, X, fx, fy, J)) continue;  // invalid pixel: zero weight, no gradient
+            const float iz = J.iz, iz2 = iz * iz;
+            const float a = pa[i], dzf = pdzf[i], mu = pmu[i], gwz = pgwz[i], gC = pgC[i], Q = pQ[i];
+            const float rr[2] = {__ldg(tp + p) - (fx * J.P[0] * iz + cx), __ldg(tp + HW + p) - (fy * J.P[1] * iz + cy)};
+            const float wc[2] = {0.001f * __ldg(wp + p), 0.001f * __ldg(wp + HW + p)};
+            // the edge's fixed directions lam, dxi, dxi~ and the per-pixel damping direction beta
+            DirPix D[4];
+#pragma unroll
+            for (int dir = 0; dir < 3; dir++) dir_pix(Eq, X, J.P, Eq + 48 + 12 * dir, D[dir]);
+            float beta[12];
+            {
+                float tv[6];
+                if (!stereo) {
+                    if (grp[q] < 0) {
+#pragma unroll
+                        for (int n = 0; n < 6; n++) {
+                            tv[n] = 0.f;
+#pragma unroll
+                            for (int ch = 0; ch < 2; ch++) tv[n] += act * act * wc[ch] * J.jz[ch] * J.J[ch][6 + n];
+                        }
+                    } else {
+                        float t2[6];
+                        for (int n = 0; n < 6; n++) tv[n] = 0.f;
+                        for (int q2 = grp[q]; q2 < deg; q2++)
+                            if (grp[q2] == grp[q]) {
+                                tvec(q2, X, p, t2);
+                                for (int n = 0; n < 6; n++) tv[n] += t2[n];
+                            }
+                    }
+                }
+#pragma unroll
+                for (int n = 0; n < 6; n++) {
+                    const float es = pEs[n * CH + i];
+                    beta[n] = 2.f * Q * Eq[84 + n] * es;
+                    beta[6 + n] = 2.f * Q * Eq[90 + n] * (stereo ? es : tv[n]);
+                }
+            }
+            dir_pix(Eq, X, J.P, beta, D[3]);
+            float g0h[3] = {0.f, 0.f, 0.f}, g0x[3] = {0.f, 0.f, 0.f}, om[3] = {0.f, 0.f, 0.f}, g4[3] = {0.f, 0.f, 0.f};
+            float gdp = 0.f;
+#pragma unroll
+            for (int ch = 0; ch < 2; ch++) {
+                const float* g = J.gf[ch];
+                const float fxy = ch == 0 ? fx : fy;
+                float ft[3];
+#pragma unroll
+                for (int dir = 0; dir < 3; dir++) ft[dir] = g[0] * D[dir].Pt[0] + g[1] * D[dir].Pt[1] + g[2] * D[dir].Pt[2];
+                const float fjz = J.jz[ch];
+                const float fb = g[0] * D[3].Pt[0] + g[1] * D[3].Pt[1] + g[2] * D[3].Pt[2];  // J . beta
+                float gam[12], fg = 0.f;  // damping direction of the B diagonal: lm lam dxi * J
+#pragma unroll
+                for (int n = 0; n < 12; n++) {
+                    gam[n] = Eq[84 + n] * J.J[ch][n];
+                    fg += gam[n] * J.J[ch][n];
+                }
+                const float wpc = stereo ? 0.f : wc[ch];
+                const float A = act * act * wc[ch];
+                const float G3 = -dzf * ft[0] + mu * ft[1] - a * ft[2];
+                const float c0 = -wpc * ft[0] - A * gwz * fjz;
+                const float c1 = wpc * (rr[ch] - ft[1]) - A * fjz * dzf;
+                const float c2 = -wpc * ft[0] + A * fjz * mu;
+                const float c3 = -A * fjz * a;
+                const float c4 = A * (gwz * rr[ch] + 2.f * gC * fjz + G3 + fb);
+                const float cB = -2.f * wpc;
+                const float cE = A * fjz;
+                gtp[(size_t)ch * HW + p] += wpc * ft[0] + A * gwz * fjz;
+                gwp[(size_t)ch * HW + p] +=
+                    0.001f * ((stereo ? 0.f : ft[0] * (rr[ch] - ft[1]) - fg) +
+                              act * act * (gwz * fjz * rr[ch] + gC * fjz * fjz + fjz * (G3 + fb)));
+                // first derivatives (s part) and the depth t-direction (column 3 of G0)
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    g0h[r] += c0 * g[r];
+                    g4[r] += c4 * g[r];
+                }
+                // depth t-direction: h part with Pt = t, ft = Jz
+                g0h[ch] += c4 * (-fxy * iz2 * Eq[4 * 2 + 3]);
+                g0h[2] += c4 * (fxy * iz2 * Eq[4 * ch + 3] - 2.f * iz * fjz);
+                // pose-type directions
+                gdp += mixed(J, ch, fxy, Eq + 48, D[0], ft[0], c1, g0h, g0x, om);
+                gdp += mixed(J, ch, fxy, Eq + 60, D[1], ft[1], c2, g0h, g0x, om);
+                gdp += mixed(J, ch, fxy, Eq + 72, D[2], ft[2], c3, g0h, g0x, om);
+                gdp += mixed(J, ch, fxy, beta, D[3], fb, cE, g0h, g0x, om);
+                if (!stereo) {
+                    DirPix Dg;
+                    dir_pix(Eq, X, J.P, gam, Dg);
+                    gdp += mixed(J, ch, fxy, gam, Dg, fg, cB, g0h, g0x, om);
+                }
+            }
+            // depth s-direction of this pixel: Ps = t (column 3 of M0)
+            gdp += g0h[0] * Eq[3] + g0h[1] * Eq[7] + g0h[2] * Eq[11];
+            pgd[i] += gdp;
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                const float gr = g0h[r] + g0x[r];
+                mom[4 * r + 0] += gr * X[0];
+                mom[4 * r + 1] += gr * X[1];
+                mom[4 * r + 2] += gr;
+                mom[4 * r + 3] += gr * X[3] + g4[r];
+                mom[12 + r] += om[r];
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < 15; m++) {
+            const float sv = warp_sum(mom[m]);
+            if (lane == 0) red[warp][m] = sv;
+        }
+        __syncthreads();
+        if (tid < 15) {
+            float sv = 0.f;
+            for (int r = 0; r < kAdjThreads / 32; r++) sv += red[r][tid];
+            w.adj_gpart[((size_t)e * d.CF + c) * kAdjAcc + tid] = stereo ? 0.f : sv;
+        }
+        __syncthreads();
+    }
+    // ---- pass-through plus this iteration's depth gradient
+    for (int i = tid; i < np_; i += kAdjThreads) io.g_disps[(size_t)k * HW + p0 + i] += pgd[i];
+}
+
+// per edge: the 12 pose gradients from the moments: <M^s_k, G0> plus, for the
+// rotation dofs, -om (target pose) or R^T om (source pose)
+// (k < 6: source pose i, M^s = -T hat(e_k); k >= 6: target pose j, M^s = hat(e_{k-6}) T)
+__global__ void ba_adj_edge_reduce_kernel(BAPtrs base, Batch B) {
+    BA_BIND(B, base);
+    if (w.status[0]) return;
+    __shared__ double G[15];
+    const int e = local_, tid = threadIdx.x;
+    for (int m = tid; m < 15; m += blockDim.x) {
+        double sv = 0.0;
+        for (int c = 0; c < d.CF; c++) sv += (double)w.adj_gpart[((size_t)e * d.CF + c) * kAdjAcc + m];
+        G[m] = sv;
+    }
+    __syncthreads();
+    if (tid >= 12) return;
+    const int ia = (int)io.ii[e], ib = (int)io.jj[e];
+    double out = 0.0;
+    if (ia != ib) {
+        const M4 T = edge_matrix(io.poses, ia, ib);
+        double unit[6] = {0, 0, 0, 0, 0, 0};
+        unit[tid % 6] = 1.0;
+        const M4 H = hat(unit);
+        const bool src = tid < 6;
+        const M4 Ms = src ? madd(mzero(), mmul(T, H), -1.0) : mmul(H, T);
+        for (int r = 0; r < 3; r++)
+            for (int col = 0; col < 4; col++) out += Ms.m[4 * r + col] * G[4 * r + col];
+        const int n = tid % 6;
+        if (n >= 3) {
+            if (src)
+                out += T.m[0 * 4 + (n - 3)] * G[12] + T.m[1 * 4 + (n - 3)] * G[13] + T.m[2 * 4 + (n - 3)] * G[14];
+            else
+                out -= G[12 + n - 3];
+        }
+    }
+    w.adj_gedge[(size_t)e * 12 + tid] = out;
+}
+
+// gT[f] += per-edge pose gradients (every frame of the graph, fixed ones too);
+// one warp per frame, edges in index order, fixed reduction order.
+__global__ void ba_adj_pose_kernel(BAPtrs base, Batch B) {
+    BA_BIND(B, base);
+    if (w.status[0]) return;
+    const int lane = threadIdx.x & 31;
+    for (int f = threadIdx.x >> 5; f < d.N; f += blockDim.x >> 5) {
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        for (int e = lane; e < d.E; e += 32) {
+            const int ia = (int)io.ii[e], ib = (int)io.jj[e];
+            if (ia == f)
+                for (int n = 0; n < 6; n++) acc[n] += w.adj_gedge[(size_t)e * 12 + n];
+            if (ib == f)
+                for (int n = 0; n < 6; n++) acc[n] += w.adj_gedge[(size_t)e * 12 + 6 + n];
+        }
+        for (int n = 0; n < 6; n++) {
+            const double sv = warp_sum(acc[n]);
+            if (lane == 0) w.adj_gT[(size_t)f * 6 + n] += sv;
+        }
+    }
+}
+
+__global__ void ba_adj_finish_kernel(BAPtrs base, Batch B) {
+    BA_BIND(B, base);
+    for (int q = threadIdx.x; q < d.N * 7; q += blockDim.x) {
+        const int f = q / 7, n = q % 7;
+        io.g_poses[q] = n < 6 ? (float)w.adj_gT[(size_t)f * 6 + n] : 0.f;
+    }
+}
+
+__global__ void ba_adj_status_kernel(BAPtrs base, Batch B) {
+    BA_BIND(B, base);
+    if (w.status[0] && io.status) atomicOr(io.status, w.status[0]);
+}
+
+}  // namespace ba
+}  // namespace vipe
+
+using namespace vipe;
+using namespace vipe::ba;
+
+extern "C" int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const float* tape_poses,
+                                           const float* tape_disps, const float* intrinsics, const float* disps_sens,
+                                           const float* targets, const float* weights, const float* eta,
+                                           const int64_t* ii, const int64_t* jj, const float* depth_active,
+                                           int iterations, float lm, float ep, float alpha, float* grad_poses,
+                                           float* grad_disps, float* grad_targets, float* grad_weights,
+                                           float* grad_eta, float* grad_disps_sens, float* dx_scratch,
+                                           int32_t* dev_status, void* stream) {
+    if (!plan) return VIPE_ERR_ARG;
+    if (!plan->d_table) {
+        set_last_error("vipe_slam_ba_batch_backward: plan is not bound to a workspace");
+        return VIPE_ERR_WORKSPACE;
+    }
+    if (!plan->adjoint) {
+        set_last_error("vipe_slam_ba_batch_backward: plan was created without the adjoint buffers");
+        return VIPE_ERR_ARG;
+    }
+    if (iterations < 0 || !tape_poses || !tape_disps || !intrinsics || !disps_sens || !eta || !depth_active ||
+        !grad_poses || !grad_disps || !grad_eta || !grad_disps_sens || !dx_scratch)
+        return VIPE_ERR_ARG;
+    if (plan->edges > 0 && (!targets || !weights || !ii || !jj || !grad_targets || !grad_weights))
+        return VIPE_ERR_ARG;
+    size_t smem_b = 0;
+    for (const auto& gd : plan->gds) smem_b = std::max(smem_b, (size_t)kPixF * gd.d.chunk_f * sizeof(float));
+    if (smem_b > (size_t)kPixF * kAdjMaxChunk * sizeof(float)) {
+        set_last_error("vipe_slam_ba_batch_backward: pixel chunk beyond 3072 (use more frame_chunks)");
+        return VIPE_ERR_CAPACITY;
+    }
+    cudaStream_t st = as_stream(stream);
+    const Geometry& geo = plan->geo;
+    const long HW = (long)plan->ht * plan->wd;
+    const int G = geo.G;
+    const Batch per_graph{plan->d_table, nullptr, G};
+    if (plan->edges > 0) {
+        VIPE_CUDA_TRY(cudaMemsetAsync(grad_targets, 0, sizeof(float) * plan->edges * 2 * HW, st));
+        VIPE_CUDA_TRY(cudaMemsetAsync(grad_weights, 0, sizeof(float) * plan->edges * 2 * HW, st));
+    }
+    VIPE_CUDA_TRY(cudaMemsetAsync(grad_eta, 0, sizeof(float) * plan->kx * HW, st));
+    VIPE_CUDA_TRY(cudaMemsetAsync(grad_disps_sens, 0, sizeof(float) * plan->frames * HW, st));
+    VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_adj_frame_b_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(kPixF * kAdjMaxChunk * sizeof(float))));
+    BAPtrs base{const_cast<float*>(tape_poses), const_cast<float*>(tape_disps), const_cast<float*>(intrinsics),
+                disps_sens, targets, weights, eta, ii, jj, depth_active, dx_scratch, nullptr, nullptr, dev_status,
+                0, 1, grad_poses, grad_disps, grad_targets, grad_weights, grad_eta, grad_disps_sens};
+    int rc = launch_index(geo, plan->d_table, base, nullptr, st);
+    if (rc != VIPE_OK) return rc;
+    ba_adj_init_kernel<<<G, 256, 0, st>>>(base, per_graph);
+    VIPE_LAUNCH_CHECK();
+    SolveArgs a{1, lm, ep, alpha, 0, 0, 1e-6f, 1e-6f, 1.f, 0};
+    auto grid = [&](int k) { return (unsigned)geo.off[k][G]; };
+    const Batch frames{plan->d_table, plan->d_off + (size_t)kOffFrame * (G + 1), G};
+    const Batch edges{plan->d_table, plan->d_off + (size_t)kOffEdgeRed * (G + 1), G};
+    for (int itr = iterations - 1; itr >= 0; itr--) {
+        base.poses = const_cast<float*>(tape_poses) + (size_t)itr * plan->frames * 7;
+        base.disps = const_cast<float*>(tape_disps) + (size_t)itr * plan->frames * HW;
+        if ((rc = launch_linearize_solve(geo, plan->d_table, plan->d_off, base, a, itr, st)) != VIPE_OK) return rc;
+        {
+            VIPE_PROF("ba_adj_prep", st);
+            ba_adj_prep_kernel<<<G, 128, 0, st>>>(base, per_graph);
+        }
+        VIPE_LAUNCH_CHECK();
+        if (grid(kOffFrame) > 0) {
+            VIPE_PROF("ba_adj_frame_a", st);
+            ba_adj_frame_a_kernel<<<grid(kOffFrame), kAdjThreads, 0, st>>>(base, frames);
+        }
+        VIPE_LAUNCH_CHECK();
+        {
+            VIPE_PROF("ba_adj_rhs", st);
+            ba_adj_rhs_kernel<<<G, 256, 0, st>>>(base, per_graph);
+        }
+        VIPE_LAUNCH_CHECK();
+        if ((rc = launch_chol_resolve(geo, plan->d_table, base, st)) != VIPE_OK) return rc;
+        if (grid(kOffFrame) > 0) {
+            VIPE_PROF("ba_adj_frame_b", st);
+            ba_adj_frame_b_kernel<<<grid(kOffFrame), kAdjThreads, smem_b, st>>>(base, frames, alpha, lm);
+        }
+        VIPE_LAUNCH_CHECK();
+        if (grid(kOffEdgeRed) > 0) {
+            VIPE_PROF("ba_adj_edge_reduce", st);
+            ba_adj_edge_reduce_kernel<<<grid(kOffEdgeRed), 32, 0, st>>>(base, edges);
+        }
+        VIPE_LAUNCH_CHECK();
+        {
+            VIPE_PROF("ba_adj_pose", st);
+            ba_adj_pose_kernel<<<G, 256, 0, st>>>(base, per_graph);
+        }
+        VIPE_LAUNCH_CHECK();
+    }
+    ba_adj_finish_kernel<<<G, 256, 0, st>>>(base, per_graph);
+    VIPE_LAUNCH_CHECK();
+    if (dev_status) {
+        ba_adj_status_kernel<<<G, 1, 0, st>>>(base, per_graph);
+        VIPE_LAUNCH_CHECK();
+    }
+    return VIPE_OK;
+}

@@ -1,0 +1,393 @@
+// Internals shared by the bundle-adjustment translation units (ba.cu: index
+// build, linearisation, assembly, Cholesky, update; ba_adjoint.cu: the
+// hand-written adjoint).  Not part of the C ABI.
+#pragma once
+
+#include "common.cuh"
+
+#include <algorithm>
+#include <vector>
+
+namespace vipe {
+namespace ba {
+
+constexpr int kMaxSlots = 32;          // window poses coupled to one depth frame
+constexpr int kMaxPoses = 127;         // t1 - t0: 6P+1 unknowns fit the staged Cholesky panel
+constexpr int kNT = 105;               // per-edge terms, see term layout below
+constexpr int kEdgeThreads = 256;
+constexpr int kFrameThreads = 256;
+constexpr int kTilesPerThread = 5;     // 4x4 SYRK tiles held in registers per thread
+constexpr int kStageFloats = 25872;    // e' staging: Dp rows x (T + 4) pixels, <= 101 KiB
+constexpr int kIndexThreads = 1024;
+
+// per-edge term layout
+//   [0,78)   upper triangle (row-major, n >= m) of the 12x12 block [Ji Jj]^T W [Ji Jj]
+//   [78,84)  vi     [84,90) vj     [90,96) fi    [96,102) fj
+//   102 hf   103 vf   104 flow energy
+constexpr int kTV = 78, kTF = 90, kTHF = 102, kTVF = 103, kTEN = 104;
+
+__host__ __device__ inline int tri12(int r, int c) { return r >= c ? r * (r + 1) / 2 + c : c * (c + 1) / 2 + r; }
+
+struct Dims {
+    int N, H, W, HW, E, K, t0, t1, P, dim;
+    int CHe, chunk_e;  // edge kernel pixel chunks
+    int CF, chunk_f;   // frame kernel pixel chunks
+    long tile_cap;     // capacity of frame SYRK tiles
+    int adj;           // 1: the workspace also holds the adjoint buffers
+};
+
+struct Work {
+    int* status;   // [0] error code
+    int* meta;     // [0] nkx [1] sum_m [2] sum_tiles [3] max_m
+    int* flag;
+    int* rank;
+    int* kx;
+    int* fe_ptr;
+    int* fe_list;
+    int* edge_slot;
+    int* fp_ptr;
+    int* fp_list;
+    int* self_slot;
+    int* ftile_off;
+    int* pe_ptr;
+    int* pe_list;
+    int* pf_ptr;
+    int* pf_list;
+    float* epart;    // E * CHe * kNT
+    double* eterm;   // E * kNT
+    float* spart;    // tile_cap * CF * 16
+    float* fen;      // K * CF
+    float* qwf;      // K * HW * 3
+    double* Hm;      // dim * dim
+    double* bv;      // dim
+    double* df;      // 1
+    double* linv;    // inverse diagonal blocks of the Cholesky factor
+    // adjoint (carved only when Dims::adj)
+    double* adj_gT;    // N * 6   running left-tangent gradient of every pose
+    double* adj_rhs;   // dim     g_dxi, then g_dxi - E~ Q g_dz
+    double* adj_lam;   // dim     lambda = S'^-1 rhs
+    float* adj_aslot;  // E * CF * 12  per (edge, pixel chunk): sum a act wd Jz [Ji, Jj]
+    float* adj_gpart;  // E * CF * kAdjAcc  per (edge, pixel chunk) pose-gradient moments
+    double* adj_gedge; // E * 12  per-edge pose gradient [source pose, target pose]
+};
+
+constexpr int kAdjAcc = 48;  // 4 moment matrices of 3 x 4 per edge
+
+__host__ __device__ inline int npt_of(int m) {
+    int nt = (6 * m + 2 + 3) / 4;
+    return nt * (nt + 1) / 2;
+}
+
+// che / cf: pixel-chunk counts of the per-edge and per-frame kernels; 0 picks
+// them so that one graph alone launches about two CTAs per SM.
+inline Dims make_dims(int N, int H, int W, int E, int K, int t0, int t1, int che = 0, int cf = 0) {
+    Dims d;
+    d.N = N; d.H = H; d.W = W; d.HW = H * W; d.E = E; d.K = K; d.t0 = t0; d.t1 = t1;
+    d.P = t1 - t0;
+    d.dim = 6 * d.P + 1;
+    const int target = 2 * 148;
+    if (che <= 0) che = E > 0 ? (target + E - 1) / E : 1;
+    che = std::max(1, std::min(che, std::max(1, d.HW / 1024)));
+    d.chunk_e = (d.HW + che - 1) / che;
+    d.CHe = (d.HW + d.chunk_e - 1) / d.chunk_e;
+    if (cf <= 0) cf = K > 0 ? (target + K - 1) / K : 1;
+    cf = std::max(1, std::min(cf, 8));
+    int chunk = (d.HW + cf - 1) / cf;
+    chunk = ((chunk + 255) / 256) * 256;
+    d.chunk_f = chunk;
+    d.CF = (d.HW + chunk - 1) / chunk;
+    // Upper bound of sum over frames of npt(m_s): slots are <= kMaxSlots per
+    // frame and sum_s m_s <= E + K.  npt(m) <= (1.5 m + 3.25)^2 / 2.
+    const int M = std::max(1, std::min(kMaxSlots, d.P));
+    double b1 = (double)K * npt_of(M);
+    double b2 = (1.5 * M + 3.25) / 2.0 * (1.5 * (double)(E + K) + 3.25 * K);
+    d.tile_cap = (long)std::min(b1, b2) + K + 1;
+    d.adj = 0;
+    return d;
+}
+
+template <typename C>
+inline void carve(C& c, const Dims& d, Work* w) {
+    const size_t N = d.N, E = d.E, K = d.K, P = d.P;
+    auto take_i = [&](int*& dst, size_t n) {
+        auto p = c.template take<int>(n);
+        if (w) dst = (int*)p;
+    };
+    int* dummy;
+    take_i(w ? w->status : dummy, 4);
+    take_i(w ? w->meta : dummy, 8);
+    take_i(w ? w->flag : dummy, N);
+    take_i(w ? w->rank : dummy, N);
+    take_i(w ? w->kx : dummy, N);
+    take_i(w ? w->fe_ptr : dummy, K + 1);
+    take_i(w ? w->fe_list : dummy, E + 1);
+    take_i(w ? w->edge_slot : dummy, E + 1);
+    take_i(w ? w->fp_ptr : dummy, K + 1);
+    take_i(w ? w->fp_list : dummy, E + K + 1);
+    take_i(w ? w->self_slot : dummy, K + 1);
+    take_i(w ? w->ftile_off : dummy, K + 1);
+    take_i(w ? w->pe_ptr : dummy, P + 1);
+    take_i(w ? w->pe_list : dummy, 2 * E + 1);
+    take_i(w ? w->pf_ptr : dummy, P + 1);
+    take_i(w ? w->pf_list : dummy, E + K + 1);
+    auto pf = c.template take<float>((size_t)std::max<size_t>(1, E) * d.CHe * 36);
+    auto pd = c.template take<double>((size_t)std::max<size_t>(1, E) * kNT);
+    auto ps = c.template take<float>((size_t)d.tile_cap * d.CF * 16);
+    auto pen = c.template take<float>(K * d.CF + 1);
+    auto pq = c.template take<float>(K * (size_t)d.HW * 3);
+    auto pH = c.template take<double>((size_t)d.dim * d.dim);
+    auto pb = c.template take<double>((size_t)d.dim);
+    auto pdf = c.template take<double>(4);
+    auto pli = c.template take<double>((size_t)((d.dim + 31) / 32) * 32 * 32);
+    if (w) {
+        w->epart = (float*)pf;
+        w->eterm = (double*)pd;
+        w->spart = (float*)ps;
+        w->fen = (float*)pen;
+        w->qwf = (float*)pq;
+        w->Hm = (double*)pH;
+        w->bv = (double*)pb;
+        w->df = (double*)pdf;
+        w->linv = (double*)pli;
+        w->adj_gT = nullptr;
+        w->adj_rhs = w->adj_lam = nullptr;
+        w->adj_aslot = w->adj_gpart = nullptr;
+        w->adj_gedge = nullptr;
+    }
+    if (d.adj) {
+        auto g1 = c.template take<double>(N * 6);
+        auto g2 = c.template take<double>((size_t)d.dim);
+        auto g3 = c.template take<double>((size_t)d.dim);
+        auto g4 = c.template take<float>((size_t)std::max<size_t>(1, E) * d.CF * 12);
+        auto g5 = c.template take<float>((size_t)std::max<size_t>(1, E) * d.CF * kAdjAcc);
+        auto g6 = c.template take<double>((size_t)std::max<size_t>(1, E) * 12);
+        if (w) {
+            w->adj_gT = (double*)g1;
+            w->adj_rhs = (double*)g2;
+            w->adj_lam = (double*)g3;
+            w->adj_aslot = (float*)g4;
+            w->adj_gpart = (float*)g5;
+            w->adj_gedge = (double*)g6;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- graph table
+//
+// Every kernel runs over a table of graphs.  A single solve is a table of one;
+// a batch places many clips' graphs side by side: inputs are concatenated
+// along their leading axis (frames, edges, depth rows, window poses) and each
+// graph's descriptor holds its sizes, its carve of the workspace and its
+// offsets into the concatenated tensors.  Edge indices stay local to their
+// graph.  A launch over the batch is one flat grid: per kernel, boff[g] is the
+// first block of graph g (boff[G] = total), found by binary search.
+
+struct BAPtrs {
+    float* poses;              // (frames, 7)
+    float* disps;              // (frames, H, W)
+    float* intr;               // (graphs, 4)
+    const float* disps_sens;   // (frames, H, W)
+    const float* targets;      // (edges, 2, H, W)
+    const float* weights;      // (edges, 2, H, W)
+    const float* eta;          // (depth rows, H, W)
+    const int64_t* ii;         // (edges,) local frame index
+    const int64_t* jj;
+    const float* depth_active; // (frames,)
+    float* dx;                 // (window poses, 6)
+    float* dz;                 // (depth rows, H*W)
+    float* energy;             // (graphs, energy_stride)
+    int32_t* status;           // device status word(s): graph g uses status[g * status_stride]
+    int energy_stride;
+    int status_stride;
+    // adjoint inputs/outputs (frames/edges/depth rows concatenated like the inputs)
+    float* g_poses;    // (frames, 7) in: d loss / d poses_out; out: d loss / d poses_in (left tangent, [6] = 0)
+    float* g_disps;    // (frames, H, W) in: d loss / d disps_out; out: d loss / d disps_in
+    float* g_targets;  // (edges, 2, H, W) out (accumulated)
+    float* g_weights;  // (edges, 2, H, W) out (accumulated)
+    float* g_eta;      // (depth rows, H, W) out (accumulated)
+    float* g_dsens;    // (frames, H, W) out (accumulated)
+};
+
+struct GraphDesc {
+    Dims d;
+    Work w;
+    long frame_off, edge_off, kx_off, pose_off;
+    int g;
+};
+
+struct Batch {
+    const GraphDesc* gds;  // device table
+    const int* boff;       // per-kernel block offsets, or nullptr (see locate)
+    int G;
+};
+
+// Graph of this block.  With boff: flat grid over all graphs.  Without: a
+// single graph (G == 1, local = blockIdx.x) or one block per graph (g = blockIdx.x).
+__device__ __forceinline__ int locate(const Batch& B, int& local) {
+    if (B.boff == nullptr) {
+        if (B.G == 1) {
+            local = blockIdx.x;
+            return 0;
+        }
+        local = 0;
+        return blockIdx.x;
+    }
+    const int x = blockIdx.x;
+    int lo = 0, hi = B.G;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(B.boff + mid) <= x) lo = mid; else hi = mid;
+    }
+    local = x - __ldg(B.boff + lo);
+    return lo;
+}
+
+__device__ __forceinline__ BAPtrs rebase(const BAPtrs& b, const GraphDesc& g) {
+    const long HW = g.d.HW;
+    BAPtrs p;
+    p.poses = b.poses + g.frame_off * 7;
+    p.disps = b.disps + g.frame_off * HW;
+    p.intr = b.intr + (long)g.g * 4;
+    p.disps_sens = b.disps_sens + g.frame_off * HW;
+    p.targets = b.targets ? b.targets + g.edge_off * 2 * HW : nullptr;
+    p.weights = b.weights ? b.weights + g.edge_off * 2 * HW : nullptr;
+    p.eta = b.eta + g.kx_off * HW;
+    p.ii = b.ii ? b.ii + g.edge_off : nullptr;
+    p.jj = b.jj ? b.jj + g.edge_off : nullptr;
+    p.depth_active = b.depth_active + g.frame_off;
+    p.dx = b.dx + g.pose_off * 6;
+    p.dz = b.dz ? b.dz + g.kx_off * HW : nullptr;
+    p.energy = b.energy ? b.energy + (long)g.g * b.energy_stride : nullptr;
+    p.status = b.status ? b.status + (long)g.g * b.status_stride : nullptr;
+    p.energy_stride = b.energy_stride;
+    p.status_stride = b.status_stride;
+    p.g_poses = b.g_poses ? b.g_poses + g.frame_off * 7 : nullptr;
+    p.g_disps = b.g_disps ? b.g_disps + g.frame_off * HW : nullptr;
+    p.g_targets = b.g_targets ? b.g_targets + g.edge_off * 2 * HW : nullptr;
+    p.g_weights = b.g_weights ? b.g_weights + g.edge_off * 2 * HW : nullptr;
+    p.g_eta = b.g_eta ? b.g_eta + g.kx_off * HW : nullptr;
+    p.g_dsens = b.g_dsens ? b.g_dsens + g.frame_off * HW : nullptr;
+    return p;
+}
+
+// binds d, w, P (rebased pointers) and local_ (block index within the graph)
+#define BA_BIND(B, base)                                \
+    int local_;                                         \
+    const int g_ = locate(B, local_);                   \
+    const GraphDesc* __restrict__ gd_ = (B).gds + g_;   \
+    const Dims d = gd_->d;                              \
+    const Work w = gd_->w;                              \
+    const BAPtrs io = rebase(base, *gd_);                \
+    (void)io;                                           \
+    (void)d;
+
+struct EdgeArgs {
+    const float* poses;
+    const float* disps;
+    const float* intr;
+    const float* targets;
+    const float* weights;
+    const int64_t* ii;
+    const int64_t* jj;
+    float iscale;
+};
+
+// Per-pixel accumulation needs only the target-pose block: the source-pose
+// Jacobian of every pixel is Ji = -M Jj with M = Ad^T(Tij) constant per edge
+// (the adjoint pull-back used by the reference, geom_kernels.cu:88-102), so
+//   Hii = M Hjj M^T,  Hij = -M Hjj,  vi = -M vj,  fi = -M fj.
+// Chunk partial layout (kNE floats): [0,21) Hjj upper triangle (n >= m),
+// [21,27) vj, [27,33) fj, 33 hf, 34 vf, 35 flow energy.
+constexpr int kNE = 36;
+
+__host__ __device__ inline int tri6(int r, int c) { return r >= c ? r * (r + 1) / 2 + c : c * (c + 1) / 2 + r; }
+
+struct FrameArgs {
+    const float* poses;
+    const float* disps;
+    const float* disps_sens;
+    const float* intr;
+    const float* targets;
+    const float* weights;
+    const float* eta;
+    const float* depth_active;
+    const int64_t* jj;
+    float alpha;
+    float iscale;
+};
+
+constexpr int kCholThreads = 512;
+constexpr int kNB = 32;
+constexpr int kPanelRows = 768;  // systems up to 768 unknowns stage their panel in shared memory
+
+__host__ __device__ inline int chol_ldr(int dim) {
+    // transposed panel row length: >= max(dim, 32) + 4 (tiles read up to 3 rows
+    // past the last panel row, which are zero-filled), == 2 (mod 4) doubles so
+    // that 16-byte row-pair loads stay aligned
+    int r = (dim < kNB ? kNB : dim) + 4;
+    r = (r + 3) & ~3;
+    return r + 2;
+}
+
+// Launch geometry of a table of graphs: per kernel, the flat block count of
+// each graph and their running offsets (uploaded as Batch::boff for batches).
+enum { kOffEdge = 0, kOffEdgeRed, kOffFrame, kOffPairs, kOffRhs, kOffRetr, kNumOff };
+
+struct Geometry {
+    int G = 0;
+    std::vector<int> off[kNumOff];  // G + 1 entries each
+    size_t chol_smem = 0;
+    bool any_edges = false;
+};
+
+inline void fill_geometry(const std::vector<Dims>& dims, Geometry& geo) {
+    geo.G = (int)dims.size();
+    for (int k = 0; k < kNumOff; k++) geo.off[k].assign(geo.G + 1, 0);
+    for (int g = 0; g < geo.G; g++) {
+        const Dims& d = dims[g];
+        const long npairs = (long)d.P * (d.P + 1) / 2;
+        const int cnt[kNumOff] = {d.E * d.CHe, d.E, d.K * d.CF, (int)ceil_div(npairs, 8), (int)ceil_div(d.P + 1, 8),
+                                  (int)ceil_div(d.P, 128)};
+        for (int k = 0; k < kNumOff; k++) geo.off[k][g + 1] = geo.off[k][g] + cnt[k];
+        geo.chol_smem = std::max(geo.chol_smem, (size_t)chol_ldr(d.dim) * kNB * sizeof(double));
+        geo.any_edges |= d.E > 0;
+    }
+}
+
+struct SolveArgs {
+    int iterations;
+    float lm, ep, alpha;
+    int motion_only, intr;
+    float ilm, iep, iscale;
+    int compute_energy;
+};
+
+// host launchers implemented in ba.cu
+int check_dims(int num_frames, int ht, int wd, int num_edges, int num_kx, int t0, int t1);
+int ensure_attributes();
+int launch_index(const Geometry& geo, const GraphDesc* d_table, const BAPtrs& base, const GraphDesc* init,
+                 cudaStream_t st);
+// one LM step's linearisation, assembly and factorised solve (dx = Delta xi) at
+// the state held by base.poses / base.disps; nothing is updated
+int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const int* d_off, const BAPtrs& base,
+                           const SolveArgs& a, int itr, cudaStream_t st);
+// adj_lam = S'^-1 adj_rhs per graph, with the factor left by the last solve
+int launch_chol_resolve(const Geometry& geo, const GraphDesc* d_table, const BAPtrs& base, cudaStream_t st);
+
+}  // namespace ba
+}  // namespace vipe
+
+// Host-side plan of a batch of graphs (opaque to C callers).
+struct vipe_ba_batch_plan {
+    int G = 0;
+    int adjoint = 0;
+    std::vector<vipe::ba::GraphDesc> gds;  // Work pointers valid once bound
+    vipe::ba::Geometry geo;
+    size_t bytes = 0;
+    long frames = 0, edges = 0, kx = 0, poses = 0;
+    int ht = 0, wd = 0;
+    void* ws = nullptr;  // workspace the table was uploaded to
+    vipe::ba::GraphDesc* d_table = nullptr;
+    int* d_off = nullptr;
+    std::vector<int> off_host;  // kNumOff x (G + 1), the image of d_off
+};
