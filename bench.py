@@ -2,27 +2,33 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload (default): the plain FP32 drop-in ``slam_ext.ba_extended`` at ViPE scale
-— 64 keyframes of 48x64 inverse depth, SE3, 628 edges (|i-j| <= 3 plus 128
-random long-range pairs, both directions), 4 LM iterations, first two poses
-fixed; seeded synthetic inputs (vipe_b200.workloads.ba_config1).  One step is
-one full BA solve (index build + 4 LM iterations) over one graph.
+Workload: 256 clips of the bundle-adjustment generative model with uneven
+sizes (keyframes ~U{8..96} at 48x64, SE3, edges |i-j| <= 3 plus Poisson(4) loop
+pairs, 1% outlier flow), 4 LM iterations, first two poses of each clip fixed;
+seeded synthetic inputs generated on the GPU (vipe_b200.workloads).  One step =
+one batched forward solve of all 256 clips recording its state tape plus the
+hand-written adjoint for fixed incoming gradients (gradients for poses, depths,
+targets, weights, eta, disps_sens).  The metric counts clip solves per second.
 
 Reported (one JSON line on rank 0):
-  value     device-timed solves/s with inputs resident in HBM, L2 flushed
-            (256 MiB write) between steps outside the timed region, CUDA events
-            on the launching stream, max over ranks;
-  e2e       the same solve through the public Python API (vipe_b200.ext.slam_ext)
-            from pinned host buffers: host->device copy of the step's inputs,
-            the solve, device->host copy of poses/disps/intrinsics/dx/dz, all
-            inside the timed region;
-  roofline  the dominant kernel of the solve, timed live with the library's
-            launch profiler (events on the launching stream), algorithmic bytes
-            per launch over its average duration against MEASURED_PEAKS.json;
-  cpu_baseline  the CPU oracle (restatement of the reference's ba_cuda_impl,
-            FP32 math, dense FP64 solve) on a bounded sample, all host threads.
+  value      device-timed solves/s (fwd+adjoint), inputs resident in HBM
+             (about 4.5 GB, larger than L2), CUDA events on the launching stream,
+             max over ranks;
+  e2e        the same through the public API from pinned host tensors: inputs
+             and incoming gradients copied in, outputs and all input gradients
+             copied out, inside the timed region;
+  batched    the forward alone (CUDA graph of the LM loop), its roofline, the
+             plain FP32 drop-in slam_ext.ba_extended on the same 256 clips one
+             call per clip (the "plain form on the same GPU"), accuracy against
+             the FP64 oracle, the autotuner's table;
+  plain_cfg1 the plain drop-in on the 64-keyframe / 628-edge graph;
+  corr       the correlation volume + pyramid build (640 edges) and the
+             reference's cuBLAS + avg_pool2d path timed on the same GPU;
+  cpu_baseline  the CPU oracle (restatement of the reference's ba_cuda_impl:
+             FP32 per-edge math, dense FP64 Cholesky; forward only, the
+             reference has no BA backward) on clips of the batch, all host threads.
 
-Multi-GPU: graphs are independent, so N GPUs run N replicas (weak scaling, no
+Multi-GPU: clips are independent, so N GPUs run N replicas (weak scaling, no
 collective on the data path); value = solves of all ranks / max rank time.
 """
 
@@ -40,7 +46,7 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "batched BA solves/s"
+METRIC = "batched BA solves/s (fwd+adjoint)"
 WORKLOAD = (
     "batched BA: 256 clips, keyframes ~U{8..96} at 48x64, SE3, edges |i-j|<=3 + Poisson(4) loop pairs "
     "(|i-j|>8, both directions), 1% outlier flow (U(-20,20) px, weight 0.05), 4 LM iterations, t0=2"
@@ -495,8 +501,131 @@ def batched_leg(dev, args, world, dist, flush, stream):
     }
     e2e_line = {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "vipe_b200.ba_batch.BatchPlan.solve (pinned host tensors copied in and out each step)"}
+    extras["tune"] = (tune.edge_chunks, tune.frame_chunks)
     del plan, cap, static, work, clips
-    return value, e2e_line, extras, b.G, n
+    return value, e2e_line, extras, b.G, n, b
+
+
+def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
+    """Forward + hand-written adjoint of the batched BA on the same batch.
+
+    One step: the forward solve recording its state tape, then the backward for
+    fixed incoming gradients (a random-weighted sum of pose log-errors and depth
+    errors has constant gradients with respect to the outputs' tangents and
+    depths: N(0,1) per entry), producing gradients for poses, depths, targets,
+    weights, eta and disps_sens."""
+    import torch
+
+    from vipe_b200 import _lib, ba_batch as BB
+
+    lib = _lib.load()
+    iters, lm, ep, alpha = 4, 1e-4, 0.1, 0.001
+    plan = BB.BatchPlan(*b.sizes, b.ht, b.wd, dev, edge_chunks=tune[0], frame_chunks=tune[1], adjoint=True)
+    T = b.tensors
+    F, H, W = plan.total_frames, plan.ht, plan.wd
+    static = {k: v.clone() for k, v in T.items()}
+    out = plan.outputs(iters)
+    tape_p = torch.empty(iters, F, 7, device=dev)
+    tape_d = torch.empty(iters, F, H, W, device=dev)
+    g = torch.Generator(device=dev).manual_seed(1005)
+    gin_p = torch.randn(F, 7, generator=g, device=dev)
+    gin_p[:, 6] = 0
+    gin_d = torch.randn(F, H, W, generator=g, device=dev)
+    gp, gd = torch.empty_like(gin_p), torch.empty_like(gin_d)
+    gt, gw = torch.empty_like(T["targets"]), torch.empty_like(T["weights"])
+    ge, gs = torch.empty_like(T["eta"]), torch.empty_like(T["disps_sens"])
+    dxs = torch.empty(plan.total_poses, 6, device=dev)
+    st = torch.zeros(plan.G, dtype=torch.int32, device=dev)
+    mutable = ("poses", "disps", "intrinsics")
+
+    def reset():
+        for k in mutable:
+            static[k].copy_(T[k])
+
+    def fwd_adj():
+        plan.solve(**static, iterations=iters, lm=lm, ep=ep, alpha=alpha, out=out, check=False, tape=(tape_p, tape_d))
+        gp.copy_(gin_p)
+        gd.copy_(gin_d)
+        rc = lib.vipe_slam_ba_batch_backward(
+            plan._h, tape_p.data_ptr(), tape_d.data_ptr(), static["intrinsics"].data_ptr(),
+            static["disps_sens"].data_ptr(), static["targets"].data_ptr(), static["weights"].data_ptr(),
+            static["eta"].data_ptr(), static["ii"].data_ptr(), static["jj"].data_ptr(),
+            static["depth_active"].data_ptr(), iters, lm, ep, alpha, gp.data_ptr(), gd.data_ptr(), gt.data_ptr(),
+            gw.data_ptr(), ge.data_ptr(), gs.data_ptr(), dxs.data_ptr(), st.data_ptr(), stream.cuda_stream)
+        _lib.check(rc, "batched backward")
+
+    for _ in range(max(3, args.warmup)):
+        reset()
+        fwd_adj()
+    torch.cuda.synchronize(dev)
+    n = max(3, args.steps // 4)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+    if world > 1:
+        dist.barrier()
+    for k in range(n):
+        reset()
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        fwd_adj()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    t = torch.tensor([sum(a.elapsed_time(c) for a, c in ev)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms = float(t.item()) / n
+    value = world * b.G / (step_ms / 1e3)
+    status_nonzero = int((st != 0).sum().item())
+
+    # live per-kernel profile of one step
+    def once():
+        reset()
+        flush.fill_(1.0)
+        fwd_adj()
+
+    prof = profile_kernels(lib, once, 2)
+    total = sum(v[0] for v in prof.values())
+    breakdown = {k: {"ms_per_step": v[0] / 2, "share": v[0] / total} for k, v in prof.items()}
+    launches = sum(v[1] for v in prof.values()) / 2
+
+    # end to end: pinned host inputs and incoming gradients in, outputs and all gradients out
+    host_in = {k: v.cpu().pin_memory() for k, v in T.items()}
+    host_g = [gin_p.cpu().pin_memory(), gin_d.cpu().pin_memory()]
+    h2d = sum(v.numel() * v.element_size() for v in host_in.values()) + sum(x.numel() * 4 for x in host_g)
+    outs = [static["poses"], static["disps"], gp, gd, gt, gw, ge, gs]
+    out_host = [torch.empty_like(o, device="cpu").pin_memory() for o in outs]
+    d2h = sum(h.numel() * h.element_size() for h in out_host)
+    e2e = []
+    for k in range(3):
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.fill_(float(k))
+        a.record(stream)
+        for key, v in host_in.items():
+            static[key].copy_(v, non_blocking=True)
+        gin_p.copy_(host_g[0], non_blocking=True)
+        gin_d.copy_(host_g[1], non_blocking=True)
+        fwd_adj()
+        for o, h in zip(outs, out_host):
+            h.copy_(o, non_blocking=True)
+        c.record(stream)
+        torch.cuda.synchronize(dev)
+        if k >= 1:
+            e2e.append(a.elapsed_time(c))
+    te = torch.tensor([sum(e2e)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * b.G * len(e2e) / (float(te.item()) / 1e3)
+    del plan, static, tape_p, tape_d, gt, gw
+    return {
+        "value": value,
+        "ms_per_step": step_ms,
+        "steps": n,
+        "status_nonzero": status_nonzero,
+        "kernel_breakdown": breakdown,
+        "gpu_launches_per_step": launches,
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "api": "vipe_b200.ba_batch.BatchPlan.solve with tape + vipe_slam_ba_batch_backward (pinned host "
+                       "tensors in: inputs and incoming gradients; out: poses, depths and every input gradient)"},
+    }
 
 
 def plain_cfg1_leg(dev, args, flush, stream):
@@ -563,7 +692,14 @@ def run_ours(args):
     stream = torch.cuda.current_stream(dev)
 
     with ClockSampler(local) as clk:
-        value, e2e, extras, G, n = batched_leg(dev, args, world, dist, flush, stream)
+        fwd_value, fwd_e2e, extras, G, n_fwd, b = batched_leg(dev, args, world, dist, flush, stream)
+        torch.cuda.empty_cache()
+        adj = adjoint_leg(b, extras.pop("tune"), dev, args, world, dist, flush, stream)
+    del b
+    value, e2e, n = adj["value"], adj.pop("e2e"), adj["steps"]
+    extras["forward_only"] = {"value": fwd_value, "unit": "solves/s", "ms_per_batch": extras["batch_ms"],
+                              "steps": n_fwd, "e2e": fwd_e2e, "form": "CUDA graph of the whole LM loop"}
+    extras["speedup_fwd_adj_vs_plain_forward_same_gpu"] = value / extras["plain_same_gpu"]["value"]
     torch.cuda.empty_cache()
     plain = plain_cfg1_leg(dev, args, flush, stream)
     hbm, bf16, src = measured_peaks()
@@ -580,7 +716,7 @@ def run_ours(args):
             "n_gpus": world,
             "steps": n,
             "warmup": max(3, args.warmup),
-            "ms_per_step": extras["batch_ms"],
+            "ms_per_step": adj["ms_per_step"],
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
@@ -592,14 +728,16 @@ def run_ours(args):
                 "per_gpu_batch": G,
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "l2": "inputs (about 4 GB) larger than L2; 256 MiB flush write between steps",
-                "form": "batched, CUDA-graph captured LM loop, autotuned pixel chunking; FP32 linearisation, "
-                "FP64 block sums and Cholesky",
+                "form": "batched forward + hand-written adjoint per step (forward recording its state tape, "
+                "backward re-solving the same reduced systems); autotuned pixel chunking; FP32 linearisation, "
+                "FP64 block sums, Cholesky and re-solve",
             },
             "e2e": e2e,
             "roofline": extras.pop("roofline"),
-            "gpu_launches": int(extras["gpu_launches_per_batch"] * n),
+            "gpu_launches": int(adj["gpu_launches_per_step"] * n),
             "clocks": clk.summary(),
             "batched": extras,
+            "adjoint": adj,
             "plain_cfg1": plain,
             "corr": corr,
         }
