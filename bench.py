@@ -525,8 +525,7 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
     F, H, W = plan.total_frames, plan.ht, plan.wd
     static = {k: v.clone() for k, v in T.items()}
     out = plan.outputs(iters)
-    tape_p = torch.empty(iters, F, 7, device=dev)
-    tape_d = torch.empty(iters, F, H, W, device=dev)
+    tape = plan.make_tape(iters)
     g = torch.Generator(device=dev).manual_seed(1005)
     gin_p = torch.randn(F, 7, generator=g, device=dev)
     gin_p[:, 6] = 0
@@ -534,7 +533,6 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
     gp, gd = torch.empty_like(gin_p), torch.empty_like(gin_d)
     gt, gw = torch.empty_like(T["targets"]), torch.empty_like(T["weights"])
     ge, gs = torch.empty_like(T["eta"]), torch.empty_like(T["disps_sens"])
-    dxs = torch.empty(plan.total_poses, 6, device=dev)
     st = torch.zeros(plan.G, dtype=torch.int32, device=dev)
     mutable = ("poses", "disps", "intrinsics")
 
@@ -543,15 +541,15 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
             static[k].copy_(T[k])
 
     def fwd_adj():
-        plan.solve(**static, iterations=iters, lm=lm, ep=ep, alpha=alpha, out=out, check=False, tape=(tape_p, tape_d))
+        plan.solve(**static, iterations=iters, lm=lm, ep=ep, alpha=alpha, out=out, check=False, tape=tape)
         gp.copy_(gin_p)
         gd.copy_(gin_d)
         rc = lib.vipe_slam_ba_batch_backward(
-            plan._h, tape_p.data_ptr(), tape_d.data_ptr(), static["intrinsics"].data_ptr(),
+            plan._h, *[t.data_ptr() for t in tape], static["intrinsics"].data_ptr(),
             static["disps_sens"].data_ptr(), static["targets"].data_ptr(), static["weights"].data_ptr(),
             static["eta"].data_ptr(), static["ii"].data_ptr(), static["jj"].data_ptr(),
             static["depth_active"].data_ptr(), iters, lm, ep, alpha, gp.data_ptr(), gd.data_ptr(), gt.data_ptr(),
-            gw.data_ptr(), ge.data_ptr(), gs.data_ptr(), dxs.data_ptr(), st.data_ptr(), stream.cuda_stream)
+            gw.data_ptr(), ge.data_ptr(), gs.data_ptr(), st.data_ptr(), stream.cuda_stream)
         _lib.check(rc, "batched backward")
 
     for _ in range(max(3, args.warmup)):
@@ -614,7 +612,7 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world * b.G * len(e2e) / (float(te.item()) / 1e3)
-    del plan, static, tape_p, tape_d, gt, gw
+    del plan, static, tape, gt, gw
     return {
         "value": value,
         "ms_per_step": step_ms,

@@ -157,15 +157,18 @@ int vipe_slam_ba_extended_noalloc(float* poses_io, float* disps_io, float* intri
  * edge_chunks / frame_chunks: pixel chunks per edge / per depth frame for the
  * linearisation kernels (0 = chosen from the batch size).  with_adjoint: also
  * reserve the buffers of vipe_slam_ba_batch_backward.
- * tape_poses / tape_disps (optional, both or neither): receive the state that
- * enters each iteration, (iterations, sum frames, 7) and
- * (iterations, sum frames, ht, wd) — the input of the backward pass. */
+ * tape_poses, tape_disps, tape_factor, tape_dx (optional, all or none): the
+ * record the backward pass reads — per iteration the state entering it,
+ * (iterations, sum frames, 7) and (iterations, sum frames, ht, wd), the
+ * factorised reduced system, (iterations, totals_out[4]) doubles, and the pose
+ * step, (iterations, sum (t1-t0), 6). */
 typedef struct vipe_ba_batch_plan vipe_ba_batch_plan;
 int vipe_slam_ba_batch_plan_create(int num_graphs, const int* num_frames, const int* num_edges, const int* num_kx,
                                    const int* t0, const int* t1, int ht, int wd, int edge_chunks, int frame_chunks,
                                    int with_adjoint, vipe_ba_batch_plan** plan_out);
 size_t vipe_slam_ba_batch_workspace_size(const vipe_ba_batch_plan* plan);
-/* totals_out[4] = {sum frames, sum edges, sum kx, sum (t1-t0)} */
+/* totals_out[5] = {sum frames, sum edges, sum kx, sum (t1-t0), doubles of one
+ * iteration of the factor tape} */
 int vipe_slam_ba_batch_totals(const vipe_ba_batch_plan* plan, int64_t* totals_out);
 int vipe_slam_ba_batch_bind(vipe_ba_batch_plan* plan, void* workspace, size_t workspace_bytes, void* stream);
 int vipe_slam_ba_batch_solve(const vipe_ba_batch_plan* plan, float* poses_io, float* disps_io, float* intrinsics_io,
@@ -174,7 +177,8 @@ int vipe_slam_ba_batch_solve(const vipe_ba_batch_plan* plan, float* poses_io, fl
                              float lm, float ep, int motion_only, float alpha, int optimize_intrinsics,
                              float intrinsics_lm, float intrinsics_ep, float intrinsics_scale, int compute_energy,
                              float* dx_out, float* dz_out, float* energy_out, int32_t* dev_status,
-                             float* tape_poses, float* tape_disps, void* stream);
+                             float* tape_poses, float* tape_disps, double* tape_factor, float* tape_dx,
+                             void* stream);
 void vipe_slam_ba_batch_plan_destroy(vipe_ba_batch_plan* plan);
 
 /* Adjoint of vipe_slam_ba_batch_solve (no counterpart in the reference, which
@@ -183,7 +187,8 @@ void vipe_slam_ba_batch_plan_destroy(vipe_ba_batch_plan* plan);
  * inputs; the plan must have been created with_adjoint.  Every LM step is
  * differentiated exactly, with its linear solve differentiated implicitly (the
  * same damped reduced system re-solved with the incoming gradients), the LM
- * damping ep + lm*diag(S) included; Jacobians are recomputed from the tape.
+ * damping ep + lm*diag(S) included; Jacobians are recomputed from the tape
+ * and the factorised reduced system is read back from it.
  * Not covered: motion_only and optimize_intrinsics solves.
  *   grad_poses (sum frames, 7): in, d loss / d poses_out as left-tangent
  *     gradients in columns 0..5 (lietorch's layout for group gradients,
@@ -191,15 +196,14 @@ void vipe_slam_ba_batch_plan_destroy(vipe_ba_batch_plan* plan);
  *     layout, column 6 = 0;
  *   grad_disps (sum frames, ht, wd): in, d loss / d disps_out; out, d loss / d disps_in;
  *   grad_targets, grad_weights (sum edges, 2, ht, wd), grad_eta (sum kx, ht, wd),
- *   grad_disps_sens (sum frames, ht, wd): out;
- *   dx_scratch (sum (t1-t0), 6): scratch.  dev_status as in the solve. */
+ *   grad_disps_sens (sum frames, ht, wd): out.  dev_status as in the solve. */
 int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const float* tape_poses, const float* tape_disps,
-                                const float* intrinsics, const float* disps_sens, const float* targets,
-                                const float* weights, const float* eta, const int64_t* ii, const int64_t* jj,
-                                const float* depth_active, int iterations, float lm, float ep, float alpha,
-                                float* grad_poses, float* grad_disps, float* grad_targets, float* grad_weights,
-                                float* grad_eta, float* grad_disps_sens, float* dx_scratch, int32_t* dev_status,
-                                void* stream);
+                                const double* tape_factor, const float* tape_dx, const float* intrinsics,
+                                const float* disps_sens, const float* targets, const float* weights, const float* eta,
+                                const int64_t* ii, const int64_t* jj, const float* depth_active, int iterations,
+                                float lm, float ep, float alpha, float* grad_poses, float* grad_disps,
+                                float* grad_targets, float* grad_weights, float* grad_eta, float* grad_disps_sens,
+                                int32_t* dev_status, void* stream);
 
 /* Debug view of the device-built graph index (bit-exact tests).  Runs only the
  * index construction of vipe_slam_ba_extended into `workspace` and copies:

@@ -47,12 +47,12 @@ _SIGS: dict[str, tuple] = {
     "vipe_slam_ba_batch_bind": (I, [P, P, SZ, P]),
     "vipe_slam_ba_batch_solve": (
         I,
-        [P, P, P, P, P, P, P, P, P, P, P, I, F, F, I, F, I, F, F, F, I, P, P, P, P, P, P, P],
+        [P, P, P, P, P, P, P, P, P, P, P, I, F, F, I, F, I, F, F, F, I, P, P, P, P, P, P, P, P, P],
     ),
     "vipe_slam_ba_batch_plan_destroy": (None, [P]),
     "vipe_slam_ba_batch_backward": (
         I,
-        [P, P, P, P, P, P, P, P, P, P, P, I, F, F, F, P, P, P, P, P, P, P, P, P],
+        [P, P, P, P, P, P, P, P, P, P, P, P, P, I, F, F, F, P, P, P, P, P, P, P, P],
     ),
     "vipe_slam_ba_index_debug": (I, [P, P, I, I, I, I, I, P, P, P, I, P, P, SZ, P]),
     "vipe_slam_frame_distance": (I, [P, P, P, P, P, P, P, P, I, I, I, I, I, I, F, P, P]),

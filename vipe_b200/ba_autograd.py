@@ -6,7 +6,8 @@
     loss(poses_out, disps_out).backward()
 
 The forward is the batched FP32 solve (vipe_slam_ba_batch_solve) run on copies
-of poses/disps, recording the state entering every LM iteration; the backward
+of poses/disps, recording the state entering every LM iteration, the factorised
+reduced system and the pose step (no Jacobian is stored); the backward
 is vipe_slam_ba_batch_backward: each LM step differentiated exactly (second
 derivatives of the reprojection and the LM damping ep + lm*diag(S) included),
 its linear solve differentiated implicitly by re-solving the same damped reduced
@@ -39,11 +40,10 @@ class _BundleAdjust(torch.autograd.Function):
         disps_out = disps.detach().clone().contiguous()
         intr = intrinsics.detach().clone().contiguous()
         dev = poses.device
-        tape_p = torch.empty(iterations, plan.total_frames, 7, dtype=torch.float32, device=dev)
-        tape_d = torch.empty(iterations, plan.total_frames, plan.ht, plan.wd, dtype=torch.float32, device=dev)
+        tape = plan.make_tape(iterations)
         plan.solve(poses_out, disps_out, intr, disps_sens.detach(), targets.detach(), weights.detach(), eta.detach(),
-                   ii, jj, depth_active.detach(), iterations, lm, ep, alpha=alpha, tape=(tape_p, tape_d))
-        ctx.save_for_backward(tape_p, tape_d, targets.detach(), weights.detach(), eta.detach(), disps_sens.detach(),
+                   ii, jj, depth_active.detach(), iterations, lm, ep, alpha=alpha, tape=tape)
+        ctx.save_for_backward(*tape, targets.detach(), weights.detach(), eta.detach(), disps_sens.detach(),
                               intrinsics.detach(), ii, jj, depth_active.detach())
         ctx.plan = plan
         ctx.cfg = (iterations, float(lm), float(ep), float(alpha))
@@ -51,7 +51,8 @@ class _BundleAdjust(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g_poses, g_disps):
-        tape_p, tape_d, targets, weights, eta, disps_sens, intrinsics, ii, jj, depth_active = ctx.saved_tensors
+        tape_p, tape_d, tape_f, tape_x, targets, weights, eta, disps_sens, intrinsics, ii, jj, depth_active = (
+            ctx.saved_tensors)
         plan = ctx.plan
         iterations, lm, ep, alpha = ctx.cfg
         dev = tape_p.device
@@ -66,13 +67,12 @@ class _BundleAdjust(torch.autograd.Function):
         gw = torch.empty_like(weights)
         ge = torch.empty_like(eta)
         gs = torch.empty_like(disps_sens)
-        dx = torch.empty(max(1, plan.total_poses), 6, dtype=torch.float32, device=dev)
         status = torch.zeros(plan.G, dtype=torch.int32, device=dev)
         rc = _lib.load().vipe_slam_ba_batch_backward(
-            plan._h, tape_p.data_ptr(), tape_d.data_ptr(), intrinsics.contiguous().data_ptr(),
-            disps_sens.data_ptr(), targets.data_ptr(), weights.data_ptr(), eta.data_ptr(), ii.data_ptr(),
-            jj.data_ptr(), depth_active.data_ptr(), iterations, lm, ep, alpha, gp.data_ptr(), gd.data_ptr(),
-            gt.data_ptr(), gw.data_ptr(), ge.data_ptr(), gs.data_ptr(), dx.data_ptr(), status.data_ptr(),
+            plan._h, tape_p.data_ptr(), tape_d.data_ptr(), tape_f.data_ptr(), tape_x.data_ptr(),
+            intrinsics.contiguous().data_ptr(), disps_sens.data_ptr(), targets.data_ptr(), weights.data_ptr(),
+            eta.data_ptr(), ii.data_ptr(), jj.data_ptr(), depth_active.data_ptr(), iterations, lm, ep, alpha,
+            gp.data_ptr(), gd.data_ptr(), gt.data_ptr(), gw.data_ptr(), ge.data_ptr(), gs.data_ptr(), status.data_ptr(),
             torch.cuda.current_stream(dev).cuda_stream,
         )
         _lib.check(rc, "bundle_adjust backward")

@@ -55,9 +55,10 @@ class BatchPlan:
                                                 int(self.adjoint), ctypes.byref(h))
         _lib.check(rc, "BatchPlan")
         self._h = h
-        tot = (ctypes.c_int64 * 4)()
+        tot = (ctypes.c_int64 * 5)()
         _lib.check(lib.vipe_slam_ba_batch_totals(h, tot), "BatchPlan")
-        self.total_frames, self.total_edges, self.total_kx, self.total_poses = (int(x) for x in tot)
+        self.total_frames, self.total_edges, self.total_kx, self.total_poses, self.factor_tape_doubles = (
+            int(x) for x in tot)
         nbytes = int(lib.vipe_slam_ba_batch_workspace_size(h))
         with torch.cuda.device(self.device):
             self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
@@ -103,6 +104,15 @@ class BatchPlan:
             if t.device != self.device:
                 raise RuntimeError(f"BatchPlan.solve: {name} is on {t.device}, the plan on {self.device}")
 
+    def make_tape(self, iterations: int):
+        """Buffers of the record the backward pass reads: per iteration the state
+        entering it (poses, disps), the factorised reduced system and the pose step."""
+        dev, it = self.device, int(iterations)
+        return (torch.empty(it, self.total_frames, 7, dtype=torch.float32, device=dev),
+                torch.empty(it, self.total_frames, self.ht, self.wd, dtype=torch.float32, device=dev),
+                torch.empty(it, max(1, self.factor_tape_doubles), dtype=torch.float64, device=dev),
+                torch.empty(it, max(1, self.total_poses), 6, dtype=torch.float32, device=dev))
+
     def outputs(self, iterations: int, motion_only: bool = False, compute_energy: bool = False):
         dev = self.device
         dx = torch.zeros(self.total_poses, 6, dtype=torch.float32, device=dev)
@@ -121,8 +131,7 @@ class BatchPlan:
         (0, a vipe_status error, or VIPE_WARN_SOLVER when that graph's Cholesky
         failed and its dx is 0).  ``out`` reuses preallocated outputs (for
         CUDA-graph capture); ``check`` validates shapes on the host; ``tape``
-        = (tape_poses (iterations, frames, 7), tape_disps (iterations, frames,
-        H, W)) receives the state entering each iteration (the backward's input).
+        (from make_tape) receives the record the backward pass reads.
         """
         if check:
             self._check(poses, disps, intrinsics, disps_sens, targets, weights, eta, ii, jj, depth_active)
@@ -136,8 +145,8 @@ class BatchPlan:
             depth_active.data_ptr(), iterations, float(lm), float(ep), int(bool(motion_only)), float(alpha),
             int(bool(optimize_intrinsics)), float(intrinsics_lm), float(intrinsics_ep), float(intrinsics_scale),
             int(bool(compute_energy)), dx.data_ptr(), _lib.ptr(dz), energy.data_ptr() if compute_energy else None,
-            status.data_ptr(), None if tape is None else tape[0].data_ptr(),
-            None if tape is None else tape[1].data_ptr(), torch.cuda.current_stream(self.device).cuda_stream,
+            status.data_ptr(), *([None] * 4 if tape is None else [t.data_ptr() for t in tape]),
+            torch.cuda.current_stream(self.device).cuda_stream,
         )
         _lib.check(rc, "BatchPlan.solve")
         return dx, dz, energy, status

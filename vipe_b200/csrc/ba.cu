@@ -526,11 +526,17 @@ __global__ void __launch_bounds__(kFrameThreads) ba_frame_kernel(BAPtrs base, Ba
     const int LD = T + 4;  // entry-major staging: element (entry q, pixel p) at q * LD + p
     const float fx = A.intr[0], fy = A.intr[1], cx = A.intr[2], cy = A.intr[3];
 
+    // Few tiles (small frames) leave most threads idle in the SYRK: then the
+    // pixels of each staged tile are split among KS thread groups, each group
+    // covering every tile over T / KS pixels, and the groups' partial sums are
+    // added once at the end.
+    const int KS = npt > kFrameThreads / 2 ? 1 : (npt > kFrameThreads / 4 ? 2 : 4);
+    const int kgrp = KS > 1 ? tid / npt : 0;
     int ti[kTilesPerThread], tj[kTilesPerThread];
     float acc[kTilesPerThread][16];
 #pragma unroll
     for (int i = 0; i < kTilesPerThread; i++) {
-        const int tau = tid + i * kFrameThreads;
+        const int tau = KS > 1 ? (i == 0 && tid < KS * npt ? tid % npt : npt) : tid + i * kFrameThreads;
         if (tau < npt) {
             decode_tile(tau, nt, ti[i], tj[i]);
         } else {
@@ -605,7 +611,8 @@ __global__ void __launch_bounds__(kFrameThreads) ba_frame_kernel(BAPtrs base, Ba
             if (ti[i] >= 0) {
                 const float* ra = stage + (size_t)(4 * ti[i]) * LD;
                 const float* rb = stage + (size_t)(4 * tj[i]) * LD;
-                for (int q = 0; q < T; q += 4) {
+                const int qlo = kgrp * (T / KS), qhi = qlo + T / KS;
+                for (int q = qlo; q < qhi; q += 4) {
                     float4 x[4], y[4];
 #pragma unroll
                     for (int r = 0; r < 4; r++) {
@@ -629,6 +636,20 @@ __global__ void __launch_bounds__(kFrameThreads) ba_frame_kernel(BAPtrs base, Ba
         __syncthreads();
     }
     const int toff = w.ftile_off[s];
+    if (KS > 1) {
+        // stage is free after the last SYRK step's barrier: add the groups' partials
+        if (tid < KS * npt)
+#pragma unroll
+            for (int q = 0; q < 16; q++) stage[(size_t)tid * 16 + q] = acc[0][q];
+        __syncthreads();
+        if (tid < npt)
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                float sv = 0.f;
+                for (int g = 0; g < KS; g++) sv += stage[((size_t)g * npt + tid) * 16 + q];
+                acc[0][q] = sv;
+            }
+    }
 #pragma unroll
     for (int i = 0; i < kTilesPerThread; i++) {
         const int tau = tid + i * kFrameThreads;
@@ -1041,10 +1062,21 @@ __global__ void __launch_bounds__(kCholThreads, 1)
     }
 }
 
-// Second solve with the factor the Cholesky kernel left in Hm (L in the lower
-// triangle) and linv (inverse diagonal blocks): adj_lam = S'^-1 adj_rhs over the
-// 6P pose unknowns; zero when the factorisation failed (the forward step was
-// dx = 0 then).  One CTA per graph.
+// Copies the factor the Cholesky kernel left in Hm / linv (and its failure
+// flag) into this iteration's slot of the factor tape.  One CTA per graph.
+__global__ void ba_tape_factor_kernel(BAPtrs base, Batch B) {
+    BA_BIND(B, base);
+    if (w.status[0]) return;
+    const long nH = (long)d.dim * d.dim, nL = (long)((d.dim + 31) / 32) * 32 * 32;
+    for (long q = threadIdx.x; q < nH; q += blockDim.x) io.ftape[q] = w.Hm[q];
+    for (long q = threadIdx.x; q < nL; q += blockDim.x) io.ftape[nH + q] = w.linv[q];
+    if (threadIdx.x == 0) io.ftape[nH + nL] = (double)w.meta[4];
+}
+
+// Second solve with a recorded factor (L in the lower triangle of the first
+// dim x dim doubles, then the inverse diagonal blocks, then the failure flag):
+// adj_lam = S'^-1 adj_rhs over the 6P pose unknowns; zero when that
+// factorisation failed (the forward step was dx = 0 then).  One CTA per graph.
 __global__ void __launch_bounds__(kCholThreads) ba_chol_resolve_kernel(BAPtrs base, Batch B) {
     BA_BIND(B, base);
     if (w.status[0]) return;
@@ -1052,9 +1084,10 @@ __global__ void __launch_bounds__(kCholThreads) ba_chol_resolve_kernel(BAPtrs ba
     __shared__ double ysh[kNB];
     const int tid = threadIdx.x;
     const int n = 6 * d.P, ld = d.dim;
-    const double* A = w.Hm;
-    const double* Linv = w.linv;
-    const bool fail = w.meta[4] != 0;
+    const double* A = io.ftape;
+    const long nH = (long)d.dim * d.dim, nL = (long)((d.dim + 31) / 32) * 32 * 32;
+    const double* Linv = io.ftape + nH;
+    const bool fail = io.ftape[nH + nL] != 0.0;
     for (int i = tid; i < n; i += kCholThreads) xs[i] = fail ? 0.0 : w.adj_rhs[i];
     __syncthreads();
     if (!fail) {
@@ -1347,19 +1380,34 @@ static int launch_update(const Geometry& geo, const GraphDesc* d_table, const in
 // table.  With a tape, the state (poses, disps) entering iteration k is first
 // copied to tape_poses + k * frames * 7 and tape_disps + k * frames * H * W
 // (device-to-device copies, capturable like the kernels).
+struct Tape {
+    float* poses = nullptr;   // (iterations, frames, 7)
+    float* disps = nullptr;   // (iterations, frames, H, W)
+    double* factor = nullptr; // (iterations, factor stride)
+    float* dx = nullptr;      // (iterations, window poses, 6)
+    long frames = 0, hw = 0, factor_stride = 0, poses6 = 0;
+};
+
 int run_solve(const Geometry& geo, const GraphDesc* d_table, const int* d_off, const BAPtrs& base,
-              const GraphDesc* init, const SolveArgs& a, cudaStream_t st, float* tape_poses = nullptr,
-              float* tape_disps = nullptr, long tape_frames = 0, long hw = 0) {
+              const GraphDesc* init, const SolveArgs& a, cudaStream_t st, const Tape* tape = nullptr) {
     int rc = launch_index(geo, d_table, base, init, st);
     if (rc != VIPE_OK) return rc;
     for (int itr = 0; itr < a.iterations; itr++) {
-        if (tape_poses) {
-            VIPE_CUDA_TRY(cudaMemcpyAsync(tape_poses + (size_t)itr * tape_frames * 7, base.poses,
-                                          sizeof(float) * tape_frames * 7, cudaMemcpyDeviceToDevice, st));
-            VIPE_CUDA_TRY(cudaMemcpyAsync(tape_disps + (size_t)itr * tape_frames * hw, base.disps,
-                                          sizeof(float) * tape_frames * hw, cudaMemcpyDeviceToDevice, st));
+        if (tape) {
+            VIPE_CUDA_TRY(cudaMemcpyAsync(tape->poses + (size_t)itr * tape->frames * 7, base.poses,
+                                          sizeof(float) * tape->frames * 7, cudaMemcpyDeviceToDevice, st));
+            VIPE_CUDA_TRY(cudaMemcpyAsync(tape->disps + (size_t)itr * tape->frames * tape->hw, base.disps,
+                                          sizeof(float) * tape->frames * tape->hw, cudaMemcpyDeviceToDevice, st));
         }
         if ((rc = launch_linearize_solve(geo, d_table, d_off, base, a, itr, st)) != VIPE_OK) return rc;
+        if (tape) {
+            BAPtrs tb = base;
+            tb.ftape = tape->factor + (size_t)itr * tape->factor_stride;
+            ba_tape_factor_kernel<<<geo.G, 256, 0, st>>>(tb, Batch{d_table, nullptr, geo.G});
+            VIPE_LAUNCH_CHECK();
+            VIPE_CUDA_TRY(cudaMemcpyAsync(tape->dx + (size_t)itr * tape->poses6, base.dx, sizeof(float) * tape->poses6,
+                                          cudaMemcpyDeviceToDevice, st));
+        }
         if ((rc = launch_update(geo, d_table, d_off, base, a, st)) != VIPE_OK) return rc;
     }
     if (base.status) {
@@ -1491,6 +1539,8 @@ extern "C" int vipe_slam_ba_batch_plan_create(int num_graphs, const int* num_fra
         gd.edge_off = plan->edges;
         gd.kx_off = plan->kx;
         gd.pose_off = plan->poses;
+        gd.ftape_off = plan->ftape_stride;
+        plan->ftape_stride += factor_slot_doubles(gd.d);
         gd.g = g;
         plan->frames += num_frames[g];
         plan->edges += num_edges[g];
@@ -1525,6 +1575,7 @@ extern "C" int vipe_slam_ba_batch_totals(const vipe_ba_batch_plan* plan, int64_t
     totals_out[1] = plan->edges;
     totals_out[2] = plan->kx;
     totals_out[3] = plan->poses;
+    totals_out[4] = plan->ftape_stride;
     return VIPE_OK;
 }
 
@@ -1557,9 +1608,11 @@ extern "C" int vipe_slam_ba_batch_solve(const vipe_ba_batch_plan* plan, float* p
                                         int motion_only, float alpha, int optimize_intrinsics, float intrinsics_lm,
                                         float intrinsics_ep, float intrinsics_scale, int compute_energy,
                                         float* dx_out, float* dz_out, float* energy_out, int32_t* dev_status,
-                                        float* tape_poses, float* tape_disps, void* stream) {
+                                        float* tape_poses, float* tape_disps, double* tape_factor, float* tape_dx,
+                                        void* stream) {
     if (!plan) return VIPE_ERR_ARG;
-    if ((tape_poses == nullptr) != (tape_disps == nullptr)) return VIPE_ERR_ARG;
+    const int ntape = (tape_poses != nullptr) + (tape_disps != nullptr) + (tape_factor != nullptr) + (tape_dx != nullptr);
+    if (ntape != 0 && ntape != 4) return VIPE_ERR_ARG;
     if (!plan->d_table) {
         set_last_error("vipe_slam_ba_batch_solve: plan is not bound to a workspace");
         return VIPE_ERR_WORKSPACE;
@@ -1572,8 +1625,17 @@ extern "C" int vipe_slam_ba_batch_solve(const vipe_ba_batch_plan* plan, float* p
                 iterations, 1};
     SolveArgs a{iterations, lm, ep, alpha, motion_only, optimize_intrinsics, intrinsics_lm, intrinsics_ep,
                 intrinsics_scale, compute_energy};
-    return run_solve(plan->geo, plan->d_table, plan->d_off, base, nullptr, a, as_stream(stream), tape_poses,
-                     tape_disps, plan->frames, (long)plan->ht * plan->wd);
+    Tape tape;
+    tape.poses = tape_poses;
+    tape.disps = tape_disps;
+    tape.factor = tape_factor;
+    tape.dx = tape_dx;
+    tape.frames = plan->frames;
+    tape.hw = (long)plan->ht * plan->wd;
+    tape.factor_stride = plan->ftape_stride;
+    tape.poses6 = plan->poses * 6;
+    return run_solve(plan->geo, plan->d_table, plan->d_off, base, nullptr, a, as_stream(stream),
+                     ntape ? &tape : nullptr);
 }
 
 extern "C" void vipe_slam_ba_batch_plan_destroy(vipe_ba_batch_plan* plan) { delete plan; }

@@ -200,12 +200,16 @@ __global__ void ba_adj_prep_kernel(BAPtrs base, Batch B) {
     }
 }
 
-// per (depth frame, pixel chunk): for each edge leaving the frame, the 12 sums
-//   sum_p a_p act wd_c Jz_c [Ji_c, Jj_c],  a_p = Q_p g_d(p)
-__global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_a_kernel(BAPtrs base, Batch B) {
+// per (depth frame, pixel chunk): first the per-pixel C = 1/Q and w of the
+// forward step (recomputed from the tape state exactly as the forward frame
+// kernel forms them, and stored for ba_adj_frame_b_kernel), then for each edge
+// leaving the frame the 12 sums  sum_p a_p act wd_c Jz_c [Ji_c, Jj_c],
+// a_p = Q_p g_d(p).
+__global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_a_kernel(BAPtrs base, Batch B, float alpha) {
     BA_BIND(B, base);
     if (w.status[0]) return;
     __shared__ float red[kAdjThreads / 32][12];
+    __shared__ float pa[kAdjMaxChunk];
     const int s = local_ % d.K, c = local_ / d.K, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int HW = d.HW, W = d.W;
@@ -213,7 +217,44 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_a_kernel(BAPtrs base
     const float act = io.depth_active[k];
     const float fx = io.intr[0], fy = io.intr[1], cx = io.intr[2], cy = io.intr[3];
     const int p0 = c * d.chunk_f, p1 = min(HW, p0 + d.chunk_f);
-    for (int q = w.fe_ptr[s]; q < w.fe_ptr[s + 1]; q++) {
+    if (d.chunk_f > kAdjMaxChunk) {
+        if (tid == 0) atomicOr(w.status, VIPE_ERR_CAPACITY);
+        return;
+    }
+    const int eb = w.fe_ptr[s], ee = w.fe_ptr[s + 1];
+    for (int p = p0 + tid; p < p1; p += kAdjThreads) {
+        const float u = (float)(p % W), v = (float)(p / W);
+        const float disp = io.disps[(size_t)k * HW + p];
+        float csum = 0.f, bsum = 0.f;
+        for (int q = eb; q < ee; q++) {
+            const int e = w.fe_list[q];
+            const int b = (int)io.jj[e];
+            float tij[3], qij[4];
+            edge_pose(io.poses, k, b, tij, qij);
+            const float* tp = io.targets + (size_t)e * 2 * HW;
+            const float* wp = io.weights + (size_t)e * 2 * HW;
+            PixelLin L;
+            linearize<false, true>(tij, qij, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p), __ldg(wp + HW + p),
+                                   __ldg(tp + p), __ldg(tp + HW + p), act, 1.f, L);
+#pragma unroll
+            for (int ch = 0; ch < 2; ch++) {
+                const float g = L.wd[ch] * L.Jz[ch];
+                csum += g * L.Jz[ch];
+                bsum += L.wd[ch] * L.r[ch] * L.Jz[ch];
+            }
+        }
+        const float dsens = io.disps_sens[(size_t)k * HW + p];
+        const float msk = (dsens > 0.f ? 1.f : 0.f) * act;
+        const float C = act * (csum + io.eta[(size_t)s * HW + p] + msk * alpha) + (1.f - act);
+        const float Q = 1.f / C;
+        const float wv = act * (bsum - msk * alpha * (disp - dsens));
+        float* qw = w.qwf + ((size_t)s * HW + p) * 3;
+        qw[0] = Q;
+        qw[1] = wv;
+        pa[p - p0] = Q * io.g_disps[(size_t)k * HW + p];
+    }
+    __syncthreads();
+    for (int q = eb; q < ee; q++) {
         const int e = w.fe_list[q];
         const int b = (int)io.jj[e];
         float tij[3], qij[4];
@@ -226,7 +267,7 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_a_kernel(BAPtrs base
             for (int p = p0 + tid; p < p1; p += kAdjThreads) {
                 const float u = (float)(p % W), v = (float)(p / W);
                 const float disp = io.disps[(size_t)k * HW + p];
-                const float a = w.qwf[((size_t)s * HW + p) * 3] * io.g_disps[(size_t)k * HW + p];
+                const float a = pa[p - p0];
                 PixelLin L;
                 linearize<false, false>(tij, qij, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p),
                                         __ldg(wp + HW + p), 0.f, 0.f, act, 1.f, L);
@@ -797,13 +838,14 @@ using namespace vipe;
 using namespace vipe::ba;
 
 extern "C" int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const float* tape_poses,
-                                           const float* tape_disps, const float* intrinsics, const float* disps_sens,
-                                           const float* targets, const float* weights, const float* eta,
-                                           const int64_t* ii, const int64_t* jj, const float* depth_active,
-                                           int iterations, float lm, float ep, float alpha, float* grad_poses,
-                                           float* grad_disps, float* grad_targets, float* grad_weights,
-                                           float* grad_eta, float* grad_disps_sens, float* dx_scratch,
-                                           int32_t* dev_status, void* stream) {
+                                           const float* tape_disps, const double* tape_factor, const float* tape_dx,
+                                           const float* intrinsics, const float* disps_sens, const float* targets,
+                                           const float* weights, const float* eta, const int64_t* ii,
+                                           const int64_t* jj, const float* depth_active, int iterations, float lm,
+                                           float ep, float alpha, float* grad_poses, float* grad_disps,
+                                           float* grad_targets, float* grad_weights, float* grad_eta,
+                                           float* grad_disps_sens, int32_t* dev_status, void* stream) {
+    (void)ep;  // the damping's constant part has no derivative; only lm enters the adjoint
     if (!plan) return VIPE_ERR_ARG;
     if (!plan->d_table) {
         set_last_error("vipe_slam_ba_batch_backward: plan is not bound to a workspace");
@@ -813,8 +855,8 @@ extern "C" int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const
         set_last_error("vipe_slam_ba_batch_backward: plan was created without the adjoint buffers");
         return VIPE_ERR_ARG;
     }
-    if (iterations < 0 || !tape_poses || !tape_disps || !intrinsics || !disps_sens || !eta || !depth_active ||
-        !grad_poses || !grad_disps || !grad_eta || !grad_disps_sens || !dx_scratch)
+    if (iterations < 0 || !tape_poses || !tape_disps || !tape_factor || !tape_dx || !intrinsics || !disps_sens ||
+        !eta || !depth_active || !grad_poses || !grad_disps || !grad_eta || !grad_disps_sens)
         return VIPE_ERR_ARG;
     if (plan->edges > 0 && (!targets || !weights || !ii || !jj || !grad_targets || !grad_weights))
         return VIPE_ERR_ARG;
@@ -838,20 +880,21 @@ extern "C" int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const
     VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_adj_frame_b_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(kPixF * kAdjMaxChunk * sizeof(float))));
     BAPtrs base{const_cast<float*>(tape_poses), const_cast<float*>(tape_disps), const_cast<float*>(intrinsics),
-                disps_sens, targets, weights, eta, ii, jj, depth_active, dx_scratch, nullptr, nullptr, dev_status,
-                0, 1, grad_poses, grad_disps, grad_targets, grad_weights, grad_eta, grad_disps_sens};
+                disps_sens, targets, weights, eta, ii, jj, depth_active, const_cast<float*>(tape_dx), nullptr,
+                nullptr, dev_status, 0, 1, grad_poses, grad_disps, grad_targets, grad_weights, grad_eta,
+                grad_disps_sens, const_cast<double*>(tape_factor)};
     int rc = launch_index(geo, plan->d_table, base, nullptr, st);
     if (rc != VIPE_OK) return rc;
     ba_adj_init_kernel<<<G, 256, 0, st>>>(base, per_graph);
     VIPE_LAUNCH_CHECK();
-    SolveArgs a{1, lm, ep, alpha, 0, 0, 1e-6f, 1e-6f, 1.f, 0};
     auto grid = [&](int k) { return (unsigned)geo.off[k][G]; };
     const Batch frames{plan->d_table, plan->d_off + (size_t)kOffFrame * (G + 1), G};
     const Batch edges{plan->d_table, plan->d_off + (size_t)kOffEdgeRed * (G + 1), G};
     for (int itr = iterations - 1; itr >= 0; itr--) {
         base.poses = const_cast<float*>(tape_poses) + (size_t)itr * plan->frames * 7;
         base.disps = const_cast<float*>(tape_disps) + (size_t)itr * plan->frames * HW;
-        if ((rc = launch_linearize_solve(geo, plan->d_table, plan->d_off, base, a, itr, st)) != VIPE_OK) return rc;
+        base.dx = const_cast<float*>(tape_dx) + (size_t)itr * plan->poses * 6;
+        base.ftape = const_cast<double*>(tape_factor) + (size_t)itr * plan->ftape_stride;
         {
             VIPE_PROF("ba_adj_prep", st);
             ba_adj_prep_kernel<<<G, 128, 0, st>>>(base, per_graph);
@@ -859,7 +902,7 @@ extern "C" int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const
         VIPE_LAUNCH_CHECK();
         if (grid(kOffFrame) > 0) {
             VIPE_PROF("ba_adj_frame_a", st);
-            ba_adj_frame_a_kernel<<<grid(kOffFrame), kAdjThreads, 0, st>>>(base, frames);
+            ba_adj_frame_a_kernel<<<grid(kOffFrame), kAdjThreads, 0, st>>>(base, frames, alpha);
         }
         VIPE_LAUNCH_CHECK();
         {

@@ -206,12 +206,20 @@ struct BAPtrs {
     float* g_weights;  // (edges, 2, H, W) out (accumulated)
     float* g_eta;      // (depth rows, H, W) out (accumulated)
     float* g_dsens;    // (frames, H, W) out (accumulated)
+    double* ftape;     // one iteration of the factor tape (graph slots at ftape_off)
 };
+
+// factor tape slot of one graph: the Cholesky factor (dim x dim, lower
+// triangle used), the inverse diagonal blocks, and the failure flag
+__host__ __device__ inline long factor_slot_doubles(const Dims& d) {
+    return (long)d.dim * d.dim + (long)((d.dim + 31) / 32) * 32 * 32 + 2;
+}
 
 struct GraphDesc {
     Dims d;
     Work w;
     long frame_off, edge_off, kx_off, pose_off;
+    long ftape_off;  // doubles: this graph's slot in one iteration of the factor tape
     int g;
 };
 
@@ -267,6 +275,7 @@ __device__ __forceinline__ BAPtrs rebase(const BAPtrs& b, const GraphDesc& g) {
     p.g_weights = b.g_weights ? b.g_weights + g.edge_off * 2 * HW : nullptr;
     p.g_eta = b.g_eta ? b.g_eta + g.kx_off * HW : nullptr;
     p.g_dsens = b.g_dsens ? b.g_dsens + g.frame_off * HW : nullptr;
+    p.ftape = b.ftape ? b.ftape + g.ftape_off : nullptr;
     return p;
 }
 
@@ -371,7 +380,7 @@ int launch_index(const Geometry& geo, const GraphDesc* d_table, const BAPtrs& ba
 // the state held by base.poses / base.disps; nothing is updated
 int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const int* d_off, const BAPtrs& base,
                            const SolveArgs& a, int itr, cudaStream_t st);
-// adj_lam = S'^-1 adj_rhs per graph, with the factor left by the last solve
+// adj_lam = S'^-1 adj_rhs per graph, with the factor recorded in base.ftape
 int launch_chol_resolve(const Geometry& geo, const GraphDesc* d_table, const BAPtrs& base, cudaStream_t st);
 
 }  // namespace ba
@@ -385,6 +394,7 @@ struct vipe_ba_batch_plan {
     vipe::ba::Geometry geo;
     size_t bytes = 0;
     long frames = 0, edges = 0, kx = 0, poses = 0;
+    long ftape_stride = 0;  // doubles of one iteration of the factor tape
     int ht = 0, wd = 0;
     void* ws = nullptr;  // workspace the table was uploaded to
     vipe::ba::GraphDesc* d_table = nullptr;
