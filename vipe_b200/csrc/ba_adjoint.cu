@@ -47,7 +47,7 @@ namespace ba {
 
 constexpr int kAdjThreads = 256;
 constexpr int kAdjMaxDeg = 64;       // edges leaving one depth frame
-constexpr int kAdjMaxChunk = 3072;   // pixels of one (frame, chunk) block
+constexpr int kAdjMaxChunk = 1536;   // pixels of one (frame, chunk) block (two blocks per SM fit)
 
 // ---------------------------------------------------------------- small helpers
 
@@ -423,12 +423,12 @@ __device__ __forceinline__ float mixed(const PixJ& J, int ch, float fxy, const f
 }
 
 constexpr int kPixF = 14;   // per-pixel floats kept in shared memory by ba_adj_frame_b_kernel
-constexpr int kEdgeF = 96;  // per-edge floats: M0, Mt x3, directions x3, damping weights
+constexpr int kEdgeF = 60;  // per-edge floats: M0, directions x3, damping weights
 
 // per (depth frame, pixel chunk): the per-pixel adjoint quantities, then the
 // gradient of phi (with the exact derivative of the LM damping) for every edge
 // leaving the frame.  Dynamic shared memory: kPixF floats per pixel.
-__global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_b_kernel(BAPtrs base, Batch B, float alpha, float lm) {
+__global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs base, Batch B, float alpha, float lm) {
     BA_BIND(B, base);
     if (w.status[0]) return;
     extern __shared__ float pix[];  // [kPixF][chunk]: a, dzf, mu, gwz, gC, gd, disp, Q, Es[6]
@@ -461,47 +461,31 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_b_kernel(BAPtrs base
     float* pEs = pix + 8 * CH;  // 6 x CH: the frame's own-pose slot of E at each pixel
     const bool self_in = k >= t0 && k < t0 + P;
 
-    // per-edge data: [0,12) M0, [12,48) Mt for lam, dxi, dxi~, [48,84) the directions, [84,96) damping lm*lam*dxi
+    // per-edge data: [0,12) M0 = Tij[0:3], [12,48) the directions lam, dxi, dxi~ (12 each),
+    // [48,60) damping weights lm lam dxi of the edge's two poses
     if (tid == 0) any_dup = 0;
     __syncthreads();
     for (int q = warp; q < deg; q += kAdjThreads / 32) {
         const int e = w.fe_list[eb + q];
         const int b = (int)io.jj[e];
         float* Eq = Esh[q];
-        if (lane < 16) {
-            const int dir = lane >> 2;
-            const int row = lane & 3;
-            if (row < 3) {
-                const M4 T = edge_matrix(io.poses, k, b);
-                double out[4];
-                if (dir == 0) {
-                    for (int col = 0; col < 4; col++) out[col] = T.m[4 * row + col];
-                } else {
-                    double v[12];
-                    if (dir == 1)
-                        edge_dir(w.adj_lam, k, b, t0, P, false, v);
-                    else
-                        edge_dir(io.dx, k, b, t0, P, dir == 3, v);
-                    const M4 Vi = hat(v), Vj = hat(v + 6);
-                    const M4 Mt = madd(mmul(Vj, T), mmul(T, Vi), -1.0);
-                    for (int col = 0; col < 4; col++) out[col] = Mt.m[4 * row + col];
-                }
-                for (int col = 0; col < 4; col++) Eq[12 * dir + 4 * row + col] = (float)out[col];
-            }
-        } else if (lane < 19) {
-            const int dir = lane - 16;
+        if (lane < 3) {
+            const M4 T = edge_matrix(io.poses, k, b);
+            for (int col = 0; col < 4; col++) Eq[4 * lane + col] = (float)T.m[4 * lane + col];
+        } else if (lane < 6) {
+            const int dir = lane - 3;
             double v[12];
             if (dir == 0)
                 edge_dir(w.adj_lam, k, b, t0, P, false, v);
             else
                 edge_dir(io.dx, k, b, t0, P, dir == 2, v);
-            for (int n = 0; n < 12; n++) Eq[48 + 12 * dir + n] = (float)v[n];
-        } else if (lane == 19) {
+            for (int n = 0; n < 12; n++) Eq[12 + 12 * dir + n] = (float)v[n];
+        } else if (lane == 6) {
             double vl[12], vd[12];
             edge_dir(w.adj_lam, k, b, t0, P, false, vl);
             edge_dir(io.dx, k, b, t0, P, false, vd);
-            for (int n = 0; n < 12; n++) Eq[84 + n] = (float)((double)lm * vl[n] * vd[n]);
-        } else if (lane == 20) {
+            for (int n = 0; n < 12; n++) Eq[48 + n] = (float)((double)lm * vl[n] * vd[n]);
+        } else if (lane == 7) {
             int g = -1;
             if (b != k)
                 for (int q2 = 0; q2 < deg; q2++) {
@@ -561,9 +545,9 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_b_kernel(BAPtrs base
                     float jl = 0.f, jd = 0.f, jdt = 0.f;
 #pragma unroll
                     for (int n = 0; n < 12; n++) {
-                        jl += J.J[ch][n] * Eq[48 + n];
-                        jd += J.J[ch][n] * Eq[60 + n];
-                        jdt += J.J[ch][n] * Eq[72 + n];
+                        jl += J.J[ch][n] * Eq[12 + n];
+                        jd += J.J[ch][n] * Eq[24 + n];
+                        jdt += J.J[ch][n] * Eq[36 + n];
                     }
                     eL += g * jl;
                     eD += g * jd;
@@ -577,7 +561,7 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_b_kernel(BAPtrs base
                 }
                 if (!stereo && grp[q] < 0)
 #pragma unroll
-                    for (int n = 0; n < 6; n++) dampC += Eq[90 + n] * tv[n] * tv[n];
+                    for (int n = 0; n < 6; n++) dampC += Eq[54 + n] * tv[n] * tv[n];
             }
             if (dup) {  // targets shared by several edges: the slot holds their sum
                 for (int q = 0; q < deg; q++) {
@@ -588,13 +572,13 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_b_kernel(BAPtrs base
                             tvec(q2, X, p, tv);
                             for (int n = 0; n < 6; n++) sum[n] += tv[n];
                         }
-                    for (int n = 0; n < 6; n++) dampC += Esh[q][90 + n] * sum[n] * sum[n];
+                    for (int n = 0; n < 6; n++) dampC += Esh[q][54 + n] * sum[n] * sum[n];
                 }
             }
             if (self_in && deg > 0) {
                 // lm lam dxi of the frame's own pose: the source half of any edge's damping weights
 #pragma unroll
-                for (int n = 0; n < 6; n++) dampC += Esh[0][84 + n] * Es[n] * Es[n];
+                for (int n = 0; n < 6; n++) dampC += Esh[0][48 + n] * Es[n] * Es[n];
             }
         }
         const float* qw = w.qwf + ((size_t)s * HW + p) * 3;
@@ -645,10 +629,7 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_b_kernel(BAPtrs base
             const float a = pa[i], dzf = pdzf[i], mu = pmu[i], gwz = pgwz[i], gC = pgC[i], Q = pQ[i];
             const float rr[2] = {__ldg(tp + p) - (fx * J.P[0] * iz + cx), __ldg(tp + HW + p) - (fy * J.P[1] * iz + cy)};
             const float wc[2] = {0.001f * __ldg(wp + p), 0.001f * __ldg(wp + HW + p)};
-            // the edge's fixed directions lam, dxi, dxi~ and the per-pixel damping direction beta
-            DirPix D[4];
-#pragma unroll
-            for (int dir = 0; dir < 3; dir++) dir_pix(Eq, X, J.P, Eq + 48 + 12 * dir, D[dir]);
+            // the per-pixel damping direction beta (slot E values of this edge's two poses)
             float beta[12];
             {
                 float tv[6];
@@ -673,28 +654,28 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_b_kernel(BAPtrs base
 #pragma unroll
                 for (int n = 0; n < 6; n++) {
                     const float es = pEs[n * CH + i];
-                    beta[n] = 2.f * Q * Eq[84 + n] * es;
-                    beta[6 + n] = 2.f * Q * Eq[90 + n] * (stereo ? es : tv[n]);
+                    beta[n] = 2.f * Q * Eq[48 + n] * es;
+                    beta[6 + n] = 2.f * Q * Eq[54 + n] * (stereo ? es : tv[n]);
                 }
             }
-            dir_pix(Eq, X, J.P, beta, D[3]);
             float g0h[3] = {0.f, 0.f, 0.f}, g0x[3] = {0.f, 0.f, 0.f}, om[3] = {0.f, 0.f, 0.f}, g4[3] = {0.f, 0.f, 0.f};
             float gdp = 0.f;
 #pragma unroll
             for (int ch = 0; ch < 2; ch++) {
                 const float* g = J.gf[ch];
                 const float fxy = ch == 0 ? fx : fy;
-                float ft[3];
-#pragma unroll
-                for (int dir = 0; dir < 3; dir++) ft[dir] = g[0] * D[dir].Pt[0] + g[1] * D[dir].Pt[1] + g[2] * D[dir].Pt[2];
-                const float fjz = J.jz[ch];
-                const float fb = g[0] * D[3].Pt[0] + g[1] * D[3].Pt[1] + g[2] * D[3].Pt[2];  // J . beta
-                float gam[12], fg = 0.f;  // damping direction of the B diagonal: lm lam dxi * J
+                // J . v for the edge's directions lam, dxi, dxi~, beta and the damping sum lm lam dxi J^2
+                float ft[3] = {0.f, 0.f, 0.f}, fb = 0.f, fg = 0.f;
 #pragma unroll
                 for (int n = 0; n < 12; n++) {
-                    gam[n] = Eq[84 + n] * J.J[ch][n];
-                    fg += gam[n] * J.J[ch][n];
+                    const float jn = J.J[ch][n];
+                    ft[0] += jn * Eq[12 + n];
+                    ft[1] += jn * Eq[24 + n];
+                    ft[2] += jn * Eq[36 + n];
+                    fb += jn * beta[n];
+                    fg += Eq[48 + n] * jn * jn;
                 }
+                const float fjz = J.jz[ch];
                 const float wpc = stereo ? 0.f : wc[ch];
                 const float A = act * act * wc[ch];
                 const float G3 = -dzf * ft[0] + mu * ft[1] - a * ft[2];
@@ -703,8 +684,8 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_b_kernel(BAPtrs base
                 const float c2 = -wpc * ft[0] + A * fjz * mu;
                 const float c3 = -A * fjz * a;
                 const float c4 = A * (gwz * rr[ch] + 2.f * gC * fjz + G3 + fb);
-                const float cB = -2.f * wpc;
-                const float cE = A * fjz;
+                const float cB = -2.f * wpc;  // along gamma = lm lam dxi o J
+                const float cE = A * fjz;     // along beta
                 gtp[(size_t)ch * HW + p] += wpc * ft[0] + A * gwz * fjz;
                 gwp[(size_t)ch * HW + p] +=
                     0.001f * ((stereo ? 0.f : ft[0] * (rr[ch] - ft[1]) - fg) +
@@ -715,19 +696,20 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_b_kernel(BAPtrs base
                     g0h[r] += c0 * g[r];
                     g4[r] += c4 * g[r];
                 }
-                // depth t-direction: h part with Pt = t, ft = Jz
-                g0h[ch] += c4 * (-fxy * iz2 * Eq[4 * 2 + 3]);
+                g0h[ch] += c4 * (-fxy * iz2 * Eq[11]);
                 g0h[2] += c4 * (fxy * iz2 * Eq[4 * ch + 3] - 2.f * iz * fjz);
-                // pose-type directions
-                gdp += mixed(J, ch, fxy, Eq + 48, D[0], ft[0], c1, g0h, g0x, om);
-                gdp += mixed(J, ch, fxy, Eq + 60, D[1], ft[1], c2, g0h, g0x, om);
-                gdp += mixed(J, ch, fxy, Eq + 72, D[2], ft[2], c3, g0h, g0x, om);
-                gdp += mixed(J, ch, fxy, beta, D[3], fb, cE, g0h, g0x, om);
-                if (!stereo) {
-                    DirPix Dg;
-                    dir_pix(Eq, X, J.P, gam, Dg);
-                    gdp += mixed(J, ch, fxy, gam, Dg, fg, cB, g0h, g0x, om);
-                }
+                // every tangent direction enters linearly: one combined direction
+                float ud[12];
+#pragma unroll
+                for (int n = 0; n < 12; n++)
+                    ud[n] = c1 * Eq[12 + n] + c2 * Eq[24 + n] + c3 * Eq[36 + n] + cE * beta[n] +
+                            cB * Eq[48 + n] * J.J[ch][n];
+                float fu = 0.f;
+#pragma unroll
+                for (int n = 0; n < 12; n++) fu += J.J[ch][n] * ud[n];
+                DirPix D;
+                dir_pix(Eq, X, J.P, ud, D);
+                gdp += mixed(J, ch, fxy, ud, D, fu, 1.f, g0h, g0x, om);
             }
             // depth s-direction of this pixel: Ps = t (column 3 of M0)
             gdp += g0h[0] * Eq[3] + g0h[1] * Eq[7] + g0h[2] * Eq[11];
@@ -863,7 +845,7 @@ extern "C" int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const
     size_t smem_b = 0;
     for (const auto& gd : plan->gds) smem_b = std::max(smem_b, (size_t)kPixF * gd.d.chunk_f * sizeof(float));
     if (smem_b > (size_t)kPixF * kAdjMaxChunk * sizeof(float)) {
-        set_last_error("vipe_slam_ba_batch_backward: pixel chunk beyond 3072 (use more frame_chunks)");
+        set_last_error("vipe_slam_ba_batch_backward: pixel chunk beyond 1536 (use more frame_chunks)");
         return VIPE_ERR_CAPACITY;
     }
     cudaStream_t st = as_stream(stream);
