@@ -3,6 +3,7 @@
     python -m vipe_b200.run_case ba1 --reps 2        # 64 keyframes, 628 edges, 4 LM iterations
     python -m vipe_b200.run_case ba0                 # 8 keyframes, 26 edges, 2 LM iterations
     python -m vipe_b200.run_case corr_build --edges 64
+    python -m vipe_b200.run_case batch --clips 32    # batched forward + adjoint, 4 LM iterations
 
 Every repetition runs the full operation on fresh inputs; the process exits 0
 only if every call returned success.
@@ -42,14 +43,47 @@ def run_corr_build(edges: int, reps: int) -> None:
     torch.cuda.synchronize()
 
 
+def run_batch(clips: int, reps: int) -> None:
+    from . import _lib
+    from . import workloads as W
+    from .ba_batch import BatchPlan
+
+    b = W.make_ba_batch(clips, seed=1004, device="cuda")
+    plan = BatchPlan(*b.sizes, b.ht, b.wd, "cuda", adjoint=True)
+    it = 4
+    tape = plan.make_tape(it)
+    T = b.tensors
+    g = torch.Generator(device="cuda").manual_seed(1005)
+    for _ in range(reps):
+        s = {k: v.clone() for k, v in T.items()}
+        _, _, _, st = plan.solve(**s, iterations=it, lm=1e-4, ep=0.1, tape=tape)
+        gp = torch.randn(plan.total_frames, 7, generator=g, device="cuda")
+        gp[:, 6] = 0
+        gd = torch.randn(plan.total_frames, b.ht, b.wd, generator=g, device="cuda")
+        out = [torch.empty_like(T[k]) for k in ("targets", "weights", "eta", "disps_sens")]
+        st2 = torch.zeros(plan.G, dtype=torch.int32, device="cuda")
+        rc = _lib.load().vipe_slam_ba_batch_backward(
+            plan._h, *[t.data_ptr() for t in tape], s["intrinsics"].data_ptr(), s["disps_sens"].data_ptr(),
+            s["targets"].data_ptr(), s["weights"].data_ptr(), s["eta"].data_ptr(), s["ii"].data_ptr(),
+            s["jj"].data_ptr(), s["depth_active"].data_ptr(), it, 1e-4, 0.1, 0.001, gp.data_ptr(), gd.data_ptr(),
+            *[o.data_ptr() for o in out], st2.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        _lib.check(rc, "batch backward")
+        torch.cuda.synchronize()
+        if int(st.abs().sum()) or int(st2.abs().sum()):
+            raise RuntimeError("device status set")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["ba0", "ba1", "corr_build"])
+    ap.add_argument("case", choices=["ba0", "ba1", "corr_build", "batch"])
+    ap.add_argument("--clips", type=int, default=32)
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--edges", type=int, default=64)
     a = ap.parse_args()
     if a.case in ("ba0", "ba1"):
         run_ba(a.case, a.reps)
+    elif a.case == "batch":
+        run_batch(a.clips, a.reps)
     else:
         run_corr_build(a.edges, a.reps)
     print("ok")
