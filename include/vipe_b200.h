@@ -157,6 +157,12 @@ int vipe_slam_ba_extended_noalloc(float* poses_io, float* disps_io, float* intri
  * edge_chunks / frame_chunks: pixel chunks per edge / per depth frame for the
  * linearisation kernels (0 = chosen from the batch size).  with_adjoint: also
  * reserve the buffers of vipe_slam_ba_batch_backward.
+ * group_id: 3 = SE3 (poses (.., 7), dx (.., 6)), or 4 = Sim3: poses (.., 8)
+ * [tx ty tz qx qy qz qw s], dx (.., 7) [tau phi sigma], the same residuals,
+ * weights, masks and solver with 7x7 pose blocks and retraction
+ * T <- Exp(dx) T in Sim3 (no counterpart in the reference, whose fused BA is
+ * SE3-only); window sizes up to 109 poses; no focal-length optimisation and no
+ * adjoint for Sim3.
  * tape_poses, tape_disps, tape_factor, tape_dx (optional, all or none): the
  * record the backward pass reads — per iteration the state entering it,
  * (iterations, sum frames, 7) and (iterations, sum frames, ht, wd), the
@@ -165,7 +171,7 @@ int vipe_slam_ba_extended_noalloc(float* poses_io, float* disps_io, float* intri
 typedef struct vipe_ba_batch_plan vipe_ba_batch_plan;
 int vipe_slam_ba_batch_plan_create(int num_graphs, const int* num_frames, const int* num_edges, const int* num_kx,
                                    const int* t0, const int* t1, int ht, int wd, int edge_chunks, int frame_chunks,
-                                   int with_adjoint, vipe_ba_batch_plan** plan_out);
+                                   int group_id, int with_adjoint, vipe_ba_batch_plan** plan_out);
 size_t vipe_slam_ba_batch_workspace_size(const vipe_ba_batch_plan* plan);
 /* totals_out[5] = {sum frames, sum edges, sum kx, sum (t1-t0), doubles of one
  * iteration of the factor tape} */

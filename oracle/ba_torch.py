@@ -15,7 +15,9 @@ with it False (as the CUDA adjoint does) the damping's dependence on diag(S) is
 differentiated as well.
 
 Poses use lietorch's SE3 layout [tx ty tz qx qy qz qw] (world-to-camera), and
-tangent vectors [tau, phi]; gradients with respect to poses are taken as left
+tangent vectors [tau, phi]; Sim3 poses (N, 8) [t q s] with tangents [tau, phi,
+sigma] select the Sim3 form (no counterpart in the reference, whose fused BA is
+SE3-only: the same residuals, weights and solver with 7x7 pose blocks); gradients with respect to poses are taken as left
 tangent perturbations T -> Exp(eps) T (see ``perturb``).
 """
 
@@ -86,6 +88,60 @@ def se3_log(X):
     return torch.cat([tau, phi], -1)
 
 
+# ---------------------------------------------------------------- Sim3 [t q s], tangent [tau phi sigma]
+
+def sim3_mul(X, Y):
+    t = X[..., :3] + X[..., 7:8] * quat_rot(X[..., 3:7], Y[..., :3])
+    return torch.cat([t, quat_mul(X[..., 3:7], Y[..., 3:7]), X[..., 7:8] * Y[..., 7:8]], -1)
+
+
+def sim3_inv(X):
+    qi = X[..., 3:7] * X.new_tensor([-1.0, -1.0, -1.0, 1.0])
+    si = 1.0 / X[..., 7:8]
+    return torch.cat([-si * quat_rot(qi, X[..., :3]), qi, si], -1)
+
+
+def _sim3_W(phi, sig):
+    """3x3 W(phi, sigma) of the Sim3 exponential (translation = W tau), closed form with
+    the small-angle / small-scale limits (the published Sim3 exponential used by lietorch)."""
+    th = torch.linalg.norm(phi)
+    Ph = torch.zeros(3, 3, dtype=phi.dtype)
+    Ph[0, 1], Ph[0, 2], Ph[1, 0], Ph[1, 2], Ph[2, 0], Ph[2, 1] = -phi[2], phi[1], phi[2], -phi[0], -phi[1], phi[0]
+    P2 = Ph @ Ph
+    sc = torch.exp(sig)
+    eps = 1e-6
+    if abs(float(sig)) < eps:
+        C = torch.ones((), dtype=phi.dtype)
+        if float(th) < eps:
+            A, B = 0.5 * C, C / 6.0
+        else:
+            A = (1 - torch.cos(th)) / (th * th)
+            B = (th - torch.sin(th)) / th**3
+    else:
+        C = (sc - 1) / sig
+        if float(th) < eps:
+            s2 = sig * sig
+            A = ((sig - 1) * sc + 1) / s2
+            B = (sc * 0.5 * s2 + sc - 1 - sig * sc) / (s2 * sig)
+        else:
+            a = sc * torch.sin(th)
+            b = sc * torch.cos(th)
+            c = th * th + sig * sig
+            A = (a * sig + (1 - b) * th) / (th * c)
+            B = (C - ((b - 1) * sig + a * th) / c) / (th * th)
+    return A * Ph + B * P2 + C * torch.eye(3, dtype=phi.dtype)
+
+
+def sim3_exp(xi):
+    """(P, 7) -> (P, 8)"""
+    out = []
+    for r in xi:
+        q = se3_exp(torch.cat([torch.zeros(3, dtype=r.dtype), r[3:6]]))[3:]
+        t = _sim3_W(r[3:6], r[6]) @ r[:3]
+        out.append(torch.cat([t, q, torch.exp(r[6:7])]))
+    return torch.stack(out)
+
+
 def perturb(poses, eps):
     """Left tangent perturbation Exp(eps) * poses (eps (N, 6); eps = 0 gives poses)."""
     return se3_mul(se3_exp(eps), poses)
@@ -119,24 +175,30 @@ def ba_torch(poses, disps, intrinsics, disps_sens, targets, weights, eta, ii, jj
     act_f = depth_active.to(dt)
     poses = poses.to(dt)
     disps = disps.to(dt)
+    sim3 = poses.shape[-1] == 8
+    D = 7 if sim3 else 6
     dx = dz = None
     for _ in range(iterations):
-        Bm = torch.zeros(6 * P, 6 * P, dtype=dt)
-        vb = torch.zeros(6 * P, dtype=dt)
-        Em = [torch.zeros(6 * P, HW, dtype=dt) for _ in range(K)]
+        Bm = torch.zeros(D * P, D * P, dtype=dt)
+        vb = torch.zeros(D * P, dtype=dt)
+        Em = [torch.zeros(D * P, HW, dtype=dt) for _ in range(K)]
         Csum = [torch.zeros(HW, dtype=dt) for _ in range(K)]
         bsum = [torch.zeros(HW, dtype=dt) for _ in range(K)]
         for e in range(E):
             a, b = ii_l[e], jj_l[e]
+            sij = torch.ones((), dtype=dt)
             if a == b:
                 tij = torch.tensor([-0.1, 0.0, 0.0], dtype=dt)
                 qij = torch.tensor([0.0, 0.0, 0.0, 1.0], dtype=dt)
+            elif sim3:
+                Tij = sim3_mul(poses[b], sim3_inv(poses[a]))
+                tij, qij, sij = Tij[:3], Tij[3:7], Tij[7]
             else:
                 Tij = se3_mul(poses[b], se3_inv(poses[a]))
                 tij, qij = Tij[:3], Tij[3:]
             d = disps[a].reshape(-1)
             Xi = torch.stack([(uu - cx) / fx, (vv - cy) / fy, torch.ones_like(uu)], -1)
-            Xj = quat_rot(qij.expand(HW, 4), Xi) + d[:, None] * tij[None]
+            Xj = sij * quat_rot(qij.expand(HW, 4), Xi) + d[:, None] * tij[None]
             x, y, z, h = Xj[:, 0], Xj[:, 1], Xj[:, 2], d
             ok = (z >= MIN_DEPTH).detach()
             zi = torch.where(ok, 1.0 / torch.where(ok, z, torch.ones_like(z)), torch.zeros_like(z))
@@ -152,8 +214,19 @@ def ba_torch(poses, disps, intrinsics, disps_sens, targets, weights, eta, ii, jj
                                 fy * x * zi], -1)
             Jz_u = fx * (tij[0] * zi - tij[2] * x * zi2)
             Jz_v = fy * (tij[1] * zi - tij[2] * y * zi2)
-            Ji_u = -_adj_t(tij.expand(HW, 3), qij.expand(HW, 4), Jj_u)
-            Ji_v = -_adj_t(tij.expand(HW, 3), qij.expand(HW, 4), Jj_v)
+            if sim3:
+                # target: tau d grad f, phi P x grad f, sigma 0; source: -d g, -(X3 x g), -X3.g, g = s R^T grad f
+                qc = qij * qij.new_tensor([-1.0, -1.0, -1.0, 1.0])
+                rows = []
+                for gf in (torch.stack([fx * zi, zero, -fx * x * zi2], -1), torch.stack([zero, fy * zi, -fy * y * zi2], -1)):
+                    g = sij * quat_rot(qc.expand(HW, 4), gf)
+                    Ji = torch.cat([-h[:, None] * g, -torch.cross(Xi, g, dim=-1), -(Xi * g).sum(-1, keepdim=True)], -1)
+                    Jj = torch.cat([h[:, None] * gf, torch.cross(Xj, gf, dim=-1), zero[:, None]], -1)
+                    rows.append((Ji, Jj))
+                (Ji_u, Jj_u), (Ji_v, Jj_v) = rows
+            else:
+                Ji_u = -_adj_t(tij.expand(HW, 3), qij.expand(HW, 4), Jj_u)
+                Ji_v = -_adj_t(tij.expand(HW, 3), qij.expand(HW, 4), Jj_v)
             act = act_f[a]
             k = row_of[a]
             wpu, wpv = (wu * 0, wv * 0) if a == b else (wu, wv)
@@ -163,13 +236,13 @@ def ba_torch(poses, disps, intrinsics, disps_sens, targets, weights, eta, ii, jj
             if t0 <= b < t1:
                 slots.append((b - t0, Jj_u, Jj_v))
             for (pa, Ja_u, Ja_v) in slots:
-                vb = vb.index_add(0, torch.arange(6 * pa, 6 * pa + 6),
+                vb = vb.index_add(0, torch.arange(D * pa, D * pa + D),
                                   (wpu * ru)[:, None].mul(Ja_u).sum(0) + (wpv * rv)[:, None].mul(Ja_v).sum(0))
                 for (pb, Jb_u, Jb_v) in slots:
                     blk = (Ja_u * wpu[:, None]).T @ Jb_u + (Ja_v * wpv[:, None]).T @ Jb_v
-                    Bm = Bm.index_put((torch.arange(6 * pa, 6 * pa + 6)[:, None],
-                                       torch.arange(6 * pb, 6 * pb + 6)[None, :]), blk, accumulate=True)
-                Em[k] = Em[k].index_put((torch.arange(6 * pa, 6 * pa + 6),),
+                    Bm = Bm.index_put((torch.arange(D * pa, D * pa + D)[:, None],
+                                       torch.arange(D * pb, D * pb + D)[None, :]), blk, accumulate=True)
+                Em[k] = Em[k].index_put((torch.arange(D * pa, D * pa + D),),
                                         act * (act * wu * Jz_u)[None, :] * Ja_u.T
                                         + act * (act * wv * Jz_v)[None, :] * Ja_v.T, accumulate=True)
             Csum[k] = Csum[k] + act * wu * Jz_u * Jz_u + act * wv * Jz_v * Jz_v
@@ -192,11 +265,11 @@ def ba_torch(poses, disps, intrinsics, disps_sens, targets, weights, eta, ii, jj
         damp = ep + lm * (dg.detach() if detach_damping else dg)
         Sd = S + torch.diag(damp)
         dxi = torch.linalg.solve(Sd, yv)
-        mask_rows = torch.ones(6 * P, dtype=dt)
-        mask_rows[:6] = 0.0  # pose t0's rows are left out of the back-substitution
+        mask_rows = torch.ones(D * P, dtype=dt)
+        mask_rows[:D] = 0.0  # pose t0's rows are left out of the back-substitution
         dzv = Q * (wz - Ef.T @ (dxi * mask_rows))
-        dxf = dxi.view(P, 6)
-        newp = se3_mul(se3_exp(dxf), poses[t0:t1])
+        dxf = dxi.view(P, D)
+        newp = sim3_mul(sim3_exp(dxf), poses[t0:t1]) if sim3 else se3_mul(se3_exp(dxf), poses[t0:t1])
         poses = torch.cat([poses[:t0], newp, poses[t1:]], 0)
         dzr = dzv.view(K, H, W)
         idx = torch.tensor(kx)

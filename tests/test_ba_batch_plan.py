@@ -12,11 +12,11 @@ def _ints(xs):
     return (ctypes.c_int * len(xs))(*xs)
 
 
-def _plan(nf, ne, nk, t0, t1, ht=48, wd=64, ec=0, fc=0):
+def _plan(nf, ne, nk, t0, t1, ht=48, wd=64, ec=0, fc=0, group=3, adjoint=0):
     lib = _lib.load()
     h = ctypes.c_void_p()
     rc = lib.vipe_slam_ba_batch_plan_create(len(nf), _ints(nf), _ints(ne), _ints(nk), _ints(t0), _ints(t1), ht, wd,
-                                            ec, fc, 0, ctypes.byref(h))
+                                            ec, fc, group, adjoint, ctypes.byref(h))
     return rc, h
 
 
@@ -72,3 +72,20 @@ def test_batch_generator_layout():
         eo += b.num_edges[g]
     p = b.clip(1)
     assert p.poses.shape[0] == b.num_frames[1] and p.ii.shape[0] == b.num_edges[1]
+
+
+def test_plan_groups():
+    sz = ([8, 10], [26, 34], [6, 8], [2, 2], [8, 10])
+    rc, h = _plan(*sz, group=4)
+    assert rc == 0
+    lib = _lib.load()
+    tot = (ctypes.c_int64 * 5)()
+    lib.vipe_slam_ba_batch_totals(h, tot)
+    rc3, h3 = _plan(*sz, group=3)
+    assert lib.vipe_slam_ba_batch_workspace_size(h) > lib.vipe_slam_ba_batch_workspace_size(h3)  # 7x7 blocks
+    lib.vipe_slam_ba_batch_plan_destroy(h)
+    lib.vipe_slam_ba_batch_plan_destroy(h3)
+    assert _plan(*sz, group=5)[0] == _lib.VIPE_ERR_GROUP
+    assert _plan(*sz, group=4, adjoint=1)[0] == _lib.VIPE_ERR_GROUP
+    # Sim3 windows are limited to 109 poses (7 P + 1 unknowns in the staged Cholesky panel)
+    assert _plan([120], [200], [118], [2], [120], group=4)[0] == _lib.VIPE_ERR_CAPACITY

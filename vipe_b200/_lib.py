@@ -41,7 +41,7 @@ _SIGS: dict[str, tuple] = {
         I,
         [P, P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, F, I, F, I, F, F, F, I, P, P, P, P, P],
     ),
-    "vipe_slam_ba_batch_plan_create": (I, [I, P, P, P, P, P, I, I, I, I, I, P]),
+    "vipe_slam_ba_batch_plan_create": (I, [I, P, P, P, P, P, I, I, I, I, I, I, P]),
     "vipe_slam_ba_batch_workspace_size": (SZ, [P]),
     "vipe_slam_ba_batch_totals": (I, [P, P]),
     "vipe_slam_ba_batch_bind": (I, [P, P, SZ, P]),
@@ -85,6 +85,7 @@ VIPE_ERR_INDEX = 2
 VIPE_ERR_RANGE = 3
 VIPE_ERR_KX_MISMATCH = 4
 VIPE_ERR_CAPACITY = 6
+VIPE_ERR_GROUP = 9
 VIPE_WARN_SOLVER = 16
 
 # dtypes (enum vipe_dtype)

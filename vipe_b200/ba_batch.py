@@ -36,7 +36,7 @@ class BatchPlan:
     """A bound plan: graph table uploaded into a device workspace on `device`."""
 
     def __init__(self, num_frames, num_edges, num_kx, t0, t1, ht: int, wd: int, device, edge_chunks: int = 0,
-                 frame_chunks: int = 0, adjoint: bool = False):
+                 frame_chunks: int = 0, adjoint: bool = False, group: str = "se3"):
         lib = _lib.load()
         self.G = len(num_frames)
         if not (len(num_edges) == len(num_kx) == len(t0) == len(t1) == self.G) or self.G == 0:
@@ -49,10 +49,14 @@ class BatchPlan:
                       tuple(map(int, t0)), tuple(map(int, t1)))
         self.edge_chunks, self.frame_chunks = int(edge_chunks), int(frame_chunks)
         self.adjoint = bool(adjoint)
+        if group not in ("se3", "sim3"):
+            raise RuntimeError("BatchPlan: group must be 'se3' or 'sim3'")
+        self.group = group
+        self.dof = 7 if group == "sim3" else 6
         h = ctypes.c_void_p()
         rc = lib.vipe_slam_ba_batch_plan_create(self.G, _ints(num_frames), _ints(num_edges), _ints(num_kx), _ints(t0),
                                                 _ints(t1), self.ht, self.wd, self.edge_chunks, self.frame_chunks,
-                                                int(self.adjoint), ctypes.byref(h))
+                                                3 if group == "se3" else 4, int(self.adjoint), ctypes.byref(h))
         _lib.check(rc, "BatchPlan")
         self._h = h
         tot = (ctypes.c_int64 * 5)()
@@ -84,7 +88,7 @@ class BatchPlan:
     def _check(self, poses, disps, intrinsics, disps_sens, targets, weights, eta, ii, jj, depth_active):
         HW = (self.ht, self.wd)
         want = {
-            "poses": (poses, (self.total_frames, 7), torch.float32),
+            "poses": (poses, (self.total_frames, self.dof + 1), torch.float32),
             "disps": (disps, (self.total_frames, *HW), torch.float32),
             "intrinsics": (intrinsics, (self.G, 4), torch.float32),
             "disps_sens": (disps_sens, (self.total_frames, *HW), torch.float32),
@@ -108,14 +112,14 @@ class BatchPlan:
         """Buffers of the record the backward pass reads: per iteration the state
         entering it (poses, disps), the factorised reduced system and the pose step."""
         dev, it = self.device, int(iterations)
-        return (torch.empty(it, self.total_frames, 7, dtype=torch.float32, device=dev),
+        return (torch.empty(it, self.total_frames, self.dof + 1, dtype=torch.float32, device=dev),
                 torch.empty(it, self.total_frames, self.ht, self.wd, dtype=torch.float32, device=dev),
                 torch.empty(it, max(1, self.factor_tape_doubles), dtype=torch.float64, device=dev),
-                torch.empty(it, max(1, self.total_poses), 6, dtype=torch.float32, device=dev))
+                torch.empty(it, max(1, self.total_poses), self.dof, dtype=torch.float32, device=dev))
 
     def outputs(self, iterations: int, motion_only: bool = False, compute_energy: bool = False):
         dev = self.device
-        dx = torch.zeros(self.total_poses, 6, dtype=torch.float32, device=dev)
+        dx = torch.zeros(self.total_poses, self.dof, dtype=torch.float32, device=dev)
         dz = None if motion_only else torch.empty(self.total_kx, self.ht * self.wd, dtype=torch.float32, device=dev)
         energy = torch.zeros(self.G, iterations if compute_energy else 0, dtype=torch.float32, device=dev)
         status = torch.zeros(self.G, dtype=torch.int32, device=dev)
@@ -126,7 +130,7 @@ class BatchPlan:
               intrinsics_ep=1e-6, intrinsics_scale=1.0, compute_energy=False, out=None, check=True, tape=None):
         """LM iterations on every graph; poses/disps/intrinsics are updated in place.
 
-        Returns (dx, dz, energy, status): dx (sum P, 6), dz (sum K, H*W) or None,
+        Returns (dx, dz, energy, status): dx (sum P, 6 or 7), dz (sum K, H*W) or None,
         energy (G, iterations) or (G, 0), status (G,) int32 device words
         (0, a vipe_status error, or VIPE_WARN_SOLVER when that graph's Cholesky
         failed and its dx is 0).  ``out`` reuses preallocated outputs (for
@@ -216,19 +220,19 @@ CANDIDATES = ((1, 1), (2, 1), (1, 2), (2, 2), (3, 2), (3, 4))
 
 
 def autotune(plan_sizes: tuple, ht: int, wd: int, batch: dict, iterations: int, lm: float, ep: float, device,
-             candidates=CANDIDATES, reps: int = 3, **kw) -> TuneResult:
+             candidates=CANDIDATES, reps: int = 3, group: str = "se3", **kw) -> TuneResult:
     """Times each (edge_chunks, frame_chunks) candidate on copies of `batch` and returns the fastest.
 
     plan_sizes = (num_frames, num_edges, num_kx, t0, t1) lists.  Results are
     cached per (sizes, ht, wd, iterations, motion_only)."""
-    key = (tuple(tuple(x) for x in plan_sizes), ht, wd, int(iterations), bool(kw.get("motion_only", False)))
+    key = (tuple(tuple(x) for x in plan_sizes), ht, wd, int(iterations), bool(kw.get("motion_only", False)), group)
     if key in _TUNE_CACHE:
         return _TUNE_CACHE[key]
     mutable = ("poses", "disps", "intrinsics")
     work = {k: (v.clone() if k in mutable else v) for k, v in batch.items()}
     table = []
     for ec, fc in candidates:
-        plan = BatchPlan(*plan_sizes, ht, wd, device, edge_chunks=ec, frame_chunks=fc)
+        plan = BatchPlan(*plan_sizes, ht, wd, device, edge_chunks=ec, frame_chunks=fc, group=group)
         out = plan.outputs(iterations, kw.get("motion_only", False), kw.get("compute_energy", False))
         times = []
         for r in range(reps + 1):

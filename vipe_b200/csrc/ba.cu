@@ -38,6 +38,7 @@
 // skips rows whose pose is t0 (geom_kernels.cu:1186), retraction order.
 
 #include "ba_internal.cuh"
+#include "lie_group.cuh"
 #include "se3_device.cuh"
 
 #include <algorithm>
@@ -213,8 +214,8 @@ __global__ void __launch_bounds__(kIndexThreads)
         if (lane == 0) {
             w.fe_ptr[s] = deg;
             w.fp_ptr[s] = m;
-            w.ftile_off[s] = npt_of(m);
-            if (m > kMaxSlots) atomicOr(&sh_flag, 2);
+            w.ftile_off[s] = npt_of(m, d.dof);
+            if (m > max_slots(d.dof)) atomicOr(&sh_flag, 2);
         }
     }
     __syncthreads();
@@ -341,27 +342,153 @@ __global__ void __launch_bounds__(kIndexThreads)
     }
 }
 
+// ---------------------------------------------------------------- pose groups
+//
+// SE3 (D = 6) keeps the reference's per-pixel formulas (se3_device.cuh).  Sim3
+// (D = 7, poses (N, 8) [t q s], tangent [tau phi sigma]; no counterpart in the
+// reference's fused BA, whose kernels are SE3-only) uses the same residual,
+// weighting, depth mask and stereo rule with the relative pose
+// Tij = Tj Ti^-1 acting on X = (x, y, 1, d) as X' = s R X3 + t d:
+//   target pose  tau: d grad f,  phi: P x grad f,  sigma: grad f . P = 0
+//   source pose  tau: -d g,  phi: -(X3 x g),  sigma: -X3 . g   with g = s R^T grad f
+//   depth        grad f . t
+// (the source rows equal -J_target Ad(Tij), Ad the Sim3 adjoint).
+
+struct PixelLin7 {
+    float Ji[2][7];
+    float Jj[2][7];
+    float Jz[2];
+    float w[2];
+    float wd[2];
+    float we[2];
+    float r[2];
+    float Jf[2];
+};
+
+template <int D>
+struct LinOf;
+template <>
+struct LinOf<6> {
+    using T = PixelLin;
+};
+template <>
+struct LinOf<7> {
+    using T = PixelLin7;
+};
+
+struct EdgeTf {
+    float t[3], q[4], s;
+};
+
+template <int D>
+__device__ __forceinline__ void edge_tf(const float* poses, int a, int b, EdgeTf& T) {
+    if (D == 6) {
+        edge_pose(poses, a, b, T.t, T.q);
+        T.s = 1.f;
+    } else if (a == b) {
+        T.t[0] = -0.1f; T.t[1] = 0.f; T.t[2] = 0.f;
+        T.q[0] = 0.f; T.q[1] = 0.f; T.q[2] = 0.f; T.q[3] = 1.f;
+        T.s = 1.f;
+    } else {
+        float pi[8], pj[8];
+#pragma unroll
+        for (int n = 0; n < 8; n++) {
+            pi[n] = __ldg(poses + 8 * a + n);
+            pj[n] = __ldg(poses + 8 * b + n);
+        }
+        const lie::Sim3<float> G = lie::Sim3<float>::load(pj) * lie::Sim3<float>::load(pi).inv();
+        T.t[0] = G.t[0]; T.t[1] = G.t[1]; T.t[2] = G.t[2];
+        T.q[0] = G.r.q.x; T.q[1] = G.r.q.y; T.q[2] = G.r.q.z; T.q[3] = G.r.q.w;
+        T.s = G.r.s;
+    }
+}
+
+template <bool kResidual>
+__device__ __forceinline__ void linearize_sim3(const EdgeTf& T, bool stereo, float fx, float fy, float cx, float cy,
+                                               float u, float v, float disp, float wu_in, float wv_in, float tu,
+                                               float tv, float act, PixelLin7& L) {
+    const float X3[3] = {(u - cx) / fx, (v - cy) / fy, 1.0f};
+    float RX[3];
+    qrot(T.q, X3, RX);
+    const float P[3] = {T.s * RX[0] + T.t[0] * disp, T.s * RX[1] + T.t[1] * disp, T.s * RX[2] + T.t[2] * disp};
+    const bool ok = !(P[2] < 0.25f);
+    const float iz = ok ? 1.0f / P[2] : 0.0f;
+    const float iz2 = iz * iz;
+    const float wu = ok ? 0.001f * wu_in : 0.0f;
+    const float wv = ok ? 0.001f * wv_in : 0.0f;
+    if (kResidual) {
+        L.r[0] = tu - (fx * P[0] * iz + cx);
+        L.r[1] = tv - (fy * P[1] * iz + cy);
+    } else {
+        L.r[0] = 0.0f;
+        L.r[1] = 0.0f;
+    }
+    const float qc[4] = {-T.q[0], -T.q[1], -T.q[2], T.q[3]};
+#pragma unroll
+    for (int ch = 0; ch < 2; ch++) {
+        const float gfv[3] = {ch == 0 ? fx * iz : 0.0f, ch == 0 ? 0.0f : fy * iz,
+                              ch == 0 ? -fx * P[0] * iz2 : -fy * P[1] * iz2};
+        float g[3];
+        qrot(qc, gfv, g);
+        g[0] *= T.s; g[1] *= T.s; g[2] *= T.s;
+        L.Ji[ch][0] = -disp * g[0];
+        L.Ji[ch][1] = -disp * g[1];
+        L.Ji[ch][2] = -disp * g[2];
+        L.Ji[ch][3] = -(X3[1] * g[2] - X3[2] * g[1]);
+        L.Ji[ch][4] = -(X3[2] * g[0] - X3[0] * g[2]);
+        L.Ji[ch][5] = -(X3[0] * g[1] - X3[1] * g[0]);
+        L.Ji[ch][6] = -(X3[0] * g[0] + X3[1] * g[1] + X3[2] * g[2]);
+        L.Jj[ch][0] = disp * gfv[0];
+        L.Jj[ch][1] = disp * gfv[1];
+        L.Jj[ch][2] = disp * gfv[2];
+        L.Jj[ch][3] = P[1] * gfv[2] - P[2] * gfv[1];
+        L.Jj[ch][4] = P[2] * gfv[0] - P[0] * gfv[2];
+        L.Jj[ch][5] = P[0] * gfv[1] - P[1] * gfv[0];
+        L.Jj[ch][6] = 0.0f;
+        L.Jz[ch] = gfv[0] * T.t[0] + gfv[1] * T.t[1] + gfv[2] * T.t[2];
+        L.Jf[ch] = 0.0f;
+    }
+    L.we[0] = wu;
+    L.we[1] = wv;
+    L.wd[0] = wu * act;
+    L.wd[1] = wv * act;
+    L.w[0] = stereo ? 0.0f : wu;
+    L.w[1] = stereo ? 0.0f : wv;
+}
+
+template <int D, bool kIntr, bool kResidual>
+__device__ __forceinline__ void linearize_d(const EdgeTf& T, bool stereo, float fx, float fy, float cx, float cy,
+                                            float u, float v, float disp, float wu, float wv, float tu, float tv,
+                                            float act, float iscale, typename LinOf<D>::T& L) {
+    if constexpr (D == 6)
+        linearize<kIntr, kResidual>(T.t, T.q, stereo, fx, fy, cx, cy, u, v, disp, wu, wv, tu, tv, act, iscale, L);
+    else
+        linearize_sim3<kResidual>(T, stereo, fx, fy, cx, cy, u, v, disp, wu, wv, tu, tv, act, L);
+}
+
 // ---------------------------------------------------------------- per-edge terms
 
-template <bool kIntr>
+template <bool kIntr, int D>
 __global__ void __launch_bounds__(kEdgeThreads) ba_edge_kernel(BAPtrs base, Batch B, float iscale) {
     BA_BIND(B, base);
     if (w.status[0]) return;
     const EdgeArgs A{io.poses, io.disps, io.intr, io.targets, io.weights, io.ii, io.jj, iscale};
-    __shared__ float red[kEdgeThreads / 32][kNE];
+    constexpr int NH = D * (D + 1) / 2;
+    constexpr int NE = NH + 2 * D + 3;
+    __shared__ float red[kEdgeThreads / 32][NE];
     const int e = local_ % d.E, c = local_ / d.E;
     const int a = (int)A.ii[e], b = (int)A.jj[e];
     const bool stereo = a == b;
-    float tij[3], qij[4];
-    edge_pose(A.poses, a, b, tij, qij);
+    EdgeTf Tf;
+    edge_tf<D>(A.poses, a, b, Tf);
     const float fx = A.intr[0], fy = A.intr[1], cx = A.intr[2], cy = A.intr[3];
 
-    float H[21], vj[6], fj[6];
+    float H[NH], vj[D], fj[D];
     float hf = 0.f, vf = 0.f, en = 0.f;
 #pragma unroll
-    for (int n = 0; n < 21; n++) H[n] = 0.f;
+    for (int n = 0; n < NH; n++) H[n] = 0.f;
 #pragma unroll
-    for (int n = 0; n < 6; n++) {
+    for (int n = 0; n < D; n++) {
         vj[n] = 0.f;
         fj[n] = 0.f;
     }
@@ -372,121 +499,149 @@ __global__ void __launch_bounds__(kEdgeThreads) ba_edge_kernel(BAPtrs base, Batc
     const float* dp = A.disps + (size_t)a * HW;
     for (int p = p0 + threadIdx.x; p < p1; p += kEdgeThreads) {
         const float u = (float)(p % W), v = (float)(p / W);
-        PixelLin L;
-        linearize<kIntr, true>(tij, qij, stereo, fx, fy, cx, cy, u, v, __ldg(dp + p), __ldg(wu + p),
-                               __ldg(wu + HW + p), __ldg(tu + p), __ldg(tu + HW + p), 1.0f, A.iscale, L);
+        typename LinOf<D>::T L;
+        linearize_d<D, kIntr, true>(Tf, stereo, fx, fy, cx, cy, u, v, __ldg(dp + p), __ldg(wu + p),
+                                    __ldg(wu + HW + p), __ldg(tu + p), __ldg(tu + HW + p), 1.0f, A.iscale, L);
         en += L.we[0] * L.r[0] * L.r[0] + L.we[1] * L.r[1] * L.r[1];
 #pragma unroll
         for (int ch = 0; ch < 2; ch++) {
             const float wt = L.w[ch];
             int l = 0;
 #pragma unroll
-            for (int n = 0; n < 6; n++) {
+            for (int n = 0; n < D; n++) {
                 const float wjn = wt * L.Jj[ch][n];
 #pragma unroll
                 for (int m = 0; m <= n; m++) H[l++] += wjn * L.Jj[ch][m];
             }
             const float wr = wt * L.r[ch];
 #pragma unroll
-            for (int n = 0; n < 6; n++) vj[n] += wr * L.Jj[ch][n];
+            for (int n = 0; n < D; n++) vj[n] += wr * L.Jj[ch][n];
             if (kIntr) {
                 const float wf = wt * L.Jf[ch];
 #pragma unroll
-                for (int n = 0; n < 6; n++) fj[n] += wf * L.Jj[ch][n];
+                for (int n = 0; n < D; n++) fj[n] += wf * L.Jj[ch][n];
                 hf += wf * L.Jf[ch];
                 vf += wr * L.Jf[ch];
             }
         }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float vals[kNE];
+    float vals[NE];
 #pragma unroll
-    for (int n = 0; n < 21; n++) vals[n] = H[n];
+    for (int n = 0; n < NH; n++) vals[n] = H[n];
 #pragma unroll
-    for (int n = 0; n < 6; n++) {
-        vals[21 + n] = vj[n];
-        vals[27 + n] = fj[n];
+    for (int n = 0; n < D; n++) {
+        vals[NH + n] = vj[n];
+        vals[NH + D + n] = fj[n];
     }
-    vals[33] = hf;
-    vals[34] = vf;
-    vals[35] = en;
+    vals[NH + 2 * D] = hf;
+    vals[NH + 2 * D + 1] = vf;
+    vals[NH + 2 * D + 2] = en;
 #pragma unroll
-    for (int n = 0; n < kNE; n++) {
-        if (!kIntr && n >= 27 && n < 35) continue;
+    for (int n = 0; n < NE; n++) {
+        if (!kIntr && n >= NH + D && n < NH + 2 * D + 2) continue;
         const float sv = warp_sum(vals[n]);
         if (lane == 0) red[warp][n] = sv;
     }
     __syncthreads();
-    for (int n = threadIdx.x; n < kNE; n += kEdgeThreads) {
+    for (int n = threadIdx.x; n < NE; n += kEdgeThreads) {
         float sv = 0.f;
-        if (kIntr || n < 27 || n == 35) {
+        if (kIntr || n < NH + D || n == NH + 2 * D + 2) {
 #pragma unroll
             for (int q = 0; q < kEdgeThreads / 32; q++) sv += red[q][n];
         }
-        w.epart[((size_t)e * d.CHe + c) * kNE + n] = sv;
+        w.epart[((size_t)e * d.CHe + c) * NE + n] = sv;
     }
 }
 
-// Chunk partials -> FP64 per-edge terms in the 12x12 layout (kNT values).
+// Chunk partials -> FP64 per-edge terms (nt_of(dof) values): the (2 dof)^2
+// block over J = [Ji, Jj] from Hjj and M = Ad(Tij)^T (Ji = -Jj Ad, so
+// Hii = M Hjj M^T, Hji = -Hjj M^T, vi = -M vj, fi = -M fj).
 __global__ void ba_edge_reduce(BAPtrs base, Batch B) {
     BA_BIND(B, base);
     if (w.status[0]) return;
     const EdgeArgs A{io.poses, io.disps, io.intr, io.targets, io.weights, io.ii, io.jj, 1.f};
-    __shared__ double t[kNE];
-    __shared__ double M[6][6];
+    __shared__ double t[kMaxNE];
+    __shared__ double M[7][7];
     const int e = local_, tid = threadIdx.x;
-    for (int n = tid; n < kNE; n += blockDim.x) {
+    const int D = d.dof, NH = D * (D + 1) / 2, NE = ne_of(D);
+    for (int n = tid; n < NE; n += blockDim.x) {
         double sv = 0.0;
-        for (int c = 0; c < d.CHe; c++) sv += (double)w.epart[((size_t)e * d.CHe + c) * kNE + n];
+        for (int c = 0; c < d.CHe; c++) sv += (double)w.epart[((size_t)e * d.CHe + c) * NE + n];
         t[n] = sv;
     }
-    if (tid < 6) {
-        float tij[3], qij[4];
-        edge_pose(A.poses, (int)A.ii[e], (int)A.jj[e], tij, qij);
-        float ek[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, col[6];
-        ek[tid] = 1.f;
-        adj_t(tij, qij, ek, col);
-        for (int r = 0; r < 6; r++) M[r][tid] = (double)col[r];
+    if (D == 6) {
+        if (tid < 6) {
+            float tij[3], qij[4];
+            edge_pose(A.poses, (int)A.ii[e], (int)A.jj[e], tij, qij);
+            float ek[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, col[6];
+            ek[tid] = 1.f;
+            adj_t(tij, qij, ek, col);
+            for (int r = 0; r < 6; r++) M[r][tid] = (double)col[r];
+        }
+    } else if (tid == 0) {
+        // Sim3 adjoint Ad = [[s R, [t]x R, -t], [0, R, 0], [0, 0, 1]]; M = Ad^T
+        EdgeTf T;
+        edge_tf<7>(A.poses, (int)A.ii[e], (int)A.jj[e], T);
+        const double x = T.q[0], y = T.q[1], z = T.q[2], qw = T.q[3];
+        const double R[3][3] = {{1 - 2 * (y * y + z * z), 2 * (x * y - qw * z), 2 * (x * z + qw * y)},
+                                {2 * (x * y + qw * z), 1 - 2 * (x * x + z * z), 2 * (y * z - qw * x)},
+                                {2 * (x * z - qw * y), 2 * (y * z + qw * x), 1 - 2 * (x * x + y * y)}};
+        const double tt[3] = {T.t[0], T.t[1], T.t[2]};
+        double Ad[7][7] = {};
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) {
+                Ad[r][c] = (double)T.s * R[r][c];
+                Ad[3 + r][3 + c] = R[r][c];
+                // ([t]x R)[r][c] = sum_k [t]x[r][k] R[k][c]
+                const double tx[3] = {r == 0 ? 0.0 : (r == 1 ? tt[2] : -tt[1]), r == 0 ? -tt[2] : (r == 1 ? 0.0 : tt[0]),
+                                      r == 0 ? tt[1] : (r == 1 ? -tt[0] : 0.0)};
+                Ad[r][3 + c] = tx[0] * R[0][c] + tx[1] * R[1][c] + tx[2] * R[2][c];
+            }
+        for (int r = 0; r < 3; r++) Ad[r][6] = -tt[r];
+        Ad[6][6] = 1.0;
+        for (int r = 0; r < 7; r++)
+            for (int c = 0; c < 7; c++) M[r][c] = Ad[c][r];
     }
     __syncthreads();
-    double* out = w.eterm + (size_t)e * kNT;
-    // full 12x12 over J = [Ji, Jj]: thread per (row, col) of the lower triangle
-    for (int q = tid; q < 78; q += blockDim.x) {
+    double* out = w.eterm + (size_t)e * nt_of(D);
+    // full (2D)x(2D) over J = [Ji, Jj]: thread per (row, col) of the lower triangle
+    for (int q = tid; q < tri_of(D); q += blockDim.x) {
         int r = 0;
         while ((r + 1) * (r + 2) / 2 <= q) r++;
         const int c = q - r * (r + 1) / 2;  // c <= r
         double v;
-        if (r >= 6 && c >= 6) {
-            v = t[tri6(r - 6, c - 6)];  // Hjj
-        } else if (r >= 6) {
-            // entry (Jj_{r-6}, Ji_c) = sum w Jj Ji = -(Hjj M^T)[r-6][c]
+        if (r >= D && c >= D) {
+            v = t[tri6(r - D, c - D)];  // Hjj
+        } else if (r >= D) {
+            // entry (Jj_{r-D}, Ji_c) = sum w Jj Ji = -(Hjj M^T)[r-D][c]
             double sacc = 0.0;
-            for (int k = 0; k < 6; k++) sacc += t[tri6(r - 6, k)] * M[c][k];
+            for (int k = 0; k < D; k++) sacc += t[tri6(r - D, k)] * M[c][k];
             v = -sacc;
         } else {
             // Hii = M Hjj M^T
             double sacc = 0.0;
-            for (int k = 0; k < 6; k++)
-                for (int l = 0; l < 6; l++) sacc += M[r][k] * t[tri6(k, l)] * M[c][l];
+            for (int k = 0; k < D; k++)
+                for (int l = 0; l < D; l++) sacc += M[r][k] * t[tri6(k, l)] * M[c][l];
             v = sacc;
         }
         out[q] = v;
     }
-    if (tid < 6) {
+    if (tid < D) {
         double vi = 0.0, fi = 0.0;
-        for (int k = 0; k < 6; k++) {
-            vi -= M[tid][k] * t[21 + k];
-            fi -= M[tid][k] * t[27 + k];
+        for (int k = 0; k < D; k++) {
+            vi -= M[tid][k] * t[NH + k];
+            fi -= M[tid][k] * t[NH + D + k];
         }
-        out[kTV + tid] = vi;
-        out[kTV + 6 + tid] = t[21 + tid];
-        out[kTF + tid] = fi;
-        out[kTF + 6 + tid] = t[27 + tid];
+        out[tv_of(D) + tid] = vi;
+        out[tv_of(D) + D + tid] = t[NH + tid];
+        out[tf_of(D) + tid] = fi;
+        out[tf_of(D) + D + tid] = t[NH + D + tid];
     }
     if (tid == 0) {
-        out[kTHF] = t[33];
-        out[kTVF] = t[34];
-        out[kTEN] = t[35];
+        out[thf_of(D)] = t[NH + 2 * D];
+        out[thf_of(D) + 1] = t[NH + 2 * D + 1];
+        out[thf_of(D) + 2] = t[NH + 2 * D + 2];
     }
 }
 
@@ -502,7 +657,7 @@ __device__ __forceinline__ void decode_tile(int tau, int nt, int& ti, int& tj) {
     tj = r + rem;
 }
 
-template <bool kIntr>
+template <bool kIntr, int D>
 __global__ void __launch_bounds__(kFrameThreads) ba_frame_kernel(BAPtrs base, Batch B, float alpha, float iscale) {
     BA_BIND(B, base);
     if (w.status[0]) return;
@@ -518,8 +673,8 @@ __global__ void __launch_bounds__(kFrameThreads) ba_frame_kernel(BAPtrs base, Ba
     const int m = w.fp_ptr[s + 1] - w.fp_ptr[s];
     const int self = w.self_slot[s];
     const int eb = w.fe_ptr[s], ee = w.fe_ptr[s + 1];
-    const int D = 6 * m + 2;
-    const int nt = (D + 3) / 4;
+    const int Dr = D * m + 2;
+    const int nt = (Dr + 3) / 4;
     const int Dp = 4 * nt;
     const int npt = nt * (nt + 1) / 2;
     const int T = (Dp * (256 + 4) <= kStageFloats) ? 256 : 128;
@@ -561,13 +716,14 @@ __global__ void __launch_bounds__(kFrameThreads) ba_frame_kernel(BAPtrs base, Ba
                     const int e = w.fe_list[q];
                     const int b = (int)A.jj[e];
                     const int sl = w.edge_slot[e];
-                    float tij[3], qij[4];
-                    edge_pose(A.poses, k, b, tij, qij);
+                    EdgeTf Tf;
+                    edge_tf<D>(A.poses, k, b, Tf);
                     const float* tp = A.targets + (size_t)e * 2 * HW;
                     const float* wp = A.weights + (size_t)e * 2 * HW;
-                    PixelLin L;
-                    linearize<kIntr, true>(tij, qij, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p),
-                                           __ldg(wp + HW + p), __ldg(tp + p), __ldg(tp + HW + p), act, A.iscale, L);
+                    typename LinOf<D>::T L;
+                    linearize_d<D, kIntr, true>(Tf, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p),
+                                                __ldg(wp + HW + p), __ldg(tp + p), __ldg(tp + HW + p), act, A.iscale,
+                                                L);
 #pragma unroll
                     for (int ch = 0; ch < 2; ch++) {
                         const float g = L.wd[ch] * L.Jz[ch];
@@ -576,11 +732,11 @@ __global__ void __launch_bounds__(kFrameThreads) ba_frame_kernel(BAPtrs base, Ba
                         if (kIntr) efsum += g * L.Jf[ch];
                         if (self >= 0) {
 #pragma unroll
-                            for (int n = 0; n < 6; n++) row[(6 * self + n) * LD] += g * L.Ji[ch][n];
+                            for (int n = 0; n < D; n++) row[(D * self + n) * LD] += g * L.Ji[ch][n];
                         }
                         if (sl >= 0) {
 #pragma unroll
-                            for (int n = 0; n < 6; n++) row[(6 * sl + n) * LD] += g * L.Jj[ch][n];
+                            for (int n = 0; n < D; n++) row[(D * sl + n) * LD] += g * L.Jj[ch][n];
                         }
                     }
                 }
@@ -598,9 +754,9 @@ __global__ void __launch_bounds__(kFrameThreads) ba_frame_kernel(BAPtrs base, Ba
                 qwf[2] = Ef;
                 const float sq = sqrtf(Q);
                 const float scale = act * sq;
-                for (int q = 0; q < 6 * m; q++) row[q * LD] *= scale;
-                row[(6 * m) * LD] = sq * wv;
-                row[(6 * m + 1) * LD] = sq * Ef;
+                for (int q = 0; q < D * m; q++) row[q * LD] *= scale;
+                row[(D * m) * LD] = sq * wv;
+                row[(D * m + 1) * LD] = sq * Ef;
             }
         }
         __syncthreads();
@@ -673,7 +829,7 @@ __global__ void __launch_bounds__(kFrameThreads) ba_frame_kernel(BAPtrs base, Ba
 
 // entry (R, C) of frame s's Schur-augmented matrix, summed over pixel chunks
 __device__ __forceinline__ double frame_entry(const Work& w, const Dims& d, int s, int m, int R, int C) {
-    const int nt = (6 * m + 2 + 3) / 4;
+    const int nt = (d.dof * m + 2 + 3) / 4;
     int r4 = R >> 2, c4 = C >> 2, rr = R & 3, cc = C & 3;
     if (r4 > c4) {
         int t = r4; r4 = c4; c4 = t;
@@ -718,23 +874,24 @@ __global__ void ba_assemble_blocks(BAPtrs base, Batch B, int with_frames) {
     const int b = a + (int)rem;
     const int dim = d.dim;
     double acc[2] = {0.0, 0.0};
-    const int nidx = lane < 4 ? 2 : 1;  // entries lane and lane+32 (< 36)
+    const int D = d.dof, D2 = D * D;
+    const int nidx = lane + 32 < D2 ? 2 : 1;  // entries lane and lane+32 (< D^2)
     for (int q = w.pe_ptr[a]; q < w.pe_ptr[a + 1]; q++) {
         const int ent = w.pe_list[q];
         const int e = ent >> 2, fl = ent & 3;
         const int ia = (int)ii[e] - d.t0, ib = (int)jj[e] - d.t0;
-        const double* T = w.eterm + (size_t)e * kNT;
+        const double* T = w.eterm + (size_t)e * nt_of(D);
         for (int x = 0; x < nidx; x++) {
             const int idx = lane + 32 * x;
-            const int r = idx / 6, cc = idx % 6;
+            const int r = idx / D, cc = idx % D;
             double v = 0.0;
             if (a == b) {
                 if (fl & 1) v += T[tri12(r, cc)];
-                if (fl & 2) v += T[tri12(6 + r, 6 + cc)];
-                if (fl == 3) v += T[tri12(r, 6 + cc)] + T[tri12(6 + r, cc)];
+                if (fl & 2) v += T[tri12(D + r, D + cc)];
+                if (fl == 3) v += T[tri12(r, D + cc)] + T[tri12(D + r, cc)];
             } else {
-                if ((fl & 1) && ib == b) v += T[tri12(r, 6 + cc)];
-                if ((fl & 2) && ia == b) v += T[tri12(6 + r, cc)];
+                if ((fl & 1) && ib == b) v += T[tri12(r, D + cc)];
+                if ((fl & 2) && ia == b) v += T[tri12(D + r, cc)];
             }
             acc[x] += v;
         }
@@ -748,16 +905,16 @@ __global__ void ba_assemble_blocks(BAPtrs base, Batch B, int with_frames) {
             const int m = w.fp_ptr[s + 1] - w.fp_ptr[s];
             for (int x = 0; x < nidx; x++) {
                 const int idx = lane + 32 * x;
-                const int r = idx / 6, cc = idx % 6;
-                acc[x] -= frame_entry(w, d, s, m, 6 * al + r, 6 * be + cc);
+                const int r = idx / D, cc = idx % D;
+                acc[x] -= frame_entry(w, d, s, m, D * al + r, D * be + cc);
             }
         }
     }
     for (int x = 0; x < nidx; x++) {
         const int idx = lane + 32 * x;
-        const int r = idx / 6, cc = idx % 6;
-        w.Hm[(size_t)(6 * a + r) * dim + 6 * b + cc] = acc[x];
-        if (a != b) w.Hm[(size_t)(6 * b + cc) * dim + 6 * a + r] = acc[x];
+        const int r = idx / D, cc = idx % D;
+        w.Hm[(size_t)(D * a + r) * dim + D * b + cc] = acc[x];
+        if (a != b) w.Hm[(size_t)(D * b + cc) * dim + D * a + r] = acc[x];
     }
 }
 
@@ -767,55 +924,55 @@ __global__ void ba_assemble_rhs(BAPtrs base, Batch B, int with_frames, int with_
     if (w.status[0]) return;
     const int lane = threadIdx.x & 31;
     const int a = local_ * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int P = d.P, dim = d.dim;
+    const int P = d.P, dim = d.dim, D = d.dof, NT = nt_of(D);
     if (a < P) {
-        // lanes 0..5: rhs entries; lanes 8..13: focal column entries
+        // lanes 0..D-1: rhs entries; lanes 8..8+D-1: focal column entries
         const int r = lane & 7;
-        const bool isF = lane >= 8 && lane < 14;
-        const bool isV = lane < 6;
+        const bool isF = lane >= 8 && lane < 8 + D;
+        const bool isV = lane < D;
         double acc = 0.0;
         if (isF || isV) {
             for (int q = w.pe_ptr[a]; q < w.pe_ptr[a + 1]; q++) {
                 const int ent = w.pe_list[q];
                 const int e = ent >> 2, fl = ent & 3;
-                const double* T = w.eterm + (size_t)e * kNT;
-                const int off = isV ? kTV : kTF;
+                const double* T = w.eterm + (size_t)e * NT;
+                const int off = isV ? tv_of(D) : tf_of(D);
                 if (fl & 1) acc += T[off + r];
-                if (fl & 2) acc += T[off + 6 + r];
+                if (fl & 2) acc += T[off + D + r];
             }
             if (with_frames) {
                 for (int q = w.pf_ptr[a]; q < w.pf_ptr[a + 1]; q++) {
                     const int ent = w.pf_list[q];
                     const int s = ent >> 5, al = ent & 31;
                     const int m = w.fp_ptr[s + 1] - w.fp_ptr[s];
-                    acc -= frame_entry(w, d, s, m, 6 * al + r, 6 * m + (isV ? 0 : 1));
+                    acc -= frame_entry(w, d, s, m, D * al + r, D * m + (isV ? 0 : 1));
                 }
             }
         }
-        if (isV) w.bv[6 * a + r] = acc;
+        if (isV) w.bv[D * a + r] = acc;
         if (isF) {
             const double v = with_intr ? acc : 0.0;
-            w.Hm[(size_t)(6 * a + r) * dim + 6 * P] = v;
-            w.Hm[(size_t)(6 * P) * dim + 6 * a + r] = v;
+            w.Hm[(size_t)(D * a + r) * dim + D * P] = v;
+            w.Hm[(size_t)(D * P) * dim + D * a + r] = v;
         }
     } else if (a == P && lane == 0) {
         double hff = 0.0, vf = 0.0;
         if (with_intr) {
             for (int e = 0; e < d.E; e++) {
-                hff += w.eterm[(size_t)e * kNT + kTHF];
-                vf += w.eterm[(size_t)e * kNT + kTVF];
+                hff += w.eterm[(size_t)e * NT + thf_of(D)];
+                vf += w.eterm[(size_t)e * NT + thf_of(D) + 1];
             }
             if (with_frames) {
                 for (int s = 0; s < d.K; s++) {
                     const int m = w.fp_ptr[s + 1] - w.fp_ptr[s];
-                    hff -= frame_entry(w, d, s, m, 6 * m + 1, 6 * m + 1);
-                    vf -= frame_entry(w, d, s, m, 6 * m, 6 * m + 1);
+                    hff -= frame_entry(w, d, s, m, D * m + 1, D * m + 1);
+                    vf -= frame_entry(w, d, s, m, D * m, D * m + 1);
                 }
             }
         }
         // without focal optimisation the extra unknown is decoupled: H = 1, b = 0
-        w.Hm[(size_t)(6 * P) * dim + 6 * P] = with_intr ? hff : 1.0;
-        w.bv[6 * P] = with_intr ? vf : 0.0;
+        w.Hm[(size_t)(D * P) * dim + D * P] = with_intr ? hff : 1.0;
+        w.bv[D * P] = with_intr ? vf : 0.0;
     }
 }
 
@@ -853,7 +1010,7 @@ __global__ void __launch_bounds__(kCholThreads, 1)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = with_intr ? d.dim : d.dim - 1;
     const int ld = d.dim;
-    const int np = 6 * d.P;
+    const int np = d.dof * d.P;
     const int LDR = chol_ldr(d.dim);
     double* A = w.Hm;
     double* x = w.bv;
@@ -1083,7 +1240,7 @@ __global__ void __launch_bounds__(kCholThreads) ba_chol_resolve_kernel(BAPtrs ba
     __shared__ double xs[kPanelRows];
     __shared__ double ysh[kNB];
     const int tid = threadIdx.x;
-    const int n = 6 * d.P, ld = d.dim;
+    const int n = d.dof * d.P, ld = d.dim;
     const double* A = io.ftape;
     const long nH = (long)d.dim * d.dim, nL = (long)((d.dim + 31) / 32) * 32 * 32;
     const double* Linv = io.ftape + nH;
@@ -1132,7 +1289,7 @@ __global__ void __launch_bounds__(kCholThreads) ba_chol_resolve_kernel(BAPtrs ba
 
 // ---------------------------------------------------------------- back substitution
 
-template <bool kIntr>
+template <bool kIntr, int D>
 __global__ void __launch_bounds__(256) ba_backsub_kernel(BAPtrs base, Batch B) {
     BA_BIND(B, base);
     if (w.status[0]) return;
@@ -1164,22 +1321,22 @@ __global__ void __launch_bounds__(256) ba_backsub_kernel(BAPtrs base, Batch B) {
             const int bp = b - d.t0;
             const bool on = sl >= 0 && bp > 0 && bp < P;
             if (!on && !self_on) continue;
-            float tij[3], qij[4];
-            edge_pose(A.poses, k, b, tij, qij);
+            EdgeTf Tf;
+            edge_tf<D>(A.poses, k, b, Tf);
             const float* wp = A.weights + (size_t)e * 2 * HW;
-            PixelLin L;
-            linearize<false, false>(tij, qij, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p), __ldg(wp + HW + p),
-                                    0.f, 0.f, act, 1.f, L);
+            typename LinOf<D>::T L;
+            linearize_d<D, false, false>(Tf, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p), __ldg(wp + HW + p),
+                                         0.f, 0.f, act, 1.f, L);
 #pragma unroll
             for (int ch = 0; ch < 2; ch++) {
                 const float g = L.wd[ch] * L.Jz[ch];
                 if (self_on) {
 #pragma unroll
-                    for (int n = 0; n < 6; n++) dot += g * L.Ji[ch][n] * dx[6 * selfpose + n];
+                    for (int n = 0; n < D; n++) dot += g * L.Ji[ch][n] * dx[D * selfpose + n];
                 }
                 if (on) {
 #pragma unroll
-                    for (int n = 0; n < 6; n++) dot += g * L.Jj[ch][n] * dx[6 * bp + n];
+                    for (int n = 0; n < D; n++) dot += g * L.Jj[ch][n] * dx[D * bp + n];
                 }
             }
         }
@@ -1200,13 +1357,20 @@ __global__ void ba_retract_kernel(BAPtrs base, Batch B, int with_intr, float isc
     float* poses_io = io.poses;
     float* intr_io = io.intr;
     const int t = local_ * blockDim.x + threadIdx.x;
-    if (t < d.P) {
+    if (t < d.P && d.dof == 6) {
         float xi[6], T[7];
         for (int n = 0; n < 6; n++) xi[n] = dx[6 * t + n];
         float* pz = poses_io + (size_t)(d.t0 + t) * 7;
         for (int n = 0; n < 7; n++) T[n] = pz[n];
         retract_pose(xi, T);
         for (int n = 0; n < 7; n++) pz[n] = T[n];
+    } else if (t < d.P) {
+        // Sim3: T <- Exp(xi) T
+        float xi[7];
+        for (int n = 0; n < 7; n++) xi[n] = dx[7 * t + n];
+        float* pz = poses_io + (size_t)(d.t0 + t) * 8;
+        const lie::Sim3<float> G = lie::Sim3<float>::Exp(xi) * lie::Sim3<float>::load(pz);
+        G.store(pz);
     }
     if (with_intr && local_ == 0 && threadIdx.x == 0) {
         const float dfs = (float)(w.df[0] * (double)iscale);
@@ -1221,7 +1385,7 @@ __global__ void ba_energy_kernel(BAPtrs base, Batch B, int with_frames, int itr)
     float* energy_out = io.energy;
     __shared__ double red[32];
     double s = 0.0;
-    for (int e = threadIdx.x; e < d.E; e += blockDim.x) s += w.eterm[(size_t)e * kNT + kTEN];
+    for (int e = threadIdx.x; e < d.E; e += blockDim.x) s += w.eterm[(size_t)e * nt_of(d.dof) + thf_of(d.dof) + 2];
     if (with_frames)
         for (int q = threadIdx.x; q < d.K * d.CF; q += blockDim.x) s += (double)w.fen[q];
     s = warp_sum(s);
@@ -1258,9 +1422,11 @@ int ensure_attributes() {
     int dev = 0;
     VIPE_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 64 && !g_smem_set[dev]) {
-        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<true, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            kStageFloats * 4));
-        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<false, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kStageFloats * 4));
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<false, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            kStageFloats * 4));
         VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_cholesky_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            chol_ldr(kPanelRows) * kNB * (int)sizeof(double)));
@@ -1298,11 +1464,14 @@ int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const 
     if (geo.any_edges) {
         {
             VIPE_PROF("ba_edge", st);
-            if (intr)
-                ba_edge_kernel<true><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(
+            if (geo.dof == 7)
+                ba_edge_kernel<false, 7><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(
+                    base, batch_of(geo, d_table, d_off, kOffEdge), a.iscale);
+            else if (intr)
+                ba_edge_kernel<true, 6><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(
                     base, batch_of(geo, d_table, d_off, kOffEdge), a.iscale);
             else
-                ba_edge_kernel<false><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(
+                ba_edge_kernel<false, 6><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(
                     base, batch_of(geo, d_table, d_off, kOffEdge), a.iscale);
         }
         VIPE_LAUNCH_CHECK();
@@ -1314,11 +1483,14 @@ int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const 
     }
     if (with_frames && grid(kOffFrame) > 0) {
         VIPE_PROF("ba_frame", st);
-        if (intr)
-            ba_frame_kernel<true><<<grid(kOffFrame), kFrameThreads, kStageFloats * 4, st>>>(
+        if (geo.dof == 7)
+            ba_frame_kernel<false, 7><<<grid(kOffFrame), kFrameThreads, kStageFloats * 4, st>>>(
+                base, batch_of(geo, d_table, d_off, kOffFrame), a.alpha, a.iscale);
+        else if (intr)
+            ba_frame_kernel<true, 6><<<grid(kOffFrame), kFrameThreads, kStageFloats * 4, st>>>(
                 base, batch_of(geo, d_table, d_off, kOffFrame), a.alpha, a.iscale);
         else
-            ba_frame_kernel<false><<<grid(kOffFrame), kFrameThreads, kStageFloats * 4, st>>>(
+            ba_frame_kernel<false, 6><<<grid(kOffFrame), kFrameThreads, kStageFloats * 4, st>>>(
                 base, batch_of(geo, d_table, d_off, kOffFrame), a.alpha, a.iscale);
         VIPE_LAUNCH_CHECK();
     }
@@ -1361,10 +1533,12 @@ static int launch_update(const Geometry& geo, const GraphDesc* d_table, const in
     const bool intr = a.intr != 0;
     if (!a.motion_only && grid(kOffFrame) > 0) {
         VIPE_PROF("ba_backsub", st);
-        if (intr)
-            ba_backsub_kernel<true><<<grid(kOffFrame), 256, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffFrame));
+        if (geo.dof == 7)
+            ba_backsub_kernel<false, 7><<<grid(kOffFrame), 256, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffFrame));
+        else if (intr)
+            ba_backsub_kernel<true, 6><<<grid(kOffFrame), 256, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffFrame));
         else
-            ba_backsub_kernel<false><<<grid(kOffFrame), 256, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffFrame));
+            ba_backsub_kernel<false, 6><<<grid(kOffFrame), 256, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffFrame));
         VIPE_LAUNCH_CHECK();
     }
     {
@@ -1394,8 +1568,8 @@ int run_solve(const Geometry& geo, const GraphDesc* d_table, const int* d_off, c
     if (rc != VIPE_OK) return rc;
     for (int itr = 0; itr < a.iterations; itr++) {
         if (tape) {
-            VIPE_CUDA_TRY(cudaMemcpyAsync(tape->poses + (size_t)itr * tape->frames * 7, base.poses,
-                                          sizeof(float) * tape->frames * 7, cudaMemcpyDeviceToDevice, st));
+            VIPE_CUDA_TRY(cudaMemcpyAsync(tape->poses + (size_t)itr * tape->frames * (geo.dof + 1), base.poses,
+                                          sizeof(float) * tape->frames * (geo.dof + 1), cudaMemcpyDeviceToDevice, st));
             VIPE_CUDA_TRY(cudaMemcpyAsync(tape->disps + (size_t)itr * tape->frames * tape->hw, base.disps,
                                           sizeof(float) * tape->frames * tape->hw, cudaMemcpyDeviceToDevice, st));
         }
@@ -1497,15 +1671,25 @@ extern "C" int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* in
 
 extern "C" int vipe_slam_ba_batch_plan_create(int num_graphs, const int* num_frames, const int* num_edges,
                                               const int* num_kx, const int* t0, const int* t1, int ht, int wd,
-                                              int edge_chunks, int frame_chunks, int with_adjoint,
-                                              vipe_ba_batch_plan** plan_out) {
+                                              int edge_chunks, int frame_chunks, int group_id,
+                                              int with_adjoint, vipe_ba_batch_plan** plan_out) {
     if (!plan_out) return VIPE_ERR_ARG;
     *plan_out = nullptr;
     if (num_graphs <= 0 || !num_frames || !num_edges || !num_kx || !t0 || !t1) return VIPE_ERR_ARG;
     if (edge_chunks < 0 || frame_chunks < 0) return VIPE_ERR_ARG;
+    if (group_id != 3 && group_id != 4) {
+        set_last_error("batched BA: group_id must be 3 (SE3) or 4 (Sim3)");
+        return VIPE_ERR_GROUP;
+    }
+    const int dof = group_id == 4 ? 7 : 6;
+    if (with_adjoint && dof != 6) {
+        set_last_error("batched BA: the adjoint is implemented for SE3 graphs");
+        return VIPE_ERR_GROUP;
+    }
     long sumE = 0, sumK = 0;
     for (int g = 0; g < num_graphs; g++) {
-        const int rc = check_dims(num_frames[g], ht, wd, num_edges[g], num_kx[g], t0[g], t1[g]);
+        int rc = check_dims(num_frames[g], ht, wd, num_edges[g], num_kx[g], t0[g], t1[g]);
+        if (rc == VIPE_OK && dof * (t1[g] - t0[g]) + 1 > kPanelRows) rc = VIPE_ERR_CAPACITY;
         if (rc != VIPE_OK) {
             char msg[96];
             snprintf(msg, sizeof(msg), "graph %d of the batch has invalid sizes", g);
@@ -1533,7 +1717,7 @@ extern "C" int vipe_slam_ba_batch_plan_create(int num_graphs, const int* num_fra
     for (int g = 0; g < num_graphs; g++) {
         GraphDesc& gd = plan->gds[g];
         gd = GraphDesc{};
-        gd.d = make_dims(num_frames[g], ht, wd, num_edges[g], num_kx[g], t0[g], t1[g], che, cf);
+        gd.d = make_dims(num_frames[g], ht, wd, num_edges[g], num_kx[g], t0[g], t1[g], che, cf, dof);
         gd.d.adj = plan->adjoint;
         gd.frame_off = plan->frames;
         gd.edge_off = plan->edges;
@@ -1620,6 +1804,10 @@ extern "C" int vipe_slam_ba_batch_solve(const vipe_ba_batch_plan* plan, float* p
     int rc = check_ba_args(poses_io, disps_io, intrinsics_io, disps_sens, targets, weights, eta, ii, jj, depth_active,
                            plan->edges, iterations, motion_only, compute_energy, dx_out, dz_out, energy_out);
     if (rc != VIPE_OK) return rc;
+    if (optimize_intrinsics && plan->geo.dof != 6) {
+        set_last_error("batched BA: focal-length optimisation is implemented for SE3 graphs");
+        return VIPE_ERR_ARG;
+    }
     BAPtrs base{poses_io, disps_io, intrinsics_io, disps_sens, targets, weights, eta, ii, jj, depth_active,
                 dx_out, motion_only ? nullptr : dz_out, compute_energy ? energy_out : nullptr, dev_status,
                 iterations, 1};
@@ -1633,7 +1821,7 @@ extern "C" int vipe_slam_ba_batch_solve(const vipe_ba_batch_plan* plan, float* p
     tape.frames = plan->frames;
     tape.hw = (long)plan->ht * plan->wd;
     tape.factor_stride = plan->ftape_stride;
-    tape.poses6 = plan->poses * 6;
+    tape.poses6 = plan->poses * plan->geo.dof;
     return run_solve(plan->geo, plan->d_table, plan->d_off, base, nullptr, a, as_stream(stream),
                      ntape ? &tape : nullptr);
 }

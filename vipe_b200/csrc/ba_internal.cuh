@@ -11,7 +11,7 @@
 namespace vipe {
 namespace ba {
 
-constexpr int kMaxSlots = 32;          // window poses coupled to one depth frame
+constexpr int kMaxSlots = 32;          // window poses coupled to one depth frame (SE3; Sim3: 27)
 constexpr int kMaxPoses = 127;         // t1 - t0: 6P+1 unknowns fit the staged Cholesky panel
 constexpr int kNT = 105;               // per-edge terms, see term layout below
 constexpr int kEdgeThreads = 256;
@@ -34,7 +34,21 @@ struct Dims {
     int CF, chunk_f;   // frame kernel pixel chunks
     long tile_cap;     // capacity of frame SYRK tiles
     int adj;           // 1: the workspace also holds the adjoint buffers
+    int dof;           // pose tangent size: 6 (SE3) or 7 (Sim3)
 };
+
+// Per-edge term layouts for pose tangent size `dof`:
+//   chunk partials (ne_of):  Hjj upper triangle (dof(dof+1)/2), vj, fj, hf, vf, energy
+//   FP64 terms (nt_of):      upper triangle of the (2 dof)^2 block [Ji Jj]^T W [Ji Jj],
+//                            [vi; vj], [fi; fj], hf, vf, energy
+__host__ __device__ inline int ne_of(int dof) { return dof * (dof + 1) / 2 + 2 * dof + 3; }
+__host__ __device__ inline int tri_of(int dof) { return (2 * dof) * (2 * dof + 1) / 2; }
+__host__ __device__ inline int nt_of(int dof) { return tri_of(dof) + 4 * dof + 3; }
+__host__ __device__ inline int tv_of(int dof) { return tri_of(dof); }
+__host__ __device__ inline int tf_of(int dof) { return tri_of(dof) + 2 * dof; }
+__host__ __device__ inline int thf_of(int dof) { return tri_of(dof) + 4 * dof; }
+__host__ __device__ inline int max_slots(int dof) { return dof == 6 ? kMaxSlots : 27; }
+constexpr int kMaxNE = 45;  // ne_of(7)
 
 struct Work {
     int* status;   // [0] error code
@@ -73,18 +87,19 @@ struct Work {
 
 constexpr int kAdjAcc = 48;  // 4 moment matrices of 3 x 4 per edge
 
-__host__ __device__ inline int npt_of(int m) {
-    int nt = (6 * m + 2 + 3) / 4;
+__host__ __device__ inline int npt_of(int m, int dof = 6) {
+    int nt = (dof * m + 2 + 3) / 4;
     return nt * (nt + 1) / 2;
 }
 
 // che / cf: pixel-chunk counts of the per-edge and per-frame kernels; 0 picks
 // them so that one graph alone launches about two CTAs per SM.
-inline Dims make_dims(int N, int H, int W, int E, int K, int t0, int t1, int che = 0, int cf = 0) {
+inline Dims make_dims(int N, int H, int W, int E, int K, int t0, int t1, int che = 0, int cf = 0, int dof = 6) {
     Dims d;
     d.N = N; d.H = H; d.W = W; d.HW = H * W; d.E = E; d.K = K; d.t0 = t0; d.t1 = t1;
     d.P = t1 - t0;
-    d.dim = 6 * d.P + 1;
+    d.dof = dof;
+    d.dim = dof * d.P + 1;
     const int target = 2 * 148;
     if (che <= 0) che = E > 0 ? (target + E - 1) / E : 1;
     che = std::max(1, std::min(che, std::max(1, d.HW / 1024)));
@@ -96,11 +111,12 @@ inline Dims make_dims(int N, int H, int W, int E, int K, int t0, int t1, int che
     chunk = ((chunk + 255) / 256) * 256;
     d.chunk_f = chunk;
     d.CF = (d.HW + chunk - 1) / chunk;
-    // Upper bound of sum over frames of npt(m_s): slots are <= kMaxSlots per
-    // frame and sum_s m_s <= E + K.  npt(m) <= (1.5 m + 3.25)^2 / 2.
-    const int M = std::max(1, std::min(kMaxSlots, d.P));
-    double b1 = (double)K * npt_of(M);
-    double b2 = (1.5 * M + 3.25) / 2.0 * (1.5 * (double)(E + K) + 3.25 * K);
+    // Upper bound of sum over frames of npt(m_s): slots are <= max_slots per
+    // frame and sum_s m_s <= E + K.  npt(m) <= (a m + 3.25)^2 / 2, a = dof / 4.
+    const int M = std::max(1, std::min(max_slots(dof), d.P));
+    const double a = dof / 4.0;
+    double b1 = (double)K * npt_of(M, dof);
+    double b2 = (a * M + 3.25) / 2.0 * (a * (double)(E + K) + 3.25 * K);
     d.tile_cap = (long)std::min(b1, b2) + K + 1;
     d.adj = 0;
     return d;
@@ -130,8 +146,8 @@ inline void carve(C& c, const Dims& d, Work* w) {
     take_i(w ? w->pe_list : dummy, 2 * E + 1);
     take_i(w ? w->pf_ptr : dummy, P + 1);
     take_i(w ? w->pf_list : dummy, E + K + 1);
-    auto pf = c.template take<float>((size_t)std::max<size_t>(1, E) * d.CHe * 36);
-    auto pd = c.template take<double>((size_t)std::max<size_t>(1, E) * kNT);
+    auto pf = c.template take<float>((size_t)std::max<size_t>(1, E) * d.CHe * ne_of(d.dof));
+    auto pd = c.template take<double>((size_t)std::max<size_t>(1, E) * nt_of(d.dof));
     auto ps = c.template take<float>((size_t)d.tile_cap * d.CF * 16);
     auto pen = c.template take<float>(K * d.CF + 1);
     auto pq = c.template take<float>(K * (size_t)d.HW * 3);
@@ -253,7 +269,7 @@ __device__ __forceinline__ int locate(const Batch& B, int& local) {
 __device__ __forceinline__ BAPtrs rebase(const BAPtrs& b, const GraphDesc& g) {
     const long HW = g.d.HW;
     BAPtrs p;
-    p.poses = b.poses + g.frame_off * 7;
+    p.poses = b.poses + g.frame_off * (g.d.dof + 1);
     p.disps = b.disps + g.frame_off * HW;
     p.intr = b.intr + (long)g.g * 4;
     p.disps_sens = b.disps_sens + g.frame_off * HW;
@@ -263,13 +279,13 @@ __device__ __forceinline__ BAPtrs rebase(const BAPtrs& b, const GraphDesc& g) {
     p.ii = b.ii ? b.ii + g.edge_off : nullptr;
     p.jj = b.jj ? b.jj + g.edge_off : nullptr;
     p.depth_active = b.depth_active + g.frame_off;
-    p.dx = b.dx + g.pose_off * 6;
+    p.dx = b.dx + g.pose_off * g.d.dof;
     p.dz = b.dz ? b.dz + g.kx_off * HW : nullptr;
     p.energy = b.energy ? b.energy + (long)g.g * b.energy_stride : nullptr;
     p.status = b.status ? b.status + (long)g.g * b.status_stride : nullptr;
     p.energy_stride = b.energy_stride;
     p.status_stride = b.status_stride;
-    p.g_poses = b.g_poses ? b.g_poses + g.frame_off * 7 : nullptr;
+    p.g_poses = b.g_poses ? b.g_poses + g.frame_off * (g.d.dof + 1) : nullptr;
     p.g_disps = b.g_disps ? b.g_disps + g.frame_off * HW : nullptr;
     p.g_targets = b.g_targets ? b.g_targets + g.edge_off * 2 * HW : nullptr;
     p.g_weights = b.g_weights ? b.g_weights + g.edge_off * 2 * HW : nullptr;
@@ -344,6 +360,7 @@ enum { kOffEdge = 0, kOffEdgeRed, kOffFrame, kOffPairs, kOffRhs, kOffRetr, kNumO
 
 struct Geometry {
     int G = 0;
+    int dof = 6;
     std::vector<int> off[kNumOff];  // G + 1 entries each
     size_t chol_smem = 0;
     bool any_edges = false;
@@ -360,6 +377,7 @@ inline void fill_geometry(const std::vector<Dims>& dims, Geometry& geo) {
         for (int k = 0; k < kNumOff; k++) geo.off[k][g + 1] = geo.off[k][g] + cnt[k];
         geo.chol_smem = std::max(geo.chol_smem, (size_t)chol_ldr(d.dim) * kNB * sizeof(double));
         geo.any_edges |= d.E > 0;
+        geo.dof = d.dof;
     }
 }
 

@@ -77,6 +77,12 @@ def se3_inv(X):
     return np.concatenate([-_quat_rot(qi, X[..., :3]), qi], -1)
 
 
+def sim3_mul(X, Y):
+    """(..., 8) Sim3 [t q s] composition X * Y = (tX + sX R_X tY, qX qY, sX sY)."""
+    t = X[..., :3] + X[..., 7:8] * _quat_rot(X[..., 3:7], Y[..., :3])
+    return np.concatenate([t, _quat_mul(X[..., 3:7], Y[..., 3:7]), X[..., 7:8] * Y[..., 7:8]], -1)
+
+
 def se3_log(X):
     """(..., 7) -> (..., 6) [tau, phi]."""
     q = X[..., 3:] / np.linalg.norm(X[..., 3:], axis=-1, keepdims=True)
@@ -274,8 +280,14 @@ def _torch_quat_mul(a, b):
 
 
 def _torch_relative(Ti, Tj):
-    """Tij = Tj * Ti^-1 for (..., 7) SE3 poses."""
-    qi_inv = Ti[..., 3:] * Ti.new_tensor([-1.0, -1.0, -1.0, 1.0])
+    """Tij = Tj * Ti^-1 for (..., 7) SE3 or (..., 8) Sim3 poses."""
+    qi_inv = Ti[..., 3:7] * Ti.new_tensor([-1.0, -1.0, -1.0, 1.0])
+    if Ti.shape[-1] == 8:
+        si_inv = 1.0 / Ti[..., 7:8]
+        ti_inv = -si_inv * _torch_quat_rot(qi_inv, Ti[..., :3])
+        q = _torch_quat_mul(Tj[..., 3:7], qi_inv)
+        t = Tj[..., :3] + Tj[..., 7:8] * _torch_quat_rot(Tj[..., 3:7], ti_inv)
+        return torch.cat([t, q, Tj[..., 7:8] * si_inv], -1)
     ti_inv = -_torch_quat_rot(qi_inv, Ti[..., :3])
     q = _torch_quat_mul(Tj[..., 3:], qi_inv)
     t = Tj[..., :3] + _torch_quat_rot(Tj[..., 3:], ti_inv)
@@ -320,7 +332,7 @@ class BABatch:
 
 def make_ba_batch(num_clips: int, seed: int, frames_range=(8, 96), radius: int = 3, loops_mean: float = 4.0,
                   loop_gap: int = 8, outlier_frac: float = 0.01, ht: int = 48, wd: int = 64, t0: int = 2,
-                  intrinsics=(60.0, 60.0, 32.0, 24.0), device="cpu") -> BABatch:
+                  intrinsics=(60.0, 60.0, 32.0, 24.0), device="cpu", group: str = "se3") -> BABatch:
     """Many clips of the BA generative model with uneven sizes.
 
     Keyframe counts ~ U{frames_range}; edges |i-j| <= radius plus Poisson(loops_mean)
@@ -328,7 +340,10 @@ def make_ba_batch(num_clips: int, seed: int, frames_range=(8, 96), radius: int =
     `outlier_frac` of target entries is replaced by U(-20, 20) px with weight
     0.05.  Structure comes from numpy (seeded), the bulk noise from a seeded
     torch generator on `device` (generation runs on the GPU for large batches).
+    group="sim3": poses are Sim3 [t q s]; each trajectory step also scales by
+    exp(N(0, 0.02^2)) and the initial poses by exp(N(0, 0.01^2)).
     """
+    sim3 = group == "sim3"
     rng = np.random.default_rng(seed)
     dev = torch.device(device)
     gen = torch.Generator(device=dev)
@@ -350,8 +365,14 @@ def make_ba_batch(num_clips: int, seed: int, frames_range=(8, 96), radius: int =
         T = np.zeros((n, 7))
         T[0] = [0, 0, 0, 0, 0, 0, 1]
         steps = np.concatenate([rng.normal(0, 0.05, (n, 3)), rng.normal(0, 0.02, (n, 3))], 1)
-        for i in range(1, n):
-            T[i] = se3_mul(se3_exp(steps[i]), T[i - 1])
+        if sim3:
+            T = np.concatenate([T, np.ones((n, 1))], 1)
+            sc = np.exp(rng.normal(0, 0.02, n))
+            for i in range(1, n):
+                T[i] = sim3_mul(np.concatenate([se3_exp(steps[i]), [sc[i]]]), T[i - 1])
+        else:
+            for i in range(1, n):
+                T[i] = se3_mul(se3_exp(steps[i]), T[i - 1])
         T_all.append(T)
     Nt, Et, Kt = sum(nf), sum(ne), sum(nk)
     T_gt = torch.from_numpy(np.concatenate(T_all)).to(dev)
@@ -381,8 +402,11 @@ def make_ba_batch(num_clips: int, seed: int, frames_range=(8, 96), radius: int =
     chunk = 4096
     for e0 in range(0, Et, chunk):
         e1 = min(Et, e0 + chunk)
-        Tij = _torch_relative(T_gt[gi[e0:e1]], T_gt[gj[e0:e1]])  # (c, 7)
-        Xj = _torch_quat_rot(Tij[:, None, None, 3:], X[None]) + d_gt[gi[e0:e1]][..., None] * Tij[:, None, None, :3]
+        Tij = _torch_relative(T_gt[gi[e0:e1]], T_gt[gj[e0:e1]])  # (c, 7) or (c, 8)
+        RX = _torch_quat_rot(Tij[:, None, None, 3:7], X[None])
+        if sim3:
+            RX = RX * Tij[:, None, None, 7:8]
+        Xj = RX + d_gt[gi[e0:e1]][..., None] * Tij[:, None, None, :3]
         z = Xj[..., 2]
         tg = torch.stack([fx * Xj[..., 0] / z + cx, fy * Xj[..., 1] / z + cy], 1)
         tg = tg + 0.5 * torch.randn(tg.shape, generator=gen, device=dev, dtype=torch.float64)
@@ -396,7 +420,12 @@ def make_ba_batch(num_clips: int, seed: int, frames_range=(8, 96), radius: int =
     # initial state
     delta = torch.cat([torch.randn(Nt, 3, generator=gen, device=dev, dtype=torch.float64) * (0.02 / math.sqrt(3)),
                        torch.randn(Nt, 3, generator=gen, device=dev, dtype=torch.float64) * (0.01 / math.sqrt(3))], 1)
-    P0 = torch.from_numpy(se3_mul(se3_exp(delta.cpu().numpy()), T_gt.cpu().numpy())).to(dev)
+    if sim3:
+        ds = torch.exp(0.01 * torch.randn(Nt, 1, generator=gen, device=dev, dtype=torch.float64))
+        dl = np.concatenate([se3_exp(delta.cpu().numpy()), ds.cpu().numpy()], 1)
+        P0 = torch.from_numpy(sim3_mul(dl, T_gt.cpu().numpy())).to(dev)
+    else:
+        P0 = torch.from_numpy(se3_mul(se3_exp(delta.cpu().numpy()), T_gt.cpu().numpy())).to(dev)
     d0 = d_gt * (1 + 0.05 * torch.randn(d_gt.shape, generator=gen, device=dev, dtype=torch.float64))
     eta = 0.2 * (torch.rand(Kt, ht, wd, generator=gen, device=dev, dtype=torch.float64) * (1e-2 - 1e-4) + 1e-4) + 1e-7
     tensors = dict(
@@ -412,3 +441,8 @@ def make_ba_batch(num_clips: int, seed: int, frames_range=(8, 96), radius: int =
 def ba_config4_se3(device="cpu", num_clips: int = 256) -> BABatch:
     """256 clips, keyframes ~ U{8..96}, |i-j| <= 3 + Poisson(4) loops, 1% outliers (SE3 form)."""
     return make_ba_batch(num_clips, seed=1004, device=device)
+
+
+def ba_config4(device="cpu", num_clips: int = 256) -> BABatch:
+    """256 clips, keyframes ~ U{8..96}, |i-j| <= 3 + Poisson(4) loops, 1% outliers, Sim3 poses."""
+    return make_ba_batch(num_clips, seed=1004, device=device, group="sim3")
