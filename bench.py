@@ -344,6 +344,10 @@ def batch_kernel_bytes(b, name):
         return E * HW * 16 + K * HW * 24
     if name == "ba_backsub":
         return E * HW * 8 + K * HW * 24
+    if name == "ba_adj_frame_a":  # targets + weights, disps/eta/disps_sens/g_disps in, Q and w out
+        return E * HW * 16 + K * HW * 24
+    if name == "ba_adj_frame_b":  # targets + weights in, their gradients read-modify-written; per-pixel state
+        return E * HW * 48 + K * HW * 40
     return None
 
 
@@ -584,6 +588,18 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
     total = sum(v[0] for v in prof.values())
     breakdown = {k: {"ms_per_step": v[0] / 2, "share": v[0] / total} for k, v in prof.items()}
     launches = sum(v[1] for v in prof.values()) / 2
+    hbm, _, src = measured_peaks()
+    roof = None
+    for name, (kms, cnt) in sorted(prof.items(), key=lambda kv: -kv[1][0]):
+        nbytes = batch_kernel_bytes(b, name)
+        if nbytes is None:
+            continue
+        avg_s = kms / cnt / 1e3
+        ach = nbytes / avg_s / 1e9
+        roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "traffic": None, "peak_source": src, "bytes_per_launch": nbytes, "avg_launch_ms": avg_s * 1e3,
+                "note": "FP32-issue bound: HBM is the algorithmic bound, not the limiter (profiles/)"}
+        break
 
     # end to end: pinned host inputs and incoming gradients in, outputs and all gradients out
     host_in = {k: v.cpu().pin_memory() for k, v in T.items()}
@@ -619,11 +635,76 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
         "steps": n,
         "status_nonzero": status_nonzero,
         "kernel_breakdown": breakdown,
+        "roofline": roof,
         "gpu_launches_per_step": launches,
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "vipe_b200.ba_batch.BatchPlan.solve with tape + vipe_slam_ba_batch_backward (pinned host "
                        "tensors in: inputs and incoming gradients; out: poses, depths and every input gradient)"},
     }
+
+
+def sim3_leg(dev, args, flush, stream):
+    """The Sim3 form on the 256-clip batch (cfg4 proper): forward solves/s with the LM
+    loop as a CUDA graph, and the error against the FP64 torch oracle on the two
+    smallest clips."""
+    import torch
+
+    from oracle import ba_torch as bt
+    from vipe_b200 import ba_batch as BB, workloads as Wk
+
+    b = Wk.ba_config4(device=dev)
+    iters, lm, ep = 4, 1e-4, 0.1
+    tune = BB.autotune(b.sizes, b.ht, b.wd, b.tensors, iters, lm, ep, dev, reps=1, group="sim3",
+                       candidates=((1, 1), (2, 1), (1, 2)))
+    plan = BB.BatchPlan(*b.sizes, b.ht, b.wd, dev, edge_chunks=tune.edge_chunks, frame_chunks=tune.frame_chunks,
+                        group="sim3")
+    static = {k: v.clone() for k, v in b.tensors.items()}
+    cap = plan.capture(static, iterations=iters, lm=lm, ep=ep)
+
+    def reset():
+        for k in ("poses", "disps", "intrinsics"):
+            static[k].copy_(b.tensors[k])
+
+    for _ in range(3):
+        reset()
+        cap.replay()
+    torch.cuda.synchronize(dev)
+    n = max(3, args.steps // 4)
+    ms = []
+    for k in range(n):
+        reset()
+        flush.fill_(float(k))
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        cap.replay()
+        c.record(stream)
+        torch.cuda.synchronize(dev)
+        ms.append(a.elapsed_time(c))
+    batch_ms = sum(ms) / n
+    status = cap.out[3].cpu().tolist()
+    errs = []
+    order = sorted(range(b.G), key=lambda g: b.num_frames[g])[:2]
+    offs = [sum(b.num_frames[:g]) for g in range(b.G)]
+    for g in order:
+        p = b.clip(g)
+        out = bt.ba_torch(p.poses.double(), p.disps.double(), p.intrinsics.double(), p.disps_sens.double(),
+                          p.targets.double(), p.weights.double(), p.eta.double(), p.ii, p.jj, p.depth_active.double(),
+                          p.t0, p.t1, iters, lm, ep, p.alpha)
+        got = static["poses"][offs[g]:offs[g] + b.num_frames[g]].double().cpu()
+        errs.append(float((got - out[0]).abs().max()))
+    res = {
+        "workload": "256 clips, keyframes ~U{8..96} at 48x64, Sim3 poses, |i-j|<=3 + Poisson(4) loops, "
+        "1% outliers, 4 LM iterations",
+        "value": b.G / (batch_ms / 1e3),
+        "unit": "solves/s",
+        "ms_per_batch": batch_ms,
+        "status_nonzero": sum(1 for x in status if x),
+        "autotune": [tune.edge_chunks, tune.frame_chunks],
+        "max_pose_err_vs_fp64_oracle": max(errs),
+        "oracle_clips": [b.num_frames[g] for g in order],
+    }
+    del plan, cap, static, b
+    return res
 
 
 def plain_cfg1_leg(dev, args, flush, stream):
@@ -696,10 +777,13 @@ def run_ours(args):
     del b
     value, e2e, n = adj["value"], adj.pop("e2e"), adj["steps"]
     extras["forward_only"] = {"value": fwd_value, "unit": "solves/s", "ms_per_batch": extras["batch_ms"],
+                              "roofline": extras.pop("roofline"),
                               "steps": n_fwd, "e2e": fwd_e2e, "form": "CUDA graph of the whole LM loop"}
     extras["speedup_fwd_adj_vs_plain_forward_same_gpu"] = value / extras["plain_same_gpu"]["value"]
     torch.cuda.empty_cache()
     plain = plain_cfg1_leg(dev, args, flush, stream)
+    torch.cuda.empty_cache()
+    sim3 = sim3_leg(dev, args, flush, stream)
     hbm, bf16, src = measured_peaks()
     corr = None
     if not args.no_corr:
@@ -731,12 +815,13 @@ def run_ours(args):
                 "FP64 block sums, Cholesky and re-solve",
             },
             "e2e": e2e,
-            "roofline": extras.pop("roofline"),
+            "roofline": adj.pop("roofline"),
             "gpu_launches": int(adj["gpu_launches_per_step"] * n),
             "clocks": clk.summary(),
             "batched": extras,
             "adjoint": adj,
             "plain_cfg1": plain,
+            "sim3_batched": sim3,
             "corr": corr,
         }
         if not args.no_cpu_baseline:

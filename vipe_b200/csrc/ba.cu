@@ -1290,7 +1290,7 @@ __global__ void __launch_bounds__(kCholThreads) ba_chol_resolve_kernel(BAPtrs ba
 // ---------------------------------------------------------------- back substitution
 
 template <bool kIntr, int D>
-__global__ void __launch_bounds__(256) ba_backsub_kernel(BAPtrs base, Batch B) {
+__global__ void __launch_bounds__(256, 3) ba_backsub_kernel(BAPtrs base, Batch B) {
     BA_BIND(B, base);
     if (w.status[0]) return;
     const FrameArgs A{io.poses, io.disps, io.disps_sens, io.intr, io.targets, io.weights, io.eta, io.depth_active, io.jj,
