@@ -492,35 +492,54 @@ __global__ void __launch_bounds__(kThreads, 1)
 // ---------------------------------------------------------------- pack pass
 
 // F (num, C, H, W) -> rows (num, HW, Kp) of 16-bit type, scaled by 1/4;
-// permute: target-block pixel order (8 x TW blocks) for the B operand.
+// permute: target-block pixel order (8 x TW blocks) for the B operand.  One
+// CTA transposes a 64-channel x 64-pixel tile through shared memory with
+// 16-byte global loads (along pixels) and 16-byte stores (along channels).
 template <typename TIn, typename TOp>
-__global__ void pack_kernel(const TIn* __restrict__ f, TOp* __restrict__ out, int C, int Kp, int H, int W, int TW,
-                            int permute) {
-    __shared__ float tile[32][65];
+__global__ void __launch_bounds__(256) pack_kernel(const TIn* __restrict__ f, TOp* __restrict__ out, int C, int Kp,
+                                                   int H, int W, int TW, int permute) {
+    constexpr int kPx = 64, kCh = 64, LDT = kPx + 8;  // 16-bit tile rows padded by 16 bytes
+    __shared__ __align__(16) TOp tile[kCh][LDT];
     const int e = blockIdx.z;
     const int HW = H * W;
-    const int p0 = blockIdx.x * 32;          // 32 pixels
-    const int c0 = blockIdx.y * 64;          // 64 channels
+    const int p0 = blockIdx.x * kPx;
+    const int c0 = blockIdx.y * kCh;
     const TIn* src = f + (size_t)e * C * HW;
-    for (int i = threadIdx.x; i < 32 * 64; i += blockDim.x) {
-        const int cc = i / 32, pp = i % 32;
-        const int c = c0 + cc, px = p0 + pp;
-        float v = 0.f;
-        if (c < C && px < HW) v = static_cast<float>(src[(size_t)c * HW + px]);
-        tile[pp][cc] = v * 0.25f;
+    constexpr int V = 16 / (int)sizeof(TIn);  // input elements per 16-byte load
+    const bool vec_ok = (HW % V) == 0 && (reinterpret_cast<uintptr_t>(f) % 16) == 0;
+    for (int i = threadIdx.x; i < kCh * (kPx / V); i += blockDim.x) {
+        const int cc = i / (kPx / V), pv = (i % (kPx / V)) * V;
+        const int c = c0 + cc, px = p0 + pv;
+        float v[V];
+        if (c < C && vec_ok && px + V <= HW) {
+            const uint4 raw = __ldg(reinterpret_cast<const uint4*>(src + (size_t)c * HW + px));
+            const TIn* rv = reinterpret_cast<const TIn*>(&raw);
+#pragma unroll
+            for (int k = 0; k < V; k++) v[k] = static_cast<float>(rv[k]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < V; k++)
+                v[k] = (c < C && px + k < HW) ? static_cast<float>(src[(size_t)c * HW + px + k]) : 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < V; k++) tile[cc][pv + k] = static_cast<TOp>(v[k] * 0.25f);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < 32 * 64; i += blockDim.x) {
-        const int pp = i / 64, cc = i % 64;
+    // each thread writes 8 consecutive channels (16 bytes) of one pixel
+    for (int i = threadIdx.x; i < kPx * (kCh / 8); i += blockDim.x) {
+        const int pp = i / (kCh / 8), cg = (i % (kCh / 8)) * 8;
         const int px = p0 + pp;
-        if (px >= HW || c0 + cc >= Kp) continue;
+        if (px >= HW || c0 + cg >= Kp) continue;
         int row = px;
         if (permute) {
             const int h = px / W, w = px % W;
             const int hb = h / kTH, r = h % kTH, wb = w / TW, c = w % TW;
             row = ((hb * (W / TW) + wb) * kTH + r) * TW + c;
         }
-        out[((size_t)e * HW + row) * Kp + c0 + cc] = static_cast<TOp>(tile[pp][cc]);
+        __align__(16) TOp o[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) o[k] = tile[cg + k][pp];
+        *reinterpret_cast<uint4*>(out + ((size_t)e * HW + row) * Kp + c0 + cg) = *reinterpret_cast<const uint4*>(o);
     }
 }
 
@@ -611,7 +630,7 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
 
     // operand type: FP16 inputs stay FP16, others go to BF16
     const int op_fmt = (in_dtype == VIPE_F16) ? 0 : 1;
-    dim3 pg(ceil_div(HW, 32), Kp / kKC, num);
+    dim3 pg(ceil_div(HW, 64), Kp / kKC, num);
     {
         VIPE_PROF("corr_pack", st);
         for (int side = 0; side < 2; side++) {
