@@ -41,6 +41,8 @@ enum vipe_status {
     VIPE_ERR_CUDA = 7,         /* a CUDA runtime call failed                  */
     VIPE_ERR_DTYPE = 8,        /* unsupported element type                    */
     VIPE_ERR_GROUP = 9,        /* unsupported Lie group id                    */
+    VIPE_ERR_DEVICE_WAIT = 10, /* a kernel's bounded wait on its tensor-core   */
+                               /* work expired; the call's outputs are invalid */
     VIPE_WARN_SOLVER = 16      /* (dev_status only) Cholesky failed: dx = 0   */
 };
 
@@ -88,7 +90,10 @@ size_t vipe_slam_ba_workspace_size(int num_frames, int ht, int wd, int num_edges
  * dev_status: optional device int32; receives VIPE_ERR_INDEX /
  *   VIPE_ERR_KX_MISMATCH / VIPE_ERR_CAPACITY found on the device (the call then
  *   leaves poses/disps untouched) or VIPE_WARN_SOLVER (dx = 0, as the reference
- *   does on Cholesky failure). */
+ *   does on Cholesky failure).
+ * Capacity (VIPE_ERR_CAPACITY): t1 - t0 <= 127 window poses, and at most 31
+ *   window poses (27 for Sim3) coupled to one depth frame (its own pose plus
+ *   the distinct targets of its edges). */
 int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* intrinsics_io, const float* disps_sens,
                           const float* targets, const float* weights, const float* eta, const int64_t* ii,
                           const int64_t* jj, const float* depth_active, int num_frames, int ht, int wd,

@@ -86,6 +86,7 @@ VIPE_ERR_RANGE = 3
 VIPE_ERR_KX_MISMATCH = 4
 VIPE_ERR_CAPACITY = 6
 VIPE_ERR_GROUP = 9
+VIPE_ERR_DEVICE_WAIT = 10
 VIPE_WARN_SOLVER = 16
 
 # dtypes (enum vipe_dtype)

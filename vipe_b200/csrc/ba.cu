@@ -20,9 +20,10 @@
 //   ba_frame_kernel     per (depth frame, pixel chunk): recomputes each edge's
 //                       pose/depth coupling at every pixel, forms C, w, Q, and
 //                       the Schur products sum_p Q e_p e_p^T of the frame's
-//                       slots as a register-tiled SYRK over shared memory.  The
-//                       gradient v = E Q w and the focal couplings ride along as
-//                       two extra columns of e_p.
+//                       slots on tcgen05 tensor cores (split TF32, FP32
+//                       accumulation restarted every 128 pixels and summed with
+//                       round-to-nearest).  The gradient v = E Q w and the focal
+//                       couplings ride along as two extra columns of e_p.
 //   ba_assemble_blocks  one warp per pose pair: the dense FP64 reduced matrix
 //                       A - S from per-edge and per-frame terms, summed in a
 //                       fixed order (deterministic, atomic-free).
@@ -40,6 +41,7 @@
 #include "ba_internal.cuh"
 #include "lie_group.cuh"
 #include "se3_device.cuh"
+#include "tcgen05.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -647,98 +649,217 @@ __global__ void ba_edge_reduce(BAPtrs base, Batch B) {
 
 // ---------------------------------------------------------------- per-frame Schur
 
-__device__ __forceinline__ void decode_tile(int tau, int nt, int& ti, int& tj) {
-    int r = 0, rem = tau;
-    while (rem >= nt - r) {
-        rem -= nt - r;
-        r++;
-    }
-    ti = r;
-    tj = r + rem;
+// Per (depth frame, pixel chunk) CTA: the Schur product sum_p Q_p e_p e_p^T of
+// the frame's slots on tcgen05 tensor cores.
+//
+//   e_p (Dr = dof*m + 2 entries) = sqrt(Q_p) * [slot couplings sum_ch w Jz Jpose,
+//   w_p, Ef_p]: the coupling of each slot pose with the depth at pixel p, plus the
+//   reduced gradient and the focal coupling as two extra columns.
+//
+// One thread stages one pixel: it accumulates e_p in FP32 straight into the
+// operand buffer, then splits each entry into TF32 hi = rna(x) and lo =
+// rna(x - hi).  The buffer holds nk blocks of 32 pixels, each block the hi and
+// the lo operand as K-major 128-byte swizzled matrices (entries x pixels), so
+// one elected thread issues
+//     D += Hi Hi^T + Hi Lo^T + Lo Hi^T        (kind::tf32, M = 128, K = 8)
+// per 8 pixels into an FP32 accumulator in tensor memory: the split keeps the
+// product at FP32 accuracy (the dropped Lo Lo^T term is 2^-22 relative).
+// Entries past Dr in the M / N ranges read whatever follows in shared memory:
+// they only reach accumulator rows / columns >= Dr, which are never stored.
+// Frames with Dr > 128 add a second M tile (entries 128.., N1 columns).  The
+// epilogue reads one accumulator row per thread (tcgen05.ld 32x32b) and writes
+// the upper-triangle 4x4 tiles of the chunk partial (FP64 sums over chunks
+// happen in assembly).  Three CTAs share an SM: their staging overlaps the
+// others' MMAs.
+constexpr int kFrameSmem = 75 * 1024;            // dynamic shared memory of one CTA (3 per SM)
+constexpr int kEdgeCache = 64;                   // edges whose relative pose is cached per CTA
+constexpr uint64_t kFrameWaitNs = 2000000000ull;  // bound on every MMA-completion wait
+
+struct FrameSmemHead {
+    uint64_t mma_bar;
+    uint32_t tmem_base;
+    int fail;
+    float red[kFrameThreads / 32];
+    float etf[kEdgeCache][8];  // relative pose t[3], q[4], scale
+    int eslot[kEdgeCache];
+};
+
+// byte offset of entry q, pixel i (0..31) inside one 128-byte swizzled operand block
+__device__ __forceinline__ uint32_t sw128_off(int q, int i) {
+    return (uint32_t)q * 128u + ((uint32_t)(((i >> 2) ^ q) & 7) << 4) + (uint32_t)(i & 3) * 4u;
 }
 
 template <bool kIntr, int D>
-__global__ void __launch_bounds__(kFrameThreads) ba_frame_kernel(BAPtrs base, Batch B, float alpha, float iscale) {
+__global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base, Batch B, float alpha, float iscale) {
     BA_BIND(B, base);
     if (w.status[0]) return;
     const FrameArgs A{io.poses, io.disps, io.disps_sens, io.intr, io.targets, io.weights, io.eta, io.depth_active, io.jj,
                       alpha, iscale};
-    extern __shared__ float4 stage4[];
-    float* stage = reinterpret_cast<float*>(stage4);
-    __shared__ float red[kFrameThreads / 32];
-    const int s = local_ % d.K, c = local_ / d.K, tid = threadIdx.x;
+    extern __shared__ uint8_t fsm_raw[];
+    FrameSmemHead& sh = *reinterpret_cast<FrameSmemHead*>(fsm_raw);
+    const uint32_t raw_addr = tc::smem_u32(fsm_raw);
+    const uint32_t ops_off = ((raw_addr + (uint32_t)sizeof(FrameSmemHead) + 1023u) & ~1023u) - raw_addr;
+    uint8_t* ops = fsm_raw + ops_off;
+    const uint32_t avail = (uint32_t)kFrameSmem - ops_off;
+
+    const int s = local_ % d.K, c = local_ / d.K, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int HW = d.HW, W = d.W;
     const int k = w.kx[s];
     const float act = A.depth_active[k];
     const int m = w.fp_ptr[s + 1] - w.fp_ptr[s];
     const int self = w.self_slot[s];
     const int eb = w.fe_ptr[s], ee = w.fe_ptr[s + 1];
-    const int Dr = D * m + 2;
+    const int Dm = D * m, Dr = Dm + 2;
     const int nt = (Dr + 3) / 4;
-    const int Dp = 4 * nt;
-    const int npt = nt * (nt + 1) / 2;
-    const int T = (Dp * (256 + 4) <= kStageFloats) ? 256 : 128;
-    const int LD = T + 4;  // entry-major staging: element (entry q, pixel p) at q * LD + p
+    const int R8 = (Dr + 7) & ~7;                          // staged rows (entries)
+    const int N0 = (Dr + 15) & ~15;                        // MMA tile 0: rows 0..127, every column
+    const int N1 = Dr > 128 ? ((Dr - 128 + 15) & ~15) : 0;  // MMA tile 1: rows and columns 128..
+    const int NA = N0 + N1;                                // accumulator columns (stage sum; total follows)
+    uint32_t ncols = 32;
+    while (ncols < (uint32_t)(2 * NA)) ncols <<= 1;
+    const uint32_t half_bytes = (uint32_t)R8 * 128u;   // one operand (hi or lo) of a 32-pixel block
+    const uint32_t blk_bytes = 2u * half_bytes;
+    const uint32_t rows_read = Dr > 128 ? 256u : 128u;  // M rows the A operand spans
+    const uint32_t slack = rows_read > (uint32_t)R8 ? (rows_read - (uint32_t)R8) * 128u : 0u;
+    const int nk = (int)min(4u, (avail - slack) / blk_bytes);  // >= 1 for every admissible frame
+    const int T = 32 * nk;
     const float fx = A.intr[0], fy = A.intr[1], cx = A.intr[2], cy = A.intr[3];
 
-    // Few tiles (small frames) leave most threads idle in the SYRK: then the
-    // pixels of each staged tile are split among KS thread groups, each group
-    // covering every tile over T / KS pixels, and the groups' partial sums are
-    // added once at the end.
-    const int KS = npt > kFrameThreads / 2 ? 1 : (npt > kFrameThreads / 4 ? 2 : 4);
-    const int kgrp = KS > 1 ? tid / npt : 0;
-    int ti[kTilesPerThread], tj[kTilesPerThread];
-    float acc[kTilesPerThread][16];
-#pragma unroll
-    for (int i = 0; i < kTilesPerThread; i++) {
-        const int tau = KS > 1 ? (i == 0 && tid < KS * npt ? tid % npt : npt) : tid + i * kFrameThreads;
-        if (tau < npt) {
-            decode_tile(tau, nt, ti[i], tj[i]);
-        } else {
-            ti[i] = -1;
-            tj[i] = -1;
-        }
-#pragma unroll
-        for (int q = 0; q < 16; q++) acc[i][q] = 0.f;
+    if (tid == 0) {
+        tc::mbar_init(&sh.mma_bar, 1);
+        sh.fail = 0;
+        tc::fence_barrier_init();
     }
+    if (warp == 0) tc::tmem_alloc(&sh.tmem_base, ncols);
+    for (int q = tid; q < min(ee - eb, kEdgeCache); q += kFrameThreads) {
+        const int e = w.fe_list[eb + q];
+        EdgeTf Tf;
+        edge_tf<D>(A.poses, k, (int)A.jj[e], Tf);
+        float* o = sh.etf[q];
+        o[0] = Tf.t[0]; o[1] = Tf.t[1]; o[2] = Tf.t[2];
+        o[3] = Tf.q[0]; o[4] = Tf.q[1]; o[5] = Tf.q[2]; o[6] = Tf.q[3];
+        o[7] = Tf.s;
+        sh.eslot[q] = w.edge_slot[e];
+    }
+    {
+        uint4* z = reinterpret_cast<uint4*>(ops);
+        for (uint32_t i = tid; i < (uint32_t)nk * blk_bytes / 16u; i += kFrameThreads) z[i] = make_uint4(0, 0, 0, 0);
+        tc::fence_proxy_async();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = sh.tmem_base;
+
     float en_alpha = 0.f;
     const int p0 = c * d.chunk_f, p1 = min(HW, p0 + d.chunk_f);
-    for (int base = p0; base < p1; base += T) {
+    const int nst = max(1, (p1 - p0 + T - 1) / T);
+    const int kb = tid >> 5, pi = tid & 31;  // this thread's pixel block and lane inside it
+    uint8_t* hb = ops + (size_t)kb * blk_bytes;
+    uint8_t* lb = hb + half_bytes;
+    const uint32_t idesc0 = tc::instr_desc(tc::kFmtTF32, 128, N0);
+    const uint32_t idesc1 = tc::instr_desc(tc::kFmtTF32, 128, N1 > 0 ? N1 : 16);
+    const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+    // Tensor-core accumulation rounds toward zero, so its bias grows with the
+    // chain length: the MMAs restart the stage accumulator X (columns
+    // [0, NA)) every stage and the stage's sum joins the running total
+    // (columns [NA, 2 NA)) through an FP32 round-to-nearest add.
+    auto flush = [&](bool first) {
+        for (int c0 = 0; c0 < NA; c0 += 16) {
+            float x[16], t[16];
+            tc::tmem_ld16(tmem + lane_base + (uint32_t)c0, x);
+            if (!first) tc::tmem_ld16(tmem + lane_base + (uint32_t)(NA + c0), t);
+            tc::tmem_wait_ld();
+            if (!first) {
+#pragma unroll
+                for (int i = 0; i < 16; i++) x[i] += t[i];
+            }
+            tc::tmem_st16(tmem + lane_base + (uint32_t)(NA + c0), x);
+        }
+        tc::tmem_wait_st();
+    };
+    bool failed = false;
+    int committed = 0;  // MMA batches committed to mma_bar
+    for (int st = 0; st < nst; st++) {
+        if (st > 0) {
+            // the previous stage's MMAs must be done reading before it is overwritten
+            if (tid == 0 && !tc::mbar_wait_bounded(&sh.mma_bar, (uint32_t)(st - 1) & 1u, kFrameWaitNs)) sh.fail = 1;
+            __syncthreads();
+            if (sh.fail) {
+                failed = true;
+                break;
+            }
+            tc::tc_fence_after();
+            flush(st == 1);
+            tc::tc_fence_before();
+        }
         if (tid < T) {
-            float* row = stage + tid;  // this pixel's column, stride LD
-            for (int q = 0; q < Dp; q++) row[q * LD] = 0.f;
-            const int p = base + tid;
+            const int p = p0 + st * T + tid;
             if (p < p1) {
                 const float u = (float)(p % W), v = (float)(p / W);
                 const float disp = A.disps[(size_t)k * HW + p];
+                for (int q = 0; q < Dm; q++) *reinterpret_cast<float*>(hb + sw128_off(q, pi)) = 0.f;
+                float es[D];
+#pragma unroll
+                for (int n = 0; n < D; n++) es[n] = 0.f;
                 float csum = 0.f, bsum = 0.f, efsum = 0.f;
                 for (int q = eb; q < ee; q++) {
                     const int e = w.fe_list[q];
-                    const int b = (int)A.jj[e];
-                    const int sl = w.edge_slot[e];
                     EdgeTf Tf;
-                    edge_tf<D>(A.poses, k, b, Tf);
+                    int sl;
+                    if (q - eb < kEdgeCache) {
+                        const float* o = sh.etf[q - eb];
+                        Tf.t[0] = o[0]; Tf.t[1] = o[1]; Tf.t[2] = o[2];
+                        Tf.q[0] = o[3]; Tf.q[1] = o[4]; Tf.q[2] = o[5]; Tf.q[3] = o[6];
+                        Tf.s = o[7];
+                        sl = sh.eslot[q - eb];
+                    } else {
+                        edge_tf<D>(A.poses, k, (int)A.jj[e], Tf);
+                        sl = w.edge_slot[e];
+                    }
+                    const bool stereo = (int)A.jj[e] == k;
                     const float* tp = A.targets + (size_t)e * 2 * HW;
                     const float* wp = A.weights + (size_t)e * 2 * HW;
                     typename LinOf<D>::T L;
-                    linearize_d<D, kIntr, true>(Tf, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p),
+                    linearize_d<D, kIntr, true>(Tf, stereo, fx, fy, cx, cy, u, v, disp, __ldg(wp + p),
                                                 __ldg(wp + HW + p), __ldg(tp + p), __ldg(tp + HW + p), act, A.iscale,
                                                 L);
+                    const float g0 = L.wd[0] * L.Jz[0], g1 = L.wd[1] * L.Jz[1];
+                    csum += g0 * L.Jz[0] + g1 * L.Jz[1];
+                    bsum += g0 * L.r[0] + g1 * L.r[1];
+                    if (kIntr) efsum += g0 * L.Jf[0] + g1 * L.Jf[1];
+                    float ej[D], ei[D];
 #pragma unroll
-                    for (int ch = 0; ch < 2; ch++) {
-                        const float g = L.wd[ch] * L.Jz[ch];
-                        csum += g * L.Jz[ch];
-                        bsum += L.wd[ch] * L.r[ch] * L.Jz[ch];
-                        if (kIntr) efsum += g * L.Jf[ch];
-                        if (self >= 0) {
+                    for (int n = 0; n < D; n++) ej[n] = g0 * L.Jj[0][n] + g1 * L.Jj[1][n];
+                    if constexpr (D == 6) {
+                        // source rows are -Ad^T(Tij) of the target rows, once per pixel
+                        adj_t(Tf.t, Tf.q, ej, ei);
 #pragma unroll
-                            for (int n = 0; n < D; n++) row[(D * self + n) * LD] += g * L.Ji[ch][n];
-                        }
-                        if (sl >= 0) {
+                        for (int n = 0; n < D; n++) ei[n] = -ei[n];
+                    } else {
 #pragma unroll
-                            for (int n = 0; n < D; n++) row[(D * sl + n) * LD] += g * L.Jj[ch][n];
+                        for (int n = 0; n < D; n++) ei[n] = g0 * L.Ji[0][n] + g1 * L.Ji[1][n];
+                    }
+                    if (self >= 0) {
+#pragma unroll
+                        for (int n = 0; n < D; n++) es[n] += ei[n];
+                    }
+                    if (sl >= 0) {
+                        if (sl == self) {
+#pragma unroll
+                            for (int n = 0; n < D; n++) es[n] += ej[n];
+                        } else {
+#pragma unroll
+                            for (int n = 0; n < D; n++) {
+                                float* dst = reinterpret_cast<float*>(hb + sw128_off(D * sl + n, pi));
+                                *dst += ej[n];
+                            }
                         }
                     }
+                }
+                if (self >= 0) {
+#pragma unroll
+                    for (int n = 0; n < D; n++) *reinterpret_cast<float*>(hb + sw128_off(D * self + n, pi)) = es[n];
                 }
                 const float dsens = A.disps_sens[(size_t)k * HW + p];
                 const float msk = (dsens > 0.f ? 1.f : 0.f) * act;
@@ -754,76 +875,101 @@ __global__ void __launch_bounds__(kFrameThreads) ba_frame_kernel(BAPtrs base, Ba
                 qwf[2] = Ef;
                 const float sq = sqrtf(Q);
                 const float scale = act * sq;
-                for (int q = 0; q < D * m; q++) row[q * LD] *= scale;
-                row[(D * m) * LD] = sq * wv;
-                row[(D * m + 1) * LD] = sq * Ef;
+                for (int q = 0; q < Dr; q++) {
+                    float* hp = reinterpret_cast<float*>(hb + sw128_off(q, pi));
+                    const float x = q < Dm ? *hp * scale : (q == Dm ? sq * wv : sq * Ef);
+                    const float hi = tc::to_tf32(x);
+                    *hp = hi;
+                    *reinterpret_cast<float*>(lb + sw128_off(q, pi)) = tc::to_tf32(x - hi);
+                }
+            } else {
+                for (int q = 0; q < Dr; q++) {
+                    *reinterpret_cast<float*>(hb + sw128_off(q, pi)) = 0.f;
+                    *reinterpret_cast<float*>(lb + sw128_off(q, pi)) = 0.f;
+                }
             }
+            tc::fence_proxy_async();
         }
         __syncthreads();
-        // SYRK over this pixel tile: 4x4 output tiles, 4 pixels per step
-        // (columns of pixels past the chunk end are zero)
+        if (tid == 0) {
+            tc::tc_fence_after();
+            for (int b = 0; b < nk; b++) {
+                const uint8_t* hbb = ops + (size_t)b * blk_bytes;
+                const uint64_t dh = tc::smem_desc_sw128(hbb), dl = tc::smem_desc_sw128(hbb + half_bytes);
 #pragma unroll
-        for (int i = 0; i < kTilesPerThread; i++) {
-            if (ti[i] >= 0) {
-                const float* ra = stage + (size_t)(4 * ti[i]) * LD;
-                const float* rb = stage + (size_t)(4 * tj[i]) * LD;
-                const int qlo = kgrp * (T / KS), qhi = qlo + T / KS;
-                for (int q = qlo; q < qhi; q += 4) {
-                    float4 x[4], y[4];
-#pragma unroll
-                    for (int r = 0; r < 4; r++) {
-                        x[r] = *reinterpret_cast<const float4*>(ra + (size_t)r * LD + q);
-                        y[r] = *reinterpret_cast<const float4*>(rb + (size_t)r * LD + q);
+                for (int kk = 0; kk < 4; kk++) {
+                    const uint64_t o = (uint64_t)(kk * 2);  // 8 TF32 pixels = 32 bytes along the swizzled row
+                    const uint32_t acc = (b | kk) ? 1u : 0u;
+                    tc::mma_tf32(tmem, dh + o, dh + o, idesc0, acc);
+                    tc::mma_tf32(tmem, dh + o, dl + o, idesc0, 1u);
+                    tc::mma_tf32(tmem, dl + o, dh + o, idesc0, 1u);
+                    if (N1 > 0) {
+                        // entries 128..: rows 128.. of the same operands (16 KiB in, atom aligned)
+                        const uint64_t r128 = (uint64_t)(16384 >> 4);
+                        tc::mma_tf32(tmem + (uint32_t)N0, dh + r128 + o, dh + r128 + o, idesc1, acc);
+                        tc::mma_tf32(tmem + (uint32_t)N0, dh + r128 + o, dl + r128 + o, idesc1, 1u);
+                        tc::mma_tf32(tmem + (uint32_t)N0, dl + r128 + o, dh + r128 + o, idesc1, 1u);
                     }
+                }
+            }
+            tc::mma_commit(&sh.mma_bar);
+        }
+        committed++;
+    }
+    if (!failed) {
+        if (tid == 0 && !tc::mbar_wait_bounded(&sh.mma_bar, (uint32_t)(nst - 1) & 1u, kFrameWaitNs)) sh.fail = 1;
+        __syncthreads();
+        failed = sh.fail != 0;
+    }
+    tc::tc_fence_after();
+    if (!failed) {
+        flush(nst == 1);
+        const int toff = w.ftile_off[s];
+        for (int t = 0; t < (N1 > 0 ? 2 : 1); t++) {
+            const int row = (t ? 128 : 0) + 32 * warp + lane;
+            const int ncol = t ? N1 : N0;
+            const int cbase = t ? 128 : 0;
+            const int ti = row >> 2;
+            for (int c0 = 0; c0 < ncol; c0 += 16) {
+                float vv[16];
+                tc::tmem_ld16(tmem + lane_base + (uint32_t)(NA + (t ? N0 : 0) + c0), vv);
+                tc::tmem_wait_ld();
+                if (ti < nt) {
 #pragma unroll
-                    for (int r = 0; r < 4; r++)
-#pragma unroll
-                        for (int cc = 0; cc < 4; cc++) {
-                            float a0 = acc[i][r * 4 + cc];
-                            a0 += x[r].x * y[cc].x;
-                            a0 += x[r].y * y[cc].y;
-                            a0 += x[r].z * y[cc].z;
-                            a0 += x[r].w * y[cc].w;
-                            acc[i][r * 4 + cc] = a0;
+                    for (int g = 0; g < 4; g++) {
+                        const int cg = (cbase + c0) / 4 + g;
+                        if (cg >= ti && cg < nt) {
+                            float4 o;
+                            o.x = (row < Dr && 4 * cg + 0 < Dr) ? vv[4 * g + 0] : 0.f;
+                            o.y = (row < Dr && 4 * cg + 1 < Dr) ? vv[4 * g + 1] : 0.f;
+                            o.z = (row < Dr && 4 * cg + 2 < Dr) ? vv[4 * g + 2] : 0.f;
+                            o.w = (row < Dr && 4 * cg + 3 < Dr) ? vv[4 * g + 3] : 0.f;
+                            const int tau = ti * nt - (ti * (ti - 1)) / 2 + (cg - ti);
+                            *reinterpret_cast<float4*>(w.spart + (((size_t)(toff + tau)) * d.CF + c) * 16 +
+                                                       (row & 3) * 4) = o;
                         }
+                    }
                 }
             }
         }
-        __syncthreads();
-    }
-    const int toff = w.ftile_off[s];
-    if (KS > 1) {
-        // stage is free after the last SYRK step's barrier: add the groups' partials
-        if (tid < KS * npt)
-#pragma unroll
-            for (int q = 0; q < 16; q++) stage[(size_t)tid * 16 + q] = acc[0][q];
-        __syncthreads();
-        if (tid < npt)
-#pragma unroll
-            for (int q = 0; q < 16; q++) {
-                float sv = 0.f;
-                for (int g = 0; g < KS; g++) sv += stage[((size_t)g * npt + tid) * 16 + q];
-                acc[0][q] = sv;
-            }
-    }
-#pragma unroll
-    for (int i = 0; i < kTilesPerThread; i++) {
-        const int tau = tid + i * kFrameThreads;
-        if (tau < npt) {
-            float4* dst = reinterpret_cast<float4*>(w.spart + (((size_t)(toff + tau)) * d.CF + c) * 16);
-            dst[0] = make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
-            dst[1] = make_float4(acc[i][4], acc[i][5], acc[i][6], acc[i][7]);
-            dst[2] = make_float4(acc[i][8], acc[i][9], acc[i][10], acc[i][11]);
-            dst[3] = make_float4(acc[i][12], acc[i][13], acc[i][14], acc[i][15]);
-        }
+    } else if (tid == 0) {
+        w.status[0] = VIPE_ERR_DEVICE_WAIT;
+        // give the last committed MMAs one more bounded chance to finish
+        // before their tensor memory is released
+        if (committed > 0) tc::mbar_wait_bounded(&sh.mma_bar, (uint32_t)(committed - 1) & 1u, kFrameWaitNs);
     }
     const float sres = warp_sum(en_alpha);
-    if ((tid & 31) == 0) red[tid >> 5] = sres;
+    if (lane == 0) sh.red[warp] = sres;
+    tc::tc_fence_before();
     __syncthreads();
     if (tid == 0) {
-        float t = 0.f;
-        for (int q = 0; q < kFrameThreads / 32; q++) t += red[q];
-        w.fen[(size_t)s * d.CF + c] = t;
+        float tsum = 0.f;
+        for (int q = 0; q < kFrameThreads / 32; q++) tsum += sh.red[q];
+        w.fen[(size_t)s * d.CF + c] = tsum;
+    }
+    if (warp == 0) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, ncols);
     }
 }
 
@@ -1423,11 +1569,11 @@ int ensure_attributes() {
     VIPE_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 64 && !g_smem_set[dev]) {
         VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<true, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           kStageFloats * 4));
+                                           kFrameSmem));
         VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<false, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           kStageFloats * 4));
+                                           kFrameSmem));
         VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<false, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           kStageFloats * 4));
+                                           kFrameSmem));
         VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_cholesky_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            chol_ldr(kPanelRows) * kNB * (int)sizeof(double)));
         g_smem_set[dev] = true;
@@ -1484,13 +1630,13 @@ int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const 
     if (with_frames && grid(kOffFrame) > 0) {
         VIPE_PROF("ba_frame", st);
         if (geo.dof == 7)
-            ba_frame_kernel<false, 7><<<grid(kOffFrame), kFrameThreads, kStageFloats * 4, st>>>(
+            ba_frame_kernel<false, 7><<<grid(kOffFrame), kFrameThreads, kFrameSmem, st>>>(
                 base, batch_of(geo, d_table, d_off, kOffFrame), a.alpha, a.iscale);
         else if (intr)
-            ba_frame_kernel<true, 6><<<grid(kOffFrame), kFrameThreads, kStageFloats * 4, st>>>(
+            ba_frame_kernel<true, 6><<<grid(kOffFrame), kFrameThreads, kFrameSmem, st>>>(
                 base, batch_of(geo, d_table, d_off, kOffFrame), a.alpha, a.iscale);
         else
-            ba_frame_kernel<false, 6><<<grid(kOffFrame), kFrameThreads, kStageFloats * 4, st>>>(
+            ba_frame_kernel<false, 6><<<grid(kOffFrame), kFrameThreads, kFrameSmem, st>>>(
                 base, batch_of(geo, d_table, d_off, kOffFrame), a.alpha, a.iscale);
         VIPE_LAUNCH_CHECK();
     }

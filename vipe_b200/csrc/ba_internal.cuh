@@ -11,13 +11,12 @@
 namespace vipe {
 namespace ba {
 
-constexpr int kMaxSlots = 32;          // window poses coupled to one depth frame (SE3; Sim3: 27)
+constexpr int kMaxSlots = 31;          // window poses coupled to one depth frame (SE3; Sim3: 27):
+                                       // 2 x (accumulator columns) of the frame kernel <= 512
 constexpr int kMaxPoses = 127;         // t1 - t0: 6P+1 unknowns fit the staged Cholesky panel
 constexpr int kNT = 105;               // per-edge terms, see term layout below
 constexpr int kEdgeThreads = 256;
-constexpr int kFrameThreads = 256;
-constexpr int kTilesPerThread = 5;     // 4x4 SYRK tiles held in registers per thread
-constexpr int kStageFloats = 25872;    // e' staging: Dp rows x (T + 4) pixels, <= 101 KiB
+constexpr int kFrameThreads = 128;     // one pixel per thread; 32-pixel blocks per warp
 constexpr int kIndexThreads = 1024;
 
 // per-edge term layout

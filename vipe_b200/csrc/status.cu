@@ -106,6 +106,7 @@ extern "C" __attribute__((visibility("default"))) const char* vipe_status_string
         case VIPE_ERR_CUDA: return "CUDA runtime error";
         case VIPE_ERR_DTYPE: return "unsupported dtype";
         case VIPE_ERR_GROUP: return "unsupported Lie group id";
+        case VIPE_ERR_DEVICE_WAIT: return "a kernel's bounded wait on tensor-core work expired";
         case VIPE_WARN_SOLVER: return "reduced camera system not positive definite: dx = 0";
         default: return "unknown status";
     }
