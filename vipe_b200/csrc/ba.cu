@@ -717,10 +717,18 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
     const int NA = N0 + N1;                                // accumulator columns (stage sum; total follows)
     uint32_t ncols = 32;
     while (ncols < (uint32_t)(2 * NA)) ncols <<= 1;
-    const uint32_t half_bytes = (uint32_t)R8 * 128u;   // one operand (hi or lo) of a 32-pixel block
+    // Frames of <= 64 entries stack the hi rows (0..63) and the lo rows
+    // (64..127) of a block into one M = 128 operand: a single MMA against the
+    // hi rows yields Hi Hi^T in accumulator lanes 0..63 and Lo Hi^T in lanes
+    // 64..127; Hi Lo^T is the transpose of the latter, added in the epilogue.
+    const bool pack = Dr <= 64;
+    const int HR = pack ? 64 : R8;                      // rows of one operand half
+    const uint32_t half_bytes = (uint32_t)HR * 128u;    // one operand (hi or lo) of a 32-pixel block
     const uint32_t blk_bytes = 2u * half_bytes;
-    const uint32_t rows_read = Dr > 128 ? 256u : 128u;  // M rows the A operand spans
-    const uint32_t slack = rows_read > (uint32_t)R8 ? (rows_read - (uint32_t)R8) * 128u : 0u;
+    const uint32_t rows_read = Dr > 128 ? 256u : 128u;  // M rows an A operand spans from its base
+    // the highest A base is the lo half (split path) or the block itself (packed)
+    const uint32_t a_top = pack ? blk_bytes : half_bytes + rows_read * 128u;
+    const uint32_t slack = a_top > blk_bytes ? a_top - blk_bytes : 0u;
     const int nk = (int)min(4u, (avail - slack) / blk_bytes);  // >= 1 for every admissible frame
     const int T = 32 * nk;
     const float fx = A.intr[0], fy = A.intr[1], cx = A.intr[2], cy = A.intr[3];
@@ -900,6 +908,10 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
                 for (int kk = 0; kk < 4; kk++) {
                     const uint64_t o = (uint64_t)(kk * 2);  // 8 TF32 pixels = 32 bytes along the swizzled row
                     const uint32_t acc = (b | kk) ? 1u : 0u;
+                    if (pack) {
+                        tc::mma_tf32(tmem, dh + o, dh + o, idesc0, acc);  // A = [Hi; Lo], B = Hi
+                        continue;
+                    }
                     tc::mma_tf32(tmem, dh + o, dh + o, idesc0, acc);
                     tc::mma_tf32(tmem, dh + o, dl + o, idesc0, 1u);
                     tc::mma_tf32(tmem, dl + o, dh + o, idesc0, 1u);
@@ -922,7 +934,51 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
         failed = sh.fail != 0;
     }
     tc::tc_fence_after();
-    if (!failed) {
+    if (!failed && pack) {
+        flush(nst == 1);
+        // S = X + Z + Z^T with X = Hi Hi^T (lanes 0..63) and Z = Lo Hi^T (lanes 64..127)
+        float* zs = reinterpret_cast<float*>(ops);  // [64][N0 + 1], the operands are free
+        const int ZL = N0 + 1;
+        if (warp >= 2) {
+            for (int c0 = 0; c0 < N0; c0 += 16) {
+                float vv[16];
+                tc::tmem_ld16(tmem + lane_base + (uint32_t)(NA + c0), vv);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int j = 0; j < 16; j++) zs[(32 * (warp - 2) + lane) * ZL + c0 + j] = vv[j];
+            }
+        }
+        __syncthreads();
+        if (warp < 2) {
+            const int toff = w.ftile_off[s];
+            const int row = 32 * warp + lane;
+            const int ti = row >> 2;
+            for (int c0 = 0; c0 < N0; c0 += 16) {
+                float vv[16];
+                tc::tmem_ld16(tmem + lane_base + (uint32_t)(NA + c0), vv);
+                tc::tmem_wait_ld();
+                if (ti < nt) {
+#pragma unroll
+                    for (int g = 0; g < 4; g++) {
+                        const int cg = c0 / 4 + g;
+                        if (cg >= ti && cg < nt) {
+                            float o4[4];
+#pragma unroll
+                            for (int j = 0; j < 4; j++) {
+                                const int col = 4 * cg + j;
+                                o4[j] = (row < Dr && col < Dr)
+                                            ? vv[4 * g + j] + zs[row * ZL + col] + zs[col * ZL + row]
+                                            : 0.f;
+                            }
+                            const int tau = ti * nt - (ti * (ti - 1)) / 2 + (cg - ti);
+                            *reinterpret_cast<float4*>(w.spart + (((size_t)(toff + tau)) * d.CF + c) * 16 +
+                                                       (row & 3) * 4) = make_float4(o4[0], o4[1], o4[2], o4[3]);
+                        }
+                    }
+                }
+            }
+        }
+    } else if (!failed) {
         flush(nst == 1);
         const int toff = w.ftile_off[s];
         for (int t = 0; t < (N1 > 0 ? 2 : 1); t++) {
