@@ -155,6 +155,23 @@ class BatchPlan:
         _lib.check(rc, "BatchPlan.solve")
         return dx, dz, energy, status
 
+    def backward(self, tape, intrinsics, disps_sens, targets, weights, eta, ii, jj, depth_active, iterations, lm, ep,
+                 alpha, grad_poses, grad_disps, grad_targets, grad_weights, grad_eta, grad_disps_sens, status):
+        """Hand-written adjoint of the solve that filled ``tape`` (plan created with adjoint=True).
+
+        grad_poses (frames, dof+1) and grad_disps (frames, H, W) hold the incoming
+        gradients of the solve's outputs and receive those of its input poses and
+        depths; grad_targets, grad_weights, grad_eta, grad_disps_sens are written;
+        status (G,) int32 receives per-graph device status.  Only enqueues work on
+        the current stream (no allocation, copy or synchronisation)."""
+        rc = _lib.load().vipe_slam_ba_batch_backward(
+            self._h, *[t.data_ptr() for t in tape], intrinsics.data_ptr(), disps_sens.data_ptr(), targets.data_ptr(),
+            weights.data_ptr(), eta.data_ptr(), ii.data_ptr(), jj.data_ptr(), depth_active.data_ptr(), int(iterations),
+            float(lm), float(ep), float(alpha), grad_poses.data_ptr(), grad_disps.data_ptr(), grad_targets.data_ptr(),
+            grad_weights.data_ptr(), grad_eta.data_ptr(), grad_disps_sens.data_ptr(), status.data_ptr(),
+            torch.cuda.current_stream(self.device).cuda_stream)
+        _lib.check(rc, "BatchPlan.backward")
+
     def capture(self, batch: dict, iterations: int, lm: float, ep: float, **kw) -> "CapturedSolve":
         """Captures the whole solve (index build + LM loop) on `batch`'s tensors as a CUDA graph."""
         return CapturedSolve(self, batch, iterations, lm, ep, **kw)

@@ -47,7 +47,6 @@ namespace ba {
 
 constexpr int kAdjThreads = 256;
 constexpr int kAdjMaxDeg = 64;       // edges leaving one depth frame
-constexpr int kAdjMaxChunk = 1536;   // pixels of one (frame, chunk) block (two blocks per SM fit)
 
 // ---------------------------------------------------------------- small helpers
 
@@ -611,7 +610,11 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
         const int e = w.fe_list[eb + q];
         const int b = (int)io.jj[e];
         const bool stereo = k == b;
-        const float* Eq = Esh[q];
+        // read through a volatile view: every use reloads from shared memory instead of
+        // the compiler hoisting the edge's 60 constants into registers for the pixel loop
+        // (which spilled the loop's own state)
+        const volatile float* Eq = Esh[q];
+        const float* Eqc = Esh[q];
         const float* tp = io.targets + (size_t)e * 2 * HW;
         const float* wp = io.weights + (size_t)e * 2 * HW;
         float* gtp = io.g_targets + (size_t)e * 2 * HW;
@@ -624,7 +627,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
             const float u = (float)(p % W), v = (float)(p / W);
             const float X[4] = {(u - cx) / fx, (v - cy) / fy, 1.f, pdisp[i]};
             PixJ J;
-            if (!pix_jac(Eq, X, fx, fy, J)) continue;  // invalid pixel: zero weight, no gradient
+            if (!pix_jac(Eqc, X, fx, fy, J)) continue;  // invalid pixel: zero weight, no gradient
             const float iz = J.iz, iz2 = iz * iz;
             const float a = pa[i], dzf = pdzf[i], mu = pmu[i], gwz = pgwz[i], gC = pgC[i], Q = pQ[i];
             const float rr[2] = {__ldg(tp + p) - (fx * J.P[0] * iz + cx), __ldg(tp + HW + p) - (fy * J.P[1] * iz + cy)};
@@ -708,7 +711,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
 #pragma unroll
                 for (int n = 0; n < 12; n++) fu += J.J[ch][n] * ud[n];
                 DirPix D;
-                dir_pix(Eq, X, J.P, ud, D);
+                dir_pix(Eqc, X, J.P, ud, D);
                 gdp += mixed(J, ch, fxy, ud, D, fu, 1.f, g0h, g0x, om);
             }
             // depth s-direction of this pixel: Ps = t (column 3 of M0)
