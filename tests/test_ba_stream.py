@@ -73,3 +73,26 @@ def test_streamed_step_equals_one_plan():
     assert int(runner.status().abs().sum()) == 0
     for k in OUTPUT_KEYS:
         torch.testing.assert_close(out[k], want[k].cpu(), rtol=0, atol=0, msg=k)
+
+
+@pytest.mark.gpu
+def test_streamed_forward_only_equals_one_plan():
+    from vipe_b200 import workloads as W
+    from vipe_b200.ba_batch import BATCH_KEYS, BatchPlan
+    from vipe_b200.ba_stream import StreamedBundleAdjust
+
+    b = W.make_ba_batch(9, seed=78, frames_range=(8, 24), device="cuda")
+    it, lm, ep = 3, 1e-4, 0.1
+    T = b.tensors
+    plan = BatchPlan(*b.sizes, b.ht, b.wd, "cuda", edge_chunks=2, frame_chunks=1)
+    s = {k: v.clone() for k, v in T.items()}
+    plan.solve(**s, iterations=it, lm=lm, ep=ep)
+    runner = StreamedBundleAdjust(b.sizes, b.ht, b.wd, "cuda", parts=4, iterations=it, lm=lm, ep=ep, edge_chunks=2,
+                                  frame_chunks=1, adjoint=False)
+    host = {k: T[k].cpu().pin_memory() for k in BATCH_KEYS}
+    out = runner.host_outputs()
+    assert set(out) == {"poses", "disps"}
+    runner.step(host, None, None, out)
+    torch.cuda.current_stream().synchronize()
+    torch.testing.assert_close(out["poses"], s["poses"].cpu(), rtol=0, atol=0)
+    torch.testing.assert_close(out["disps"], s["disps"].cpu(), rtol=0, atol=0)

@@ -74,7 +74,7 @@ class StreamedBundleAdjust:
 
     def __init__(self, sizes, ht: int, wd: int, device, parts: int = 8, iterations: int = 4, lm: float = 1e-4,
                  ep: float = 0.1, alpha: float = 0.001, edge_chunks: int = 0, frame_chunks: int = 0,
-                 group: str = "se3"):
+                 group: str = "se3", adjoint: bool = True):
         num_frames, num_edges, num_kx, t0, t1 = (list(map(int, x)) for x in sizes)
         self.device = torch.device(device)
         if self.device.type == "cuda" and self.device.index is None:
@@ -84,14 +84,17 @@ class StreamedBundleAdjust:
         self.G = len(num_frames)
         self.total_frames, self.total_edges, self.total_kx = sum(num_frames), sum(num_edges), sum(num_kx)
         self.dof = 7 if group == "sim3" else 6
+        self.adjoint = bool(adjoint)
+        if self.adjoint and group != "se3":
+            raise RuntimeError("StreamedBundleAdjust: the adjoint covers SE3 graphs only")
         self.parts: list[_Part] = []
         HW = (self.ht, self.wd)
         f0 = e0 = k0 = 0
         for ga, gb in split_clips(num_edges, parts):
             nf, ne, nk = sum(num_frames[ga:gb]), sum(num_edges[ga:gb]), sum(num_kx[ga:gb])
             plan = BatchPlan(num_frames[ga:gb], num_edges[ga:gb], num_kx[ga:gb], t0[ga:gb], t1[ga:gb], self.ht,
-                             self.wd, self.device, edge_chunks=edge_chunks, frame_chunks=frame_chunks, adjoint=True,
-                             group=group)
+                             self.wd, self.device, edge_chunks=edge_chunks, frame_chunks=frame_chunks,
+                             adjoint=self.adjoint, group=group)
             dev = self.device
             f32 = dict(dtype=torch.float32, device=dev)
             d = {
@@ -113,10 +116,11 @@ class StreamedBundleAdjust:
                 "grad_weights": torch.empty(ne, 2, *HW, **f32),
                 "grad_eta": torch.empty(nk, *HW, **f32),
                 "grad_disps_sens": torch.empty(nf, *HW, **f32),
-            }
+            } if self.adjoint else {}
             self.parts.append(_Part(g=(ga, gb), f=(f0, f0 + nf), e=(e0, e0 + ne), k=(k0, k0 + nk), plan=plan,
                                     stream=torch.cuda.Stream(dev), dev=d, grads=grads,
-                                    tape=plan.make_tape(self.iterations), out=plan.outputs(self.iterations),
+                                    tape=plan.make_tape(self.iterations) if self.adjoint else None,
+                                    out=plan.outputs(self.iterations),
                                     status=torch.zeros(gb - ga, dtype=torch.int32, device=dev),
                                     done=torch.cuda.Event()))
             f0, e0, k0 = f0 + nf, e0 + ne, k0 + nk
@@ -126,6 +130,8 @@ class StreamedBundleAdjust:
         HW = (self.ht, self.wd)
         pin = dict(dtype=torch.float32, pin_memory=True)
         F, E, K = self.total_frames, self.total_edges, self.total_kx
+        if not self.adjoint:
+            return {"poses": torch.empty(F, self.dof + 1, **pin), "disps": torch.empty(F, *HW, **pin)}
         return {
             "poses": torch.empty(F, self.dof + 1, **pin),
             "disps": torch.empty(F, *HW, **pin),
@@ -146,14 +152,15 @@ class StreamedBundleAdjust:
             return part.g
         return part.f
 
-    def step(self, host: dict, host_grad_poses: torch.Tensor, host_grad_disps: torch.Tensor, host_out: dict,
-             stream: torch.cuda.Stream | None = None) -> None:
-        """Enqueues one forward + backward over the batch held in pinned host tensors.
+    def step(self, host: dict, host_grad_poses: torch.Tensor | None, host_grad_disps: torch.Tensor | None,
+             host_out: dict, stream: torch.cuda.Stream | None = None) -> None:
+        """Enqueues one forward (+ backward) over the batch held in pinned host tensors.
 
         ``host`` holds the batched inputs (BATCH_KEYS, concatenated layout),
         host_grad_poses / host_grad_disps the incoming gradients of the solved
-        poses and depths; ``host_out`` (from host_outputs) receives the solved
-        state and every input gradient.  Work starts after what is already queued
+        poses and depths (None for a forward-only runner); ``host_out`` (from
+        host_outputs) receives the solved state and, with the adjoint, every
+        input gradient.  Work starts after what is already queued
         on ``stream`` (default: the current stream) and that stream waits for all
         of it, so events recorded there bracket the whole step."""
         caller = stream if stream is not None else torch.cuda.current_stream(self.device)
@@ -166,16 +173,18 @@ class StreamedBundleAdjust:
                     a, b = self._rows(part, key)
                     part.dev[key].copy_(host[key][a:b], non_blocking=True)
                 fa, fb = part.f
-                part.grads["grad_poses"].copy_(host_grad_poses[fa:fb], non_blocking=True)
-                part.grads["grad_disps"].copy_(host_grad_disps[fa:fb], non_blocking=True)
                 d, gr = part.dev, part.grads
+                if self.adjoint:
+                    gr["grad_poses"].copy_(host_grad_poses[fa:fb], non_blocking=True)
+                    gr["grad_disps"].copy_(host_grad_disps[fa:fb], non_blocking=True)
                 part.plan.solve(**d, iterations=self.iterations, lm=self.lm, ep=self.ep, alpha=self.alpha,
                                 out=part.out, check=False, tape=part.tape)
-                part.plan.backward(part.tape, d["intrinsics"], d["disps_sens"], d["targets"], d["weights"], d["eta"],
-                                   d["ii"], d["jj"], d["depth_active"], self.iterations, self.lm, self.ep, self.alpha,
-                                   gr["grad_poses"], gr["grad_disps"], gr["grad_targets"], gr["grad_weights"],
-                                   gr["grad_eta"], gr["grad_disps_sens"], part.status)
-                for key in OUTPUT_KEYS:
+                if self.adjoint:
+                    part.plan.backward(part.tape, d["intrinsics"], d["disps_sens"], d["targets"], d["weights"],
+                                       d["eta"], d["ii"], d["jj"], d["depth_active"], self.iterations, self.lm, self.ep,
+                                       self.alpha, gr["grad_poses"], gr["grad_disps"], gr["grad_targets"],
+                                       gr["grad_weights"], gr["grad_eta"], gr["grad_disps_sens"], part.status)
+                for key in host_out:
                     a, b = self._rows(part, key)
                     src = d[key] if key in d else gr[key]
                     host_out[key][a:b].copy_(src, non_blocking=True)
@@ -187,8 +196,8 @@ class StreamedBundleAdjust:
         return torch.cat([p.out[3] | p.status for p in self.parts])
 
     def h2d_bytes(self, host: dict) -> int:
-        return sum(host[k].numel() * host[k].element_size() for k in BATCH_KEYS) + \
-            self.total_frames * (self.dof + 1) * 4 + self.total_frames * self.ht * self.wd * 4
+        grads = self.total_frames * (self.dof + 1) * 4 + self.total_frames * self.ht * self.wd * 4
+        return sum(host[k].numel() * host[k].element_size() for k in BATCH_KEYS) + (grads if self.adjoint else 0)
 
     def d2h_bytes(self, host_out: dict) -> int:
         return sum(v.numel() * v.element_size() for v in host_out.values())

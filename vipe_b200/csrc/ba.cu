@@ -405,6 +405,28 @@ __device__ __forceinline__ void edge_tf(const float* poses, int a, int b, EdgeTf
     }
 }
 
+// y = Ad(Tij) x for a tangent x of the source pose: the source-pose Jacobian rows
+// are -Ad^T(Tij) times the target-pose rows, so Ji . x = -Jj . (Ad x).
+//   SE3:  Ad = [[R, [t]x R], [0, R]];   Sim3: Ad = [[s R, [t]x R, -t], [0, R, 0], [0, 0, 1]]
+template <int D>
+__device__ __forceinline__ void edge_ad_apply(const EdgeTf& T, const float* x, float* y) {
+    float rt[3], rp[3];
+    qrot(T.q, x, rt);
+    qrot(T.q, x + 3, rp);
+    y[0] = T.s * rt[0] + (T.t[1] * rp[2] - T.t[2] * rp[1]);
+    y[1] = T.s * rt[1] + (T.t[2] * rp[0] - T.t[0] * rp[2]);
+    y[2] = T.s * rt[2] + (T.t[0] * rp[1] - T.t[1] * rp[0]);
+    y[3] = rp[0];
+    y[4] = rp[1];
+    y[5] = rp[2];
+    if constexpr (D == 7) {
+        y[0] -= T.t[0] * x[6];
+        y[1] -= T.t[1] * x[6];
+        y[2] -= T.t[2] * x[6];
+        y[6] = x[6];
+    }
+}
+
 template <bool kResidual>
 __device__ __forceinline__ void linearize_sim3(const EdgeTf& T, bool stereo, float fx, float fy, float cx, float cy,
                                                float u, float v, float disp, float wu_in, float wv_in, float tu,
@@ -672,7 +694,6 @@ __global__ void ba_edge_reduce(BAPtrs base, Batch B) {
 // happen in assembly).  Three CTAs share an SM: their staging overlaps the
 // others' MMAs.
 constexpr int kFrameSmem = 75 * 1024;            // dynamic shared memory of one CTA (3 per SM)
-constexpr int kEdgeCache = 64;                   // edges whose relative pose is cached per CTA
 constexpr uint64_t kFrameWaitNs = 2000000000ull;  // bound on every MMA-completion wait
 
 struct FrameSmemHead {
@@ -681,7 +702,8 @@ struct FrameSmemHead {
     int fail;
     float red[kFrameThreads / 32];
     float etf[kEdgeCache][8];  // relative pose t[3], q[4], scale
-    int eslot[kEdgeCache];
+    int eslot[kEdgeCache];     // slot of the edge's target pose (-1: outside the window)
+    int eid[kEdgeCache];       // edge index; bit 31: stereo edge
 };
 
 // byte offset of entry q, pixel i (0..31) inside one 128-byte swizzled operand block
@@ -748,6 +770,7 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
         o[3] = Tf.q[0]; o[4] = Tf.q[1]; o[5] = Tf.q[2]; o[6] = Tf.q[3];
         o[7] = Tf.s;
         sh.eslot[q] = w.edge_slot[e];
+        sh.eid[q] = e | ((int)A.jj[e] == k ? (int)0x80000000u : 0);
     }
     {
         uint4* z = reinterpret_cast<uint4*>(ops);
@@ -811,8 +834,31 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
 #pragma unroll
                 for (int n = 0; n < D; n++) es[n] = 0.f;
                 float csum = 0.f, bsum = 0.f, efsum = 0.f;
-                for (int q = eb; q < ee; q++) {
+                // edge id (bit 31: stereo) of frame edge q, from the cache when it holds it
+                auto edge_of = [&](int q) {
+                    if (q - eb < kEdgeCache) return sh.eid[q - eb];
                     const int e = w.fe_list[q];
+                    return e | ((int)A.jj[e] == k ? (int)0x80000000u : 0);
+                };
+                // this pixel's targets and weights of the next edge are loaded one edge ahead
+                float nw0 = 0.f, nw1 = 0.f, nt0 = 0.f, nt1 = 0.f;
+                int enext = eb < ee ? edge_of(eb) : 0;
+                if (eb < ee) {
+                    const size_t o = (size_t)(enext & 0x7fffffff) * 2 * HW + p;
+                    nw0 = __ldg(A.weights + o); nw1 = __ldg(A.weights + o + HW);
+                    nt0 = __ldg(A.targets + o); nt1 = __ldg(A.targets + o + HW);
+                }
+                for (int q = eb; q < ee; q++) {
+                    const int ecode = enext;
+                    const int e = ecode & 0x7fffffff;
+                    const bool stereo = ecode < 0;
+                    const float w0 = nw0, w1 = nw1, t0v = nt0, t1v = nt1;
+                    if (q + 1 < ee) {
+                        enext = edge_of(q + 1);
+                        const size_t o = (size_t)(enext & 0x7fffffff) * 2 * HW + p;
+                        nw0 = __ldg(A.weights + o); nw1 = __ldg(A.weights + o + HW);
+                        nt0 = __ldg(A.targets + o); nt1 = __ldg(A.targets + o + HW);
+                    }
                     EdgeTf Tf;
                     int sl;
                     if (q - eb < kEdgeCache) {
@@ -825,13 +871,9 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
                         edge_tf<D>(A.poses, k, (int)A.jj[e], Tf);
                         sl = w.edge_slot[e];
                     }
-                    const bool stereo = (int)A.jj[e] == k;
-                    const float* tp = A.targets + (size_t)e * 2 * HW;
-                    const float* wp = A.weights + (size_t)e * 2 * HW;
                     typename LinOf<D>::T L;
-                    linearize_d<D, kIntr, true>(Tf, stereo, fx, fy, cx, cy, u, v, disp, __ldg(wp + p),
-                                                __ldg(wp + HW + p), __ldg(tp + p), __ldg(tp + HW + p), act, A.iscale,
-                                                L);
+                    linearize_d<D, kIntr, true>(Tf, stereo, fx, fy, cx, cy, u, v, disp, w0, w1, t0v, t1v, act,
+                                                A.iscale, L);
                     const float g0 = L.wd[0] * L.Jz[0], g1 = L.wd[1] * L.Jz[1];
                     csum += g0 * L.Jz[0] + g1 * L.Jz[1];
                     bsum += g0 * L.r[0] + g1 * L.r[1];
@@ -1511,6 +1553,29 @@ __global__ void __launch_bounds__(256, 3) ba_backsub_kernel(BAPtrs base, Batch B
     const int eb = w.fe_ptr[s], ee = w.fe_ptr[s + 1];
     const float fx = A.intr[0], fy = A.intr[1], cx = A.intr[2], cy = A.intr[3];
     const float df = kIntr ? (float)w.df[0] : 0.f;
+    // per edge, once per CTA: the relative pose and v = dx_j - Ad(Tij) dx_i, so the
+    // pixel's E~^T dx term is sum_c g_c Jj_c . v (rows of pose t0 and of poses
+    // outside the window contribute nothing)
+    __shared__ float etf[kEdgeCache][8];
+    __shared__ float ev[kEdgeCache][8];  // v (D entries); [7] > 0: the edge contributes
+    const int ncache = min(ee - eb, kEdgeCache);
+    for (int q = threadIdx.x; q < ncache; q += blockDim.x) {
+        const int e = w.fe_list[eb + q];
+        const int b = (int)A.jj[e];
+        const int bp = b - d.t0;
+        const bool on = w.edge_slot[e] >= 0 && bp > 0 && bp < P;
+        EdgeTf Tf;
+        edge_tf<D>(A.poses, k, b, Tf);
+        float vi[D], vo[D];
+        for (int n = 0; n < D; n++) vi[n] = self_on ? dx[D * selfpose + n] : 0.f;
+        edge_ad_apply<D>(Tf, vi, vo);
+        for (int n = 0; n < D; n++) ev[q][n] = (on ? dx[D * bp + n] : 0.f) - (self_on ? vo[n] : 0.f);
+        ev[q][7] = (on || self_on) ? 1.f : 0.f;
+        etf[q][0] = Tf.t[0]; etf[q][1] = Tf.t[1]; etf[q][2] = Tf.t[2];
+        etf[q][3] = Tf.q[0]; etf[q][4] = Tf.q[1]; etf[q][5] = Tf.q[2]; etf[q][6] = Tf.q[3];
+        etf[q][7] = Tf.s;
+    }
+    __syncthreads();
     const int p0 = c * d.chunk_f, p1 = min(HW, p0 + d.chunk_f);
     for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
         const float u = (float)(p % W), v = (float)(p / W);
@@ -1519,12 +1584,29 @@ __global__ void __launch_bounds__(256, 3) ba_backsub_kernel(BAPtrs base, Batch B
         for (int q = eb; q < ee; q++) {
             const int e = w.fe_list[q];
             const int b = (int)A.jj[e];
-            const int sl = w.edge_slot[e];
-            const int bp = b - d.t0;
-            const bool on = sl >= 0 && bp > 0 && bp < P;
-            if (!on && !self_on) continue;
             EdgeTf Tf;
-            edge_tf<D>(A.poses, k, b, Tf);
+            float vv[D];
+            if (q - eb < kEdgeCache) {
+                const float* o = ev[q - eb];
+                if (o[7] == 0.f) continue;
+#pragma unroll
+                for (int n = 0; n < D; n++) vv[n] = o[n];
+                const float* t = etf[q - eb];
+                Tf.t[0] = t[0]; Tf.t[1] = t[1]; Tf.t[2] = t[2];
+                Tf.q[0] = t[3]; Tf.q[1] = t[4]; Tf.q[2] = t[5]; Tf.q[3] = t[6];
+                Tf.s = t[7];
+            } else {
+                const int bp = b - d.t0;
+                const bool on = w.edge_slot[e] >= 0 && bp > 0 && bp < P;
+                if (!on && !self_on) continue;
+                edge_tf<D>(A.poses, k, b, Tf);
+                float vi[D], vo[D];
+#pragma unroll
+                for (int n = 0; n < D; n++) vi[n] = self_on ? dx[D * selfpose + n] : 0.f;
+                edge_ad_apply<D>(Tf, vi, vo);
+#pragma unroll
+                for (int n = 0; n < D; n++) vv[n] = (on ? dx[D * bp + n] : 0.f) - (self_on ? vo[n] : 0.f);
+            }
             const float* wp = A.weights + (size_t)e * 2 * HW;
             typename LinOf<D>::T L;
             linearize_d<D, false, false>(Tf, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p), __ldg(wp + HW + p),
@@ -1532,14 +1614,10 @@ __global__ void __launch_bounds__(256, 3) ba_backsub_kernel(BAPtrs base, Batch B
 #pragma unroll
             for (int ch = 0; ch < 2; ch++) {
                 const float g = L.wd[ch] * L.Jz[ch];
-                if (self_on) {
+                float jv = 0.f;
 #pragma unroll
-                    for (int n = 0; n < D; n++) dot += g * L.Ji[ch][n] * dx[D * selfpose + n];
-                }
-                if (on) {
-#pragma unroll
-                    for (int n = 0; n < D; n++) dot += g * L.Jj[ch][n] * dx[D * bp + n];
-                }
+                for (int n = 0; n < D; n++) jv += L.Jj[ch][n] * vv[n];
+                dot += g * jv;
             }
         }
         dot *= act;

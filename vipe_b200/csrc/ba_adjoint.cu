@@ -221,6 +221,13 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_a_kernel(BAPtrs base
         return;
     }
     const int eb = w.fe_ptr[s], ee = w.fe_ptr[s + 1];
+    // relative pose of each edge, once per CTA
+    __shared__ float etf[kEdgeCache][7];
+    for (int q = tid; q < min(ee - eb, kEdgeCache); q += kAdjThreads) {
+        const int e = w.fe_list[eb + q];
+        edge_pose(io.poses, k, (int)io.jj[e], etf[q], etf[q] + 3);
+    }
+    __syncthreads();
     for (int p = p0 + tid; p < p1; p += kAdjThreads) {
         const float u = (float)(p % W), v = (float)(p / W);
         const float disp = io.disps[(size_t)k * HW + p];
@@ -229,7 +236,13 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_a_kernel(BAPtrs base
             const int e = w.fe_list[q];
             const int b = (int)io.jj[e];
             float tij[3], qij[4];
-            edge_pose(io.poses, k, b, tij, qij);
+            if (q - eb < kEdgeCache) {
+                const float* o = etf[q - eb];
+                tij[0] = o[0]; tij[1] = o[1]; tij[2] = o[2];
+                qij[0] = o[3]; qij[1] = o[4]; qij[2] = o[5]; qij[3] = o[6];
+            } else {
+                edge_pose(io.poses, k, b, tij, qij);
+            }
             const float* tp = io.targets + (size_t)e * 2 * HW;
             const float* wp = io.weights + (size_t)e * 2 * HW;
             PixelLin L;
@@ -258,9 +271,11 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_a_kernel(BAPtrs base
         const int b = (int)io.jj[e];
         float tij[3], qij[4];
         edge_pose(io.poses, k, b, tij, qij);
-        float acc[12];
+        // source rows are -Ad^T(Tij) of the target rows, so only the target-pose sums
+        // are accumulated per pixel; the source half follows once per edge
+        float acc[6];
 #pragma unroll
-        for (int n = 0; n < 12; n++) acc[n] = 0.f;
+        for (int n = 0; n < 6; n++) acc[n] = 0.f;
         if (act != 0.f) {
             const float* wp = io.weights + (size_t)e * 2 * HW;
             for (int p = p0 + tid; p < p1; p += kAdjThreads) {
@@ -274,23 +289,29 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_a_kernel(BAPtrs base
                 for (int ch = 0; ch < 2; ch++) {
                     const float g = a * act * L.wd[ch] * L.Jz[ch];
 #pragma unroll
-                    for (int n = 0; n < 6; n++) {
-                        acc[n] += g * L.Ji[ch][n];
-                        acc[6 + n] += g * L.Jj[ch][n];
-                    }
+                    for (int n = 0; n < 6; n++) acc[n] += g * L.Jj[ch][n];
                 }
             }
         }
 #pragma unroll
-        for (int n = 0; n < 12; n++) {
+        for (int n = 0; n < 6; n++) {
             const float sv = warp_sum(acc[n]);
             if (lane == 0) red[warp][n] = sv;
         }
         __syncthreads();
-        if (tid < 12) {
-            float sv = 0.f;
-            for (int r = 0; r < kAdjThreads / 32; r++) sv += red[r][tid];
-            w.adj_aslot[((size_t)e * d.CF + c) * 12 + tid] = sv;
+        if (tid == 0) {
+            float sj[6], si[6];
+            for (int n = 0; n < 6; n++) {
+                float sv = 0.f;
+                for (int r = 0; r < kAdjThreads / 32; r++) sv += red[r][n];
+                sj[n] = sv;
+            }
+            adj_t(tij, qij, sj, si);
+            float* o = w.adj_aslot + ((size_t)e * d.CF + c) * 12;
+            for (int n = 0; n < 6; n++) {
+                o[n] = -si[n];
+                o[6 + n] = sj[n];
+            }
         }
         __syncthreads();
     }

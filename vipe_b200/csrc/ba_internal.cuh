@@ -18,6 +18,7 @@ constexpr int kNT = 105;               // per-edge terms, see term layout below
 constexpr int kEdgeThreads = 256;
 constexpr int kFrameThreads = 128;     // one pixel per thread; 32-pixel blocks per warp
 constexpr int kIndexThreads = 1024;
+constexpr int kEdgeCache = 64;        // edges of a depth frame whose per-edge constants a CTA caches
 constexpr int kAdjMaxChunk = 1536;    // pixels of one (frame, chunk) block of the adjoint frame kernels
 
 // per-edge term layout
