@@ -207,7 +207,8 @@ void vipe_slam_ba_batch_plan_destroy(vipe_ba_batch_plan* plan);
  *     layout, column 6 = 0;
  *   grad_disps (sum frames, ht, wd): in, d loss / d disps_out; out, d loss / d disps_in;
  *   grad_targets, grad_weights (sum edges, 2, ht, wd), grad_eta (sum kx, ht, wd),
- *   grad_disps_sens (sum frames, ht, wd): out.  dev_status as in the solve. */
+ *   grad_disps_sens (sum frames, ht, wd): out.  dev_status as in the solve; the
+ *   gradients of a graph whose status holds an error code are undefined. */
 int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const float* tape_poses, const float* tape_disps,
                                 const double* tape_factor, const float* tape_dx, const float* intrinsics,
                                 const float* disps_sens, const float* targets, const float* weights, const float* eta,

@@ -443,12 +443,13 @@ __device__ __forceinline__ float mixed(const PixJ& J, int ch, float fxy, const f
 }
 
 constexpr int kPixF = 14;   // per-pixel floats kept in shared memory by ba_adj_frame_b_kernel
-constexpr int kEdgeF = 60;  // per-edge floats: M0, directions x3, damping weights
+constexpr int kEdgeF = 78;  // per-edge floats: M0, directions x3, damping weights, the directions in target form
 
 // per (depth frame, pixel chunk): the per-pixel adjoint quantities, then the
 // gradient of phi (with the exact derivative of the LM damping) for every edge
 // leaving the frame.  Dynamic shared memory: kPixF floats per pixel.
-__global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs base, Batch B, float alpha, float lm) {
+__global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs base, Batch B, float alpha, float lm,
+                                                                          int first) {
     BA_BIND(B, base);
     if (w.status[0]) return;
     extern __shared__ float pix[];  // [kPixF][chunk]: a, dzf, mu, gwz, gC, gd, disp, Q, Es[6]
@@ -505,6 +506,28 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
             edge_dir(w.adj_lam, k, b, t0, P, false, vl);
             edge_dir(io.dx, k, b, t0, P, false, vd);
             for (int n = 0; n < 12; n++) Eq[48 + n] = (float)((double)lm * vl[n] * vd[n]);
+        } else if (lane >= 8 && lane < 11) {
+            // J . v = Jj . (v_j - Ad(Tij) v_i) (source rows are -Ad^T of the target rows):
+            // the three directions as one 6-vector each, Ad v_i = (R v_tau + t x R v_phi, R v_phi)
+            const int dir = lane - 8;
+            double v[12];
+            if (dir == 0)
+                edge_dir(w.adj_lam, k, b, t0, P, false, v);
+            else
+                edge_dir(io.dx, k, b, t0, P, dir == 2, v);
+            const M4 T = edge_matrix(io.poses, k, b);
+            double rt[3], rp[3];
+            for (int r = 0; r < 3; r++) {
+                rt[r] = T.m[4 * r] * v[0] + T.m[4 * r + 1] * v[1] + T.m[4 * r + 2] * v[2];
+                rp[r] = T.m[4 * r] * v[3] + T.m[4 * r + 1] * v[4] + T.m[4 * r + 2] * v[5];
+            }
+            const double t[3] = {T.m[3], T.m[7], T.m[11]};
+            double tx[3];
+            cross3(t, rp, tx);
+            for (int r = 0; r < 3; r++) {
+                Eq[60 + 6 * dir + r] = (float)(v[6 + r] - (rt[r] + tx[r]));
+                Eq[60 + 6 * dir + 3 + r] = (float)(v[9 + r] - rp[r]);
+            }
         } else if (lane == 7) {
             int g = -1;
             if (b != k)
@@ -564,10 +587,11 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                     const float g = act * act * wc[ch] * J.jz[ch];
                     float jl = 0.f, jd = 0.f, jdt = 0.f;
 #pragma unroll
-                    for (int n = 0; n < 12; n++) {
-                        jl += J.J[ch][n] * Eq[12 + n];
-                        jd += J.J[ch][n] * Eq[24 + n];
-                        jdt += J.J[ch][n] * Eq[36 + n];
+                    for (int n = 0; n < 6; n++) {
+                        const float jn = J.J[ch][6 + n];
+                        jl += jn * Eq[60 + n];
+                        jd += jn * Eq[66 + n];
+                        jdt += jn * Eq[72 + n];
                     }
                     eL += g * jl;
                     eD += g * jd;
@@ -648,7 +672,15 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
             const float u = (float)(p % W), v = (float)(p / W);
             const float X[4] = {(u - cx) / fx, (v - cy) / fy, 1.f, pdisp[i]};
             PixJ J;
-            if (!pix_jac(Eqc, X, fx, fy, J)) continue;  // invalid pixel: zero weight, no gradient
+            if (!pix_jac(Eqc, X, fx, fy, J)) {  // invalid pixel: zero weight, no gradient
+                if (first) {
+                    gtp[p] = 0.f;
+                    gtp[HW + p] = 0.f;
+                    gwp[p] = 0.f;
+                    gwp[HW + p] = 0.f;
+                }
+                continue;
+            }
             const float iz = J.iz, iz2 = iz * iz;
             const float a = pa[i], dzf = pdzf[i], mu = pmu[i], gwz = pgwz[i], gC = pgC[i], Q = pQ[i];
             const float rr[2] = {__ldg(tp + p) - (fx * J.P[0] * iz + cx), __ldg(tp + HW + p) - (fy * J.P[1] * iz + cy)};
@@ -691,11 +723,15 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                 // J . v for the edge's directions lam, dxi, dxi~, beta and the damping sum lm lam dxi J^2
                 float ft[3] = {0.f, 0.f, 0.f}, fb = 0.f, fg = 0.f;
 #pragma unroll
+                for (int n = 0; n < 6; n++) {
+                    const float jn = J.J[ch][6 + n];
+                    ft[0] += jn * Eq[60 + n];
+                    ft[1] += jn * Eq[66 + n];
+                    ft[2] += jn * Eq[72 + n];
+                }
+#pragma unroll
                 for (int n = 0; n < 12; n++) {
                     const float jn = J.J[ch][n];
-                    ft[0] += jn * Eq[12 + n];
-                    ft[1] += jn * Eq[24 + n];
-                    ft[2] += jn * Eq[36 + n];
                     fb += jn * beta[n];
                     fg += Eq[48 + n] * jn * jn;
                 }
@@ -710,10 +746,12 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                 const float c4 = A * (gwz * rr[ch] + 2.f * gC * fjz + G3 + fb);
                 const float cB = -2.f * wpc;  // along gamma = lm lam dxi o J
                 const float cE = A * fjz;     // along beta
-                gtp[(size_t)ch * HW + p] += wpc * ft[0] + A * gwz * fjz;
-                gwp[(size_t)ch * HW + p] +=
-                    0.001f * ((stereo ? 0.f : ft[0] * (rr[ch] - ft[1]) - fg) +
-                              act * act * (gwz * fjz * rr[ch] + gC * fjz * fjz + fjz * (G3 + fb)));
+                // the first backward iteration writes (the buffers are not cleared beforehand)
+                const size_t pc = (size_t)ch * HW + p;
+                gtp[pc] = (first ? 0.f : gtp[pc]) + wpc * ft[0] + A * gwz * fjz;
+                gwp[pc] = (first ? 0.f : gwp[pc]) +
+                          0.001f * ((stereo ? 0.f : ft[0] * (rr[ch] - ft[1]) - fg) +
+                                    act * act * (gwz * fjz * rr[ch] + gC * fjz * fjz + fjz * (G3 + fb)));
                 // first derivatives (s part) and the depth t-direction (column 3 of G0)
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
@@ -728,9 +766,8 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                 for (int n = 0; n < 12; n++)
                     ud[n] = c1 * Eq[12 + n] + c2 * Eq[24 + n] + c3 * Eq[36 + n] + cE * beta[n] +
                             cB * Eq[48 + n] * J.J[ch][n];
-                float fu = 0.f;
-#pragma unroll
-                for (int n = 0; n < 12; n++) fu += J.J[ch][n] * ud[n];
+                // J . ud from the dot products above (ud is their linear combination)
+                const float fu = c1 * ft[0] + c2 * ft[1] + c3 * ft[2] + cE * fb + cB * fg;
                 DirPix D;
                 dir_pix(Eqc, X, J.P, ud, D);
                 gdp += mixed(J, ch, fxy, ud, D, fu, 1.f, g0h, g0x, om);
@@ -877,7 +914,8 @@ extern "C" int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const
     const long HW = (long)plan->ht * plan->wd;
     const int G = geo.G;
     const Batch per_graph{plan->d_table, nullptr, G};
-    if (plan->edges > 0) {
+    // with iterations the first backward iteration writes every target / weight gradient
+    if (plan->edges > 0 && iterations == 0) {
         VIPE_CUDA_TRY(cudaMemsetAsync(grad_targets, 0, sizeof(float) * plan->edges * 2 * HW, st));
         VIPE_CUDA_TRY(cudaMemsetAsync(grad_weights, 0, sizeof(float) * plan->edges * 2 * HW, st));
     }
@@ -919,7 +957,8 @@ extern "C" int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const
         if ((rc = launch_chol_resolve(geo, plan->d_table, base, st)) != VIPE_OK) return rc;
         if (grid(kOffFrame) > 0) {
             VIPE_PROF("ba_adj_frame_b", st);
-            ba_adj_frame_b_kernel<<<grid(kOffFrame), kAdjThreads, smem_b, st>>>(base, frames, alpha, lm);
+            ba_adj_frame_b_kernel<<<grid(kOffFrame), kAdjThreads, smem_b, st>>>(base, frames, alpha, lm,
+                                                                                 itr == iterations - 1 ? 1 : 0);
         }
         VIPE_LAUNCH_CHECK();
         if (grid(kOffEdgeRed) > 0) {
