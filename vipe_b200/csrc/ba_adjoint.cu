@@ -442,8 +442,31 @@ __device__ __forceinline__ float mixed(const PixJ& J, int ch, float fxy, const f
     return cd * (g[0] * D.dPt[0] + g[1] * D.dPt[1] + g[2] * D.dPt[2]);
 }
 
+// n consecutive per-edge constants (16-byte aligned shared memory) into registers
+// with 16-byte loads
+template <int n>
+__device__ __forceinline__ void lds_row(const float* p, float* out) {
+#pragma unroll
+    for (int k = 0; k < n; k += 4) {
+        const float4 v = *reinterpret_cast<const float4*>(p + k);
+        out[k] = v.x;
+        if (k + 1 < n) out[k + 1] = v.y;
+        if (k + 2 < n) out[k + 2] = v.z;
+        if (k + 3 < n) out[k + 3] = v.w;
+    }
+}
+
+// 0 that the compiler cannot see through: adding it to a loop's shared-memory
+// address keeps the loads inside the loop (not hoisted into registers)
+__device__ __forceinline__ int opaque_zero() {
+    int z;
+    asm volatile("mov.u32 %0, 0;" : "=r"(z));
+    return z;
+}
+
 constexpr int kPixF = 14;   // per-pixel floats kept in shared memory by ba_adj_frame_b_kernel
-constexpr int kEdgeF = 78;  // per-edge floats: M0, directions x3, damping weights, the directions in target form
+constexpr int kEdgeF = 80;  // per-edge floats: M0, directions x3, damping weights, the directions in target form
+                            // (78 used; rows stay 16-byte aligned for vector reads)
 
 // per (depth frame, pixel chunk): the per-pixel adjoint quantities, then the
 // gradient of phi (with the exact derivative of the LM damping) for every edge
@@ -453,7 +476,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
     BA_BIND(B, base);
     if (w.status[0]) return;
     extern __shared__ float pix[];  // [kPixF][chunk]: a, dzf, mu, gwz, gC, gd, disp, Q, Es[6]
-    __shared__ float Esh[kAdjMaxDeg][kEdgeF];
+    __shared__ __align__(16) float Esh[kAdjMaxDeg][kEdgeF];
     __shared__ int grp[kAdjMaxDeg];  // -1: unique target; else index of the first edge with the same target
     __shared__ float red[kAdjThreads / 32][16];
     __shared__ int any_dup;
@@ -668,6 +691,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
 #pragma unroll
         for (int m = 0; m < 15; m++) mom[m] = 0.f;
         for (int i = tid; i < np_; i += kAdjThreads) {
+            const float* Eqv = Esh[q] + opaque_zero();  // per-pixel re-reads, see opaque_zero
             const int p = p0 + i;
             const float u = (float)(p % W), v = (float)(p / W);
             const float X[4] = {(u - cx) / fx, (v - cy) / fy, 1.f, pdisp[i]};
@@ -707,11 +731,13 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                             }
                     }
                 }
+                float dmp[12];  // damping weights lm lam dxi of the edge's two poses
+                lds_row<12>(Eqv + 48, dmp);
 #pragma unroll
                 for (int n = 0; n < 6; n++) {
                     const float es = pEs[n * CH + i];
-                    beta[n] = 2.f * Q * Eq[48 + n] * es;
-                    beta[6 + n] = 2.f * Q * Eq[54 + n] * (stereo ? es : tv[n]);
+                    beta[n] = 2.f * Q * dmp[n] * es;
+                    beta[6 + n] = 2.f * Q * dmp[6 + n] * (stereo ? es : tv[n]);
                 }
             }
             float g0h[3] = {0.f, 0.f, 0.f}, g0x[3] = {0.f, 0.f, 0.f}, om[3] = {0.f, 0.f, 0.f}, g4[3] = {0.f, 0.f, 0.f};
@@ -722,18 +748,26 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                 const float fxy = ch == 0 ? fx : fy;
                 // J . v for the edge's directions lam, dxi, dxi~, beta and the damping sum lm lam dxi J^2
                 float ft[3] = {0.f, 0.f, 0.f}, fb = 0.f, fg = 0.f;
+                {
+                    float wv[18];
+                    lds_row<18>(Eqv + 60, wv);
 #pragma unroll
-                for (int n = 0; n < 6; n++) {
-                    const float jn = J.J[ch][6 + n];
-                    ft[0] += jn * Eq[60 + n];
-                    ft[1] += jn * Eq[66 + n];
-                    ft[2] += jn * Eq[72 + n];
+                    for (int n = 0; n < 6; n++) {
+                        const float jn = J.J[ch][6 + n];
+                        ft[0] += jn * wv[n];
+                        ft[1] += jn * wv[6 + n];
+                        ft[2] += jn * wv[12 + n];
+                    }
                 }
+                {
+                    float dmp[12];
+                    lds_row<12>(Eqv + 48, dmp);
 #pragma unroll
-                for (int n = 0; n < 12; n++) {
-                    const float jn = J.J[ch][n];
-                    fb += jn * beta[n];
-                    fg += Eq[48 + n] * jn * jn;
+                    for (int n = 0; n < 12; n++) {
+                        const float jn = J.J[ch][n];
+                        fb += jn * beta[n];
+                        fg += dmp[n] * jn * jn;
+                    }
                 }
                 const float fjz = J.jz[ch];
                 const float wpc = stereo ? 0.f : wc[ch];
@@ -762,10 +796,21 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                 g0h[2] += c4 * (fxy * iz2 * Eq[4 * ch + 3] - 2.f * iz * fjz);
                 // every tangent direction enters linearly: one combined direction
                 float ud[12];
+                {
+                    float dv[12];
+                    lds_row<12>(Eqv + 48, dv);
 #pragma unroll
-                for (int n = 0; n < 12; n++)
-                    ud[n] = c1 * Eq[12 + n] + c2 * Eq[24 + n] + c3 * Eq[36 + n] + cE * beta[n] +
-                            cB * Eq[48 + n] * J.J[ch][n];
+                    for (int n = 0; n < 12; n++) ud[n] = cE * beta[n] + cB * dv[n] * J.J[ch][n];
+                    lds_row<12>(Eqv + 12, dv);
+#pragma unroll
+                    for (int n = 0; n < 12; n++) ud[n] += c1 * dv[n];
+                    lds_row<12>(Eqv + 24, dv);
+#pragma unroll
+                    for (int n = 0; n < 12; n++) ud[n] += c2 * dv[n];
+                    lds_row<12>(Eqv + 36, dv);
+#pragma unroll
+                    for (int n = 0; n < 12; n++) ud[n] += c3 * dv[n];
+                }
                 // J . ud from the dot products above (ud is their linear combination)
                 const float fu = c1 * ft[0] + c2 * ft[1] + c3 * ft[2] + cE * fb + cB * fg;
                 DirPix D;
