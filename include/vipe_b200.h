@@ -171,15 +171,16 @@ int vipe_slam_ba_extended_noalloc(float* poses_io, float* disps_io, float* intri
  * tape_poses, tape_disps, tape_factor, tape_dx (optional, all or none): the
  * record the backward pass reads — per iteration the state entering it,
  * (iterations, sum frames, 7) and (iterations, sum frames, ht, wd), the
- * factorised reduced system, (iterations, totals_out[4]) doubles, and the pose
- * step, (iterations, sum (t1-t0), 6). */
+ * factorised reduced system with the depth elimination's per-pixel (Q, w),
+ * (iterations, totals_out[4]) doubles, and the pose step,
+ * (iterations, sum (t1-t0), 6). */
 typedef struct vipe_ba_batch_plan vipe_ba_batch_plan;
 int vipe_slam_ba_batch_plan_create(int num_graphs, const int* num_frames, const int* num_edges, const int* num_kx,
                                    const int* t0, const int* t1, int ht, int wd, int edge_chunks, int frame_chunks,
                                    int group_id, int with_adjoint, vipe_ba_batch_plan** plan_out);
 size_t vipe_slam_ba_batch_workspace_size(const vipe_ba_batch_plan* plan);
 /* totals_out[5] = {sum frames, sum edges, sum kx, sum (t1-t0), doubles of one
- * iteration of the factor tape} */
+ * iteration of the tape_factor record} */
 int vipe_slam_ba_batch_totals(const vipe_ba_batch_plan* plan, int64_t* totals_out);
 int vipe_slam_ba_batch_bind(vipe_ba_batch_plan* plan, void* workspace, size_t workspace_bytes, void* stream);
 int vipe_slam_ba_batch_solve(const vipe_ba_batch_plan* plan, float* poses_io, float* disps_io, float* intrinsics_io,
@@ -199,7 +200,7 @@ void vipe_slam_ba_batch_plan_destroy(vipe_ba_batch_plan* plan);
  * differentiated exactly, with its linear solve differentiated implicitly (the
  * same damped reduced system re-solved with the incoming gradients), the LM
  * damping ep + lm*diag(S) included; Jacobians are recomputed from the tape
- * and the factorised reduced system is read back from it.
+ * and the factorised reduced system and per-pixel (Q, w) are read back from it.
  * Not covered: motion_only and optimize_intrinsics solves.
  *   grad_poses (sum frames, 7): in, d loss / d poses_out as left-tangent
  *     gradients in columns 0..5 (lietorch's layout for group gradients,

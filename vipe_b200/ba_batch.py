@@ -110,7 +110,8 @@ class BatchPlan:
 
     def make_tape(self, iterations: int):
         """Buffers of the record the backward pass reads: per iteration the state
-        entering it (poses, disps), the factorised reduced system and the pose step."""
+        entering it (poses, disps), the factorised reduced system with the per-pixel (Q, w)
+        of the depth elimination, and the pose step."""
         dev, it = self.device, int(iterations)
         return (torch.empty(it, self.total_frames, self.dof + 1, dtype=torch.float32, device=dev),
                 torch.empty(it, self.total_frames, self.ht, self.wd, dtype=torch.float32, device=dev),

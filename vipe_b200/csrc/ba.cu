@@ -923,6 +923,7 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
                 qwf[0] = Q;
                 qwf[1] = wv;
                 qwf[2] = Ef;
+                if (io.ftape) tape_qw(io.ftape, d)[(size_t)s * HW + p] = make_float2(Q, wv);  // taped solve
                 const float sq = sqrtf(Q);
                 const float scale = act * sq;
                 for (int q = 0; q < Dr; q++) {
@@ -1853,7 +1854,12 @@ int run_solve(const Geometry& geo, const GraphDesc* d_table, const int* d_off, c
             VIPE_CUDA_TRY(cudaMemcpyAsync(tape->disps + (size_t)itr * tape->frames * tape->hw, base.disps,
                                           sizeof(float) * tape->frames * tape->hw, cudaMemcpyDeviceToDevice, st));
         }
-        if ((rc = launch_linearize_solve(geo, d_table, d_off, base, a, itr, st)) != VIPE_OK) return rc;
+        {
+            // a taped solve's frame kernel also records the per-pixel (Q, w) in the iteration's slot
+            BAPtrs lb = base;
+            lb.ftape = tape ? tape->factor + (size_t)itr * tape->factor_stride : nullptr;
+            if ((rc = launch_linearize_solve(geo, d_table, d_off, lb, a, itr, st)) != VIPE_OK) return rc;
+        }
         if (tape) {
             BAPtrs tb = base;
             tb.ftape = tape->factor + (size_t)itr * tape->factor_stride;
@@ -2004,7 +2010,7 @@ extern "C" int vipe_slam_ba_batch_plan_create(int num_graphs, const int* num_fra
         gd.kx_off = plan->kx;
         gd.pose_off = plan->poses;
         gd.ftape_off = plan->ftape_stride;
-        plan->ftape_stride += factor_slot_doubles(gd.d);
+        plan->ftape_stride += tape_slot_doubles(gd.d);
         gd.g = g;
         plan->frames += num_frames[g];
         plan->edges += num_edges[g];

@@ -199,11 +199,10 @@ __global__ void ba_adj_prep_kernel(BAPtrs base, Batch B) {
     }
 }
 
-// per (depth frame, pixel chunk): first the per-pixel C = 1/Q and w of the
-// forward step (recomputed from the tape state exactly as the forward frame
-// kernel forms them, and stored for ba_adj_frame_b_kernel), then for each edge
-// leaving the frame the 12 sums  sum_p a_p act wd_c Jz_c [Ji_c, Jj_c],
-// a_p = Q_p g_d(p).
+// per (depth frame, pixel chunk): first the per-pixel Q = 1/C and w of the
+// forward step (read from the tape, where the forward frame kernel recorded
+// them, and stored for ba_adj_frame_b_kernel), then for each edge leaving the
+// frame the 12 sums  sum_p a_p act wd_c Jz_c [Ji_c, Jj_c],  a_p = Q_p g_d(p).
 __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_a_kernel(BAPtrs base, Batch B, float alpha) {
     BA_BIND(B, base);
     if (w.status[0]) return;
@@ -221,49 +220,14 @@ __global__ void __launch_bounds__(kAdjThreads) ba_adj_frame_a_kernel(BAPtrs base
         return;
     }
     const int eb = w.fe_ptr[s], ee = w.fe_ptr[s + 1];
-    // relative pose of each edge, once per CTA
-    __shared__ float etf[kEdgeCache][7];
-    for (int q = tid; q < min(ee - eb, kEdgeCache); q += kAdjThreads) {
-        const int e = w.fe_list[eb + q];
-        edge_pose(io.poses, k, (int)io.jj[e], etf[q], etf[q] + 3);
-    }
-    __syncthreads();
+    // (Q, w) of the forward step, as its frame kernel recorded them in the tape
+    const float2* qt = tape_qw(io.ftape, d);
     for (int p = p0 + tid; p < p1; p += kAdjThreads) {
-        const float u = (float)(p % W), v = (float)(p / W);
-        const float disp = io.disps[(size_t)k * HW + p];
-        float csum = 0.f, bsum = 0.f;
-        for (int q = eb; q < ee; q++) {
-            const int e = w.fe_list[q];
-            const int b = (int)io.jj[e];
-            float tij[3], qij[4];
-            if (q - eb < kEdgeCache) {
-                const float* o = etf[q - eb];
-                tij[0] = o[0]; tij[1] = o[1]; tij[2] = o[2];
-                qij[0] = o[3]; qij[1] = o[4]; qij[2] = o[5]; qij[3] = o[6];
-            } else {
-                edge_pose(io.poses, k, b, tij, qij);
-            }
-            const float* tp = io.targets + (size_t)e * 2 * HW;
-            const float* wp = io.weights + (size_t)e * 2 * HW;
-            PixelLin L;
-            linearize<false, true>(tij, qij, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p), __ldg(wp + HW + p),
-                                   __ldg(tp + p), __ldg(tp + HW + p), act, 1.f, L);
-#pragma unroll
-            for (int ch = 0; ch < 2; ch++) {
-                const float g = L.wd[ch] * L.Jz[ch];
-                csum += g * L.Jz[ch];
-                bsum += L.wd[ch] * L.r[ch] * L.Jz[ch];
-            }
-        }
-        const float dsens = io.disps_sens[(size_t)k * HW + p];
-        const float msk = (dsens > 0.f ? 1.f : 0.f) * act;
-        const float C = act * (csum + io.eta[(size_t)s * HW + p] + msk * alpha) + (1.f - act);
-        const float Q = 1.f / C;
-        const float wv = act * (bsum - msk * alpha * (disp - dsens));
+        const float2 qw2 = qt[(size_t)s * HW + p];
         float* qw = w.qwf + ((size_t)s * HW + p) * 3;
-        qw[0] = Q;
-        qw[1] = wv;
-        pa[p - p0] = Q * io.g_disps[(size_t)k * HW + p];
+        qw[0] = qw2.x;
+        qw[1] = qw2.y;
+        pa[p - p0] = qw2.x * io.g_disps[(size_t)k * HW + p];
     }
     __syncthreads();
     for (int q = eb; q < ee; q++) {

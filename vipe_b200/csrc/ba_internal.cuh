@@ -223,13 +223,19 @@ struct BAPtrs {
     float* g_weights;  // (edges, 2, H, W) out (accumulated)
     float* g_eta;      // (depth rows, H, W) out (accumulated)
     float* g_dsens;    // (frames, H, W) out (accumulated)
-    double* ftape;     // one iteration of the factor tape (graph slots at ftape_off)
+    double* ftape;     // one iteration of the tape record (graph slots at ftape_off): factor, (Q, w)
 };
 
 // factor tape slot of one graph: the Cholesky factor (dim x dim, lower
-// triangle used), the inverse diagonal blocks, and the failure flag
+// triangle used), the inverse diagonal blocks, and the failure flag ...
 __host__ __device__ inline long factor_slot_doubles(const Dims& d) {
     return (long)d.dim * d.dim + (long)((d.dim + 31) / 32) * 32 * 32 + 2;
+}
+// ... followed by the depth elimination's per-pixel (Q, w) of every depth row,
+// (K, HW) float pairs, as the forward frame kernel formed them
+__host__ __device__ inline long tape_slot_doubles(const Dims& d) { return factor_slot_doubles(d) + (long)d.K * d.HW; }
+__device__ __forceinline__ float2* tape_qw(double* slot, const Dims& d) {
+    return reinterpret_cast<float2*>(slot + factor_slot_doubles(d));
 }
 
 struct GraphDesc {
