@@ -1791,7 +1791,8 @@ int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const 
     }
     {
         VIPE_PROF("ba_cholesky", st);
-        ba_cholesky_kernel<<<G, kCholThreads, geo.chol_smem, st>>>(base, per_graph, a.lm, a.ep, a.ilm, a.iep,
+        const Batch longest_first{d_table, nullptr, G, d_off ? d_off + (size_t)kNumOff * (G + 1) : nullptr};
+        ba_cholesky_kernel<<<G, kCholThreads, geo.chol_smem, st>>>(base, longest_first, a.lm, a.ep, a.ilm, a.iep,
                                                                    intr ? 1 : 0);
     }
     VIPE_LAUNCH_CHECK();
@@ -1890,7 +1891,7 @@ template <typename C>
 void carve_batch(C& c, std::vector<GraphDesc>& gds, GraphDesc** table, int** off) {
     const int G = (int)gds.size();
     *table = c.template take<GraphDesc>(G);
-    *off = c.template take<int>((size_t)kNumOff * (G + 1));
+    *off = c.template take<int>((size_t)kNumOff * (G + 1) + G);  // block offsets, then the Cholesky order
     for (int g = 0; g < G; g++) carve(c, gds[g].d, &gds[g].w);
 }
 
@@ -2024,9 +2025,17 @@ extern "C" int vipe_slam_ba_batch_plan_create(int num_graphs, const int* num_fra
             delete plan;
             return VIPE_ERR_CAPACITY;
         }
-    plan->off_host.resize((size_t)kNumOff * (num_graphs + 1));
+    plan->off_host.resize((size_t)kNumOff * (num_graphs + 1) + num_graphs);
     for (int k = 0; k < kNumOff; k++)
         std::copy(plan->geo.off[k].begin(), plan->geo.off[k].end(), plan->off_host.begin() + (size_t)k * (num_graphs + 1));
+    {
+        // one Cholesky CTA per graph, about one per SM: start the largest systems
+        // first so that the last wave holds the small ones (longest-first order)
+        int* order = plan->off_host.data() + (size_t)kNumOff * (num_graphs + 1);
+        for (int g = 0; g < num_graphs; g++) order[g] = g;
+        std::stable_sort(order, order + num_graphs,
+                         [&](int a, int b) { return plan->gds[a].d.dim > plan->gds[b].d.dim; });
+    }
     Sizer sz;
     GraphDesc* t;
     int* o;

@@ -250,6 +250,7 @@ struct Batch {
     const GraphDesc* gds;  // device table
     const int* boff;       // per-kernel block offsets, or nullptr (see locate)
     int G;
+    const int* order = nullptr;  // one block per graph: block b runs graph order[b] (else graph b)
 };
 
 // Graph of this block.  With boff: flat grid over all graphs.  Without: a
@@ -261,7 +262,7 @@ __device__ __forceinline__ int locate(const Batch& B, int& local) {
             return 0;
         }
         local = 0;
-        return blockIdx.x;
+        return B.order ? __ldg(B.order + blockIdx.x) : (int)blockIdx.x;
     }
     const int x = blockIdx.x;
     int lo = 0, hi = B.G;
