@@ -114,6 +114,9 @@ def test_altcorr_index_matches_oracle_and_reference_property():
         (torch.float16, torch.bfloat16, (2, 64, 8, 16)),
         (torch.float32, torch.float32, (2, 96, 8, 8)),
         (torch.bfloat16, torch.float32, (2, 128, 8, 24)),
+        # 16-bit output, 32-wide target blocks: level 0 leaves the epilogue as 32-byte row stores
+        (torch.bfloat16, torch.float16, (2, 128, 48, 64)),
+        (torch.float16, torch.bfloat16, (1, 128, 16, 64)),
     ],
 )
 def test_volume_build_pyramid(in_dtype, out_dtype, shape):
