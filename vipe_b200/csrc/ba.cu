@@ -43,6 +43,8 @@
 #include "se3_device.cuh"
 #include "tcgen05.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -1241,10 +1243,31 @@ __device__ __forceinline__ double damped(double dg, bool scalar, float lm, float
 // The inverse diagonal blocks are kept (Linv) for the backward substitution.
 // On a non-positive pivot x = 0 and VIPE_WARN_SOLVER is raised, as the
 // reference falls back to dx = 0 (geom_kernels.cu:1283-1285).
+// One graph per cluster of B.blocks_per_graph CTAs (rank = local_).  Every CTA
+// of the cluster factors the 32x32 diagonal block and solves the panel in its
+// own shared memory (identical arithmetic on identical data, so every branch
+// below is cluster-uniform); the O(n^3) trailing update is split across the
+// cluster's CTAs, and a cluster barrier (release / acquire: global writes become
+// visible) ends every panel.  Rank 0 alone writes the factor, the right-hand side
+// and the results.
+// A and x entries that other CTAs of the cluster update are read from L2
+// (ld.global.cg); a single-CTA launch keeps its L1-cached loads
+__device__ __forceinline__ double chol_ld(const double* p, int C) { return C > 1 ? __ldcg(p) : *p; }
+
+__device__ __forceinline__ void chol_cluster_sync(int C) {
+    if (C > 1)
+        cooperative_groups::this_cluster().sync();
+    else
+        __syncthreads();
+}
+
 __global__ void __launch_bounds__(kCholThreads, 1)
     ba_cholesky_kernel(BAPtrs base, Batch B, float lm, float ep, float ilm, float iep, int with_intr) {
     BA_BIND(B, base);
     if (w.status[0]) return;
+    const int C = B.G == 1 ? (int)gridDim.x : B.blocks_per_graph;
+    const int rank = local_;
+    const bool lead = rank == 0;
     float* dx_out = io.dx;
     extern __shared__ double pT[];  // kNB columns x LDR rows (transposed panel)
     __shared__ double Li[kNB][kNB + 1];  // inverse of the diagonal block, Li[row][col]
@@ -1261,9 +1284,10 @@ __global__ void __launch_bounds__(kCholThreads, 1)
     double* x = w.bv;
     double* Linv = w.linv;  // nblk x kNB x kNB
     if (tid == 0) fail = 0;
-    for (int i = tid; i < n; i += kCholThreads)
-        A[(size_t)i * ld + i] = damped(A[(size_t)i * ld + i], i >= np, lm, ep, ilm, iep);
-    __syncthreads();
+    if (lead)
+        for (int i = tid; i < n; i += kCholThreads)
+            A[(size_t)i * ld + i] = damped(A[(size_t)i * ld + i], i >= np, lm, ep, ilm, iep);
+    chol_cluster_sync(C);
     const int nblk = (n + kNB - 1) / kNB;
     for (int kb = 0; kb < nblk; kb++) {
         const int k0 = kb * kNB, kn = min(kNB, n - k0), nr = n - k0;
@@ -1275,7 +1299,7 @@ __global__ void __launch_bounds__(kCholThreads, 1)
                 for (int u = 0; u < 4; u++) {
                     const int q = q0 + u * kCholThreads;
                     const int r = q / kNB, c = q % kNB;
-                    v[u] = (q < tot && c < kn) ? A[(size_t)(k0 + r) * ld + k0 + c] : 0.0;
+                    v[u] = (q < tot && c < kn) ? chol_ld(A + (size_t)(k0 + r) * ld + k0 + c, C) : 0.0;
                 }
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
@@ -1283,7 +1307,7 @@ __global__ void __launch_bounds__(kCholThreads, 1)
                     if (q < tot) pT[(q % kNB) * LDR + q / kNB] = v[u];
                 }
             }
-            if (tid < kNB) bsh[tid] = tid < kn ? x[k0 + tid] : 0.0;
+            if (tid < kNB) bsh[tid] = tid < kn ? chol_ld(x + k0 + tid, C) : 0.0;
         }
         __syncthreads();
         if (warp == 0) {
@@ -1337,8 +1361,9 @@ __global__ void __launch_bounds__(kCholThreads, 1)
         }
         __syncthreads();
         if (fail) break;
-        for (int q = tid; q < kNB * kNB; q += kCholThreads)
-            Linv[(size_t)kb * kNB * kNB + q] = Li[q / kNB][q % kNB];
+        if (lead)
+            for (int q = tid; q < kNB * kNB; q += kCholThreads)
+                Linv[(size_t)kb * kNB * kNB + q] = Li[q / kNB][q % kNB];
         // panel below the diagonal block: X = A L_kk^-T  (X[r][c] = sum_{t<=c} A[r][t] Li[c][t])
         // (Li is read through a volatile pointer so the compiler does not hoist
         // all 528 coefficients out of the row loop into registers)
@@ -1374,16 +1399,18 @@ __global__ void __launch_bounds__(kCholThreads, 1)
             ysh[tid] = tid < kn ? y0 + y1 : 0.0;
         }
         __syncthreads();
-        if (tid < kn) x[k0 + tid] = ysh[tid];
-        for (int q = tid; q < nr * kNB; q += kCholThreads) {
-            const int r = q / kNB, c = q % kNB;
-            if (c < kn && (r >= kn || c <= r)) A[(size_t)(k0 + r) * ld + k0 + c] = pT[c * LDR + r];
-        }
-        for (int r = kn + tid; r < nr; r += kCholThreads) {
-            double sacc = 0.0;
+        if (lead) {
+            if (tid < kn) x[k0 + tid] = ysh[tid];
+            for (int q = tid; q < nr * kNB; q += kCholThreads) {
+                const int r = q / kNB, c = q % kNB;
+                if (c < kn && (r >= kn || c <= r)) A[(size_t)(k0 + r) * ld + k0 + c] = pT[c * LDR + r];
+            }
+            for (int r = kn + tid; r < nr; r += kCholThreads) {
+                double sacc = 0.0;
 #pragma unroll 8
-            for (int t = 0; t < kNB; t++) sacc += pT[t * LDR + r] * ysh[t];
-            x[k0 + r] -= sacc;
+                for (int t = 0; t < kNB; t++) sacc += pT[t * LDR + r] * ysh[t];
+                x[k0 + r] -= sacc;
+            }
         }
         // trailing update of the lower triangle, 4x4 register tiles from the staged panel
         // (panel rows past nr are zero-filled below, so tiles need no row predicates)
@@ -1396,7 +1423,7 @@ __global__ void __launch_bounds__(kCholThreads, 1)
             }
             __syncthreads();
             const int ntile = n4 * (n4 + 1) / 2;
-            for (int t = tid; t < ntile; t += kCholThreads) {
+            for (int t = tid + rank * kCholThreads; t < ntile; t += kCholThreads * C) {
                 int bi = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
                 while (bi * (bi + 1) / 2 > t) bi--;
                 while ((bi + 1) * (bi + 2) / 2 <= t) bi++;
@@ -1424,12 +1451,16 @@ __global__ void __launch_bounds__(kCholThreads, 1)
 #pragma unroll
                     for (int c = 0; c < 4; c++) {
                         const int gi = k0 + ri + r, gj = k0 + rj + c;
-                        if (gi < n && gj <= gi) A[(size_t)gi * ld + gj] -= c4[r][c];
+                        if (gi < n && gj <= gi) {
+                            double* a = A + (size_t)gi * ld + gj;
+                            *a = chol_ld(a, C) - c4[r][c];
+                        }
                     }
             }
         }
-        __syncthreads();
+        chol_cluster_sync(C);
     }
+    if (!lead) return;  // the rest (substitution, results) is rank 0's
     if (!fail) {
         // backward substitution L^T x = y: x_k = L_kk^-T y_k, then y_i -= L_ki^T x_k for i < k0
         for (int kb = nblk - 1; kb >= 0; kb--) {
@@ -1791,9 +1822,27 @@ int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const 
     }
     {
         VIPE_PROF("ba_cholesky", st);
-        const Batch longest_first{d_table, nullptr, G, d_off ? d_off + (size_t)kNumOff * (G + 1) : nullptr};
-        ba_cholesky_kernel<<<G, kCholThreads, geo.chol_smem, st>>>(base, longest_first, a.lm, a.ep, a.ilm, a.iep,
-                                                                   intr ? 1 : 0);
+        const int C = geo.chol_cluster;
+        const Batch longest_first{d_table, nullptr, G, d_off ? d_off + (size_t)kNumOff * (G + 1) : nullptr, C};
+        if (C > 1) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)(G * C));
+            cfg.blockDim = dim3(kCholThreads);
+            cfg.dynamicSmemBytes = geo.chol_smem;
+            cfg.stream = st;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = (unsigned)C;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            VIPE_CUDA_TRY(cudaLaunchKernelEx(&cfg, ba_cholesky_kernel, base, longest_first, a.lm, a.ep, a.ilm,
+                                             a.iep, intr ? 1 : 0));
+        } else {
+            ba_cholesky_kernel<<<G, kCholThreads, geo.chol_smem, st>>>(base, longest_first, a.lm, a.ep, a.ilm,
+                                                                       a.iep, intr ? 1 : 0);
+        }
     }
     VIPE_LAUNCH_CHECK();
     return VIPE_OK;

@@ -250,19 +250,22 @@ struct Batch {
     const GraphDesc* gds;  // device table
     const int* boff;       // per-kernel block offsets, or nullptr (see locate)
     int G;
-    const int* order = nullptr;  // one block per graph: block b runs graph order[b] (else graph b)
+    const int* order = nullptr;  // per-graph grids: block slot b runs graph order[b] (else graph b)
+    int blocks_per_graph = 1;    // per-graph grids: consecutive blocks of one graph (a cluster)
 };
 
 // Graph of this block.  With boff: flat grid over all graphs.  Without: a
-// single graph (G == 1, local = blockIdx.x) or one block per graph (g = blockIdx.x).
+// single graph (G == 1, local = blockIdx.x) or blocks_per_graph consecutive
+// blocks per graph (slot = blockIdx.x / blocks_per_graph, in `order` when given).
 __device__ __forceinline__ int locate(const Batch& B, int& local) {
     if (B.boff == nullptr) {
         if (B.G == 1) {
             local = blockIdx.x;
             return 0;
         }
-        local = 0;
-        return B.order ? __ldg(B.order + blockIdx.x) : (int)blockIdx.x;
+        const int slot = (int)blockIdx.x / B.blocks_per_graph;
+        local = (int)blockIdx.x % B.blocks_per_graph;
+        return B.order ? __ldg(B.order + slot) : slot;
     }
     const int x = blockIdx.x;
     int lo = 0, hi = B.G;
@@ -371,6 +374,7 @@ struct Geometry {
     int dof = 6;
     std::vector<int> off[kNumOff];  // G + 1 entries each
     size_t chol_smem = 0;
+    int chol_cluster = 1;  // CTAs (one cluster) per graph in the Cholesky launch
     bool any_edges = false;
 };
 
@@ -384,6 +388,9 @@ inline void fill_geometry(const std::vector<Dims>& dims, Geometry& geo) {
                                   (int)ceil_div(d.P, 128)};
         for (int k = 0; k < kNumOff; k++) geo.off[k][g + 1] = geo.off[k][g] + cnt[k];
         geo.chol_smem = std::max(geo.chol_smem, (size_t)chol_ldr(d.dim) * kNB * sizeof(double));
+        // a single large reduced system splits its trailing updates over a cluster of
+        // CTAs (batches already fill the GPU with one CTA per graph)
+        geo.chol_cluster = dims.size() == 1 ? (d.dim >= 256 ? 8 : (d.dim >= 128 ? 4 : 1)) : 1;
         geo.any_edges |= d.E > 0;
         geo.dof = d.dof;
     }
