@@ -16,13 +16,19 @@
 //     K = 16 per instruction, FP32 accumulator in tensor memory, two TMEM
 //     accumulator buffers (2 x 256 columns) so the MMA of tile t+1 overlaps the
 //     epilogue of tile t;
-//   * warps 4-7: epilogue.  tcgen05.ld puts one source pixel's row (the whole
-//     8 x TW target block) in each thread's registers, so the 2x2 / 4x4 / 8x8
-//     average pools of levels 1-3 close inside the thread; every level is
-//     converted and stored straight from registers.
+//   * warps 0-7: epilogue.  tcgen05.ld puts one source pixel's accumulator row
+//     in each thread's registers, so the 2x2 / 4x4 average pools close inside
+//     the thread; the levels are staged per warp in shared memory and written
+//     with 16-byte stores in which consecutive lanes cover contiguous bytes.
+//     16-bit output with 32-wide target blocks (the production shape) uses the
+//     row-split mapping (kR0 below): each warp owns 4 of the 8 target rows, so
+//     level-0 stores cover 64 contiguous bytes, level-1 rows whole 32-byte
+//     sectors, and level 3 is pooled from the stored level 2 afterwards
+//     (pool_level_kernel) instead of in 4-byte pieces; other shapes split the
+//     tile's columns between warp halves and pool all levels in the epilogue.
 // The output write (sum over levels of num*HW*HW/4^l elements) is the HBM
-// roofline of this kernel.
-//
+// roofline of this kernel: it is write-only traffic.
+
 // Every mbarrier wait is bounded: on expiry the CTA records an error, stops
 // issuing work, drains its in-flight copies (bounded) and frees tensor memory.
 
@@ -54,6 +60,7 @@ struct Params {
     int out_dtype;
     void* out[4];
     int* err;
+    int rowsplit;  // 1: the row-split epilogue (16-bit output, TW = 32); level 3 by pool_level_kernel
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -112,6 +119,16 @@ struct Stage {
     static constexpr int r3 = 16;                       // level 3
     static constexpr int per_warp = 32 * (r0 + r1 + r2 + r3);
 };
+
+// Row-split epilogue (16-bit output, TW = 32): warp (q, rh) owns TMEM lane
+// quarter q and target rows 4 rh .. 4 rh + 3 of the 8 x 32 tile, all 32 columns.
+// Per source row it stages level 0 as 4 rows of 64 B, level 1 as 2 rows of 32 B
+// and level 2 as one 16-byte row, so each level-0 store instruction covers 8
+// segments of 64 contiguous bytes, level-1 rows leave as whole 32-byte sectors
+// and a level-2 row's two 16-byte halves come from consecutive tiles of the same
+// warp.  Level 3 (2x2 of level 2) is pooled afterwards from the stored level 2.
+constexpr int kR0 = 4 * 64 + 16, kR1 = 2 * 32 + 16, kR2 = 16 + 16;  // staged row strides (bytes)
+static_assert(32 * (kR0 + kR1 + kR2) <= 12800, "row-split staging exceeds the per-warp staging region");
 
 template <typename T>
 __device__ __forceinline__ uint32_t pack2(float a, float b);
@@ -369,6 +386,74 @@ __global__ void __launch_bounds__(kThreads, 1)
                     if (lane == 0) mbar_arrive(&barAcc_empty[acc]);
                     continue;
                 }
+                if constexpr (sizeof(TOut) == 2) {
+                    if (p.rowsplit) {
+                        const int rh = warp >> 2;
+                        uint8_t* s0 = st;
+                        uint8_t* s1 = st + 32 * kR0;
+                        uint8_t* s2 = st + 32 * (kR0 + kR1);
+#pragma unroll 1
+                        for (int cb = 0; cb < 4; cb++) {
+                            float blk[4][8];
+#pragma unroll
+                            for (int r = 0; r < 4; r++)
+                                tmem_ld8(tmem + lane_addr + (uint32_t)(acc * 256 + (4 * rh + r) * 32 + cb * 8), blk[r]);
+                            tmem_wait_ld();
+#pragma unroll
+                            for (int r = 0; r < 4; r++) sts_n<TOut, 8>(s0 + lane * kR0 + r * 64 + cb * 16, blk[r]);
+                            float l1[2][4];
+#pragma unroll
+                            for (int r = 0; r < 2; r++)
+#pragma unroll
+                                for (int c2 = 0; c2 < 4; c2++)
+                                    l1[r][c2] = 0.25f * ((blk[2 * r][2 * c2] + blk[2 * r][2 * c2 + 1]) +
+                                                         (blk[2 * r + 1][2 * c2] + blk[2 * r + 1][2 * c2 + 1]));
+#pragma unroll
+                            for (int r = 0; r < 2; r++) sts_n<TOut, 4>(s1 + lane * kR1 + r * 32 + cb * 8, l1[r]);
+                            float l2[2];
+#pragma unroll
+                            for (int c2 = 0; c2 < 2; c2++)
+                                l2[c2] = 0.25f * ((l1[0][2 * c2] + l1[0][2 * c2 + 1]) + (l1[1][2 * c2] + l1[1][2 * c2 + 1]));
+                            sts_n<TOut, 2>(s2 + lane * kR2 + cb * 4, l2);
+                        }
+                        // the whole accumulator slice of this warp is read: release TMEM
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&barAcc_empty[acc]);
+                        __syncwarp();
+                        const int h0 = hb * kTH, w0 = wb * TW;
+                        {
+                            uint8_t* g0 = static_cast<uint8_t*>(p.out[0]) + (size_t)row0 * rs[0] +
+                                          ((size_t)(h0 + 4 * rh) * W + w0) * sz;
+#pragma unroll 4
+                            for (int it = 0; it < 16; it++) {
+                                const int j = lane + 32 * it, i = j >> 4, r = (j >> 2) & 3, k = j & 3;
+                                if (i < nrows)
+                                    *reinterpret_cast<uint4*>(g0 + (size_t)i * rs[0] + (size_t)r * ss[0] + k * 16) =
+                                        *reinterpret_cast<const uint4*>(s0 + i * kR0 + r * 64 + k * 16);
+                            }
+                        }
+                        if (p.levels > 1) {
+                            uint8_t* g1 = static_cast<uint8_t*>(p.out[1]) + (size_t)row0 * rs[1] +
+                                          ((size_t)(h0 / 2 + 2 * rh) * (W / 2) + w0 / 2) * sz;
+#pragma unroll
+                            for (int it = 0; it < 4; it++) {
+                                const int j = lane + 32 * it, i = j >> 2, r = (j >> 1) & 1, k = j & 1;
+                                if (i < nrows)
+                                    *reinterpret_cast<uint4*>(g1 + (size_t)i * rs[1] + (size_t)r * ss[1] + k * 16) =
+                                        *reinterpret_cast<const uint4*>(s1 + i * kR1 + r * 32 + k * 16);
+                            }
+                        }
+                        if (p.levels > 2 && lane < nrows) {
+                            uint8_t* g2 = static_cast<uint8_t*>(p.out[2]) + (size_t)row0 * rs[2] +
+                                          ((size_t)(h0 / 4 + rh) * (W / 4) + w0 / 4) * sz;
+                            *reinterpret_cast<uint4*>(g2 + (size_t)lane * rs[2]) =
+                                *reinterpret_cast<const uint4*>(s2 + lane * kR2);
+                        }
+                        __syncwarp();
+                        continue;
+                    }
+                }
                 for (int c = col_lo; c < col_hi; c += PW) {
                     const int pw = min(PW, col_hi - c);  // PW, or 8 when TW = 8
                     for (int cb = 0; cb < pw / 8; cb++) {
@@ -407,6 +492,27 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (warp == kMmaWarp) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+    }
+}
+
+// ---------------------------------------------------------------- level 3
+
+// out (rows, Hi/2, Wi/2) = 2x2 average of in (rows, Hi, Wi), 16-bit, FP32 sums
+// (the row-split epilogue's level 3 from its stored level 2)
+template <typename T>
+__global__ void __launch_bounds__(256) pool_level_kernel(const T* __restrict__ in, T* __restrict__ out, long rows,
+                                                         int Hi, int Wi) {
+    const int Ho = Hi / 2, Wo = Wi / 2;
+    const long n = rows * Ho * Wo;
+    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(idx % Wo);
+        const long t = idx / Wo;
+        const int y = (int)(t % Ho);
+        const long r = t / Ho;
+        const T* src = in + (r * Hi + 2 * y) * Wi + 2 * x;
+        const float v = 0.25f * ((static_cast<float>(src[0]) + static_cast<float>(src[1])) +
+                                 (static_cast<float>(src[Wi]) + static_cast<float>(src[Wi + 1])));
+        out[idx] = cvt<T>(v);
     }
 }
 
@@ -586,6 +692,9 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
     p.out_dtype = out_dtype;
     for (int l = 0; l < 4; l++) p.out[l] = l < num_levels ? level_out[l] : nullptr;
     p.err = err;
+    bool al16 = true;
+    for (int l = 0; l < num_levels; l++) al16 &= (reinterpret_cast<uintptr_t>(level_out[l]) % 16) == 0;
+    p.rowsplit = (out_dtype != VIPE_F32 && TW == 32 && al16) ? 1 : 0;
 
     int dev = 0, sms = 148;
     VIPE_CUDA_TRY(cudaGetDevice(&dev));
@@ -605,13 +714,30 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
         g_attr_set[dev] = true;
     }
     const int grid = (int)std::min<long>(p.items, (long)sms);
-    VIPE_PROF("corr_build", st);
-    if (out_dtype == VIPE_F32)
-        corr_build_kernel<float><<<grid, kThreads, smem, st>>>(mA, mB, p, op_fmt);
-    else if (out_dtype == VIPE_F16)
-        corr_build_kernel<__half><<<grid, kThreads, smem, st>>>(mA, mB, p, op_fmt);
-    else
-        corr_build_kernel<__nv_bfloat16><<<grid, kThreads, smem, st>>>(mA, mB, p, op_fmt);
+    {
+        VIPE_PROF("corr_build", st);
+        if (out_dtype == VIPE_F32)
+            corr_build_kernel<float><<<grid, kThreads, smem, st>>>(mA, mB, p, op_fmt);
+        else if (out_dtype == VIPE_F16)
+            corr_build_kernel<__half><<<grid, kThreads, smem, st>>>(mA, mB, p, op_fmt);
+        else
+            corr_build_kernel<__nv_bfloat16><<<grid, kThreads, smem, st>>>(mA, mB, p, op_fmt);
+    }
     VIPE_LAUNCH_CHECK();
+    if (p.rowsplit && num_levels > 3) {
+        const long rows = (long)num * HW;
+        const long n3 = rows * (ht / 8) * (wd / 8);
+        const unsigned pgrid = (unsigned)std::min<long>((n3 + 255) / 256, (long)sms * 16);
+        VIPE_PROF("corr_pool_level", st);
+        if (out_dtype == VIPE_F16)
+            pool_level_kernel<__half><<<pgrid, 256, 0, st>>>(static_cast<const __half*>(level_out[2]),
+                                                               static_cast<__half*>(level_out[3]), rows, ht / 4,
+                                                               wd / 4);
+        else
+            pool_level_kernel<__nv_bfloat16><<<pgrid, 256, 0, st>>>(
+                static_cast<const __nv_bfloat16*>(level_out[2]), static_cast<__nv_bfloat16*>(level_out[3]), rows,
+                ht / 4, wd / 4);
+        VIPE_LAUNCH_CHECK();
+    }
     return VIPE_OK;
 }
