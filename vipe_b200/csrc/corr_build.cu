@@ -498,21 +498,35 @@ __global__ void __launch_bounds__(kThreads, 1)
 // ---------------------------------------------------------------- level 3
 
 // out (rows, Hi/2, Wi/2) = 2x2 average of in (rows, Hi, Wi), 16-bit, FP32 sums
-// (the row-split epilogue's level 3 from its stored level 2)
+// (the row-split epilogue's level 3 from its stored level 2).  One thread per
+// output row: two 2*Wi-byte input rows in, one Wi-byte row out, 16-byte accesses
+// (Wi = 16: level 2 of a 64-wide map; the host launches it only then).
 template <typename T>
 __global__ void __launch_bounds__(256) pool_level_kernel(const T* __restrict__ in, T* __restrict__ out, long rows,
                                                          int Hi, int Wi) {
-    const int Ho = Hi / 2, Wo = Wi / 2;
-    const long n = rows * Ho * Wo;
+    const int Ho = Hi / 2;
+    const long n = rows * Ho;
     for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
-        const int x = (int)(idx % Wo);
-        const long t = idx / Wo;
-        const int y = (int)(t % Ho);
-        const long r = t / Ho;
-        const T* src = in + (r * Hi + 2 * y) * Wi + 2 * x;
-        const float v = 0.25f * ((static_cast<float>(src[0]) + static_cast<float>(src[1])) +
-                                 (static_cast<float>(src[Wi]) + static_cast<float>(src[Wi + 1])));
-        out[idx] = cvt<T>(v);
+        const int y = (int)(idx % Ho);
+        const long r = idx / Ho;
+        const uint4* s0 = reinterpret_cast<const uint4*>(in + (r * Hi + 2 * y) * Wi);
+        const uint4* s1 = reinterpret_cast<const uint4*>(in + (r * Hi + 2 * y + 1) * Wi);
+        const uint4 a0 = s0[0], a1 = s0[1], b0 = s1[0], b1 = s1[1];
+        const T* ra = reinterpret_cast<const T*>(&a0);
+        const T* rb = reinterpret_cast<const T*>(&a1);
+        const T* sa = reinterpret_cast<const T*>(&b0);
+        const T* sb = reinterpret_cast<const T*>(&b1);
+        float v[8];
+#pragma unroll
+        for (int x = 0; x < 8; x++) {
+            const T* u = x < 4 ? ra : rb;
+            const T* w = x < 4 ? sa : sb;
+            const int c = 2 * (x & 3);
+            v[x] = 0.25f * ((static_cast<float>(u[c]) + static_cast<float>(u[c + 1])) +
+                            (static_cast<float>(w[c]) + static_cast<float>(w[c + 1])));
+        }
+        *reinterpret_cast<uint4*>(out + (r * Ho + y) * (Wi / 2)) =
+            make_uint4(pack2<T>(v[0], v[1]), pack2<T>(v[2], v[3]), pack2<T>(v[4], v[5]), pack2<T>(v[6], v[7]));
     }
 }
 
@@ -520,12 +534,12 @@ __global__ void __launch_bounds__(256) pool_level_kernel(const T* __restrict__ i
 
 // F (num, C, H, W) -> rows (num, HW, Kp) of 16-bit type, scaled by 1/4;
 // permute: target-block pixel order (8 x TW blocks) for the B operand.  One
-// CTA transposes a 64-channel x 64-pixel tile through shared memory with
+// CTA transposes a 64-channel x 128-pixel tile through shared memory with
 // 16-byte global loads (along pixels) and 16-byte stores (along channels).
 template <typename TIn, typename TOp>
 __global__ void __launch_bounds__(256) pack_kernel(const TIn* __restrict__ f, TOp* __restrict__ out, int C, int Kp,
                                                    int H, int W, int TW, int permute) {
-    constexpr int kPx = 64, kCh = 64, LDT = kPx + 8;  // 16-bit tile rows padded by 16 bytes
+    constexpr int kPx = 128, kCh = 64, LDT = kPx + 8;  // 16-bit tile rows padded by 16 bytes
     __shared__ __align__(16) TOp tile[kCh][LDT];
     const int e = blockIdx.z;
     const int HW = H * W;
@@ -657,7 +671,7 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
 
     // operand type: FP16 inputs stay FP16, others go to BF16
     const int op_fmt = (in_dtype == VIPE_F16) ? 0 : 1;
-    dim3 pg(ceil_div(HW, 64), Kp / kKC, num);
+    dim3 pg(ceil_div(HW, 128), Kp / kKC, num);
     {
         VIPE_PROF("corr_pack", st);
         for (int side = 0; side < 2; side++) {
@@ -694,7 +708,8 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
     p.err = err;
     bool al16 = true;
     for (int l = 0; l < num_levels; l++) al16 &= (reinterpret_cast<uintptr_t>(level_out[l]) % 16) == 0;
-    p.rowsplit = (out_dtype != VIPE_F32 && TW == 32 && al16) ? 1 : 0;
+    // (level 3 of the row-split path is pooled by a 16-byte-row kernel for 64-wide maps)
+    p.rowsplit = (out_dtype != VIPE_F32 && TW == 32 && al16 && (num_levels < 4 || wd == 64)) ? 1 : 0;
 
     int dev = 0, sms = 148;
     VIPE_CUDA_TRY(cudaGetDevice(&dev));
@@ -725,8 +740,12 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
     }
     VIPE_LAUNCH_CHECK();
     if (p.rowsplit && num_levels > 3) {
+        if (wd != 64) {
+            set_last_error("corr_volume_build: level 3 of the row-split path expects 64-wide maps");
+            return VIPE_ERR_CAPACITY;
+        }
         const long rows = (long)num * HW;
-        const long n3 = rows * (ht / 8) * (wd / 8);
+        const long n3 = rows * (ht / 8);
         const unsigned pgrid = (unsigned)std::min<long>((n3 + 255) / 256, (long)sms * 16);
         VIPE_PROF("corr_pool_level", st);
         if (out_dtype == VIPE_F16)
