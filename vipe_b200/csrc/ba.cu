@@ -1243,6 +1243,61 @@ __device__ __forceinline__ double damped(double dg, bool scalar, float lm, float
 // The inverse diagonal blocks are kept (Linv) for the backward substitution.
 // On a non-positive pivot x = 0 and VIPE_WARN_SOLVER is raised, as the
 // reference falls back to dx = 0 (geom_kernels.cu:1283-1285).
+// Cholesky of the (identity-padded) 32x32 diagonal block held in pT (transposed:
+// D[r][c] = pT[c * LDR + r]; rows and columns >= kn are the identity), one warp,
+// lane = row.  Writes L back into pT (rows < kn, strict upper part zero), L^-1 into
+// Li (Li[t][j]) and 1 / L[j][j] into dinv; returns true (on every lane) when a pivot
+// was not positive.  Registers hold the row (rv) and the inverse column (z), L[c][j]
+// arrives by shuffle and the inverse's coefficients are shared-memory broadcasts.
+// Kept out of line: inside the panel loop the compiler does not unroll the 496-step
+// triangular nest, and the dynamically indexed rows then live in local memory.
+__device__ __noinline__ bool chol_diag_block(double* pT, int LDR, int kn, int lane, double (*Li)[kNB + 1],
+                                             double* dinv) {
+    double rv[kNB];
+#pragma unroll
+    for (int c = 0; c < kNB; c++) rv[c] = (lane < kn && c < kn) ? pT[c * LDR + lane] : (lane == c ? 1.0 : 0.0);
+    bool bad = false;
+    double my_dinv = 1.0;
+#pragma unroll
+    for (int j = 0; j < kNB; j++) {
+        const double piv = __shfl_sync(0xffffffffu, rv[j], j);
+        bad |= !(piv > 0.0);
+        const double l = piv > 0.0 ? sqrt(piv) : 1.0;
+        const double il = 1.0 / l;
+        if (lane == j) my_dinv = il;
+        rv[j] = (lane == j) ? l : (lane > j ? rv[j] * il : 0.0);
+#pragma unroll
+        for (int c = j + 1; c < kNB; c++) {
+            const double lcj = __shfl_sync(0xffffffffu, rv[j], c);
+            if (lane >= c) rv[c] -= rv[j] * lcj;
+        }
+    }
+    dinv[lane] = my_dinv;
+    // L (padded) row-major into Li for the inverse, the panel's copy into pT
+#pragma unroll
+    for (int c = 0; c < kNB; c++) {
+        const double v = (c <= lane) ? rv[c] : 0.0;
+        if (lane < kn) pT[c * LDR + lane] = v;
+        Li[lane][c] = v;
+    }
+    __syncwarp();
+    // inverse: lane j solves L z = e_j (column j of L^-1)
+    double z[kNB];
+#pragma unroll
+    for (int t = 0; t < kNB; t++) {
+        double s0 = (t == lane) ? 1.0 : 0.0, s1 = 0.0;
+#pragma unroll
+        for (int q = 0; q < t; q++) {
+            if (q & 1) s1 -= Li[t][q] * z[q]; else s0 -= Li[t][q] * z[q];
+        }
+        z[t] = (t < lane) ? 0.0 : (s0 + s1) * dinv[t];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < kNB; t++) Li[t][lane] = z[t];
+    return __any_sync(0xffffffffu, bad);
+}
+
 // One graph per cluster of B.blocks_per_graph CTAs (rank = local_).  Every CTA
 // of the cluster factors the 32x32 diagonal block and solves the panel in its
 // own shared memory (identical arithmetic on identical data, so every branch
@@ -1311,53 +1366,8 @@ __global__ void __launch_bounds__(kCholThreads, 1)
         }
         __syncthreads();
         if (warp == 0) {
-            // register Cholesky of the (identity-padded) diagonal block; lane = row
-            double rv[kNB];
-#pragma unroll
-            for (int c = 0; c < kNB; c++)
-                rv[c] = (lane < kn && c < kn) ? pT[c * LDR + lane] : (lane == c ? 1.0 : 0.0);
-            bool bad = false;
-            double my_dinv = 1.0;
-#pragma unroll
-            for (int j = 0; j < kNB; j++) {
-                const double piv = __shfl_sync(0xffffffffu, rv[j], j);
-                bad |= !(piv > 0.0);
-                const double l = piv > 0.0 ? sqrt(piv) : 1.0;
-                const double il = 1.0 / l;
-                if (lane == j) my_dinv = il;
-                rv[j] = (lane == j) ? l : (lane > j ? rv[j] * il : rv[j]);
-#pragma unroll
-                for (int c = j + 1; c < kNB; c++) {
-                    const double lcj = __shfl_sync(0xffffffffu, rv[j], c);
-                    if (lane >= c) rv[c] -= rv[j] * lcj;
-                }
-            }
+            const bool bad = chol_diag_block(pT, LDR, kn, lane, Li, dinv);
             if (bad && lane == 0) fail = 1;
-            dinv[lane] = my_dinv;
-            // the factor goes to Li's shared buffer first (row-major), then is inverted in place by columns
-#pragma unroll
-            for (int c = 0; c < kNB; c++) {
-                const double v = (c <= lane) ? rv[c] : 0.0;
-                if (lane < kn) pT[c * LDR + lane] = v;
-                Li[lane][c] = v;  // L (padded) row-major, temporarily
-            }
-            __syncwarp();
-            // inverse: lane j solves L z = e_j; coefficients L[t][q] are warp broadcasts
-            double z[kNB];
-#pragma unroll
-            for (int t = 0; t < kNB; t++) {
-                double s0 = (t == lane) ? 1.0 : 0.0, s1 = 0.0;
-#pragma unroll
-                for (int q = 0; q + 1 < t; q += 2) {
-                    s0 -= Li[t][q] * z[q];
-                    s1 -= Li[t][q + 1] * z[q + 1];
-                }
-                if (t & 1) s0 -= Li[t][t - 1] * z[t - 1];
-                z[t] = (t < lane) ? 0.0 : (s0 + s1) * dinv[t];
-            }
-            __syncwarp();
-#pragma unroll
-            for (int t = 0; t < kNB; t++) Li[t][lane] = z[t];
         }
         __syncthreads();
         if (fail) break;

@@ -352,7 +352,7 @@ struct FrameArgs {
     float iscale;
 };
 
-constexpr int kCholThreads = 512;
+constexpr int kCholThreads = 256;
 constexpr int kNB = 32;
 constexpr int kPanelRows = 768;  // systems up to 768 unknowns stage their panel in shared memory
 
