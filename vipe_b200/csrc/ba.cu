@@ -831,6 +831,9 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
             if (p < p1) {
                 const float u = (float)(p % W), v = (float)(p / W);
                 const float disp = A.disps[(size_t)k * HW + p];
+                // loaded before the edge loop so that their latency hides under it
+                const float dsens = __ldg(A.disps_sens + (size_t)k * HW + p);
+                const float eta_p = __ldg(A.eta + (size_t)s * HW + p);
                 for (int q = 0; q < Dm; q++) *reinterpret_cast<float*>(hb + sw128_off(q, pi)) = 0.f;
                 float es[D];
 #pragma unroll
@@ -913,9 +916,8 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
 #pragma unroll
                     for (int n = 0; n < D; n++) *reinterpret_cast<float*>(hb + sw128_off(D * self + n, pi)) = es[n];
                 }
-                const float dsens = A.disps_sens[(size_t)k * HW + p];
                 const float msk = (dsens > 0.f ? 1.f : 0.f) * act;
-                const float C = act * (csum + A.eta[(size_t)s * HW + p] + msk * A.alpha) + (1.f - act);
+                const float C = act * (csum + eta_p + msk * A.alpha) + (1.f - act);
                 const float Q = 1.f / C;
                 const float dd = disp - dsens;
                 const float wv = act * (bsum - msk * A.alpha * dd);
@@ -1622,6 +1624,9 @@ __global__ void __launch_bounds__(256, 3) ba_backsub_kernel(BAPtrs base, Batch B
     for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
         const float u = (float)(p % W), v = (float)(p / W);
         const float disp = disps_io[(size_t)k * HW + p];
+        // the pixel's Q, w, Ef are read before the edge loop so that their latency hides under it
+        const float* qwf = w.qwf + ((size_t)s * HW + p) * 3;
+        const float Q = qwf[0], wv = qwf[1], qef = kIntr ? qwf[2] : 0.f;
         float dot = 0.f;
         for (int q = eb; q < ee; q++) {
             const int e = w.fe_list[q];
@@ -1663,10 +1668,8 @@ __global__ void __launch_bounds__(256, 3) ba_backsub_kernel(BAPtrs base, Batch B
             }
         }
         dot *= act;
-        const float* qwf = w.qwf + ((size_t)s * HW + p) * 3;
-        const float Q = qwf[0], wv = qwf[1];
         float dz = Q * (wv - dot);
-        if (kIntr) dz = dz - Q * qwf[2] * df;
+        if (kIntr) dz = dz - Q * qef * df;
         dz_out[(size_t)s * HW + p] = dz;
         disps_io[(size_t)k * HW + p] = disp + dz;
     }
