@@ -311,6 +311,14 @@ int vipe_corr_index_forward(int dtype, const void* volume, const float* coords, 
 int vipe_corr_index_backward(int dtype, const float* coords, const void* corr_grad, int B, int h1, int w1, int h2,
                              int w2, int radius, void* volume_grad_out, void* stream);
 
+/* Coordinate gradient of corr_index_forward (no reference counterpart: the
+ * reference's CorrSampler.backward returns no coordinate gradient,
+ * vipe/slam/networks/droid_net.py:40-45).  The exact derivative of the bilinear
+ * weights inside each cell, contracted with corr_grad (B, 2r+1, 2r+1, h1, w1)
+ * dtype -> coords_grad_out (B, 2, h1, w1) f32 (written completely). */
+int vipe_corr_index_coords_backward(int dtype, const void* volume, const float* coords, const void* corr_grad, int B,
+                                    int h1, int w1, int h2, int w2, int radius, float* coords_grad_out, void* stream);
+
 /* altcorr_forward (altcorr_kernel.cu:26-138,368-392).
  * fmap1 (B,H1,W1,C), fmap2 (B,H2,W2,C) dtype, coords (B,S,H1,W1,2) f32
  * -> corr_out (B,S,(2r+1)^2,H1,W1) dtype. */
@@ -334,6 +342,20 @@ int vipe_altcorr_index_forward(int dtype, const void* fmap1, const void* const* 
                                const int* W2, int num_levels, const float* coords, const int64_t* ii,
                                const int64_t* jj, int B, int Nf, int M, int H, int W, int C, int radius,
                                float* corr_out, void* stream);
+
+/* Adjoint of altcorr_index_forward (no reference counterpart: the reference
+ * binds only the forward, droid.cpp:75-81).  corr_grad (B, M, L*(2r+1)^2, H, W)
+ * f32 -> fmap1_grad_out (B, Nf, H, W, C) f32, level_grads_out[l]
+ * (B, Nf, H2[l], W2[l], C) f32 (all zeroed here, then accumulated with
+ * atomics: edges sharing a frame add into the same rows) and, when not NULL,
+ * coords_grad_out (B, M, H, W, 2) f32: the exact derivative of the bilinear
+ * weights summed over levels (level l scaled by 2^-l) if exact_coords_grad,
+ * zeros otherwise.  dtype VIPE_F32, VIPE_F16 or VIPE_BF16 (the maps). */
+int vipe_altcorr_index_backward(int dtype, const void* fmap1, const void* const* fmap2_levels, const int* H2,
+                                const int* W2, int num_levels, const float* coords, const int64_t* ii,
+                                const int64_t* jj, const float* corr_grad, int B, int Nf, int M, int H, int W, int C,
+                                int radius, int exact_coords_grad, float* fmap1_grad_out,
+                                float* const* level_grads_out, float* coords_grad_out, void* stream);
 
 /* All-pairs correlation volume with its average-pooled pyramid — the build of
  * CorrBlock (vipe/slam/networks/droid_net.py:56-69,94-102): for each of the

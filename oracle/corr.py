@@ -12,7 +12,12 @@ Follows the reference:
     per pyramid level; output f32 for the indexed form).
 The reference's altcorr_backward leaves the coords gradient at zero
 (altcorr_kernel.cu:440); `altcorr_backward(..., exact_coords=True)` here returns
-the derivative of the bilinear weights instead.
+the derivative of the bilinear weights instead.  `corr_index_coords_backward`
+is that derivative for the volume lookup (the reference's CorrSampler returns
+none, droid_net.py:40-45), and `corr_pyramid_backward` the feature-map gradient
+of the pyramid that torch autograd forms in the reference (matmul and
+avg_pool2d, droid_net.py:56-69, 94-102): every level gradient spread back to
+level 0, then the two products with the other feature map.
 """
 
 from __future__ import annotations
@@ -104,6 +109,46 @@ def corr_index_backward(volume_shape, coords, grad, r):
     return out
 
 
+def corr_index_coords_backward(volume, coords, grad, r):
+    """volume (B,h1,w1,h2,w2), coords (B,2,h1,w1), grad (B,rd,rd,h1,w1) -> (B,2,h1,w1)."""
+    vol = np.asarray(volume, np.float64)
+    c = np.asarray(coords, np.float64)
+    g = np.asarray(grad, np.float64)
+    B, h1, w1, h2, w2 = vol.shape
+    x, y = c[:, 0], c[:, 1]
+    dx = (x - np.floor(x))[..., None, None]
+    dy = (y - np.floor(y))[..., None, None]
+    X, Y = _tap_index(x, y, r)
+    ok = (X >= 0) & (X < w2) & (Y >= 0) & (Y < h2)
+    bb = np.arange(B)[:, None, None, None, None]
+    pp = np.arange(h1)[None, :, None, None, None]
+    qq = np.arange(w1)[None, None, :, None, None]
+    t = vol[bb, pp, qq, np.clip(Y, 0, h2 - 1), np.clip(X, 0, w2 - 1)] * ok  # (B,h1,w1,rd+1,rd+1) [x off][y off]
+    a00, a10, a01, a11 = t[..., :-1, :-1], t[..., 1:, :-1], t[..., :-1, 1:], t[..., 1:, 1:]
+    ddx = (1 - dy) * (a10 - a00) + dy * (a11 - a01)
+    ddy = (1 - dx) * (a01 - a00) + dx * (a11 - a10)
+    gg = g.transpose(0, 3, 4, 1, 2)
+    return np.stack([(gg * ddx).sum((-1, -2)), (gg * ddy).sum((-1, -2))], 1)
+
+
+def corr_pyramid_backward(fmap1, fmap2, level_grads):
+    """fmap1, fmap2 (B,C,H,W); level_grads[l] (B,H,W,H>>l,W>>l) (None: no gradient) -> (d fmap1, d fmap2)."""
+    f1 = np.asarray(fmap1, np.float64)
+    f2 = np.asarray(fmap2, np.float64)
+    B, C, H, W = f1.shape
+    g0 = np.zeros((B, H * W, H, W))
+    for l, G in enumerate(level_grads):
+        if G is None:
+            continue
+        G = np.asarray(G, np.float64).reshape(B, H * W, H >> l, W >> l)
+        # adjoint of l average pools: each pooled value spread evenly over its 2^l x 2^l block
+        g0 += np.repeat(np.repeat(G, 2**l, axis=2), 2**l, axis=3) / 4.0**l
+    g0 = g0.reshape(B, H * W, H * W)
+    d1 = np.einsum("bpq,bcq->bcp", g0, f2.reshape(B, C, H * W)) / 16.0
+    d2 = np.einsum("bpq,bcp->bcq", g0, f1.reshape(B, C, H * W)) / 16.0
+    return d1.reshape(B, C, H, W), d2.reshape(B, C, H, W)
+
+
 def _window_dots(f1, f2, x, y, r):
     """f1 (H1,W1,C), f2 (H2,W2,C), x,y (H1,W1) -> taps (H1,W1,rd+1,rd+1)."""
     H2, W2, C = f2.shape
@@ -186,3 +231,25 @@ def altcorr_index_forward(fmap1, levels, coords, ii, jj, r):
                 o = _bilinear_from_taps(t, x, y, r)
                 out[b, m, l * rd * rd:(l + 1) * rd * rd] = o.reshape(H, W, rd * rd).transpose(2, 0, 1)
     return out
+
+
+def altcorr_index_backward(fmap1, levels, coords, ii, jj, grad, r, exact_coords=False):
+    """Adjoint of altcorr_index_forward: -> (d fmap1, [d level], d coords), each edge and level
+    the per-level altcorr_backward at coords / 2^l (coords gradient scaled back by 2^-l)."""
+    f1 = np.asarray(fmap1, np.float64)
+    c = np.asarray(coords, np.float64)
+    g = np.asarray(grad, np.float64)
+    B, M, H, W, _ = c.shape
+    rd = 2 * r + 1
+    g1 = np.zeros_like(f1)
+    gl = [np.zeros(np.shape(lv)) for lv in levels]
+    gc = np.zeros_like(c)
+    for l, lv in enumerate(levels):
+        f2 = np.asarray(lv, np.float64)
+        for m in range(M):
+            a, b, cc = altcorr_backward(f1[:, ii[m]], f2[:, jj[m]], c[:, m:m + 1] / 2 ** l,
+                                        g[:, m:m + 1, l * rd * rd:(l + 1) * rd * rd], r, exact_coords=exact_coords)
+            g1[:, ii[m]] += a
+            gl[l][:, jj[m]] += b
+            gc[:, m] += cc[:, 0] / 2 ** l
+    return g1, gl, gc

@@ -155,3 +155,126 @@ def test_volume_build_shapes_and_corrblock():
     c4 = coords[0].permute(0, 3, 1, 2).cpu().numpy()
     want = np.concatenate([oc.corr_index_forward(pyr[l], c4 / 2**l, 3).reshape(N, 49, H, W) for l in range(4)], 1)
     np.testing.assert_allclose(out[0].double().cpu().numpy(), want, atol=1e-2)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float16, torch.float64])
+def test_corr_index_coords_backward(dtype):
+    g = torch.Generator().manual_seed(16)
+    B, h1, w1, h2, w2 = 2, 6, 8, 6, 8
+    vol = torch.randn(B, h1, w1, h2, w2, generator=g)
+    coords = _grid_coords(B, h1, w1, g, 1.5, spill=5.0)
+    grad = torch.randn(B, 7, 7, h1, w1, generator=g)
+    out = _dne().corr_index_coords_backward(vol.to(dtype).cuda(), coords.cuda(), grad.to(dtype).cuda(), 3)[0]
+    want = oc.corr_index_coords_backward(vol.to(dtype).double().numpy(), coords.numpy(),
+                                         grad.to(dtype).double().numpy(), 3)
+    tol = {torch.float32: 1e-4, torch.float16: 2e-2, torch.float64: 1e-5}[dtype]  # f64 result is stored as f32
+    np.testing.assert_allclose(out.double().cpu().numpy(), want, atol=tol, rtol=1e-5)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float16])
+def test_corrblock_gradients_fmaps_and_coords(dtype):
+    """CorrBlock forward + backward: gradients to both feature maps and to the coordinates
+    against the FP64 oracle (lookup adjoint per level, then the pyramid backward) on the
+    operands the tensor cores multiplied."""
+    from vipe_b200.droid_corr import CorrBlock, CorrSampler
+
+    g = torch.Generator().manual_seed(17)
+    B, N, C, H, W = 1, 2, 64, 16, 32
+    f1 = (torch.randn(B, N, C, H, W, generator=g) / 2).to(dtype).cuda().requires_grad_()
+    f2 = (torch.randn(B, N, C, H, W, generator=g) / 2).to(dtype).cuda().requires_grad_()
+    coords = _grid_coords(B * N, H, W, g, 1.5).permute(0, 2, 3, 1).reshape(B, N, H, W, 2)
+    coords = coords.cuda().requires_grad_()
+    R = torch.randn(B, N, 4 * 49, H, W, generator=g)
+    CorrSampler.exact_coords_grad = True
+    try:
+        # 16-bit inputs keep a 16-bit volume: lookup and level gradients in FP16, products in FP16
+        out_dtype = torch.float32 if dtype == torch.float32 else dtype
+        out = CorrBlock(f1, f2, num_levels=4, radius=3, out_dtype=out_dtype)(coords)
+        (out * R.to(out_dtype).cuda()).sum().backward()
+    finally:
+        CorrSampler.exact_coords_grad = False
+    op = torch.bfloat16 if dtype == torch.float32 else dtype
+    a1 = f1.detach().to(op).double().cpu().numpy()[0]
+    a2 = f2.detach().to(op).double().cpu().numpy()[0]
+    pyr = oc.corr_pyramid(a1, a2, 4)
+    c4 = coords.detach()[0].permute(0, 3, 1, 2).cpu().double().numpy()
+    Rn = R[0].to(dtype).double().numpy().reshape(N, 4, 7, 7, H, W)
+    lg, gc = [], np.zeros_like(c4)
+    for l in range(4):
+        lg.append(oc.corr_index_backward(pyr[l].shape, c4 / 2**l, Rn[:, l], 3))
+        gc += oc.corr_index_coords_backward(pyr[l], c4 / 2**l, Rn[:, l], 3) / 2**l
+    w1, w2 = oc.corr_pyramid_backward(a1, a2, lg)
+    got1 = f1.grad[0].double().cpu().numpy()
+    got2 = f2.grad[0].double().cpu().numpy()
+    gotc = coords.grad[0].permute(0, 3, 1, 2).double().cpu().numpy()
+    # FP32: FP32 products of FP32 level gradients; FP16: every level gradient and product rounded to FP16
+    tol = 1e-4 if dtype == torch.float32 else 1e-2
+    for got, want in ((got1, w1), (got2, w2)):
+        assert np.abs(got - want).max() <= tol * np.abs(want).max()
+    # the coordinate gradient differences neighbouring volume taps (FP32-accumulated on the GPU, FP16-stored
+    # for FP16 inputs)
+    ctol = 2e-3 if dtype == torch.float32 else 2e-2
+    assert np.abs(gotc - gc).max() <= ctol * np.abs(gc).max()
+
+
+@pytest.mark.parametrize("dtype,C", [(torch.float32, 32), (torch.float32, 30), (torch.float16, 64),
+                                     (torch.bfloat16, 128)])
+def test_altcorr_index_backward(dtype, C):
+    g = torch.Generator().manual_seed(18)
+    B, Nf, H, W, M = 1, 4, 16, 24, 5
+    f = (torch.randn(B, Nf, H, W, C, generator=g) / 4).to(dtype)
+    levels = [f]
+    for _ in range(3):
+        t = levels[-1].float().permute(0, 1, 4, 2, 3).reshape(B * Nf, C, levels[-1].shape[2], levels[-1].shape[3])
+        t = torch.nn.functional.avg_pool2d(t, 2, stride=2)
+        levels.append(t.reshape(B, Nf, C, t.shape[-2], t.shape[-1]).permute(0, 1, 3, 4, 2).contiguous().to(dtype))
+    ii = torch.tensor([0, 1, 2, 0, 3])
+    jj = torch.tensor([1, 2, 3, 2, 2])  # frames 0 and 2 are each used by two edges: overlapping scatters
+    coords = _grid_coords(B * M, H, W, g, 1.5, spill=3.0).reshape(B, M, 2, H, W).permute(0, 1, 3, 4, 2).contiguous()
+    grad = torch.randn(B, M, 4 * 49, H, W, generator=g)
+    g1, gl, gc = _dne().altcorr_index_backward(f.cuda(), [lv.cuda() for lv in levels], coords.cuda(), ii.cuda(),
+                                               jj.cuda(), grad.cuda(), 3, True)
+    w1, wl, wc = oc.altcorr_index_backward(f.double().numpy(), [lv.double().numpy() for lv in levels],
+                                           coords.numpy(), ii.numpy(), jj.numpy(), grad.numpy(), 3,
+                                           exact_coords=True)
+    np.testing.assert_allclose(g1.cpu().numpy(), w1, atol=2e-4)
+    for a, b in zip(gl, wl):
+        np.testing.assert_allclose(a.cpu().numpy(), b, atol=2e-4)
+    np.testing.assert_allclose(gc.cpu().numpy(), wc, atol=2e-4)
+    # without the exact flag the coordinate gradient is zero
+    gz = _dne().altcorr_index_backward(f.cuda(), [lv.cuda() for lv in levels], coords.cuda(), ii.cuda(), jj.cuda(),
+                                       grad.cuda(), 3, False)[2]
+    assert float(gz.abs().max()) == 0.0
+
+
+def test_altcorrblock_indexed_gradients_match_per_level_route():
+    """AltCorrBlock: gradients (feature maps through the pooled pyramid, coordinates) of the
+    indexed lookup equal those of the per-level on-the-fly route (the reference's checking route
+    for the forward, tests/test_altcorr_indexed.py)."""
+    from vipe_b200.droid_corr import AltCorrBlock, AltCorrIndex, CorrLayer
+
+    g = torch.Generator().manual_seed(19)
+    B, N, C, H, W, E = 1, 5, 64, 16, 32, 6
+    fmaps0 = torch.randn(B, N, C, H, W, generator=g).cuda()
+    ii = torch.tensor([0, 1, 2, 3, 0, 4], device="cuda")
+    jj = torch.tensor([1, 2, 3, 4, 2, 2], device="cuda")
+    yy, xx = torch.meshgrid(torch.arange(H), torch.arange(W), indexing="ij")
+    coords0 = (torch.stack([xx, yy], -1).float()[None].repeat(B, E, 1, 1, 1)
+               + 0.8 * torch.randn(B, E, H, W, 2, generator=g)).cuda()
+    R = torch.randn(B, E, 4 * 49, H, W, generator=g).cuda()
+    grads = []
+    for route in ("indexed", "reference"):
+        fm = fmaps0.clone().requires_grad_()
+        co = coords0.clone().requires_grad_()
+        AltCorrIndex.exact_coords_grad = CorrLayer.exact_coords_grad = True
+        try:
+            blk = AltCorrBlock(fm)
+            cs = co.unsqueeze(-2)
+            out = blk.corr_fn_indexed(cs, ii, jj) if route == "indexed" else blk.corr_fn_reference(cs, ii, jj)
+            (out[..., 0] * R).sum().backward()
+        finally:
+            AltCorrIndex.exact_coords_grad = CorrLayer.exact_coords_grad = False
+        grads.append((fm.grad, co.grad))
+    (a1, ac), (b1, bc) = grads
+    torch.testing.assert_close(a1, b1, atol=1e-4, rtol=1e-4)
+    torch.testing.assert_close(ac, bc, atol=1e-4, rtol=1e-4)

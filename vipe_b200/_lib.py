@@ -61,9 +61,11 @@ _SIGS: dict[str, tuple] = {
     "vipe_slam_iproj": (I, [P, P, P, I, I, I, P, P]),
     "vipe_corr_index_forward": (I, [I, P, P, I, I, I, I, I, I, P, P]),
     "vipe_corr_index_backward": (I, [I, P, P, I, I, I, I, I, I, P, P]),
+    "vipe_corr_index_coords_backward": (I, [I, P, P, P, I, I, I, I, I, I, P, P]),
     "vipe_altcorr_forward": (I, [I, P, P, P, I, I, I, I, I, I, I, I, P, P]),
     "vipe_altcorr_backward": (I, [P, P, P, P, I, I, I, I, I, I, I, I, I, P, P, P, P]),
     "vipe_altcorr_index_forward": (I, [I, P, P, P, P, I, P, P, P, I, I, I, I, I, I, I, P, P]),
+    "vipe_altcorr_index_backward": (I, [I, P, P, P, P, I, P, P, P, P, I, I, I, I, I, I, I, I, P, P, P, P]),
     "vipe_corr_volume_workspace_size": (SZ, [I, I, I, I]),
     "vipe_corr_volume_build": (I, [I, I, P, P, I, I, I, I, I, P, P, SZ, P]),
 }

@@ -7,6 +7,10 @@
 //       feature maps (altcorr_kernel.cu:26-138, 242-366)
 //   altcorr_index_forward           indexed, multi-level on-the-fly lookup
 //       (altcorr_kernel.cu:140-240, 394-424)
+//   corr_index_coords_backward, altcorr_index_backward
+//                                   adjoints the reference does not have: the
+//       coordinate gradient of the volume lookup and the map / pyramid /
+//       coordinate gradients of the indexed lookup
 //
 // Conventions kept from the reference: taps at floor(x) - r + i, floor(y) - r
 // + j for i, j in [0, 2r+1]; output channel = i * (2r+1) + j (x-offset major);
@@ -187,6 +191,58 @@ __global__ void corr_index_bwd_kernel<double>(const float* __restrict__ coords, 
             if (i < rd && j < rd) s += go[(int64_t)(i * rd + j) * HW1] * (1 - dx) * (1 - dy);
             plane[(int64_t)y1 * w2 + x1] = s;
         }
+}
+
+// Exact coordinate gradient of the lookup (the reference's CorrSampler returns
+// none): with taps v00 = V[y, x], v10 = V[y, x+1], v01 = V[y+1, x], v11 = V[y+1, x+1]
+// of output (i, j),  d/dx = (1-dy)(v10 - v00) + dy (v11 - v01),
+//                    d/dy = (1-dx)(v01 - v00) + dx (v11 - v10),
+// contracted with the output gradient over the (2r+1)^2 channels.  The floor is
+// piecewise constant, so the derivative is the one-sided one inside each cell.
+// One thread per pixel; the (2r+2)^2 window of its plane is read once.
+template <typename A, typename T>
+__device__ __forceinline__ A load_acc(const T* p) {
+    return (A)to_f(*p);
+}
+template <>
+__device__ __forceinline__ double load_acc<double, double>(const double* p) {
+    return *p;
+}
+
+template <typename T>
+__global__ void corr_index_coords_bwd_kernel(const T* __restrict__ vol, const float* __restrict__ coords,
+                                             const T* __restrict__ g, float* __restrict__ cgrad, int B, int h1,
+                                             int w1, int h2, int w2, int r) {
+    using A = typename Acc<T>::type;
+    const int64_t HW1 = (int64_t)h1 * w1;
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= B * HW1) return;
+    const int n = (int)(idx / HW1);
+    const int64_t pix = idx % HW1;
+    const float x0 = coords[((int64_t)n * 2 + 0) * HW1 + pix];
+    const float y0 = coords[((int64_t)n * 2 + 1) * HW1 + pix];
+    const float fx0 = floorf(x0), fy0 = floorf(y0);
+    const A dx = (A)(x0 - fx0), dy = (A)(y0 - fy0);
+    const int bx = (int)fx0 - r, by = (int)fy0 - r;
+    const int rd = 2 * r + 1;
+    const T* plane = vol + ((int64_t)n * HW1 + pix) * ((int64_t)h2 * w2);
+    const T* go = g + (int64_t)n * rd * rd * HW1 + pix;
+    auto tap = [&](int x, int y) -> A { return inb(y, x, h2, w2) ? load_acc<A>(plane + (int64_t)y * w2 + x) : (A)0; };
+    A gx = 0, gy = 0;
+    for (int i = 0; i < rd; i++) {
+        // column pair x = bx + i, bx + i + 1 walked down the rows: each row's taps are reused by the next j
+        A v00 = tap(bx + i, by), v10 = tap(bx + i + 1, by);
+        for (int j = 0; j < rd; j++) {
+            const A v01 = tap(bx + i, by + j + 1), v11 = tap(bx + i + 1, by + j + 1);
+            const A gij = load_acc<A>(go + (int64_t)(i * rd + j) * HW1);
+            gx += gij * ((1 - dy) * (v10 - v00) + dy * (v11 - v01));
+            gy += gij * ((1 - dx) * (v01 - v00) + dx * (v11 - v10));
+            v00 = v01;
+            v10 = v11;
+        }
+    }
+    cgrad[((int64_t)n * 2 + 0) * HW1 + pix] = (float)gx;
+    cgrad[((int64_t)n * 2 + 1) * HW1 + pix] = (float)gy;
 }
 
 // ---------------------------------------------------------------- on-the-fly lookup (warp per pixel)
@@ -453,11 +509,180 @@ __global__ void __launch_bounds__(kWarps * 32)
     for (int c = lane; c < C; c += 32) q1[c] = acc1[warp][c];
 }
 
+// four consecutive channels as floats (16-bit types: one 8-byte load, f32: one 16-byte load)
+template <typename T>
+__device__ __forceinline__ void load4(const T* p, float* v) {
+    const uint2 raw = __ldg(reinterpret_cast<const uint2*>(p));
+    const T* e = reinterpret_cast<const T*>(&raw);
+#pragma unroll
+    for (int k = 0; k < 4; k++) v[k] = to_f(e[k]);
+}
+template <>
+__device__ __forceinline__ void load4<float>(const float* p, float* v) {
+    const float4 raw = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = raw.x;
+    v[1] = raw.y;
+    v[2] = raw.z;
+    v[3] = raw.w;
+}
+
+struct LevelGrads {
+    float* p[8];
+};
+
+// Adjoint of altcorr_index_forward (the reference has none): gradients to the
+// level-0 map fmap1 (B,Nf,H,W,C), to every pyramid level (B,Nf,H2[l],W2[l],C)
+// and, with exact_coords, to coords (B,M,H,W,2) (sum over levels of 2^-l times
+// the derivative of the bilinear weights at level l; zeros otherwise).  All
+// gradients are f32; the map gradients must be zero on entry.  One warp per
+// (pixel, edge): tap gradients from the bilinear adjoint per level; the
+// fmap1 gradient is gathered in registers over all levels' taps and added once
+// (edges sharing a source frame add into the same row); the level gradients
+// are scattered into the window rows (windows of neighbouring pixels and of
+// edges sharing a target overlap).  Both use 16-byte vector atomics when
+// `vec` (C % 4 == 0 and aligned rows), one lane per 4 channels.
+// grid (ceil(W / kWarps), H, B * M)
+template <typename T>
+__global__ void __launch_bounds__(kWarps * 32)
+    altcorr_index_bwd_kernel(const T* __restrict__ fmap1, LevelPtrs lv, LevelGrads lg, int L,
+                             const float* __restrict__ coords, const int64_t* __restrict__ ii,
+                             const int64_t* __restrict__ jj, const float* __restrict__ g, float* __restrict__ g1,
+                             float* __restrict__ gc, int B, int Nf, int M, int H, int W, int C, int r,
+                             int exact_coords, int vec) {
+    __shared__ float f1s[kWarps][kMaxC];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bm = blockIdx.z, b = bm / M, m = bm % M;
+    const int h = blockIdx.y, w = blockIdx.x * kWarps + warp;
+    if (w >= W) return;
+    const int src = (int)ii[m], dst = (int)jj[m];
+    const int rd = 2 * r + 1, nch = rd * rd, ne = rd + 1, nt = ne * ne;
+    const int64_t HW = (int64_t)H * W;
+    const T* f1 = fmap1 + ((((int64_t)b * Nf + src) * H + h) * W + w) * C;
+    for (int c = lane; c < C; c += 32) f1s[warp][c] = to_f(f1[c]);
+    __syncwarp();
+    // this lane's channels of the fmap1 gradient: vector path c = 4 lane + 128 k, scalar path c = lane + 32 k
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float* cp = coords + (((int64_t)bm * H + h) * W + w) * 2;
+    float gcx = 0.f, gcy = 0.f;
+    for (int l = 0; l < L; l++) {
+        const float scale = (float)(1 << l);
+        const float xc = cp[0] / scale, yc = cp[1] / scale;
+        const float dx = xc - floorf(xc), dy = yc - floorf(yc);
+        const int bx = (int)floorf(xc) - r, by = (int)floorf(yc) - r;
+        const int H2 = lv.H2[l], W2 = lv.W2[l];
+        const int64_t plane = ((int64_t)b * Nf + dst) * H2 * W2;
+        const T* f2base = static_cast<const T*>(lv.p[l]) + plane * C;
+        float* g2base = lg.p[l] + plane * C;
+        const float* gp = g + ((int64_t)bm * L * nch + (int64_t)l * nch) * HW + (int64_t)h * W + w;
+        float gt[2];
+#pragma unroll
+        for (int hh = 0; hh < 2; hh++) {
+            const int tap = lane + 32 * hh;
+            float v = 0.f;
+            if (tap < nt) {
+                const int i = tap / ne, j = tap % ne;
+                if (i > 0 && j > 0) v += gp[(int64_t)((i - 1) * rd + (j - 1)) * HW] * dx * dy;
+                if (i > 0 && j < rd) v += gp[(int64_t)((i - 1) * rd + j) * HW] * dx * (1.f - dy);
+                if (i < rd && j > 0) v += gp[(int64_t)(i * rd + (j - 1)) * HW] * (1.f - dx) * dy;
+                if (i < rd && j < rd) v += gp[(int64_t)(i * rd + j) * HW] * (1.f - dx) * (1.f - dy);
+            }
+            gt[hh] = v;
+        }
+        if (exact_coords) {
+            float t0, t1;
+            window_dots<T, float>(f2base, H2, W2, C, f1s[warp], xc, yc, r, t0, t1);
+            float cx = 0.f, cy = 0.f;
+#pragma unroll
+            for (int hh = 0; hh < 2; hh++) {
+                const int ch = lane + 32 * hh;
+                const int chc = ch < nch ? ch : 0;
+                const int i = chc / rd, j = chc % rd;
+                const float a00 = tap_value(t0, t1, ne, i, j);
+                const float a10 = tap_value(t0, t1, ne, i + 1, j);
+                const float a01 = tap_value(t0, t1, ne, i, j + 1);
+                const float a11 = tap_value(t0, t1, ne, i + 1, j + 1);
+                if (ch < nch) {
+                    const float go = gp[(int64_t)ch * HW];
+                    cx += go * ((1.f - dy) * (a10 - a00) + dy * (a11 - a01));
+                    cy += go * ((1.f - dx) * (a01 - a00) + dx * (a11 - a10));
+                }
+            }
+            gcx += warp_sum(cx) / scale;
+            gcy += warp_sum(cy) / scale;
+        }
+        for (int tap = 0; tap < nt; tap++) {
+            const float gv = __shfl_sync(0xffffffffu, gt[tap >> 5], tap & 31);
+            const int ix = tap / ne, iy = tap % ne;
+            const int x2 = bx + ix, y2 = by + iy;
+            if (gv == 0.f || !inb(y2, x2, H2, W2)) continue;  // warp-uniform
+            const int64_t row = ((int64_t)y2 * W2 + x2) * C;
+            if (vec) {
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    const int c = 4 * lane + 128 * k;
+                    if (c >= C) break;
+                    float f2v[4];
+                    load4<T>(f2base + row + c, f2v);
+                    float4 add;
+                    add.x = gv * f1s[warp][c];
+                    add.y = gv * f1s[warp][c + 1];
+                    add.z = gv * f1s[warp][c + 2];
+                    add.w = gv * f1s[warp][c + 3];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) acc[4 * k + q] += gv * f2v[q];
+                    atomicAdd(reinterpret_cast<float4*>(g2base + row + c), add);
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const int c = lane + 32 * k;
+                    if (c >= C) break;
+                    acc[k] += gv * to_f(f2base[row + c]);
+                    atomicAdd(g2base + row + c, gv * f1s[warp][c]);
+                }
+            }
+        }
+    }
+    float* q1 = g1 + ((((int64_t)b * Nf + src) * H + h) * W + w) * C;
+    if (vec) {
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int c = 4 * lane + 128 * k;
+            if (c >= C) break;
+            atomicAdd(reinterpret_cast<float4*>(q1 + c), make_float4(acc[4 * k], acc[4 * k + 1], acc[4 * k + 2],
+                                                                     acc[4 * k + 3]));
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int c = lane + 32 * k;
+            if (c >= C) break;
+            atomicAdd(q1 + c, acc[k]);
+        }
+    }
+    if (gc && lane == 0) {
+        float* o = gc + (((int64_t)bm * H + h) * W + w) * 2;
+        o[0] = gcx;
+        o[1] = gcy;
+    }
+}
+
 template <typename F>
 int dispatch(int dtype, F&& f) {
     switch (dtype) {
         case VIPE_F32: return f(float());
         case VIPE_F64: return f(double());
+        case VIPE_F16: return f(__half());
+        case VIPE_BF16: return f(__nv_bfloat16());
+        default: return VIPE_ERR_DTYPE;
+    }
+}
+
+// f32 / f16 / bf16 only
+template <typename F>
+int dispatch_no_f64(int dtype, F&& f) {
+    switch (dtype) {
+        case VIPE_F32: return f(float());
         case VIPE_F16: return f(__half());
         case VIPE_BF16: return f(__nv_bfloat16());
         default: return VIPE_ERR_DTYPE;
@@ -500,6 +725,24 @@ extern "C" int vipe_corr_index_backward(int dtype, const float* coords, const vo
         corr_index_bwd_kernel<T><<<ceil_div(n, 256), 256, 0, st>>>(coords, static_cast<const T*>(corr_grad),
                                                                    static_cast<T*>(volume_grad_out), B, h1, w1, h2,
                                                                    w2, radius);
+        VIPE_LAUNCH_CHECK();
+        return (int)VIPE_OK;
+    });
+}
+
+extern "C" int vipe_corr_index_coords_backward(int dtype, const void* volume, const float* coords,
+                                               const void* corr_grad, int B, int h1, int w1, int h2, int w2,
+                                               int radius, float* coords_grad_out, void* stream) {
+    if (B < 0 || h1 < 0 || w1 < 0 || h2 <= 0 || w2 <= 0 || radius < 0) return VIPE_ERR_ARG;
+    const int64_t n = (int64_t)B * h1 * w1;
+    if (n == 0) return VIPE_OK;
+    cudaStream_t st = as_stream(stream);
+    return dispatch(dtype, [&](auto tag) {
+        using T = decltype(tag);
+        VIPE_PROF("corr_index_coords_bwd", st);
+        corr_index_coords_bwd_kernel<T><<<ceil_div(n, 256), 256, 0, st>>>(
+            static_cast<const T*>(volume), coords, static_cast<const T*>(corr_grad), coords_grad_out, B, h1, w1, h2,
+            w2, radius);
         VIPE_LAUNCH_CHECK();
         return (int)VIPE_OK;
     });
@@ -570,6 +813,44 @@ extern "C" int vipe_altcorr_index_forward(int dtype, const void* fmap1, const vo
         altcorr_index_fwd_kernel<T><<<grid, kWarps * 32, 0, st>>>(static_cast<const T*>(fmap1), lv, num_levels,
                                                                    coords, ii, jj, corr_out, B, Nf, M, H, W, C,
                                                                    radius);
+        VIPE_LAUNCH_CHECK();
+        return (int)VIPE_OK;
+    });
+}
+
+extern "C" int vipe_altcorr_index_backward(int dtype, const void* fmap1, const void* const* fmap2_levels,
+                                           const int* H2, const int* W2, int num_levels, const float* coords,
+                                           const int64_t* ii, const int64_t* jj, const float* corr_grad, int B,
+                                           int Nf, int M, int H, int W, int C, int radius, int exact_coords_grad,
+                                           float* fmap1_grad_out, float* const* level_grads_out,
+                                           float* coords_grad_out, void* stream) {
+    if (B < 0 || Nf <= 0 || M < 0 || H < 0 || W < 0 || C <= 0 || num_levels <= 0) return VIPE_ERR_ARG;
+    if (num_levels > kMaxL || C > kMaxC || radius < 0 || radius > kMaxR) return VIPE_ERR_CAPACITY;
+    if (!fmap1_grad_out || !level_grads_out) return VIPE_ERR_ARG;
+    cudaStream_t st = as_stream(stream);
+    const size_t esz = dtype == VIPE_F32 ? 4 : 2;
+    LevelPtrs lv;
+    LevelGrads lg;
+    bool aligned = C % 4 == 0 && (uintptr_t)fmap1 % 16 == 0 && (uintptr_t)fmap1_grad_out % 16 == 0;
+    for (int l = 0; l < num_levels; l++) {
+        if (H2[l] <= 0 || W2[l] <= 0 || !fmap2_levels[l] || !level_grads_out[l]) return VIPE_ERR_ARG;
+        lv.p[l] = fmap2_levels[l];
+        lv.H2[l] = H2[l];
+        lv.W2[l] = W2[l];
+        lg.p[l] = level_grads_out[l];
+        aligned = aligned && (uintptr_t)fmap2_levels[l] % (4 * esz) == 0 && (uintptr_t)level_grads_out[l] % 16 == 0;
+        VIPE_CUDA_TRY(cudaMemsetAsync(level_grads_out[l], 0, (size_t)B * Nf * H2[l] * W2[l] * C * sizeof(float), st));
+    }
+    VIPE_CUDA_TRY(cudaMemsetAsync(fmap1_grad_out, 0, (size_t)B * Nf * H * W * C * sizeof(float), st));
+    if ((int64_t)B * M * H * W == 0) return VIPE_OK;
+    if (B * M > 65535 || H > 65535) return VIPE_ERR_CAPACITY;
+    dim3 grid(ceil_div(W, kWarps), H, B * M);
+    return dispatch_no_f64(dtype, [&](auto tag) {
+        using T = decltype(tag);
+        VIPE_PROF("altcorr_index_bwd", st);
+        altcorr_index_bwd_kernel<T><<<grid, kWarps * 32, 0, st>>>(
+            static_cast<const T*>(fmap1), lv, lg, num_levels, coords, ii, jj, corr_grad, fmap1_grad_out,
+            coords_grad_out, B, Nf, M, H, W, C, radius, exact_coords_grad, aligned ? 1 : 0);
         VIPE_LAUNCH_CHECK();
         return (int)VIPE_OK;
     });

@@ -10,7 +10,14 @@ can switch by import.  Differences from the reference:
     of torch.matmul followed by three avg_pool2d passes;
   * CorrSampler / CorrLayer backward return the exact coordinate gradient of the
     bilinear lookup when ``exact_coords_grad`` is set (the reference returns no
-    or zero coordinate gradient).
+    or zero coordinate gradient);
+  * with autograd recording and a feature map that requires grad, the pyramid
+    is built by CorrVolume, whose backward returns the feature-map gradients of
+    every level at once (the reference differentiates torch.matmul and the
+    avg_pool2d passes);
+  * AltCorrBlock's indexed lookup is differentiable (AltCorrIndex: gradients to
+    the maps, the pyramid levels and optionally the coordinates); the
+    reference's has no backward.
 """
 
 from __future__ import annotations
@@ -22,20 +29,87 @@ from .ext import droid_net_ext
 
 
 class CorrSampler(torch.autograd.Function):
-    """Lookup in a materialised volume (reference droid_net.py:32-45)."""
+    """Lookup in a materialised volume (reference droid_net.py:32-45).
+
+    Like the reference, backward returns no coordinate gradient unless the class
+    attribute ``exact_coords_grad`` is set.
+    """
+
+    exact_coords_grad = False
 
     @staticmethod
     def forward(ctx, volume, coords, radius):
         ctx.save_for_backward(volume, coords)
         ctx.radius = radius
+        ctx.exact = CorrSampler.exact_coords_grad
         (corr,) = droid_net_ext.corr_index_forward(volume, coords, radius)
         return corr
 
     @staticmethod
     def backward(ctx, grad_output):
         volume, coords = ctx.saved_tensors
-        (grad_volume,) = droid_net_ext.corr_index_backward(volume, coords, grad_output.contiguous(), ctx.radius)
-        return grad_volume, None, None
+        grad_output = grad_output.contiguous()
+        grad_volume = grad_coords = None
+        if ctx.needs_input_grad[0]:
+            (grad_volume,) = droid_net_ext.corr_index_backward(volume, coords, grad_output, ctx.radius)
+        if ctx.exact and ctx.needs_input_grad[1]:
+            (grad_coords,) = droid_net_ext.corr_index_coords_backward(volume, coords, grad_output, ctx.radius)
+        return grad_volume, grad_coords, None
+
+
+def _operand_dtype(fmap, compute_dtype):
+    """Tensor-core operand type of the volume build: float16 stays FP16, the rest runs as BF16."""
+    if compute_dtype is not None:
+        return compute_dtype
+    return fmap.dtype if fmap.dtype in (torch.float16, torch.bfloat16) else torch.bfloat16
+
+
+class CorrVolume(torch.autograd.Function):
+    """Volume pyramid (num, C, H, W) x2 -> levels l of (num, H*W, H >> l, W >> l).
+
+    Backward, with G_l the level gradients, P_l the l-fold 2x2 average pool over
+    the target axes and U_l its adjoint (each pooled value spread over its
+    2^l x 2^l block, divided by 4^l):
+        d fmap1 = 1/16 sum_l P_l(fmap2) G_l^T,   d fmap2 = 1/16 sum_l U_l(fmap1 G_l)
+    taken at the rounded operands the forward multiplied (straight through the
+    rounding).  The products are plain batched GEMMs (cuBLAS through torch.bmm):
+    in the operand type when the level gradient already has it, else in FP32;
+    the levels are summed in FP32.
+    """
+
+    @staticmethod
+    def forward(ctx, fmap1, fmap2, num_levels, out_dtype, compute_dtype):
+        from .corr_build import corr_volume_pyramid
+
+        ctx.save_for_backward(fmap1, fmap2)
+        ctx.op = _operand_dtype(fmap1, compute_dtype)
+        return tuple(corr_volume_pyramid(fmap1, fmap2, num_levels, out_dtype=out_dtype, compute_dtype=compute_dtype))
+
+    @staticmethod
+    def backward(ctx, *grads):
+        fmap1, fmap2 = ctx.saved_tensors
+        num, C, H, W = fmap1.shape
+        f1 = fmap1.to(ctx.op).reshape(num, C, H * W)
+        f2 = fmap2.to(ctx.op)
+        g1 = torch.zeros(num, C, H * W, dtype=torch.float32, device=fmap1.device) if ctx.needs_input_grad[0] else None
+        g2 = torch.zeros(num, C, H, W, dtype=torch.float32, device=fmap1.device) if ctx.needs_input_grad[1] else None
+        for l, G in enumerate(grads):
+            if G is None:
+                continue
+            h, w = H >> l, W >> l
+            mm = G.dtype if G.dtype == ctx.op else torch.float32
+            G = G.reshape(num, H * W, h * w).to(mm)
+            if g1 is not None:
+                p2 = F.avg_pool2d(f2.float(), 2**l) if l else f2.float()
+                g1 += torch.bmm(p2.reshape(num, C, h * w).to(mm), G.transpose(1, 2)).float()
+            if g2 is not None:
+                m = torch.bmm(f1.to(mm), G).float().reshape(num, C, h, w)
+                if l:
+                    m = m.repeat_interleave(2**l, dim=2).repeat_interleave(2**l, dim=3) / float(4**l)
+                g2 += m
+        d1 = None if g1 is None else (g1 / 16.0).reshape(num, C, H, W).to(fmap1.dtype)
+        d2 = None if g2 is None else (g2 / 16.0).to(fmap2.dtype)
+        return d1, d2, None, None, None
 
 
 class CorrBlock:
@@ -52,10 +126,14 @@ class CorrBlock:
         batch, num, dim, ht, wd = fmap1.shape
         if out_dtype is None:
             out_dtype = fmap1.dtype if fmap1.dtype in (torch.float16, torch.bfloat16) else torch.float32
-        from .corr_build import corr_volume_pyramid
+        f1 = fmap1.reshape(batch * num, dim, ht, wd)
+        f2 = fmap2.reshape(batch * num, dim, ht, wd)
+        if torch.is_grad_enabled() and (fmap1.requires_grad or fmap2.requires_grad):
+            levels = CorrVolume.apply(f1, f2, num_levels, out_dtype, compute_dtype)
+        else:
+            from .corr_build import corr_volume_pyramid
 
-        levels = corr_volume_pyramid(fmap1.reshape(batch * num, dim, ht, wd), fmap2.reshape(batch * num, dim, ht, wd),
-                                     num_levels, out_dtype=out_dtype, compute_dtype=compute_dtype)
+            levels = corr_volume_pyramid(f1, f2, num_levels, out_dtype=out_dtype, compute_dtype=compute_dtype)
         self.corr_pyramid = [lv.view(batch * num, ht, wd, lv.shape[-2], lv.shape[-1]) for lv in levels]
 
     def __call__(self, coords):
@@ -80,11 +158,9 @@ class CorrBlock:
     @staticmethod
     def corr(fmap1, fmap2):
         """All-pairs correlation (batch, num, H, W, H, W) of (fmap1/4)^T (fmap2/4)."""
-        from .corr_build import corr_volume_pyramid
-
         batch, num, dim, ht, wd = fmap1.shape
-        (v,) = corr_volume_pyramid(fmap1.reshape(batch * num, dim, ht, wd), fmap2.reshape(batch * num, dim, ht, wd),
-                                   1, out_dtype=torch.float32)
+        (v,) = CorrVolume.apply(fmap1.reshape(batch * num, dim, ht, wd), fmap2.reshape(batch * num, dim, ht, wd), 1,
+                                torch.float32, None)
         return v.view(batch, num, ht, wd, ht, wd)
 
 
@@ -106,6 +182,30 @@ class CorrLayer(torch.autograd.Function):
         g1, g2, gc = droid_net_ext.altcorr_backward(fmap1, fmap2, coords, grad_corr.contiguous(), ctx.r,
                                                     CorrLayer.exact_coords_grad)
         return g1, g2, gc, None
+
+
+class AltCorrIndex(torch.autograd.Function):
+    """Indexed multi-level lookup with its adjoint (the reference binds only the
+    forward).  Gradients go to fmap1, every pyramid level and, when the class
+    attribute ``exact_coords_grad`` is set, to the coordinates."""
+
+    exact_coords_grad = False
+
+    @staticmethod
+    def forward(ctx, coords, ii, jj, radius, fmap1, *levels):
+        ctx.save_for_backward(coords, ii, jj, fmap1, *levels)
+        ctx.radius = radius
+        ctx.exact = AltCorrIndex.exact_coords_grad
+        (corr,) = droid_net_ext.altcorr_index_forward(fmap1, levels, coords, ii, jj, radius)
+        return corr
+
+    @staticmethod
+    def backward(ctx, grad):
+        coords, ii, jj, fmap1, *levels = ctx.saved_tensors
+        g1, gl, gc = droid_net_ext.altcorr_index_backward(fmap1, levels, coords, ii, jj, grad.float().contiguous(),
+                                                          ctx.radius, ctx.exact)
+        gcoords = gc if ctx.exact and ctx.needs_input_grad[0] else None
+        return (gcoords, None, None, None, g1.to(fmap1.dtype), *[g.to(lv.dtype) for g, lv in zip(gl, levels)])
 
 
 class AltCorrBlock:
@@ -144,8 +244,11 @@ class AltCorrBlock:
         if coords.shape[-2] != 1:
             return self.corr_fn_reference(coords, ii, jj)
         coords = coords.squeeze(dim=-2).contiguous()
-        (corr,) = droid_net_ext.altcorr_index_forward(self.pyramid[0], self.pyramid, coords, ii.contiguous(),
-                                                      jj.contiguous(), self.radius)
+        ii, jj = ii.contiguous(), jj.contiguous()
+        if torch.is_grad_enabled() and (coords.requires_grad or any(p.requires_grad for p in self.pyramid)):
+            corr = AltCorrIndex.apply(coords, ii, jj, self.radius, self.pyramid[0], *self.pyramid)
+        else:
+            (corr,) = droid_net_ext.altcorr_index_forward(self.pyramid[0], self.pyramid, coords, ii, jj, self.radius)
         return corr.unsqueeze(dim=-1)
 
     def corr_fn(self, coords, ii, jj):

@@ -5,7 +5,10 @@ names, positional arguments and list returns.  Lookups accumulate in FP32 and
 write each output once (the reference accumulates in the volume dtype).
 ``altcorr_backward`` returns a zero coords gradient like the reference unless
 ``exact_coords_grad=True`` is passed (then the derivative of the bilinear
-lookup is returned).
+lookup is returned).  ``corr_index_coords_backward`` (not in the reference) is
+the same derivative for the materialised-volume lookup, and
+``altcorr_index_backward`` (not in the reference either) the adjoint of the
+indexed lookup.
 """
 
 from __future__ import annotations
@@ -49,6 +52,23 @@ def corr_index_backward(volume, coords, corr_grad, radius):
                                               B, h1, w1, h2, w2, int(radius), vg.data_ptr(), _lib.stream_of(volume))
     _lib.check(rc, "droid_net_ext.corr_index_backward")
     return [vg]
+
+
+def corr_index_coords_backward(volume, coords, corr_grad, radius):
+    """-> [coords_grad (B, 2, h1, w1) f32]: exact derivative of corr_index_forward in coords."""
+    _check("volume", volume)
+    _check("coords", coords)
+    _check("corr_grad", corr_grad)
+    _lib.require_dtype("coords", coords, torch.float32)
+    B, h1, w1, h2, w2 = volume.shape
+    if corr_grad.dtype != volume.dtype:
+        raise RuntimeError("corr_grad must have the volume's dtype")
+    cg = torch.empty(B, 2, h1, w1, dtype=torch.float32, device=volume.device)
+    rc = _lib.load().vipe_corr_index_coords_backward(_lib.DTYPE_CODE[volume.dtype], volume.data_ptr(),
+                                                     coords.data_ptr(), corr_grad.data_ptr(), B, h1, w1, h2, w2,
+                                                     int(radius), cg.data_ptr(), _lib.stream_of(volume))
+    _lib.check(rc, "droid_net_ext.corr_index_coords_backward")
+    return [cg]
 
 
 def altcorr_forward(fmap1, fmap2, coords, radius):
@@ -117,3 +137,37 @@ def altcorr_index_forward(fmap1, fmap2_pyramid, coords, ii, jj, radius):
                                                 int(radius), corr.data_ptr(), _lib.stream_of(fmap1))
     _lib.check(rc, "droid_net_ext.altcorr_index_forward")
     return [corr]
+
+
+def altcorr_index_backward(fmap1, fmap2_pyramid, coords, ii, jj, corr_grad, radius, exact_coords_grad=False):
+    """Adjoint of altcorr_index_forward (not in the reference) -> [fmap1_grad (B,Nf,H,W,C) f32,
+    [level grads (B,Nf,H_l,W_l,C) f32], coords_grad (B,M,H,W,2) f32 (zeros unless exact_coords_grad)]."""
+    for n, t in (("fmap1", fmap1), ("coords", coords), ("ii", ii), ("jj", jj), ("corr_grad", corr_grad)):
+        _check(n, t)
+    _lib.require_dtype("coords", coords, torch.float32)
+    _lib.require_dtype("corr_grad", corr_grad, torch.float32)
+    _lib.require_dtype("ii", ii, torch.int64)
+    _lib.require_dtype("jj", jj, torch.int64)
+    levels = list(fmap2_pyramid)
+    for l, f in enumerate(levels):
+        _check(f"fmap2_pyramid[{l}]", f)
+        if f.dtype != fmap1.dtype:
+            raise RuntimeError("pyramid levels must share fmap1's dtype")
+    B, Nf, H, W, C = fmap1.shape
+    M = coords.shape[1]
+    L = len(levels)
+    dev = fmap1.device
+    g1 = torch.empty(B, Nf, H, W, C, dtype=torch.float32, device=dev)
+    gl = [torch.empty(f.shape, dtype=torch.float32, device=dev) for f in levels]
+    gc = torch.empty(B, M, H, W, 2, dtype=torch.float32, device=dev)
+    ptrs = (ctypes.c_void_p * L)(*[f.data_ptr() for f in levels])
+    gptrs = (ctypes.c_void_p * L)(*[g.data_ptr() for g in gl])
+    h2 = (ctypes.c_int * L)(*[f.shape[2] for f in levels])
+    w2 = (ctypes.c_int * L)(*[f.shape[3] for f in levels])
+    rc = _lib.load().vipe_altcorr_index_backward(_lib.DTYPE_CODE[fmap1.dtype], fmap1.data_ptr(), ptrs, h2, w2, L,
+                                                 coords.data_ptr(), ii.data_ptr(), jj.data_ptr(),
+                                                 corr_grad.data_ptr(), B, Nf, M, H, W, C, int(radius),
+                                                 int(bool(exact_coords_grad)), g1.data_ptr(), gptrs, gc.data_ptr(),
+                                                 _lib.stream_of(fmap1))
+    _lib.check(rc, "droid_net_ext.altcorr_index_backward")
+    return [g1, gl, gc]
