@@ -255,6 +255,7 @@ def corr_build_bench(dev, steps, hbm_peak, peak_src, bf16_peak):
         wms.append(e0.elapsed_time(e1))
     write_gbs = buf.numel() * 2 / (min(wms) / 1e3) / 1e9
     del buf
+    lookup = corr_lookup_bench(dev, f1, f2, g, hbm_peak)
     return {
         "workload": "correlation volume + 4-level avg-pool pyramid, 640 edges, 128 ch, 48x64, BF16 operands, "
         "FP32 accumulate, FP16 volume",
@@ -273,6 +274,75 @@ def corr_build_bench(dev, steps, hbm_peak, peak_src, bf16_peak):
         "tensor_frac_of_bf16_peak": flops / (ms / 1e3) / 1e12 / bf16_peak,
         "reference_cublas_matmul_avgpool_ms": ref_ms,
         "speedup_vs_reference_gpu_path": ref_ms / ms,
+        "lookup": lookup,
+    }
+
+
+def corr_lookup_bench(dev, f1, f2, g, hbm_peak):
+    """Radius-3 lookups over the same 640 edges (48x64, 4 levels, 196 channels out).
+
+    Volume lookup (corr_index_forward per level on the FP16 pyramid; CorrBlock):
+    algorithmic bytes per pixel = 8 (coords) + 4 x 64 x 2 (window taps) + 196 x 2
+    (FP16 out).  Indexed on-the-fly lookup (altcorr_index_forward, FP16 maps of 64
+    frames, no volume): 2 x 4 x 64 x 128 flop and 196 x 4 B (f32 out) + 128 x 2 B
+    (fmap1 row) + 8 B per pixel.  Coordinates: a per-edge shift plus N(0, 1) px.
+    """
+    import torch
+    import torch.nn.functional as F
+
+    from vipe_b200.corr_build import corr_volume_pyramid
+    from vipe_b200.ext import droid_net_ext as dne
+
+    E, C, H, W = f1.shape
+    HW = H * W
+    stream = torch.cuda.current_stream(dev)
+    lv = corr_volume_pyramid(f1, f2, 4, out_dtype=torch.float16, check=False)
+    vols = [v.view(E, H, W, H >> l, W >> l) for l, v in enumerate(lv)]
+    yy, xx = torch.meshgrid(torch.arange(H, device=dev), torch.arange(W, device=dev), indexing="ij")
+    base = torch.stack([xx, yy], 0).float()
+    coords = base[None] + 2.0 * torch.randn(E, 2, 1, 1, generator=g, device=dev)
+    coords = (coords + torch.randn(E, 2, H, W, generator=g, device=dev)).contiguous()
+    scaled = [(coords / 2**l).contiguous() for l in range(4)]
+
+    def timed(fn, n=5):
+        fn()
+        torch.cuda.synchronize(dev)
+        ts = []
+        for _ in range(n):
+            a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            c.record(stream)
+            torch.cuda.synchronize(dev)
+            ts.append(a.elapsed_time(c))
+        return sorted(ts)[n // 2]
+
+    vol_ms = timed(lambda: [dne.corr_index_forward(vols[l], scaled[l], 3) for l in range(4)])
+    vol_bytes = E * HW * (8 + 4 * 64 * 2 + 196 * 2)
+    del vols, lv
+    # indexed form: 64 frames' maps, 640 edges (i, i + 1..3 mod 64 and longer pairs)
+    Nf = 64
+    fm = (torch.randn(1, Nf, C, H, W, generator=g, device=dev) / C**0.5).half() / 4.0
+    pyr = []
+    t = fm.view(Nf, C, H, W)
+    for l in range(4):
+        pyr.append(t.permute(0, 2, 3, 1).contiguous().view(1, Nf, H >> l, W >> l, C))
+        t = F.avg_pool2d(t.float(), 2, stride=2).half()
+    e = torch.arange(E, device=dev)
+    ii = e % Nf
+    jj = (ii + 1 + (e // Nf) % 7) % Nf
+    c5 = coords.permute(0, 2, 3, 1).reshape(1, E, H, W, 2).contiguous()
+    idx_ms = timed(lambda: dne.altcorr_index_forward(pyr[0], pyr, c5, ii, jj, 3))
+    idx_bytes = E * HW * (196 * 4 + C * 2 + 8)
+    idx_flops = 2.0 * E * HW * 4 * 64 * C
+    return {
+        "volume_lookup": {"kernel": "corr_index_fwd x 4 levels", "ms": vol_ms, "bytes": vol_bytes,
+                          "achieved": vol_bytes / (vol_ms / 1e3) / 1e9, "unit": "GB/s",
+                          "frac": vol_bytes / (vol_ms / 1e3) / 1e9 / hbm_peak},
+        "indexed_lookup": {"kernel": "altcorr_index_fwd", "ms": idx_ms, "bytes": idx_bytes,
+                           "achieved": idx_bytes / (idx_ms / 1e3) / 1e9, "unit": "GB/s",
+                           "frac": idx_bytes / (idx_ms / 1e3) / 1e9 / hbm_peak,
+                           "fp32_tflops": idx_flops / (idx_ms / 1e3) / 1e12},
     }
 
 

@@ -50,6 +50,26 @@ def test_corr_index_forward_backward(dtype):
     np.testing.assert_allclose(vg.double().cpu().numpy(), wv, atol=tol * 4)
 
 
+@pytest.mark.parametrize("dtype,w2", [(torch.float16, 32), (torch.bfloat16, 16), (torch.float32, 12),
+                                      (torch.float32, 6), (torch.float16, 6)])
+def test_corr_index_forward_vector_and_scalar_paths(dtype, w2):
+    """Radius 3 takes the 16-byte row-chunk path when w2 * size is a multiple of 16 (w2 = 32, 16, 12
+    here) and the element path otherwise (w2 = 6); windows straddle every border, and far-away
+    coordinates read only zeros."""
+    g = torch.Generator().manual_seed(20)
+    B, h1, w1, h2 = 2, 5, 7, 9
+    vol = torch.randn(B, h1, w1, h2, w2, generator=g)
+    coords = torch.stack([torch.rand(B, h1, w1, generator=g) * (w2 + 10) - 5,
+                          torch.rand(B, h1, w1, generator=g) * (h2 + 10) - 5], 1)
+    coords[0, :, 0, 0] = 1e9  # far outside: all taps zero
+    coords[1, :, 1, 1] = -3e9
+    out = _dne().corr_index_forward(vol.to(dtype).cuda(), coords.cuda(), 3)[0]
+    want = oc.corr_index_forward(vol.to(dtype).double().numpy(), coords.double().numpy(), 3)
+    tol = {torch.float32: 1e-5, torch.float16: 4e-3, torch.bfloat16: 3e-2}[dtype]
+    np.testing.assert_allclose(out.double().cpu().numpy(), want, atol=tol)
+    assert float(out[0, :, :, 0, 0].abs().max()) == 0.0 and float(out[1, :, :, 1, 1].abs().max()) == 0.0
+
+
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float16])
 def test_altcorr_forward(dtype):
     g = torch.Generator().manual_seed(12)

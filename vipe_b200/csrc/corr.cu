@@ -30,6 +30,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <type_traits>
+
 namespace vipe {
 namespace corr {
 
@@ -70,6 +72,14 @@ struct Acc<double> {
 
 __device__ __forceinline__ bool inb(int h, int w, int H, int W) { return h >= 0 && h < H && w >= 0 && w < W; }
 
+// Integer window origin floor(c) - r.  The floored coordinate is clamped to
+// +-2^24 first: any coordinate beyond that is outside every map anyway, and the
+// clamp keeps the window arithmetic (origin + tap offset) clear of int overflow
+// for huge or non-finite coordinates, whose taps then all fail the bounds test.
+__device__ __forceinline__ int window_origin(float floored, int r) {
+    return (int)fminf(fmaxf(floored, -16777216.f), 16777216.f) - r;
+}
+
 // ---------------------------------------------------------------- materialised-volume lookup
 
 template <typename T>
@@ -85,7 +95,7 @@ __global__ void corr_index_fwd_kernel(const T* __restrict__ vol, const float* __
     const float y0 = coords[((int64_t)n * 2 + 1) * HW1 + pix];
     const float fx0 = floorf(x0), fy0 = floorf(y0);
     const A dx = (A)(x0 - fx0), dy = (A)(y0 - fy0);
-    const int bx = (int)fx0 - r, by = (int)fy0 - r;
+    const int bx = window_origin(fx0, r), by = window_origin(fy0, r);
     const int rd = 2 * r + 1;
     const T* plane = vol + ((int64_t)n * HW1 + pix) * ((int64_t)h2 * w2);
     T* o = out + (int64_t)n * rd * rd * HW1 + pix;
@@ -115,7 +125,7 @@ __global__ void corr_index_fwd_kernel<double>(const double* __restrict__ vol, co
     const float y0 = coords[((int64_t)n * 2 + 1) * HW1 + pix];
     const float fx0 = floorf(x0), fy0 = floorf(y0);
     const double dx = (double)(x0 - fx0), dy = (double)(y0 - fy0);
-    const int bx = (int)fx0 - r, by = (int)fy0 - r;
+    const int bx = window_origin(fx0, r), by = window_origin(fy0, r);
     const int rd = 2 * r + 1;
     const double* plane = vol + ((int64_t)n * HW1 + pix) * ((int64_t)h2 * w2);
     double* o = out + (int64_t)n * rd * rd * HW1 + pix;
@@ -128,6 +138,88 @@ __global__ void corr_index_fwd_kernel<double>(const double* __restrict__ vol, co
             if (inb(ya + 1, xa, h2, w2)) v += (1 - dx) * dy * plane[(int64_t)(ya + 1) * w2 + xa];
             if (inb(ya + 1, xa + 1, h2, w2)) v += dx * dy * plane[(int64_t)(ya + 1) * w2 + xa + 1];
             o[(int64_t)(i * rd + j) * HW1] = v;
+        }
+}
+
+// Radius-3 lookup with vector loads.  Each pixel reads its own plane, so the
+// lanes of a warp never share a row: instead of 196 scattered element loads,
+// each of the 8 window rows is read as the aligned 16-byte chunks covering
+// [bx, bx + 8) (two for 16-bit types, three for f32) and shifted into place in
+// registers.  Needs rows that are a whole number of 16-byte chunks (w2 * size
+// a multiple of 16) and a 16-byte aligned volume; a chunk is then either inside
+// the row or entirely outside it, and outside chunks read as zeros.
+template <typename T>
+__device__ __forceinline__ void window_row8(const T* __restrict__ plane, int h2, int w2, int y, int x0, float* t) {
+    const bool rowok = y >= 0 && y < h2;
+    const T* rp = plane + (int64_t)(rowok ? y : 0) * w2;
+    if constexpr (sizeof(T) == 2) {
+        const int o = x0 & 7, a = x0 - o;  // floor to a multiple of 8 elements (also for x0 < 0)
+        uint4 c0 = make_uint4(0, 0, 0, 0), c1 = c0;
+        if (rowok && a >= 0 && a < w2) c0 = __ldg(reinterpret_cast<const uint4*>(rp + a));
+        if (rowok && a + 8 >= 0 && a + 8 < w2) c1 = __ldg(reinterpret_cast<const uint4*>(rp + a + 8));
+        const uint32_t w[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+        uint32_t wa[6], wb[5];
+#pragma unroll
+        for (int k = 0; k < 6; k++) wa[k] = (o & 4) ? w[k + 2] : w[k];  // shift by 2 words
+#pragma unroll
+        for (int k = 0; k < 5; k++) wb[k] = (o & 2) ? wa[k + 1] : wa[k];  // by 1 word
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            // word k holds elements o + 2k (low half) and o + 2k + 1 (high half)
+            const uint32_t v = (o & 1) ? __funnelshift_r(wb[k], wb[k + 1], 16) : wb[k];
+            const T* e = reinterpret_cast<const T*>(&v);
+            t[2 * k] = to_f(e[0]);
+            t[2 * k + 1] = to_f(e[1]);
+        }
+    } else {
+        const int o = x0 & 3, a = x0 - o;
+        float4 c[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            c[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+            const int s = a + 4 * q;
+            if (rowok && s >= 0 && s < w2) c[q] = __ldg(reinterpret_cast<const float4*>(rp + s));
+        }
+        const float f[12] = {c[0].x, c[0].y, c[0].z, c[0].w, c[1].x, c[1].y,
+                             c[1].z, c[1].w, c[2].x, c[2].y, c[2].z, c[2].w};
+        float fa[10];
+#pragma unroll
+        for (int k = 0; k < 10; k++) fa[k] = (o & 2) ? f[k + 2] : f[k];
+#pragma unroll
+        for (int k = 0; k < 8; k++) t[k] = (o & 1) ? fa[k + 1] : fa[k];
+    }
+}
+
+template <typename T>
+__global__ void corr_index_fwd_r3_kernel(const T* __restrict__ vol, const float* __restrict__ coords,
+                                         T* __restrict__ out, int B, int h1, int w1, int h2, int w2) {
+    const int64_t HW1 = (int64_t)h1 * w1;
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= B * HW1) return;
+    const int n = (int)(idx / HW1);
+    const int64_t pix = idx % HW1;
+    const float x0 = coords[((int64_t)n * 2 + 0) * HW1 + pix];
+    const float y0 = coords[((int64_t)n * 2 + 1) * HW1 + pix];
+    const float fx0 = floorf(x0), fy0 = floorf(y0);
+    // far-away or non-finite coordinates read only zeros (and their weights are zeroed too,
+    // so the output is 0 rather than 0 * NaN)
+    const bool near = fabsf(x0) < 1e6f && fabsf(y0) < 1e6f;
+    const float dx = near ? x0 - fx0 : 0.f, dy = near ? y0 - fy0 : 0.f;
+    const int bx = near ? window_origin(fx0, 3) : -64, by = near ? window_origin(fy0, 3) : -64;
+    const T* plane = vol + ((int64_t)n * HW1 + pix) * ((int64_t)h2 * w2);
+    float t[8][8];  // [y offset][x offset]
+#pragma unroll
+    for (int j = 0; j < 8; j++) window_row8<T>(plane, h2, w2, by + j, bx, t[j]);
+    T* o = out + (int64_t)n * 49 * HW1 + pix;
+#pragma unroll
+    for (int i = 0; i < 7; i++)
+#pragma unroll
+        for (int j = 0; j < 7; j++) {
+            float v = (1 - dx) * (1 - dy) * t[j][i];
+            v += dx * (1 - dy) * t[j][i + 1];
+            v += (1 - dx) * dy * t[j + 1][i];
+            v += dx * dy * t[j + 1][i + 1];
+            o[(int64_t)(i * 7 + j) * HW1] = from_f<T>(v);
         }
 }
 
@@ -146,7 +238,7 @@ __global__ void corr_index_bwd_kernel(const float* __restrict__ coords, const T*
     const float y0 = coords[((int64_t)n * 2 + 1) * HW1 + pix];
     const float fx0 = floorf(x0), fy0 = floorf(y0);
     const A dx = (A)(x0 - fx0), dy = (A)(y0 - fy0);
-    const int bx = (int)fx0 - r, by = (int)fy0 - r;
+    const int bx = window_origin(fx0, r), by = window_origin(fy0, r);
     const int rd = 2 * r + 1;
     T* plane = vgrad + ((int64_t)n * HW1 + pix) * ((int64_t)h2 * w2);
     const T* go = g + (int64_t)n * rd * rd * HW1 + pix;
@@ -176,7 +268,7 @@ __global__ void corr_index_bwd_kernel<double>(const float* __restrict__ coords, 
     const float y0 = coords[((int64_t)n * 2 + 1) * HW1 + pix];
     const float fx0 = floorf(x0), fy0 = floorf(y0);
     const double dx = x0 - fx0, dy = y0 - fy0;
-    const int bx = (int)fx0 - r, by = (int)fy0 - r;
+    const int bx = window_origin(fx0, r), by = window_origin(fy0, r);
     const int rd = 2 * r + 1;
     double* plane = vgrad + ((int64_t)n * HW1 + pix) * ((int64_t)h2 * w2);
     const double* go = g + (int64_t)n * rd * rd * HW1 + pix;
@@ -223,7 +315,7 @@ __global__ void corr_index_coords_bwd_kernel(const T* __restrict__ vol, const fl
     const float y0 = coords[((int64_t)n * 2 + 1) * HW1 + pix];
     const float fx0 = floorf(x0), fy0 = floorf(y0);
     const A dx = (A)(x0 - fx0), dy = (A)(y0 - fy0);
-    const int bx = (int)fx0 - r, by = (int)fy0 - r;
+    const int bx = window_origin(fx0, r), by = window_origin(fy0, r);
     const int rd = 2 * r + 1;
     const T* plane = vol + ((int64_t)n * HW1 + pix) * ((int64_t)h2 * w2);
     const T* go = g + (int64_t)n * rd * rd * HW1 + pix;
@@ -280,7 +372,7 @@ __device__ __forceinline__ void window_dots(const T* __restrict__ fmap2, int H2,
     const int lane = threadIdx.x & 31;
     const int ne = 2 * r + 2;
     const int nt = ne * ne;
-    const int bx = (int)floorf(xc) - r, by = (int)floorf(yc) - r;
+    const int bx = window_origin(floorf(xc), r), by = window_origin(floorf(yc), r);
     t0 = 0;
     t1 = 0;
 #pragma unroll
@@ -444,7 +536,7 @@ __global__ void __launch_bounds__(kWarps * 32)
         const float* cp = coords + ((bs * H1 + h1) * W1 + w1) * 2;
         const float xc = cp[0], yc = cp[1];
         const float dx = xc - floorf(xc), dy = yc - floorf(yc);
-        const int bx = (int)floorf(xc) - r, by = (int)floorf(yc) - r;
+        const int bx = window_origin(floorf(xc), r), by = window_origin(floorf(yc), r);
         const float* gp = g + bs * rd * rd * HW1 + (int64_t)h1 * W1 + w1;
         float gt[2];
 #pragma unroll
@@ -568,7 +660,7 @@ __global__ void __launch_bounds__(kWarps * 32)
         const float scale = (float)(1 << l);
         const float xc = cp[0] / scale, yc = cp[1] / scale;
         const float dx = xc - floorf(xc), dy = yc - floorf(yc);
-        const int bx = (int)floorf(xc) - r, by = (int)floorf(yc) - r;
+        const int bx = window_origin(floorf(xc), r), by = window_origin(floorf(yc), r);
         const int H2 = lv.H2[l], W2 = lv.W2[l];
         const int64_t plane = ((int64_t)b * Nf + dst) * H2 * W2;
         const T* f2base = static_cast<const T*>(lv.p[l]) + plane * C;
@@ -704,6 +796,14 @@ extern "C" int vipe_corr_index_forward(int dtype, const void* volume, const floa
     return dispatch(dtype, [&](auto tag) {
         using T = decltype(tag);
         VIPE_PROF("corr_index_fwd", st);
+        if constexpr (!std::is_same<T, double>::value) {
+            if (radius == 3 && ((size_t)w2 * sizeof(T)) % 16 == 0 && (uintptr_t)volume % 16 == 0) {
+                corr_index_fwd_r3_kernel<T><<<ceil_div(n, 256), 256, 0, st>>>(
+                    static_cast<const T*>(volume), coords, static_cast<T*>(corr_out), B, h1, w1, h2, w2);
+                VIPE_LAUNCH_CHECK();
+                return (int)VIPE_OK;
+            }
+        }
         corr_index_fwd_kernel<T><<<ceil_div(n, 256), 256, 0, st>>>(static_cast<const T*>(volume), coords,
                                                                    static_cast<T*>(corr_out), B, h1, w1, h2, w2,
                                                                    radius);

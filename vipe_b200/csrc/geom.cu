@@ -159,7 +159,10 @@ __global__ void depth_filter_kernel(const float* __restrict__ poses, const float
     const float uj = fx * (Xj[0] / Xj[2]) + cx;
     const float vj = fy * (Xj[1] / Xj[2]) + cy;
     const float dj = Xj[3] / Xj[2];
-    const int u0 = (int)floorf(uj), v0 = (int)floorf(vj);
+    // clamp before the conversion: a projection at infinity or NaN (Xj[2] = 0) must not
+    // reach an out-of-range float -> int conversion, whose result the bounds test could not trust
+    const int u0 = (int)fminf(fmaxf(floorf(uj), -1.f), (float)wd);
+    const int v0 = (int)fminf(fmaxf(floorf(vj), -1.f), (float)ht);
     if (u0 >= 0 && v0 >= 0 && u0 < wd - 1 && v0 < ht - 1) {
         const float* dpj = disps + (size_t)jx * HW;
         const double idj = 1.0 / (double)dj;
