@@ -503,6 +503,122 @@ __global__ void __launch_bounds__(kWarps * 32)
     }
 }
 
+// Indexed lookup for 16-bit maps, radius 3, C in {64, 128, 256}, on the tensor cores
+// (warp-level mma.sync m16n8k16, FP32 accumulation): per (pixel, level) the 64
+// window taps are the M = 64 rows of A (four 16-row tiles, tap t = 8 ix + iy,
+// rows outside the map read as zeros) and the pixel's fmap1 row is every
+// column of B, so each lane ends with the dot products of the taps of its
+// row group (column redundancy instead of per-element half -> float
+// conversions).  Channels are permuted identically in A and B so that one
+// 16-byte load per row gives a lane its A (and B) elements of two
+// consecutive k-steps: k-step s, lane quad index q, element e in 0..3 reads
+// channel 32 (s / 2) + 8 q + 4 (s % 2) + e (a dot product is invariant to the
+// channel order).  Taps go through shared memory to the bilinear combination.
+template <typename T>
+__device__ __forceinline__ void mma_16816(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                          uint32_t b1) {
+    if constexpr (std::is_same<T, __half>::value) {
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+            "{%0, %1, %2, %3};"
+            : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+            : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+    } else {
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+            "{%0, %1, %2, %3};"
+            : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+            : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+    }
+}
+
+template <typename T, int NK>  // NK = C / 32
+__global__ void __launch_bounds__(kWarps * 32)
+    altcorr_index_fwd_mma_kernel(const T* __restrict__ fmap1, LevelPtrs lv, int L, const float* __restrict__ coords,
+                                 const int64_t* __restrict__ ii, const int64_t* __restrict__ jj,
+                                 float* __restrict__ out, int B, int Nf, int M, int H, int W) {
+    constexpr int C = 32 * NK;
+    __shared__ float os[kMaxL * 49][kTile];
+    __shared__ float tsm[kWarps][64];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane >> 2, quad = lane & 3;
+    const int bm = blockIdx.z, b = bm / M, m = bm % M;
+    const int h = blockIdx.y, w0 = blockIdx.x * kTile;
+    const int src = (int)ii[m], dst = (int)jj[m];
+    const int64_t HW = (int64_t)H * W;
+    const int nw = min(kTile, W - w0);
+    for (int pp = warp; pp < nw; pp += kWarps) {
+        const int w = w0 + pp;
+        const T* f1 = fmap1 + ((((int64_t)b * Nf + src) * H + h) * W + w) * C + 8 * quad;
+        uint4 bf[NK];  // 16-byte chunks of the pixel's fmap1 row held by this lane
+#pragma unroll
+        for (int t = 0; t < NK; t++) bf[t] = __ldg(reinterpret_cast<const uint4*>(f1 + 32 * t));
+        const float* cp = coords + (((int64_t)bm * H + h) * W + w) * 2;
+        for (int l = 0; l < L; l++) {
+            // coords / 2^l at level l (droid_net.py:78, altcorr_kernel.cu:182-183)
+            const float scale = (float)(1 << l);
+            const float xc = cp[0] / scale, yc = cp[1] / scale;
+            const int bx = window_origin(floorf(xc), 3), by = window_origin(floorf(yc), 3);
+            const int H2 = lv.H2[l], W2 = lv.W2[l];
+            const T* f2 = static_cast<const T*>(lv.p[l]) + ((int64_t)b * Nf + dst) * H2 * W2 * C + 8 * quad;
+            // this lane's two rows per 16-row tile: taps 16 mt + grp and 16 mt + grp + 8
+            int off[8];
+            bool ok[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const int tap = 16 * (q >> 1) + grp + 8 * (q & 1);
+                const int x2 = bx + (tap >> 3), y2 = by + (tap & 7);
+                ok[q] = inb(y2, x2, H2, W2);
+                off[q] = ok[q] ? (y2 * W2 + x2) * C : 0;
+            }
+            float acc[4][4];
+#pragma unroll
+            for (int mt = 0; mt < 4; mt++)
+#pragma unroll
+                for (int e = 0; e < 4; e++) acc[mt][e] = 0.f;
+#pragma unroll
+            for (int t = 0; t < NK; t++) {
+#pragma unroll
+                for (int mt = 0; mt < 4; mt++) {
+                    const uint4 z = make_uint4(0, 0, 0, 0);
+                    const uint4 r0 = ok[2 * mt] ? __ldg(reinterpret_cast<const uint4*>(f2 + off[2 * mt] + 32 * t)) : z;
+                    const uint4 r1 =
+                        ok[2 * mt + 1] ? __ldg(reinterpret_cast<const uint4*>(f2 + off[2 * mt + 1] + 32 * t)) : z;
+                    // k-step 2t: elements 0..3 of the chunk; k-step 2t + 1: elements 4..7
+                    mma_16816<T>(acc[mt], r0.x, r1.x, r0.y, r1.y, bf[t].x, bf[t].y);
+                    mma_16816<T>(acc[mt], r0.z, r1.z, r0.w, r1.w, bf[t].z, bf[t].w);
+                }
+            }
+            // every column of D holds the same dot products: lanes with quad 0 publish the taps
+            __syncwarp();
+            if (quad == 0)
+#pragma unroll
+                for (int mt = 0; mt < 4; mt++) {
+                    tsm[warp][16 * mt + grp] = acc[mt][0];
+                    tsm[warp][16 * mt + grp + 8] = acc[mt][2];
+                }
+            __syncwarp();
+            const float dx = xc - floorf(xc), dy = yc - floorf(yc);
+#pragma unroll
+            for (int hh = 0; hh < 2; hh++) {
+                const int ch = lane + 32 * hh;
+                if (ch < 49) {
+                    const int i = ch / 7, j = ch % 7;
+                    const float* tp = tsm[warp];
+                    const float v = (1.f - dx) * (1.f - dy) * tp[8 * i + j] + dx * (1.f - dy) * tp[8 * (i + 1) + j] +
+                                    (1.f - dx) * dy * tp[8 * i + j + 1] + dx * dy * tp[8 * (i + 1) + j + 1];
+                    os[l * 49 + ch][pp] = v;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < L * 49 * kTile; q += blockDim.x) {
+        const int ch = q / kTile, pp = q % kTile;
+        if (pp < nw) out[((int64_t)bm * L * 49 + ch) * HW + (int64_t)h * W + w0 + pp] = os[ch][pp];
+    }
+}
+
 // altcorr_backward (f32): fmap1_grad (B,H1,W1,C) and fmap2_grad (B,H2,W2,C) must
 // be zero on entry.  Per (pixel, sample) warp: tap gradients from the bilinear
 // adjoint; fmap1_grad gathered per pixel (owned by the warp across samples);
@@ -907,9 +1023,27 @@ extern "C" int vipe_altcorr_index_forward(int dtype, const void* fmap1, const vo
     }
     cudaStream_t st = as_stream(stream);
     dim3 grid(ceil_div(W, kTile), H, B * M);
+    bool aligned16 = (uintptr_t)fmap1 % 16 == 0;
+    for (int l = 0; l < num_levels; l++) aligned16 = aligned16 && (uintptr_t)fmap2_levels[l] % 16 == 0;
     return dispatch(dtype, [&](auto tag) {
         using T = decltype(tag);
         VIPE_PROF("altcorr_index_fwd", st);
+        if constexpr (sizeof(T) == 2) {
+            if (radius == 3 && (C == 64 || C == 128 || C == 256) && aligned16) {
+                const T* f1 = static_cast<const T*>(fmap1);
+                if (C == 64)
+                    altcorr_index_fwd_mma_kernel<T, 2><<<grid, kWarps * 32, 0, st>>>(f1, lv, num_levels, coords, ii,
+                                                                                     jj, corr_out, B, Nf, M, H, W);
+                else if (C == 128)
+                    altcorr_index_fwd_mma_kernel<T, 4><<<grid, kWarps * 32, 0, st>>>(f1, lv, num_levels, coords, ii,
+                                                                                     jj, corr_out, B, Nf, M, H, W);
+                else
+                    altcorr_index_fwd_mma_kernel<T, 8><<<grid, kWarps * 32, 0, st>>>(f1, lv, num_levels, coords, ii,
+                                                                                     jj, corr_out, B, Nf, M, H, W);
+                VIPE_LAUNCH_CHECK();
+                return (int)VIPE_OK;
+            }
+        }
         altcorr_index_fwd_kernel<T><<<grid, kWarps * 32, 0, st>>>(static_cast<const T*>(fmap1), lv, num_levels,
                                                                    coords, ii, jj, corr_out, B, Nf, M, H, W, C,
                                                                    radius);
