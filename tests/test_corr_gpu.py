@@ -298,3 +298,27 @@ def test_altcorrblock_indexed_gradients_match_per_level_route():
     (a1, ac), (b1, bc) = grads
     torch.testing.assert_close(a1, b1, atol=1e-4, rtol=1e-4)
     torch.testing.assert_close(ac, bc, atol=1e-4, rtol=1e-4)
+
+
+@pytest.mark.parametrize("dtype,C,sigma,W", [(torch.float16, 128, 0.4, 64), (torch.bfloat16, 64, 6.0, 20),
+                                             (torch.float16, 256, 1.0, 13), (torch.float32, 32, 1.0, 16)])
+def test_altcorr_index_forward_paths(dtype, C, sigma, W):
+    """Indexed lookup vs the FP64 oracle: 16-bit maps with C in {64, 128, 256} take the tensor-core
+    union-box kernel (smooth coordinates: one box per 8 pixels; sigma = 6 px: boxes too large, one
+    pass per pixel; W not a multiple of 8: partial warps); f32 maps the element kernel."""
+    g = torch.Generator().manual_seed(21)
+    B, Nf, H, M = 1, 4, 8, 3
+    f = (torch.randn(B, Nf, H, W, C, generator=g) / C**0.5).to(dtype)
+    levels = [f]
+    for _ in range(3):
+        t = levels[-1].float().permute(0, 1, 4, 2, 3).reshape(B * Nf, C, levels[-1].shape[2], levels[-1].shape[3])
+        t = torch.nn.functional.avg_pool2d(t, 2, stride=2)
+        levels.append(t.reshape(B, Nf, C, t.shape[-2], t.shape[-1]).permute(0, 1, 3, 4, 2).contiguous().to(dtype))
+    ii, jj = torch.tensor([0, 1, 3]), torch.tensor([1, 2, 1])
+    coords = _grid_coords(B * M, H, W, g, sigma).reshape(B, M, 2, H, W).permute(0, 1, 3, 4, 2).contiguous()
+    coords[0, 0, 0, 0] = torch.tensor([1e9, -1e9])  # far away: zeros, and the box falls back to per-pixel passes
+    out = _dne().altcorr_index_forward(f.cuda(), [lv.cuda() for lv in levels], coords.cuda(), ii.cuda(), jj.cuda(),
+                                       3)[0]
+    want = oc.altcorr_index_forward(f.double().numpy(), [lv.double().numpy() for lv in levels], coords.numpy(),
+                                    ii.numpy(), jj.numpy(), 3)
+    np.testing.assert_allclose(out.double().cpu().numpy(), want, atol=1e-4)

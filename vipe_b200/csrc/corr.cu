@@ -30,6 +30,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <climits>
 #include <type_traits>
 
 namespace vipe {
@@ -503,17 +504,21 @@ __global__ void __launch_bounds__(kWarps * 32)
     }
 }
 
-// Indexed lookup for 16-bit maps, radius 3, C in {64, 128, 256}, on the tensor cores
-// (warp-level mma.sync m16n8k16, FP32 accumulation): per (pixel, level) the 64
-// window taps are the M = 64 rows of A (four 16-row tiles, tap t = 8 ix + iy,
-// rows outside the map read as zeros) and the pixel's fmap1 row is every
-// column of B, so each lane ends with the dot products of the taps of its
-// row group (column redundancy instead of per-element half -> float
-// conversions).  Channels are permuted identically in A and B so that one
-// 16-byte load per row gives a lane its A (and B) elements of two
-// consecutive k-steps: k-step s, lane quad index q, element e in 0..3 reads
-// channel 32 (s / 2) + 8 q + 4 (s % 2) + e (a dot product is invariant to the
-// channel order).  Taps go through shared memory to the bilinear combination.
+// Indexed lookup for 16-bit maps, radius 3, C in {64, 128, 256}, on the tensor
+// cores (warp-level mma.sync m16n8k16, FP32 accumulation).  A warp owns 8
+// consecutive pixels of one row (the 8 columns of B: each pixel's fmap1 row)
+// and, per level, the union box of their 8x8 windows: the box taps are the M
+// rows of A (16-row tiles, row r = tap (X0 + r % bw, Y0 + r / bw), rows
+// outside the map read as zeros), so D holds the dot product of every box tap
+// with every pixel, and each pixel's window is a sub-box of D.  For smooth
+// coordinates the windows of neighbouring pixels overlap and the box holds far
+// fewer taps than 8 x 64 (about 200 at level 0, 90 at level 3); a box above
+// kMaxBox taps falls back to one pass per pixel over its own window.
+// Channels are permuted identically in A and B so that one 16-byte load per
+// row gives a lane its elements of two consecutive k-steps: k-step s, lane quad
+// index q, element e in 0..3 reads channel 32 (s / 2) + 8 q + 4 (s % 2) + e (a
+// dot product is invariant to the channel order).  D goes through shared
+// memory to the bilinear combination; outputs leave as 32-byte row segments.
 template <typename T>
 __device__ __forceinline__ void mma_16816(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
                                           uint32_t b1) {
@@ -532,90 +537,121 @@ __device__ __forceinline__ void mma_16816(float* d, uint32_t a0, uint32_t a1, ui
     }
 }
 
+constexpr int kUnionTile = 64;  // pixels per CTA (8 per warp)
+constexpr int kMaxBox = 384;    // union taps per warp pass (24 row tiles)
+constexpr size_t kUnionSmem = (size_t)kWarps * kMaxBox * 8 * sizeof(float);
+
 template <typename T, int NK>  // NK = C / 32
-__global__ void __launch_bounds__(kWarps * 32)
+__global__ void __launch_bounds__(kWarps * 32, 2)
     altcorr_index_fwd_mma_kernel(const T* __restrict__ fmap1, LevelPtrs lv, int L, const float* __restrict__ coords,
                                  const int64_t* __restrict__ ii, const int64_t* __restrict__ jj,
                                  float* __restrict__ out, int B, int Nf, int M, int H, int W) {
     constexpr int C = 32 * NK;
-    __shared__ float os[kMaxL * 49][kTile];
-    __shared__ float tsm[kWarps][64];
+    constexpr unsigned kFull = 0xffffffffu;
+    extern __shared__ float dsm_all[];  // [kWarps][kMaxBox][8]: D of the current box pass
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grp = lane >> 2, quad = lane & 3;
+    float* Dsm = dsm_all + (size_t)warp * kMaxBox * 8;
     const int bm = blockIdx.z, b = bm / M, m = bm % M;
-    const int h = blockIdx.y, w0 = blockIdx.x * kTile;
+    const int h = blockIdx.y;
+    const int wbase = blockIdx.x * kUnionTile + 8 * warp;  // the warp's first pixel
+    if (wbase >= W) return;                                // whole warp (no block-level barrier below)
     const int src = (int)ii[m], dst = (int)jj[m];
     const int64_t HW = (int64_t)H * W;
-    const int nw = min(kTile, W - w0);
-    for (int pp = warp; pp < nw; pp += kWarps) {
-        const int w = w0 + pp;
-        const T* f1 = fmap1 + ((((int64_t)b * Nf + src) * H + h) * W + w) * C + 8 * quad;
-        uint4 bf[NK];  // 16-byte chunks of the pixel's fmap1 row held by this lane
+    // B column grp: pixel wbase + grp (zeros past the row end)
+    const int pg = wbase + grp;
+    const bool gvalid = pg < W;
+    uint4 bf[NK];
+    const T* f1 = fmap1 + ((((int64_t)b * Nf + src) * H + h) * W + (gvalid ? pg : wbase)) * C + 8 * quad;
 #pragma unroll
-        for (int t = 0; t < NK; t++) bf[t] = __ldg(reinterpret_cast<const uint4*>(f1 + 32 * t));
-        const float* cp = coords + (((int64_t)bm * H + h) * W + w) * 2;
-        for (int l = 0; l < L; l++) {
-            // coords / 2^l at level l (droid_net.py:78, altcorr_kernel.cu:182-183)
-            const float scale = (float)(1 << l);
-            const float xc = cp[0] / scale, yc = cp[1] / scale;
-            const int bx = window_origin(floorf(xc), 3), by = window_origin(floorf(yc), 3);
-            const int H2 = lv.H2[l], W2 = lv.W2[l];
-            const T* f2 = static_cast<const T*>(lv.p[l]) + ((int64_t)b * Nf + dst) * H2 * W2 * C + 8 * quad;
-            // this lane's two rows per 16-row tile: taps 16 mt + grp and 16 mt + grp + 8
-            int off[8];
-            bool ok[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                const int tap = 16 * (q >> 1) + grp + 8 * (q & 1);
-                const int x2 = bx + (tap >> 3), y2 = by + (tap & 7);
-                ok[q] = inb(y2, x2, H2, W2);
-                off[q] = ok[q] ? (y2 * W2 + x2) * C : 0;
-            }
-            float acc[4][4];
-#pragma unroll
-            for (int mt = 0; mt < 4; mt++)
-#pragma unroll
-                for (int e = 0; e < 4; e++) acc[mt][e] = 0.f;
-#pragma unroll
-            for (int t = 0; t < NK; t++) {
-#pragma unroll
-                for (int mt = 0; mt < 4; mt++) {
-                    const uint4 z = make_uint4(0, 0, 0, 0);
-                    const uint4 r0 = ok[2 * mt] ? __ldg(reinterpret_cast<const uint4*>(f2 + off[2 * mt] + 32 * t)) : z;
-                    const uint4 r1 =
-                        ok[2 * mt + 1] ? __ldg(reinterpret_cast<const uint4*>(f2 + off[2 * mt + 1] + 32 * t)) : z;
-                    // k-step 2t: elements 0..3 of the chunk; k-step 2t + 1: elements 4..7
-                    mma_16816<T>(acc[mt], r0.x, r1.x, r0.y, r1.y, bf[t].x, bf[t].y);
-                    mma_16816<T>(acc[mt], r0.z, r1.z, r0.w, r1.w, bf[t].z, bf[t].w);
-                }
-            }
-            // every column of D holds the same dot products: lanes with quad 0 publish the taps
-            __syncwarp();
-            if (quad == 0)
-#pragma unroll
-                for (int mt = 0; mt < 4; mt++) {
-                    tsm[warp][16 * mt + grp] = acc[mt][0];
-                    tsm[warp][16 * mt + grp + 8] = acc[mt][2];
-                }
-            __syncwarp();
-            const float dx = xc - floorf(xc), dy = yc - floorf(yc);
-#pragma unroll
-            for (int hh = 0; hh < 2; hh++) {
-                const int ch = lane + 32 * hh;
-                if (ch < 49) {
-                    const int i = ch / 7, j = ch % 7;
-                    const float* tp = tsm[warp];
-                    const float v = (1.f - dx) * (1.f - dy) * tp[8 * i + j] + dx * (1.f - dy) * tp[8 * (i + 1) + j] +
-                                    (1.f - dx) * dy * tp[8 * i + j + 1] + dx * dy * tp[8 * (i + 1) + j + 1];
-                    os[l * 49 + ch][pp] = v;
-                }
-            }
-        }
+    for (int t = 0; t < NK; t++)
+        bf[t] = gvalid ? __ldg(reinterpret_cast<const uint4*>(f1 + 32 * t)) : make_uint4(0, 0, 0, 0);
+    float xc = 0.f, yc = 0.f;
+    if (gvalid) {
+        const float* cp = coords + (((int64_t)bm * H + h) * W + pg) * 2;
+        xc = cp[0];
+        yc = cp[1];
     }
-    __syncthreads();
-    for (int q = threadIdx.x; q < L * 49 * kTile; q += blockDim.x) {
-        const int ch = q / kTile, pp = q % kTile;
-        if (pp < nw) out[((int64_t)bm * L * 49 + ch) * HW + (int64_t)h * W + w0 + pp] = os[ch][pp];
+    // the pixel this lane writes outputs for (fixed: lane + 32 k has the same low 3 bits)
+    const int n = lane & 7;
+    const bool nvalid = wbase + n < W;
+    for (int l = 0; l < L; l++) {
+        // coords / 2^l at level l (droid_net.py:78, altcorr_kernel.cu:182-183)
+        const float scale = (float)(1 << l);
+        const float xl = xc / scale, yl = yc / scale;
+        const int bx = window_origin(floorf(xl), 3), by = window_origin(floorf(yl), 3);
+        const int H2 = lv.H2[l], W2 = lv.W2[l];
+        const T* f2 = static_cast<const T*>(lv.p[l]) + ((int64_t)b * Nf + dst) * H2 * W2 * C + 8 * quad;
+        const int bxn = __shfl_sync(kFull, bx, 4 * n), byn = __shfl_sync(kFull, by, 4 * n);
+        const float xln = __shfl_sync(kFull, xl, 4 * n), yln = __shfl_sync(kFull, yl, 4 * n);
+        const float dxn = xln - floorf(xln), dyn = yln - floorf(yln);
+        const int X0 = __reduce_min_sync(kFull, gvalid ? bx : INT_MAX);
+        const int X1 = __reduce_max_sync(kFull, gvalid ? bx : INT_MIN) + 7;
+        const int Y0 = __reduce_min_sync(kFull, gvalid ? by : INT_MAX);
+        const int Y1 = __reduce_max_sync(kFull, gvalid ? by : INT_MIN) + 7;
+        // window origins are clamped to +-2^24, so the extents fit an int and their product an int64
+        const bool joint = (int64_t)(X1 - X0 + 1) * (Y1 - Y0 + 1) <= kMaxBox;
+        const int npass = joint ? 1 : 8;
+        for (int pass = 0; pass < npass; pass++) {
+            const int sx = __shfl_sync(kFull, bx, 4 * pass), sy = __shfl_sync(kFull, by, 4 * pass);
+            if (!joint && wbase + pass >= W) break;  // warp-uniform
+            const int bx0 = joint ? X0 : sx, by0 = joint ? Y0 : sy;
+            const int bw = joint ? X1 - X0 + 1 : 8, bh = joint ? Y1 - Y0 + 1 : 8;
+            const unsigned mask = joint ? 0xffu : 1u << pass;
+            const int nbox = bw * bh;
+            const int ntile = (nbox + 15) >> 4;
+            for (int mt = 0; mt < ntile; mt += 2) {  // two row tiles per step (rows past nbox are zeros)
+                int off[4];
+                bool ok[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int r = 16 * (mt + (q >> 1)) + grp + 8 * (q & 1);
+                    const int x = bx0 + r % bw, y = by0 + r / bw;
+                    ok[q] = r < nbox && inb(y, x, H2, W2);
+                    off[q] = ok[q] ? (y * W2 + x) * C : 0;
+                }
+                float acc[2][4];
+#pragma unroll
+                for (int tt = 0; tt < 2; tt++)
+#pragma unroll
+                    for (int e = 0; e < 4; e++) acc[tt][e] = 0.f;
+#pragma unroll
+                for (int t = 0; t < NK; t++) {
+                    uint4 rows[4];
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        rows[q] = ok[q] ? __ldg(reinterpret_cast<const uint4*>(f2 + off[q] + 32 * t))
+                                        : make_uint4(0, 0, 0, 0);
+#pragma unroll
+                    for (int tt = 0; tt < 2; tt++) {
+                        const uint4 r0 = rows[2 * tt], r1 = rows[2 * tt + 1];
+                        // k-step 2t: elements 0..3 of the chunk; k-step 2t + 1: elements 4..7
+                        mma_16816<T>(acc[tt], r0.x, r1.x, r0.y, r1.y, bf[t].x, bf[t].y);
+                        mma_16816<T>(acc[tt], r0.z, r1.z, r0.w, r1.w, bf[t].z, bf[t].w);
+                    }
+                }
+#pragma unroll
+                for (int tt = 0; tt < 2; tt++) {
+                    const int row = 16 * (mt + tt) + grp;
+                    *reinterpret_cast<float2*>(Dsm + row * 8 + 2 * quad) = make_float2(acc[tt][0], acc[tt][1]);
+                    *reinterpret_cast<float2*>(Dsm + (row + 8) * 8 + 2 * quad) = make_float2(acc[tt][2], acc[tt][3]);
+                }
+            }
+            __syncwarp();
+            if (((mask >> n) & 1u) && nvalid) {
+                const int px = bxn - bx0, py = byn - by0;  // the pixel's window inside the box
+                const float* col = Dsm + n;
+                for (int o = lane; o < 49 * 8; o += 32) {
+                    const int ch = o >> 3;
+                    const int i = ch / 7, j = ch % 7;
+                    const int r = (py + j) * bw + px + i;
+                    const float v = (1.f - dxn) * (1.f - dyn) * col[r * 8] + dxn * (1.f - dyn) * col[(r + 1) * 8] +
+                                    (1.f - dxn) * dyn * col[(r + bw) * 8] + dxn * dyn * col[(r + bw + 1) * 8];
+                    out[((int64_t)bm * L * 49 + l * 49 + ch) * HW + (int64_t)h * W + wbase + n] = v;
+                }
+            }
+            __syncwarp();
+        }
     }
 }
 
@@ -1031,17 +1067,18 @@ extern "C" int vipe_altcorr_index_forward(int dtype, const void* fmap1, const vo
         if constexpr (sizeof(T) == 2) {
             if (radius == 3 && (C == 64 || C == 128 || C == 256) && aligned16) {
                 const T* f1 = static_cast<const T*>(fmap1);
-                if (C == 64)
-                    altcorr_index_fwd_mma_kernel<T, 2><<<grid, kWarps * 32, 0, st>>>(f1, lv, num_levels, coords, ii,
-                                                                                     jj, corr_out, B, Nf, M, H, W);
-                else if (C == 128)
-                    altcorr_index_fwd_mma_kernel<T, 4><<<grid, kWarps * 32, 0, st>>>(f1, lv, num_levels, coords, ii,
-                                                                                     jj, corr_out, B, Nf, M, H, W);
-                else
-                    altcorr_index_fwd_mma_kernel<T, 8><<<grid, kWarps * 32, 0, st>>>(f1, lv, num_levels, coords, ii,
-                                                                                     jj, corr_out, B, Nf, M, H, W);
-                VIPE_LAUNCH_CHECK();
-                return (int)VIPE_OK;
+                const dim3 ug(ceil_div(W, kUnionTile), H, B * M);
+                auto go = [&](auto kern) -> int {
+                    VIPE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)kUnionSmem));
+                    kern<<<ug, kWarps * 32, kUnionSmem, st>>>(f1, lv, num_levels, coords, ii, jj, corr_out, B, Nf, M,
+                                                             H, W);
+                    VIPE_LAUNCH_CHECK();
+                    return (int)VIPE_OK;
+                };
+                if (C == 64) return go(altcorr_index_fwd_mma_kernel<T, 2>);
+                if (C == 128) return go(altcorr_index_fwd_mma_kernel<T, 4>);
+                return go(altcorr_index_fwd_mma_kernel<T, 8>);
             }
         }
         altcorr_index_fwd_kernel<T><<<grid, kWarps * 32, 0, st>>>(static_cast<const T*>(fmap1), lv, num_levels,
