@@ -63,6 +63,12 @@ const char* vipe_last_error(void);
 void vipe_profile_enable(int on);
 int vipe_profile_collect(char* names, int name_stride, float* total_ms, int* launches, int max_kernels);
 
+/* HBM write-bandwidth probe (no counterpart in the reference; a measurement
+ * helper for write-bound kernels' rooflines): writes `bytes` (a multiple of 16,
+ * 16-byte aligned `dst`) with 16-byte stores, one per thread, over a grid that
+ * covers the buffer once.  Time it with events on `stream`. */
+int vipe_hbm_write_probe(void* dst, size_t bytes, void* stream);
+
 /* =====================================================================
  * slam_ext — dense bundle adjustment and geometry helpers
  * ===================================================================== */

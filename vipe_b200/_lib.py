@@ -67,6 +67,7 @@ _SIGS: dict[str, tuple] = {
     "vipe_altcorr_index_forward": (I, [I, P, P, P, P, I, P, P, P, I, I, I, I, I, I, I, P, P]),
     "vipe_altcorr_index_backward": (I, [I, P, P, P, P, I, P, P, P, P, I, I, I, I, I, I, I, I, P, P, P, P]),
     "vipe_corr_volume_workspace_size": (SZ, [I, I, I, I]),
+    "vipe_hbm_write_probe": (I, [P, SZ, P]),
     "vipe_corr_volume_build": (I, [I, I, P, P, I, I, I, I, I, P, P, SZ, P]),
 }
 for _op in ("expm", "logm", "inv", "as_matrix", "projector"):

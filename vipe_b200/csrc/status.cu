@@ -111,3 +111,30 @@ extern "C" __attribute__((visibility("default"))) const char* vipe_status_string
         default: return "unknown status";
     }
 }
+
+// ---------------------------------------------------------------- write-bandwidth probe
+namespace vipe {
+namespace {
+__global__ void write_probe_kernel(uint4* __restrict__ p, size_t n) {
+    // four 16-byte stores per thread, consecutive threads on consecutive addresses
+    const size_t base = blockIdx.x * (size_t)blockDim.x * 4 + threadIdx.x;
+    const uint4 v = make_uint4(0x3c003c00u, 0x3c003c00u, 0x3c003c00u, 0x3c003c00u);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const size_t i = base + (size_t)k * blockDim.x;
+        if (i < n) p[i] = v;
+    }
+}
+}  // namespace
+}  // namespace vipe
+
+extern "C" __attribute__((visibility("default"))) int vipe_hbm_write_probe(void* dst, size_t bytes, void* stream) {
+    if (!dst || bytes % 16 != 0 || (uintptr_t)dst % 16 != 0) return VIPE_ERR_ARG;
+    const size_t n = bytes / 16;
+    if (n == 0) return VIPE_OK;
+    const size_t blocks = (n + 1023) / 1024;
+    if (blocks > 0x7fffffffull) return VIPE_ERR_CAPACITY;
+    vipe::write_probe_kernel<<<(unsigned)blocks, 256, 0, vipe::as_stream(stream)>>>(static_cast<uint4*>(dst), n);
+    VIPE_LAUNCH_CHECK();
+    return VIPE_OK;
+}
