@@ -536,11 +536,15 @@ __global__ void __launch_bounds__(256) pool_level_kernel(const T* __restrict__ i
 // permute: target-block pixel order (8 x TW blocks) for the B operand.  One
 // CTA transposes a 64-channel x 128-pixel tile through shared memory with
 // 16-byte global loads (along pixels) and 16-byte stores (along channels).
+// The tile is held pixel-major (128 rows of 64 channels = 128 B); the 16-byte
+// channel chunk c8 of pixel row p sits at chunk c8 ^ ((p >> 3) & 7), so the
+// 2-byte stores of 16 lanes with pixels 8 apart spread over 8 bank groups and a
+// pixel row's eight chunks are read conflict-free as one 16-byte load each.
 template <typename TIn, typename TOp>
 __global__ void __launch_bounds__(256) pack_kernel(const TIn* __restrict__ f, TOp* __restrict__ out, int C, int Kp,
                                                    int H, int W, int TW, int permute) {
-    constexpr int kPx = 128, kCh = 64, LDT = kPx + 8;  // 16-bit tile rows padded by 16 bytes
-    __shared__ __align__(16) TOp tile[kCh][LDT];
+    constexpr int kPx = 128, kCh = 64;
+    __shared__ __align__(16) TOp tile[kPx][kCh];
     const int e = blockIdx.z;
     const int HW = H * W;
     const int p0 = blockIdx.x * kPx;
@@ -563,12 +567,15 @@ __global__ void __launch_bounds__(256) pack_kernel(const TIn* __restrict__ f, TO
                 v[k] = (c < C && px + k < HW) ? static_cast<float>(src[(size_t)c * HW + px + k]) : 0.f;
         }
 #pragma unroll
-        for (int k = 0; k < V; k++) tile[cc][pv + k] = static_cast<TOp>(v[k] * 0.25f);
+        for (int k = 0; k < V; k++) {
+            const int pp = pv + k;
+            tile[pp][(((cc >> 3) ^ ((pp >> 3) & 7)) << 3) | (cc & 7)] = static_cast<TOp>(v[k] * 0.25f);
+        }
     }
     __syncthreads();
     // each thread writes 8 consecutive channels (16 bytes) of one pixel
     for (int i = threadIdx.x; i < kPx * (kCh / 8); i += blockDim.x) {
-        const int pp = i / (kCh / 8), cg = (i % (kCh / 8)) * 8;
+        const int pp = i / (kCh / 8), c8 = i % (kCh / 8), cg = c8 * 8;
         const int px = p0 + pp;
         if (px >= HW || c0 + cg >= Kp) continue;
         int row = px;
@@ -577,10 +584,8 @@ __global__ void __launch_bounds__(256) pack_kernel(const TIn* __restrict__ f, TO
             const int hb = h / kTH, r = h % kTH, wb = w / TW, c = w % TW;
             row = ((hb * (W / TW) + wb) * kTH + r) * TW + c;
         }
-        __align__(16) TOp o[8];
-#pragma unroll
-        for (int k = 0; k < 8; k++) o[k] = tile[cg + k][pp];
-        *reinterpret_cast<uint4*>(out + ((size_t)e * HW + row) * Kp + c0 + cg) = *reinterpret_cast<const uint4*>(o);
+        *reinterpret_cast<uint4*>(out + ((size_t)e * HW + row) * Kp + c0 + cg) =
+            *reinterpret_cast<const uint4*>(&tile[pp][(c8 ^ ((pp >> 3) & 7)) << 3]);
     }
 }
 
