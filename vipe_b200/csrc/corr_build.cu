@@ -272,7 +272,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int N = p.N;
     auto sa = [&](int kc) { return sbase + (size_t)kc * kBM * 128; };
     auto sb = [&](int st, int kc) { return sbase + a_region(KC) + ((size_t)st * KC + kc) * b_box(N); };
-    const int NBS = 1;  // one B stage: the MMA + load of tile t+1 hide under the epilogue of tile t
+    // One B stage, filled and drained per 64-channel box: box kc of tile t+1 loads as soon as
+    // the MMAs of box kc of tile t have read it, so loads overlap the other box's MMAs; the
+    // MMA of tile t+1 overlaps the epilogue of tile t through the two TMEM accumulators.
+    const int NBS = 1;
     const size_t stage_off = a_region(KC) + (size_t)NBS * KC * b_box(N);
 
     if (tid == 0) {
@@ -297,33 +300,36 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t tmem = tmem_base;
 
     const uint32_t a_bytes = (uint32_t)kBM * 128u * KC;
-    const uint32_t b_bytes = (uint32_t)N * 128u * KC;
+    const uint32_t box_bytes = (uint32_t)N * 128u;  // one 64-channel box of a B tile
 
     if (warp == kTmaWarp && lane == 0) {
         // ------------------------------------------------ TMA producer
         uint32_t t = 0, it = 0;
+        uint32_t issued[kMaxKC] = {0, 0};  // B box loads issued per box slot
         for (long item = blockIdx.x; item < p.items && !fail; item += gridDim.x, it++) {
             const int e = (int)(item / p.mtiles), mt = (int)(item % p.mtiles);
             if (it > 0 && !mbar_wait(&barA_empty, (it - 1) & 1, &fail)) break;
             mbar_expect_tx(&barA_full, a_bytes);
             for (int kc = 0; kc < KC; kc++)
                 tma_load_2d(sa(kc), &mapA, &barA_full, kc * kKC, e * p.HW + mt * kBM);
-            for (int nt = 0; nt < p.ntiles; nt++, t++) {
-                const int s = (int)(t % NBS);
-                const uint32_t use = t / NBS;
-                if (use >= 1 && !mbar_wait(&barB_empty[s], (use - 1) & 1, &fail)) break;
-                mbar_expect_tx(&barB_full[s], b_bytes);
-                for (int kc = 0; kc < KC; kc++)
-                    tma_load_2d(sb(s, kc), &mapB, &barB_full[s], kc * kKC, e * p.HW + nt * N);
+            for (int nt = 0; nt < p.ntiles && !fail; nt++, t++) {
+                // box kc of this tile (barB_full/empty[kc]: one phase per tile)
+                for (int kc = 0; kc < KC; kc++) {
+                    if (t >= 1 && !mbar_wait(&barB_empty[kc], (t - 1) & 1, &fail)) break;
+                    mbar_expect_tx(&barB_full[kc], box_bytes);
+                    tma_load_2d(sb(0, kc), &mapB, &barB_full[kc], kc * kKC, e * p.HW + nt * N);
+                    issued[kc]++;
+                }
             }
         }
-        // drain: the last loads issued must land before the CTA exits
-        if (fail && t > 0) {
-            // bounded; returns at once if the last stage already completed
-            const uint32_t last = t - 1;
+        // drain: the last loads issued must land before the CTA exits (bounded; returns at
+        // once for a box whose last load already completed)
+        if (fail) {
             const uint64_t t0 = gtimer();
-            while (!mbar_try_wait(&barB_full[last % NBS], (last / NBS) & 1) && gtimer() - t0 < kWaitNs) {
-            }
+            for (int kc = 0; kc < KC; kc++)
+                if (issued[kc] > 0)
+                    while (!mbar_try_wait(&barB_full[kc], (issued[kc] - 1) & 1) && gtimer() - t0 < kWaitNs) {
+                    }
         }
     } else if (warp == kMmaWarp && lane == 0) {
         // ------------------------------------------------ MMA issuer
@@ -332,22 +338,27 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (long item = blockIdx.x; item < p.items && !fail; item += gridDim.x, it++) {
             if (!mbar_wait(&barA_full, it & 1, &fail)) break;
             tc_fence_after();
-            for (int nt = 0; nt < p.ntiles; nt++, t++) {
-                const int s = (int)(t % NBS), acc = t & 1;
-                if (!mbar_wait(&barB_full[s], (t / NBS) & 1, &fail)) break;
+            for (int nt = 0; nt < p.ntiles && !fail; nt++, t++) {
+                const int acc = t & 1;
                 if (t >= 2 && !mbar_wait(&barAcc_empty[acc], ((t >> 1) - 1) & 1, &fail)) break;
-                tc_fence_after();
                 const uint32_t d = tmem + (uint32_t)(acc * 256);
+                bool ok = true;
                 for (int kc = 0; kc < KC; kc++) {
+                    if (!mbar_wait(&barB_full[kc], t & 1, &fail)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
                     const uint64_t da = smem_desc_sw128(sa(kc));
-                    const uint64_t db = smem_desc_sw128(sb(s, kc));
+                    const uint64_t db = smem_desc_sw128(sb(0, kc));
 #pragma unroll
                     for (int k = 0; k < kKC / 16; k++) {
                         // advance 16 channels = 32 bytes inside the swizzled row
                         mma_f16(d, da + (uint64_t)(k * 2), db + (uint64_t)(k * 2), idesc, (kc | k) ? 1u : 0u);
                     }
+                    mma_commit(&barB_empty[kc]);  // box kc of this tile is read once these MMAs complete
                 }
-                mma_commit(&barB_empty[s]);
+                if (!ok) break;
                 mma_commit(&barAcc_full[acc]);
             }
             mma_commit(&barA_empty);
