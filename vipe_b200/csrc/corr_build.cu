@@ -52,6 +52,7 @@ constexpr int kThreads = 320;  // 8 epilogue warps, 1 TMA warp, 1 MMA warp
 constexpr int kEpiWarps = 8;
 constexpr int kTmaWarp = 8, kMmaWarp = 9;
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s bound on any mbarrier wait
+constexpr int kTmaStage = 12288;  // per-warp staging of the TMA-store epilogue (1024-B aligned; <= Stage::per_warp)
 
 struct Params {
     int num, C, Kp, H, W, HW, TW, N, levels;
@@ -61,6 +62,8 @@ struct Params {
     void* out[4];
     int* err;
     int rowsplit;  // 1: the row-split epilogue (16-bit output, TW = 32); level 3 by pool_level_kernel
+    int tma_store;  // 1: full-row tiles (4 target rows x 64 columns, W = 64) stored by TMA (levels 0-2)
+    int th;         // target rows per N tile: 8, or 4 for full-row tiles
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -89,6 +92,20 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
         : "memory");
 }
 
+
+// TMA tensor store of a staged box (3-D map: target columns, source pixels, target
+// rows); completion is tracked per thread with bulk groups
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int x, int y, int z) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// the staged boxes of every committed store have been read (the buffer may be rewritten)
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// every committed store has completed
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 // ---------------------------------------------------------------- output stores
 
@@ -257,8 +274,9 @@ __host__ __device__ inline size_t b_box(int N) { return (size_t)N * 128; }
 
 template <typename TOut>
 __global__ void __launch_bounds__(kThreads, 1)
-    corr_build_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, Params p,
-                      int ab_format) {
+    corr_build_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                      const __grid_constant__ CUtensorMap mapO0, const __grid_constant__ CUtensorMap mapO1,
+                      const __grid_constant__ CUtensorMap mapO2, Params p, int ab_format) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* sbase = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     __shared__ uint64_t barA_full, barA_empty;
@@ -398,6 +416,64 @@ __global__ void __launch_bounds__(kThreads, 1)
                     continue;
                 }
                 if constexpr (sizeof(TOut) == 2) {
+                    if (p.tma_store) {
+                        // Full-row tiles (4 target rows x 64 columns): warp (q, ch) owns TMEM lane
+                        // quarter q and column half ch, so the two halves of every 128-byte level-0
+                        // row leave in the same tile.  Levels 0-2 are staged as the boxes of three
+                        // TMA tensor stores (source pixel = lane): level 0 [4 rows][32 px][64 B] with
+                        // the 64-byte swizzle (16-byte chunk c of a 64-byte row at c ^ ((px >> 1) & 3)),
+                        // level 1 [2][32][32 B] with the 32-byte swizzle (chunk c at
+                        // c ^ ((px >> 2) & 1)), level 2 [32][16 B]; the swizzles keep each
+                        // quarter-warp's 16-byte stores on distinct bank groups.
+                        const int ch = warp >> 2;
+                        uint8_t* t0s = sbase + stage_off + (size_t)warp * kTmaStage;
+                        uint8_t* t1s = t0s + 8192;
+                        uint8_t* t2s = t0s + 10240;
+                        if (lane == 0) bulk_wait_read_all();  // the previous tile's boxes have been read
+                        __syncwarp();
+#pragma unroll 1
+                        for (int cb = 0; cb < 4; cb++) {
+                            float blk[4][8];
+#pragma unroll
+                            for (int r = 0; r < 4; r++)
+                                tmem_ld8(tmem + lane_addr + (uint32_t)(acc * 256 + r * 64 + ch * 32 + cb * 8), blk[r]);
+                            tmem_wait_ld();
+#pragma unroll
+                            for (int r = 0; r < 4; r++)
+                                sts_n<TOut, 8>(t0s + (r * 32 + lane) * 64 + ((cb ^ ((lane >> 1) & 3)) << 4), blk[r]);
+                            float l1[2][4];
+#pragma unroll
+                            for (int r = 0; r < 2; r++)
+#pragma unroll
+                                for (int c2 = 0; c2 < 4; c2++)
+                                    l1[r][c2] = 0.25f * ((blk[2 * r][2 * c2] + blk[2 * r][2 * c2 + 1]) +
+                                                         (blk[2 * r + 1][2 * c2] + blk[2 * r + 1][2 * c2 + 1]));
+#pragma unroll
+                            for (int r = 0; r < 2; r++)
+                                sts_n<TOut, 4>(t1s + (r * 32 + lane) * 32 + (((cb >> 1) ^ ((lane >> 2) & 1)) << 4) +
+                                                   (cb & 1) * 8,
+                                               l1[r]);
+                            float l2[2];
+#pragma unroll
+                            for (int c2 = 0; c2 < 2; c2++)
+                                l2[c2] = 0.25f * ((l1[0][2 * c2] + l1[0][2 * c2 + 1]) + (l1[1][2 * c2] + l1[1][2 * c2 + 1]));
+                            sts_n<TOut, 2>(t2s + lane * 16 + cb * 4, l2);
+                        }
+                        tc_fence_before();
+                        fence_proxy_async();  // generic-proxy staging writes -> the TMA engine
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&barAcc_empty[acc]);
+                        if (lane == 0 && nrows > 0) {
+                            const int h0 = hb * 4;  // the tile's first target row
+                            const int y = (int)row0;
+                            tma_store_3d(&mapO0, t0s, ch * 32, y, h0);
+                            if (p.levels > 1) tma_store_3d(&mapO1, t1s, ch * 16, y, h0 / 2);
+                            if (p.levels > 2) tma_store_3d(&mapO2, t2s, ch * 8, y, h0 / 4);
+                            bulk_commit();
+                        }
+                        __syncwarp();
+                        continue;
+                    }
                     if (p.rowsplit) {
                         const int rh = warp >> 2;
                         uint8_t* s0 = st;
@@ -432,7 +508,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         __syncwarp();
                         if (lane == 0) mbar_arrive(&barAcc_empty[acc]);
                         __syncwarp();
-                        const int h0 = hb * kTH, w0 = wb * TW;
+                        const int h0 = hb * p.th, w0 = wb * TW;
                         {
                             uint8_t* g0 = static_cast<uint8_t*>(p.out[0]) + (size_t)row0 * rs[0] +
                                           ((size_t)(h0 + 4 * rh) * W + w0) * sz;
@@ -482,7 +558,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         if (lane == 0) mbar_arrive(&barAcc_empty[acc]);
                     }
                     __syncwarp();
-                    const int h0 = hb * kTH, w0 = wb * TW + c;
+                    const int h0 = hb * p.th, w0 = wb * TW + c;
                     uint8_t* lvl[4];
                     for (int l = 0; l < 4; l++)
                         lvl[l] = l < p.levels
@@ -498,6 +574,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
         }
     }
+    // every TMA store of this thread has completed before the CTA exits
+    if (p.tma_store && warp < kEpiWarps && lane == 0) bulk_wait_all();
     __syncthreads();
     if (fail && tid == 0) atomicExch(p.err, 1);
     if (warp == kMmaWarp) {
@@ -544,7 +622,7 @@ __global__ void __launch_bounds__(256) pool_level_kernel(const T* __restrict__ i
 // ---------------------------------------------------------------- pack pass
 
 // F (num, C, H, W) -> rows (num, HW, Kp) of 16-bit type, scaled by 1/4;
-// permute: target-block pixel order (8 x TW blocks) for the B operand.  One
+// permute: target-block pixel order (th x TW blocks) for the B operand.  One
 // CTA transposes a 64-channel x 128-pixel tile through shared memory with
 // 16-byte global loads (along pixels) and 16-byte stores (along channels).
 // The tile is held pixel-major (128 rows of 64 channels = 128 B); the 16-byte
@@ -553,7 +631,7 @@ __global__ void __launch_bounds__(256) pool_level_kernel(const T* __restrict__ i
 // pixel row's eight chunks are read conflict-free as one 16-byte load each.
 template <typename TIn, typename TOp>
 __global__ void __launch_bounds__(256) pack_kernel(const TIn* __restrict__ f, TOp* __restrict__ out, int C, int Kp,
-                                                   int H, int W, int TW, int permute) {
+                                                   int H, int W, int TW, int th, int permute) {
     constexpr int kPx = 128, kCh = 64;
     __shared__ __align__(16) TOp tile[kPx][kCh];
     const int e = blockIdx.z;
@@ -592,8 +670,8 @@ __global__ void __launch_bounds__(256) pack_kernel(const TIn* __restrict__ f, TO
         int row = px;
         if (permute) {
             const int h = px / W, w = px % W;
-            const int hb = h / kTH, r = h % kTH, wb = w / TW, c = w % TW;
-            row = ((hb * (W / TW) + wb) * kTH + r) * TW + c;
+            const int hb = h / th, r = h % th, wb = w / TW, c = w % TW;
+            row = ((hb * (W / TW) + wb) * th + r) * TW + c;
         }
         *reinterpret_cast<uint4*>(out + ((size_t)e * HW + row) * Kp + c0 + cg) =
             *reinterpret_cast<const uint4*>(&tile[pp][(c8 ^ ((pp >> 3) & 7)) << 3]);
@@ -632,6 +710,22 @@ int make_map(CUtensorMap* map, void* base, CUtensorMapDataType dt, uint64_t rows
     return r == CUDA_SUCCESS ? VIPE_OK : VIPE_ERR_CUDA;
 }
 
+// output level l (16-bit) as a 3-D map: dim 0 target columns (W_l), dim 1 source pixels
+// (num * H * W, stride one level plane), dim 2 target rows (H_l, stride one target row);
+// box (32 >> l, 32, 4 >> l) = one epilogue warp's rows of one tile
+int make_out_map(CUtensorMap* map, void* base, CUtensorMapDataType dt, uint64_t src_rows, int Hl, int Wl, int l,
+                 CUtensorMapSwizzle swz) {
+    EncodeTiled enc = get_encode();
+    if (!enc) return VIPE_ERR_CUDA;
+    const cuuint64_t dims[3] = {(cuuint64_t)Wl, (cuuint64_t)src_rows, (cuuint64_t)Hl};
+    const cuuint64_t strides[2] = {(cuuint64_t)Hl * Wl * 2, (cuuint64_t)Wl * 2};
+    const cuuint32_t box[3] = {(cuuint32_t)(32 >> l), 32u, (cuuint32_t)(4 >> l)};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(map, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
+                     CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? VIPE_OK : VIPE_ERR_CUDA;
+}
+
 int pick_tw(int W) {
     if (W % 32 == 0) return 32;
     if (W % 16 == 0) return 16;
@@ -667,7 +761,7 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
     if (!fmap1 || !fmap2 || !level_out || !workspace) return VIPE_ERR_ARG;
     for (int l = 0; l < num_levels; l++)
         if (!level_out[l]) return VIPE_ERR_ARG;
-    const int TW = pick_tw(wd);
+    int TW = pick_tw(wd);
     if (TW == 0 || ht % kTH != 0) return VIPE_ERR_CAPACITY;  // fused pooling needs 8 x 8 closable blocks
     const int Kp = ((C + kKC - 1) / kKC) * kKC;
     if (Kp / kKC > kMaxKC) return VIPE_ERR_CAPACITY;
@@ -685,6 +779,34 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
     void* pb = ws + 256 + op_bytes;
     VIPE_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
 
+    // epilogue mode, decided before the pack (it fixes the B pixel order): 16-bit 64-wide maps
+    // use full-row tiles (4 x 64) stored by TMA when the output maps encode; other 16-bit
+    // shapes with 32-wide blocks the row-split epilogue; the rest the column-half epilogue
+    bool al16 = true;
+    for (int l = 0; l < num_levels; l++) al16 &= (reinterpret_cast<uintptr_t>(level_out[l]) % 16) == 0;
+    // (level 3 of the row-split and full-row paths is pooled by a 16-byte-row kernel for 64-wide maps)
+    const int rowsplit = (out_dtype != VIPE_F32 && TW == 32 && al16 && (num_levels < 4 || wd == 64)) ? 1 : 0;
+    CUtensorMap mO[3];
+    int tma_store = 0, th = kTH;
+    if (rowsplit && wd == 64 && HW % 32 == 0) {
+        const CUtensorMapDataType odt =
+            out_dtype == VIPE_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+        const CUtensorMapSwizzle swz[3] = {CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_SWIZZLE_32B,
+                                           CU_TENSOR_MAP_SWIZZLE_NONE};
+        bool ok = true;
+        const int nl = std::min(num_levels, 3);
+        for (int l = 0; l < 3 && ok; l++) {
+            const int ll = l < nl ? l : 0;  // unused maps repeat level 0 (never issued)
+            ok = make_out_map(&mO[l], level_out[ll], odt, (uint64_t)num * HW, ht >> ll, wd >> ll, ll, swz[ll]) ==
+                 VIPE_OK;
+        }
+        if (ok) {
+            tma_store = 1;
+            TW = 64;
+            th = 4;
+        }
+    }
+
     // operand type: FP16 inputs stay FP16, others go to BF16
     const int op_fmt = (in_dtype == VIPE_F16) ? 0 : 1;
     dim3 pg(ceil_div(HW, 128), Kp / kKC, num);
@@ -696,18 +818,18 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
             const int perm = side;
             if (in_dtype == VIPE_F16)
                 pack_kernel<__half, __half><<<pg, 256, 0, st>>>(static_cast<const __half*>(src),
-                                                                static_cast<__half*>(dst), C, Kp, ht, wd, TW, perm);
+                                                                static_cast<__half*>(dst), C, Kp, ht, wd, TW, th, perm);
             else if (in_dtype == VIPE_BF16)
                 pack_kernel<__nv_bfloat16, __nv_bfloat16><<<pg, 256, 0, st>>>(
-                    static_cast<const __nv_bfloat16*>(src), static_cast<__nv_bfloat16*>(dst), C, Kp, ht, wd, TW, perm);
+                    static_cast<const __nv_bfloat16*>(src), static_cast<__nv_bfloat16*>(dst), C, Kp, ht, wd, TW, th, perm);
             else
                 pack_kernel<float, __nv_bfloat16><<<pg, 256, 0, st>>>(static_cast<const float*>(src),
                                                                       static_cast<__nv_bfloat16*>(dst), C, Kp, ht,
-                                                                      wd, TW, perm);
+                                                                      wd, TW, th, perm);
             VIPE_LAUNCH_CHECK();
         }
     }
-    const int N = kTH * TW;
+    const int N = th * TW;
     CUtensorMap mA, mB;
     const CUtensorMapDataType dt = op_fmt == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     int rc;
@@ -722,10 +844,10 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
     p.out_dtype = out_dtype;
     for (int l = 0; l < 4; l++) p.out[l] = l < num_levels ? level_out[l] : nullptr;
     p.err = err;
-    bool al16 = true;
-    for (int l = 0; l < num_levels; l++) al16 &= (reinterpret_cast<uintptr_t>(level_out[l]) % 16) == 0;
-    // (level 3 of the row-split path is pooled by a 16-byte-row kernel for 64-wide maps)
-    p.rowsplit = (out_dtype != VIPE_F32 && TW == 32 && al16 && (num_levels < 4 || wd == 64)) ? 1 : 0;
+    p.rowsplit = rowsplit;
+    p.tma_store = tma_store;
+    p.th = th;
+    if (!p.tma_store) mO[0] = mO[1] = mO[2] = mA;  // placeholders, never used
 
     int dev = 0, sms = 148;
     VIPE_CUDA_TRY(cudaGetDevice(&dev));
@@ -748,11 +870,11 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
     {
         VIPE_PROF("corr_build", st);
         if (out_dtype == VIPE_F32)
-            corr_build_kernel<float><<<grid, kThreads, smem, st>>>(mA, mB, p, op_fmt);
+            corr_build_kernel<float><<<grid, kThreads, smem, st>>>(mA, mB, mO[0], mO[1], mO[2], p, op_fmt);
         else if (out_dtype == VIPE_F16)
-            corr_build_kernel<__half><<<grid, kThreads, smem, st>>>(mA, mB, p, op_fmt);
+            corr_build_kernel<__half><<<grid, kThreads, smem, st>>>(mA, mB, mO[0], mO[1], mO[2], p, op_fmt);
         else
-            corr_build_kernel<__nv_bfloat16><<<grid, kThreads, smem, st>>>(mA, mB, p, op_fmt);
+            corr_build_kernel<__nv_bfloat16><<<grid, kThreads, smem, st>>>(mA, mB, mO[0], mO[1], mO[2], p, op_fmt);
     }
     VIPE_LAUNCH_CHECK();
     if (p.rowsplit && num_levels > 3) {
