@@ -20,12 +20,14 @@
 //     in each thread's registers, so the 2x2 / 4x4 average pools close inside
 //     the thread; the levels are staged per warp in shared memory and written
 //     with 16-byte stores in which consecutive lanes cover contiguous bytes.
-//     16-bit output with 32-wide target blocks (the production shape) uses the
-//     row-split mapping (kR0 below): each warp owns 4 of the 8 target rows, so
-//     level-0 stores cover 64 contiguous bytes, level-1 rows whole 32-byte
-//     sectors, and level 3 is pooled from the stored level 2 afterwards
-//     (pool_level_kernel) instead of in 4-byte pieces; other shapes split the
-//     tile's columns between warp halves and pool all levels in the epilogue.
+//     16-bit output on 64-wide maps (the production shape) uses full-row tiles
+//     (4 target rows x 64 columns): each warp owns a column half of all 4 rows,
+//     stages levels 0-2 in swizzled boxes and writes them with TMA tensor
+//     stores, and level 3 is pooled from the stored level 2 afterwards
+//     (pool_level_kernel).  Other 16-bit shapes with 32-wide target blocks use
+//     the row-split mapping (kR0 below: each warp owns 4 of 8 target rows,
+//     16-byte st.global from staging); the rest split the tile's columns
+//     between warp halves and pool all levels in the epilogue.
 // The output write (sum over levels of num*HW*HW/4^l elements) is the HBM
 // roofline of this kernel: it is write-only traffic.
 
