@@ -133,6 +133,21 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- helpers
 
+def max_over_ranks(ms, world, dist, dev):
+    """The slowest rank's time (every rank calls it at the same point; one all-reduce)."""
+    import torch
+
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, units_per_rank, ms):
+    """Units per second of the whole job: every rank processed `units_per_rank` in at most `ms`."""
+    return world * units_per_rank / (ms / 1e3)
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -479,12 +494,8 @@ def batched_leg(dev, args, world, dist, flush, stream):
         cap.replay()
         ev[k][1].record(stream)
     torch.cuda.synchronize(dev)
-    dev_ms = sum(a.elapsed_time(c) for a, c in ev)
-    t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    batch_ms = float(t.item()) / n
-    value = world * b.G / (batch_ms / 1e3)
+    batch_ms = max_over_ranks(sum(a.elapsed_time(c) for a, c in ev), world, dist, dev) / n
+    value = whole_job_rate(world, b.G, batch_ms)
     status = cap.out[3].cpu().tolist()
 
     # accuracy of the batch against the FP64 oracle on a few clips
@@ -541,14 +552,8 @@ def batched_leg(dev, args, world, dist, flush, stream):
         torch.cuda.synchronize(dev)
         if k >= 1:
             seq.append(a.elapsed_time(c))
-    ts = torch.tensor([sum(seq)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(ts, op=dist.ReduceOp.MAX)
-    seq_value = world * b.G * len(seq) / (float(ts.item()) / 1e3)
-    te = torch.tensor([sum(e2e)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * b.G * len(e2e) / (float(te.item()) / 1e3)
+    seq_value = whole_job_rate(world, b.G * len(seq), max_over_ranks(sum(seq), world, dist, dev))
+    e2e_value = whole_job_rate(world, b.G * len(e2e), max_over_ranks(sum(e2e), world, dist, dev))
 
     # live per-kernel profile of one eager batched solve
     lib = _lib.load()
@@ -692,11 +697,8 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
         fwd_adj()
         ev[k][1].record(stream)
     torch.cuda.synchronize(dev)
-    t = torch.tensor([sum(a.elapsed_time(c) for a, c in ev)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    step_ms = float(t.item()) / n
-    value = world * b.G / (step_ms / 1e3)
+    step_ms = max_over_ranks(sum(a.elapsed_time(c) for a, c in ev), world, dist, dev) / n
+    value = whole_job_rate(world, b.G, step_ms)
     status_nonzero = int((st != 0).sum().item())
 
     # live per-kernel profile of one step
@@ -746,10 +748,7 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
         if k >= 1:
             e2e.append(a.elapsed_time(c))
     stream_status = int((runner.status() != 0).sum().item())
-    te = torch.tensor([sum(e2e)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * b.G * len(e2e) / (float(te.item()) / 1e3)
+    e2e_value = whole_job_rate(world, b.G * len(e2e), max_over_ranks(sum(e2e), world, dist, dev))
     nparts = len(runner.parts)
     del runner
 
@@ -771,10 +770,7 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
         torch.cuda.synchronize(dev)
         if k >= 1:
             seq.append(a.elapsed_time(c))
-    ts = torch.tensor([sum(seq)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(ts, op=dist.ReduceOp.MAX)
-    seq_value = world * b.G * len(seq) / (float(ts.item()) / 1e3)
+    seq_value = whole_job_rate(world, b.G * len(seq), max_over_ranks(sum(seq), world, dist, dev))
     del plan, static, tape, gt, gw
     return {
         "value": value,
