@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--cpu-sample-s", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-corr", action="store_true")
-    ap.add_argument("--e2e-parts", type=int, default=16,
+    ap.add_argument("--e2e-parts", type=int, default=24,
                     help="host batch split into this many streamed parts for the end-to-end leg")
     return ap.parse_args()
 
