@@ -30,3 +30,36 @@ def test_library_exports_every_declared_symbol():
 def test_status_strings():
     assert _lib.status_string(0)
     assert "index" in _lib.status_string(_lib.VIPE_ERR_INDEX).lower()
+
+
+def test_argument_checks_run_before_any_device_work():
+    """Entry points reject bad sizes and pointers with a status before touching the GPU, so
+    these calls are safe without one (null device pointers are never dereferenced)."""
+    import ctypes
+
+    lib = _lib.load()
+    null = ctypes.c_void_p(0)
+    # write probe: null destination, size not a multiple of 16
+    assert lib.vipe_hbm_write_probe(null, 16, null) == _lib.VIPE_ERR_ARG
+    assert lib.vipe_hbm_write_probe(ctypes.c_void_p(16), 15, null) == _lib.VIPE_ERR_ARG
+    # coordinate gradient of the volume lookup: negative sizes
+    assert lib.vipe_corr_index_coords_backward(0, null, null, null, -1, 4, 4, 4, 4, 3, null, null) == \
+        _lib.VIPE_ERR_ARG
+    # indexed lookup backward: no levels, too many channels, missing outputs
+    h2 = (ctypes.c_int * 1)(8)
+    w2 = (ctypes.c_int * 1)(8)
+    lv = (ctypes.c_void_p * 1)(16)
+    args = dict(dtype=0, f1=ctypes.c_void_p(16), lv=lv, h2=h2, w2=w2, L=1, B=1, Nf=2, M=1, H=8, W=8, C=32, r=3)
+
+    def call(**kw):
+        a = {**args, **kw}
+        g1 = kw.get("g1", ctypes.c_void_p(16))
+        gl = kw.get("gl", lv)
+        return lib.vipe_altcorr_index_backward(a["dtype"], a["f1"], a["lv"], a["h2"], a["w2"], a["L"], null, null,
+                                               null, null, a["B"], a["Nf"], a["M"], a["H"], a["W"], a["C"], a["r"],
+                                               0, g1, gl, null, null)
+
+    assert call(L=0) == _lib.VIPE_ERR_ARG
+    assert call(C=512) == _lib.VIPE_ERR_CAPACITY
+    assert call(r=4) == _lib.VIPE_ERR_CAPACITY
+    assert call(g1=null) == _lib.VIPE_ERR_ARG
