@@ -444,6 +444,22 @@ def run_reference(args):
 
 # ---------------------------------------------------------------- our arm
 
+# Measured DRAM traffic per edge of one launch (dram__bytes_read.sum + dram__bytes_write.sum
+# from an ncu capture of the first 32 clips of the same batch generator, mean over the LM
+# iterations' launches, divided by that case's 8938 edges; profiles/ba_kernels_traffic_32clips.md).
+# Traffic grows with the edges (every edge-pixel is read once per launch), so a launch over this
+# batch moves about `per edge x edges`.
+TRAFFIC_PER_EDGE = {
+    "ba_frame": 584.0e6 / 8938,
+    "ba_adj_frame_b": (1133.0e6 + 3 * 1573.0e6) / 4 / 8938,
+}
+
+
+def batch_kernel_traffic(b, name):
+    per_edge = TRAFFIC_PER_EDGE.get(name)
+    return None if per_edge is None else per_edge * sum(b.num_edges)
+
+
 def batch_kernel_bytes(b, name):
     """Algorithmic DRAM bytes of one launch of a BA kernel over the whole batch (fp32 = 4 B)."""
     HW = b.ht * b.wd
@@ -576,7 +592,8 @@ def batched_leg(dev, args, world, dist, flush, stream):
         avg_s = ms / cnt / 1e3
         ach = nbytes / avg_s / 1e9
         roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                "traffic": None, "peak_source": src, "bytes_per_launch": nbytes, "avg_launch_ms": avg_s * 1e3}
+                "traffic": batch_kernel_traffic(b, name), "peak_source": src, "bytes_per_launch": nbytes,
+                "avg_launch_ms": avg_s * 1e3}
         break
 
     # the plain drop-in on the same batch, clip by clip, same GPU (the 5x comparison)
@@ -720,7 +737,8 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
         avg_s = kms / cnt / 1e3
         ach = nbytes / avg_s / 1e9
         roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                "traffic": None, "peak_source": src, "bytes_per_launch": nbytes, "avg_launch_ms": avg_s * 1e3,
+                "traffic": batch_kernel_traffic(b, name), "peak_source": src, "bytes_per_launch": nbytes,
+                "avg_launch_ms": avg_s * 1e3,
                 "note": "FP32-issue bound: HBM is the algorithmic bound, not the limiter (profiles/)"}
         break
 
