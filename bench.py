@@ -366,6 +366,55 @@ def corr_lookup_bench(dev, f1, f2, g, hbm_peak):
     }
 
 
+def lie_bench(dev, hbm_peak):
+    """SE3 group kernels over 16M elements (f32; HBM bound): bytes = elements x (inputs +
+    outputs) x 4 B.  Outputs are preallocated; each op is one launch, median of 5."""
+    import torch
+
+    from vipe_b200 import _lib
+
+    lib = _lib.load()
+    B = 16 * 1024 * 1024
+    g = torch.Generator(device=dev).manual_seed(1003)
+    a = 0.3 * torch.randn(B, 6, generator=g, device=dev)
+    X = torch.empty(B, 7, device=dev)
+    Y = torch.empty(B, 7, device=dev)
+    Z = torch.empty(B, 7, device=dev)
+    pts = torch.randn(B, 3, generator=g, device=dev)
+    q = torch.empty(B, 3, device=dev)
+    la = torch.empty(B, 6, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    st = stream.cuda_stream
+    SE3, F32 = 3, 0
+    _lib.check(lib.vipe_lie_expm(SE3, F32, B, a.data_ptr(), X.data_ptr(), st), "expm")
+    _lib.check(lib.vipe_lie_expm(SE3, F32, B, (0.5 * a).data_ptr(), Y.data_ptr(), st), "expm")
+    ops = {
+        "expm": (lambda: lib.vipe_lie_expm(SE3, F32, B, a.data_ptr(), Z.data_ptr(), st), 6 + 7),
+        "logm": (lambda: lib.vipe_lie_logm(SE3, F32, B, X.data_ptr(), la.data_ptr(), st), 7 + 6),
+        "inv": (lambda: lib.vipe_lie_inv(SE3, F32, B, X.data_ptr(), Z.data_ptr(), st), 7 + 7),
+        "mul": (lambda: lib.vipe_lie_mul(SE3, F32, B, X.data_ptr(), Y.data_ptr(), Z.data_ptr(), st), 7 + 7 + 7),
+        "act": (lambda: lib.vipe_lie_act(SE3, F32, B, X.data_ptr(), pts.data_ptr(), q.data_ptr(), st), 7 + 3 + 3),
+    }
+    out = {}
+    for name, (fn, floats) in ops.items():
+        fn()
+        torch.cuda.synchronize(dev)
+        ts = []
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rc = fn()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            _lib.check(rc, name)
+            ts.append(e0.elapsed_time(e1))
+        ms = sorted(ts)[2]
+        nbytes = B * floats * 4
+        out[name] = {"ms": ms, "bytes": nbytes, "achieved": nbytes / (ms / 1e3) / 1e9, "unit": "GB/s",
+                     "frac": nbytes / (ms / 1e3) / 1e9 / hbm_peak}
+    return {"workload": "SE3 group ops, 16M elements, f32 (lietorch_ext kernels)", "ops": out}
+
+
 def _cpu_clip_solves(sample_s, max_clips=256):
     """Solves clips of the 256-clip batch one after another on the CPU oracle until
     `sample_s` seconds have passed; returns (solves, seconds, threads)."""
@@ -954,6 +1003,8 @@ def run_ours(args):
     if not args.no_corr:
         torch.cuda.empty_cache()
         corr = corr_build_bench(dev, 5, hbm, src, bf16)
+    torch.cuda.empty_cache()
+    lie = lie_bench(dev, hbm)
 
     if rank == 0:
         line = {
@@ -988,6 +1039,7 @@ def run_ours(args):
             "plain_cfg1": plain,
             "sim3_batched": sim3,
             "corr": corr,
+            "lie": lie,
         }
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.cpu_sample_s)
