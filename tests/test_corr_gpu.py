@@ -322,3 +322,21 @@ def test_altcorr_index_forward_paths(dtype, C, sigma, W):
     want = oc.altcorr_index_forward(f.double().numpy(), [lv.double().numpy() for lv in levels], coords.numpy(),
                                     ii.numpy(), jj.numpy(), 3)
     np.testing.assert_allclose(out.double().cpu().numpy(), want, atol=1e-4)
+
+
+@pytest.mark.parametrize("levels", [1, 2, 3])
+def test_volume_build_full_row_path_fewer_levels(levels):
+    """64-wide 16-bit maps take the full-row TMA-store epilogue; with fewer than 4 levels only the
+    requested levels are stored (and no level-3 pooling pass runs)."""
+    from vipe_b200.corr_build import corr_volume_pyramid
+
+    g = torch.Generator().manual_seed(22)
+    num, C, H, W = 2, 128, 16, 64
+    f1 = (torch.randn(num, C, H, W, generator=g) / np.sqrt(C) * 4).to(torch.bfloat16)
+    f2 = (torch.randn(num, C, H, W, generator=g) / np.sqrt(C) * 4).to(torch.bfloat16)
+    got = corr_volume_pyramid(f1.cuda(), f2.cuda(), levels, out_dtype=torch.float16)
+    assert len(got) == levels
+    want = oc.corr_pyramid(f1.double().numpy(), f2.double().numpy(), levels)
+    for l, (a, w) in enumerate(zip(got, want)):
+        a = a.cpu().double().numpy().reshape(w.shape)
+        assert np.abs(a - w).max() <= 2e-3 * np.abs(w).max(), l
