@@ -66,6 +66,8 @@ struct Params {
     int rowsplit;  // 1: the row-split epilogue (16-bit output, TW = 32); level 3 by pool_level_kernel
     int tma_store;  // 1: full-row tiles (4 target rows x 64 columns, W = 64) stored by TMA (levels 0-2)
     int th;         // target rows per N tile: 8, or 4 for full-row tiles
+    int direct;     // 1: the A operand (source pixels) is loaded by TMA straight from the 16-bit fmap1 (MN-major)
+                    // and the product scaled by 1/4 in the epilogue; only fmap2 is packed (full-row tiles only)
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -94,6 +96,27 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
         : "memory");
 }
 
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+// Shared-memory descriptor of an MN-major, 128-byte swizzled 16-bit operand: 64-element MN
+// atoms (128-byte rows, one per K index) `atom_bytes` apart, 8-row K groups 1024 B apart.
+__device__ __forceinline__ uint64_t smem_desc_sw128_mn(const void* base, uint32_t atom_bytes) {
+    const uint64_t addr = smem_u32(base);
+    uint64_t d = 0;
+    d |= (addr >> 4) & 0x3FFFull;                       // start address
+    d |= (uint64_t)((atom_bytes >> 4) & 0x3FFF) << 16;  // leading byte offset: next MN atom
+    d |= (uint64_t)(1024 >> 4) << 32;                   // stride byte offset: next 8 K rows
+    d |= (uint64_t)1 << 46;                             // descriptor version (sm100)
+    d |= (uint64_t)2 << 61;                             // SWIZZLE_128B
+    return d;
+}
 
 // TMA tensor store of a staged box (3-D map: target columns, source pixels, target
 // rows); completion is tracked per thread with bulk groups
@@ -330,8 +353,15 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int e = (int)(item / p.mtiles), mt = (int)(item % p.mtiles);
             if (it > 0 && !mbar_wait(&barA_empty, (it - 1) & 1, &fail)) break;
             mbar_expect_tx(&barA_full, a_bytes);
-            for (int kc = 0; kc < KC; kc++)
-                tma_load_2d(sa(kc), &mapA, &barA_full, kc * kKC, e * p.HW + mt * kBM);
+            for (int kc = 0; kc < KC; kc++) {
+                if (p.direct) {
+                    // two 64-pixel MN atoms of 64 channels each from fmap1 (pixels past H*W read zeros)
+                    for (int h = 0; h < kBM / 64; h++)
+                        tma_load_3d(sa(kc) + h * 8192, &mapA, &barA_full, mt * kBM + 64 * h, kc * kKC, e);
+                } else {
+                    tma_load_2d(sa(kc), &mapA, &barA_full, kc * kKC, e * p.HW + mt * kBM);
+                }
+            }
             for (int nt = 0; nt < p.ntiles && !fail; nt++, t++) {
                 // box kc of this tile (barB_full/empty[kc]: one phase per tile)
                 for (int kc = 0; kc < KC; kc++) {
@@ -353,7 +383,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     } else if (warp == kMmaWarp && lane == 0) {
         // ------------------------------------------------ MMA issuer
-        const uint32_t idesc = instr_desc(ab_format, kBM, N);
+        // MN-major A (direct loads): transpose bit 15 of the instruction descriptor
+        const uint32_t idesc = instr_desc(ab_format, kBM, N) | (p.direct ? (1u << 15) : 0u);
         uint32_t t = 0, it = 0;
         for (long item = blockIdx.x; item < p.items && !fail; item += gridDim.x, it++) {
             if (!mbar_wait(&barA_full, it & 1, &fail)) break;
@@ -369,13 +400,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                         break;
                     }
                     tc_fence_after();
-                    const uint64_t da = smem_desc_sw128(sa(kc));
+                    const uint64_t da = p.direct ? smem_desc_sw128_mn(sa(kc), 8192) : smem_desc_sw128(sa(kc));
                     const uint64_t db = smem_desc_sw128(sb(0, kc));
+                    // K step of 16 channels: 32 bytes inside the swizzled row (K-major) or 16 rows of
+                    // 128 bytes (MN-major A)
+                    const uint64_t astep = p.direct ? (uint64_t)(2048 >> 4) : 2u;
 #pragma unroll
-                    for (int k = 0; k < kKC / 16; k++) {
-                        // advance 16 channels = 32 bytes inside the swizzled row
-                        mma_f16(d, da + (uint64_t)(k * 2), db + (uint64_t)(k * 2), idesc, (kc | k) ? 1u : 0u);
-                    }
+                    for (int k = 0; k < kKC / 16; k++)
+                        mma_f16(d, da + (uint64_t)k * astep, db + (uint64_t)(k * 2), idesc, (kc | k) ? 1u : 0u);
                     mma_commit(&barB_empty[kc]);  // box kc of this tile is read once these MMAs complete
                 }
                 if (!ok) break;
@@ -440,6 +472,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                             for (int r = 0; r < 4; r++)
                                 tmem_ld8(tmem + lane_addr + (uint32_t)(acc * 256 + r * 64 + ch * 32 + cb * 8), blk[r]);
                             tmem_wait_ld();
+                            if (p.direct) {  // fmap1's 1/4 scale (fmap2's is in its pack), applied here (exact)
+#pragma unroll
+                                for (int r = 0; r < 4; r++)
+#pragma unroll
+                                    for (int j = 0; j < 8; j++) blk[r][j] *= 0.25f;
+                            }
 #pragma unroll
                             for (int r = 0; r < 4; r++)
                                 sts_n<TOut, 8>(t0s + (r * 32 + lane) * 64 + ((cb ^ ((lane >> 1) & 3)) << 4), blk[r]);
@@ -728,6 +766,20 @@ int make_out_map(CUtensorMap* map, void* base, CUtensorMapDataType dt, uint64_t 
     return r == CUDA_SUCCESS ? VIPE_OK : VIPE_ERR_CUDA;
 }
 
+// a 16-bit feature map (num, C, H*W) as a 3-D map: dim 0 pixels, dim 1 channels, dim 2 maps;
+// box 64 pixels x 64 channels (one MN-major 128-byte swizzled operand atom column)
+int make_fmap_map(CUtensorMap* map, const void* base, CUtensorMapDataType dt, int HW, int C, int num) {
+    EncodeTiled enc = get_encode();
+    if (!enc) return VIPE_ERR_CUDA;
+    const cuuint64_t dims[3] = {(cuuint64_t)HW, (cuuint64_t)C, (cuuint64_t)num};
+    const cuuint64_t strides[2] = {(cuuint64_t)HW * 2, (cuuint64_t)C * HW * 2};
+    const cuuint32_t box[3] = {64u, (cuuint32_t)kKC, 1u};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(map, dt, 3, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? VIPE_OK : VIPE_ERR_CUDA;
+}
+
 int pick_tw(int W) {
     if (W % 32 == 0) return 32;
     if (W % 16 == 0) return 16;
@@ -811,10 +863,19 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
 
     // operand type: FP16 inputs stay FP16, others go to BF16
     const int op_fmt = (in_dtype == VIPE_F16) ? 0 : 1;
+    const CUtensorMapDataType dt = op_fmt == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    // Full-row tiles of 16-bit maps with whole 64-channel boxes load the A operand (read once per
+    // work item) straight from fmap1 (num, C, H*W): for a fixed channel the pixels are contiguous,
+    // which is the MN-major operand layout.  The B operand, re-read by every work item of its edge,
+    // stays packed K-major (contiguous 128-byte rows load faster than 64 strided ones).
+    CUtensorMap mA, mB;
+    int direct = 0;
+    if (tma_store && in_dtype != VIPE_F32 && C == Kp && (HW % 8) == 0 && reinterpret_cast<uintptr_t>(fmap1) % 16 == 0)
+        direct = make_fmap_map(&mA, fmap1, dt, HW, C, num) == VIPE_OK;
     dim3 pg(ceil_div(HW, 128), Kp / kKC, num);
     {
         VIPE_PROF("corr_pack", st);
-        for (int side = 0; side < 2; side++) {
+        for (int side = direct ? 1 : 0; side < 2; side++) {
             const void* src = side == 0 ? fmap1 : fmap2;
             void* dst = side == 0 ? pa : pb;
             const int perm = side;
@@ -832,10 +893,8 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
         }
     }
     const int N = th * TW;
-    CUtensorMap mA, mB;
-    const CUtensorMapDataType dt = op_fmt == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     int rc;
-    if ((rc = make_map(&mA, pa, dt, rows, Kp, kBM)) != VIPE_OK) return rc;
+    if (!direct && (rc = make_map(&mA, pa, dt, rows, Kp, kBM)) != VIPE_OK) return rc;
     if ((rc = make_map(&mB, pb, dt, rows, Kp, N)) != VIPE_OK) return rc;
 
     Params p;
@@ -849,6 +908,7 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
     p.rowsplit = rowsplit;
     p.tma_store = tma_store;
     p.th = th;
+    p.direct = direct;
     if (!p.tma_store) mO[0] = mO[1] = mO[2] = mA;  // placeholders, never used
 
     int dev = 0, sms = 148;
