@@ -8,11 +8,13 @@
 // Data path (one persistent launch, one CTA per SM):
 //   * pack pass: F1, F2 (num, C, H, W) -> K-major BF16/FP16 rows (num, H*W, Kp)
 //     scaled by 1/4 (exact), F2's pixels reordered so that 256 consecutive rows
-//     are an 8 x TW block of the target image (TW = 32, 16 or 8 | W);
-//   * warp 0 lane 0: TMA loads (SWIZZLE_128B, 64-channel boxes) of the A tile
+//     are a th x TW block of the target image (8 x 32/16/8, or 4 x 64 for the
+//     full-row tiles of 64-wide maps); with 16-bit 64-wide maps only F2 is
+//     packed and the A operand is read from F1 itself (MN-major, below);
+//   * warp 8 lane 0: TMA loads (SWIZZLE_128B, 64-channel boxes) of the A tile
 //     (128 source pixels x Kp, reused for all N tiles of the work item) and of
-//     the B tiles (8 x TW target pixels x Kp, double-buffered);
-//   * warp 1 lane 0: tcgen05.mma.cta_group::1.kind::f16, M = 128, N = 8*TW,
+//     the B tiles (one stage, filled and drained per 64-channel box);
+//   * warp 9 lane 0: tcgen05.mma.cta_group::1.kind::f16, M = 128, N = th*TW,
 //     K = 16 per instruction, FP32 accumulator in tensor memory, two TMEM
 //     accumulator buffers (2 x 256 columns) so the MMA of tile t+1 overlaps the
 //     epilogue of tile t;
