@@ -25,10 +25,12 @@
 //     16-bit output on 64-wide maps (the production shape) uses full-row tiles
 //     (4 target rows x 64 columns): each warp owns a column half of all 4 rows,
 //     stages levels 0-2 in swizzled boxes and writes them with TMA tensor
-//     stores, and level 3 is pooled from the stored level 2 afterwards
-//     (pool_level_kernel).  Other 16-bit shapes with 32-wide target blocks use
+//     stores, and pools level 3 from the level-2 rows of two consecutive tiles
+//     (the even tile's row carried in registers).  Other 16-bit shapes with
+//     32-wide target blocks use
 //     the row-split mapping (kR0 below: each warp owns 4 of 8 target rows,
-//     16-byte st.global from staging); the rest split the tile's columns
+//     16-byte st.global from staging; level 3 pooled afterwards from the stored
+//     level 2 by pool_level_kernel); the rest split the tile's columns
 //     between warp halves and pool all levels in the epilogue.
 // The output write (sum over levels of num*HW*HW/4^l elements) is the HBM
 // roofline of this kernel: it is write-only traffic.
@@ -173,6 +175,10 @@ struct Stage {
 // warp.  Level 3 (2x2 of level 2) is pooled afterwards from the stored level 2.
 constexpr int kR0 = 4 * 64 + 16, kR1 = 2 * 32 + 16, kR2 = 16 + 16;  // staged row strides (bytes)
 static_assert(32 * (kR0 + kR1 + kR2) <= 12800, "row-split staging exceeds the per-warp staging region");
+
+__device__ __forceinline__ float to_float(__half v) { return __half2float(v); }
+__device__ __forceinline__ float to_float(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float to_float(float v) { return v; }
 
 template <typename T>
 __device__ __forceinline__ uint32_t pack2(float a, float b);
@@ -435,6 +441,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             ss[l] = (uint32_t)((W >> l) * sz);             // one target row of level l
         }
         uint32_t t = 0;
+        uint4 l2_carry = make_uint4(0, 0, 0, 0);  // full-row tiles: the previous tile's staged level-2 row
         for (long item = blockIdx.x; item < p.items && !fail; item += gridDim.x) {
             const int e = (int)(item / p.mtiles), mt = (int)(item % p.mtiles);
             const int m0 = mt * kBM + q * 32;               // first source row of this warp
@@ -500,6 +507,28 @@ __global__ void __launch_bounds__(kThreads, 1)
                             for (int c2 = 0; c2 < 2; c2++)
                                 l2[c2] = 0.25f * ((l1[0][2 * c2] + l1[0][2 * c2 + 1]) + (l1[1][2 * c2] + l1[1][2 * c2 + 1]));
                             sts_n<TOut, 2>(t2s + lane * 16 + cb * 4, l2);
+                        }
+                        if (p.levels > 3) {
+                            // level 3 row hb / 2 pools the level-2 rows of tiles hb - 1 and hb (consecutive
+                            // tiles of this warp): even tiles keep their staged row in registers, odd tiles
+                            // write 4 values of this lane's column half (the stored FP16 level 2, FP32 sums)
+                            const uint4 cur = *reinterpret_cast<const uint4*>(t2s + lane * 16);
+                            if ((hb & 1) == 0) {
+                                l2_carry = cur;
+                            } else if (lane < nrows) {
+                                const TOut* a2 = reinterpret_cast<const TOut*>(&l2_carry);
+                                const TOut* b2 = reinterpret_cast<const TOut*>(&cur);
+                                float l3[4];
+#pragma unroll
+                                for (int c3 = 0; c3 < 4; c3++)
+                                    l3[c3] = 0.25f * ((to_float(a2[2 * c3]) + to_float(a2[2 * c3 + 1])) +
+                                                      (to_float(b2[2 * c3]) + to_float(b2[2 * c3 + 1])));
+                                uint8_t* g3 = static_cast<uint8_t*>(p.out[3]) +
+                                              ((size_t)(row0 + lane) * (size_t)((p.H >> 3) * (p.W >> 3)) +
+                                               (size_t)(hb >> 1) * (p.W >> 3) + ch * 4) * sizeof(TOut);
+                                *reinterpret_cast<uint2*>(g3) = make_uint2(pack2<TOut>(l3[0], l3[1]),
+                                                                           pack2<TOut>(l3[2], l3[3]));
+                            }
                         }
                         tc_fence_before();
                         fence_proxy_async();  // generic-proxy staging writes -> the TMA engine
@@ -941,7 +970,7 @@ extern "C" int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* f
             corr_build_kernel<__nv_bfloat16><<<grid, kThreads, smem, st>>>(mA, mB, mO[0], mO[1], mO[2], p, op_fmt);
     }
     VIPE_LAUNCH_CHECK();
-    if (p.rowsplit && num_levels > 3) {
+    if (p.rowsplit && num_levels > 3 && !p.tma_store) {  // (full-row tiles pool level 3 in the epilogue)
         if (wd != 64) {
             set_last_error("corr_volume_build: level 3 of the row-split path expects 64-wide maps");
             return VIPE_ERR_CAPACITY;
