@@ -137,6 +137,10 @@ def test_altcorr_index_matches_oracle_and_reference_property():
         # 16-bit output, 32-wide target blocks: level 0 leaves the epilogue as 32-byte row stores
         (torch.bfloat16, torch.float16, (2, 128, 48, 64)),
         (torch.float16, torch.bfloat16, (1, 128, 16, 64)),
+        # 64-wide 16-bit: one 64-channel box (A read from fmap1 directly), and C = 96 (padded to 128:
+        # both operands packed, full-row TMA-store epilogue)
+        (torch.bfloat16, torch.bfloat16, (2, 64, 16, 64)),
+        (torch.float16, torch.float16, (1, 96, 16, 64)),
     ],
 )
 def test_volume_build_pyramid(in_dtype, out_dtype, shape):
