@@ -195,15 +195,15 @@ def test_corr_index_coords_backward(dtype):
     np.testing.assert_allclose(out.double().cpu().numpy(), want, atol=tol, rtol=1e-5)
 
 
-@pytest.mark.parametrize("dtype", [torch.float32, torch.float16])
-def test_corrblock_gradients_fmaps_and_coords(dtype):
+@pytest.mark.parametrize("dtype,W", [(torch.float32, 32), (torch.float16, 32), (torch.float16, 64)])
+def test_corrblock_gradients_fmaps_and_coords(dtype, W):
     """CorrBlock forward + backward: gradients to both feature maps and to the coordinates
     against the FP64 oracle (lookup adjoint per level, then the pyramid backward) on the
     operands the tensor cores multiplied."""
     from vipe_b200.droid_corr import CorrBlock, CorrSampler
 
     g = torch.Generator().manual_seed(17)
-    B, N, C, H, W = 1, 2, 64, 16, 32
+    B, N, C, H = 1, 2, 64, 16  # W = 64 with 16-bit maps: full-row tiles, A operand read from fmap1
     f1 = (torch.randn(B, N, C, H, W, generator=g) / 2).to(dtype).cuda().requires_grad_()
     f2 = (torch.randn(B, N, C, H, W, generator=g) / 2).to(dtype).cuda().requires_grad_()
     coords = _grid_coords(B * N, H, W, g, 1.5).permute(0, 2, 3, 1).reshape(B, N, H, W, 2)
