@@ -1518,8 +1518,22 @@ __global__ void ba_tape_factor_kernel(BAPtrs base, Batch B) {
     BA_BIND(B, base);
     if (w.status[0]) return;
     const long nH = (long)d.dim * d.dim, nL = (long)((d.dim + 31) / 32) * 32 * 32;
-    for (long q = threadIdx.x; q < nH; q += blockDim.x) io.ftape[q] = w.Hm[q];
-    for (long q = threadIdx.x; q < nL; q += blockDim.x) io.ftape[nH + q] = w.linv[q];
+    // four independent loads in flight per thread before their stores (a plain copy is
+    // latency-bound at one CTA per graph)
+    const long stride = blockDim.x;
+    auto copy = [&](double* __restrict__ dst, const double* __restrict__ src, long n) {
+        long q = threadIdx.x;
+        for (; q + 3 * stride < n; q += 4 * stride) {
+            const double v0 = src[q], v1 = src[q + stride], v2 = src[q + 2 * stride], v3 = src[q + 3 * stride];
+            dst[q] = v0;
+            dst[q + stride] = v1;
+            dst[q + 2 * stride] = v2;
+            dst[q + 3 * stride] = v3;
+        }
+        for (; q < n; q += stride) dst[q] = src[q];
+    };
+    copy(io.ftape, w.Hm, nH);
+    copy(io.ftape + nH, w.linv, nL);
     if (threadIdx.x == 0) io.ftape[nH + nL] = (double)w.meta[4];
 }
 
