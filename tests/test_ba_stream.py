@@ -17,6 +17,12 @@ def test_split_clips_contiguous_and_nonempty(G, parts):
     rnd = random.Random(G * 1000 + parts)
     for _ in range(20):
         ne = [rnd.randint(0, 400) for _ in range(G)]
+        for taper in (1.0, 0.25):
+            r = split_clips(ne, parts, taper)
+            assert len(r) == min(parts, G)
+            assert r[0][0] == 0 and r[-1][1] == G
+            assert all(a < b for a, b in r)
+            assert all(r[i][1] == r[i + 1][0] for i in range(len(r) - 1))
         r = split_clips(ne, parts)
         assert len(r) == min(parts, G)
         assert r[0][0] == 0 and r[-1][1] == G
@@ -28,6 +34,17 @@ def test_split_clips_balances_edges():
     ne = [100] * 64
     r = split_clips(ne, 8)
     assert [b - a for a, b in r] == [8] * 8
+
+
+def test_split_clips_taper_shrinks_the_end_parts():
+    ne = [100] * 64
+    r = split_clips(ne, 8, taper=0.25)
+    sizes = [b - a for a, b in r]
+    assert len(sizes) == 8 and sum(sizes) == 64
+    # the end parts hold about 0.25 / 6.5 of the edges each (cuts fall on whole graphs)
+    assert max(sizes[0], sizes[-1]) <= 3
+    assert all(s > max(sizes[0], sizes[-1]) for s in sizes[1:-1])
+    assert split_clips(ne, 2, taper=0.25) == split_clips(ne, 2)  # fewer than 3 parts: no taper
 
 
 @pytest.mark.gpu

@@ -34,19 +34,29 @@ OUTPUT_KEYS = ("poses", "disps", "grad_poses", "grad_disps", "grad_targets", "gr
                "grad_disps_sens")
 
 
-def split_clips(num_edges, parts: int) -> list[tuple[int, int]]:
+def split_clips(num_edges, parts: int, taper: float = 1.0) -> list[tuple[int, int]]:
     """Cuts graphs 0..G-1 into at most ``parts`` non-empty ranges of consecutive
-    graphs with about equal edge totals (each graph's edges + 1, so edge-free
-    graphs still count)."""
+    graphs with edge totals (each graph's edges + 1, so edge-free graphs still
+    count) in proportion to the part weights: 1 for every part, ``taper`` for the
+    first and the last of three or more.  A small first part starts the solves
+    sooner (its copy-in is the only one nothing overlaps) and a small last part
+    ends the step sooner (likewise its copy-out)."""
     G = len(num_edges)
     parts = max(1, min(int(parts), G))
     w = [int(e) + 1 for e in num_edges]
     total = sum(w)
+    pw = [1.0] * parts
+    if parts >= 3:
+        pw[0] = pw[-1] = float(taper)
+    bounds, run = [], 0.0
+    for x in pw:
+        run += x
+        bounds.append(run / sum(pw))  # cumulative share ending each part
     cuts, acc, k = [0], 0, 1
     for g in range(G):
         acc += w[g]
         left = G - (g + 1)  # graphs after this one; every remaining part needs one
-        if k < parts and left >= parts - k and (acc >= total * k / parts or left == parts - k):
+        if k < parts and left >= parts - k and (acc >= total * bounds[k - 1] or left == parts - k):
             cuts.append(g + 1)
             k += 1
     cuts.append(G)
@@ -74,7 +84,7 @@ class StreamedBundleAdjust:
 
     def __init__(self, sizes, ht: int, wd: int, device, parts: int = 8, iterations: int = 4, lm: float = 1e-4,
                  ep: float = 0.1, alpha: float = 0.001, edge_chunks: int = 0, frame_chunks: int = 0,
-                 group: str = "se3", adjoint: bool = True):
+                 group: str = "se3", adjoint: bool = True, taper: float = 0.25):
         num_frames, num_edges, num_kx, t0, t1 = (list(map(int, x)) for x in sizes)
         self.device = torch.device(device)
         if self.device.type == "cuda" and self.device.index is None:
@@ -90,7 +100,7 @@ class StreamedBundleAdjust:
         self.parts: list[_Part] = []
         HW = (self.ht, self.wd)
         f0 = e0 = k0 = 0
-        for ga, gb in split_clips(num_edges, parts):
+        for ga, gb in split_clips(num_edges, parts, taper):
             nf, ne, nk = sum(num_frames[ga:gb]), sum(num_edges[ga:gb]), sum(num_kx[ga:gb])
             plan = BatchPlan(num_frames[ga:gb], num_edges[ga:gb], num_kx[ga:gb], t0[ga:gb], t1[ga:gb], self.ht,
                              self.wd, self.device, edge_chunks=edge_chunks, frame_chunks=frame_chunks,
