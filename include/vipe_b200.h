@@ -134,7 +134,10 @@ int vipe_slam_ba(float* poses_io, float* disps_io, float* intrinsics_io, const f
  *     about 12 MiB.
  *   - The first call on a device looks up the scratch's device address there
  *     (cudaGetSymbolAddress, which loads the library's module on that device);
- *     make that first call before any stream capture.
+ *     make that first call before any stream capture.  The address is kept for
+ *     the life of the process, so the device must not be reset
+ *     (cudaDeviceReset) between calls.
+ *   - Invalid sizes give the same status codes as vipe_slam_ba_extended.
  *   - Every call on a device shares the one array and the next call overwrites
  *     it: calls whose work overlaps on the GPU (different streams, or
  *     concurrent host threads) race and must be serialised by the caller. */
@@ -224,16 +227,23 @@ int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const float* tap
                                 float* grad_targets, float* grad_weights, float* grad_eta, float* grad_disps_sens,
                                 int32_t* dev_status, void* stream);
 
-/* Debug view of the device-built graph index (bit-exact tests).  Runs only the
+/* Debug view of the device-built graph index (bit-exact tests against the
+ * reference's host-side index: _unique/kk_exp geom_kernels.cu:1649-1656, the
+ * accum CSR :1043-1089, the Schur pair enumeration :1440-1468).  Runs only the
  * index construction of vipe_slam_ba_extended into `workspace` and copies:
  *   kx_out (num_kx) int64 — sorted unique depth frames
  *   kk_out (t1-t0+num_edges) int64 — inverse map of cat(arange(t0,t1), ii)
  *   pair_out: up to pair_cap (a, b) pose pairs (int32, local ids) that receive
  *   a Schur block, sorted; *num_pairs gets the count.
+ *   csr_ptr_out (num_kx+1), csr_idx_out (num_edges) int64, optional (both or
+ *   neither): the device's per-depth-row edge lists — the edges whose source
+ *   frame is kx[s], ascending — i.e. the CSR of the reference's
+ *   accum_cuda(., ii, kx) (geom_kernels.cu:1766-1785).
  * Synchronises `stream`. */
 int vipe_slam_ba_index_debug(const int64_t* ii, const int64_t* jj, int num_frames, int num_edges, int num_kx, int t0,
                              int t1, int64_t* kx_out, int64_t* kk_out, int32_t* pair_out, int pair_cap,
-                             int* num_pairs, void* workspace, size_t workspace_bytes, void* stream);
+                             int* num_pairs, int64_t* csr_ptr_out, int64_t* csr_idx_out, void* workspace,
+                             size_t workspace_bytes, void* stream);
 
 /* Replaces slam_ext.frame_distance (reference: geom_kernels.cu:613-768,
  * 1849-1877).  poses (num_poses,7), disps (num_disps,ht,wd), intrinsics

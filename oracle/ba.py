@@ -35,6 +35,10 @@ def lib():
         _lib.oracle_set_threads.restype = None
         _lib.oracle_set_threads.argtypes = [I]
         _lib.oracle_set_threads(1)
+        _lib.oracle_accum_csr.restype = I
+        _lib.oracle_accum_csr.argtypes = [L, L, I, I, I, L, L]
+        _lib.oracle_set_backsub_all_rows.restype = None
+        _lib.oracle_set_backsub_all_rows.argtypes = [I]
     return _lib
 
 
@@ -51,9 +55,12 @@ def _p(a, t):
 
 
 def ba(p, *, fp64: bool, motion_only=False, optimize_intrinsics=False, intrinsics_lm=1e-6, intrinsics_ep=1e-6,
-       intrinsics_scale=1.0, compute_energy=False, iterations=None, lm=None, ep=None, alpha=None):
+       intrinsics_scale=1.0, compute_energy=False, iterations=None, lm=None, ep=None, alpha=None,
+       backsub_all_rows=False):
     """Runs the oracle on a workloads.BAProblem-like object (CPU tensors or arrays).
 
+    backsub_all_rows=True keeps the depth back-substitution rows of pose t0, which the
+    reference's fused kernel skips (geom_kernels.cu:1186) and its generic solver keeps.
     Returns dict(poses, disps, intrinsics, dx, dz, energy) as float64 arrays.
     """
     poses = _d(np.asarray(p.poses, dtype=np.float64)).copy()
@@ -76,6 +83,7 @@ def ba(p, *, fp64: bool, motion_only=False, optimize_intrinsics=False, intrinsic
     en = np.zeros(max(iters, 1))
     D = ctypes.c_double
     L = ctypes.c_int64
+    lib().oracle_set_backsub_all_rows(int(bool(backsub_all_rows)))
     rc = lib().oracle_ba(
         1 if fp64 else 0, _p(poses, D), _p(disps, D), _p(intr, D), _p(sens, D), _p(tg, D), _p(wt, D), _p(eta, D),
         _p(ii, L), _p(jj, L), _p(act, D), N, H, W, E, K, p.t0, p.t1, iters,
@@ -83,6 +91,7 @@ def ba(p, *, fp64: bool, motion_only=False, optimize_intrinsics=False, intrinsic
         p.alpha if alpha is None else alpha, int(optimize_intrinsics), intrinsics_lm, intrinsics_ep,
         intrinsics_scale, int(compute_energy), _p(dx, D), _p(dz, D), _p(en, D),
     )
+    lib().oracle_set_backsub_all_rows(0)
     if rc != 0:
         raise RuntimeError(f"oracle_ba failed with code {rc}")
     return dict(poses=poses, disps=disps, intrinsics=intr, dx=dx, dz=None if motion_only else dz,
@@ -112,3 +121,14 @@ def schur_pairs(ii, jj, t0, t1):
     tr = np.zeros(3 * n, dtype=np.int64)
     lib().oracle_schur_pairs(_p(ii, L), _p(jj, L), ii.shape[0], t0, t1, _p(pi, L), _p(pj, L), _p(tr, L))
     return pi, pj, tr.reshape(-1, 3)
+
+
+def accum_csr(ii, jj, t0, t1):
+    """(ptr, idx): the edges grouped by source depth frame, as accum_cuda(., ii, kx) builds them."""
+    ii = np.ascontiguousarray(np.asarray(ii), dtype=np.int64)
+    jj = np.ascontiguousarray(np.asarray(jj), dtype=np.int64)
+    L = ctypes.c_int64
+    ptr = np.zeros(t1 - t0 + ii.shape[0] + 1, dtype=np.int64)
+    idx = np.zeros(max(ii.shape[0], 1), dtype=np.int64)
+    K = lib().oracle_accum_csr(_p(ii, L), _p(jj, L), ii.shape[0], t0, t1, _p(ptr, L), _p(idx, L))
+    return ptr[:K + 1], idx[:ii.shape[0]]

@@ -39,6 +39,7 @@ namespace {
 
 // Number of host threads the oracle may use (set by oracle_set_threads).
 int g_threads = 1;
+int g_backsub_all_rows = 0;  // see oracle_set_backsub_all_rows
 
 // Static-chunked parallel for over [0, n) on g_threads std::threads (the
 // toolchain here ships no OpenMP runtime).
@@ -521,7 +522,7 @@ int run_ba(double* poses_io, double* disps_io, double* intr_io, const double* di
             std::vector<S> dwsum((size_t)K * HW, S(0));
             for (int r = 0; r < R; r++) {
                 const int64_t pr = ix.jj_exp[r] - t0;
-                if (pr <= 0 || pr >= P) continue;
+                if (pr < (g_backsub_all_rows ? 0 : 1) || pr >= P) continue;
                 const int k = (int)ix.kk_exp[r];
                 for (int p = 0; p < HW; p++) {
                     S s = 0;
@@ -625,5 +626,35 @@ long oracle_schur_pairs(const int64_t* ii, const int64_t* jj, int E, int t0, int
     }
     return (long)pi.size();
 }
+
+// CSR of accum_cuda(data, ix = ii, jx = kx) (geom_kernels.cu:1043-1089): for each
+// depth frame kx[s], the rows (edges) whose ii equals it, taken in argsort(ii)
+// order (a stable sort here: ascending edge index within a frame).  Returns the
+// number of depth frames; ptr_out (K+1), idx_out (E).
+int oracle_accum_csr(const int64_t* ii, const int64_t* jj, int E, int t0, int t1, int64_t* ptr_out,
+                     int64_t* idx_out) {
+    Index ix = build_index(ii, jj, E, t0, t1);
+    std::vector<int64_t> order(E);
+    for (int e = 0; e < E; e++) order[e] = e;
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return ii[a] < ii[b]; });
+    size_t i = 0;
+    int64_t n = 0;
+    ptr_out[0] = 0;
+    for (size_t j = 0; j < ix.kx.size(); j++) {
+        while (i < order.size() && ii[order[i]] <= ix.kx[j]) {
+            if (ii[order[i]] == ix.kx[j]) idx_out[n++] = order[i];
+            i++;
+        }
+        ptr_out[j + 1] = n;
+    }
+    return (int)ix.kx.size();
+}
+
+// Back-substitution rows: the reference's EvT6x1_kernel skips the rows whose
+// target pose is t0 (`idx <= 0`, geom_kernels.cu:1186), although pose t0 is
+// optimised.  all_rows = 1 restores them (the generic solver's Schur
+// back-substitution, vipe/slam/ba/solver.py:183-186, has no such skip); the
+// default 0 is the fused kernel's behaviour.
+void oracle_set_backsub_all_rows(int all_rows) { g_backsub_all_rows = all_rows ? 1 : 0; }
 
 }  // extern "C"

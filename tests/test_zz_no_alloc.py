@@ -5,8 +5,9 @@ memory (hosts that forbid allocation after start-up, and C/cgo/JNI bindings
 with no CUDA allocator of their own).  It runs on a 16 MiB scratch array built
 into the library instead of a caller-provided workspace.  These tests check
 that it gives the same answer as vipe_slam_ba_extended on two calls in a row
-(the second one reuses the scratch left by the first), and that a graph too
-large for the scratch is refused before anything is launched.
+(the second one reuses the scratch left by the first), that a call after one
+that left NaN across the scratch is unaffected, and that a graph too large for
+the scratch is refused before anything is launched.
 
 The file name sorts last so that a stop-at-first-failure run has already run
 every other test when it gets here.
@@ -22,7 +23,15 @@ from vipe_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 
-def _call(p, noalloc: bool):
+def _poisoned(p):
+    """Problem `p` with NaN targets and weights: a solve of it leaves NaN across the scratch."""
+    q = p.clone()
+    q.targets.fill_(float("nan"))
+    q.weights.fill_(float("nan"))
+    return q
+
+
+def _call(p, noalloc: bool, expect_ok: bool = True):
     """One ba_extended solve of problem `p` through the chosen C entry point."""
     lib = _lib.load()
     g = p.to("cuda")
@@ -45,7 +54,8 @@ def _call(p, noalloc: bool):
         rc = lib.vipe_slam_ba_extended(*args, ws.data_ptr(), ws_bytes, status.data_ptr(), stream)
     assert rc == 0, _lib.status_string(rc)
     torch.cuda.synchronize()
-    assert int(status.item()) == 0
+    if expect_ok:
+        assert int(status.item()) == 0
     return {k: v.cpu().double().numpy() for k, v in
             dict(poses=g.poses, disps=g.disps, dx=dx, dz=dz, energy=energy).items()}
 
@@ -67,6 +77,17 @@ def test_noalloc_matches_workspace_entry_on_consecutive_calls():
     second = _call(small, noalloc=True)  # runs on the scratch the first call left behind
     _assert_same(first, _call(big, noalloc=False))
     _assert_same(second, _call(small, noalloc=False))
+
+
+def test_noalloc_ignores_what_a_previous_call_left_in_the_scratch():
+    """A solve of NaN inputs fills the shared scratch with NaN; a following good call must not read
+    any of it (every scratch word it reads, it writes first)."""
+    big, small = W.ba_config1(), W.ba_config0()
+    _call(_poisoned(big), noalloc=True, expect_ok=False)
+    after = _call(small, noalloc=True)
+    for k, v in after.items():
+        assert np.all(np.isfinite(v)), k
+    _assert_same(after, _call(small, noalloc=False))
 
 
 def test_noalloc_rejects_graph_beyond_scratch():

@@ -54,7 +54,7 @@ _SIGS: dict[str, tuple] = {
         I,
         [P, P, P, P, P, P, P, P, P, P, P, P, P, I, F, F, F, P, P, P, P, P, P, P, P],
     ),
-    "vipe_slam_ba_index_debug": (I, [P, P, I, I, I, I, I, P, P, P, I, P, P, SZ, P]),
+    "vipe_slam_ba_index_debug": (I, [P, P, I, I, I, I, I, P, P, P, I, P, P, P, P, SZ, P]),
     "vipe_slam_frame_distance": (I, [P, P, P, P, P, P, P, P, I, I, I, I, I, I, F, P, P]),
     "vipe_slam_projmap": (I, [P, P, P, P, P, I, I, I, I, P, P, P]),
     "vipe_slam_depth_filter": (I, [P, P, P, P, P, I, I, I, I, P, P]),

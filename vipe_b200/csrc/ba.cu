@@ -2224,8 +2224,9 @@ extern "C" int vipe_slam_ba(float* poses_io, float* disps_io, float* intrinsics_
 
 extern "C" int vipe_slam_ba_index_debug(const int64_t* ii, const int64_t* jj, int num_frames, int num_edges,
                                         int num_kx, int t0, int t1, int64_t* kx_out, int64_t* kk_out,
-                                        int32_t* pair_out, int pair_cap, int* num_pairs, void* workspace,
-                                        size_t workspace_bytes, void* stream) {
+                                        int32_t* pair_out, int pair_cap, int* num_pairs, int64_t* csr_ptr_out,
+                                        int64_t* csr_idx_out, void* workspace, size_t workspace_bytes,
+                                        void* stream) {
     int rc = check_dims(num_frames, 1, 1, num_edges, num_kx, t0, t1);
     if (rc != VIPE_OK) return rc;
     cudaStream_t st = as_stream(stream);
@@ -2246,16 +2247,24 @@ extern "C" int vipe_slam_ba_index_debug(const int64_t* ii, const int64_t* jj, in
     VIPE_CUDA_TRY(cudaStreamSynchronize(st));
     if (status) return status;
     const int K = d.K, E = d.E, P = d.P;
-    std::vector<int> kx(K), rank(num_frames), fp_ptr(K + 1), fp_list(E + K + 1);
+    std::vector<int> kx(K), rank(num_frames), fp_ptr(K + 1), fp_list(E + K + 1), fe_ptr(K + 1), fe_list(E + 1);
     std::vector<int64_t> iih(E);
     VIPE_CUDA_TRY(cudaMemcpy(kx.data(), w.kx, K * sizeof(int), cudaMemcpyDeviceToHost));
     VIPE_CUDA_TRY(cudaMemcpy(rank.data(), w.rank, num_frames * sizeof(int), cudaMemcpyDeviceToHost));
     VIPE_CUDA_TRY(cudaMemcpy(fp_ptr.data(), w.fp_ptr, (K + 1) * sizeof(int), cudaMemcpyDeviceToHost));
     VIPE_CUDA_TRY(cudaMemcpy(fp_list.data(), w.fp_list, (E + K + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+    VIPE_CUDA_TRY(cudaMemcpy(fe_ptr.data(), w.fe_ptr, (K + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+    if (E > 0) VIPE_CUDA_TRY(cudaMemcpy(fe_list.data(), w.fe_list, E * sizeof(int), cudaMemcpyDeviceToHost));
     if (E > 0) VIPE_CUDA_TRY(cudaMemcpy(iih.data(), ii, E * sizeof(int64_t), cudaMemcpyDeviceToHost));
     for (int s = 0; s < K; s++) kx_out[s] = kx[s];
     for (int t = 0; t < P; t++) kk_out[t] = rank[t0 + t];
     for (int e = 0; e < E; e++) kk_out[P + e] = rank[iih[e]];
+    // the device's per-depth-row edge lists, i.e. the CSR of the reference's accum_cuda(., ii, kx)
+    // (the edges whose source frame is kx[s], geom_kernels.cu:1766-1785)
+    if (csr_ptr_out && csr_idx_out) {
+        for (int s = 0; s <= K; s++) csr_ptr_out[s] = fe_ptr[s];
+        for (int x = 0; x < E; x++) csr_idx_out[x] = fe_list[x];
+    }
     std::vector<char> seen((size_t)P * P, 0);
     for (int s = 0; s < K; s++)
         for (int x = fp_ptr[s]; x < fp_ptr[s + 1]; x++)

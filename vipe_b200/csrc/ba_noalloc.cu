@@ -8,6 +8,7 @@
 // vipe_slam_ba_extended_noalloc runs the same solve with its scratch in a
 // file-scope device array of VIPE_BA_NOALLOC_SCRATCH_BYTES, which every GPU
 // that loads this library holds until the process exits.
+#include "ba_internal.cuh"
 #include "common.cuh"
 
 #include <cstdio>
@@ -25,7 +26,10 @@ std::mutex g_scratch_mu;
 void* g_scratch_ptr[kMaxDevices] = {nullptr};
 
 // Device address of g_ba_scratch on the current device, looked up once per
-// device (the first call on a device therefore loads this module there).
+// device (the first call on a device therefore loads this module there).  The
+// cached address belongs to that device's primary context: a device reset
+// (cudaDeviceReset) between calls would invalidate it, so callers of this entry
+// point must not reset the device while the library is loaded.
 int scratch_on_current_device(void** out) {
     int dev = 0;
     VIPE_CUDA_TRY(cudaGetDevice(&dev));
@@ -57,6 +61,9 @@ extern "C" int vipe_slam_ba_extended_noalloc(float* poses_io, float* disps_io, f
                                              float intrinsics_lm, float intrinsics_ep, float intrinsics_scale,
                                              int compute_energy, float* dx_out, float* dz_out, float* energy_out,
                                              int32_t* dev_status, void* stream) {
+    // the same size checks, with the same status codes, as vipe_slam_ba_extended
+    const int dims_rc = ba::check_dims(num_frames, ht, wd, num_edges, num_kx, t0, t1);
+    if (dims_rc != VIPE_OK) return dims_rc;
     const size_t need = vipe_slam_ba_workspace_size(num_frames, ht, wd, num_edges, num_kx, t0, t1);
     if (need == 0) return VIPE_ERR_ARG;
     if (need > (size_t)VIPE_BA_NOALLOC_SCRATCH_BYTES) {
