@@ -64,6 +64,11 @@ def parse():
     ap.add_argument("--no-corr", action="store_true")
     ap.add_argument("--e2e-parts", type=int, default=24,
                     help="host batch split into this many streamed parts for the end-to-end leg")
+    ap.add_argument("--case", choices=["ba0", "ba1", "corr_build", "batch", "lookup"],
+                    help="run one workload --reps times and exit (for profiler captures; no JSON line)")
+    ap.add_argument("--clips", type=int, default=32)
+    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--edges", type=int, default=64)
     return ap.parse_args()
 
 
@@ -415,34 +420,50 @@ def lie_bench(dev, hbm_peak):
     return {"workload": "SE3 group ops, 16M elements, f32 (lietorch_ext kernels)", "ops": out}
 
 
-def _cpu_clip_solves(sample_s, max_clips=256):
-    """Solves clips of the 256-clip batch one after another on the CPU oracle until
-    `sample_s` seconds have passed; returns (solves, seconds, threads)."""
+def _clip_order(G):
+    """A fixed shuffled order of the batch's clips, so that any prefix samples clip sizes evenly."""
+    import numpy as np
+
+    return np.random.default_rng(4242).permutation(G).tolist()
+
+
+def _cpu_clip_solves(b, sample_s, start=0, max_clips=256):
+    """Solves clips of batch `b` (the 256-clip batch) one after another on the CPU oracle, in a
+    fixed shuffled order from position `start`, forward only, until `sample_s` seconds have
+    passed; returns (solves, seconds, threads, next position)."""
     import oracle.ba as ob
-    from vipe_b200 import workloads as Wk
 
     threads = os.cpu_count() or 1
     ob.set_threads(threads)
-    b = Wk.ba_config4_se3(device="cpu", num_clips=24)  # the batch's first clips (same sizes and model)
-    ob.ba(b.clip(0), fp64=False, iterations=1)  # warm (builds the oracle if needed)
+    order = _clip_order(b.G)
+    clips = {}
+
+    def clip(g):
+        if g not in clips:
+            clips[g] = b.clip(g)
+        return clips[g]
+
+    ob.ba(clip(order[start % b.G]), fp64=False, iterations=1)  # warm (builds the oracle if needed)
     n, t0 = 0, time.perf_counter()
     while n < max_clips:
-        ob.ba(b.clip(n % b.G), fp64=False, iterations=4)
+        q = clip(order[(start + n) % b.G])
+        ob.ba(q, fp64=False, iterations=4)
         n += 1
         if time.perf_counter() - t0 >= sample_s:
             break
-    return n, time.perf_counter() - t0, threads
+    return n, time.perf_counter() - t0, threads, start + n
 
 
-def cpu_baseline(sample_s):
-    n, el, threads = _cpu_clip_solves(sample_s)
+def cpu_baseline(b, sample_s):
+    n, el, threads, _ = _cpu_clip_solves(b, sample_s)
     return {
         "value": n / el,
         "unit": "solves/s",
         "cores": threads,
         "kind": "port",
-        "sample": f"{n} clip solves cycling over the first 24 clips of the 256-clip batch, 4 LM iterations each, in {el:.1f} s "
-        f"(oracle/ba_oracle.cpp, FP32 per-edge math on {threads} threads, dense FP64 Cholesky)",
+        "sample": f"{n} clips of the 256-clip batch (fixed shuffled order), FORWARD solves only (4 LM iterations; "
+        f"the reference has no BA backward), in {el:.1f} s (oracle/ba_oracle.cpp: the reference's ba_cuda_impl "
+        f"restated, FP32 per-edge math on {threads} threads, dense FP64 Cholesky)",
     }
 
 
@@ -452,11 +473,18 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    per_step = 10.0
-    solves, secs = 0, 0.0
+    import torch
+
+    from vipe_b200 import workloads as Wk
+
+    # the same 256-clip batch as our arm (generated on the GPU when there is one: the generator's
+    # random streams are per device), solved clip by clip on the host cores
+    b = Wk.ba_config4_se3(device="cuda" if torch.cuda.is_available() else "cpu")
+    per_step = 6.0
+    solves, secs, pos = 0, 0.0, 0
     threads = os.cpu_count() or 1
     for k in range(max(0, args.warmup) + args.steps):
-        n, el, threads = _cpu_clip_solves(per_step if k >= args.warmup else 2.0, max_clips=64)
+        n, el, threads, pos = _cpu_clip_solves(b, per_step if k >= args.warmup else 1.0, start=pos, max_clips=64)
         if k >= args.warmup:
             solves += n
             secs += el
@@ -481,9 +509,10 @@ def run_reference(args):
             "unit": "solves/s",
             "cores": threads,
             "kind": "port",
-            "sample": f"{solves} clip solves of the 256-clip batch (each step solves clips for about {per_step:.0f} s; "
-            f"oracle/ba_oracle.cpp, the reference's ba_cuda_impl restated on the CPU; the reference extension "
-            f"needs Eigen and CUDA and is not built here)",
+            "sample": f"{solves} clips of the 256-clip batch in a fixed shuffled order, FORWARD solves only (the "
+            f"reference has no BA backward; each step solves clips for about {per_step:.0f} s; "
+            f"oracle/ba_oracle.cpp, the reference's ba_cuda_impl restated on the CPU: the reference's slam_ext "
+            f"needs Eigen 3.4, which is downloaded at build time, and cannot be built here)",
         },
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -495,7 +524,8 @@ def run_reference(args):
 
 # Measured DRAM traffic per edge of one launch (dram__bytes_read.sum + dram__bytes_write.sum
 # from an ncu capture of the first 32 clips of the same batch generator, mean over the LM
-# iterations' launches, divided by that case's 8938 edges; profiles/ba_kernels_traffic_32clips.md).
+# iterations' launches, divided by that case's 8938 edges; captured with
+# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum ... python bench.py --case batch --clips 32 --reps 1`).
 # Traffic grows with the edges (every edge-pixel is read once per launch), so a launch over this
 # batch moves about `per edge x edges`.
 TRAFFIC_PER_EDGE = {
@@ -548,7 +578,7 @@ def batched_leg(dev, args, world, dist, flush, stream):
         reset()
         cap.replay()
     torch.cuda.synchronize(dev)
-    n = max(3, args.steps // 2)
+    n = args.steps
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
     if world > 1:
         dist.barrier()
@@ -752,7 +782,7 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
         reset()
         fwd_adj()
     torch.cuda.synchronize(dev)
-    n = max(3, args.steps // 4)
+    n = args.steps
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
     if world > 1:
         dist.barrier()
@@ -788,7 +818,8 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
         roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                 "traffic": batch_kernel_traffic(b, name), "peak_source": src, "bytes_per_launch": nbytes,
                 "avg_launch_ms": avg_s * 1e3,
-                "note": "FP32-issue bound: HBM is the algorithmic bound, not the limiter (profiles/)"}
+                "note": "FP32-issue bound: HBM is the algorithmic bound, not the limiter (ncu: issue active "
+                        "57%, FMA pipe 40%, DRAM 12% of peak on the 32-clip case)"}
         break
 
     # end to end: pinned host inputs and incoming gradients in, outputs and all gradients out.
@@ -805,14 +836,14 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
     h2d = runner.h2d_bytes(host_in)
     d2h = runner.d2h_bytes(run_out)
     e2e = []
-    for k in range(4):
+    for k in range(max(3, args.warmup) + args.steps):
         a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         flush.fill_(float(k))
         a.record(stream)
         runner.step(host_in, host_g[0], host_g[1], run_out, stream=stream)
         c.record(stream)
         torch.cuda.synchronize(dev)
-        if k >= 1:
+        if k >= max(3, args.warmup):
             e2e.append(a.elapsed_time(c))
     stream_status = int((runner.status() != 0).sum().item())
     e2e_value = whole_job_rate(world, b.G * len(e2e), max_over_ranks(sum(e2e), world, dist, dev))
@@ -883,7 +914,7 @@ def sim3_leg(dev, args, flush, stream):
         reset()
         cap.replay()
     torch.cuda.synchronize(dev)
-    n = max(3, args.steps // 4)
+    n = args.steps
     ms = []
     for k in range(n):
         reset()
@@ -988,7 +1019,6 @@ def run_ours(args):
         fwd_value, fwd_e2e, extras, G, n_fwd, b = batched_leg(dev, args, world, dist, flush, stream)
         torch.cuda.empty_cache()
         adj = adjoint_leg(b, extras.pop("tune"), dev, args, world, dist, flush, stream)
-    del b
     value, e2e, n = adj["value"], adj.pop("e2e"), adj["steps"]
     extras["forward_only"] = {"value": fwd_value, "unit": "solves/s", "ms_per_batch": extras["batch_ms"],
                               "roofline": extras.pop("roofline"),
@@ -1042,7 +1072,7 @@ def run_ours(args):
             "lie": lie,
         }
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(args.cpu_sample_s)
+            line["cpu_baseline"] = cpu_baseline(b, args.cpu_sample_s)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -1050,8 +1080,123 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------- profiling cases
+# `python bench.py --case <name>` runs one workload --reps times on fresh inputs and exits 0 only if
+# every call succeeded: the command line that profiler captures run.
+#   ba0 / ba1     8 keyframes / 26 edges, 2 LM iterations; 64 keyframes / 628 edges, 4 iterations
+#   corr_build    --edges pairs of 128-channel 48x64 BF16 maps -> FP16 4-level pyramid
+#   batch         --clips clips of the uneven batch, forward (4 iterations, tape) + adjoint
+#   lookup        radius-3 lookups of --edges edges: volume (4 levels) and indexed
+
+import torch  # noqa: E402  (the cases below run under torch; the benchmark legs import it lazily)
+
+
+def case_ba(which: str, reps: int) -> None:
+    from vipe_b200 import workloads as W
+    from vipe_b200.ext import slam_ext
+
+    p = W.ba_config1() if which == "ba1" else W.ba_config0()
+    g0 = p.to("cuda")
+    for _ in range(reps):
+        q = g0.clone()
+        slam_ext.ba_extended(q.poses, q.disps, q.intrinsics, q.disps_sens, q.targets, q.weights, q.eta, q.ii, q.jj,
+                             q.depth_active, q.t0, q.t1, q.iterations, q.lm, q.ep, False, q.alpha, False, 1e-6, 1e-6,
+                             1.0, False)
+    torch.cuda.synchronize()
+
+
+def case_corr_build(edges: int, reps: int) -> None:
+    from vipe_b200.corr_build import corr_volume_pyramid
+
+    C, H, Wd = 128, 48, 64
+    g = torch.Generator(device="cuda").manual_seed(1002)
+    f1 = (torch.randn(edges, C, H, Wd, generator=g, device="cuda") / C**0.5).to(torch.bfloat16)
+    f2 = (torch.randn(edges, C, H, Wd, generator=g, device="cuda") / C**0.5).to(torch.bfloat16)
+    for _ in range(reps):
+        lv = corr_volume_pyramid(f1, f2, 4, out_dtype=torch.float16, check=True)
+        del lv
+    torch.cuda.synchronize()
+
+
+def case_lookup(edges: int, reps: int) -> None:
+    """FP16 pyramid of `edges` edges (128 ch, 48x64) looked up per level with corr_index_forward,
+    then the indexed on-the-fly lookup of the same edges over 16 frames' FP16 maps."""
+    import torch.nn.functional as F
+
+    from vipe_b200.corr_build import corr_volume_pyramid
+    from vipe_b200.ext import droid_net_ext as dne
+
+    C, H, Wd, Nf = 128, 48, 64, 16
+    g = torch.Generator(device="cuda").manual_seed(1002)
+    f1 = (torch.randn(edges, C, H, Wd, generator=g, device="cuda") / C**0.5).to(torch.bfloat16)
+    f2 = (torch.randn(edges, C, H, Wd, generator=g, device="cuda") / C**0.5).to(torch.bfloat16)
+    lv = corr_volume_pyramid(f1, f2, 4, out_dtype=torch.float16, check=True)
+    vols = [v.view(edges, H, Wd, H >> l, Wd >> l) for l, v in enumerate(lv)]
+    yy, xx = torch.meshgrid(torch.arange(H, device="cuda"), torch.arange(Wd, device="cuda"), indexing="ij")
+    coords = torch.stack([xx, yy], 0).float()[None] + 2.0 * torch.randn(edges, 2, 1, 1, generator=g, device="cuda")
+    coords = (coords + torch.randn(edges, 2, H, Wd, generator=g, device="cuda")).contiguous()
+    fm = (torch.randn(Nf, C, H, Wd, generator=g, device="cuda") / C**0.5).half() / 4.0
+    pyr, t = [], fm
+    for l in range(4):
+        pyr.append(t.permute(0, 2, 3, 1).contiguous().view(1, Nf, H >> l, Wd >> l, C))
+        t = F.avg_pool2d(t.float(), 2, stride=2).half()
+    e = torch.arange(edges, device="cuda")
+    ii, jj = e % Nf, (e % Nf + 1 + (e // Nf) % 7) % Nf
+    c5 = coords.permute(0, 2, 3, 1).reshape(1, edges, H, Wd, 2).contiguous()
+    for _ in range(reps):
+        for l in range(4):
+            dne.corr_index_forward(vols[l], (coords / 2**l).contiguous(), 3)
+        dne.altcorr_index_forward(pyr[0], pyr, c5, ii, jj, 3)
+    torch.cuda.synchronize()
+
+
+def case_batch(clips: int, reps: int) -> None:
+    from vipe_b200 import _lib
+    from vipe_b200 import workloads as W
+    from vipe_b200.ba_batch import BatchPlan
+
+    b = W.make_ba_batch(clips, seed=1004, device="cuda")
+    plan = BatchPlan(*b.sizes, b.ht, b.wd, "cuda", adjoint=True)
+    it = 4
+    tape = plan.make_tape(it)
+    T = b.tensors
+    g = torch.Generator(device="cuda").manual_seed(1005)
+    for _ in range(reps):
+        s = {k: v.clone() for k, v in T.items()}
+        _, _, _, st = plan.solve(**s, iterations=it, lm=1e-4, ep=0.1, tape=tape)
+        gp = torch.randn(plan.total_frames, 7, generator=g, device="cuda")
+        gp[:, 6] = 0
+        gd = torch.randn(plan.total_frames, b.ht, b.wd, generator=g, device="cuda")
+        out = [torch.empty_like(T[k]) for k in ("targets", "weights", "eta", "disps_sens")]
+        st2 = torch.zeros(plan.G, dtype=torch.int32, device="cuda")
+        rc = _lib.load().vipe_slam_ba_batch_backward(
+            plan._h, *[t.data_ptr() for t in tape], s["intrinsics"].data_ptr(), s["disps_sens"].data_ptr(),
+            s["targets"].data_ptr(), s["weights"].data_ptr(), s["eta"].data_ptr(), s["ii"].data_ptr(),
+            s["jj"].data_ptr(), s["depth_active"].data_ptr(), it, 1e-4, 0.1, 0.001, gp.data_ptr(), gd.data_ptr(),
+            *[o.data_ptr() for o in out], st2.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        _lib.check(rc, "batch backward")
+        torch.cuda.synchronize()
+        if int(st.abs().sum()) or int(st2.abs().sum()):
+            raise RuntimeError("device status set")
+
+
+def run_case(args):
+    if args.case in ("ba0", "ba1"):
+        case_ba(args.case, args.reps)
+    elif args.case == "batch":
+        case_batch(args.clips, args.reps)
+    elif args.case == "lookup":
+        case_lookup(args.edges, args.reps)
+    else:
+        case_corr_build(args.edges, args.reps)
+    print("ok")
+    return 0
+
+
 def main():
     args = parse()
+    if args.case:
+        return run_case(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
