@@ -97,9 +97,12 @@ size_t vipe_slam_ba_workspace_size(int num_frames, int ht, int wd, int num_edges
  *   VIPE_ERR_KX_MISMATCH / VIPE_ERR_CAPACITY found on the device (the call then
  *   leaves poses/disps untouched) or VIPE_WARN_SOLVER (dx = 0, as the reference
  *   does on Cholesky failure).
- * Capacity (VIPE_ERR_CAPACITY): t1 - t0 <= 127 window poses, and at most 31
- *   window poses (27 for Sim3) coupled to one depth frame (its own pose plus
- *   the distinct targets of its edges). */
+ * Capacity (VIPE_ERR_CAPACITY): t1 - t0 <= 1024 window poses (ViPE's keyframe
+ *   buffer: the backend's global BA over every keyframe).  Any number of window
+ *   poses may be coupled to one depth frame: frames coupled to more than 31 take
+ *   a wide-frame kernel instead of the tensor-core one, and reduced systems of
+ *   more than 768 unknowns a multi-launch blocked Cholesky.  The workspace grows
+ *   with the window (vipe_slam_ba_workspace_size). */
 int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* intrinsics_io, const float* disps_sens,
                           const float* targets, const float* weights, const float* eta, const int64_t* ii,
                           const int64_t* jj, const float* depth_active, int num_frames, int ht, int wd,
@@ -125,13 +128,13 @@ int vipe_slam_ba(float* poses_io, float* disps_io, float* intrinsics_io, const f
  * whose runtime has no CUDA allocator, cannot provide the workspace that
  * vipe_slam_ba_extended takes.  This entry point runs the same solve, with the
  * same arguments minus workspace/workspace_bytes, on a scratch array compiled
- * into the library: VIPE_BA_NOALLOC_SCRATCH_BYTES (16 MiB) of device memory on
+ * into the library: VIPE_BA_NOALLOC_SCRATCH_BYTES (32 MiB) of device memory on
  * every GPU that loads the library, held until the process exits.  It calls no
  * cudaMalloc/cudaFree.
  *   - Graphs whose vipe_slam_ba_workspace_size() exceeds the scratch are
  *     rejected with VIPE_ERR_CAPACITY before any launch (vipe_last_error()
  *     names both sizes).  A 64-keyframe 48x64 graph with 628 edges needs
- *     about 12 MiB.
+ *     about 16.4 MiB.
  *   - The first call on a device looks up the scratch's device address there
  *     (cudaGetSymbolAddress, which loads the library's module on that device);
  *     make that first call before any stream capture.  The address is kept for
@@ -141,7 +144,7 @@ int vipe_slam_ba(float* poses_io, float* disps_io, float* intrinsics_io, const f
  *   - Every call on a device shares the one array and the next call overwrites
  *     it: calls whose work overlaps on the GPU (different streams, or
  *     concurrent host threads) race and must be serialised by the caller. */
-#define VIPE_BA_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define VIPE_BA_NOALLOC_SCRATCH_BYTES (32u << 20)
 int vipe_slam_ba_extended_noalloc(float* poses_io, float* disps_io, float* intrinsics_io, const float* disps_sens,
                                   const float* targets, const float* weights, const float* eta, const int64_t* ii,
                                   const int64_t* jj, const float* depth_active, int num_frames, int ht, int wd,

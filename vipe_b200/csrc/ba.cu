@@ -218,8 +218,8 @@ __global__ void __launch_bounds__(kIndexThreads)
         if (lane == 0) {
             w.fe_ptr[s] = deg;
             w.fp_ptr[s] = m;
-            w.ftile_off[s] = npt_of(m, d.dof);
-            if (m > max_slots(d.dof)) atomicOr(&sh_flag, 2);
+            w.ftile_off[s] = m > max_slots(d.dof) ? 0 : npt_of(m, d.dof);  // wide frames: wtile
+            if (m > slot_cap(d)) atomicOr(&sh_flag, 2);
         }
     }
     __syncthreads();
@@ -237,6 +237,21 @@ __global__ void __launch_bounds__(kIndexThreads)
         w.meta[1] = w.fp_ptr[K];
         w.meta[2] = w.ftile_off[K];
         if ((long)w.ftile_off[K] > d.tile_cap) w.status[0] = VIPE_ERR_WORKSPACE;
+        // frames beyond the tensor-core kernel's slot limit, for the wide-frame kernel, and
+        // their Gram tiles' place in wtile
+        int nw = 0;
+        long wt = 0;
+        if (d.wide)
+            for (int s = 0; s < K; s++) {
+                const int ms = w.fp_ptr[s + 1] - w.fp_ptr[s];
+                w.wtile_off[s] = (int)wt;
+                if (ms > max_slots(d.dof)) {
+                    w.wide_list[nw++] = s;
+                    wt += npt_of(ms, d.dof);
+                }
+            }
+        w.meta[5] = nw;
+        if (wt > d.wtile_cap) w.status[0] = VIPE_ERR_WORKSPACE;
     }
     __syncthreads();
     if (w.status[0]) return;
@@ -340,7 +355,7 @@ __global__ void __launch_bounds__(kIndexThreads)
                 alpha = lo - w.fp_ptr[s];
             }
             const unsigned bal = __ballot_sync(0xffffffffu, hit);
-            if (hit) w.pf_list[pos + __popc(bal & lanemask_lt())] = s * 32 + alpha;
+            if (hit) w.pf_list[pos + __popc(bal & lanemask_lt())] = s * 1024 + alpha;  // alpha < P <= 1024
             pos += __popc(bal);
         }
     }
@@ -734,6 +749,7 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
     const int k = w.kx[s];
     const float act = A.depth_active[k];
     const int m = w.fp_ptr[s + 1] - w.fp_ptr[s];
+    if (m > max_slots(D)) return;  // a wide frame (single graphs only): ba_frame_wide_kernel's
     const int self = w.self_slot[s];
     const int eb = w.fe_ptr[s], ee = w.fe_ptr[s + 1];
     const int Dm = D * m, Dr = Dm + 2;
@@ -1079,6 +1095,206 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
     }
 }
 
+// ---------------------------------------------------------------- wide frames
+//
+// Depth frames coupled to more window poses than the tensor-core frame kernel's
+// accumulator holds (single graphs only: a backend window whose keyframes carry many
+// proximity and loop edges).  One cooperative launch walks the wide frames and their
+// pixel chunks in order.  For each (frame, chunk):
+//   1. every thread of the grid stages pixels: the frame kernel's linearisation and
+//      depth elimination, writing Q, w, Ef and the scaled rows
+//      e_p = act sqrt(Q_p) [slot couplings; w_p; Ef_p] entry-major into ebuf (plus the
+//      pixel's depth-prior energy in the row after them);
+//   2. after a grid barrier the CTAs share the 64 x 64 blocks of the chunk's Gram
+//      matrix sum_p e_p e_p^T (FP32 FMA, 4 x 4 register tiles over 32-pixel slabs),
+//      written as the frame kernel writes its chunk partials (upper-triangle 4 x 4
+//      tiles, zero outside the frame's entries); CTA 0 sums the energy row in pixel
+//      order;
+//   3. a second grid barrier frees ebuf for the next (frame, chunk).
+// Deterministic (fixed summation orders, no atomics).  The grid is sized to be
+// co-resident (cudaLaunchCooperativeKernel checks it), so the barriers always complete.
+constexpr int kWideThreads = 256;
+
+template <bool kIntr>
+__global__ void __launch_bounds__(kWideThreads) ba_frame_wide_kernel(BAPtrs base, Batch B, float alpha,
+                                                                     float iscale) {
+    BA_BIND(B, base);
+    constexpr int D = 6;
+    // both values are written before this launch and read by every CTA: uniform exits
+    if (w.status[0]) return;
+    const int nw = w.meta[5];
+    if (nw == 0) return;
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    const FrameArgs A{io.poses, io.disps, io.disps_sens, io.intr, io.targets, io.weights, io.eta, io.depth_active, io.jj,
+                      alpha, iscale};
+    __shared__ float As[kWideTile][33];
+    __shared__ float Bs[kWideTile][33];
+    __shared__ float red[kWideThreads / 32];
+    const int tid = threadIdx.x;
+    const int HW = d.HW, W = d.W, LD = d.chunk_f;
+    const float fx = A.intr[0], fy = A.intr[1], cx = A.intr[2], cy = A.intr[3];
+    const long gthreads = (long)gridDim.x * blockDim.x;
+    const long gtid = (long)blockIdx.x * blockDim.x + tid;
+    float* __restrict__ eb_ = w.ebuf;
+    for (int i = 0; i < nw; i++) {
+        const int s = w.wide_list[i];
+        const int k = w.kx[s];
+        const float act = A.depth_active[k];
+        const int m = w.fp_ptr[s + 1] - w.fp_ptr[s];
+        const int self = w.self_slot[s];
+        const int eb = w.fe_ptr[s], ee = w.fe_ptr[s + 1];
+        const int Dm = D * m, Dr = Dm + 2;
+        const int nt = (Dr + 3) / 4;
+        const int toff = w.wtile_off[s];
+        for (int c = 0; c < d.CF; c++) {
+            const int p0 = c * d.chunk_f, p1 = min(HW, p0 + d.chunk_f), np_ = p1 - p0;
+            // 1. staging
+            for (long pp = gtid; pp < np_; pp += gthreads) {
+                const int p = p0 + (int)pp;
+                const float u = (float)(p % W), v = (float)(p / W);
+                const float disp = A.disps[(size_t)k * HW + p];
+                const float dsens = __ldg(A.disps_sens + (size_t)k * HW + p);
+                const float eta_p = __ldg(A.eta + (size_t)s * HW + p);
+                for (int q = 0; q < Dm; q++) eb_[(size_t)q * LD + pp] = 0.f;
+                float es[D] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                float csum = 0.f, bsum = 0.f, efsum = 0.f;
+                for (int q = eb; q < ee; q++) {
+                    const int e = w.fe_list[q];
+                    const int b = (int)A.jj[e];
+                    const size_t o = (size_t)e * 2 * HW + p;
+                    EdgeTf Tf;
+                    edge_tf<D>(A.poses, k, b, Tf);
+                    const int sl = w.edge_slot[e];
+                    PixelLin L;
+                    linearize_d<D, kIntr, true>(Tf, b == k, fx, fy, cx, cy, u, v, disp, __ldg(A.weights + o),
+                                                __ldg(A.weights + o + HW), __ldg(A.targets + o),
+                                                __ldg(A.targets + o + HW), act, A.iscale, L);
+                    const float g0 = L.wd[0] * L.Jz[0], g1 = L.wd[1] * L.Jz[1];
+                    csum += g0 * L.Jz[0] + g1 * L.Jz[1];
+                    bsum += g0 * L.r[0] + g1 * L.r[1];
+                    if (kIntr) efsum += g0 * L.Jf[0] + g1 * L.Jf[1];
+                    float ej[D], ei[D];
+#pragma unroll
+                    for (int n = 0; n < D; n++) ej[n] = g0 * L.Jj[0][n] + g1 * L.Jj[1][n];
+                    adj_t(Tf.t, Tf.q, ej, ei);  // source rows are -Ad^T(Tij) of the target rows
+                    if (self >= 0) {
+#pragma unroll
+                        for (int n = 0; n < D; n++) es[n] -= ei[n];
+                    }
+                    if (sl >= 0) {
+                        if (sl == self) {
+#pragma unroll
+                            for (int n = 0; n < D; n++) es[n] += ej[n];
+                        } else {
+#pragma unroll
+                            for (int n = 0; n < D; n++) eb_[(size_t)(D * sl + n) * LD + pp] += ej[n];
+                        }
+                    }
+                }
+                if (self >= 0) {
+#pragma unroll
+                    for (int n = 0; n < D; n++) eb_[(size_t)(D * self + n) * LD + pp] = es[n];
+                }
+                const float msk = (dsens > 0.f ? 1.f : 0.f) * act;
+                const float C = act * (csum + eta_p + msk * A.alpha) + (1.f - act);
+                const float Q = 1.f / C;
+                const float dd = disp - dsens;
+                const float wv = act * (bsum - msk * A.alpha * dd);
+                const float Ef = efsum * act;
+                float* qwf = w.qwf + ((size_t)s * HW + p) * 3;
+                qwf[0] = Q;
+                qwf[1] = wv;
+                qwf[2] = Ef;
+                if (io.ftape) tape_qw(io.ftape, d)[(size_t)s * HW + p] = make_float2(Q, wv);
+                const float sq = sqrtf(Q);
+                const float scale = act * sq;
+                for (int q = 0; q < Dm; q++) eb_[(size_t)q * LD + pp] *= scale;
+                eb_[(size_t)Dm * LD + pp] = sq * wv;
+                eb_[(size_t)(Dm + 1) * LD + pp] = sq * Ef;
+                eb_[(size_t)(Dm + 2) * LD + pp] = msk * A.alpha * dd * dd;
+            }
+            __threadfence();
+            grid.sync();
+            // 2. Gram blocks (bi <= bj) of the chunk
+            const int nb = (Dr + kWideTile - 1) / kWideTile;
+            const int nblk = nb * (nb + 1) / 2;
+            const int tr = tid >> 4, tcol = tid & 15;
+            for (int t = blockIdx.x; t < nblk; t += gridDim.x) {
+                int bi = 0, rem = t;
+                while (rem >= nb - bi) {
+                    rem -= nb - bi;
+                    bi++;
+                }
+                const int bj = bi + rem;
+                float acc[4][4];
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++) acc[r][q] = 0.f;
+                for (int q0 = 0; q0 < np_; q0 += 32) {
+                    for (int idx = tid; idx < kWideTile * 32; idx += kWideThreads) {
+                        const int r = idx >> 5, px = idx & 31;
+                        const int ra = bi * kWideTile + r, rb = bj * kWideTile + r;
+                        const bool inpx = q0 + px < np_;
+                        As[r][px] = (ra < Dr && inpx) ? eb_[(size_t)ra * LD + q0 + px] : 0.f;
+                        Bs[r][px] = (rb < Dr && inpx) ? eb_[(size_t)rb * LD + q0 + px] : 0.f;
+                    }
+                    __syncthreads();
+#pragma unroll 8
+                    for (int px = 0; px < 32; px++) {
+                        float a4[4], b4[4];
+#pragma unroll
+                        for (int r = 0; r < 4; r++) {
+                            a4[r] = As[4 * tr + r][px];
+                            b4[r] = Bs[4 * tcol + r][px];
+                        }
+#pragma unroll
+                        for (int r = 0; r < 4; r++)
+#pragma unroll
+                            for (int q = 0; q < 4; q++) acc[r][q] += a4[r] * b4[q];
+                    }
+                    __syncthreads();
+                }
+                const int ti = bi * (kWideTile / 4) + tr, cg = bj * (kWideTile / 4) + tcol;
+                if (ti < nt && cg < nt && cg >= ti) {
+                    // the tile's running sum over chunks: this thread owns it in every chunk
+                    // (same work-item mapping), the grid barriers order the chunks
+                    const int tau = ti * nt - (ti * (ti - 1)) / 2 + (cg - ti);
+                    float* dst = w.wtile + ((size_t)(toff + tau)) * 16;
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
+                        const int row = 4 * ti + r;
+                        float4 o;
+                        o.x = (row < Dr && 4 * cg + 0 < Dr) ? acc[r][0] : 0.f;
+                        o.y = (row < Dr && 4 * cg + 1 < Dr) ? acc[r][1] : 0.f;
+                        o.z = (row < Dr && 4 * cg + 2 < Dr) ? acc[r][2] : 0.f;
+                        o.w = (row < Dr && 4 * cg + 3 < Dr) ? acc[r][3] : 0.f;
+                        if (c > 0) {
+                            const float4 pr = *reinterpret_cast<const float4*>(dst + r * 4);
+                            o.x += pr.x; o.y += pr.y; o.z += pr.z; o.w += pr.w;
+                        }
+                        *reinterpret_cast<float4*>(dst + r * 4) = o;
+                    }
+                }
+            }
+            if (blockIdx.x == 0) {
+                float en = 0.f;
+                for (int pp = tid; pp < np_; pp += kWideThreads) en += eb_[(size_t)(Dm + 2) * LD + pp];
+                en = warp_sum(en);
+                if ((tid & 31) == 0) red[tid >> 5] = en;
+                __syncthreads();
+                if (tid == 0) {
+                    float tsum = 0.f;
+                    for (int q = 0; q < kWideThreads / 32; q++) tsum += red[q];
+                    w.fen[(size_t)s * d.CF + c] = tsum;
+                }
+            }
+            __threadfence();
+            grid.sync();  // 3. ebuf is rewritten by the next (frame, chunk)
+        }
+    }
+}
+
 // entry (R, C) of frame s's Schur-augmented matrix, summed over pixel chunks
 __device__ __forceinline__ double frame_entry(const Work& w, const Dims& d, int s, int m, int R, int C) {
     const int nt = (d.dof * m + 2 + 3) / 4;
@@ -1088,6 +1304,8 @@ __device__ __forceinline__ double frame_entry(const Work& w, const Dims& d, int 
         t = rr; rr = cc; cc = t;
     }
     const int tau = r4 * nt - (r4 * (r4 - 1)) / 2 + (c4 - r4);
+    if (m > max_slots(d.dof))  // a wide frame: one tile holds the sum over chunks
+        return (double)w.wtile[((size_t)(w.wtile_off[s] + tau)) * 16 + rr * 4 + cc];
     const float* src = w.spart + ((size_t)(w.ftile_off[s] + tau)) * d.CF * 16 + rr * 4 + cc;
     double acc = 0.0;
     for (int c = 0; c < d.CF; c++) acc += (double)src[(size_t)c * 16];
@@ -1153,7 +1371,7 @@ __global__ void __launch_bounds__(256, 8) ba_assemble_blocks(BAPtrs base, Batch 
     if (with_frames) {
         for (int q = w.pf_ptr[a]; q < w.pf_ptr[a + 1]; q++) {
             const int ent = w.pf_list[q];
-            const int s = ent >> 5, al = ent & 31;
+            const int s = ent >> 10, al = ent & 1023;
             const int be = (a == b) ? al : find_slot(w, s, b);
             if (be < 0) continue;
             const int m = w.fp_ptr[s + 1] - w.fp_ptr[s];
@@ -1197,7 +1415,7 @@ __global__ void ba_assemble_rhs(BAPtrs base, Batch B, int with_frames, int with_
             if (with_frames) {
                 for (int q = w.pf_ptr[a]; q < w.pf_ptr[a + 1]; q++) {
                     const int ent = w.pf_list[q];
-                    const int s = ent >> 5, al = ent & 31;
+                    const int s = ent >> 10, al = ent & 1023;
                     const int m = w.fp_ptr[s + 1] - w.fp_ptr[s];
                     acc -= frame_entry(w, d, s, m, D * al + r, D * m + (isV ? 0 : 1));
                 }
@@ -1512,6 +1730,200 @@ __global__ void __launch_bounds__(kCholThreads, 1)
     }
 }
 
+// ---------------------------------------------------------------- multi-launch Cholesky
+//
+// A single graph whose reduced system (n > kPanelRows unknowns, up to 6 x 1024 + 1)
+// does not fit the staged panel: the same damped LL^T and solve, blocked over 32-column
+// panels, one launch per step (the host knows n, so every grid is exact):
+//   ba_chol_big_damp    diag += ep + lm diag (iep + ilm diag for the focal row), clears
+//                       the failure flag;
+//   ba_chol_big_panel   panel kb: every CTA factors the 32 x 32 diagonal block in shared
+//                       memory (identical arithmetic, so identical results), then solves
+//                       its 64 rows of the panel below, X = A L_kk^-T, and applies the
+//                       forward substitution to them (b_r -= X_r y_k with y_k = L_kk^-1 b_k);
+//                       CTA 0 writes L_kk, its inverse and y_k;
+//   ba_chol_big_update  the trailing lower triangle, A_ij -= X_i X_j^T, one 64 x 64 block
+//                       per CTA (FP64, 4 x 4 register tiles);
+//   ba_chol_big_solve   one CTA: the backward substitution L^T x = y with the inverse
+//                       diagonal blocks, then dx, the focal step and the status.
+// A non-positive pivot sets the flag; later launches see it and the solve returns
+// dx = 0 with VIPE_WARN_SOLVER, as the single-launch kernel does.
+constexpr int kBigRows = 64;
+
+__global__ void ba_chol_big_damp(BAPtrs base, Batch B, float lm, float ep, float ilm, float iep, int with_intr) {
+    BA_BIND(B, base);
+    if (w.status[0]) return;
+    const int n = with_intr ? d.dim : d.dim - 1;
+    const int np = d.dof * d.P;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) w.meta[4] = 0;
+    if (i < n) {
+        double* a = w.Hm + (size_t)i * d.dim + i;
+        *a = damped(*a, i >= np, lm, ep, ilm, iep);
+    }
+}
+
+__global__ void __launch_bounds__(kCholThreads) ba_chol_big_panel(BAPtrs base, Batch B, int kb, int with_intr) {
+    BA_BIND(B, base);
+    if (w.status[0] || w.meta[4]) return;
+    constexpr int LDR = kNB + 2;
+    __shared__ double pT[kNB * LDR];  // the diagonal block, transposed (pT[c * LDR + r])
+    __shared__ double Li[kNB][kNB + 1];
+    __shared__ double dinv[kNB];
+    __shared__ double ysh[kNB];
+    __shared__ int fail;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = with_intr ? d.dim : d.dim - 1;
+    const int ld = d.dim;
+    double* A = w.Hm;
+    double* x = w.bv;
+    const int k0 = kb * kNB, kn = min(kNB, n - k0);
+    for (int q = tid; q < kNB * kNB; q += kCholThreads) {
+        const int r = q / kNB, c = q % kNB;
+        pT[c * LDR + r] = (r < kn && c < kn) ? A[(size_t)(k0 + r) * ld + k0 + c] : 0.0;
+    }
+    if (tid == 0) fail = 0;
+    __syncthreads();
+    if (warp == 0) {
+        const bool bad = chol_diag_block(pT, LDR, kn, lane, Li, dinv);
+        if (bad && lane == 0) fail = 1;
+    }
+    __syncthreads();
+    if (fail) {
+        if (blockIdx.x == 0 && tid == 0) w.meta[4] = 1;
+        return;
+    }
+    // y_k = L_kk^-1 b_k (b_k is final: earlier panels have updated it, this launch does not)
+    if (tid < kNB) {
+        double y = 0.0;
+        for (int t = 0; t <= tid; t++) y += Li[tid][t] * (t < kn ? x[k0 + t] : 0.0);
+        ysh[tid] = tid < kn ? y : 0.0;
+    }
+    __syncthreads();
+    if (blockIdx.x == 0) {
+        for (int q = tid; q < kNB * kNB; q += kCholThreads) {
+            const int r = q / kNB, c = q % kNB;
+            w.linv[(size_t)kb * kNB * kNB + q] = Li[r][c];
+            if (r < kn && c < kn && c <= r) A[(size_t)(k0 + r) * ld + k0 + c] = pT[c * LDR + r];
+        }
+        if (tid < kn) w.yv[k0 + tid] = ysh[tid];
+    }
+    // this CTA's rows of the panel below the diagonal block
+    const int r0 = k0 + kn + blockIdx.x * kBigRows;
+    for (int rr = warp; rr < kBigRows; rr += kCholThreads / 32) {
+        const int r = r0 + rr;
+        if (r >= n) break;
+        const double a = lane < kn ? A[(size_t)r * ld + k0 + lane] : 0.0;
+        // X[r][c] = sum_{t <= c} A[r][t] Li[c][t]: lane c gathers A[r][t] by shuffle
+        double xr = 0.0;
+        for (int t = 0; t < kNB; t++) {
+            const double at = __shfl_sync(0xffffffffu, a, t);
+            if (t <= lane) xr += at * Li[lane][t];
+        }
+        if (lane < kn) A[(size_t)r * ld + k0 + lane] = xr;
+        double sy = lane < kn ? xr * ysh[lane] : 0.0;
+        sy = warp_sum(sy);
+        if (lane == 0) x[r] -= sy;
+    }
+}
+
+__global__ void __launch_bounds__(256) ba_chol_big_update(BAPtrs base, Batch B, int kb, int with_intr) {
+    BA_BIND(B, base);
+    if (w.status[0] || w.meta[4]) return;
+    __shared__ double Xi[kBigRows][kNB + 1];
+    __shared__ double Xj[kBigRows][kNB + 1];
+    const int tid = threadIdx.x;
+    const int n = with_intr ? d.dim : d.dim - 1;
+    const int ld = d.dim;
+    double* A = w.Hm;
+    const int k0 = kb * kNB, kn = min(kNB, n - k0);
+    const int base_r = k0 + kn;
+    const int nr = n - base_r;
+    const int nbt = (nr + kBigRows - 1) / kBigRows;
+    // block pair (bi >= bj) of the lower triangle, row-major
+    const int t = blockIdx.x;
+    int bi = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while (bi * (bi + 1) / 2 > t) bi--;
+    while ((bi + 1) * (bi + 2) / 2 <= t) bi++;
+    const int bj = t - bi * (bi + 1) / 2;
+    if (bi >= nbt) return;
+    const int ri = base_r + bi * kBigRows, rj = base_r + bj * kBigRows;
+    for (int q = tid; q < kBigRows * kNB; q += 256) {
+        const int r = q / kNB, c = q % kNB;
+        Xi[r][c] = (ri + r < n && c < kn) ? A[(size_t)(ri + r) * ld + k0 + c] : 0.0;
+        Xj[r][c] = (rj + r < n && c < kn) ? A[(size_t)(rj + r) * ld + k0 + c] : 0.0;
+    }
+    __syncthreads();
+    const int tr = tid >> 4, tc = tid & 15;
+    double acc[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[r][c] = 0.0;
+#pragma unroll 4
+    for (int tt = 0; tt < kNB; tt++) {
+        double a4[4], b4[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            a4[r] = Xi[4 * tr + r][tt];
+            b4[r] = Xj[4 * tc + r][tt];
+        }
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[r][c] += a4[r] * b4[c];
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int gi = ri + 4 * tr + r, gj = rj + 4 * tc + c;
+            if (gi < n && gj <= gi) A[(size_t)gi * ld + gj] -= acc[r][c];
+        }
+}
+
+__global__ void __launch_bounds__(1024) ba_chol_big_solve(BAPtrs base, Batch B, int with_intr) {
+    BA_BIND(B, base);
+    if (w.status[0]) return;
+    __shared__ double Li[kNB][kNB + 1];
+    __shared__ double ysh[kNB];
+    const int tid = threadIdx.x;
+    const int n = with_intr ? d.dim : d.dim - 1;
+    const int ld = d.dim;
+    const int np = d.dof * d.P;
+    const double* A = w.Hm;
+    double* x = w.bv;
+    const int fail = w.meta[4];
+    const int nblk = (n + kNB - 1) / kNB;
+    if (!fail) {
+        for (int i = tid; i < n; i += blockDim.x) x[i] = w.yv[i];
+        __syncthreads();
+        for (int kb = nblk - 1; kb >= 0; kb--) {
+            const int k0 = kb * kNB, kn = min(kNB, n - k0);
+            for (int q = tid; q < kNB * kNB; q += blockDim.x) Li[q / kNB][q % kNB] = w.linv[(size_t)kb * kNB * kNB + q];
+            __syncthreads();
+            double xv = 0.0;
+            if (tid < kn)
+                for (int t = tid; t < kn; t++) xv += Li[t][tid] * x[k0 + t];  // (L^-T)[tid][t] = Li[t][tid]
+            __syncthreads();
+            if (tid < kNB) ysh[tid] = tid < kn ? xv : 0.0;
+            if (tid < kn) x[k0 + tid] = xv;
+            __syncthreads();
+            for (int i = tid; i < k0; i += blockDim.x) {
+                double sacc = 0.0;
+                for (int t = 0; t < kn; t++) sacc += A[(size_t)(k0 + t) * ld + i] * ysh[t];
+                x[i] -= sacc;
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = tid; i < np; i += blockDim.x) io.dx[i] = fail ? 0.f : (float)x[i];
+    if (tid == 0) {
+        w.df[0] = (fail || !with_intr) ? 0.0 : x[np];
+        if (fail && io.status) atomicOr(io.status, VIPE_WARN_SOLVER);
+    }
+}
+
 // Copies the factor the Cholesky kernel left in Hm / linv (and its failure
 // flag) into this iteration's slot of the factor tape.  One CTA per graph.
 __global__ void ba_tape_factor_kernel(BAPtrs base, Batch B) {
@@ -1763,11 +2175,19 @@ int check_dims(int num_frames, int ht, int wd, int num_edges, int num_kx, int t0
 }
 
 bool g_smem_set[64] = {false};
+int g_wide_grid[64] = {0};  // co-resident CTAs of the wide-frame kernel (cooperative launch)
 
 int ensure_attributes() {
     int dev = 0;
     VIPE_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 64 && !g_smem_set[dev]) {
+        int sms = 0, per_sm_a = 0, per_sm_b = 0;
+        VIPE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        VIPE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_a, ba_frame_wide_kernel<false>,
+                                                                    kWideThreads, 0));
+        VIPE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_b, ba_frame_wide_kernel<true>,
+                                                                    kWideThreads, 0));
+        g_wide_grid[dev] = sms * std::max(1, std::min(2, std::min(per_sm_a, per_sm_b)));
         VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<true, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            kFrameSmem));
         VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<false, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1840,6 +2260,19 @@ int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const 
                 base, batch_of(geo, d_table, d_off, kOffFrame), a.alpha, a.iscale);
         VIPE_LAUNCH_CHECK();
     }
+    if (with_frames && geo.wide) {
+        // frames beyond the tensor-core kernel's slots (their CTAs above returned at once)
+        VIPE_PROF("ba_frame_wide", st);
+        int dev = 0;
+        VIPE_CUDA_TRY(cudaGetDevice(&dev));
+        BAPtrs b = base;
+        Batch bt = batch_of(geo, d_table, d_off, kOffFrame);
+        float alpha = a.alpha, iscale = a.iscale;
+        void* args[] = {&b, &bt, &alpha, &iscale};
+        const void* fn = intr ? (const void*)ba_frame_wide_kernel<true> : (const void*)ba_frame_wide_kernel<false>;
+        VIPE_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3((unsigned)g_wide_grid[dev < 64 ? dev : 0]),
+                                                  dim3(kWideThreads), args, 0, st));
+    }
     {
         VIPE_PROF("ba_assemble", st);
         ba_assemble_blocks<<<grid(kOffPairs), 256, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffPairs),
@@ -1853,6 +2286,28 @@ int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const 
         VIPE_PROF("ba_energy", st);
         ba_energy_kernel<<<G, 256, 0, st>>>(base, per_graph, with_frames, itr);
         VIPE_LAUNCH_CHECK();
+    }
+    if (geo.chol_big) {
+        VIPE_PROF("ba_cholesky", st);
+        const Batch one{d_table, nullptr, 1};
+        const int n = intr ? geo.dim : geo.dim - 1;
+        const int wi = intr ? 1 : 0;
+        ba_chol_big_damp<<<ceil_div(n, 256), 256, 0, st>>>(base, one, a.lm, a.ep, a.ilm, a.iep, wi);
+        VIPE_LAUNCH_CHECK();
+        const int nblk = (n + kNB - 1) / kNB;
+        for (int kb = 0; kb < nblk; kb++) {
+            const int k0 = kb * kNB, kn = std::min(kNB, n - k0), nr = n - k0 - kn;
+            ba_chol_big_panel<<<std::max(1u, ceil_div(nr, kBigRows)), kCholThreads, 0, st>>>(base, one, kb, wi);
+            VIPE_LAUNCH_CHECK();
+            if (nr > 0) {
+                const unsigned nbt = ceil_div(nr, kBigRows);
+                ba_chol_big_update<<<nbt * (nbt + 1) / 2, 256, 0, st>>>(base, one, kb, wi);
+                VIPE_LAUNCH_CHECK();
+            }
+        }
+        ba_chol_big_solve<<<1, 1024, 0, st>>>(base, one, wi);
+        VIPE_LAUNCH_CHECK();
+        return VIPE_OK;
     }
     {
         VIPE_PROF("ba_cholesky", st);
@@ -1988,7 +2443,7 @@ using namespace vipe::ba;
 extern "C" size_t vipe_slam_ba_workspace_size(int num_frames, int ht, int wd, int num_edges, int num_kx, int t0,
                                               int t1) {
     if (check_dims(num_frames, ht, wd, num_edges, num_kx, t0, t1) != VIPE_OK) return 0;
-    Dims d = make_dims(num_frames, ht, wd, num_edges, num_kx, t0, t1);
+    Dims d = make_dims(num_frames, ht, wd, num_edges, num_kx, t0, t1, 0, 0, 6, true);
     Sizer s;
     carve_single(s, d, nullptr);
     return s.used + 256;
@@ -2022,7 +2477,7 @@ extern "C" int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* in
     if (rc != VIPE_OK) return rc;
     cudaStream_t st = as_stream(stream);
     GraphDesc gd{};
-    gd.d = make_dims(num_frames, ht, wd, num_edges, num_kx, t0, t1);
+    gd.d = make_dims(num_frames, ht, wd, num_edges, num_kx, t0, t1, 0, 0, 6, true);
     Carver cv(workspace, workspace_bytes);
     GraphDesc* table = carve_single(cv, gd.d, &gd.w);
     if (!cv.ok) return VIPE_ERR_WORKSPACE;
@@ -2231,7 +2686,7 @@ extern "C" int vipe_slam_ba_index_debug(const int64_t* ii, const int64_t* jj, in
     if (rc != VIPE_OK) return rc;
     cudaStream_t st = as_stream(stream);
     GraphDesc gd{};
-    gd.d = make_dims(num_frames, 1, 1, num_edges, num_kx, t0, t1);
+    gd.d = make_dims(num_frames, 1, 1, num_edges, num_kx, t0, t1, 0, 0, 6, true);
     const Dims& d = gd.d;
     const Work& w = gd.w;
     Carver cv(workspace, workspace_bytes);

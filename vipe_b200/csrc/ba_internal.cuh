@@ -11,9 +11,13 @@
 namespace vipe {
 namespace ba {
 
-constexpr int kMaxSlots = 31;          // window poses coupled to one depth frame (SE3; Sim3: 27):
-                                       // 2 x (accumulator columns) of the frame kernel <= 512
-constexpr int kMaxPoses = 127;         // t1 - t0: 6P+1 unknowns fit the staged Cholesky panel
+constexpr int kMaxSlots = 31;          // window poses coupled to one depth frame that the tensor-core
+                                       // frame kernel takes (SE3; Sim3: 27): 2 x (accumulator
+                                       // columns) <= 512; a single graph's wider frames take the
+                                       // wide-frame kernel, a batch refuses them
+constexpr int kMaxPoses = 1024;        // t1 - t0 of a single graph (the index kernel's pose bitmask);
+                                       // batches: 6P+1 unknowns must fit the staged Cholesky panel
+constexpr int kWideTile = 64;          // output block of the wide-frame Gram product
 constexpr int kNT = 105;               // per-edge terms, see term layout below
 constexpr int kEdgeThreads = 256;
 constexpr int kFrameThreads = 128;     // one pixel per thread; 32-pixel blocks per warp
@@ -33,9 +37,12 @@ struct Dims {
     int N, H, W, HW, E, K, t0, t1, P, dim;
     int CHe, chunk_e;  // edge kernel pixel chunks
     int CF, chunk_f;   // frame kernel pixel chunks
-    long tile_cap;     // capacity of frame SYRK tiles
+    long tile_cap;     // capacity of frame SYRK tiles (tensor-core frames, per pixel chunk)
+    long wtile_cap;    // capacity of wide-frame Gram tiles (summed over pixel chunks)
     int adj;           // 1: the workspace also holds the adjoint buffers
     int dof;           // pose tangent size: 6 (SE3) or 7 (Sim3)
+    int wide;          // 1: depth frames may couple more than max_slots window poses (single SE3
+                       // graphs with P > max_slots): those frames take the wide-frame kernel
 };
 
 // Per-edge term layouts for pose tangent size `dof`:
@@ -77,6 +84,11 @@ struct Work {
     double* bv;      // dim
     double* df;      // 1
     double* linv;    // inverse diagonal blocks of the Cholesky factor
+    double* yv;      // dim: forward-substitution result of the multi-launch Cholesky
+    int* wide_list;  // K: depth rows whose slot count exceeds max_slots (wide frames), ascending
+    float* ebuf;     // (dof * P + 3) x chunk_f: one wide frame's scaled rows e_p over one pixel chunk
+    int* wtile_off;  // K + 1: first Gram tile of each wide frame in wtile
+    float* wtile;    // wtile_cap x 16: wide frames' upper-triangle 4 x 4 Gram tiles, all chunks summed
     // adjoint (carved only when Dims::adj)
     double* adj_gT;    // N * 6   running left-tangent gradient of every pose
     double* adj_rhs;   // dim     g_dxi, then g_dxi - E~ Q g_dz
@@ -93,9 +105,19 @@ __host__ __device__ inline int npt_of(int m, int dof = 6) {
     return nt * (nt + 1) / 2;
 }
 
+// slots (window poses) a depth frame of graph d may couple: the tensor-core frame kernel's
+// limit, or any number up to the window for graphs that take the wide-frame kernel
+__host__ __device__ inline int slot_cap(const Dims& d) { return d.wide ? d.P : max_slots(d.dof); }
+
+// rows of the wide-frame staging buffer: one frame's entries at most, plus one row of
+// per-pixel depth-prior energies
+__host__ __device__ inline long wide_rows(const Dims& d) { return d.wide ? (long)d.dof * d.P + 3 : 0; }
+
 // che / cf: pixel-chunk counts of the per-edge and per-frame kernels; 0 picks
-// them so that one graph alone launches about two CTAs per SM.
-inline Dims make_dims(int N, int H, int W, int E, int K, int t0, int t1, int che = 0, int cf = 0, int dof = 6) {
+// them so that one graph alone launches about two CTAs per SM.  single: a graph
+// solved on its own (not in a batch), which may hold wide frames.
+inline Dims make_dims(int N, int H, int W, int E, int K, int t0, int t1, int che = 0, int cf = 0, int dof = 6,
+                      bool single = false) {
     Dims d;
     d.N = N; d.H = H; d.W = W; d.HW = H * W; d.E = E; d.K = K; d.t0 = t0; d.t1 = t1;
     d.P = t1 - t0;
@@ -112,13 +134,18 @@ inline Dims make_dims(int N, int H, int W, int E, int K, int t0, int t1, int che
     chunk = ((chunk + 255) / 256) * 256;
     d.chunk_f = chunk;
     d.CF = (d.HW + chunk - 1) / chunk;
-    // Upper bound of sum over frames of npt(m_s): slots are <= max_slots per
-    // frame and sum_s m_s <= E + K.  npt(m) <= (a m + 3.25)^2 / 2, a = dof / 4.
-    const int M = std::max(1, std::min(max_slots(dof), d.P));
-    const double a = dof / 4.0;
-    double b1 = (double)K * npt_of(M, dof);
-    double b2 = (a * M + 3.25) / 2.0 * (a * (double)(E + K) + 3.25 * K);
-    d.tile_cap = (long)std::min(b1, b2) + K + 1;
+    d.wide = (single && dof == 6 && d.P > max_slots(dof)) ? 1 : 0;
+    // Upper bound of sum over frames of npt(m_s): slots are <= M per frame and
+    // sum_s m_s <= E + K.  npt(m) <= (a m + 3.25)^2 / 2, a = dof / 4.
+    auto tiles_bound = [&](int M) {
+        M = std::max(1, std::min(M, d.P));
+        const double a = dof / 4.0;
+        const double b1 = (double)K * npt_of(M, dof);
+        const double b2 = (a * M + 3.25) / 2.0 * (a * (double)(E + K) + 3.25 * K);
+        return (long)std::min(b1, b2) + K + 1;
+    };
+    d.tile_cap = tiles_bound(max_slots(dof));
+    d.wtile_cap = d.wide ? tiles_bound(d.P) : 1;
     d.adj = 0;
     return d;
 }
@@ -156,6 +183,11 @@ inline void carve(C& c, const Dims& d, Work* w) {
     auto pb = c.template take<double>((size_t)d.dim);
     auto pdf = c.template take<double>(4);
     auto pli = c.template take<double>((size_t)((d.dim + 31) / 32) * 32 * 32);
+    auto pyv = c.template take<double>((size_t)d.dim);
+    auto pwl = c.template take<int>(K + 1);
+    auto peb = c.template take<float>(d.wide ? (size_t)wide_rows(d) * d.chunk_f : 1);
+    auto pwo = c.template take<int>(K + 1);
+    auto pwt = c.template take<float>((size_t)d.wtile_cap * 16);
     if (w) {
         w->epart = (float*)pf;
         w->eterm = (double*)pd;
@@ -166,6 +198,11 @@ inline void carve(C& c, const Dims& d, Work* w) {
         w->bv = (double*)pb;
         w->df = (double*)pdf;
         w->linv = (double*)pli;
+        w->yv = (double*)pyv;
+        w->wide_list = (int*)pwl;
+        w->ebuf = (float*)peb;
+        w->wtile_off = (int*)pwo;
+        w->wtile = (float*)pwt;
         w->adj_gT = nullptr;
         w->adj_rhs = w->adj_lam = nullptr;
         w->adj_aslot = w->adj_gpart = nullptr;
@@ -376,6 +413,10 @@ struct Geometry {
     size_t chol_smem = 0;
     int chol_cluster = 1;  // CTAs (one cluster) per graph in the Cholesky launch
     bool any_edges = false;
+    bool chol_big = false;  // a single graph whose reduced system exceeds the staged panel:
+                            // multi-launch blocked Cholesky
+    bool wide = false;      // a single graph that may hold wide frames
+    int dim = 0;            // reduced-system size of a single graph
 };
 
 inline void fill_geometry(const std::vector<Dims>& dims, Geometry& geo) {
@@ -387,10 +428,13 @@ inline void fill_geometry(const std::vector<Dims>& dims, Geometry& geo) {
         const int cnt[kNumOff] = {d.E * d.CHe, d.E, d.K * d.CF, (int)ceil_div(npairs, 8), (int)ceil_div(d.P + 1, 8),
                                   (int)ceil_div(d.P, 128)};
         for (int k = 0; k < kNumOff; k++) geo.off[k][g + 1] = geo.off[k][g] + cnt[k];
-        geo.chol_smem = std::max(geo.chol_smem, (size_t)chol_ldr(d.dim) * kNB * sizeof(double));
+        geo.chol_big = dims.size() == 1 && d.dim > kPanelRows;
+        if (!geo.chol_big) geo.chol_smem = std::max(geo.chol_smem, (size_t)chol_ldr(d.dim) * kNB * sizeof(double));
         // a single large reduced system splits its trailing updates over a cluster of
         // CTAs (batches already fill the GPU with one CTA per graph)
         geo.chol_cluster = dims.size() == 1 ? (d.dim >= 256 ? 8 : (d.dim >= 128 ? 4 : 1)) : 1;
+        geo.wide = dims.size() == 1 && d.wide;
+        geo.dim = d.dim;
         geo.any_edges |= d.E > 0;
         geo.dof = d.dof;
     }

@@ -257,6 +257,42 @@ def ba_config1() -> BAProblem:
     return make_ba_problem(64, edges, seed=1001, t0=2, iterations=4)
 
 
+def ba_backend(n_frames: int = 256, hub_every: int = 16, hub_degree: int = 40, ht: int = 48, wd: int = 64,
+               seed: int = 1005, iterations: int = 2, t0: int = 1) -> BAProblem:
+    """A backend-style global BA window: every keyframe in [t0, n_frames) optimised,
+    edges |i-j| <= 3 plus, from every `hub_every`-th keyframe, `hub_degree` loop pairs
+    (|i-j| > 8, both directions) to random keyframes, so the hubs' depth frames are
+    coupled to hub_degree + 7 window poses (the shape proximity and loop-closure factors
+    give ViPE's backend, vipe/slam/components/factor_graph.py:376-486)."""
+    rng = np.random.default_rng(seed)
+    edges = band_edges(n_frames, 3)
+    have = set(edges)
+    for h in range(0, n_frames, hub_every):
+        far = [j for j in range(n_frames) if abs(j - h) > 8]
+        for j in rng.choice(far, size=min(hub_degree, len(far)), replace=False).tolist():
+            for e in ((h, j), (j, h)):
+                if e not in have:
+                    have.add(e)
+                    edges.append(e)
+    scale = wd / 64.0
+    return make_ba_problem(n_frames, edges, seed=seed, ht=ht, wd=wd, t0=t0, iterations=iterations,
+                           intrinsics=(60.0 * scale, 60.0 * scale, wd / 2.0, ht / 2.0))
+
+
+def frame_slots(p: BAProblem) -> np.ndarray:
+    """Window poses coupled to each depth frame of `p` (its own pose, if in the window, and the
+    distinct in-window targets of its edges), in the order of the sorted depth frames."""
+    ii, jj = p.ii.numpy(), p.jj.numpy()
+    kx = np.unique(np.concatenate([np.arange(p.t0, p.t1), ii]))
+    out = []
+    for k in kx:
+        s = {int(j) for j in jj[ii == k] if p.t0 <= j < p.t1}
+        if p.t0 <= k < p.t1:
+            s.add(int(k))
+        out.append(len(s))
+    return np.array(out)
+
+
 def ba_small(n_frames: int = 6, ht: int = 12, wd: int = 16, radius: int = 2, seed: int = 7, iterations: int = 2,
              t0: int = 1) -> BAProblem:
     """A reduced-size problem with the same generative model (fast CPU oracle cases)."""
