@@ -376,6 +376,23 @@ int vipe_altcorr_index_backward(int dtype, const void* fmap1, const void* const*
                                 int radius, int exact_coords_grad, float* fmap1_grad_out,
                                 float* const* level_grads_out, float* coords_grad_out, void* stream);
 
+/* Channels-last feature pyramid of AltCorrBlock (reference: eager torch,
+ * vipe/slam/networks/droid_net.py:130-142): level l of fmaps / 4 average-pooled
+ * l times (2x2, floor sizes), each level rounded to the element type before the
+ * next pools it, FP32 window sums in avg_pool2d's order — bit-identical to the
+ * reference's levels.  fmaps (num, C, H, W); level_out[l] (num, H>>l, W>>l, C),
+ * 16-byte aligned; dtype VIPE_F32, VIPE_F16 or VIPE_BF16; 1 <= num_levels <= 4;
+ * C a multiple of 8 (16-bit) or 4 (FP32), at most 256. */
+int vipe_corr_pyramid_nhwc(int dtype, const void* fmaps, int num, int C, int H, int W, int num_levels,
+                           void* const* level_out, void* stream);
+
+/* Adjoint of vipe_corr_pyramid_nhwc (the reference differentiates the eager ops
+ * through torch autograd): level_grads[l] (num, H>>l, W>>l, C) FP32 ->
+ * fmaps_grad_out (num, C, H, W) in dtype, written completely (FP32 sums, one
+ * rounding). */
+int vipe_corr_pyramid_nhwc_backward(int dtype, const float* const* level_grads, int num, int C, int H, int W,
+                                    int num_levels, void* fmaps_grad_out, void* stream);
+
 /* All-pairs correlation volume with its average-pooled pyramid — the build of
  * CorrBlock (vipe/slam/networks/droid_net.py:56-69,94-102): for each of the
  * `num` pairs, level l holds avg_pool^l((fmap1/4)^T (fmap2/4)) over the target

@@ -63,3 +63,21 @@ def test_argument_checks_run_before_any_device_work():
     assert call(C=512) == _lib.VIPE_ERR_CAPACITY
     assert call(r=4) == _lib.VIPE_ERR_CAPACITY
     assert call(g1=null) == _lib.VIPE_ERR_ARG
+
+
+def test_pyramid_and_window_checks_without_a_gpu():
+    """The feature-pyramid entry points reject level counts, channel counts and types before any
+    device work; the BA workspace query accepts windows of up to 1024 poses and refuses more."""
+    import ctypes
+
+    lib = _lib.load()
+    null = ctypes.c_void_p(0)
+    outs = (ctypes.c_void_p * 5)(16, 16, 16, 16, 16)
+    assert lib.vipe_corr_pyramid_nhwc(_lib.VIPE_F16, null, 1, 128, 48, 64, 5, outs, null) == _lib.VIPE_ERR_ARG
+    assert lib.vipe_corr_pyramid_nhwc(_lib.VIPE_F16, null, 1, 12, 48, 64, 4, outs, null) == _lib.VIPE_ERR_ARG
+    assert lib.vipe_corr_pyramid_nhwc(_lib.VIPE_F64, null, 1, 128, 48, 64, 4, outs, null) == _lib.VIPE_ERR_DTYPE
+    assert lib.vipe_corr_pyramid_nhwc(_lib.VIPE_F16, null, 1, 128, 4, 64, 4, outs, null) == _lib.VIPE_ERR_ARG
+    assert lib.vipe_corr_pyramid_nhwc_backward(_lib.VIPE_F32, null, 1, 128, 48, 64, 0, null, null) == \
+        _lib.VIPE_ERR_ARG
+    assert lib.vipe_slam_ba_workspace_size(1025, 8, 8, 3000, 1024, 1, 1025) > 0
+    assert lib.vipe_slam_ba_workspace_size(1026, 8, 8, 3000, 1025, 1, 1026) == 0

@@ -126,10 +126,3 @@ def test_backend_window_focal_and_motion_only():
     np.testing.assert_allclose(got["poses"], want["poses"], atol=5e-5, rtol=0)
     np.testing.assert_array_equal(got["disps"], p.disps.double().numpy())
 
-
-def test_window_capacity_limit():
-    from vipe_b200 import _lib
-
-    lib = _lib.load()
-    assert lib.vipe_slam_ba_workspace_size(1025, 8, 8, 3000, 1024, 1, 1025) > 0  # 1024 window poses
-    assert lib.vipe_slam_ba_workspace_size(1026, 8, 8, 3000, 1025, 1, 1026) == 0  # 1025: refused

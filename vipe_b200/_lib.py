@@ -66,6 +66,8 @@ _SIGS: dict[str, tuple] = {
     "vipe_altcorr_backward": (I, [P, P, P, P, I, I, I, I, I, I, I, I, I, P, P, P, P]),
     "vipe_altcorr_index_forward": (I, [I, P, P, P, P, I, P, P, P, I, I, I, I, I, I, I, P, P]),
     "vipe_altcorr_index_backward": (I, [I, P, P, P, P, I, P, P, P, P, I, I, I, I, I, I, I, I, P, P, P, P]),
+    "vipe_corr_pyramid_nhwc": (I, [I, P, I, I, I, I, I, P, P]),
+    "vipe_corr_pyramid_nhwc_backward": (I, [I, P, I, I, I, I, I, P, P]),
     "vipe_corr_volume_workspace_size": (SZ, [I, I, I, I]),
     "vipe_hbm_write_probe": (I, [P, SZ, P]),
     "vipe_corr_volume_build": (I, [I, I, P, P, I, I, I, I, I, P, P, SZ, P]),
@@ -88,6 +90,7 @@ VIPE_ERR_INDEX = 2
 VIPE_ERR_RANGE = 3
 VIPE_ERR_KX_MISMATCH = 4
 VIPE_ERR_CAPACITY = 6
+VIPE_ERR_DTYPE = 8
 VIPE_ERR_GROUP = 9
 VIPE_ERR_DEVICE_WAIT = 10
 VIPE_WARN_SOLVER = 16

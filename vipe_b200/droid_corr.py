@@ -17,7 +17,10 @@ can switch by import.  Differences from the reference:
     avg_pool2d passes);
   * AltCorrBlock's indexed lookup is differentiable (AltCorrIndex: gradients to
     the maps, the pyramid levels and optionally the coordinates); the
-    reference's has no backward.
+    reference's has no backward;
+  * AltCorrBlock's channels-last pyramid is one kernel (FeaturePyramid) with a
+    hand-written adjoint, instead of a division, three avg_pool2d passes and
+    four transposes.
 """
 
 from __future__ import annotations
@@ -208,22 +211,67 @@ class AltCorrIndex(torch.autograd.Function):
         return (gcoords, None, None, None, g1.to(fmap1.dtype), *[g.to(lv.dtype) for g, lv in zip(gl, levels)])
 
 
+def _pyramid_levels(fmaps, num_levels):
+    """(num, C, H, W) -> channels-last levels (num, H>>l, W>>l, C) of fmaps / 4 pooled l times."""
+    import ctypes
+
+    from . import _lib
+
+    _lib.require_cuda("fmaps", fmaps)
+    _lib.require_contiguous("fmaps", fmaps)
+    num, C, H, W = fmaps.shape
+    levels = [torch.empty(num, H >> l, W >> l, C, dtype=fmaps.dtype, device=fmaps.device) for l in range(num_levels)]
+    ptrs = (ctypes.c_void_p * num_levels)(*[t.data_ptr() for t in levels])
+    rc = _lib.load().vipe_corr_pyramid_nhwc(_lib.DTYPE_CODE[fmaps.dtype], fmaps.data_ptr(), num, C, H, W, num_levels,
+                                            ptrs, _lib.stream_of(fmaps))
+    _lib.check(rc, "AltCorrBlock pyramid")
+    return levels
+
+
+class FeaturePyramid(torch.autograd.Function):
+    """AltCorrBlock's channels-last pyramid (reference droid_net.py:130-142: fmaps / 4, three
+    avg_pool2d passes, four transposes) in one kernel, with a hand-written adjoint."""
+
+    @staticmethod
+    def forward(ctx, fmaps, num_levels):
+        ctx.shape = fmaps.shape
+        ctx.dtype = fmaps.dtype
+        return tuple(_pyramid_levels(fmaps, num_levels))
+
+    @staticmethod
+    def backward(ctx, *grads):
+        import ctypes
+
+        from . import _lib
+
+        num, C, H, W = ctx.shape
+        L = len(grads)
+        dev = grads[0].device if grads[0] is not None else None
+        gs = [(torch.zeros(num, H >> l, W >> l, C, device=dev) if g is None else g.float().contiguous())
+              for l, g in enumerate(grads)]
+        out = torch.empty(num, C, H, W, dtype=ctx.dtype, device=gs[0].device)
+        ptrs = (ctypes.c_void_p * L)(*[g.data_ptr() for g in gs])
+        rc = _lib.load().vipe_corr_pyramid_nhwc_backward(_lib.DTYPE_CODE[ctx.dtype], ptrs, num, C, H, W, L,
+                                                         out.data_ptr(), _lib.stream_of(out))
+        _lib.check(rc, "AltCorrBlock pyramid backward")
+        return out, None
+
+
 class AltCorrBlock:
     """Lookup without a materialised volume (reference droid_net.py:121-196).
 
     fmaps: (B, N, C, H, W).  The pyramid is fmaps / 4 average-pooled per level
-    and stored channels-last (B, N, H_l, W_l, C), floor sizes.
+    and stored channels-last (B, N, H_l, W_l, C), floor sizes, built by one kernel
+    (FeaturePyramid) whose levels equal the reference's bit for bit.
     """
 
     def __init__(self, fmaps, num_levels=4, radius=3):
         self.num_levels = num_levels
         self.radius = radius
         B, N, C, H, W = fmaps.shape
-        f = fmaps.view(B * N, C, H, W) / 4.0
-        self.pyramid = []
-        for i in range(num_levels):
-            self.pyramid.append(f.permute(0, 2, 3, 1).contiguous().view(B, N, H // 2**i, W // 2**i, C))
-            f = F.avg_pool2d(f, 2, stride=2)
+        f = fmaps.reshape(B * N, C, H, W).contiguous()
+        levels = FeaturePyramid.apply(f, num_levels)
+        self.pyramid = [lv.view(B, N, H >> i, W >> i, C) for i, lv in enumerate(levels)]
 
     def corr_fn_reference(self, coords, ii, jj):
         """Per-level on-the-fly lookup in fp32 (the reference's checking route)."""
