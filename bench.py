@@ -1001,6 +1001,55 @@ def plain_cfg1_leg(dev, args, flush, stream):
     }
 
 
+def backend_leg(dev, args, flush, stream):
+    """The plain drop-in on a backend-size window (ViPE's global BA, factor_graph.py:376-392):
+    256 keyframes at 48x64, t0 = 1 (a 1531-unknown reduced system: multi-launch blocked
+    Cholesky), |i-j| <= 3 plus 40 loop pairs from every 16th keyframe (wide frames coupled to
+    up to 52 window poses), 4 LM iterations; one graph per call."""
+    import torch
+
+    from vipe_b200 import _lib, workloads as Wk
+    from vipe_b200.ext import slam_ext as S
+
+    lib = _lib.load()
+    p = Wk.ba_backend(256, ht=48, wd=64, iterations=4)
+    g0 = p.to(dev)
+    S.CHECK_DEVICE_STATUS = False
+    for _ in range(2):
+        ba_call(S, g0.clone())
+    n = max(3, min(args.steps, 10))
+    states = [g0.clone() for _ in range(n)]
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+    torch.cuda.synchronize(dev)
+    for k in range(n):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        ba_call(S, states[k])
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in ev) / n
+    prof_states = [g0.clone() for _ in range(2)]
+    it = iter(prof_states)
+
+    def once():
+        flush.fill_(1.0)
+        ba_call(S, next(it))
+
+    prof = profile_kernels(lib, once, len(prof_states))
+    total = sum(v[0] for v in prof.values())
+    slots = Wk.frame_slots(p)
+    res = {
+        "workload": "plain FP32 drop-in slam_ext.ba_extended on a backend window: 256 keyframes 48x64 SE3, "
+        f"t0=1, {p.ii.shape[0]} edges (|i-j|<=3 + 40 loop pairs x2 from every 16th keyframe), 4 LM iterations",
+        "value": 1e3 / ms, "unit": "solves/s", "ms_per_solve": ms, "steps": n,
+        "reduced_system_unknowns": 6 * (p.t1 - p.t0) + 1,
+        "frames_beyond_tensor_core_slots": int((slots > 31).sum()), "max_slots": int(slots.max()),
+        "kernel_breakdown": {k: {"ms_per_solve": v[0] / 2, "share": v[0] / total} for k, v in prof.items()},
+    }
+    del states, prof_states, g0
+    return res
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -1026,6 +1075,8 @@ def run_ours(args):
     extras["speedup_fwd_adj_vs_plain_forward_same_gpu"] = value / extras["plain_same_gpu"]["value"]
     torch.cuda.empty_cache()
     plain = plain_cfg1_leg(dev, args, flush, stream)
+    torch.cuda.empty_cache()
+    backend = backend_leg(dev, args, flush, stream)
     torch.cuda.empty_cache()
     sim3 = sim3_leg(dev, args, flush, stream)
     hbm, bf16, src = measured_peaks()
@@ -1067,6 +1118,7 @@ def run_ours(args):
             "batched": extras,
             "adjoint": adj,
             "plain_cfg1": plain,
+            "plain_backend_256kf": backend,
             "sim3_batched": sim3,
             "corr": corr,
             "lie": lie,
