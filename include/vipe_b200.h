@@ -393,6 +393,29 @@ int vipe_corr_pyramid_nhwc(int dtype, const void* fmaps, int num, int C, int H, 
 int vipe_corr_pyramid_nhwc_backward(int dtype, const float* const* level_grads, int num, int C, int H, int W,
                                     int num_levels, void* fmaps_grad_out, void* stream);
 
+/* =====================================================================
+ * corr_ext — spatial correlation sampler of the AOT tracker's attention
+ * Bindings replaced: csrc/corr_ext/correlation_sampler.cpp:82-85 (forward,
+ * backward; kernels csrc/corr_ext/correlation_cuda_kernel.cu).
+ * ===================================================================== */
+
+/* out (num, patchH, patchW, oH, oW), oH = (H + 2 padH - ((kH-1) dilationH + 1)) / dH + 1
+ * (oW likewise): sum over channels and kernel taps of input1[y1][x1] * input2[y1 + s][x1 + t],
+ * y1 = oh dH - padH + i dilationH, s = ph dilation_patchH - dilation_patchH (patchH-1) / 2,
+ * terms outside either map skipped (the reference GPU forward's convention).  input1,
+ * input2 (num, C, H, W); dtype VIPE_F32, VIPE_F64, VIPE_F16 or VIPE_BF16 (FP32
+ * accumulation, FP64 for VIPE_F64). */
+int vipe_corr_sample_forward(int dtype, const void* input1, const void* input2, int num, int C, int H, int W, int kH,
+                             int kW, int patchH, int patchW, int padH, int padW, int dilationH, int dilationW,
+                             int dilation_patchH, int dilation_patchW, int dH, int dW, void* out, void* stream);
+
+/* Adjoint of vipe_corr_sample_forward: grad_output (num, patchH, patchW, oH, oW) ->
+ * grad_input1_out, grad_input2_out (num, C, H, W), written completely (gathers, no atomics). */
+int vipe_corr_sample_backward(int dtype, const void* input1, const void* input2, const void* grad_output, int num,
+                              int C, int H, int W, int kH, int kW, int patchH, int patchW, int padH, int padW,
+                              int dilationH, int dilationW, int dilation_patchH, int dilation_patchW, int dH, int dW,
+                              void* grad_input1_out, void* grad_input2_out, void* stream);
+
 /* All-pairs correlation volume with its average-pooled pyramid — the build of
  * CorrBlock (vipe/slam/networks/droid_net.py:56-69,94-102): for each of the
  * `num` pairs, level l holds avg_pool^l((fmap1/4)^T (fmap2/4)) over the target

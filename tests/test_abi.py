@@ -81,3 +81,30 @@ def test_pyramid_and_window_checks_without_a_gpu():
         _lib.VIPE_ERR_ARG
     assert lib.vipe_slam_ba_workspace_size(1025, 8, 8, 3000, 1024, 1, 1025) > 0
     assert lib.vipe_slam_ba_workspace_size(1026, 8, 8, 3000, 1025, 1, 1026) == 0
+
+
+def test_install_as_vipe_ext_registers_every_reference_module():
+    """`from vipe.ext import slam_ext, droid_net_ext, lietorch_ext, corr_ext` resolves to this
+    package's modules, with the reference's bound function names (slam.cpp:41-55,
+    droid.cpp:75-81, lietorch.cpp:306-336, correlation_sampler.cpp:82-85)."""
+    import sys
+
+    saved = {k: sys.modules.get(k) for k in list(sys.modules) if k == "vipe" or k.startswith("vipe.")}
+    try:
+        from vipe_b200.ext import install_as_vipe_ext
+
+        install_as_vipe_ext()
+        from vipe.ext import corr_ext, droid_net_ext, lietorch_ext, slam_ext  # noqa: F401
+
+        for name in ("ba", "ba_extended", "frame_distance", "projmap", "depth_filter", "iproj"):
+            assert callable(getattr(slam_ext, name))
+        for name in ("altcorr_forward", "altcorr_backward", "altcorr_index_forward", "corr_index_forward",
+                     "corr_index_backward"):
+            assert callable(getattr(droid_net_ext, name))
+        for name in ("expm", "logm", "inv", "mul", "adj", "adjT", "act", "act4", "as_matrix", "projector", "Jinv"):
+            assert callable(getattr(lietorch_ext, name))
+        assert callable(corr_ext.forward) and callable(corr_ext.backward)
+    finally:
+        for k in [k for k in sys.modules if k == "vipe" or k.startswith("vipe.")]:
+            del sys.modules[k]
+        sys.modules.update({k: v for k, v in saved.items() if v is not None})
