@@ -277,6 +277,23 @@ int vipe_slam_depth_filter(const float* poses, const float* disps, const float* 
 int vipe_slam_iproj(const float* poses, const float* disps, const float* intrinsics, int num_frames, int ht, int wd,
                     float* points_out, void* stream);
 
+/* Proximity-edge construction of the factor graph (reference: the host loops of
+ * FactorGraph.add_proximity_factors, vipe/slam/components/factor_graph.py:431-486),
+ * given the candidate distances.  Candidates are (i, j), i in [t0, t), j in [t1, t),
+ * row-major: d ((t-t0) x (t-t1)) f32, e.g. slam_ext.frame_distance of every pair.
+ * ii_exist, jj_exist (num_exist) int64: the graph's active then inactive edges.
+ * Emits into ii_out / jj_out (int64, out_cap >= vipe_slam_proximity_edges_capacity())
+ * exactly the reference's edge list, in its order: the neighbourhood edges, then the
+ * greedy NMS over candidates in ascending distance (ties in index order), and writes
+ * the count to *num_out (device int32).  One CTA; up to 1.7 M candidates (t = 1024,
+ * t0 = t1 = 0); workspace of vipe_slam_proximity_edges_workspace_size() bytes. */
+size_t vipe_slam_proximity_edges_workspace_size(int t0, int t1, int t);
+long vipe_slam_proximity_edges_capacity(int t0, int t1, int t, int rad, int max_factors, int cross_view);
+int vipe_slam_proximity_edges(const float* d, const int64_t* ii_exist, const int64_t* jj_exist, int num_exist, int t0,
+                              int t1, int t, int rad, int nms, float thresh, int max_factors, int cross_view,
+                              int64_t* ii_out, int64_t* jj_out, int out_cap, int* num_out, void* workspace,
+                              size_t workspace_bytes, void* stream);
+
 /* =====================================================================
  * lietorch_ext — group kernels.  group_id: 1 SO3, 2 RxSO3, 3 SE3, 4 Sim3
  * (reference dispatch: csrc/lietorch_ext/dispatch.h:17-50).  dtype VIPE_F32 or

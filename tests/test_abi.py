@@ -108,3 +108,17 @@ def test_install_as_vipe_ext_registers_every_reference_module():
         for k in [k for k in sys.modules if k == "vipe" or k.startswith("vipe.")]:
             del sys.modules[k]
         sys.modules.update({k: v for k, v in saved.items() if v is not None})
+
+
+def test_proximity_edge_checks_without_a_gpu():
+    import ctypes
+
+    lib = _lib.load()
+    null = ctypes.c_void_p(0)
+    assert lib.vipe_slam_proximity_edges_workspace_size(5, 6, 10) == 0  # t0 < t1
+    assert lib.vipe_slam_proximity_edges_capacity(0, 0, 10, 2, 48, 0) == 50
+    # more than 1.7 M candidates: refused before any device work
+    rc = lib.vipe_slam_proximity_edges(ctypes.c_void_p(16), null, null, 0, 0, 0, 1400, 2, 3, ctypes.c_float(22.0),
+                                       16 * 1400, 0, ctypes.c_void_p(16), ctypes.c_void_p(16), 1 << 20,
+                                       ctypes.c_void_p(16), ctypes.c_void_p(16), 1 << 30, null)
+    assert rc == _lib.VIPE_ERR_CAPACITY

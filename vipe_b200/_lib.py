@@ -70,6 +70,9 @@ _SIGS: dict[str, tuple] = {
     "vipe_corr_pyramid_nhwc_backward": (I, [I, P, I, I, I, I, I, P, P]),
     "vipe_corr_sample_forward": (I, [I, P, P] + [I] * 16 + [P, P]),
     "vipe_corr_sample_backward": (I, [I, P, P, P] + [I] * 16 + [P, P, P]),
+    "vipe_slam_proximity_edges_workspace_size": (SZ, [I, I, I]),
+    "vipe_slam_proximity_edges_capacity": (ctypes.c_long, [I, I, I, I, I, I]),
+    "vipe_slam_proximity_edges": (I, [P, P, P, I, I, I, I, I, I, F, I, I, P, P, I, P, P, SZ, P]),
     "vipe_corr_volume_workspace_size": (SZ, [I, I, I, I]),
     "vipe_hbm_write_probe": (I, [P, SZ, P]),
     "vipe_corr_volume_build": (I, [I, I, P, P, I, I, I, I, I, P, P, SZ, P]),
