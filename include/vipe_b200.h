@@ -443,6 +443,20 @@ int vipe_corr_sample_backward(int dtype, const void* input1, const void* input2,
  * The first int32 of `workspace` becomes nonzero if a bounded wait inside the
  * kernel expired (the output is then incomplete). */
 size_t vipe_corr_volume_workspace_size(int num, int C, int ht, int wd);
+
+/* Adjoint of vipe_corr_volume_build (the reference differentiates torch.matmul and
+ * avg_pool2d with autograd, droid_net.py:56-69,94-102): level_grads[l] (num, ht*wd,
+ * ht>>l, wd>>l) in grad_dtype (VIPE_F16, VIPE_BF16 or VIPE_F32) ->
+ * fmap1_grad_out = (1/16) fmap2 Gt^T and fmap2_grad_out = (1/16) fmap1 Gt, (num, C, ht,
+ * wd) FP32 (either may be NULL), Gt = sum_l unpool_l(G_l) / 4^l formed on the fly.
+ * fmap1, fmap2 (num, C, ht, wd) in map_dtype (VIPE_F16 / VIPE_BF16: the operands the
+ * forward multiplied).  tcgen05 tensor cores: kind::f16 for 16-bit gradients, kind::tf32
+ * with a hi + lo split of Gt for FP32 gradients.  C <= 128, ht*wd a multiple of 128, wd of
+ * 8, ht and wd of 2^(num_levels-1).  dev_status (device int32): set nonzero if a bounded
+ * wait expired (the gradients are then incomplete). */
+int vipe_corr_volume_backward(int map_dtype, int grad_dtype, const void* fmap1, const void* fmap2,
+                              const void* const* level_grads, int num, int C, int ht, int wd, int num_levels,
+                              float* fmap1_grad_out, float* fmap2_grad_out, int32_t* dev_status, void* stream);
 int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* fmap1, const void* fmap2, int num, int C, int ht,
                            int wd, int num_levels, void* const* level_out, void* workspace, size_t workspace_bytes,
                            void* stream);

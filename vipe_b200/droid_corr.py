@@ -13,8 +13,8 @@ can switch by import.  Differences from the reference:
     or zero coordinate gradient);
   * with autograd recording and a feature map that requires grad, the pyramid
     is built by CorrVolume, whose backward returns the feature-map gradients of
-    every level at once (the reference differentiates torch.matmul and the
-    avg_pool2d passes);
+    every level at once in two tcgen05 GEMMs (the reference differentiates
+    torch.matmul and the avg_pool2d passes);
   * AltCorrBlock's indexed lookup is differentiable (AltCorrIndex: gradients to
     the maps, the pyramid levels and optionally the coordinates); the
     reference's has no backward;
@@ -72,12 +72,11 @@ class CorrVolume(torch.autograd.Function):
 
     Backward, with G_l the level gradients, P_l the l-fold 2x2 average pool over
     the target axes and U_l its adjoint (each pooled value spread over its
-    2^l x 2^l block, divided by 4^l):
-        d fmap1 = 1/16 sum_l P_l(fmap2) G_l^T,   d fmap2 = 1/16 sum_l U_l(fmap1 G_l)
+    2^l x 2^l block, divided by 4^l), Gt = sum_l U_l(G_l):
+        d fmap1 = 1/16 fmap2 Gt^T,   d fmap2 = 1/16 fmap1 Gt
     taken at the rounded operands the forward multiplied (straight through the
-    rounding).  The products are plain batched GEMMs (cuBLAS through torch.bmm):
-    in the operand type when the level gradient already has it, else in FP32;
-    the levels are summed in FP32.
+    rounding): two tcgen05 GEMMs with K = H*W whose producer warps form Gt from
+    the level gradients on the fly (vipe_corr_volume_backward).
     """
 
     @staticmethod
@@ -90,28 +89,30 @@ class CorrVolume(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, *grads):
+        import ctypes
+
+        from . import _lib
+
         fmap1, fmap2 = ctx.saved_tensors
         num, C, H, W = fmap1.shape
-        f1 = fmap1.to(ctx.op).reshape(num, C, H * W)
-        f2 = fmap2.to(ctx.op)
-        g1 = torch.zeros(num, C, H * W, dtype=torch.float32, device=fmap1.device) if ctx.needs_input_grad[0] else None
-        g2 = torch.zeros(num, C, H, W, dtype=torch.float32, device=fmap1.device) if ctx.needs_input_grad[1] else None
-        for l, G in enumerate(grads):
-            if G is None:
-                continue
-            h, w = H >> l, W >> l
-            mm = G.dtype if G.dtype == ctx.op else torch.float32
-            G = G.reshape(num, H * W, h * w).to(mm)
-            if g1 is not None:
-                p2 = F.avg_pool2d(f2.float(), 2**l) if l else f2.float()
-                g1 += torch.bmm(p2.reshape(num, C, h * w).to(mm), G.transpose(1, 2)).float()
-            if g2 is not None:
-                m = torch.bmm(f1.to(mm), G).float().reshape(num, C, h, w)
-                if l:
-                    m = m.repeat_interleave(2**l, dim=2).repeat_interleave(2**l, dim=3) / float(4**l)
-                g2 += m
-        d1 = None if g1 is None else (g1 / 16.0).reshape(num, C, H, W).to(fmap1.dtype)
-        d2 = None if g2 is None else (g2 / 16.0).to(fmap2.dtype)
+        dev = fmap1.device
+        f1 = fmap1.to(ctx.op).contiguous()
+        f2 = fmap2.to(ctx.op).contiguous()
+        gdt = next((g.dtype for g in grads if g is not None), torch.float32)
+        gs = [(torch.zeros(num, H * W, H >> l, W >> l, dtype=gdt, device=dev) if g is None
+               else g.to(gdt).contiguous()) for l, g in enumerate(grads)]
+        g1 = torch.empty(num, C, H, W, dtype=torch.float32, device=dev) if ctx.needs_input_grad[0] else None
+        g2 = torch.empty(num, C, H, W, dtype=torch.float32, device=dev) if ctx.needs_input_grad[1] else None
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        ptrs = (ctypes.c_void_p * len(gs))(*[g.data_ptr() for g in gs])
+        rc = _lib.load().vipe_corr_volume_backward(
+            _lib.DTYPE_CODE[ctx.op], _lib.DTYPE_CODE[gdt], f1.data_ptr(), f2.data_ptr(), ptrs, num, C, H, W, len(gs),
+            _lib.ptr(g1), _lib.ptr(g2), status.data_ptr(), _lib.stream_of(f1))
+        _lib.check(rc, "CorrVolume backward")
+        if int(status.item()) != 0:
+            raise RuntimeError("CorrVolume backward: a bounded wait expired on the device; gradients incomplete")
+        d1 = None if g1 is None else g1.to(fmap1.dtype)
+        d2 = None if g2 is None else g2.to(fmap2.dtype)
         return d1, d2, None, None, None
 
 
