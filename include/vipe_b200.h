@@ -433,6 +433,18 @@ int vipe_corr_sample_backward(int dtype, const void* input1, const void* input2,
                               int dilationH, int dilationW, int dilation_patchH, int dilation_patchW, int dH, int dW,
                               void* grad_input1_out, void* grad_input2_out, void* stream);
 
+/* CorrBlock lookup fused with the first layer of the update operator's corr_encoder
+ * (reference: droid_net.py:94-102 then UpdateModule.corr_encoder[0:2], :455-460):
+ * out[b][o][p] = ReLU(bias[o] + sum_k weight[o][k] corr[b][k][p]) with corr the 196-channel
+ * radius-3 lookup of the 4-level pyramid at coords / 2^l (channel l*49 + i*7 + j, i the x
+ * offset).  levels[l] (B, H, W, H>>l, W>>l), coords (B, 2, H, W) f32, weight (128, 196) and
+ * out (B, 128, H, W) in dtype (VIPE_F16 or VIPE_BF16), bias (128) f32 or NULL.  tcgen05
+ * tensor cores; the lookup never leaves the chip.  dev_status (device int32): nonzero if a
+ * bounded wait expired. */
+int vipe_corr_encoder_lookup(int dtype, const void* const* levels, int num_levels, const float* coords, int B, int H,
+                             int W, const void* weight, const float* bias, void* out, int32_t* dev_status,
+                             void* stream);
+
 /* All-pairs correlation volume with its average-pooled pyramid — the build of
  * CorrBlock (vipe/slam/networks/droid_net.py:56-69,94-102): for each of the
  * `num` pairs, level l holds avg_pool^l((fmap1/4)^T (fmap2/4)) over the target

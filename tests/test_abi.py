@@ -122,3 +122,22 @@ def test_proximity_edge_checks_without_a_gpu():
                                        16 * 1400, 0, ctypes.c_void_p(16), ctypes.c_void_p(16), 1 << 20,
                                        ctypes.c_void_p(16), ctypes.c_void_p(16), 1 << 30, null)
     assert rc == _lib.VIPE_ERR_CAPACITY
+
+
+def test_fused_correlation_entry_checks_without_a_gpu():
+    import ctypes
+
+    lib = _lib.load()
+    null = ctypes.c_void_p(0)
+    lv = (ctypes.c_void_p * 4)(16, 16, 16, 16)
+    one = ctypes.c_void_p(16)
+    # three levels, a 64-bit type: refused before any device work
+    assert lib.vipe_corr_encoder_lookup(_lib.VIPE_F16, lv, 3, one, 1, 48, 64, one, null, one, one, null) == \
+        _lib.VIPE_ERR_ARG
+    assert lib.vipe_corr_encoder_lookup(_lib.VIPE_F64, lv, 4, one, 1, 48, 64, one, null, one, one, null) == \
+        _lib.VIPE_ERR_DTYPE
+    # volume adjoint: more than 128 channels, H*W not a multiple of 128
+    assert lib.vipe_corr_volume_backward(_lib.VIPE_F16, _lib.VIPE_F16, one, one, lv, 1, 256, 48, 64, 4, one, one,
+                                         one, null) == _lib.VIPE_ERR_ARG
+    assert lib.vipe_corr_volume_backward(_lib.VIPE_F16, _lib.VIPE_F16, one, one, lv, 1, 128, 10, 10, 1, one, one,
+                                         one, null) == _lib.VIPE_ERR_ARG

@@ -75,6 +75,7 @@ _SIGS: dict[str, tuple] = {
     "vipe_slam_proximity_edges": (I, [P, P, P, I, I, I, I, I, I, F, I, I, P, P, I, P, P, SZ, P]),
     "vipe_corr_volume_workspace_size": (SZ, [I, I, I, I]),
     "vipe_corr_volume_backward": (I, [I, I, P, P, P, I, I, I, I, I, P, P, P, P]),
+    "vipe_corr_encoder_lookup": (I, [I, P, I, P, I, I, I, P, P, P, P, P]),
     "vipe_hbm_write_probe": (I, [P, SZ, P]),
     "vipe_corr_volume_build": (I, [I, I, P, P, I, I, I, I, I, P, P, SZ, P]),
 }

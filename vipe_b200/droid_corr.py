@@ -168,6 +168,40 @@ class CorrBlock:
         return v.view(batch, num, ht, wd, ht, wd)
 
 
+def corr_encoder_input(corr_block, coords, weight, bias=None, check=True):
+    """The update operator's first correlation layer applied to the lookup, in one kernel:
+    ReLU(conv1x1(corr_block(coords), weight, bias)) (reference: UpdateModule.corr_encoder[0:2]
+    on CorrBlock's output, droid_net.py:94-102, 452-519), without the 196-channel lookup
+    leaving the chip (vipe_corr_encoder_lookup).
+
+    corr_block: a CorrBlock with 4 levels, radius 3 and an FP16 / BF16 volume; coords
+    (batch, num, H, W, 2); weight (128, 196[, 1, 1]), bias (128,).  Returns (batch * num, 128,
+    H, W) in the volume dtype, the input of corr_encoder[2] (the 3x3 convolution).
+    Inference only (no autograd)."""
+    import ctypes
+
+    from . import _lib
+
+    if corr_block.num_levels != 4 or corr_block.radius != 3:
+        raise RuntimeError("corr_encoder_input: the fused kernel takes 4 levels of radius 3 (196 channels)")
+    levels = [lv.contiguous() for lv in corr_block.corr_pyramid]
+    dt = levels[0].dtype
+    batch, num, ht, wd, _ = coords.shape
+    c = coords.permute(0, 1, 4, 2, 3).reshape(batch * num, 2, ht, wd).float().contiguous()
+    w = weight.reshape(128, 196).to(dt).contiguous()
+    b = None if bias is None else bias.float().contiguous()
+    out = torch.empty(batch * num, 128, ht, wd, dtype=dt, device=c.device)
+    status = torch.zeros(1, dtype=torch.int32, device=c.device)
+    ptrs = (ctypes.c_void_p * 4)(*[lv.data_ptr() for lv in levels])
+    rc = _lib.load().vipe_corr_encoder_lookup(_lib.DTYPE_CODE[dt], ptrs, 4, c.data_ptr(), batch * num, ht, wd,
+                                              w.data_ptr(), _lib.ptr(b), out.data_ptr(), status.data_ptr(),
+                                              _lib.stream_of(c))
+    _lib.check(rc, "corr_encoder_input")
+    if check and int(status.item()) != 0:
+        raise RuntimeError("corr_encoder_input: a bounded wait expired on the device; the output is incomplete")
+    return out
+
+
 class CorrLayer(torch.autograd.Function):
     """On-the-fly lookup (reference droid_net.py:105-118)."""
 
