@@ -444,14 +444,16 @@ def _cpu_clip_solves(b, sample_s, start=0, max_clips=256):
         return clips[g]
 
     ob.ba(clip(order[start % b.G]), fp64=False, iterations=1)  # warm (builds the oracle if needed)
-    n, t0 = 0, time.perf_counter()
+    n, el = 0, 0.0
     while n < max_clips:
-        q = clip(order[(start + n) % b.G])
+        q = clip(order[(start + n) % b.G])  # the clip's copy to the host is not timed
+        t0 = time.perf_counter()
         ob.ba(q, fp64=False, iterations=4)
+        el += time.perf_counter() - t0
         n += 1
-        if time.perf_counter() - t0 >= sample_s:
+        if el >= sample_s:
             break
-    return n, time.perf_counter() - t0, threads, start + n
+    return n, el, threads, start + n
 
 
 def cpu_baseline(b, sample_s):

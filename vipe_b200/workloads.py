@@ -357,12 +357,13 @@ class BABatch:
         """Clip g as a standalone BAProblem (CPU tensors), for per-graph reference solves."""
         fo, eo, ko = (sum(x[:g]) for x in (self.num_frames, self.num_edges, self.num_kx))
         n, e, k = self.num_frames[g], self.num_edges[g], self.num_kx[g]
-        t = {key: v.cpu() for key, v in self.tensors.items()}
-        return BAProblem(poses=t["poses"][fo:fo + n].clone(), disps=t["disps"][fo:fo + n].clone(),
-                         intrinsics=t["intrinsics"][g].clone(), disps_sens=t["disps_sens"][fo:fo + n].clone(),
-                         targets=t["targets"][eo:eo + e].clone(), weights=t["weights"][eo:eo + e].clone(),
-                         eta=t["eta"][ko:ko + k].clone(), ii=t["ii"][eo:eo + e].clone(), jj=t["jj"][eo:eo + e].clone(),
-                         depth_active=t["depth_active"][fo:fo + n].clone(), t0=self.t0[g], t1=self.t1[g],
+        t = self.tensors
+        # slice on the batch's device, then copy only the clip to the host
+        return BAProblem(poses=t["poses"][fo:fo + n].cpu(), disps=t["disps"][fo:fo + n].cpu(),
+                         intrinsics=t["intrinsics"][g].cpu(), disps_sens=t["disps_sens"][fo:fo + n].cpu(),
+                         targets=t["targets"][eo:eo + e].cpu(), weights=t["weights"][eo:eo + e].cpu(),
+                         eta=t["eta"][ko:ko + k].cpu(), ii=t["ii"][eo:eo + e].cpu(), jj=t["jj"][eo:eo + e].cpu(),
+                         depth_active=t["depth_active"][fo:fo + n].cpu(), t0=self.t0[g], t1=self.t1[g],
                          iterations=4, poses_gt=self.poses_gt[fo:fo + n].cpu(), disps_gt=self.disps_gt[fo:fo + n].cpu())
 
 
