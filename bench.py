@@ -371,6 +371,128 @@ def corr_lookup_bench(dev, f1, f2, g, hbm_peak):
     }
 
 
+def _time_ms(fn, reps=3):
+    """Median of `reps` CUDA-event timings of fn() on the current stream, after one warm call."""
+    import torch
+
+    fn()
+    ts = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    return sorted(ts)[len(ts) // 2]
+
+
+def corr_extras_bench(dev, hbm_peak, bf16_peak):
+    """The correlation kernels beside the build, each against the eager / library path it
+    replaces on the same GPU (config 2's shapes: 128 channels, 48x64, 4 levels, radius 3):
+      adjoint   CorrVolume backward over 640 pairs (two tcgen05 GEMM passes forming the
+                unpooled gradient on the fly) vs per-level torch.bmm + avg_pool2d +
+                repeat_interleave;
+      encoder   lookup fused with corr_encoder's 1x1 conv + ReLU over 640 pairs vs the four
+                per-level lookups, a cuDNN 1x1 conv and ReLU;
+      pyramid   AltCorrBlock's channels-last pyramid of 64 frames vs fmaps/4, avg_pool2d and
+                permute().contiguous()."""
+    import ctypes
+
+    import torch
+    import torch.nn.functional as F
+
+    from vipe_b200 import _lib
+    from vipe_b200.droid_corr import CorrBlock, _pyramid_levels, corr_encoder_input
+    from vipe_b200.ext import droid_net_ext as dne
+
+    lib = _lib.load()
+    out = {}
+    E, C, H, W = 640, 128, 48, 64
+    HW = H * W
+    g = torch.Generator(device=dev).manual_seed(1002)
+    # ---- adjoint
+    f1 = (torch.randn(E, C, H, W, generator=g, device=dev) / C**0.5).half()
+    f2 = (torch.randn(E, C, H, W, generator=g, device=dev) / C**0.5).half()
+    grads = [torch.randn(E, HW, H >> l, W >> l, generator=g, device=dev, dtype=torch.float16) for l in range(4)]
+    g1 = torch.empty(E, C, H, W, device=dev)
+    g2 = torch.empty_like(g1)
+    st = torch.zeros(1, dtype=torch.int32, device=dev)
+    ptrs = (ctypes.c_void_p * 4)(*[x.data_ptr() for x in grads])
+
+    def ours():
+        rc = lib.vipe_corr_volume_backward(_lib.VIPE_F16, _lib.VIPE_F16, f1.data_ptr(), f2.data_ptr(), ptrs, E, C, H,
+                                           W, 4, g1.data_ptr(), g2.data_ptr(), st.data_ptr(),
+                                           torch.cuda.current_stream(dev).cuda_stream)
+        _lib.check(rc, "corr volume backward")
+
+    def library():
+        a1 = torch.zeros(E, C, HW, device=dev)
+        a2 = torch.zeros(E, C, H, W, device=dev)
+        for l, G in enumerate(grads):
+            h, w = H >> l, W >> l
+            p2 = F.avg_pool2d(f2.float(), 2**l).half() if l else f2
+            a1 += torch.bmm(p2.reshape(E, C, h * w), G.reshape(E, HW, h * w).transpose(1, 2)).float()
+            m = torch.bmm(f1.reshape(E, C, HW), G.reshape(E, HW, h * w)).float().reshape(E, C, h, w)
+            if l:
+                m = m.repeat_interleave(2**l, dim=2).repeat_interleave(2**l, dim=3) / float(4**l)
+            a2 += m
+        return a1, a2
+
+    ms = _time_ms(ours)
+    ref_ms = _time_ms(library, reps=1)
+    assert int(st.item()) == 0
+    gbytes = 2 * sum(x.numel() * 2 for x in grads) + 2 * 2 * E * C * HW * 2 + 2 * E * C * HW * 4
+    flops = 2 * 2.0 * E * C * HW * HW
+    out["adjoint"] = {"workload": "CorrVolume backward, 640 pairs, FP16 maps and level gradients",
+                      "ms": ms, "algorithmic_bytes": gbytes, "achieved_gbs": gbytes / ms / 1e6,
+                      "frac_hbm": gbytes / ms / 1e6 / hbm_peak, "tflops": flops / ms / 1e9,
+                      "frac_bf16_peak": flops / ms / 1e9 / bf16_peak, "library_path_ms": ref_ms,
+                      "speedup_vs_library_path": ref_ms / ms}
+    del grads, g1, g2, f1, f2
+    torch.cuda.empty_cache()
+    # ---- fused lookup + first update-operator layer
+    fa = (torch.randn(1, E, C, H, W, generator=g, device=dev) / 4).half()
+    fb = (torch.randn(1, E, C, H, W, generator=g, device=dev) / 4).half()
+    blk = CorrBlock(fa, fb, num_levels=4, radius=3, out_dtype=torch.float16)
+    del fa, fb
+    yy, xx = torch.meshgrid(torch.arange(H, device=dev), torch.arange(W, device=dev), indexing="ij")
+    coords = torch.stack([xx, yy], -1).float()[None, None].repeat(1, E, 1, 1, 1)
+    coords = coords + torch.randn(coords.shape, generator=g, device=dev)
+    wt = torch.randn(128, 196, 1, 1, generator=g, device=dev) / 14.0
+    bs = 0.1 * torch.randn(128, generator=g, device=dev)
+    w16, b16 = wt.half(), bs.half()
+    ms_f = _time_ms(lambda: corr_encoder_input(blk, coords, wt, bs, check=False))
+    ms_u = _time_ms(lambda: F.relu(F.conv2d(blk(coords).view(E, 196, H, W), w16, b16)))
+    # algorithmic bytes per pixel: coordinates 8 B, four 8x8 windows of FP16 taps, 128 FP16 outputs
+    enc_bytes = E * HW * (8 + 4 * 64 * 2 + 128 * 2)
+    out["encoder"] = {"workload": "CorrBlock lookup (4 levels, radius 3) + corr_encoder 1x1 conv + ReLU, 640 pairs, FP16",
+                      "fused_ms": ms_f, "unfused_ms": ms_u, "speedup": ms_u / ms_f, "algorithmic_bytes": enc_bytes,
+                      "achieved_gbs": enc_bytes / ms_f / 1e6, "frac_hbm": enc_bytes / ms_f / 1e6 / hbm_peak}
+    del blk, coords
+    torch.cuda.empty_cache()
+    # ---- AltCorrBlock pyramid
+    fm = torch.randn(64, C, H, W, generator=g, device=dev).half()
+
+    def eager():
+        f = fm / 4.0
+        lv = []
+        for _ in range(4):
+            lv.append(f.permute(0, 2, 3, 1).contiguous())
+            f = F.avg_pool2d(f, 2, stride=2)
+        return lv
+
+    ms_p = _time_ms(lambda: _pyramid_levels(fm, 4))
+    ms_e = _time_ms(eager)
+    pbytes = fm.numel() * 2 * (1 + 1 + 1 / 4 + 1 / 16 + 1 / 64)
+    out["pyramid"] = {"workload": "AltCorrBlock pyramid, 64 frames of 128-channel 48x64 FP16 maps, 4 levels",
+                      "ms": ms_p, "achieved_gbs": pbytes / ms_p / 1e6, "frac_hbm": pbytes / ms_p / 1e6 / hbm_peak,
+                      "eager_ms": ms_e, "speedup": ms_e / ms_p}
+    del fm
+    torch.cuda.empty_cache()
+    return out
+
+
 def lie_bench(dev, hbm_peak):
     """SE3 group kernels over 16M elements (f32; HBM bound): bytes = elements x (inputs +
     outputs) x 4 B.  Outputs are preallocated; each op is one launch, median of 5."""
@@ -1087,6 +1209,8 @@ def run_ours(args):
         torch.cuda.empty_cache()
         corr = corr_build_bench(dev, 5, hbm, src, bf16)
     torch.cuda.empty_cache()
+    corr_extras = None if args.no_corr else corr_extras_bench(dev, hbm, bf16)
+    torch.cuda.empty_cache()
     lie = lie_bench(dev, hbm)
 
     if rank == 0:
@@ -1123,6 +1247,7 @@ def run_ours(args):
             "plain_backend_256kf": backend,
             "sim3_batched": sim3,
             "corr": corr,
+            "corr_extras": corr_extras,
             "lie": lie,
         }
         if not args.no_cpu_baseline:
