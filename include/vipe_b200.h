@@ -134,7 +134,7 @@ int vipe_slam_ba(float* poses_io, float* disps_io, float* intrinsics_io, const f
  *   - Graphs whose vipe_slam_ba_workspace_size() exceeds the scratch are
  *     rejected with VIPE_ERR_CAPACITY before any launch (vipe_last_error()
  *     names both sizes).  A 64-keyframe 48x64 graph with 628 edges needs
- *     about 16.4 MiB.
+ *     about 24 MiB.
  *   - The first call on a device looks up the scratch's device address there
  *     (cudaGetSymbolAddress, which loads the library's module on that device);
  *     make that first call before any stream capture.  The address is kept for

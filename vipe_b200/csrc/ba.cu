@@ -1111,9 +1111,32 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
 //      tiles, zero outside the frame's entries); CTA 0 sums the energy row in pixel
 //      order;
 //   3. a second grid barrier frees ebuf for the next (frame, chunk).
+// Up to kWideGroup frames go through a round together (one staging area each), so both
+// phases spread over the grid instead of over one frame's pixels and blocks.
 // Deterministic (fixed summation orders, no atomics).  The grid is sized to be
 // co-resident (cudaLaunchCooperativeKernel checks it), so the barriers always complete.
 constexpr int kWideThreads = 256;
+
+// per-frame constants of wide frame number i (in wide_list order)
+struct WideFrame {
+    int s, k, m, self, eb, ee, Dm, Dr, nt, toff, nb;
+};
+
+__device__ __forceinline__ WideFrame wide_frame(const Work& w, int i) {
+    WideFrame f;
+    f.s = w.wide_list[i];
+    f.k = w.kx[f.s];
+    f.m = w.fp_ptr[f.s + 1] - w.fp_ptr[f.s];
+    f.self = w.self_slot[f.s];
+    f.eb = w.fe_ptr[f.s];
+    f.ee = w.fe_ptr[f.s + 1];
+    f.Dm = 6 * f.m;
+    f.Dr = f.Dm + 2;
+    f.nt = (f.Dr + 3) / 4;
+    f.toff = w.wtile_off[f.s];
+    f.nb = (f.Dr + kWideTile - 1) / kWideTile;
+    return f;
+}
 
 template <bool kIntr>
 __global__ void __launch_bounds__(kWideThreads) ba_frame_wide_kernel(BAPtrs base, Batch B, float alpha,
@@ -1132,33 +1155,30 @@ __global__ void __launch_bounds__(kWideThreads) ba_frame_wide_kernel(BAPtrs base
     __shared__ float red[kWideThreads / 32];
     const int tid = threadIdx.x;
     const int HW = d.HW, W = d.W, LD = d.chunk_f;
+    const long slot_floats = wide_rows(d) * (long)LD;  // one frame's staging area
     const float fx = A.intr[0], fy = A.intr[1], cx = A.intr[2], cy = A.intr[3];
     const long gthreads = (long)gridDim.x * blockDim.x;
     const long gtid = (long)blockIdx.x * blockDim.x + tid;
-    float* __restrict__ eb_ = w.ebuf;
-    for (int i = 0; i < nw; i++) {
-        const int s = w.wide_list[i];
-        const int k = w.kx[s];
-        const float act = A.depth_active[k];
-        const int m = w.fp_ptr[s + 1] - w.fp_ptr[s];
-        const int self = w.self_slot[s];
-        const int eb = w.fe_ptr[s], ee = w.fe_ptr[s + 1];
-        const int Dm = D * m, Dr = Dm + 2;
-        const int nt = (Dr + 3) / 4;
-        const int toff = w.wtile_off[s];
+    for (int i0 = 0; i0 < nw; i0 += kWideGroup) {
+        const int ng = min(kWideGroup, nw - i0);  // frames of this round, one staging area each
         for (int c = 0; c < d.CF; c++) {
             const int p0 = c * d.chunk_f, p1 = min(HW, p0 + d.chunk_f), np_ = p1 - p0;
-            // 1. staging
-            for (long pp = gtid; pp < np_; pp += gthreads) {
-                const int p = p0 + (int)pp;
-                const float u = (float)(p % W), v = (float)(p / W);
+            // 1. staging: one thread per (frame of the round, pixel of the chunk)
+            for (long u = gtid; u < (long)ng * np_; u += gthreads) {
+                const int fi = (int)(u / np_), pp = (int)(u % np_);
+                const WideFrame F = wide_frame(w, i0 + fi);
+                float* __restrict__ eb_ = w.ebuf + (size_t)fi * slot_floats;
+                const int k = F.k, s = F.s, self = F.self;
+                const float act = A.depth_active[k];
+                const int p = p0 + pp;
+                const float uu = (float)(p % W), vv = (float)(p / W);
                 const float disp = A.disps[(size_t)k * HW + p];
                 const float dsens = __ldg(A.disps_sens + (size_t)k * HW + p);
                 const float eta_p = __ldg(A.eta + (size_t)s * HW + p);
-                for (int q = 0; q < Dm; q++) eb_[(size_t)q * LD + pp] = 0.f;
+                for (int q = 0; q < F.Dm; q++) eb_[(size_t)q * LD + pp] = 0.f;
                 float es[D] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                 float csum = 0.f, bsum = 0.f, efsum = 0.f;
-                for (int q = eb; q < ee; q++) {
+                for (int q = F.eb; q < F.ee; q++) {
                     const int e = w.fe_list[q];
                     const int b = (int)A.jj[e];
                     const size_t o = (size_t)e * 2 * HW + p;
@@ -1166,7 +1186,7 @@ __global__ void __launch_bounds__(kWideThreads) ba_frame_wide_kernel(BAPtrs base
                     edge_tf<D>(A.poses, k, b, Tf);
                     const int sl = w.edge_slot[e];
                     PixelLin L;
-                    linearize_d<D, kIntr, true>(Tf, b == k, fx, fy, cx, cy, u, v, disp, __ldg(A.weights + o),
+                    linearize_d<D, kIntr, true>(Tf, b == k, fx, fy, cx, cy, uu, vv, disp, __ldg(A.weights + o),
                                                 __ldg(A.weights + o + HW), __ldg(A.targets + o),
                                                 __ldg(A.targets + o + HW), act, A.iscale, L);
                     const float g0 = L.wd[0] * L.Jz[0], g1 = L.wd[1] * L.Jz[1];
@@ -1196,8 +1216,8 @@ __global__ void __launch_bounds__(kWideThreads) ba_frame_wide_kernel(BAPtrs base
                     for (int n = 0; n < D; n++) eb_[(size_t)(D * self + n) * LD + pp] = es[n];
                 }
                 const float msk = (dsens > 0.f ? 1.f : 0.f) * act;
-                const float C = act * (csum + eta_p + msk * A.alpha) + (1.f - act);
-                const float Q = 1.f / C;
+                const float Cc = act * (csum + eta_p + msk * A.alpha) + (1.f - act);
+                const float Q = 1.f / Cc;
                 const float dd = disp - dsens;
                 const float wv = act * (bsum - msk * A.alpha * dd);
                 const float Ef = efsum * act;
@@ -1208,24 +1228,53 @@ __global__ void __launch_bounds__(kWideThreads) ba_frame_wide_kernel(BAPtrs base
                 if (io.ftape) tape_qw(io.ftape, d)[(size_t)s * HW + p] = make_float2(Q, wv);
                 const float sq = sqrtf(Q);
                 const float scale = act * sq;
-                for (int q = 0; q < Dm; q++) eb_[(size_t)q * LD + pp] *= scale;
-                eb_[(size_t)Dm * LD + pp] = sq * wv;
-                eb_[(size_t)(Dm + 1) * LD + pp] = sq * Ef;
-                eb_[(size_t)(Dm + 2) * LD + pp] = msk * A.alpha * dd * dd;
+                for (int q = 0; q < F.Dm; q++) eb_[(size_t)q * LD + pp] *= scale;
+                eb_[(size_t)F.Dm * LD + pp] = sq * wv;
+                eb_[(size_t)(F.Dm + 1) * LD + pp] = sq * Ef;
+                eb_[(size_t)(F.Dm + 2) * LD + pp] = msk * A.alpha * dd * dd;
             }
             __threadfence();
             grid.sync();
-            // 2. Gram blocks (bi <= bj) of the chunk
-            const int nb = (Dr + kWideTile - 1) / kWideTile;
-            const int nblk = nb * (nb + 1) / 2;
+            // 2. Gram blocks (bi <= bj) of every frame of the round, and each frame's energy
+            int total = 0;
+            for (int fi = 0; fi < ng; fi++) {
+                const int nb = wide_frame(w, i0 + fi).nb;
+                total += nb * (nb + 1) / 2;
+            }
             const int tr = tid >> 4, tcol = tid & 15;
-            for (int t = blockIdx.x; t < nblk; t += gridDim.x) {
-                int bi = 0, rem = t;
-                while (rem >= nb - bi) {
-                    rem -= nb - bi;
+            for (int t = blockIdx.x; t < total + ng; t += gridDim.x) {
+                if (t >= total) {  // energy of frame t - total, summed in pixel order
+                    const int fi = t - total;
+                    const WideFrame F = wide_frame(w, i0 + fi);
+                    const float* eb_ = w.ebuf + (size_t)fi * slot_floats;
+                    float en = 0.f;
+                    for (int pp = tid; pp < np_; pp += kWideThreads) en += eb_[(size_t)(F.Dm + 2) * LD + pp];
+                    en = warp_sum(en);
+                    if ((tid & 31) == 0) red[tid >> 5] = en;
+                    __syncthreads();
+                    if (tid == 0) {
+                        float tsum = 0.f;
+                        for (int q = 0; q < kWideThreads / 32; q++) tsum += red[q];
+                        w.fen[(size_t)F.s * d.CF + c] = tsum;
+                    }
+                    __syncthreads();
+                    continue;
+                }
+                int fi = 0, rem = t;
+                WideFrame F = wide_frame(w, i0);
+                while (rem >= F.nb * (F.nb + 1) / 2) {
+                    rem -= F.nb * (F.nb + 1) / 2;
+                    fi++;
+                    F = wide_frame(w, i0 + fi);
+                }
+                const float* eb_ = w.ebuf + (size_t)fi * slot_floats;
+                int bi = 0;
+                while (rem >= F.nb - bi) {
+                    rem -= F.nb - bi;
                     bi++;
                 }
                 const int bj = bi + rem;
+                const int Dr = F.Dr, nt = F.nt;
                 float acc[4][4];
 #pragma unroll
                 for (int r = 0; r < 4; r++)
@@ -1257,10 +1306,10 @@ __global__ void __launch_bounds__(kWideThreads) ba_frame_wide_kernel(BAPtrs base
                 }
                 const int ti = bi * (kWideTile / 4) + tr, cg = bj * (kWideTile / 4) + tcol;
                 if (ti < nt && cg < nt && cg >= ti) {
-                    // the tile's running sum over chunks: this thread owns it in every chunk
-                    // (same work-item mapping), the grid barriers order the chunks
+                    // the tile's running sum over chunks: its (frame, block) item lands on the same CTA
+                    // and thread in every chunk of the round, and the grid barriers order the chunks
                     const int tau = ti * nt - (ti * (ti - 1)) / 2 + (cg - ti);
-                    float* dst = w.wtile + ((size_t)(toff + tau)) * 16;
+                    float* dst = w.wtile + ((size_t)(F.toff + tau)) * 16;
 #pragma unroll
                     for (int r = 0; r < 4; r++) {
                         const int row = 4 * ti + r;
@@ -1277,20 +1326,8 @@ __global__ void __launch_bounds__(kWideThreads) ba_frame_wide_kernel(BAPtrs base
                     }
                 }
             }
-            if (blockIdx.x == 0) {
-                float en = 0.f;
-                for (int pp = tid; pp < np_; pp += kWideThreads) en += eb_[(size_t)(Dm + 2) * LD + pp];
-                en = warp_sum(en);
-                if ((tid & 31) == 0) red[tid >> 5] = en;
-                __syncthreads();
-                if (tid == 0) {
-                    float tsum = 0.f;
-                    for (int q = 0; q < kWideThreads / 32; q++) tsum += red[q];
-                    w.fen[(size_t)s * d.CF + c] = tsum;
-                }
-            }
             __threadfence();
-            grid.sync();  // 3. ebuf is rewritten by the next (frame, chunk)
+            grid.sync();  // 3. the staging areas are rewritten by the next chunk or round
         }
     }
 }

@@ -18,6 +18,7 @@ constexpr int kMaxSlots = 31;          // window poses coupled to one depth fram
 constexpr int kMaxPoses = 1024;        // t1 - t0 of a single graph (the index kernel's pose bitmask);
                                        // batches: 6P+1 unknowns must fit the staged Cholesky panel
 constexpr int kWideTile = 64;          // output block of the wide-frame Gram product
+constexpr int kWideGroup = 8;          // wide frames staged and multiplied together
 constexpr int kNT = 105;               // per-edge terms, see term layout below
 constexpr int kEdgeThreads = 256;
 constexpr int kFrameThreads = 128;     // one pixel per thread; 32-pixel blocks per warp
@@ -86,7 +87,7 @@ struct Work {
     double* linv;    // inverse diagonal blocks of the Cholesky factor
     double* yv;      // dim: forward-substitution result of the multi-launch Cholesky
     int* wide_list;  // K: depth rows whose slot count exceeds max_slots (wide frames), ascending
-    float* ebuf;     // (dof * P + 3) x chunk_f: one wide frame's scaled rows e_p over one pixel chunk
+    float* ebuf;     // kWideGroup x (dof * P + 3) x chunk_f: wide frames' scaled rows e_p over one pixel chunk
     int* wtile_off;  // K + 1: first Gram tile of each wide frame in wtile
     float* wtile;    // wtile_cap x 16: wide frames' upper-triangle 4 x 4 Gram tiles, all chunks summed
     // adjoint (carved only when Dims::adj)
@@ -185,7 +186,7 @@ inline void carve(C& c, const Dims& d, Work* w) {
     auto pli = c.template take<double>((size_t)((d.dim + 31) / 32) * 32 * 32);
     auto pyv = c.template take<double>((size_t)d.dim);
     auto pwl = c.template take<int>(K + 1);
-    auto peb = c.template take<float>(d.wide ? (size_t)wide_rows(d) * d.chunk_f : 1);
+    auto peb = c.template take<float>(d.wide ? (size_t)kWideGroup * wide_rows(d) * d.chunk_f : 1);
     auto pwo = c.template take<int>(K + 1);
     auto pwt = c.template take<float>((size_t)d.wtile_cap * 16);
     if (w) {
