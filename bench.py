@@ -64,7 +64,8 @@ def parse():
     ap.add_argument("--no-corr", action="store_true")
     ap.add_argument("--e2e-parts", type=int, default=24,
                     help="host batch split into this many streamed parts for the end-to-end leg")
-    ap.add_argument("--case", choices=["ba0", "ba1", "corr_build", "batch", "lookup"],
+    ap.add_argument("--case", choices=["ba0", "ba1", "corr_build", "batch", "lookup", "corr_bwd", "corr_extras",
+                                       "backend"],
                     help="run one workload --reps times and exit (for profiler captures; no JSON line)")
     ap.add_argument("--clips", type=int, default=32)
     ap.add_argument("--reps", type=int, default=2)
@@ -390,9 +391,10 @@ def _time_ms(fn, reps=3):
 def corr_extras_bench(dev, hbm_peak, bf16_peak):
     """The correlation kernels beside the build, each against the eager / library path it
     replaces on the same GPU (config 2's shapes: 128 channels, 48x64, 4 levels, radius 3):
-      adjoint   CorrVolume backward over 640 pairs (two tcgen05 GEMM passes forming the
-                unpooled gradient on the fly) vs per-level torch.bmm + avg_pool2d +
-                repeat_interleave;
+      adjoint   CorrVolume backward over 640 pairs (two tcgen05 GEMM passes, level-0
+                gradient tiles by TMA, pooled levels added in shared memory) vs per-level
+                torch.bmm + avg_pool2d + repeat_interleave, and vs the producer-formed
+                kernel that other shapes take;
       encoder   lookup fused with corr_encoder's 1x1 conv + ReLU over 640 pairs vs the four
                 per-level lookups, a cuDNN 1x1 conv and ReLU;
       pyramid   AltCorrBlock's channels-last pyramid of 64 frames vs fmaps/4, avg_pool2d and
@@ -439,7 +441,12 @@ def corr_extras_bench(dev, hbm_peak, bf16_peak):
             a2 += m
         return a1, a2
 
-    ms = _time_ms(ours)
+    ms = _time_ms(ours, reps=10)
+    lib.vipe_corr_volume_backward_force_generic(1)
+    try:
+        generic_ms = _time_ms(ours, reps=3)
+    finally:
+        lib.vipe_corr_volume_backward_force_generic(0)
     ref_ms = _time_ms(library, reps=1)
     assert int(st.item()) == 0
     gbytes = 2 * sum(x.numel() * 2 for x in grads) + 2 * 2 * E * C * HW * 2 + 2 * E * C * HW * 4
@@ -448,7 +455,7 @@ def corr_extras_bench(dev, hbm_peak, bf16_peak):
                       "ms": ms, "algorithmic_bytes": gbytes, "achieved_gbs": gbytes / ms / 1e6,
                       "frac_hbm": gbytes / ms / 1e6 / hbm_peak, "tflops": flops / ms / 1e9,
                       "frac_bf16_peak": flops / ms / 1e9 / bf16_peak, "library_path_ms": ref_ms,
-                      "speedup_vs_library_path": ref_ms / ms}
+                      "speedup_vs_library_path": ref_ms / ms, "producer_formed_kernel_ms": generic_ms}
     del grads, g1, g2, f1, f2
     torch.cuda.empty_cache()
     # ---- fused lookup + first update-operator layer
@@ -1266,6 +1273,9 @@ def run_ours(args):
 #   corr_build    --edges pairs of 128-channel 48x64 BF16 maps -> FP16 4-level pyramid
 #   batch         --clips clips of the uneven batch, forward (4 iterations, tape) + adjoint
 #   lookup        radius-3 lookups of --edges edges: volume (4 levels) and indexed
+#   corr_bwd      CorrVolume backward of --edges pairs (FP16 maps and level gradients, 48x64, 4 levels)
+#   corr_extras   the correlation extras leg alone (prints its JSON)
+#   backend       the 256-keyframe backend window through slam_ext.ba_extended
 
 import torch  # noqa: E402  (the cases below run under torch; the benchmark legs import it lazily)
 
@@ -1359,9 +1369,54 @@ def case_batch(clips: int, reps: int) -> None:
             raise RuntimeError("device status set")
 
 
+def case_corr_bwd(edges: int, reps: int) -> None:
+    import ctypes
+
+    from vipe_b200 import _lib
+
+    E, C, H, W = edges, 128, 48, 64
+    g = torch.Generator(device="cuda").manual_seed(1002)
+    f1 = (torch.randn(E, C, H, W, generator=g, device="cuda") / C**0.5).half()
+    f2 = (torch.randn(E, C, H, W, generator=g, device="cuda") / C**0.5).half()
+    grads = [torch.randn(E, H * W, H >> l, W >> l, generator=g, device="cuda", dtype=torch.float16) for l in range(4)]
+    g1 = torch.empty(E, C, H, W, device="cuda")
+    g2 = torch.empty_like(g1)
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ptrs = (ctypes.c_void_p * 4)(*[x.data_ptr() for x in grads])
+    for _ in range(reps):
+        rc = _lib.load().vipe_corr_volume_backward(_lib.VIPE_F16, _lib.VIPE_F16, f1.data_ptr(), f2.data_ptr(), ptrs,
+                                                   E, C, H, W, 4, g1.data_ptr(), g2.data_ptr(), st.data_ptr(),
+                                                   torch.cuda.current_stream().cuda_stream)
+        _lib.check(rc, "corr volume backward")
+    torch.cuda.synchronize()
+    if int(st.item()):
+        raise RuntimeError("device status set")
+
+
+def case_backend(reps: int) -> None:
+    from vipe_b200 import workloads as W
+    from vipe_b200.ext import slam_ext
+
+    g0 = W.ba_backend().to("cuda")
+    for _ in range(reps):
+        q = g0.clone()
+        slam_ext.ba_extended(q.poses, q.disps, q.intrinsics, q.disps_sens, q.targets, q.weights, q.eta, q.ii, q.jj,
+                             q.depth_active, q.t0, q.t1, q.iterations, q.lm, q.ep, False, q.alpha, False, 1e-6, 1e-6,
+                             1.0, False)
+    torch.cuda.synchronize()
+
+
 def run_case(args):
+    if args.case == "corr_extras":
+        hbm, bf16, _ = measured_peaks()
+        print(json.dumps(corr_extras_bench("cuda", hbm, bf16)))
+        return 0
     if args.case in ("ba0", "ba1"):
         case_ba(args.case, args.reps)
+    elif args.case == "corr_bwd":
+        case_corr_bwd(args.edges, args.reps)
+    elif args.case == "backend":
+        case_backend(args.reps)
     elif args.case == "batch":
         case_batch(args.clips, args.reps)
     elif args.case == "lookup":

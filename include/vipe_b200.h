@@ -112,6 +112,29 @@ int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* intrinsics_io
                           float* dz_out, float* energy_out, void* workspace, size_t workspace_bytes,
                           int32_t* dev_status, void* stream);
 
+/* Fused BA with the generic solver's robust kernels (no counterpart in the reference's
+ * fused path, which refuses robust kernels, vipe/slam/components/buffer.py:531-547; the
+ * semantics are those of its generic solver, vipe/slam/ba/kernel.py:40-162 and
+ * terms.py:73-75).  Arguments of vipe_slam_ba_extended plus:
+ *   robust_kind 0 none, 1 Huber (w = 1 if |r| <= c else c/|r|), 2 Tukey
+ *     (w = max(1 - (r/c)^2, 0)^2), 3 GNC-TLS (w at scalar mu per kernel.py:97-153);
+ *     each flow channel's weight is multiplied by w(r) of its residual at the linearisation
+ *     point;
+ *   robust_threshold c > 0 (kinds 1-3);
+ *   mu_schedule (HOST array of `iterations` floats, kind 3 only): mu of each LM iteration,
+ *     +inf for the hard TLS indicator (see the generic solver's schedule, buffer.py:686-695).
+ * The depth back-substitution keeps the rows of pose t0 (the generic solver's Schur
+ * back-substitution; vipe_slam_ba_extended skips them like the reference's fused kernel). */
+int vipe_slam_ba_extended_robust(float* poses_io, float* disps_io, float* intrinsics_io, const float* disps_sens,
+                                 const float* targets, const float* weights, const float* eta, const int64_t* ii,
+                                 const int64_t* jj, const float* depth_active, int num_frames, int ht, int wd,
+                                 int num_edges, int num_kx, int t0, int t1, int iterations, float lm, float ep,
+                                 int motion_only, float alpha, int optimize_intrinsics, float intrinsics_lm,
+                                 float intrinsics_ep, float intrinsics_scale, int compute_energy, float* dx_out,
+                                 float* dz_out, float* energy_out, int robust_kind, float robust_threshold,
+                                 const float* mu_schedule, void* workspace, size_t workspace_bytes,
+                                 int32_t* dev_status, void* stream);
+
 /* Replaces slam_ext.ba (reference: csrc/slam_ext/slam.cpp:42-45,
  * geom_kernels.cu:1826-1834): ba_extended with depth_active = 1, no focal
  * optimisation and no energy.  depth_active_scratch: device f32 buffer of
@@ -464,11 +487,16 @@ size_t vipe_corr_volume_workspace_size(int num, int C, int ht, int wd);
  * fmap1, fmap2 (num, C, ht, wd) in map_dtype (VIPE_F16 / VIPE_BF16: the operands the
  * forward multiplied).  tcgen05 tensor cores: kind::f16 for 16-bit gradients, kind::tf32
  * with a hi + lo split of Gt for FP32 gradients.  C <= 128, ht*wd a multiple of 128, wd of
- * 8, ht and wd of 2^(num_levels-1).  dev_status (device int32): set nonzero if a bounded
- * wait expired (the gradients are then incomplete). */
+ * 8, ht and wd of 2^(num_levels-1).  16-bit maps and gradients of one type with wd a
+ * multiple of 64 take a TMA-fed warp-specialised kernel (G_0 tiles loaded by TMA, the pooled
+ * levels added in shared memory); other shapes form Gt in the producer warps.  dev_status
+ * (device int32): set nonzero if a bounded wait expired (the gradients are then incomplete). */
 int vipe_corr_volume_backward(int map_dtype, int grad_dtype, const void* fmap1, const void* fmap2,
                               const void* const* level_grads, int num, int C, int ht, int wd, int num_levels,
                               float* fmap1_grad_out, float* fmap2_grad_out, int32_t* dev_status, void* stream);
+/* Test hook: on != 0 sends every vipe_corr_volume_backward call through the producer-formed
+ * kernel (so the two kernels can be held to each other on the same shapes). */
+void vipe_corr_volume_backward_force_generic(int on);
 int vipe_corr_volume_build(int in_dtype, int out_dtype, const void* fmap1, const void* fmap2, int num, int C, int ht,
                            int wd, int num_levels, void* const* level_out, void* workspace, size_t workspace_bytes,
                            void* stream);

@@ -41,6 +41,33 @@ namespace {
 int g_threads = 1;
 int g_backsub_all_rows = 0;  // see oracle_set_backsub_all_rows
 
+// Robust kernel of the reference's generic solver (vipe/slam/ba/kernel.py:40-153), applied as
+// w <- w * kernel(r) per flow channel (terms.py:73-75); see oracle_set_robust.
+int g_rb_kind = 0;
+double g_rb_c = 1.0;
+std::vector<double> g_rb_mu;
+
+template <typename S>
+S robust_weight(int kind, S c, S mu, S r) {
+    if (kind == 1) {  // Huber
+        const S a = std::fabs(r);
+        return a <= c ? S(1) : c / std::max(a, S(1e-8));
+    }
+    if (kind == 2) {  // Tukey
+        const S t = std::max(S(1) - (r / c) * (r / c), S(0));
+        return t * t;
+    }
+    if (kind == 3) {  // GNC-TLS at scalar mu; mu = inf is the hard indicator
+        const S r2 = r * r, c2 = c * c;
+        if (!(mu < S(INFINITY))) return r2 < c2 ? S(1) : S(0);
+        if (r2 < (mu / (mu + S(1))) * c2) return S(1);
+        if (r2 <= ((mu + S(1)) / mu) * c2)
+            return std::max(std::sqrt(c2 * mu * (mu + S(1)) / std::max(r2, S(1e-12))) - mu, S(0));
+        return S(0);
+    }
+    return S(1);
+}
+
 // Static-chunked parallel for over [0, n) on g_threads std::threads (the
 // toolchain here ships no OpenMP runtime).
 template <typename F>
@@ -313,6 +340,11 @@ int run_ba(double* poses_io, double* disps_io, double* intr_io, const double* di
                 }
                 const S ru = S(targets[(((size_t)e * 2 + 0) * HW) + p]) - (fx * d * x + cx);
                 const S rv = S(targets[(((size_t)e * 2 + 1) * HW) + p]) - (fy * d * y + cy);
+                if (g_rb_kind != 0) {
+                    const S mu = S(g_rb_mu.empty() ? 1.0 : g_rb_mu[std::min<size_t>(itr, g_rb_mu.size() - 1)]);
+                    wu *= robust_weight(g_rb_kind, S(g_rb_c), mu, ru);
+                    wv *= robust_weight(g_rb_kind, S(g_rb_c), mu, rv);
+                }
                 T.energy += wu * ru * ru + wv * rv * rv;
                 for (int ch = 0; ch < 2; ch++) {
                     S J[12];
@@ -656,5 +688,12 @@ int oracle_accum_csr(const int64_t* ii, const int64_t* jj, int E, int t0, int t1
 // back-substitution, vipe/slam/ba/solver.py:183-186, has no such skip); the
 // default 0 is the fused kernel's behaviour.
 void oracle_set_backsub_all_rows(int all_rows) { g_backsub_all_rows = all_rows ? 1 : 0; }
+
+// kind 0 none, 1 Huber, 2 Tukey, 3 GNC-TLS; mu[i] is the GNC mu of iteration i (n entries)
+void oracle_set_robust(int kind, double c, const double* mu, int n) {
+    g_rb_kind = kind;
+    g_rb_c = c;
+    g_rb_mu.assign(mu, mu + (mu ? n : 0));
+}
 
 }  // extern "C"

@@ -27,6 +27,10 @@ steps that follow the call in the reference (`disps.clamp_(min=0.001)` and the
 intrinsics write-back, buffer.py:486-489 and :563) and compares with the generic
 solver's result at the reference test's tolerance.
 
+Robust kernels: config 0 with deterministic outlier flow is solved by the generic solver with
+Huber, Tukey and GNC-TLS (the reference's fused path refuses robust kernels); the results go
+to the "robust" entry and are held to vipe_slam_ba_extended_robust on the GPU.
+
 The same is done for a third case built from config 0 (8 keyframes, 48x64 disparity,
 26 edges, 2 iterations): GraphBuffer(384x512) is loaded with the config-0
 workload, then both solvers run as above.  Its large inputs (targets, weights)
@@ -258,6 +262,63 @@ def config0_case(rec):
             "digests": digests, "motion_only": False, "limited_disp": False, "optimize_intrinsics": False}
 
 
+ROBUST = {
+    # name: (robust_kernel, threshold, n_iters, gnc settings)
+    "huber": ("huber", 2.0, 3, {}),
+    "tukey": ("tukey", 4.0, 3, {}),
+    # GNC-TLS: two mu rounds of two iterations; mu 1 (soft weights), then min(3, 3) = mu_max
+    # (the hard TLS indicator)
+    "gnc_tls": ("gnc_tls", 3.0, 4, {"gnc_mu_init": 1.0, "gnc_mu_step": 3.0, "gnc_mu_max": 3.0,
+                                    "gnc_n_mu_steps": 2, "gnc_gn_iters_per_mu": 2}),
+}
+
+
+def robust_cases():
+    """Config 0 with deterministic outlier flow (tests/_graph_buffer_golden.with_outliers) solved
+    by the reference's generic solver with each robust kernel (buffer.py:531-695; the fused path
+    refuses robust kernels, buffer.py:541-545)."""
+    from vipe.slam.components.buffer import GraphBuffer
+    from vipe.slam.components.sparse_tracks import DummySparseTracks
+    from vipe.utils.cameras import CameraType
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    from _graph_buffer_golden import with_outliers
+
+    from vipe_b200 import workloads as W
+
+    p = W.ba_config0()
+    N, ht, wd = p.disps.shape
+    E = p.ii.shape[0]
+    targets = with_outliers(p.targets)
+    target = targets.permute(0, 2, 3, 1).reshape(E, ht * wd, 2).contiguous()
+    weight = p.weights.permute(0, 2, 3, 1).reshape(E, ht * wd, 2).contiguous()
+    disp_damping = ((p.eta.double() - 1e-7) / 0.2).float()
+    out = {}
+    for name, (kernel, thr, n_iters, gnc) in ROBUST.items():
+        cfg = _Cfg({"dense_disp_alpha": float(p.alpha), "fused": False, "intrinsics_damping_scale": 1.0,
+                    "robust_kernel": kernel, "robust_kernel_threshold": thr, "gnc_mu_init": 1.0,
+                    "gnc_mu_step": 3.0, "gnc_mu_max": 1.0e6, "gnc_n_mu_steps": 4, "gnc_gn_iters_per_mu": 6, **gnc})
+        v = GraphBuffer(height=8 * ht, width=8 * wd, n_views=1, buffer_size=N, init_disp=1.0, cross_view_idx=None,
+                        ba_config=cfg, sparse_tracks=DummySparseTracks(n_views=1), camera_type=CameraType.PINHOLE,
+                        device=torch.device("cpu"))
+        v.n_frames = N
+        v.tstamp[:N] = torch.arange(N)
+        v.intrinsics[0, :4] = p.intrinsics * 8
+        v.poses[:N] = p.poses
+        v.disps[:N, 0] = p.disps
+        v.disps_sens[:N, 0] = p.disps_sens
+        before = state_of(v)
+        v.bundle_adjustment(target=target.clone(), weight=weight.clone(), disp_damping=disp_damping.clone(),
+                            ii=p.ii.clone(), jj=p.jj.clone(), t0=p.t0, t1=p.t1, n_iters=n_iters,
+                            pose_damping=float(p.lm), pose_ep=float(p.ep), motion_only=False, limited_disp=False,
+                            optimize_intrinsics=False, optimize_rig_rotation=False, verbose=False)
+        # the starting state is config 0's (the "config0" case's "before")
+        assert torch.equal(before["poses"][:N], p.poses) and torch.equal(before["disps"][:N, 0], p.disps)
+        out[name] = {"kernel": kernel, "threshold": thr, "iterations": n_iters, "gnc": gnc,
+                     "generic": state_of(v), "n_frames": N}
+    return out
+
+
 def main(ref: Path):
     sys.path.insert(0, str(ROOT))
     rec = install_stubs(ref)
@@ -269,10 +330,12 @@ def main(ref: Path):
             mod, rec, motion_only=True, limited_disp=False, optimize_intrinsics=False, sparse=False),
         "config0": config0_case(rec),
     }
-    torch.save({"cases": cases, "torch": torch.__version__}, OUT)
+    robust = robust_cases()
+    torch.save({"cases": cases, "robust": robust, "torch": torch.__version__}, OUT)
     print(f"wrote {OUT} ({OUT.stat().st_size} bytes)")
-    for k, c in cases.items():
-        d = (c["generic"]["poses"] - c["before"]["poses"]).abs().max()
+    before = cases["config0"]["before"]["poses"]
+    for k, c in {**cases, **{"robust_" + k: v for k, v in robust.items()}}.items():
+        d = (c["generic"]["poses"] - c.get("before", {"poses": before})["poses"]).abs().max()
         print(f"  {k}: generic solver moved poses by {float(d):.3e}")
 
 

@@ -79,3 +79,46 @@ def test_volume_backward_vs_autograd_of_the_reference_ops():
     loss.backward()
     for got, want in ((d1, a.grad), (d2, b.grad)):
         assert (got.double() - want).abs().max() <= 2e-5 * want.abs().max()
+
+
+def _set_generic(on):
+    from vipe_b200 import _lib
+
+    _lib.load().vipe_corr_volume_backward_force_generic(int(on))
+
+
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+@pytest.mark.parametrize("shape,L", [((3, 128, 48, 64), 4), ((2, 96, 16, 64), 3), ((1, 128, 8, 128), 4),
+                                     ((2, 64, 8, 64), 1), ((2, 128, 16, 64), 2)])
+def test_tma_kernel_matches_producer_kernel(dtype, shape, L):
+    """The TMA-fed kernel (16-bit maps and gradients of one type, W % 64 == 0) against the
+    producer-formed kernel on the same inputs: both round Gt = G_0 + sum_l G_l / 4^l once, in
+    the same order, and accumulate the same K blocks in the same order, so the FP32 gradients
+    agree to the bit."""
+    g = torch.Generator(device="cuda").manual_seed(52)
+    num, C, H, W = shape
+    f1 = (torch.randn(num, C, H, W, generator=g, device="cuda") / C**0.5).to(dtype)
+    f2 = (torch.randn(num, C, H, W, generator=g, device="cuda") / C**0.5).to(dtype)
+    grads = [torch.randn(num, H * W, H >> l, W >> l, generator=g, device="cuda").to(dtype) for l in range(L)]
+    fast = _backward(f1, f2, grads, dtype)
+    _set_generic(True)
+    try:
+        slow = _backward(f1, f2, grads, dtype)
+    finally:
+        _set_generic(False)
+    for a, b in zip(fast, slow):
+        torch.testing.assert_close(a, b, atol=0, rtol=0)
+
+
+@pytest.mark.parametrize("shape,L", [((2, 96, 16, 64), 3), ((1, 128, 8, 128), 4)])
+def test_tma_kernel_vs_fp64_oracle(shape, L):
+    g = torch.Generator().manual_seed(53)
+    num, C, H, W = shape
+    f1 = (torch.randn(num, C, H, W, generator=g) / C**0.5).half()
+    f2 = (torch.randn(num, C, H, W, generator=g) / C**0.5).half()
+    grads = [torch.randn(num, H * W, H >> l, W >> l, generator=g).half() for l in range(L)]
+    d1, d2 = _backward(f1.cuda(), f2.cuda(), [x.cuda() for x in grads], torch.float16)
+    w1, w2 = oc.corr_pyramid_backward(f1.double().numpy(), f2.double().numpy(), [x.double().numpy() for x in grads])
+    for got, want in ((d1, w1), (d2, w2)):
+        got = got.double().cpu().numpy()
+        assert np.abs(got - want).max() <= 2e-3 * np.abs(want).max()

@@ -82,3 +82,29 @@ def test_fixture_config0_inputs_are_the_workload_generators():
     case = G.cases()["config0"]
     args = G.args_of(case)  # raises if the regenerated targets / weights differ from the recorded ones
     assert args[4].shape == (26, 2, 48, 64) and args[12] == 2
+
+
+def _oracle_robust(case, args, kernel, thr, sched, fp64):
+    kind = {"huber": 1, "tukey": 2, "gnc_tls": 3}[kernel]
+    p = types.SimpleNamespace(poses=args[0].double().numpy(), disps=args[1].double().numpy(),
+                              intrinsics=args[2].double().numpy(), disps_sens=args[3], targets=args[4],
+                              weights=args[5], eta=args[6], ii=args[7], jj=args[8], depth_active=args[9],
+                              t0=args[10], t1=args[11], iterations=args[12], lm=args[13], ep=args[14], alpha=args[16])
+    return ob.ba(p, fp64=fp64, backsub_all_rows=True, robust_kind=kind, robust_threshold=thr, mu_schedule=sched)
+
+
+@pytest.mark.parametrize("name", ["huber", "tukey", "gnc_tls"])
+def test_robust_oracle_matches_reference_generic_solver(name):
+    """The oracle's robust kernels (w <- w * kernel(r) per flow channel, all back-substitution
+    rows) against the reference's generic solver with the same kernel on config 0 with outliers;
+    the robust solve also differs from the plain one (the weights matter)."""
+    case, args, kernel, thr, sched = G.robust_setup(name)
+    r = _oracle_robust(case, args, kernel, thr, sched, fp64=False)
+    n = case["n_frames"]
+    G.assert_robust_matches_generic(name, torch.from_numpy(r["poses"]), torch.from_numpy(r["disps"])[:, None])
+    plain = ob.ba(types.SimpleNamespace(poses=args[0].double().numpy(), disps=args[1].double().numpy(),
+                                        intrinsics=args[2].double().numpy(), disps_sens=args[3], targets=args[4],
+                                        weights=args[5], eta=args[6], ii=args[7], jj=args[8], depth_active=args[9],
+                                        t0=args[10], t1=args[11], iterations=args[12], lm=args[13], ep=args[14],
+                                        alpha=args[16]), fp64=False, backsub_all_rows=True)
+    assert float(np.abs(plain["poses"][:n] - r["poses"][:n]).max()) > 1e-3

@@ -37,6 +37,11 @@ _SIGS: dict[str, tuple] = {
         [P, P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, F, I, F, I, F, F, F, I, P, P, P, P, SZ, P, P],
     ),
     "vipe_slam_ba": (I, [P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, F, I, F, P, P, P, P, SZ, P, P]),
+    "vipe_slam_ba_extended_robust": (
+        I,
+        [P, P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, F, I, F, I, F, F, F, I, P, P, P, I, F, P, P, SZ,
+         P, P],
+    ),
     "vipe_slam_ba_extended_noalloc": (
         I,
         [P, P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, F, I, F, I, F, F, F, I, P, P, P, P, P],
@@ -75,6 +80,7 @@ _SIGS: dict[str, tuple] = {
     "vipe_slam_proximity_edges": (I, [P, P, P, I, I, I, I, I, I, F, I, I, P, P, I, P, P, SZ, P]),
     "vipe_corr_volume_workspace_size": (SZ, [I, I, I, I]),
     "vipe_corr_volume_backward": (I, [I, I, P, P, P, I, I, I, I, I, P, P, P, P]),
+    "vipe_corr_volume_backward_force_generic": (None, [I]),
     "vipe_corr_encoder_lookup": (I, [I, P, I, P, I, I, I, P, P, P, P, P]),
     "vipe_hbm_write_probe": (I, [P, SZ, P]),
     "vipe_corr_volume_build": (I, [I, I, P, P, I, I, I, I, I, P, P, SZ, P]),

@@ -500,9 +500,11 @@ __device__ __forceinline__ void linearize_sim3(const EdgeTf& T, bool stereo, flo
 template <int D, bool kIntr, bool kResidual>
 __device__ __forceinline__ void linearize_d(const EdgeTf& T, bool stereo, float fx, float fy, float cx, float cy,
                                             float u, float v, float disp, float wu, float wv, float tu, float tv,
-                                            float act, float iscale, typename LinOf<D>::T& L) {
+                                            float act, float iscale, typename LinOf<D>::T& L,
+                                            const RobustSpec rb = RobustSpec{}) {
     if constexpr (D == 6)
-        linearize<kIntr, kResidual>(T.t, T.q, stereo, fx, fy, cx, cy, u, v, disp, wu, wv, tu, tv, act, iscale, L);
+        linearize<kIntr, kResidual>(T.t, T.q, stereo, fx, fy, cx, cy, u, v, disp, wu, wv, tu, tv, act, iscale, L,
+                                    rb);
     else
         linearize_sim3<kResidual>(T, stereo, fx, fy, cx, cy, u, v, disp, wu, wv, tu, tv, act, L);
 }
@@ -545,7 +547,7 @@ __global__ void __launch_bounds__(kEdgeThreads, (D == 6 && !kIntr) ? 4 : 1) ba_e
         const float u = (float)(p % W), v = (float)(p / W);
         typename LinOf<D>::T L;
         linearize_d<D, kIntr, true>(Tf, stereo, fx, fy, cx, cy, u, v, __ldg(dp + p), __ldg(wu + p),
-                                    __ldg(wu + HW + p), __ldg(tu + p), __ldg(tu + HW + p), 1.0f, A.iscale, L);
+                                    __ldg(wu + HW + p), __ldg(tu + p), __ldg(tu + HW + p), 1.0f, A.iscale, L, io.rb);
         en += L.we[0] * L.r[0] * L.r[0] + L.we[1] * L.r[1] * L.r[1];
 #pragma unroll
         for (int ch = 0; ch < 2; ch++) {
@@ -897,7 +899,7 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
                     }
                     typename LinOf<D>::T L;
                     linearize_d<D, kIntr, true>(Tf, stereo, fx, fy, cx, cy, u, v, disp, w0, w1, t0v, t1v, act,
-                                                A.iscale, L);
+                                                A.iscale, L, io.rb);
                     const float g0 = L.wd[0] * L.Jz[0], g1 = L.wd[1] * L.Jz[1];
                     csum += g0 * L.Jz[0] + g1 * L.Jz[1];
                     bsum += g0 * L.r[0] + g1 * L.r[1];
@@ -1188,7 +1190,7 @@ __global__ void __launch_bounds__(kWideThreads) ba_frame_wide_kernel(BAPtrs base
                     PixelLin L;
                     linearize_d<D, kIntr, true>(Tf, b == k, fx, fy, cx, cy, uu, vv, disp, __ldg(A.weights + o),
                                                 __ldg(A.weights + o + HW), __ldg(A.targets + o),
-                                                __ldg(A.targets + o + HW), act, A.iscale, L);
+                                                __ldg(A.targets + o + HW), act, A.iscale, L, io.rb);
                     const float g0 = L.wd[0] * L.Jz[0], g1 = L.wd[1] * L.Jz[1];
                     csum += g0 * L.Jz[0] + g1 * L.Jz[1];
                     bsum += g0 * L.r[0] + g1 * L.r[1];
@@ -2062,8 +2064,9 @@ __global__ void __launch_bounds__(256, (D == 6 && !kIntr) ? 8 : 3) ba_backsub_ke
     const float act = A.depth_active[k];
     const int self = w.self_slot[s];
     const int selfpose = self >= 0 ? w.fp_list[w.fp_ptr[s] + self] : -1;
-    // rows whose pose is t0 are skipped (geom_kernels.cu:1186)
-    const bool self_on = selfpose > 0 && selfpose < P;
+    // rows whose pose is t0 are skipped (geom_kernels.cu:1186) unless the solve asks for every row
+    const int first_row = io.exact_backsub ? 0 : 1;
+    const bool self_on = selfpose >= first_row && selfpose < P;
     const int eb = w.fe_ptr[s], ee = w.fe_ptr[s + 1];
     const float fx = A.intr[0], fy = A.intr[1], cx = A.intr[2], cy = A.intr[3];
     const float df = kIntr ? (float)w.df[0] : 0.f;
@@ -2077,7 +2080,7 @@ __global__ void __launch_bounds__(256, (D == 6 && !kIntr) ? 8 : 3) ba_backsub_ke
         const int e = w.fe_list[eb + q];
         const int b = (int)A.jj[e];
         const int bp = b - d.t0;
-        const bool on = w.edge_slot[e] >= 0 && bp > 0 && bp < P;
+        const bool on = w.edge_slot[e] >= 0 && bp >= first_row && bp < P;
         EdgeTf Tf;
         edge_tf<D>(A.poses, k, b, Tf);
         float vi[D], vo[D];
@@ -2114,7 +2117,7 @@ __global__ void __launch_bounds__(256, (D == 6 && !kIntr) ? 8 : 3) ba_backsub_ke
                 Tf.s = t[7];
             } else {
                 const int bp = b - d.t0;
-                const bool on = w.edge_slot[e] >= 0 && bp > 0 && bp < P;
+                const bool on = w.edge_slot[e] >= 0 && bp >= first_row && bp < P;
                 if (!on && !self_on) continue;
                 edge_tf<D>(A.poses, k, b, Tf);
                 float vi[D], vo[D];
@@ -2126,8 +2129,12 @@ __global__ void __launch_bounds__(256, (D == 6 && !kIntr) ? 8 : 3) ba_backsub_ke
             }
             const float* wp = A.weights + (size_t)e * 2 * HW;
             typename LinOf<D>::T L;
+            // robust reweighting needs the residual, hence the targets
+            const float* tp = A.targets + (size_t)e * 2 * HW;
+            const bool rob = io.rb.kind != 0;
             linearize_d<D, false, false>(Tf, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p), __ldg(wp + HW + p),
-                                         0.f, 0.f, act, 1.f, L);
+                                         rob ? __ldg(tp + p) : 0.f, rob ? __ldg(tp + HW + p) : 0.f, act, 1.f, L,
+                                         io.rb);
 #pragma unroll
             for (int ch = 0; ch < 2; ch++) {
                 const float g = L.wd[ch] * L.Jz[ch];
@@ -2419,11 +2426,13 @@ struct Tape {
     long frames = 0, hw = 0, factor_stride = 0, poses6 = 0;
 };
 
-int run_solve(const Geometry& geo, const GraphDesc* d_table, const int* d_off, const BAPtrs& base,
+int run_solve(const Geometry& geo, const GraphDesc* d_table, const int* d_off, const BAPtrs& base0,
               const GraphDesc* init, const SolveArgs& a, cudaStream_t st, const Tape* tape = nullptr) {
-    int rc = launch_index(geo, d_table, base, init, st);
+    int rc = launch_index(geo, d_table, base0, init, st);
     if (rc != VIPE_OK) return rc;
     for (int itr = 0; itr < a.iterations; itr++) {
+        BAPtrs base = base0;
+        if (a.mu_sched) base.rb.mu = a.mu_sched[itr];  // the GNC schedule's mu for this iteration
         if (tape) {
             VIPE_CUDA_TRY(cudaMemcpyAsync(tape->poses + (size_t)itr * tape->frames * (geo.dof + 1), base.poses,
                                           sizeof(float) * tape->frames * (geo.dof + 1), cudaMemcpyDeviceToDevice, st));
@@ -2446,8 +2455,8 @@ int run_solve(const Geometry& geo, const GraphDesc* d_table, const int* d_off, c
         }
         if ((rc = launch_update(geo, d_table, d_off, base, a, st)) != VIPE_OK) return rc;
     }
-    if (base.status) {
-        ba_status_kernel<<<geo.G, 1, 0, st>>>(base, Batch{d_table, nullptr, geo.G});
+    if (base0.status) {
+        ba_status_kernel<<<geo.G, 1, 0, st>>>(base0, Batch{d_table, nullptr, geo.G});
         VIPE_LAUNCH_CHECK();
     }
     return VIPE_OK;
@@ -2499,14 +2508,15 @@ static int check_ba_args(const float* poses_io, const float* disps_io, const flo
     return VIPE_OK;
 }
 
-extern "C" int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* intrinsics_io, const float* disps_sens,
-                                     const float* targets, const float* weights, const float* eta, const int64_t* ii,
-                                     const int64_t* jj, const float* depth_active, int num_frames, int ht, int wd,
-                                     int num_edges, int num_kx, int t0, int t1, int iterations, float lm, float ep,
-                                     int motion_only, float alpha, int optimize_intrinsics, float intrinsics_lm,
-                                     float intrinsics_ep, float intrinsics_scale, int compute_energy, float* dx_out,
-                                     float* dz_out, float* energy_out, void* workspace, size_t workspace_bytes,
-                                     int32_t* dev_status, void* stream) {
+static int ba_extended_impl(float* poses_io, float* disps_io, float* intrinsics_io, const float* disps_sens,
+                            const float* targets, const float* weights, const float* eta, const int64_t* ii,
+                            const int64_t* jj, const float* depth_active, int num_frames, int ht, int wd,
+                            int num_edges, int num_kx, int t0, int t1, int iterations, float lm, float ep,
+                            int motion_only, float alpha, int optimize_intrinsics, float intrinsics_lm,
+                            float intrinsics_ep, float intrinsics_scale, int compute_energy, float* dx_out,
+                            float* dz_out, float* energy_out, const RobustSpec& rb, int exact_backsub,
+                            const float* mu_sched, void* workspace, size_t workspace_bytes, int32_t* dev_status,
+                            void* stream) {
     int rc = check_dims(num_frames, ht, wd, num_edges, num_kx, t0, t1);
     if (rc != VIPE_OK) return rc;
     rc = check_ba_args(poses_io, disps_io, intrinsics_io, disps_sens, targets, weights, eta, ii, jj, depth_active,
@@ -2524,9 +2534,61 @@ extern "C" int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* in
     BAPtrs base{poses_io, disps_io, intrinsics_io, disps_sens, targets, weights, eta, ii, jj, depth_active,
                 dx_out, motion_only ? nullptr : dz_out, compute_energy ? energy_out : nullptr, dev_status,
                 iterations, 0};
+    base.rb = rb;
+    base.exact_backsub = exact_backsub;
     SolveArgs a{iterations, lm, ep, alpha, motion_only, optimize_intrinsics, intrinsics_lm, intrinsics_ep,
                 intrinsics_scale, compute_energy};
+    a.mu_sched = mu_sched;
     return run_solve(geo, table, nullptr, base, &gd, a, st);
+}
+
+extern "C" int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* intrinsics_io, const float* disps_sens,
+                                     const float* targets, const float* weights, const float* eta, const int64_t* ii,
+                                     const int64_t* jj, const float* depth_active, int num_frames, int ht, int wd,
+                                     int num_edges, int num_kx, int t0, int t1, int iterations, float lm, float ep,
+                                     int motion_only, float alpha, int optimize_intrinsics, float intrinsics_lm,
+                                     float intrinsics_ep, float intrinsics_scale, int compute_energy, float* dx_out,
+                                     float* dz_out, float* energy_out, void* workspace, size_t workspace_bytes,
+                                     int32_t* dev_status, void* stream) {
+    return ba_extended_impl(poses_io, disps_io, intrinsics_io, disps_sens, targets, weights, eta, ii, jj,
+                            depth_active, num_frames, ht, wd, num_edges, num_kx, t0, t1, iterations, lm, ep,
+                            motion_only, alpha, optimize_intrinsics, intrinsics_lm, intrinsics_ep, intrinsics_scale,
+                            compute_energy, dx_out, dz_out, energy_out, RobustSpec{}, 0, nullptr, workspace,
+                            workspace_bytes, dev_status, stream);
+}
+
+extern "C" int vipe_slam_ba_extended_robust(float* poses_io, float* disps_io, float* intrinsics_io,
+                                            const float* disps_sens, const float* targets, const float* weights,
+                                            const float* eta, const int64_t* ii, const int64_t* jj,
+                                            const float* depth_active, int num_frames, int ht, int wd, int num_edges,
+                                            int num_kx, int t0, int t1, int iterations, float lm, float ep,
+                                            int motion_only, float alpha, int optimize_intrinsics, float intrinsics_lm,
+                                            float intrinsics_ep, float intrinsics_scale, int compute_energy,
+                                            float* dx_out, float* dz_out, float* energy_out, int robust_kind,
+                                            float robust_threshold, const float* mu_schedule, void* workspace,
+                                            size_t workspace_bytes, int32_t* dev_status, void* stream) {
+    if (robust_kind < 0 || robust_kind > 3) {
+        set_last_error("robust BA: robust_kind must be 0 (none), 1 (Huber), 2 (Tukey) or 3 (GNC-TLS)");
+        return VIPE_ERR_ARG;
+    }
+    if (robust_kind != 0 && !(robust_threshold > 0.f)) return VIPE_ERR_ARG;
+    if (robust_kind == 3 && !mu_schedule) {
+        set_last_error("robust BA: GNC-TLS needs the mu of every iteration");
+        return VIPE_ERR_ARG;
+    }
+    if (robust_kind == 3)
+        for (int k = 0; k < iterations; k++)
+            if (!(mu_schedule[k] > 0.f)) return VIPE_ERR_ARG;
+    RobustSpec rb;
+    rb.kind = robust_kind;
+    rb.c = robust_threshold > 0.f ? robust_threshold : 1.f;
+    rb.mu = 1.f;
+    return ba_extended_impl(poses_io, disps_io, intrinsics_io, disps_sens, targets, weights, eta, ii, jj,
+                            depth_active, num_frames, ht, wd, num_edges, num_kx, t0, t1, iterations, lm, ep,
+                            motion_only, alpha, optimize_intrinsics, intrinsics_lm, intrinsics_ep, intrinsics_scale,
+                            compute_energy, dx_out, dz_out, energy_out, rb, 1,
+                            robust_kind == 3 ? mu_schedule : nullptr, workspace, workspace_bytes, dev_status,
+                            stream);
 }
 
 // ---------------------------------------------------------------- batched solve

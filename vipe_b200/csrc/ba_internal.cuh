@@ -4,6 +4,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "se3_device.cuh"
 
 #include <algorithm>
 #include <vector>
@@ -262,6 +263,10 @@ struct BAPtrs {
     float* g_eta;      // (depth rows, H, W) out (accumulated)
     float* g_dsens;    // (frames, H, W) out (accumulated)
     double* ftape;     // one iteration of the tape record (graph slots at ftape_off): factor, (Q, w)
+    RobustSpec rb;     // robust reweighting of the flow residuals (kind 0: none)
+    int exact_backsub; // 1: the depth back-substitution keeps the rows of pose t0 (the generic
+                       // solver's Schur back-substitution); 0: skips them like the reference's
+                       // fused kernel (geom_kernels.cu:1186)
 };
 
 // factor tape slot of one graph: the Cholesky factor (dim x dim, lower
@@ -341,6 +346,8 @@ __device__ __forceinline__ BAPtrs rebase(const BAPtrs& b, const GraphDesc& g) {
     p.g_eta = b.g_eta ? b.g_eta + g.kx_off * HW : nullptr;
     p.g_dsens = b.g_dsens ? b.g_dsens + g.frame_off * HW : nullptr;
     p.ftape = b.ftape ? b.ftape + g.ftape_off : nullptr;
+    p.rb = b.rb;
+    p.exact_backsub = b.exact_backsub;
     return p;
 }
 
@@ -447,6 +454,7 @@ struct SolveArgs {
     int motion_only, intr;
     float ilm, iep, iscale;
     int compute_energy;
+    const float* mu_sched = nullptr;  // host: the robust kernel's mu at each iteration (GNC), or none
 };
 
 // host launchers implemented in ba.cu

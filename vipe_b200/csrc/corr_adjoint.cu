@@ -24,17 +24,21 @@
 // 1/16 and written once.  Every mbarrier wait is bounded (2 s): on expiry the CTA sets
 // the error word, waits once more for its committed MMAs and frees its tensor memory.
 #include "common.cuh"
+#include "corr_window.cuh"
 #include "tcgen05.cuh"
+#include "tma.cuh"
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <type_traits>
 
 namespace vipe {
 namespace cadj {
 
 using namespace ::vipe::tc;
+using ::vipe::corr::to_f;
 
 constexpr int kThreads = 256;
 constexpr int kTile = 128;                   // M (channels) and N (output pixels)
@@ -279,6 +283,243 @@ __global__ void __launch_bounds__(kThreads, 1) corr_vol_bwd_kernel(Params a) {
     }
 }
 
+
+// ---------------------------------------------------------------- TMA-fed kernel
+//
+// The production shapes (16-bit maps and level gradients of one type, W a multiple of 64,
+// H and W multiples of 2^(levels-1)) take a warp-specialised persistent kernel whose
+// operands arrive by TMA:
+//   warp 8 lane 0   TMA: per 64-wide K block, the map tile (channels x 64 K, 128-byte
+//                   swizzle), the G_0 tile (output pixels x 64 target pixels; pass 1 two
+//                   64-pixel halves x 64 source rows, MN-major) and the G_l tiles that pool
+//                   those target pixels (64 >> l cells per row, unswizzled) into a stage;
+//   warps 0-3       combine: G_0 += sum_l G_l / 4^l in place, 16 bytes (8 target pixels of
+//                   one image row) per thread step, rounded once to the operand type;
+//   warp 9 lane 0   tcgen05.mma kind::f16, M = 128 channels, N = 128 output pixels, K = 16,
+//                   into one of two tensor-memory accumulators (pass 1: B MN-major);
+//   warps 4-7       epilogue: tcgen05.ld, x 1/16, FP32 stores; the accumulator is then free.
+// Four stages of 46 KB; every G_0 element is read from HBM once per pass, the level tiles
+// and the map rows come mostly from L2.
+
+constexpr int kFStages = 4;
+constexpr int kFThreads = 320;
+constexpr int kFTmaWarp = 8, kFMmaWarp = 9;
+constexpr uint32_t kFA = 16384;                 // map tile: 128 rows x 128 B
+constexpr uint32_t kFG = 16384;                 // G_0 tile
+// level-l tile bytes (l = 1..3): 128 rows (both halves in pass 1) x (128 >> l) B
+__host__ __device__ constexpr uint32_t kFL(int l) { return l == 1 ? 8192u : l == 2 ? 4096u : l == 3 ? 2048u : 0u; }
+constexpr uint32_t kFStage = kFA + kFG + 8192 + 4096 + 2048;
+
+struct FastParams {
+    float* out;
+    int* err;
+    int C, W, HW, L, pass, blocks;
+    long items;
+};
+
+__device__ __forceinline__ uint8_t* fstage(uint8_t* base, int s) { return base + (size_t)s * kFStage; }
+
+template <typename OpT>
+__global__ void __launch_bounds__(kFThreads, 1)
+    corr_vol_bwd_tma_kernel(const __grid_constant__ CUtensorMap mapF, const __grid_constant__ CUtensorMap mapG0,
+                            const __grid_constant__ CUtensorMap mapG1, const __grid_constant__ CUtensorMap mapG2,
+                            const __grid_constant__ CUtensorMap mapG3, FastParams a) {
+    constexpr int FMT = std::is_same<OpT, __half>::value ? kFmtF16 : kFmtBF16;
+    extern __shared__ uint8_t sm_raw[];
+    __shared__ uint64_t full[kFStages], ready[kFStages], empty[kFStages], accf[2], acce[2];
+    __shared__ uint32_t tmem_base;
+    __shared__ volatile int fail;
+    uint8_t* sm = sm_raw + ((1024u - (smem_u32(sm_raw) & 1023u)) & 1023u);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int pass = a.pass, W = a.W, HW = a.HW, L = a.L;
+    const int R = pass == 0 ? 128 : 64;  // G rows (K-major rows / MN-major K rows) per half
+    const int nk = HW / 64;
+    if (tid == 0) {
+        fail = 0;
+        for (int s = 0; s < kFStages; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&ready[s], 4);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&accf[b], 1);
+            mbar_init(&acce[b], 4);
+        }
+        fence_barrier_init();
+    }
+    if (warp == kFMmaWarp) tmem_alloc(&tmem_base, 2 * kTile);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base;
+    const CUtensorMap* mg[4] = {&mapG0, &mapG1, &mapG2, &mapG3};
+
+    if (warp == kFTmaWarp && lane == 0) {
+        // ------------------------------------------------ TMA producer
+        uint32_t bytes = (uint32_t)min(a.C, kTile) * 128u + kFG;
+        for (int l = 1; l < L; l++) bytes += kFL(l);
+        uint32_t g = 0;
+        for (long item = blockIdx.x; item < a.items && !fail; item += gridDim.x) {
+            const int n = (int)(item / a.blocks), o0 = (int)(item % a.blocks) * kTile;
+            for (int kb = 0; kb < nk; kb++, g++) {
+                const int s = (int)(g % kFStages);
+                if (g >= kFStages && !mbar_wait(&empty[s], ((g / kFStages) - 1) & 1, &fail)) break;
+                uint8_t* st = fstage(sm, s);
+                mbar_expect_tx(&full[s], bytes);
+                tma_load_3d(st, &mapF, &full[s], kb * 64, 0, n);
+                uint8_t* lv = st + kFA + kFG;
+                if (pass == 0) {
+                    // rows o0.. (output pixels), K = target pixels kb*64 .. +63 (one image row)
+                    const int q0 = kb * 64, y = q0 / W, x0 = q0 % W;
+                    tma_load_2d(st + kFA, mg[0], &full[s], q0, n * HW + o0);
+                    for (int l = 1; l < L; l++) {
+                        tma_load_2d(lv, mg[l], &full[s], (y >> l) * (W >> l) + (x0 >> l), n * HW + o0);
+                        lv += kFL(l);
+                    }
+                } else {
+                    // K rows = source pixels kb*64 .., two 64-pixel halves of the output block
+                    for (int h = 0; h < 2; h++) {
+                        const int q0 = o0 + 64 * h, y = q0 / W, x0 = q0 % W;
+                        tma_load_2d(st + kFA + h * 8192, mg[0], &full[s], q0, n * HW + kb * 64);
+                        uint8_t* lh = lv;
+                        for (int l = 1; l < L; l++) {
+                            tma_load_2d(lh + h * (kFL(l) / 2), mg[l], &full[s], (y >> l) * (W >> l) + (x0 >> l),
+                                        n * HW + kb * 64);
+                            lh += kFL(l);
+                        }
+                    }
+                }
+            }
+        }
+        if (fail && g > 0) {
+            // the loads already issued must land before the CTA exits (bounded)
+            const uint64_t t0 = gtimer();
+            for (uint32_t k = (g > kFStages ? g - kFStages : 0); k < g; k++)
+                while (!mbar_try_wait(&full[k % kFStages], (k / kFStages) & 1) && gtimer() - t0 < kTmaWaitNs) {
+                }
+        }
+    } else if (warp < 4) {
+        // ------------------------------------------------ combine: G_0 += sum_l G_l / 4^l
+        uint32_t g = 0;
+        for (long item = blockIdx.x; item < a.items && !fail; item += gridDim.x) {
+            for (int kb = 0; kb < nk; kb++, g++) {
+                const int s = (int)(g % kFStages);
+                if (!mbar_wait(&full[s], (g / kFStages) & 1, &fail)) break;
+                uint8_t* st = fstage(sm, s);
+                uint8_t* g0 = st + kFA;
+                const uint8_t* lv1 = st + kFA + kFG;
+                const uint8_t* lv2 = lv1 + kFL(1);
+                const uint8_t* lv3 = lv2 + kFL(2);
+                if (L > 1) {
+#pragma unroll 2
+                    for (int i = tid; i < 1024; i += 128) {
+                        const int j = i & 7;                                    // 16-byte chunk: 8 pixels
+                        const int h = pass == 0 ? 0 : (i >> 9);                 // pass 1: 64-pixel half
+                        const int r = pass == 0 ? (i >> 3) : ((i >> 3) & 63);   // G row in the half
+                        const int hr = h * R + r;                               // row in the level tiles
+                        uint4* cp = reinterpret_cast<uint4*>(g0 + h * 8192 + r * 128 + (((j ^ r) & 7) << 4));
+                        uint4 raw = *cp;
+                        OpT* v = reinterpret_cast<OpT*>(&raw);
+                        float acc[8];
+#pragma unroll
+                        for (int e = 0; e < 8; e++) acc[e] = to_f(v[e]);
+                        {
+                            const uint2 c1 = *reinterpret_cast<const uint2*>(lv1 + hr * 64 + 8 * j);
+                            const OpT* w1 = reinterpret_cast<const OpT*>(&c1);
+#pragma unroll
+                            for (int e = 0; e < 8; e++) acc[e] += 0.25f * to_f(w1[e >> 1]);
+                        }
+                        if (L > 2) {
+                            const uint32_t c2 = *reinterpret_cast<const uint32_t*>(lv2 + hr * 32 + 4 * j);
+                            const OpT* w2 = reinterpret_cast<const OpT*>(&c2);
+#pragma unroll
+                            for (int e = 0; e < 8; e++) acc[e] += 0.0625f * to_f(w2[e >> 2]);
+                        }
+                        if (L > 3) {
+                            const float w3 = 0.015625f * to_f(*reinterpret_cast<const OpT*>(lv3 + hr * 16 + 2 * j));
+#pragma unroll
+                            for (int e = 0; e < 8; e++) acc[e] += w3;
+                        }
+#pragma unroll
+                        for (int e = 0; e < 8; e++) v[e] = to_op<OpT>(acc[e]);
+                        *cp = raw;
+                    }
+                }
+                fence_proxy_async();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&ready[s]);
+            }
+        }
+    } else if (warp == kFMmaWarp && lane == 0) {
+        // ------------------------------------------------ MMA issuer
+        const uint32_t idesc = instr_desc(FMT, kTile, kTile) | (pass == 1 ? (1u << 16) : 0u);
+        uint32_t g = 0, t = 0;
+        for (long item = blockIdx.x; item < a.items && !fail; item += gridDim.x, t++) {
+            const int b = (int)(t & 1);
+            if (t >= 2 && !mbar_wait(&acce[b], ((t >> 1) - 1) & 1, &fail)) break;
+            tc_fence_after();
+            const uint32_t d = tmem + (uint32_t)(b * kTile);
+            bool ok = true;
+            for (int kb = 0; kb < nk; kb++, g++) {
+                const int s = (int)(g % kFStages);
+                if (!mbar_wait(&ready[s], (g / kFStages) & 1, &fail)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                uint8_t* st = fstage(sm, s);
+                const uint64_t da = smem_desc_sw128(st);
+                const uint64_t db = pass == 0 ? smem_desc_sw128(st + kFA) : smem_desc_sw128_mn(st + kFA, 8192);
+                const uint64_t bstep = pass == 0 ? 2u : (uint64_t)(2048 >> 4);
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    mma_f16(d, da + (uint64_t)(2 * k), db + (uint64_t)k * bstep, idesc, (kb | k) ? 1u : 0u);
+                mma_commit(&empty[s]);
+            }
+            if (!ok) break;
+            mma_commit(&accf[b]);
+        }
+        if (fail && g > 0) {
+            // the committed MMAs get one more bounded chance before their tensor memory is freed
+            const uint32_t k = g - 1;
+            mbar_wait_bounded(&empty[k % kFStages], (k / kFStages) & 1, kTmaWaitNs);
+        }
+    } else if (warp >= 4 && warp < 8) {
+        // ------------------------------------------------ epilogue
+        const int q = warp & 3;  // tensor-memory lane quarter = channels 32q ..
+        const int c = 32 * q + lane;
+        uint32_t t = 0;
+        for (long item = blockIdx.x; item < a.items && !fail; item += gridDim.x, t++) {
+            const int b = (int)(t & 1);
+            const int n = (int)(item / a.blocks), o0 = (int)(item % a.blocks) * kTile;
+            if (!mbar_wait(&accf[b], (t >> 1) & 1, &fail)) break;
+            tc_fence_after();
+            float* orow = a.out + ((size_t)n * a.C + min(c, a.C - 1)) * HW + o0;
+            for (int c0 = 0; c0 < kTile; c0 += 16) {
+                float v[16];
+                tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * kTile + c0), v);
+                tmem_wait_ld();
+                if (c < a.C) {
+#pragma unroll
+                    for (int j = 0; j < 16; j += 4)
+                        *reinterpret_cast<float4*>(orow + c0 + j) =
+                            make_float4(v[j] * 0.0625f, v[j + 1] * 0.0625f, v[j + 2] * 0.0625f, v[j + 3] * 0.0625f);
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce[b]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (fail && tid == 0) atomicOr(a.err, 1);
+    if (warp == kFMmaWarp) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 2 * kTile);
+    }
+}
+
 }  // namespace cadj
 }  // namespace vipe
 
@@ -295,11 +536,84 @@ static int launch_vol_bwd(const Params& p, cudaStream_t st) {
     return VIPE_OK;
 }
 
+// (rows, cols) 16-bit matrix with row stride `cols`; box (box_cols, box_rows)
+static int make_map_2d(CUtensorMap* map, const void* base, CUtensorMapDataType dt, uint64_t rows, uint64_t cols,
+                       int box_cols, int box_rows, CUtensorMapSwizzle swz) {
+    EncodeTiled enc = get_encode();
+    if (!enc) return VIPE_ERR_CUDA;
+    const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? VIPE_OK : VIPE_ERR_CUDA;
+}
+
+// a feature map (num, C, HW) as dim 0 pixels, dim 1 channels, dim 2 maps; box 64 pixels x C
+static int make_fmap_map(CUtensorMap* map, const void* base, CUtensorMapDataType dt, int num, int C, int HW) {
+    EncodeTiled enc = get_encode();
+    if (!enc) return VIPE_ERR_CUDA;
+    const cuuint64_t dims[3] = {(cuuint64_t)HW, (cuuint64_t)C, (cuuint64_t)num};
+    const cuuint64_t strides[2] = {(cuuint64_t)HW * 2, (cuuint64_t)C * HW * 2};
+    const cuuint32_t box[3] = {64u, (cuuint32_t)C, 1u};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(map, dt, 3, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? VIPE_OK : VIPE_ERR_CUDA;
+}
+
+static int g_sms = 0;
+
+// one pass of the TMA-fed kernel; returns VIPE_ERR_CUDA when a tensor map does not encode
+template <typename OpT>
+static int launch_fast(const Params& p, int pass, const void* fmap, float* out, cudaStream_t st) {
+    const CUtensorMapDataType dt =
+        std::is_same<OpT, __half>::value ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    const int R = pass == 0 ? 128 : 64;
+    const uint64_t rows = (uint64_t)p.num * p.HW;
+    CUtensorMap mf, mg[4];
+    int rc = make_fmap_map(&mf, fmap, dt, p.num, p.C, p.HW);
+    if (rc == VIPE_OK) rc = make_map_2d(&mg[0], p.g[0], dt, rows, (uint64_t)p.HW, 64, R, CU_TENSOR_MAP_SWIZZLE_128B);
+    for (int l = 1; l < 4 && rc == VIPE_OK; l++) {
+        // levels past num_levels get a valid map of level 0 that the kernel never reads
+        if (l < p.L)
+            rc = make_map_2d(&mg[l], p.g[l], dt, rows, (uint64_t)(p.HW >> (2 * l)), 64 >> l, R,
+                             CU_TENSOR_MAP_SWIZZLE_NONE);
+        else
+            mg[l] = mg[0];
+    }
+    if (rc != VIPE_OK) return rc;
+    if (g_sms == 0) {
+        int dev = 0;
+        VIPE_CUDA_TRY(cudaGetDevice(&dev));
+        VIPE_CUDA_TRY(cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    FastParams fp{};
+    fp.out = out;
+    fp.err = p.err;
+    fp.C = p.C; fp.W = p.W; fp.HW = p.HW; fp.L = p.L; fp.pass = pass; fp.blocks = p.blocks;
+    fp.items = (long)p.num * p.blocks;
+    const size_t smem = (size_t)kFStages * kFStage + 1024;
+    VIPE_CUDA_TRY(cudaFuncSetAttribute(corr_vol_bwd_tma_kernel<OpT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    const long grid = std::min<long>(fp.items, (long)g_sms);
+    corr_vol_bwd_tma_kernel<OpT><<<(unsigned)grid, kFThreads, smem, st>>>(mf, mg[0], mg[1], mg[2], mg[3], fp);
+    VIPE_LAUNCH_CHECK();
+    return VIPE_OK;
+}
+
 template <typename FT>
 static int launch_pass(const Params& p, bool split, cudaStream_t st) {
     if (split) return launch_vol_bwd<float, FT, true>(p, st);
     return launch_vol_bwd<FT, FT, false>(p, st);
 }
+
+static int g_force_generic = 0;
+
+// 1: every shape takes the generic (producer-formed) kernel; used by tests to hold the two
+// kernels to each other
+extern "C" void vipe_corr_volume_backward_force_generic(int on) { g_force_generic = on ? 1 : 0; }
 
 extern "C" int vipe_corr_volume_backward(int map_dtype, int grad_dtype, const void* fmap1, const void* fmap2,
                                          const void* const* level_grads, int num, int C, int H, int W,
@@ -326,6 +640,21 @@ extern "C" int vipe_corr_volume_backward(int map_dtype, int grad_dtype, const vo
     const bool split = grad_dtype == VIPE_F32;
     cudaStream_t st = as_stream(stream);
     VIPE_PROF("corr_volume_bwd", st);
+    // TMA-fed kernel: 16-bit operands of one type, 64-pixel K blocks inside one image row, and
+    // every level's row stride a multiple of 16 bytes
+    const bool fast = grad_dtype == map_dtype && W % 64 == 0 && (HW >> (2 * (num_levels - 1))) % 8 == 0 &&
+                      g_force_generic == 0;
+    if (fast) {
+        for (int pass = 0; pass < 2; pass++) {
+            float* out = pass == 0 ? fmap1_grad_out : fmap2_grad_out;
+            if (!out) continue;
+            const void* fm = pass == 0 ? fmap2 : fmap1;
+            const int rc = map_dtype == VIPE_F16 ? launch_fast<__half>(p, pass, fm, out, st)
+                                                 : launch_fast<__nv_bfloat16>(p, pass, fm, out, st);
+            if (rc != VIPE_OK) return rc;
+        }
+        return VIPE_OK;
+    }
     for (int pass = 0; pass < 2; pass++) {
         float* out = pass == 0 ? fmap1_grad_out : fmap2_grad_out;
         if (!out) continue;

@@ -40,6 +40,7 @@
 
 #include "common.cuh"
 #include "tcgen05.cuh"
+#include "tma.cuh"
 
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -57,7 +58,7 @@ constexpr int kMaxKC = 2;      // up to 128 channels (A + two B stages fit in sh
 constexpr int kThreads = 320;  // 8 epilogue warps, 1 TMA warp, 1 MMA warp
 constexpr int kEpiWarps = 8;
 constexpr int kTmaWarp = 8, kMmaWarp = 9;
-constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s bound on any mbarrier wait
+constexpr uint64_t kWaitNs = tc::kTmaWaitNs;  // 2 s bound on any mbarrier wait
 constexpr int kTmaStage = 12288;  // per-warp staging of the TMA-store epilogue (1024-B aligned; <= Stage::per_warp)
 
 struct Params {
@@ -77,50 +78,6 @@ struct Params {
 // ---------------------------------------------------------------- PTX helpers
 
 using namespace ::vipe::tc;
-
-// bounded wait; returns false (and flags the CTA) when 2 s pass or another
-// role already failed
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* fail) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const uint64_t t0 = gtimer();
-    while (true) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if (*fail) return false;
-        if (gtimer() - t0 > kWaitNs) break;
-    }
-    *fail = 1;
-    return false;
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
-            smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
-        : "memory");
-}
-
-
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(
-            smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
-        : "memory");
-}
-
-// Shared-memory descriptor of an MN-major, 128-byte swizzled 16-bit operand: 64-element MN
-// atoms (128-byte rows, one per K index) `atom_bytes` apart, 8-row K groups 1024 B apart.
-__device__ __forceinline__ uint64_t smem_desc_sw128_mn(const void* base, uint32_t atom_bytes) {
-    const uint64_t addr = smem_u32(base);
-    uint64_t d = 0;
-    d |= (addr >> 4) & 0x3FFFull;                       // start address
-    d |= (uint64_t)((atom_bytes >> 4) & 0x3FFF) << 16;  // leading byte offset: next MN atom
-    d |= (uint64_t)(1024 >> 4) << 32;                   // stride byte offset: next 8 K rows
-    d |= (uint64_t)1 << 46;                             // descriptor version (sm100)
-    d |= (uint64_t)2 << 61;                             // SWIZZLE_128B
-    return d;
-}
 
 // TMA tensor store of a staged box (3-D map: target columns, source pixels, target
 // rows); completion is tracked per thread with bulk groups
@@ -751,23 +708,6 @@ __global__ void __launch_bounds__(256) pack_kernel(const TIn* __restrict__ f, TO
 
 
 // ---------------------------------------------------------------- host side
-
-using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiled get_encode() {
-    static EncodeTiled fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiled>(p);
-    });
-    return fn;
-}
 
 int make_map(CUtensorMap* map, void* base, CUtensorMapDataType dt, uint64_t rows, int Kp, int box_rows) {
     EncodeTiled enc = get_encode();

@@ -139,10 +139,44 @@ struct PixelLin {
     float Jf[2];      // focal Jacobian (when requested)
 };
 
+// Robust reweighting of the reprojection residuals, per flow channel, at the linearisation
+// point (the reference's generic solver: vipe/slam/ba/kernel.py:40-162, applied as
+// w <- w * kernel(r) by ConcreteTermEvalReturn.apply_robust_kernel, terms.py:73-75):
+//   kind 1 Huber    1 if |r| <= c else c / max(|r|, 1e-8)
+//   kind 2 Tukey    max(1 - (r/c)^2, 0)^2
+//   kind 3 GNC-TLS  at scalar mu: 1 below mu/(mu+1) c^2, 0 above (mu+1)/mu c^2, between
+//                   max(sqrt(c^2 mu (mu+1) / r^2) - mu, 0); mu = +inf: the hard TLS 1{r^2 < c^2}
+// kind 0: no reweighting.
+struct RobustSpec {
+    int kind = 0;
+    float c = 1.0f;
+    float mu = 1.0f;
+};
+
+__device__ __forceinline__ float robust_weight(const RobustSpec& rb, float r) {
+    if (rb.kind == 1) {
+        const float a = fabsf(r);
+        return a <= rb.c ? 1.0f : rb.c / fmaxf(a, 1e-8f);
+    }
+    if (rb.kind == 2) {
+        const float t = fmaxf(1.0f - (r / rb.c) * (r / rb.c), 0.0f);
+        return t * t;
+    }
+    if (rb.kind == 3) {
+        const float r2 = r * r, c2 = rb.c * rb.c, mu = rb.mu;
+        if (!(mu < INFINITY)) return r2 < c2 ? 1.0f : 0.0f;
+        if (r2 < (mu / (mu + 1.0f)) * c2) return 1.0f;
+        if (r2 <= ((mu + 1.0f) / mu) * c2) return fmaxf(sqrtf(c2 * mu * (mu + 1.0f) / fmaxf(r2, 1e-12f)) - mu, 0.0f);
+        return 0.0f;
+    }
+    return 1.0f;
+}
+
 template <bool kIntr, bool kResidual>
 __device__ __forceinline__ void linearize(const float* tij, const float* qij, bool stereo, float fx, float fy,
                                           float cx, float cy, float u, float v, float disp, float wu_in, float wv_in,
-                                          float tu, float tv, float act, float iscale, PixelLin& L) {
+                                          float tu, float tv, float act, float iscale, PixelLin& L,
+                                          const RobustSpec rb = RobustSpec{}) {
     float Xi[4] = {(u - cx) / fx, (v - cy) / fy, 1.0f, disp};
     float Xj[4];
     act_h(tij, qij, Xi, Xj);
@@ -150,8 +184,12 @@ __device__ __forceinline__ void linearize(const float* tij, const float* qij, bo
     const bool ok = !(Xj[2] < 0.25f);
     const float d = ok ? 1.0f / Xj[2] : 0.0f;
     const float d2 = d * d;
-    const float wu = ok ? 0.001f * wu_in : 0.0f;
-    const float wv = ok ? 0.001f * wv_in : 0.0f;
+    float wu = ok ? 0.001f * wu_in : 0.0f;
+    float wv = ok ? 0.001f * wv_in : 0.0f;
+    if (rb.kind != 0) {  // needs the residual even where the caller does not
+        wu *= robust_weight(rb, tu - (fx * d * x + cx));
+        wv *= robust_weight(rb, tv - (fy * d * y + cy));
+    }
     if (kIntr) {
         float dXi[4] = {-Xi[0] / fx, -Xi[1] / fy, 0.0f, 0.0f};
         float dXj[4];
