@@ -61,37 +61,51 @@ __device__ __forceinline__ float ld_any(const void* p, size_t i, int dt) {
     return __bfloat162float(static_cast<const __nv_bfloat16*>(p)[i]);
 }
 
-// Gt[p][q .. q+7] (8 consecutive target pixels in one image row): level 0 as one row chunk,
-// level l as the 8 >> l pooled values that cover them, each / 4^l
+// Pooled part of Gt for one pair of target pixels (x, x+1 with x even): levels 1 .. L-1, each
+// / 4^l, summed in this order.  Both kernels form Gt = G_0 + level_sum, so they round alike.
+__device__ __forceinline__ float level_sum(float l1, float l2, float l3, int L) {
+    float s = 0.25f * l1;
+    if (L > 2) s = fmaf(0.0625f, l2, s);
+    if (L > 3) s = fmaf(0.015625f, l3, s);
+    return s;
+}
+
+// Gt[p][q .. q+7] (8 consecutive target pixels in one image row, q % 8 == 0): level 0 as one
+// row chunk plus level_sum of the pooled values that cover each pixel pair
 __device__ __forceinline__ void unpooled8(const Params& a, int n, int p, int q, float* o) {
     const int W = a.W, y = q / W, x = q % W;
     const size_t HW = (size_t)a.HW;
+    const size_t row0 = ((size_t)n * HW + p) * HW + (size_t)y * W + x;
+    if (a.gdt == VIPE_F32) {
+        const float4* src = reinterpret_cast<const float4*>(static_cast<const float*>(a.g[0]) + row0);
+        const float4 u = src[0], v = src[1];
+        o[0] = u.x; o[1] = u.y; o[2] = u.z; o[3] = u.w;
+        o[4] = v.x; o[5] = v.y; o[6] = v.z; o[7] = v.w;
+    } else {
+        const uint4 raw = *reinterpret_cast<const uint4*>(static_cast<const uint16_t*>(a.g[0]) + row0);
+        const uint16_t* h = reinterpret_cast<const uint16_t*>(&raw);
 #pragma unroll
-    for (int i = 0; i < 8; i++) o[i] = 0.f;
-    for (int l = 0; l < a.L; l++) {
-        const int Wl = W >> l, HWl = (int)(HW >> (2 * l));
-        const size_t row = ((size_t)n * HW + p) * HWl + (size_t)(y >> l) * Wl;
-        const float s = 1.f / (float)(1 << (2 * l));
-        if (l == 0 && a.gdt == VIPE_F32) {
-            const float4* src = reinterpret_cast<const float4*>(static_cast<const float*>(a.g[0]) + row + x);
-            const float4 u = src[0], v = src[1];
-            o[0] += u.x; o[1] += u.y; o[2] += u.z; o[3] += u.w;
-            o[4] += v.x; o[5] += v.y; o[6] += v.z; o[7] += v.w;
-        } else if (l == 0) {
-            const uint4 raw = *reinterpret_cast<const uint4*>(static_cast<const uint16_t*>(a.g[0]) + row + x);
-            const uint16_t* h = reinterpret_cast<const uint16_t*>(&raw);
+        for (int i = 0; i < 8; i++)
+            o[i] = a.gdt == VIPE_F16 ? __half2float(__ushort_as_half(h[i])) : __bfloat162float(__ushort_as_bfloat16(h[i]));
+    }
+    if (a.L < 2) return;
+    float lv[4][4];  // [level][pixel pair]: the pooled value covering pair k (levels 1..3)
+    for (int l = 1; l < 4; l++) {
+        if (l >= a.L) {
 #pragma unroll
-            for (int i = 0; i < 8; i++) {
-                const uint16_t b = h[i];
-                o[i] += a.gdt == VIPE_F16 ? __half2float(__ushort_as_half(b)) : __bfloat162float(__ushort_as_bfloat16(b));
-            }
-        } else {
-            const int span = 1 << l;
-            for (int i = 0; i < 8; i += span) {
-                const float v = ld_any(a.g[l], row + ((x + i) >> l), a.gdt) * s;
-                for (int u = 0; u < span; u++) o[i + u] += v;
-            }
+            for (int k = 0; k < 4; k++) lv[l][k] = 0.f;
+            continue;
         }
+        const int Wl = W >> l, HWl = (int)(HW >> (2 * l));
+        const size_t row = ((size_t)n * HW + p) * HWl + (size_t)(y >> l) * Wl + (x >> l);
+#pragma unroll
+        for (int k = 0; k < 4; k++) lv[l][k] = ld_any(a.g[l], row + ((2 * k) >> l), a.gdt);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const float sk = level_sum(lv[1][k], lv[2][k], lv[3][k], a.L);
+        o[2 * k] += sk;
+        o[2 * k + 1] += sk;
     }
 }
 
@@ -289,23 +303,25 @@ __global__ void __launch_bounds__(kThreads, 1) corr_vol_bwd_kernel(Params a) {
 // The production shapes (16-bit maps and level gradients of one type, W a multiple of 64,
 // H and W multiples of 2^(levels-1)) take a warp-specialised persistent kernel whose
 // operands arrive by TMA:
-//   warp 8 lane 0   TMA: per 64-wide K block, the map tile (channels x 64 K, 128-byte
+//   warp 12 lane 0  TMA: per 64-wide K block, the map tile (channels x 64 K, 128-byte
 //                   swizzle), the G_0 tile (output pixels x 64 target pixels; pass 1 two
 //                   64-pixel halves x 64 source rows, MN-major) and the G_l tiles that pool
 //                   those target pixels (64 >> l cells per row, unswizzled) into a stage;
-//   warps 0-3       combine: G_0 += sum_l G_l / 4^l in place, 16 bytes (8 target pixels of
-//                   one image row) per thread step, rounded once to the operand type;
-//   warp 9 lane 0   tcgen05.mma kind::f16, M = 128 channels, N = 128 output pixels, K = 16,
+//   warps 0-7       combine: G_0 += level_sum in place, 16 bytes (8 target pixels of one
+//                   image row) per step, rounded once to the operand type;
+//   warp 13 lane 0  tcgen05.mma kind::f16, M = 128 channels, N = 128 output pixels, K = 16,
 //                   into one of two tensor-memory accumulators (pass 1: B MN-major);
-//   warps 4-7       epilogue: tcgen05.ld, x 1/16, FP32 stores; the accumulator is then free.
+//   warps 8-11      epilogue: tcgen05.ld, x 1/16, FP32 stores; the accumulator is then free.
 // Four stages of 46 KB; every G_0 element is read from HBM once per pass, the level tiles
 // and the map rows come mostly from L2.
 
 constexpr int kFStages = 4;
-constexpr int kFThreads = 320;
-constexpr int kFTmaWarp = 8, kFMmaWarp = 9;
-constexpr uint32_t kFA = 16384;                 // map tile: 128 rows x 128 B
-constexpr uint32_t kFG = 16384;                 // G_0 tile
+constexpr int kFCombineWarps = 8;
+constexpr int kFEpiWarp0 = 8;
+constexpr int kFTmaWarp = 12, kFMmaWarp = 13;
+constexpr int kFThreads = 32 * 14;
+constexpr uint32_t kFA = 16384;  // map tile: 128 rows x 128 B
+constexpr uint32_t kFG = 16384;  // G_0 tile
 // level-l tile bytes (l = 1..3): 128 rows (both halves in pass 1) x (128 >> l) B
 __host__ __device__ constexpr uint32_t kFL(int l) { return l == 1 ? 8192u : l == 2 ? 4096u : l == 3 ? 2048u : 0u; }
 constexpr uint32_t kFStage = kFA + kFG + 8192 + 4096 + 2048;
@@ -313,32 +329,78 @@ constexpr uint32_t kFStage = kFA + kFG + 8192 + 4096 + 2048;
 struct FastParams {
     float* out;
     int* err;
-    int C, W, HW, L, pass, blocks;
+    int C, W, HW, L, blocks;
     long items;
 };
 
 __device__ __forceinline__ uint8_t* fstage(uint8_t* base, int s) { return base + (size_t)s * kFStage; }
 
 template <typename OpT>
+__device__ __forceinline__ float2 to_f2(uint32_t v) {
+    if constexpr (std::is_same<OpT, __half>::value)
+        return __half22float2(*reinterpret_cast<const __half2*>(&v));
+    else
+        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&v));
+}
+
+template <typename OpT>
+__device__ __forceinline__ uint32_t from_f2(float a, float b) {
+    if constexpr (std::is_same<OpT, __half>::value) {
+        const __half2 h = __floats2half2_rn(a, b);
+        return *reinterpret_cast<const uint32_t*>(&h);
+    } else {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        return *reinterpret_cast<const uint32_t*>(&h);
+    }
+}
+
+// G_0 chunk (8 pixels, 4 pairs) += level_sum per pair, in place (the generic kernel's unpooled8)
+template <typename OpT>
+__device__ __forceinline__ void combine_chunk(uint4* cp, const uint8_t* l1p, const uint8_t* l2p, const uint8_t* l3p,
+                                              int L) {
+    uint4 raw = *cp;
+    float l1[4], l2[4] = {0.f, 0.f, 0.f, 0.f}, l3 = 0.f;
+    {
+        const uint2 c1 = *reinterpret_cast<const uint2*>(l1p);
+        const float2 a = to_f2<OpT>(c1.x), b = to_f2<OpT>(c1.y);
+        l1[0] = a.x; l1[1] = a.y; l1[2] = b.x; l1[3] = b.y;
+    }
+    if (L > 2) {
+        const float2 a = to_f2<OpT>(*reinterpret_cast<const uint32_t*>(l2p));
+        l2[0] = l2[1] = a.x;
+        l2[2] = l2[3] = a.y;
+    }
+    if (L > 3) l3 = to_f(*reinterpret_cast<const OpT*>(l3p));
+    uint32_t* w = reinterpret_cast<uint32_t*>(&raw);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const float sk = level_sum(l1[k], l2[k], l3, L);
+        const float2 g = to_f2<OpT>(w[k]);
+        w[k] = from_f2<OpT>(g.x + sk, g.y + sk);
+    }
+    *cp = raw;
+}
+
+template <typename OpT, int kPass>
 __global__ void __launch_bounds__(kFThreads, 1)
     corr_vol_bwd_tma_kernel(const __grid_constant__ CUtensorMap mapF, const __grid_constant__ CUtensorMap mapG0,
                             const __grid_constant__ CUtensorMap mapG1, const __grid_constant__ CUtensorMap mapG2,
                             const __grid_constant__ CUtensorMap mapG3, FastParams a) {
     constexpr int FMT = std::is_same<OpT, __half>::value ? kFmtF16 : kFmtBF16;
+    constexpr int R = kPass == 0 ? 128 : 64;  // G rows (K-major rows / MN-major K rows) per half
     extern __shared__ uint8_t sm_raw[];
     __shared__ uint64_t full[kFStages], ready[kFStages], empty[kFStages], accf[2], acce[2];
     __shared__ uint32_t tmem_base;
     __shared__ volatile int fail;
     uint8_t* sm = sm_raw + ((1024u - (smem_u32(sm_raw) & 1023u)) & 1023u);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int pass = a.pass, W = a.W, HW = a.HW, L = a.L;
-    const int R = pass == 0 ? 128 : 64;  // G rows (K-major rows / MN-major K rows) per half
+    const int W = a.W, HW = a.HW, L = a.L;
     const int nk = HW / 64;
     if (tid == 0) {
         fail = 0;
         for (int s = 0; s < kFStages; s++) {
             mbar_init(&full[s], 1);
-            mbar_init(&ready[s], 4);
+            mbar_init(&ready[s], kFCombineWarps);
             mbar_init(&empty[s], 1);
         }
         for (int b = 0; b < 2; b++) {
@@ -352,10 +414,10 @@ __global__ void __launch_bounds__(kFThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_base;
-    const CUtensorMap* mg[4] = {&mapG0, &mapG1, &mapG2, &mapG3};
 
     if (warp == kFTmaWarp && lane == 0) {
         // ------------------------------------------------ TMA producer
+        const CUtensorMap* mg[4] = {&mapG0, &mapG1, &mapG2, &mapG3};
         uint32_t bytes = (uint32_t)min(a.C, kTile) * 128u + kFG;
         for (int l = 1; l < L; l++) bytes += kFL(l);
         uint32_t g = 0;
@@ -368,7 +430,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
                 mbar_expect_tx(&full[s], bytes);
                 tma_load_3d(st, &mapF, &full[s], kb * 64, 0, n);
                 uint8_t* lv = st + kFA + kFG;
-                if (pass == 0) {
+                if (kPass == 0) {
                     // rows o0.. (output pixels), K = target pixels kb*64 .. +63 (one image row)
                     const int q0 = kb * 64, y = q0 / W, x0 = q0 % W;
                     tma_load_2d(st + kFA, mg[0], &full[s], q0, n * HW + o0);
@@ -398,51 +460,29 @@ __global__ void __launch_bounds__(kFThreads, 1)
                 while (!mbar_try_wait(&full[k % kFStages], (k / kFStages) & 1) && gtimer() - t0 < kTmaWaitNs) {
                 }
         }
-    } else if (warp < 4) {
-        // ------------------------------------------------ combine: G_0 += sum_l G_l / 4^l
+    } else if (warp < kFCombineWarps) {
+        // ------------------------------------------------ combine: G_0 += level_sum
+        // thread tid owns 16-byte chunk j = tid & 7 of rows r0 + 32 m (pass 0) or of row
+        // r0 + 32 (m & 1) in half m >> 1 (pass 1); the swizzle phase (r & 7) is fixed per thread
+        const int j = tid & 7, r0 = tid >> 3;
+        const uint32_t swz = (uint32_t)(((j ^ r0) & 7) << 4);
         uint32_t g = 0;
         for (long item = blockIdx.x; item < a.items && !fail; item += gridDim.x) {
             for (int kb = 0; kb < nk; kb++, g++) {
                 const int s = (int)(g % kFStages);
                 if (!mbar_wait(&full[s], (g / kFStages) & 1, &fail)) break;
-                uint8_t* st = fstage(sm, s);
-                uint8_t* g0 = st + kFA;
-                const uint8_t* lv1 = st + kFA + kFG;
-                const uint8_t* lv2 = lv1 + kFL(1);
-                const uint8_t* lv3 = lv2 + kFL(2);
                 if (L > 1) {
-#pragma unroll 2
-                    for (int i = tid; i < 1024; i += 128) {
-                        const int j = i & 7;                                    // 16-byte chunk: 8 pixels
-                        const int h = pass == 0 ? 0 : (i >> 9);                 // pass 1: 64-pixel half
-                        const int r = pass == 0 ? (i >> 3) : ((i >> 3) & 63);   // G row in the half
-                        const int hr = h * R + r;                               // row in the level tiles
-                        uint4* cp = reinterpret_cast<uint4*>(g0 + h * 8192 + r * 128 + (((j ^ r) & 7) << 4));
-                        uint4 raw = *cp;
-                        OpT* v = reinterpret_cast<OpT*>(&raw);
-                        float acc[8];
+                    uint8_t* st = fstage(sm, s);
+                    const uint8_t* lv1 = st + kFA + kFG;
+                    const uint8_t* lv2 = lv1 + kFL(1);
+                    const uint8_t* lv3 = lv2 + kFL(2);
 #pragma unroll
-                        for (int e = 0; e < 8; e++) acc[e] = to_f(v[e]);
-                        {
-                            const uint2 c1 = *reinterpret_cast<const uint2*>(lv1 + hr * 64 + 8 * j);
-                            const OpT* w1 = reinterpret_cast<const OpT*>(&c1);
-#pragma unroll
-                            for (int e = 0; e < 8; e++) acc[e] += 0.25f * to_f(w1[e >> 1]);
-                        }
-                        if (L > 2) {
-                            const uint32_t c2 = *reinterpret_cast<const uint32_t*>(lv2 + hr * 32 + 4 * j);
-                            const OpT* w2 = reinterpret_cast<const OpT*>(&c2);
-#pragma unroll
-                            for (int e = 0; e < 8; e++) acc[e] += 0.0625f * to_f(w2[e >> 2]);
-                        }
-                        if (L > 3) {
-                            const float w3 = 0.015625f * to_f(*reinterpret_cast<const OpT*>(lv3 + hr * 16 + 2 * j));
-#pragma unroll
-                            for (int e = 0; e < 8; e++) acc[e] += w3;
-                        }
-#pragma unroll
-                        for (int e = 0; e < 8; e++) v[e] = to_op<OpT>(acc[e]);
-                        *cp = raw;
+                    for (int m = 0; m < 4; m++) {
+                        const int h = kPass == 0 ? 0 : (m >> 1);
+                        const int r = kPass == 0 ? r0 + 32 * m : r0 + 32 * (m & 1);
+                        const int hr = h * R + r;  // row in the level tiles
+                        uint4* cp = reinterpret_cast<uint4*>(st + kFA + h * 8192 + r * 128 + swz);
+                        combine_chunk<OpT>(cp, lv1 + hr * 64 + 8 * j, lv2 + hr * 32 + 4 * j, lv3 + hr * 16 + 2 * j, L);
                     }
                 }
                 fence_proxy_async();
@@ -452,7 +492,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
         }
     } else if (warp == kFMmaWarp && lane == 0) {
         // ------------------------------------------------ MMA issuer
-        const uint32_t idesc = instr_desc(FMT, kTile, kTile) | (pass == 1 ? (1u << 16) : 0u);
+        const uint32_t idesc = instr_desc(FMT, kTile, kTile) | (kPass == 1 ? (1u << 16) : 0u);
         uint32_t g = 0, t = 0;
         for (long item = blockIdx.x; item < a.items && !fail; item += gridDim.x, t++) {
             const int b = (int)(t & 1);
@@ -469,8 +509,8 @@ __global__ void __launch_bounds__(kFThreads, 1)
                 tc_fence_after();
                 uint8_t* st = fstage(sm, s);
                 const uint64_t da = smem_desc_sw128(st);
-                const uint64_t db = pass == 0 ? smem_desc_sw128(st + kFA) : smem_desc_sw128_mn(st + kFA, 8192);
-                const uint64_t bstep = pass == 0 ? 2u : (uint64_t)(2048 >> 4);
+                const uint64_t db = kPass == 0 ? smem_desc_sw128(st + kFA) : smem_desc_sw128_mn(st + kFA, 8192);
+                const uint64_t bstep = kPass == 0 ? 2u : (uint64_t)(2048 >> 4);
 #pragma unroll
                 for (int k = 0; k < 4; k++)
                     mma_f16(d, da + (uint64_t)(2 * k), db + (uint64_t)k * bstep, idesc, (kb | k) ? 1u : 0u);
@@ -484,7 +524,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
             const uint32_t k = g - 1;
             mbar_wait_bounded(&empty[k % kFStages], (k / kFStages) & 1, kTmaWaitNs);
         }
-    } else if (warp >= 4 && warp < 8) {
+    } else if (warp >= kFEpiWarp0 && warp < kFEpiWarp0 + 4) {
         // ------------------------------------------------ epilogue
         const int q = warp & 3;  // tensor-memory lane quarter = channels 32q ..
         const int c = 32 * q + lane;
@@ -501,9 +541,9 @@ __global__ void __launch_bounds__(kFThreads, 1)
                 tmem_wait_ld();
                 if (c < a.C) {
 #pragma unroll
-                    for (int j = 0; j < 16; j += 4)
-                        *reinterpret_cast<float4*>(orow + c0 + j) =
-                            make_float4(v[j] * 0.0625f, v[j + 1] * 0.0625f, v[j + 2] * 0.0625f, v[j + 3] * 0.0625f);
+                    for (int jj = 0; jj < 16; jj += 4)
+                        *reinterpret_cast<float4*>(orow + c0 + jj) = make_float4(
+                            v[jj] * 0.0625f, v[jj + 1] * 0.0625f, v[jj + 2] * 0.0625f, v[jj + 3] * 0.0625f);
                 }
             }
             tc_fence_before();
@@ -592,13 +632,13 @@ static int launch_fast(const Params& p, int pass, const void* fmap, float* out, 
     FastParams fp{};
     fp.out = out;
     fp.err = p.err;
-    fp.C = p.C; fp.W = p.W; fp.HW = p.HW; fp.L = p.L; fp.pass = pass; fp.blocks = p.blocks;
+    fp.C = p.C; fp.W = p.W; fp.HW = p.HW; fp.L = p.L; fp.blocks = p.blocks;
     fp.items = (long)p.num * p.blocks;
     const size_t smem = (size_t)kFStages * kFStage + 1024;
-    VIPE_CUDA_TRY(cudaFuncSetAttribute(corr_vol_bwd_tma_kernel<OpT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
+    auto kern = pass == 0 ? corr_vol_bwd_tma_kernel<OpT, 0> : corr_vol_bwd_tma_kernel<OpT, 1>;
+    VIPE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long grid = std::min<long>(fp.items, (long)g_sms);
-    corr_vol_bwd_tma_kernel<OpT><<<(unsigned)grid, kFThreads, smem, st>>>(mf, mg[0], mg[1], mg[2], mg[3], fp);
+    kern<<<(unsigned)grid, kFThreads, smem, st>>>(mf, mg[0], mg[1], mg[2], mg[3], fp);
     VIPE_LAUNCH_CHECK();
     return VIPE_OK;
 }
