@@ -135,6 +135,22 @@ int vipe_slam_ba_extended_robust(float* poses_io, float* disps_io, float* intrin
                                  const float* mu_schedule, void* workspace, size_t workspace_bytes,
                                  int32_t* dev_status, void* stream);
 
+/* vipe_slam_ba_extended_robust with the frames' camera model (the reference's fused path takes
+ * single-view pinhole buffers only, buffer.py:387-388; its generic solver projects through
+ * vipe/slam/maths/geom.py:187-298 with any CameraType):
+ *   camera_model 0 pinhole, 1 MEI (unified model, vipe/utils/cameras.py:220-330) with
+ *     distortion = k1 in [0, 1]; intrinsics_io holds fx, fy, cx, cy at the flow resolution as
+ *     for pinhole.  MEI refuses optimize_intrinsics (VIPE_ERR_ARG). */
+int vipe_slam_ba_extended_generic(float* poses_io, float* disps_io, float* intrinsics_io, const float* disps_sens,
+                                  const float* targets, const float* weights, const float* eta, const int64_t* ii,
+                                  const int64_t* jj, const float* depth_active, int num_frames, int ht, int wd,
+                                  int num_edges, int num_kx, int t0, int t1, int iterations, float lm, float ep,
+                                  int motion_only, float alpha, int optimize_intrinsics, float intrinsics_lm,
+                                  float intrinsics_ep, float intrinsics_scale, int compute_energy, float* dx_out,
+                                  float* dz_out, float* energy_out, int robust_kind, float robust_threshold,
+                                  const float* mu_schedule, int camera_model, float distortion, void* workspace,
+                                  size_t workspace_bytes, int32_t* dev_status, void* stream);
+
 /* Replaces slam_ext.ba (reference: csrc/slam_ext/slam.cpp:42-45,
  * geom_kernels.cu:1826-1834): ba_extended with depth_active = 1, no focal
  * optimisation and no energy.  depth_active_scratch: device f32 buffer of

@@ -35,6 +35,8 @@ def lib():
         _lib.oracle_set_threads.restype = None
         _lib.oracle_set_threads.argtypes = [I]
         _lib.oracle_set_threads(1)
+        _lib.oracle_set_camera.restype = None
+        _lib.oracle_set_camera.argtypes = [I, ctypes.c_double]
         _lib.oracle_set_robust.restype = None
         _lib.oracle_set_robust.argtypes = [I, ctypes.c_double, D, I]
         _lib.oracle_accum_csr.restype = I
@@ -58,14 +60,16 @@ def _p(a, t):
 
 def ba(p, *, fp64: bool, motion_only=False, optimize_intrinsics=False, intrinsics_lm=1e-6, intrinsics_ep=1e-6,
        intrinsics_scale=1.0, compute_energy=False, iterations=None, lm=None, ep=None, alpha=None,
-       backsub_all_rows=False, robust_kind=0, robust_threshold=1.0, mu_schedule=None):
+       backsub_all_rows=False, robust_kind=0, robust_threshold=1.0, mu_schedule=None, camera_model=0,
+       distortion=0.0):
     """Runs the oracle on a workloads.BAProblem-like object (CPU tensors or arrays).
 
     backsub_all_rows=True keeps the depth back-substitution rows of pose t0, which the
     reference's fused kernel skips (geom_kernels.cu:1186) and its generic solver keeps.
     robust_kind 1/2/3 (Huber, Tukey, GNC-TLS with mu_schedule[i] for iteration i) multiplies
     each flow channel's weight by the generic solver's kernel of its residual
-    (vipe/slam/ba/kernel.py:40-153, terms.py:73-75).
+    (vipe/slam/ba/kernel.py:40-153, terms.py:73-75).  camera_model 1 projects through the MEI
+    camera with k1 = distortion (vipe/utils/cameras.py:220-330).
     Returns dict(poses, disps, intrinsics, dx, dz, energy) as float64 arrays.
     """
     poses = _d(np.asarray(p.poses, dtype=np.float64)).copy()
@@ -91,6 +95,7 @@ def ba(p, *, fp64: bool, motion_only=False, optimize_intrinsics=False, intrinsic
     lib().oracle_set_backsub_all_rows(int(bool(backsub_all_rows)))
     mu = np.ascontiguousarray(np.asarray([] if mu_schedule is None else mu_schedule, dtype=np.float64))
     lib().oracle_set_robust(int(robust_kind), float(robust_threshold), _p(mu, D) if mu.size else None, int(mu.size))
+    lib().oracle_set_camera(int(camera_model), float(distortion))
     rc = lib().oracle_ba(
         1 if fp64 else 0, _p(poses, D), _p(disps, D), _p(intr, D), _p(sens, D), _p(tg, D), _p(wt, D), _p(eta, D),
         _p(ii, L), _p(jj, L), _p(act, D), N, H, W, E, K, p.t0, p.t1, iters,
@@ -100,6 +105,7 @@ def ba(p, *, fp64: bool, motion_only=False, optimize_intrinsics=False, intrinsic
     )
     lib().oracle_set_backsub_all_rows(0)
     lib().oracle_set_robust(0, 1.0, None, 0)
+    lib().oracle_set_camera(0, 0.0)
     if rc != 0:
         raise RuntimeError(f"oracle_ba failed with code {rc}")
     return dict(poses=poses, disps=disps, intrinsics=intr, dx=dx, dz=None if motion_only else dz,

@@ -47,6 +47,22 @@ int g_rb_kind = 0;
 double g_rb_c = 1.0;
 std::vector<double> g_rb_mu;
 
+// Camera model of the frames (oracle_set_camera): 0 pinhole, 1 MEI with distortion g_k1
+// (vipe/utils/cameras.py:220-330).
+int g_cam = 0;
+double g_k1 = 0.0;
+
+// MEI unprojection of the normalised pinhole coordinates in X[0], X[1] (in place):
+// r2 = u^2 + v^2, q = sqrt(1 + (1 - k1^2) r2), s = (k1 + q) / (1 + r2), X = u s / (s - k1)
+template <typename S>
+void mei_unproject(S k1, S* X) {
+    const S u = X[0], v = X[1], r2 = u * u + v * v;
+    const S q = std::sqrt(S(1) + (S(1) - k1 * k1) * r2);
+    const S f = (k1 + q) / (S(1) + r2);
+    X[0] = u * f / (f - k1);
+    X[1] = v * f / (f - k1);
+}
+
 template <typename S>
 S robust_weight(int kind, S c, S mu, S r) {
     if (kind == 1) {  // Huber
@@ -322,12 +338,27 @@ int run_ba(double* poses_io, double* disps_io, double* intr_io, const double* di
             for (int p = 0; p < HW; p++) {
                 const int r = p / W, c = p % W;
                 S Xi[4] = {(S(c) - cx) / fx, (S(r) - cy) / fy, S(1), disps[(size_t)a * HW + p]};
+                if (g_cam == 1) mei_unproject(S(g_k1), Xi);
                 S Xj[4];
                 act_h(tij, qij, Xi, Xj);
                 const S x = Xj[0], y = Xj[1], h = Xj[3];
                 const bool ok = !(Xj[2] < S(kMinDepth));
                 const S d = ok ? S(1) / Xj[2] : S(0);
                 const S d2 = d * d;
+                // MEI: projection (pu, pv) and its gradients gm[c] in Xj (rows of the camera's Jp)
+                S pu = fx * d * x + cx, pv = fy * d * y + cy, gm[2][3] = {{0, 0, 0}, {0, 0, 0}};
+                if (g_cam == 1) {
+                    const S k1 = S(g_k1), rn = std::sqrt(x * x + y * y + Xj[2] * Xj[2]), rb = Xj[2] + k1 * rn;
+                    const S dm = ok ? S(1) / rb : S(0), iden = ok ? S(1) / (rb * rb * rn) : S(0);
+                    pu = fx * x * dm + cx;
+                    pv = fy * y * dm + cy;
+                    gm[0][0] = fx * (rb * rn - k1 * x * x) * iden;
+                    gm[0][1] = -fx * k1 * x * y * iden;
+                    gm[0][2] = -fx * x * (k1 * Xj[2] + rn) * iden;
+                    gm[1][0] = -fy * k1 * x * y * iden;
+                    gm[1][1] = fy * (rb * rn - k1 * y * y) * iden;
+                    gm[1][2] = -fy * y * (k1 * Xj[2] + rn) * iden;
+                }
                 S wu = ok ? S(0.001) * S(weights[(((size_t)e * 2 + 0) * HW) + p]) : S(0);
                 S wv = ok ? S(0.001) * S(weights[(((size_t)e * 2 + 1) * HW) + p]) : S(0);
                 S Jfu = 0, Jfv = 0;
@@ -338,8 +369,8 @@ int run_ba(double* poses_io, double* disps_io, double* intr_io, const double* di
                     Jfu = S(intr_scale) * (fx * d * dXj[0] - fx * x * d2 * dXj[2] + x * d);
                     Jfv = S(intr_scale) * (fy * d * dXj[1] - fy * y * d2 * dXj[2] + y * d);
                 }
-                const S ru = S(targets[(((size_t)e * 2 + 0) * HW) + p]) - (fx * d * x + cx);
-                const S rv = S(targets[(((size_t)e * 2 + 1) * HW) + p]) - (fy * d * y + cy);
+                const S ru = S(targets[(((size_t)e * 2 + 0) * HW) + p]) - pu;
+                const S rv = S(targets[(((size_t)e * 2 + 1) * HW) + p]) - pv;
                 if (g_rb_kind != 0) {
                     const S mu = S(g_rb_mu.empty() ? 1.0 : g_rb_mu[std::min<size_t>(itr, g_rb_mu.size() - 1)]);
                     wu *= robust_weight(g_rb_kind, S(g_rb_c), mu, ru);
@@ -361,6 +392,14 @@ int run_ba(double* poses_io, double* disps_io, double* intr_io, const double* di
                         Jj[3] = fy * (-1 - y * y * d2); Jj[4] = fy * (x * y * d2); Jj[5] = fy * (x * d);
                         Jz = fy * (tij[1] * d - tij[2] * (y * d2));
                         w = wv; res = rv; Jf = Jfv;
+                    }
+                    if (g_cam == 1) {  // any central camera: (h g, P x g) and g . t from its gradient g
+                        const S* gc = gm[ch];
+                        Jj[0] = h * gc[0]; Jj[1] = h * gc[1]; Jj[2] = h * gc[2];
+                        Jj[3] = y * gc[2] - Xj[2] * gc[1];
+                        Jj[4] = Xj[2] * gc[0] - x * gc[2];
+                        Jj[5] = x * gc[1] - y * gc[0];
+                        Jz = gc[0] * tij[0] + gc[1] * tij[1] + gc[2] * tij[2];
                     }
                     const S wd = w * act;
                     const size_t q = (size_t)e * HW + p;
@@ -688,6 +727,11 @@ int oracle_accum_csr(const int64_t* ii, const int64_t* jj, int E, int t0, int t1
 // back-substitution, vipe/slam/ba/solver.py:183-186, has no such skip); the
 // default 0 is the fused kernel's behaviour.
 void oracle_set_backsub_all_rows(int all_rows) { g_backsub_all_rows = all_rows ? 1 : 0; }
+
+void oracle_set_camera(int camera_model, double k1) {
+    g_cam = camera_model;
+    g_k1 = k1;
+}
 
 // kind 0 none, 1 Huber, 2 Tukey, 3 GNC-TLS; mu[i] is the GNC mu of iteration i (n entries)
 void oracle_set_robust(int kind, double c, const double* mu, int n) {

@@ -119,3 +119,32 @@ def assert_robust_matches_generic(name, poses, disps):
     torch.testing.assert_close(poses[:n].cpu().float(), g["poses"][:n], atol=2e-4, rtol=0)
     torch.testing.assert_close(disps[:n].cpu().float().clamp(min=0.001), g["disps"][:n], atol=3e-3, rtol=0)
     assert float((disps[:n].cpu().float().clamp(min=0.001) - g["disps"][:n]).abs().mean()) < 2e-4
+
+
+def camera_cases():
+    return torch.load(GOLDEN, weights_only=False)["camera"]
+
+
+def camera_setup(name):
+    """(case, args, kernel, threshold, k1) of an MEI-camera case: config 0's recorded arguments
+    (outlier targets for the robust one) with the case's iteration count."""
+    c = camera_cases()[name]
+    case = cases()["config0"]
+    args = args_of(case)
+    if c["outliers"]:
+        args[4] = with_outliers(args[4])
+    args[12] = c["iterations"]
+    return case, args, c["kernel"], c["threshold"], c["k1"]
+
+
+def assert_camera_matches_generic(name, poses, disps):
+    """Poses within 2e-4, disparities within 5e-3 (mean 2e-4) of the generic solver with the
+    MEI camera; the FP64 oracle itself sits 2.5e-3 / 4.0e-3 (max) from it, the generic solver's
+    FP32 rounding (means 1.4e-4 / 1.0e-4)."""
+    c = camera_cases()[name]
+    n = c["n_frames"]
+    g = c["generic"]
+    torch.testing.assert_close(poses[:n].cpu().float(), g["poses"][:n], atol=2e-4, rtol=0)
+    d = disps[:n].cpu().float().clamp(min=0.001)
+    torch.testing.assert_close(d, g["disps"][:n], atol=5e-3, rtol=0)
+    assert float((d - g["disps"][:n]).abs().mean()) < 2e-4

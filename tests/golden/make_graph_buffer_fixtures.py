@@ -29,7 +29,9 @@ solver's result at the reference test's tolerance.
 
 Robust kernels: config 0 with deterministic outlier flow is solved by the generic solver with
 Huber, Tukey and GNC-TLS (the reference's fused path refuses robust kernels); the results go
-to the "robust" entry and are held to vipe_slam_ba_extended_robust on the GPU.
+to the "robust" entry and are held to vipe_slam_ba_extended_robust on the GPU.  The same
+config 0 through the generic solver with the MEI camera (plain, and with Huber on the outlier
+targets) goes to the "camera" entry (the fused path refuses non-pinhole buffers).
 
 The same is done for a third case built from config 0 (8 keyframes, 48x64 disparity,
 26 edges, 2 iterations): GraphBuffer(384x512) is loaded with the config-0
@@ -273,6 +275,58 @@ ROBUST = {
 }
 
 
+CAMERA = {
+    # name: (camera, k1, robust_kernel, threshold, n_iters)
+    "mei": ("mei", 0.25, None, 1.0, 2),
+    "mei_huber": ("mei", 0.6, "huber", 2.0, 3),
+}
+
+
+def camera_cases():
+    """Config 0 through the reference's generic solver with the MEI camera (GraphBuffer with
+    camera_type MEI: fx, fy, cx, cy of config 0 at full resolution and k1), plain and with
+    Huber on the outlier targets.  The fused path refuses non-pinhole buffers
+    (buffer.py:387-388)."""
+    from vipe.slam.components.buffer import GraphBuffer
+    from vipe.slam.components.sparse_tracks import DummySparseTracks
+    from vipe.utils.cameras import CameraType
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    from _graph_buffer_golden import with_outliers
+
+    from vipe_b200 import workloads as W
+
+    p = W.ba_config0()
+    N, ht, wd = p.disps.shape
+    E = p.ii.shape[0]
+    weight = p.weights.permute(0, 2, 3, 1).reshape(E, ht * wd, 2).contiguous()
+    disp_damping = ((p.eta.double() - 1e-7) / 0.2).float()
+    out = {}
+    for name, (cam, k1, kernel, thr, n_iters) in CAMERA.items():
+        targets = with_outliers(p.targets) if kernel else p.targets
+        target = targets.permute(0, 2, 3, 1).reshape(E, ht * wd, 2).contiguous()
+        cfg = _Cfg({"dense_disp_alpha": float(p.alpha), "fused": False, "intrinsics_damping_scale": 1.0,
+                    "robust_kernel": kernel, "robust_kernel_threshold": thr, "gnc_mu_init": 1.0,
+                    "gnc_mu_step": 3.0, "gnc_mu_max": 1.0e6, "gnc_n_mu_steps": 4, "gnc_gn_iters_per_mu": 6})
+        v = GraphBuffer(height=8 * ht, width=8 * wd, n_views=1, buffer_size=N, init_disp=1.0, cross_view_idx=None,
+                        ba_config=cfg, sparse_tracks=DummySparseTracks(n_views=1), camera_type=CameraType.MEI,
+                        device=torch.device("cpu"))
+        v.n_frames = N
+        v.tstamp[:N] = torch.arange(N)
+        v.intrinsics[0, :4] = p.intrinsics * 8
+        v.intrinsics[0, 4] = k1
+        v.poses[:N] = p.poses
+        v.disps[:N, 0] = p.disps
+        v.disps_sens[:N, 0] = p.disps_sens
+        v.bundle_adjustment(target=target.clone(), weight=weight.clone(), disp_damping=disp_damping.clone(),
+                            ii=p.ii.clone(), jj=p.jj.clone(), t0=p.t0, t1=p.t1, n_iters=n_iters,
+                            pose_damping=float(p.lm), pose_ep=float(p.ep), motion_only=False, limited_disp=False,
+                            optimize_intrinsics=False, optimize_rig_rotation=False, verbose=False)
+        out[name] = {"camera": cam, "k1": k1, "kernel": kernel, "threshold": thr, "iterations": n_iters,
+                     "outliers": bool(kernel), "generic": state_of(v), "n_frames": N}
+    return out
+
+
 def robust_cases():
     """Config 0 with deterministic outlier flow (tests/_graph_buffer_golden.with_outliers) solved
     by the reference's generic solver with each robust kernel (buffer.py:531-695; the fused path
@@ -331,10 +385,12 @@ def main(ref: Path):
         "config0": config0_case(rec),
     }
     robust = robust_cases()
-    torch.save({"cases": cases, "robust": robust, "torch": torch.__version__}, OUT)
+    camera = camera_cases()
+    torch.save({"cases": cases, "robust": robust, "camera": camera, "torch": torch.__version__}, OUT)
     print(f"wrote {OUT} ({OUT.stat().st_size} bytes)")
     before = cases["config0"]["before"]["poses"]
-    for k, c in {**cases, **{"robust_" + k: v for k, v in robust.items()}}.items():
+    for k, c in {**cases, **{"robust_" + k: v for k, v in robust.items()},
+                 **{"camera_" + k: v for k, v in camera.items()}}.items():
         d = (c["generic"]["poses"] - c.get("before", {"poses": before})["poses"]).abs().max()
         print(f"  {k}: generic solver moved poses by {float(d):.3e}")
 

@@ -43,3 +43,8 @@ def test_threshold_must_be_positive():
 def test_cpu_tensors_are_refused():
     with pytest.raises(RuntimeError):
         R.ba_extended_robust(*_dummy(), robust_kernel="huber", threshold=1.0)
+
+
+def test_unknown_camera_raises():
+    with pytest.raises(ValueError, match="camera_type"):
+        R.ba_extended_robust(*_dummy(), camera_type="panorama")

@@ -76,3 +76,38 @@ def test_gnc_weights_follow_the_schedule():
     n = case["n_frames"]
     assert float((p1 - p2).abs().max()) > 1e-5
     torch.testing.assert_close(p2[:n].cpu().double(), torch.from_numpy(want["poses"]), atol=5e-5, rtol=0)
+
+
+@pytest.mark.parametrize("name", ["mei", "mei_huber"])
+def test_mei_camera_matches_reference_generic_solver(name):
+    """The MEI camera in the fused kernels (per-pixel unprojection, projection and its
+    gradient in every linearisation) against the reference's generic solver on a MEI
+    GraphBuffer, and against the FP32 oracle with the same camera."""
+    from vipe_b200.robust_ba import ba_extended_robust
+
+    case, args, kernel, thr, k1 = G.camera_setup(name)
+    call = [a.to("cuda").clone() if isinstance(a, torch.Tensor) else a for a in args]
+    ba_extended_robust(*call[:21], robust_kernel=kernel, threshold=thr, camera_type="mei", distortion=k1)
+    torch.cuda.synchronize()
+    poses, disps = call[0], call[1]
+    G.assert_camera_matches_generic(name, poses, disps[:, None])
+    p = types.SimpleNamespace(poses=args[0].double().numpy(), disps=args[1].double().numpy(),
+                              intrinsics=args[2].double().numpy(), disps_sens=args[3], targets=args[4],
+                              weights=args[5], eta=args[6], ii=args[7], jj=args[8], depth_active=args[9],
+                              t0=args[10], t1=args[11], iterations=args[12], lm=args[13], ep=args[14], alpha=args[16])
+    want = ob.ba(p, fp64=False, backsub_all_rows=True, robust_kind=1 if kernel else 0, robust_threshold=thr,
+                 camera_model=1, distortion=k1)
+    n = case["n_frames"]
+    torch.testing.assert_close(poses[:n].cpu().double(), torch.from_numpy(want["poses"]), atol=5e-5, rtol=0)
+    torch.testing.assert_close(disps[:n].cpu().double().clamp(min=0.001),
+                               torch.from_numpy(want["disps"]).clamp(min=0.001), atol=5e-4, rtol=0)
+
+
+def test_mei_refuses_focal_optimisation():
+    from vipe_b200.robust_ba import ba_extended_robust
+
+    case, args, kernel, thr, k1 = G.camera_setup("mei")
+    call = [a.to("cuda").clone() if isinstance(a, torch.Tensor) else a for a in args]
+    call[17] = True  # optimize_intrinsics
+    with pytest.raises(RuntimeError, match="MEI"):
+        ba_extended_robust(*call[:21], camera_type="mei", distortion=k1)

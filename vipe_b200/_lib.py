@@ -42,6 +42,11 @@ _SIGS: dict[str, tuple] = {
         [P, P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, F, I, F, I, F, F, F, I, P, P, P, I, F, P, P, SZ,
          P, P],
     ),
+    "vipe_slam_ba_extended_generic": (
+        I,
+        [P, P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, F, I, F, I, F, F, F, I, P, P, P, I, F, P, I, F, P,
+         SZ, P, P],
+    ),
     "vipe_slam_ba_extended_noalloc": (
         I,
         [P, P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, F, I, F, I, F, F, F, I, P, P, P, P, P],

@@ -511,9 +511,11 @@ __device__ __forceinline__ void linearize_d(const EdgeTf& T, bool stereo, float 
 
 // ---------------------------------------------------------------- per-edge terms
 
-template <bool kIntr, int D>
+template <bool kIntr, int D, bool kExt = false>
 // 4 CTAs per SM for the SE3 form (64 registers; 10.4 vs 11.7 ms per 256-clip step at the
-// 80 registers the compiler picks unbounded); the focal and Sim3 forms are left unbounded
+// 80 registers the compiler picks unbounded); the focal and Sim3 forms are left unbounded.
+// kExt: robust reweighting / camera model from io.rb compiled in (single solves that ask for
+// them); without it the plain pinhole linearisation carries none of that code.
 __global__ void __launch_bounds__(kEdgeThreads, (D == 6 && !kIntr) ? 4 : 1) ba_edge_kernel(BAPtrs base, Batch B,
                                                                                           float iscale) {
     BA_BIND(B, base);
@@ -547,7 +549,8 @@ __global__ void __launch_bounds__(kEdgeThreads, (D == 6 && !kIntr) ? 4 : 1) ba_e
         const float u = (float)(p % W), v = (float)(p / W);
         typename LinOf<D>::T L;
         linearize_d<D, kIntr, true>(Tf, stereo, fx, fy, cx, cy, u, v, __ldg(dp + p), __ldg(wu + p),
-                                    __ldg(wu + HW + p), __ldg(tu + p), __ldg(tu + HW + p), 1.0f, A.iscale, L, io.rb);
+                                    __ldg(wu + HW + p), __ldg(tu + p), __ldg(tu + HW + p), 1.0f, A.iscale, L,
+                                    kExt ? io.rb : RobustSpec{});
         en += L.we[0] * L.r[0] * L.r[0] + L.we[1] * L.r[1] * L.r[1];
 #pragma unroll
         for (int ch = 0; ch < 2; ch++) {
@@ -2047,9 +2050,10 @@ __global__ void __launch_bounds__(kCholThreads) ba_chol_resolve_kernel(BAPtrs ba
 
 // ---------------------------------------------------------------- back substitution
 
-template <bool kIntr, int D>
+template <bool kIntr, int D, bool kExt = false>
 // 8 CTAs per SM for the SE3 form (32 registers: latency-bound, more warps in flight beat the
-// spills; 5.5 vs 8.5 ms per 256-clip step at 3 CTAs); the focal and Sim3 forms keep 3
+// spills; 5.5 vs 8.5 ms per 256-clip step at 3 CTAs); the focal and Sim3 forms keep 3.
+// kExt as for ba_edge_kernel.
 __global__ void __launch_bounds__(256, (D == 6 && !kIntr) ? 8 : 3) ba_backsub_kernel(BAPtrs base, Batch B) {
     BA_BIND(B, base);
     if (w.status[0]) return;
@@ -2131,10 +2135,10 @@ __global__ void __launch_bounds__(256, (D == 6 && !kIntr) ? 8 : 3) ba_backsub_ke
             typename LinOf<D>::T L;
             // robust reweighting needs the residual, hence the targets
             const float* tp = A.targets + (size_t)e * 2 * HW;
-            const bool rob = io.rb.kind != 0;
+            const RobustSpec rb = kExt ? io.rb : RobustSpec{};
+            const bool rob = rb.kind != 0;
             linearize_d<D, false, false>(Tf, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p), __ldg(wp + HW + p),
-                                         rob ? __ldg(tp + p) : 0.f, rob ? __ldg(tp + HW + p) : 0.f, act, 1.f, L,
-                                         io.rb);
+                                         rob ? __ldg(tp + p) : 0.f, rob ? __ldg(tp + HW + p) : 0.f, act, 1.f, L, rb);
 #pragma unroll
             for (int ch = 0; ch < 2; ch++) {
                 const float g = L.wd[ch] * L.Jz[ch];
@@ -2270,12 +2274,19 @@ int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const 
     const Batch per_graph{d_table, nullptr, G};
     auto grid = [&](int k) { return (unsigned)geo.off[k][G]; };
     const bool intr = a.intr != 0;
+    const bool ext = base.rb.kind != 0 || base.rb.cam != 0;
     const int with_frames = a.motion_only ? 0 : 1;
     if (geo.any_edges) {
         {
             VIPE_PROF("ba_edge", st);
             if (geo.dof == 7)
                 ba_edge_kernel<false, 7><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(
+                    base, batch_of(geo, d_table, d_off, kOffEdge), a.iscale);
+            else if (ext && intr)
+                ba_edge_kernel<true, 6, true><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(
+                    base, batch_of(geo, d_table, d_off, kOffEdge), a.iscale);
+            else if (ext)
+                ba_edge_kernel<false, 6, true><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(
                     base, batch_of(geo, d_table, d_off, kOffEdge), a.iscale);
             else if (intr)
                 ba_edge_kernel<true, 6><<<grid(kOffEdge), kEdgeThreads, 0, st>>>(
@@ -2397,8 +2408,15 @@ static int launch_update(const Geometry& geo, const GraphDesc* d_table, const in
     const bool intr = a.intr != 0;
     if (!a.motion_only && grid(kOffFrame) > 0) {
         VIPE_PROF("ba_backsub", st);
+        const bool ext = base.rb.kind != 0 || base.rb.cam != 0;
         if (geo.dof == 7)
             ba_backsub_kernel<false, 7><<<grid(kOffFrame), 256, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffFrame));
+        else if (ext && intr)
+            ba_backsub_kernel<true, 6, true><<<grid(kOffFrame), 256, 0, st>>>(base,
+                                                                             batch_of(geo, d_table, d_off, kOffFrame));
+        else if (ext)
+            ba_backsub_kernel<false, 6, true><<<grid(kOffFrame), 256, 0, st>>>(base,
+                                                                              batch_of(geo, d_table, d_off, kOffFrame));
         else if (intr)
             ba_backsub_kernel<true, 6><<<grid(kOffFrame), 256, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffFrame));
         else
@@ -2557,16 +2575,29 @@ extern "C" int vipe_slam_ba_extended(float* poses_io, float* disps_io, float* in
                             workspace_bytes, dev_status, stream);
 }
 
-extern "C" int vipe_slam_ba_extended_robust(float* poses_io, float* disps_io, float* intrinsics_io,
-                                            const float* disps_sens, const float* targets, const float* weights,
-                                            const float* eta, const int64_t* ii, const int64_t* jj,
-                                            const float* depth_active, int num_frames, int ht, int wd, int num_edges,
-                                            int num_kx, int t0, int t1, int iterations, float lm, float ep,
-                                            int motion_only, float alpha, int optimize_intrinsics, float intrinsics_lm,
-                                            float intrinsics_ep, float intrinsics_scale, int compute_energy,
-                                            float* dx_out, float* dz_out, float* energy_out, int robust_kind,
-                                            float robust_threshold, const float* mu_schedule, void* workspace,
-                                            size_t workspace_bytes, int32_t* dev_status, void* stream) {
+extern "C" int vipe_slam_ba_extended_generic(float* poses_io, float* disps_io, float* intrinsics_io,
+                                             const float* disps_sens, const float* targets, const float* weights,
+                                             const float* eta, const int64_t* ii, const int64_t* jj,
+                                             const float* depth_active, int num_frames, int ht, int wd, int num_edges,
+                                             int num_kx, int t0, int t1, int iterations, float lm, float ep,
+                                             int motion_only, float alpha, int optimize_intrinsics,
+                                             float intrinsics_lm, float intrinsics_ep, float intrinsics_scale,
+                                             int compute_energy, float* dx_out, float* dz_out, float* energy_out,
+                                             int robust_kind, float robust_threshold, const float* mu_schedule,
+                                             int camera_model, float distortion, void* workspace,
+                                             size_t workspace_bytes, int32_t* dev_status, void* stream) {
+    if (camera_model != 0 && camera_model != 1) {
+        set_last_error("generic BA: camera_model must be 0 (pinhole) or 1 (MEI)");
+        return VIPE_ERR_ARG;
+    }
+    if (camera_model == 1 && optimize_intrinsics) {
+        set_last_error("generic BA: optimize_intrinsics is not supported with the MEI camera");
+        return VIPE_ERR_ARG;
+    }
+    if (camera_model == 1 && !(distortion >= 0.f && distortion <= 1.f)) {
+        set_last_error("generic BA: the MEI distortion k1 must lie in [0, 1]");
+        return VIPE_ERR_ARG;
+    }
     if (robust_kind < 0 || robust_kind > 3) {
         set_last_error("robust BA: robust_kind must be 0 (none), 1 (Huber), 2 (Tukey) or 3 (GNC-TLS)");
         return VIPE_ERR_ARG;
@@ -2583,12 +2614,32 @@ extern "C" int vipe_slam_ba_extended_robust(float* poses_io, float* disps_io, fl
     rb.kind = robust_kind;
     rb.c = robust_threshold > 0.f ? robust_threshold : 1.f;
     rb.mu = 1.f;
+    rb.cam = camera_model;
+    rb.k1 = camera_model == 1 ? distortion : 0.f;
     return ba_extended_impl(poses_io, disps_io, intrinsics_io, disps_sens, targets, weights, eta, ii, jj,
                             depth_active, num_frames, ht, wd, num_edges, num_kx, t0, t1, iterations, lm, ep,
                             motion_only, alpha, optimize_intrinsics, intrinsics_lm, intrinsics_ep, intrinsics_scale,
                             compute_energy, dx_out, dz_out, energy_out, rb, 1,
                             robust_kind == 3 ? mu_schedule : nullptr, workspace, workspace_bytes, dev_status,
                             stream);
+}
+
+extern "C" int vipe_slam_ba_extended_robust(float* poses_io, float* disps_io, float* intrinsics_io,
+                                            const float* disps_sens, const float* targets, const float* weights,
+                                            const float* eta, const int64_t* ii, const int64_t* jj,
+                                            const float* depth_active, int num_frames, int ht, int wd, int num_edges,
+                                            int num_kx, int t0, int t1, int iterations, float lm, float ep,
+                                            int motion_only, float alpha, int optimize_intrinsics, float intrinsics_lm,
+                                            float intrinsics_ep, float intrinsics_scale, int compute_energy,
+                                            float* dx_out, float* dz_out, float* energy_out, int robust_kind,
+                                            float robust_threshold, const float* mu_schedule, void* workspace,
+                                            size_t workspace_bytes, int32_t* dev_status, void* stream) {
+    return vipe_slam_ba_extended_generic(poses_io, disps_io, intrinsics_io, disps_sens, targets, weights, eta, ii, jj,
+                                         depth_active, num_frames, ht, wd, num_edges, num_kx, t0, t1, iterations, lm,
+                                         ep, motion_only, alpha, optimize_intrinsics, intrinsics_lm, intrinsics_ep,
+                                         intrinsics_scale, compute_energy, dx_out, dz_out, energy_out, robust_kind,
+                                         robust_threshold, mu_schedule, 0, 0.f, workspace, workspace_bytes,
+                                         dev_status, stream);
 }
 
 // ---------------------------------------------------------------- batched solve

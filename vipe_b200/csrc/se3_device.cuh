@@ -147,10 +147,14 @@ struct PixelLin {
 //   kind 3 GNC-TLS  at scalar mu: 1 below mu/(mu+1) c^2, 0 above (mu+1)/mu c^2, between
 //                   max(sqrt(c^2 mu (mu+1) / r^2) - mu, 0); mu = +inf: the hard TLS 1{r^2 < c^2}
 // kind 0: no reweighting.
+// Also carried here: the camera model of the frames (cam 0 pinhole; cam 1 the unified
+// (MEI) model of vipe/utils/cameras.py:220-330 with distortion k1, fx fy cx cy as for pinhole).
 struct RobustSpec {
     int kind = 0;
     float c = 1.0f;
     float mu = 1.0f;
+    int cam = 0;
+    float k1 = 0.0f;
 };
 
 __device__ __forceinline__ float robust_weight(const RobustSpec& rb, float r) {
@@ -172,11 +176,83 @@ __device__ __forceinline__ float robust_weight(const RobustSpec& rb, float r) {
     return 1.0f;
 }
 
+// The unified (MEI) camera, as the reference's MeiCameraModel (vipe/utils/cameras.py:220-330):
+// unprojection of pixel (u, v) to (X, Y, 1) with u_b = (u - cx) / fx, v_b = (v - cy) / fy,
+// r2 = u_b^2 + v_b^2, q = sqrt(1 + (1 - k1^2) r2), s = (k1 + q) / (1 + r2):
+// X = u_b s / (s - k1), Y = v_b s / (s - k1); projection of P: x = fx P0 / (P2 + k1 |P|) + cx,
+// y = fy P1 / (P2 + k1 |P|) + cy, with the projection gradient g_c (row c of its Jacobian in P).
+// The pose and depth rows follow from g_c as for any central camera: target pose
+// (h g_c, P x g_c), source pose -Ad(Tij)^T of it, inverse depth g_c . t.  The focal
+// derivative is not formed (the solver refuses optimize_intrinsics with this camera).
+template <bool kResidual>
+__device__ __forceinline__ void linearize_mei(const float* tij, const float* qij, bool stereo, float fx, float fy,
+                                              float cx, float cy, float u, float v, float disp, float wu_in,
+                                              float wv_in, float tu, float tv, float act, PixelLin& L,
+                                              const RobustSpec& rb) {
+    const float k1 = rb.k1;
+    const float ub = (u - cx) / fx, vb = (v - cy) / fy;
+    const float r2 = ub * ub + vb * vb;
+    const float qq = sqrtf(1.0f + (1.0f - k1 * k1) * r2);
+    const float fac = (k1 + qq) / (1.0f + r2);
+    const float Xi[4] = {ub * fac / (fac - k1), vb * fac / (fac - k1), 1.0f, disp};
+    float Xj[4];
+    act_h(tij, qij, Xi, Xj);
+    const float P0 = Xj[0], P1 = Xj[1], P2 = Xj[2], h = Xj[3];
+    const bool ok = !(P2 < 0.25f);
+    const float rn = sqrtf(P0 * P0 + P1 * P1 + P2 * P2);
+    const float rb_ = P2 + k1 * rn;
+    const float dm = ok ? 1.0f / rb_ : 0.0f;
+    const float iden = ok ? 1.0f / (rb_ * rb_ * rn) : 0.0f;
+    // projection gradients g[c] = d(x_c)/dP
+    float g[2][3];
+    g[0][0] = fx * (rb_ * rn - k1 * P0 * P0) * iden;
+    g[0][1] = -fx * k1 * P0 * P1 * iden;
+    g[0][2] = -fx * P0 * (k1 * P2 + rn) * iden;
+    g[1][0] = -fy * k1 * P0 * P1 * iden;
+    g[1][1] = fy * (rb_ * rn - k1 * P1 * P1) * iden;
+    g[1][2] = -fy * P1 * (k1 * P2 + rn) * iden;
+    const float xu = fx * P0 * dm + cx, xv = fy * P1 * dm + cy;
+    float wu = ok ? 0.001f * wu_in : 0.0f;
+    float wv = ok ? 0.001f * wv_in : 0.0f;
+    if (rb.kind != 0) {
+        wu *= robust_weight(rb, tu - xu);
+        wv *= robust_weight(rb, tv - xv);
+    }
+    L.Jf[0] = 0.0f;
+    L.Jf[1] = 0.0f;
+    L.r[0] = kResidual ? tu - xu : 0.0f;
+    L.r[1] = kResidual ? tv - xv : 0.0f;
+#pragma unroll
+    for (int ch = 0; ch < 2; ch++) {
+        const float* gc = g[ch];
+        L.Jj[ch][0] = h * gc[0];
+        L.Jj[ch][1] = h * gc[1];
+        L.Jj[ch][2] = h * gc[2];
+        L.Jj[ch][3] = P1 * gc[2] - P2 * gc[1];
+        L.Jj[ch][4] = P2 * gc[0] - P0 * gc[2];
+        L.Jj[ch][5] = P0 * gc[1] - P1 * gc[0];
+        L.Jz[ch] = gc[0] * tij[0] + gc[1] * tij[1] + gc[2] * tij[2];
+        adj_t(tij, qij, L.Jj[ch], L.Ji[ch]);
+#pragma unroll
+        for (int n = 0; n < 6; n++) L.Ji[ch][n] = -L.Ji[ch][n];
+    }
+    L.we[0] = wu;
+    L.we[1] = wv;
+    L.wd[0] = wu * act;
+    L.wd[1] = wv * act;
+    L.w[0] = stereo ? 0.0f : wu;
+    L.w[1] = stereo ? 0.0f : wv;
+}
+
 template <bool kIntr, bool kResidual>
 __device__ __forceinline__ void linearize(const float* tij, const float* qij, bool stereo, float fx, float fy,
                                           float cx, float cy, float u, float v, float disp, float wu_in, float wv_in,
                                           float tu, float tv, float act, float iscale, PixelLin& L,
                                           const RobustSpec rb = RobustSpec{}) {
+    if (rb.cam == 1) {
+        linearize_mei<kResidual>(tij, qij, stereo, fx, fy, cx, cy, u, v, disp, wu_in, wv_in, tu, tv, act, L, rb);
+        return;
+    }
     float Xi[4] = {(u - cx) / fx, (v - cy) / fy, 1.0f, disp};
     float Xj[4];
     act_h(tij, qij, Xi, Xj);

@@ -10,7 +10,9 @@ channel's residual at the linearisation point — exactly where the generic solv
 pose t0 as the generic solver's Schur back-substitution does.
 
   ba_extended_robust(...)      the slam_ext.ba_extended arguments plus the kernel name,
-                               threshold and, for GNC-TLS, the mu of every iteration;
+                               threshold and, for GNC-TLS, the mu of every iteration, and the
+                               camera model (pinhole, or MEI with its k1; the reference's fused
+                               path takes pinhole only, buffer.py:387-388);
   gnc_mu_schedule(...)         the generic solver's GNC schedule (buffer.py:686-695: n_mu_steps
                                rounds of gn_iters_per_mu iterations, mu <- min(mu * step, max),
                                the hard TLS indicator once mu reaches its maximum).
@@ -38,13 +40,26 @@ def gnc_mu_schedule(n_mu_steps=4, gn_iters_per_mu=6, mu_init=1.0, mu_step=1.4, m
     return out
 
 
+CAMERAS = {None: 0, "pinhole": 0, "mei": 1}
+
+
 def ba_extended_robust(poses, disps, intrinsics, disps_sens, targets, weights, eta, ii, jj, depth_active, t0, t1,
                        iterations, lm, ep, motion_only, alpha, optimize_intrinsics, intrinsics_lm, intrinsics_ep,
                        intrinsics_scale, compute_energy=False, robust_kernel=None, threshold=1.0,
-                       mu_schedule=None):
-    """slam_ext.ba_extended with a robust kernel ('huber', 'tukey', 'gnc_tls' or None) and the
-    generic solver's back-substitution.  Returns [dx, dz or None, energy]."""
+                       mu_schedule=None, camera_type=None, distortion=0.0):
+    """slam_ext.ba_extended with a robust kernel ('huber', 'tukey', 'gnc_tls' or None), the
+    generic solver's back-substitution and the frames' camera model (camera_type 'pinhole' or
+    'mei', with distortion = the MEI k1; a vipe CameraType's value works too).  Returns
+    [dx, dz or None, energy]."""
     import ctypes
+
+    cam_name = getattr(camera_type, "value", camera_type)
+    cam_name = None if cam_name is None else str(cam_name).lower()
+    if cam_name not in CAMERAS:
+        raise ValueError(f"Unsupported camera_type for the fused BA: {camera_type!r}; expected 'pinhole' or 'mei'")
+    cam = CAMERAS[cam_name]
+    if cam == 1 and optimize_intrinsics:
+        raise RuntimeError("optimize_intrinsics is not supported with the MEI camera")
 
     name = None if robust_kernel is None else str(robust_kernel).lower()
     if name not in KINDS:
@@ -81,13 +96,14 @@ def ba_extended_robust(poses, disps, intrinsics, disps_sens, targets, weights, e
         dz = None if motion_only else torch.empty(num_kx, ht * wd, dtype=torch.float32, device=dev)
         energy = torch.empty(iterations if compute_energy else 0, dtype=torch.float32, device=dev)
         status = torch.zeros(1, dtype=torch.int32, device=dev)
-        rc = lib.vipe_slam_ba_extended_robust(
+        rc = lib.vipe_slam_ba_extended_generic(
             poses.data_ptr(), disps.data_ptr(), intrinsics.data_ptr(), disps_sens.data_ptr(), _lib.ptr(targets),
             _lib.ptr(weights), eta.data_ptr(), _lib.ptr(ii), _lib.ptr(jj), depth_active.data_ptr(), num_frames, ht,
             wd, num_edges, num_kx, t0, t1, iterations, float(lm), float(ep), int(bool(motion_only)), float(alpha),
             int(bool(optimize_intrinsics)), float(intrinsics_lm), float(intrinsics_ep), float(intrinsics_scale),
             int(bool(compute_energy)), dx.data_ptr(), _lib.ptr(dz), energy.data_ptr() if compute_energy else None,
-            kind, float(threshold), None if sched is None else ctypes.cast(sched, ctypes.c_void_p), ws.data_ptr(), ws_bytes, status.data_ptr(), _lib.stream_of(poses))
+            kind, float(threshold), None if sched is None else ctypes.cast(sched, ctypes.c_void_p), cam,
+            float(distortion), ws.data_ptr(), ws_bytes, status.data_ptr(), _lib.stream_of(poses))
         _lib.check(rc, "ba_extended_robust")
         _se._raise_device_status(int(status.item()), "ba_extended_robust")
     return [dx, dz, energy]
