@@ -151,6 +151,31 @@ int vipe_slam_ba_extended_generic(float* poses_io, float* disps_io, float* intri
                                   const float* mu_schedule, int camera_model, float distortion, void* workspace,
                                   size_t workspace_bytes, int32_t* dev_status, void* stream);
 
+/* Multi-view rigs in the fused BA: the generic solver's terms with rig extrinsics
+ * (vipe/slam/ba/terms.py:98-262, vipe/slam/maths/geom.py:187-298: each term projects depth frame
+ * d_i = p_i * n_views + q_i into frame (p_j, q_j) through R_qj^-1 G_pj G_pi^-1 R_qi); the
+ * reference's fused path refuses n_views > 1 and non-identity rigs (buffer.py:387-404).
+ *   poses_io (num_keyframes, 7) keyframe poses G (updated in the window [t0, t1));
+ *   rig (n_views, 7) fixed extrinsics R_q (cam-to-central, [tx ty tz qx qy qz qw]);
+ *   disps_io, disps_sens (num_keyframes * n_views, ht, wd), depth_active (num_keyframes * n_views);
+ *   ii, jj: source and target depth-frame indices (k * n_views + q) of the num_edges terms,
+ *     ii != jj; eta (num_kx, ht*wd) over kx = unique(arange(t0 n_views, t1 n_views) ++ ii);
+ *   intrinsics (4): fx fy cx cy at the flow resolution, shared by all views (fixed);
+ *   dx_out (t1 - t0, 6) keyframe steps; dz_out (num_kx, ht*wd); energy_out (iterations) or NULL;
+ *   robust kernel, mu schedule and camera model as vipe_slam_ba_extended_generic.
+ * Generic-solver back-substitution (rows of pose t0 kept).  Limits: n_views * (t1 - t0) <= 1024.
+ * Workspace: vipe_slam_ba_rig_workspace_size. */
+size_t vipe_slam_ba_rig_workspace_size(int num_keyframes, int n_views, int ht, int wd, int num_edges, int num_kx,
+                                       int t0, int t1);
+int vipe_slam_ba_rig(float* poses_io, const float* rig, int n_views, float* disps_io, const float* intrinsics,
+                     const float* disps_sens, const float* targets, const float* weights, const float* eta,
+                     const int64_t* ii, const int64_t* jj, const float* depth_active, int num_keyframes, int ht,
+                     int wd, int num_edges, int num_kx, int t0, int t1, int iterations, float lm, float ep,
+                     int motion_only, float alpha, int compute_energy, float* dx_out, float* dz_out,
+                     float* energy_out, int robust_kind, float robust_threshold, const float* mu_schedule,
+                     int camera_model, float distortion, void* workspace, size_t workspace_bytes,
+                     int32_t* dev_status, void* stream);
+
 /* Replaces slam_ext.ba (reference: csrc/slam_ext/slam.cpp:42-45,
  * geom_kernels.cu:1826-1834): ba_extended with depth_active = 1, no focal
  * optimisation and no energy.  depth_active_scratch: device f32 buffer of

@@ -148,3 +148,90 @@ def assert_camera_matches_generic(name, poses, disps):
     d = disps[:n].cpu().float().clamp(min=0.001)
     torch.testing.assert_close(d, g["disps"][:n], atol=5e-3, rtol=0)
     assert float((d - g["disps"][:n]).abs().mean()) < 2e-4
+
+
+# ---------------------------------------------------------------- multi-view rig case
+
+RIG_T = (0.12, 0.02, -0.03)          # view 1's extrinsics (cam-to-central) translation
+RIG_AA = (0.04, -0.09, 0.02)         # and axis-angle rotation; view 0 is the identity
+
+
+def _quat_of_aa(aa):
+    import math
+
+    th = math.sqrt(sum(a * a for a in aa))
+    s = math.sin(th / 2) / th
+    return [aa[0] * s, aa[1] * s, aa[2] * s, math.cos(th / 2)]
+
+
+def _mat(T):
+    """(..., 7) [t, q] -> (..., 4, 4) float64."""
+    T = T.double()
+    x, y, z, w = T[..., 3], T[..., 4], T[..., 5], T[..., 6]
+    R = torch.stack([1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y),
+                     2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x),
+                     2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)], -1).reshape(*T.shape[:-1], 3, 3)
+    M = torch.zeros(*T.shape[:-1], 4, 4, dtype=torch.float64)
+    M[..., :3, :3] = R
+    M[..., :3, 3] = T[..., :3]
+    M[..., 3, 3] = 1
+    return M
+
+
+def rig_problem(outliers=False):
+    """A two-view rig built from config 0 (deterministic, CPU): keyframe poses, rig (2, 7), depth
+    frames k * 2 + q (view 1: 0.9 x view 0), the expanded terms of config 0's edges (edge-major,
+    view-minor, as GraphBuffer.expand_edge_multiview orders them), targets = the reprojection at
+    the initial state through the rig plus a deterministic +-0.8 px pattern (optionally the
+    outliers of with_outliers), config 0's weights per view, eta for kx, 2 LM iterations."""
+    import types
+
+    from vipe_b200 import workloads as W
+
+    p = W.ba_config0()
+    N, H, Wd = p.disps.shape
+    V = 2
+    rig = torch.zeros(V, 7)
+    rig[:, 6] = 1
+    rig[1, :3] = torch.tensor(RIG_T)
+    rig[1, 3:] = torch.tensor(_quat_of_aa(RIG_AA))
+    disps = torch.stack([p.disps, 0.9 * p.disps], 1).reshape(N * V, H, Wd).contiguous()
+    sens = torch.stack([p.disps_sens, p.disps_sens], 1).reshape(N * V, H, Wd).contiguous()
+    E = p.ii.shape[0]
+    pi = p.ii.repeat_interleave(V)
+    pj = p.jj.repeat_interleave(V)
+    q = torch.arange(V).repeat(E)
+    di, dj = pi * V + q, pj * V + q
+    fx, fy, cx, cy = [float(v) for v in p.intrinsics]
+    G, Rg = _mat(p.poses), _mat(rig)
+    T = torch.linalg.inv(Rg[q]) @ G[pj] @ torch.linalg.inv(G[pi]) @ Rg[q]
+    vv, uu = torch.meshgrid(torch.arange(H, dtype=torch.float64), torch.arange(Wd, dtype=torch.float64),
+                            indexing="ij")
+    X = torch.stack([(uu - cx) / fx, (vv - cy) / fy, torch.ones_like(uu)], 0).reshape(3, -1)
+    d = disps.double()[di].reshape(E * V, 1, -1)
+    Pp = T[:, :3, :3] @ X + T[:, :3, 3:] * d
+    z = Pp[:, 2].clamp(min=0.1)
+    tu = fx * Pp[:, 0] / z + cx
+    tv = fy * Pp[:, 1] / z + cy
+    k = torch.arange(E * V, dtype=torch.float64)[:, None]
+    pix = torch.arange(H * Wd, dtype=torch.float64)[None]
+    tu = tu + 0.8 * torch.sin(0.37 * pix + 1.1 * k)
+    tv = tv + 0.8 * torch.cos(0.23 * pix + 0.7 * k)
+    targets = torch.stack([tu, tv], 1).reshape(E * V, 2, H, Wd).float()
+    if outliers:
+        targets = with_outliers(targets)
+    weights = p.weights.repeat_interleave(V, 0).contiguous()
+    kx = torch.unique(torch.cat([torch.arange(p.t0 * V, p.t1 * V), di]))
+    disp_damping = ((p.eta.double() - 1e-7) / 0.2).float()  # per keyframe; both views share it
+    eta_frames = disp_damping.repeat_interleave(V, 0)  # (N * V, H*W) in frame order
+    eta = (0.2 * eta_frames[kx] + 1e-7).float().contiguous()
+    return types.SimpleNamespace(poses=p.poses.clone(), rig=rig, disps=disps, disps_sens=sens,
+                                 intrinsics=p.intrinsics.clone(), targets=targets.contiguous(), weights=weights,
+                                 ii=di.contiguous(), jj=dj.contiguous(), eta=eta, kx=kx,
+                                 disp_damping=disp_damping, depth_active=torch.ones(N * V), t0=p.t0, t1=p.t1,
+                                 iterations=2, lm=float(p.lm), ep=float(p.ep), alpha=float(p.alpha), N=N, V=V,
+                                 pi=pi, pj=pj, q=q)
+
+
+def rig_cases():
+    return torch.load(GOLDEN, weights_only=False)["rig"]

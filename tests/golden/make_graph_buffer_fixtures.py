@@ -31,7 +31,8 @@ Robust kernels: config 0 with deterministic outlier flow is solved by the generi
 Huber, Tukey and GNC-TLS (the reference's fused path refuses robust kernels); the results go
 to the "robust" entry and are held to vipe_slam_ba_extended_robust on the GPU.  The same
 config 0 through the generic solver with the MEI camera (plain, and with Huber on the outlier
-targets) goes to the "camera" entry (the fused path refuses non-pinhole buffers).
+targets) goes to the "camera" entry (the fused path refuses non-pinhole buffers), and a two-view rig
+(tests/_graph_buffer_golden.rig_problem) solved by GraphBuffer(n_views=2) to the "rig" entry.
 
 The same is done for a third case built from config 0 (8 keyframes, 48x64 disparity,
 26 edges, 2 iterations): GraphBuffer(384x512) is loaded with the config-0
@@ -327,6 +328,59 @@ def camera_cases():
     return out
 
 
+RIG = {
+    # name: (outliers, robust_kernel, threshold, n_iters)
+    "rig": (False, None, 1.0, 2),
+    "rig_huber": (True, "huber", 2.0, 3),
+}
+
+
+def rig_cases():
+    """A two-view rig (tests/_graph_buffer_golden.rig_problem) solved by the reference's generic
+    solver: GraphBuffer(n_views=2) with the rig extrinsics, expanded terms from
+    expand_edge_multiview (the fused path refuses n_views > 1, buffer.py:387-388)."""
+    from vipe.slam.components.buffer import GraphBuffer
+    from vipe.slam.components.sparse_tracks import DummySparseTracks
+    from vipe.utils.cameras import CameraType
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    import _graph_buffer_golden as Gd
+
+    out = {}
+    for name, (outl, kernel, thr, n_iters) in RIG.items():
+        r = Gd.rig_problem(outliers=outl)
+        N, V = r.N, r.V
+        H, Wd = r.disps.shape[1:]
+        cfg = _Cfg({"dense_disp_alpha": r.alpha, "fused": False, "intrinsics_damping_scale": 1.0,
+                    "robust_kernel": kernel, "robust_kernel_threshold": thr, "gnc_mu_init": 1.0, "gnc_mu_step": 3.0,
+                    "gnc_mu_max": 1.0e6, "gnc_n_mu_steps": 4, "gnc_gn_iters_per_mu": 6})
+        v = GraphBuffer(height=8 * H, width=8 * Wd, n_views=V, buffer_size=N, init_disp=1.0, cross_view_idx=None,
+                        ba_config=cfg, sparse_tracks=DummySparseTracks(n_views=V), camera_type=CameraType.PINHOLE,
+                        device=torch.device("cpu"))
+        v.n_frames = N
+        v.tstamp[:N] = torch.arange(N)
+        v.intrinsics[:, :4] = r.intrinsics * 8
+        v.rig[:] = r.rig
+        v.poses[:N] = r.poses
+        v.disps[:N] = r.disps.reshape(N, V, H, Wd)
+        v.disps_sens[:N] = r.disps_sens.reshape(N, V, H, Wd)
+        # the expansion the generic solver makes must be the one the problem was built on
+        pi, qi, di, pj, qj, dj = v.expand_edge_multiview(r.pi[::V], r.pj[::V])
+        assert torch.equal(di, r.ii) and torch.equal(dj, r.jj)
+        E = r.targets.shape[0]
+        target = r.targets.permute(0, 2, 3, 1).reshape(E, H * Wd, 2).contiguous()
+        weight = r.weights.permute(0, 2, 3, 1).reshape(E, H * Wd, 2).contiguous()
+        disp_damping = r.disp_damping.repeat_interleave(V, 0).reshape(N * V, H, Wd)
+        v.bundle_adjustment(target=target, weight=weight, disp_damping=disp_damping, ii=r.pi[::V].clone(),
+                            jj=r.pj[::V].clone(), t0=r.t0, t1=r.t1, n_iters=n_iters, pose_damping=r.lm,
+                            pose_ep=r.ep, motion_only=False, limited_disp=False, optimize_intrinsics=False,
+                            optimize_rig_rotation=False, verbose=False)
+        out[name] = {"outliers": outl, "kernel": kernel, "threshold": thr, "iterations": n_iters, "n_frames": N,
+                     "generic": {"poses": v.poses.clone(), "disps": v.disps.clone().reshape(-1, H, Wd)},
+                     "before": {"poses": r.poses.clone()}}
+    return out
+
+
 def robust_cases():
     """Config 0 with deterministic outlier flow (tests/_graph_buffer_golden.with_outliers) solved
     by the reference's generic solver with each robust kernel (buffer.py:531-695; the fused path
@@ -386,11 +440,12 @@ def main(ref: Path):
     }
     robust = robust_cases()
     camera = camera_cases()
-    torch.save({"cases": cases, "robust": robust, "camera": camera, "torch": torch.__version__}, OUT)
+    rig = rig_cases()
+    torch.save({"cases": cases, "robust": robust, "camera": camera, "rig": rig, "torch": torch.__version__}, OUT)
     print(f"wrote {OUT} ({OUT.stat().st_size} bytes)")
     before = cases["config0"]["before"]["poses"]
     for k, c in {**cases, **{"robust_" + k: v for k, v in robust.items()},
-                 **{"camera_" + k: v for k, v in camera.items()}}.items():
+                 **{"camera_" + k: v for k, v in camera.items()}, **{"rig_" + k: v for k, v in rig.items()}}.items():
         d = (c["generic"]["poses"] - c.get("before", {"poses": before})["poses"]).abs().max()
         print(f"  {k}: generic solver moved poses by {float(d):.3e}")
 

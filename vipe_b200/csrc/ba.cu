@@ -2268,8 +2268,9 @@ int launch_index(const Geometry& geo, const GraphDesc* d_table, const BAPtrs& ba
     return VIPE_OK;
 }
 
+// linearisation, Schur products and assembly of Hm, bv; then (solve) the damped reduced solve
 int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const int* d_off, const BAPtrs& base,
-                           const SolveArgs& a, int itr, cudaStream_t st) {
+                           const SolveArgs& a, int itr, cudaStream_t st, bool solve) {
     const int G = geo.G;
     const Batch per_graph{d_table, nullptr, G};
     auto grid = [&](int k) { return (unsigned)geo.off[k][G]; };
@@ -2342,6 +2343,14 @@ int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const 
         ba_energy_kernel<<<G, 256, 0, st>>>(base, per_graph, with_frames, itr);
         VIPE_LAUNCH_CHECK();
     }
+    return solve ? launch_cholesky(geo, d_table, d_off, base, a, st) : VIPE_OK;
+}
+
+// the damped reduced solve of every graph of the table: dx (and the focal step) from Hm, bv
+int launch_cholesky(const Geometry& geo, const GraphDesc* d_table, const int* d_off, const BAPtrs& base,
+                    const SolveArgs& a, cudaStream_t st) {
+    const int G = geo.G;
+    const bool intr = a.intr != 0;
     if (geo.chol_big) {
         VIPE_PROF("ba_cholesky", st);
         const Batch one{d_table, nullptr, 1};
@@ -2640,6 +2649,253 @@ extern "C" int vipe_slam_ba_extended_robust(float* poses_io, float* disps_io, fl
                                          intrinsics_scale, compute_energy, dx_out, dz_out, energy_out, robust_kind,
                                          robust_threshold, mu_schedule, 0, 0.f, workspace, workspace_bytes,
                                          dev_status, stream);
+}
+
+// ---------------------------------------------------------------- multi-view rigs
+//
+// The generic solver's multi-view terms (vipe/slam/ba/terms.py:98-262 through
+// vipe/slam/maths/geom.py:187-298): keyframe poses G_k, V views with fixed rig extrinsics
+// R_q (cam-to-central), depth frames d = k V + q, and each term projecting frame (pi, qi)
+// into (pj, qj) through T = R_qj^-1 G_pj G_pi^-1 R_qi.  Here every (keyframe, view) is a
+// virtual pose Tv(k, q) = R_q^-1 G_k, so T = Tv(pj, qj) Tv(pi, qi)^-1 and the single-view
+// kernels linearise, Schur-eliminate and assemble the system of the virtual window poses
+// unchanged.  A left step xi_k of G_k moves Tv(k, q) by A_q xi_k, A_q = Ad(R_q^-1), so the
+// keyframe system is S_k = A^T S_v A, b_k = A^T b_v (summed over the views of each keyframe);
+// it is damped and solved by the same Cholesky kernels, expanded back (dx_v = A_q dx_k) for the
+// depth back-substitution, and G_k is retracted by dx_k.
+
+// Tv(k, q) = R_q^-1 G_k for every keyframe and view (poses [tx ty tz qx qy qz qw])
+__global__ void ba_rig_virtual_kernel(const float* __restrict__ poses, const float* __restrict__ rig, int N, int V,
+                                      float* __restrict__ vposes) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N * V) return;
+    const int k = i / V, q = i % V;
+    const float* G = poses + (size_t)k * 7;
+    const float* R = rig + (size_t)q * 7;
+    const float rc[4] = {-R[3], -R[4], -R[5], R[6]};  // R_q^-1 rotation
+    const float* g = G + 3;
+    float* o = vposes + (size_t)i * 7;
+    // quaternion rc (x) g
+    o[3] = rc[3] * g[0] + rc[0] * g[3] + rc[1] * g[2] - rc[2] * g[1];
+    o[4] = rc[3] * g[1] + rc[1] * g[3] + rc[2] * g[0] - rc[0] * g[2];
+    o[5] = rc[3] * g[2] + rc[2] * g[3] + rc[0] * g[1] - rc[1] * g[0];
+    o[6] = rc[3] * g[3] - rc[0] * g[0] - rc[1] * g[1] - rc[2] * g[2];
+    const float dt[3] = {G[0] - R[0], G[1] - R[1], G[2] - R[2]};
+    qrot(rc, dt, o);
+}
+
+// A_q = Ad(R_q^-1) = [[Ri, [ti]x Ri], [0, Ri]] in FP64, Ri = R^T, ti = -R^T t (row-major 6 x 6)
+__global__ void ba_rig_adjoint_kernel(const float* __restrict__ rig, int V, double* __restrict__ A) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= V) return;
+    const float* R = rig + (size_t)q * 7;
+    const double x = R[3], y = R[4], z = R[5], w = R[6];
+    const double Rm[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y),
+                          2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x),
+                          2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)};
+    double Ri[9], ti[3];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) Ri[3 * r + c] = Rm[3 * c + r];
+    for (int r = 0; r < 3; r++) ti[r] = -(Ri[3 * r] * R[0] + Ri[3 * r + 1] * R[1] + Ri[3 * r + 2] * R[2]);
+    const double tx[9] = {0, -ti[2], ti[1], ti[2], 0, -ti[0], -ti[1], ti[0], 0};
+    double* o = A + (size_t)q * 36;
+    for (int r = 0; r < 6; r++)
+        for (int c = 0; c < 6; c++) o[6 * r + c] = 0.0;
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) {
+            o[6 * r + c] = Ri[3 * r + c];
+            o[6 * (r + 3) + c + 3] = Ri[3 * r + c];
+            double s = 0.0;
+            for (int m = 0; m < 3; m++) s += tx[3 * r + m] * Ri[3 * m + c];
+            o[6 * r + c + 3] = s;
+        }
+}
+
+// S_k = A^T S_v A and b_k = A^T b_v over the window (P keyframes, V views); the focal
+// row and column of S_k are zero (the rig solve keeps the intrinsics fixed)
+__global__ void ba_rig_project_kernel(const double* __restrict__ Hv, const double* __restrict__ bv, int ldv, int P,
+                                      int V, const double* __restrict__ A, double* __restrict__ Hk,
+                                      double* __restrict__ bk, int ldk) {
+    const long n = 6L * P;
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < (long)ldk * ldk) {
+        const long r = i / ldk, c = i % ldk;
+        double s = 0.0;
+        if (r < n && c < n) {
+            const int a = (int)(r / 6), ir = (int)(r % 6), b = (int)(c / 6), jc = (int)(c % 6);
+            for (int q = 0; q < V; q++) {
+                const double* Aq = A + (size_t)q * 36;
+                for (int q2 = 0; q2 < V; q2++) {
+                    const double* Aq2 = A + (size_t)q2 * 36;
+                    const double* blk = Hv + (size_t)((a * V + q) * 6) * ldv + (size_t)(b * V + q2) * 6;
+                    for (int m = 0; m < 6; m++) {
+                        double t = 0.0;
+                        for (int nn = 0; nn < 6; nn++) t += blk[(size_t)m * ldv + nn] * Aq2[6 * nn + jc];
+                        s += Aq[6 * m + ir] * t;
+                    }
+                }
+            }
+        }
+        Hk[i] = s;
+    }
+    if (i < ldk) {
+        double s = 0.0;
+        if (i < n) {
+            const int a = (int)(i / 6), ir = (int)(i % 6);
+            for (int q = 0; q < V; q++)
+                for (int m = 0; m < 6; m++) s += A[(size_t)q * 36 + 6 * m + ir] * bv[(a * V + q) * 6 + m];
+        }
+        bk[i] = s;
+    }
+}
+
+// dx_v(a V + q) = A_q dx_k(a)
+__global__ void ba_rig_expand_kernel(const float* __restrict__ dxk, const double* __restrict__ A, int P, int V,
+                                     float* __restrict__ dxv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P * V * 6) return;
+    const int av = i / 6, m = i % 6, a = av / V, q = av % V;
+    double s = 0.0;
+    for (int n = 0; n < 6; n++) s += A[(size_t)q * 36 + 6 * m + n] * (double)dxk[6 * a + n];
+    dxv[i] = (float)s;
+}
+
+// G_k <- Exp(dx_k) G_k over the keyframe window
+__global__ void ba_rig_retract_kernel(float* __restrict__ poses, const float* __restrict__ dxk, int t0, int P,
+                                      const int* __restrict__ status_v, const int* __restrict__ status_k) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P || status_v[0] || status_k[0]) return;
+    float xi[6], T[7];
+    for (int n = 0; n < 6; n++) xi[n] = dxk[6 * a + n];
+    float* pz = poses + (size_t)(t0 + a) * 7;
+    for (int n = 0; n < 7; n++) T[n] = pz[n];
+    retract_pose(xi, T);
+    for (int n = 0; n < 7; n++) pz[n] = T[n];
+}
+
+// the keyframe-solve descriptor of a rig solve (no edges, no depth frames) into the workspace
+__global__ void ba_rig_desc_kernel(GraphDesc* table, GraphDesc gd) {
+    if (threadIdx.x == 0) {
+        *table = gd;
+        for (int n = 0; n < 4; n++) gd.w.status[n] = 0;
+    }
+}
+
+static void rig_dims(int N, int V, int ht, int wd, int E, int K, int t0, int t1, Dims& dv, Dims& dk) {
+    dv = make_dims(N * V, ht, wd, E, K, t0 * V, t1 * V, 0, 0, 6, true);
+    dk = make_dims(N, ht, wd, 0, 0, t0, t1, 0, 0, 6, true);
+}
+
+template <typename C>
+static void rig_carve(C& cv, const Dims& dv, const Dims& dk, GraphDesc& gv, GraphDesc& gk, GraphDesc** tv,
+                      GraphDesc** tk, float** vposes, float** vdx, double** A, int V) {
+    *tv = carve_single(cv, dv, &gv.w);
+    *tk = carve_single(cv, dk, &gk.w);
+    *vposes = cv.template take<float>((size_t)dv.N * 7);
+    *vdx = cv.template take<float>((size_t)std::max(dv.P, 1) * 6);
+    *A = cv.template take<double>((size_t)V * 36);
+}
+
+extern "C" size_t vipe_slam_ba_rig_workspace_size(int num_keyframes, int n_views, int ht, int wd, int num_edges,
+                                                  int num_kx, int t0, int t1) {
+    if (n_views < 1 || num_keyframes < 1 || (long)num_keyframes * n_views > (1 << 30)) return 0;
+    if (check_dims(num_keyframes * n_views, ht, wd, num_edges, num_kx, t0 * n_views, t1 * n_views) != VIPE_OK)
+        return 0;
+    Dims dv, dk;
+    rig_dims(num_keyframes, n_views, ht, wd, num_edges, num_kx, t0, t1, dv, dk);
+    Sizer c;
+    GraphDesc gv{}, gk{};
+    GraphDesc *tv, *tk;
+    float *vp, *vdx;
+    double* A;
+    rig_carve(c, dv, dk, gv, gk, &tv, &tk, &vp, &vdx, &A, n_views);
+    return c.used + 256;
+}
+
+extern "C" int vipe_slam_ba_rig(float* poses_io, const float* rig, int n_views, float* disps_io,
+                                const float* intrinsics, const float* disps_sens, const float* targets,
+                                const float* weights, const float* eta, const int64_t* ii, const int64_t* jj,
+                                const float* depth_active, int num_keyframes, int ht, int wd, int num_edges,
+                                int num_kx, int t0, int t1, int iterations, float lm, float ep, int motion_only,
+                                float alpha, int compute_energy, float* dx_out, float* dz_out, float* energy_out,
+                                int robust_kind, float robust_threshold, const float* mu_schedule, int camera_model,
+                                float distortion, void* workspace, size_t workspace_bytes, int32_t* dev_status,
+                                void* stream) {
+    if (n_views < 1 || !rig) {
+        set_last_error("rig BA: n_views >= 1 and the rig extrinsics (n_views, 7) are required");
+        return VIPE_ERR_ARG;
+    }
+    if (camera_model != 0 && camera_model != 1) return VIPE_ERR_ARG;
+    if (camera_model == 1 && !(distortion >= 0.f && distortion <= 1.f)) return VIPE_ERR_ARG;
+    if (robust_kind < 0 || robust_kind > 3 || (robust_kind != 0 && !(robust_threshold > 0.f))) return VIPE_ERR_ARG;
+    if (robust_kind == 3) {
+        if (!mu_schedule) return VIPE_ERR_ARG;
+        for (int k = 0; k < iterations; k++)
+            if (!(mu_schedule[k] > 0.f)) return VIPE_ERR_ARG;
+    }
+    const int V = n_views, Nv = num_keyframes * V;
+    int rc = check_dims(Nv, ht, wd, num_edges, num_kx, t0 * V, t1 * V);
+    if (rc != VIPE_OK) return rc;
+    rc = check_ba_args(poses_io, disps_io, intrinsics, disps_sens, targets, weights, eta, ii, jj, depth_active,
+                       num_edges, iterations, motion_only, compute_energy, dx_out, dz_out, energy_out);
+    if (rc != VIPE_OK) return rc;
+    cudaStream_t st = as_stream(stream);
+    GraphDesc gv{}, gk{};
+    rig_dims(num_keyframes, V, ht, wd, num_edges, num_kx, t0, t1, gv.d, gk.d);
+    Carver cv(workspace, workspace_bytes);
+    GraphDesc *tv, *tk;
+    float *vposes, *vdx;
+    double* A;
+    rig_carve(cv, gv.d, gk.d, gv, gk, &tv, &tk, &vposes, &vdx, &A, V);
+    if (!cv.ok) return VIPE_ERR_WORKSPACE;
+    if ((rc = ensure_attributes()) != VIPE_OK) return rc;
+    Geometry geo_v, geo_k;
+    fill_geometry({gv.d}, geo_v);
+    fill_geometry({gk.d}, geo_k);
+    BAPtrs bv{vposes, disps_io, const_cast<float*>(intrinsics), disps_sens, targets, weights, eta, ii, jj,
+              depth_active, vdx, motion_only ? nullptr : dz_out, compute_energy ? energy_out : nullptr, dev_status,
+              iterations, 0};
+    bv.rb.kind = robust_kind;
+    bv.rb.c = robust_kind ? robust_threshold : 1.f;
+    bv.rb.cam = camera_model;
+    bv.rb.k1 = camera_model == 1 ? distortion : 0.f;
+    bv.exact_backsub = 1;
+    BAPtrs bk{poses_io, nullptr, const_cast<float*>(intrinsics), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+              nullptr, dx_out, nullptr, nullptr, dev_status, iterations, 0};
+    SolveArgs a{iterations, lm, ep, alpha, motion_only, 0, 1e-6f, 1e-6f, 1.f, compute_energy};
+    const int P = t1 - t0;
+    if ((rc = launch_index(geo_v, tv, bv, &gv, st)) != VIPE_OK) return rc;
+    ba_rig_desc_kernel<<<1, 32, 0, st>>>(tk, gk);
+    VIPE_LAUNCH_CHECK();
+    ba_rig_adjoint_kernel<<<1, 32 * ((V + 31) / 32), 0, st>>>(rig, V, A);
+    VIPE_LAUNCH_CHECK();
+    const int ldv = gv.d.dim, ldk = gk.d.dim;
+    for (int itr = 0; itr < iterations; itr++) {
+        BAPtrs b = bv;
+        if (robust_kind == 3) b.rb.mu = mu_schedule[itr];
+        ba_rig_virtual_kernel<<<ceil_div(Nv, 128), 128, 0, st>>>(poses_io, rig, num_keyframes, V, vposes);
+        VIPE_LAUNCH_CHECK();
+        if ((rc = launch_linearize_solve(geo_v, tv, nullptr, b, a, itr, st, false)) != VIPE_OK) return rc;
+        {
+            VIPE_PROF("ba_rig_project", st);
+            ba_rig_project_kernel<<<ceil_div((long)ldk * ldk, 256), 256, 0, st>>>(gv.w.Hm, gv.w.bv, ldv, P, V, A,
+                                                                                 gk.w.Hm, gk.w.bv, ldk);
+        }
+        VIPE_LAUNCH_CHECK();
+        if ((rc = launch_cholesky(geo_k, tk, nullptr, bk, a, st)) != VIPE_OK) return rc;
+        ba_rig_expand_kernel<<<ceil_div(P * V * 6, 128), 128, 0, st>>>(dx_out, A, P, V, vdx);
+        VIPE_LAUNCH_CHECK();
+        if ((rc = launch_update(geo_v, tv, nullptr, b, a, st)) != VIPE_OK) return rc;
+        ba_rig_retract_kernel<<<ceil_div(P, 128), 128, 0, st>>>(poses_io, dx_out, t0, P, gv.w.status, gk.w.status);
+        VIPE_LAUNCH_CHECK();
+    }
+    if (dev_status) {
+        ba_status_kernel<<<1, 1, 0, st>>>(bv, Batch{tv, nullptr, 1});
+        VIPE_LAUNCH_CHECK();
+        ba_status_kernel<<<1, 1, 0, st>>>(bk, Batch{tk, nullptr, 1});
+        VIPE_LAUNCH_CHECK();
+    }
+    return VIPE_OK;
 }
 
 // ---------------------------------------------------------------- batched solve

@@ -462,10 +462,13 @@ int check_dims(int num_frames, int ht, int wd, int num_edges, int num_kx, int t0
 int ensure_attributes();
 int launch_index(const Geometry& geo, const GraphDesc* d_table, const BAPtrs& base, const GraphDesc* init,
                  cudaStream_t st);
-// one LM step's linearisation, assembly and factorised solve (dx = Delta xi) at
+// one LM step's linearisation, assembly and (solve) factorised solve (dx = Delta xi) at
 // the state held by base.poses / base.disps; nothing is updated
 int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const int* d_off, const BAPtrs& base,
-                           const SolveArgs& a, int itr, cudaStream_t st);
+                           const SolveArgs& a, int itr, cudaStream_t st, bool solve = true);
+// the damped reduced solve alone (Hm, bv of every graph -> dx)
+int launch_cholesky(const Geometry& geo, const GraphDesc* d_table, const int* d_off, const BAPtrs& base,
+                    const SolveArgs& a, cudaStream_t st);
 // adj_lam = S'^-1 adj_rhs per graph, with the factor recorded in base.ftape
 int launch_chol_resolve(const Geometry& geo, const GraphDesc* d_table, const BAPtrs& base, cudaStream_t st);
 

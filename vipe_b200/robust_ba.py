@@ -13,6 +13,9 @@ pose t0 as the generic solver's Schur back-substitution does.
                                threshold and, for GNC-TLS, the mu of every iteration, and the
                                camera model (pinhole, or MEI with its k1; the reference's fused
                                path takes pinhole only, buffer.py:387-388);
+  ba_rig(...)                  the same over a multi-view rig: keyframe poses, fixed rig
+                               extrinsics, depth frames k * n_views + q (the reference's fused
+                               path takes single-view buffers with an identity rig only);
   gnc_mu_schedule(...)         the generic solver's GNC schedule (buffer.py:686-695: n_mu_steps
                                rounds of gn_iters_per_mu iterations, mu <- min(mu * step, max),
                                the hard TLS indicator once mu reaches its maximum).
@@ -106,4 +109,65 @@ def ba_extended_robust(poses, disps, intrinsics, disps_sens, targets, weights, e
             float(distortion), ws.data_ptr(), ws_bytes, status.data_ptr(), _lib.stream_of(poses))
         _lib.check(rc, "ba_extended_robust")
         _se._raise_device_status(int(status.item()), "ba_extended_robust")
+    return [dx, dz, energy]
+
+
+def ba_rig(poses, rig, disps, intrinsics, disps_sens, targets, weights, eta, ii, jj, depth_active, t0, t1, iterations,
+           lm, ep, motion_only, alpha, compute_energy=False, robust_kernel=None, threshold=1.0, mu_schedule=None,
+           camera_type=None, distortion=0.0):
+    """Fused BA over a multi-view rig (vipe_slam_ba_rig): keyframe poses (N, 7), fixed rig
+    extrinsics (V, 7), depth frames (N * V, H, W) indexed k * V + q, and per-term source/target
+    depth-frame indices ii, jj.  Returns [dx (t1 - t0, 6), dz or None, energy]."""
+    import ctypes
+
+    name = None if robust_kernel is None else str(robust_kernel).lower()
+    if name not in KINDS:
+        raise ValueError(f"Unknown robust_kernel: {robust_kernel!r}; expected 'huber' | 'tukey' | 'gnc_tls' | None")
+    kind = KINDS[name]
+    cam_name = getattr(camera_type, "value", camera_type)
+    cam_name = None if cam_name is None else str(cam_name).lower()
+    if cam_name not in CAMERAS:
+        raise ValueError(f"Unsupported camera_type for the fused BA: {camera_type!r}; expected 'pinhole' or 'mei'")
+    cam = CAMERAS[cam_name]
+    iterations = int(iterations)
+    sched = None
+    if kind == 3:
+        if mu_schedule is None or len(mu_schedule) != iterations:
+            raise RuntimeError("GNC-TLS needs the mu of every iteration (gnc_mu_schedule)")
+        sched = (ctypes.c_float * iterations)(*[float(m) for m in mu_schedule])
+    _se._check_ba_inputs(targets=targets, weights=weights, poses=poses, rig=rig, disps=disps, intrinsics=intrinsics,
+                         disps_sens=disps_sens, ii=ii, jj=jj, depth_active=depth_active, eta=eta)
+    for nm, t in (("poses", poses), ("rig", rig), ("disps", disps), ("intrinsics", intrinsics),
+                  ("disps_sens", disps_sens), ("targets", targets), ("weights", weights), ("eta", eta),
+                  ("depth_active", depth_active)):
+        _lib.require_dtype(nm, t, torch.float32)
+    _lib.require_dtype("ii", ii, torch.int64)
+    _lib.require_dtype("jj", jj, torch.int64)
+    N, V = poses.shape[0], rig.shape[0]
+    if disps.shape[0] != N * V:
+        raise RuntimeError("disps must hold num_keyframes * n_views depth frames")
+    t0, t1 = int(t0), int(t1)
+    _, ht, wd = disps.shape
+    num_edges, num_kx = ii.shape[0], eta.shape[0]
+    dev = poses.device
+    lib = _lib.load()
+    ws_bytes = lib.vipe_slam_ba_rig_workspace_size(N, V, ht, wd, num_edges, num_kx, t0, t1)
+    if ws_bytes == 0:
+        raise RuntimeError("rig bundle adjustment: unsupported sizes or window")
+    with torch.cuda.device(dev):
+        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+        dx = torch.zeros(max(t1 - t0, 0), 6, dtype=torch.float32, device=dev)
+        dz = None if motion_only else torch.empty(num_kx, ht * wd, dtype=torch.float32, device=dev)
+        energy = torch.empty(iterations if compute_energy else 0, dtype=torch.float32, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        rc = lib.vipe_slam_ba_rig(
+            poses.data_ptr(), rig.data_ptr(), V, disps.data_ptr(), intrinsics.data_ptr(), disps_sens.data_ptr(),
+            _lib.ptr(targets), _lib.ptr(weights), eta.data_ptr(), _lib.ptr(ii), _lib.ptr(jj), depth_active.data_ptr(),
+            N, ht, wd, num_edges, num_kx, t0, t1, iterations, float(lm), float(ep), int(bool(motion_only)),
+            float(alpha), int(bool(compute_energy)), dx.data_ptr(), _lib.ptr(dz),
+            energy.data_ptr() if compute_energy else None, kind, float(threshold),
+            None if sched is None else ctypes.cast(sched, ctypes.c_void_p), cam, float(distortion), ws.data_ptr(),
+            ws_bytes, status.data_ptr(), _lib.stream_of(poses))
+        _lib.check(rc, "ba_rig")
+        _se._raise_device_status(int(status.item()), "ba_rig")
     return [dx, dz, energy]
