@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--e2e-parts", type=int, default=24,
                     help="host batch split into this many streamed parts for the end-to-end leg")
     ap.add_argument("--case", choices=["ba0", "ba1", "corr_build", "batch", "lookup", "corr_bwd", "corr_extras",
-                                       "backend"],
+                                       "backend", "corr_encoder"],
                     help="run one workload --reps times and exit (for profiler captures; no JSON line)")
     ap.add_argument("--clips", type=int, default=32)
     ap.add_argument("--reps", type=int, default=2)
@@ -1276,6 +1276,7 @@ def run_ours(args):
 #   corr_bwd      CorrVolume backward of --edges pairs (FP16 maps and level gradients, 48x64, 4 levels)
 #   corr_extras   the correlation extras leg alone (prints its JSON)
 #   backend       the 256-keyframe backend window through slam_ext.ba_extended
+#   corr_encoder  lookup fused with corr_encoder's 1x1 conv + ReLU over --edges pairs (FP16, 4 levels)
 
 import torch  # noqa: E402  (the cases below run under torch; the benchmark legs import it lazily)
 
@@ -1393,6 +1394,24 @@ def case_corr_bwd(edges: int, reps: int) -> None:
         raise RuntimeError("device status set")
 
 
+def case_corr_encoder(edges: int, reps: int) -> None:
+    from vipe_b200.droid_corr import CorrBlock, corr_encoder_input
+
+    E, C, H, W = edges, 128, 48, 64
+    g = torch.Generator(device="cuda").manual_seed(1002)
+    fa = (torch.randn(1, E, C, H, W, generator=g, device="cuda") / 4).half()
+    fb = (torch.randn(1, E, C, H, W, generator=g, device="cuda") / 4).half()
+    blk = CorrBlock(fa, fb, num_levels=4, radius=3, out_dtype=torch.float16)
+    yy, xx = torch.meshgrid(torch.arange(H, device="cuda"), torch.arange(W, device="cuda"), indexing="ij")
+    coords = torch.stack([xx, yy], -1).float()[None, None].repeat(1, E, 1, 1, 1)
+    coords = coords + torch.randn(coords.shape, generator=g, device="cuda")
+    wt = torch.randn(128, 196, 1, 1, generator=g, device="cuda") / 14.0
+    bs = 0.1 * torch.randn(128, generator=g, device="cuda")
+    for _ in range(reps):
+        corr_encoder_input(blk, coords, wt, bs, check=True)
+    torch.cuda.synchronize()
+
+
 def case_backend(reps: int) -> None:
     from vipe_b200 import workloads as W
     from vipe_b200.ext import slam_ext
@@ -1417,6 +1436,8 @@ def run_case(args):
         case_corr_bwd(args.edges, args.reps)
     elif args.case == "backend":
         case_backend(args.reps)
+    elif args.case == "corr_encoder":
+        case_corr_encoder(args.edges, args.reps)
     elif args.case == "batch":
         case_batch(args.clips, args.reps)
     elif args.case == "lookup":
