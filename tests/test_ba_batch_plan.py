@@ -86,6 +86,8 @@ def test_plan_groups():
     lib.vipe_slam_ba_batch_plan_destroy(h)
     lib.vipe_slam_ba_batch_plan_destroy(h3)
     assert _plan(*sz, group=5)[0] == _lib.VIPE_ERR_GROUP
-    assert _plan(*sz, group=4, adjoint=1)[0] == _lib.VIPE_ERR_GROUP
+    rc7, h7 = _plan(*sz, group=4, adjoint=1)  # Sim3 plans take the adjoint too
+    assert rc7 == 0
+    lib.vipe_slam_ba_batch_plan_destroy(h7)
     # Sim3 windows are limited to 109 poses (7 P + 1 unknowns in the staged Cholesky panel)
     assert _plan([120], [200], [118], [2], [120], group=4)[0] == _lib.VIPE_ERR_CAPACITY

@@ -19,7 +19,8 @@ Gradient layout for poses follows lietorch (csrc/lietorch_ext/lietorch_gpu.cu:
 85-98): the gradient with respect to a pose tensor (N, 7) is the left-tangent
 gradient d loss / d eps of T -> Exp(eps) T in columns 0..5, column 6 zero — both
 for the gradient flowing in (as lietorch's SE3 ops produce it) and for the one
-returned.  Gradients are returned for poses, disps, targets, weights, eta and
+returned.  Sim3 plans (group="sim3", poses (N, 8) [t q s]) use the same rule with the
+tangent [tau phi sigma] in columns 0..6 and column 7 zero.  Gradients are returned for poses, disps, targets, weights, eta and
 disps_sens; not for intrinsics, ii, jj or depth_active.
 """
 
@@ -56,11 +57,12 @@ class _BundleAdjust(torch.autograd.Function):
         plan = ctx.plan
         iterations, lm, ep, alpha = ctx.cfg
         dev = tape_p.device
-        gp = torch.zeros(plan.total_frames, 7, dtype=torch.float32, device=dev)
+        D = plan.dof
+        gp = torch.zeros(plan.total_frames, D + 1, dtype=torch.float32, device=dev)
         gd = torch.zeros(plan.total_frames, plan.ht, plan.wd, dtype=torch.float32, device=dev)
         if g_poses is not None:
             gp.copy_(g_poses)
-            gp[:, 6] = 0.0
+            gp[:, D] = 0.0
         if g_disps is not None:
             gd.copy_(g_disps)
         gt = torch.empty_like(targets)

@@ -395,54 +395,6 @@ struct LinOf<7> {
     using T = PixelLin7;
 };
 
-struct EdgeTf {
-    float t[3], q[4], s;
-};
-
-template <int D>
-__device__ __forceinline__ void edge_tf(const float* poses, int a, int b, EdgeTf& T) {
-    if (D == 6) {
-        edge_pose(poses, a, b, T.t, T.q);
-        T.s = 1.f;
-    } else if (a == b) {
-        T.t[0] = -0.1f; T.t[1] = 0.f; T.t[2] = 0.f;
-        T.q[0] = 0.f; T.q[1] = 0.f; T.q[2] = 0.f; T.q[3] = 1.f;
-        T.s = 1.f;
-    } else {
-        float pi[8], pj[8];
-#pragma unroll
-        for (int n = 0; n < 8; n++) {
-            pi[n] = __ldg(poses + 8 * a + n);
-            pj[n] = __ldg(poses + 8 * b + n);
-        }
-        const lie::Sim3<float> G = lie::Sim3<float>::load(pj) * lie::Sim3<float>::load(pi).inv();
-        T.t[0] = G.t[0]; T.t[1] = G.t[1]; T.t[2] = G.t[2];
-        T.q[0] = G.r.q.x; T.q[1] = G.r.q.y; T.q[2] = G.r.q.z; T.q[3] = G.r.q.w;
-        T.s = G.r.s;
-    }
-}
-
-// y = Ad(Tij) x for a tangent x of the source pose: the source-pose Jacobian rows
-// are -Ad^T(Tij) times the target-pose rows, so Ji . x = -Jj . (Ad x).
-//   SE3:  Ad = [[R, [t]x R], [0, R]];   Sim3: Ad = [[s R, [t]x R, -t], [0, R, 0], [0, 0, 1]]
-template <int D>
-__device__ __forceinline__ void edge_ad_apply(const EdgeTf& T, const float* x, float* y) {
-    float rt[3], rp[3];
-    qrot(T.q, x, rt);
-    qrot(T.q, x + 3, rp);
-    y[0] = T.s * rt[0] + (T.t[1] * rp[2] - T.t[2] * rp[1]);
-    y[1] = T.s * rt[1] + (T.t[2] * rp[0] - T.t[0] * rp[2]);
-    y[2] = T.s * rt[2] + (T.t[0] * rp[1] - T.t[1] * rp[0]);
-    y[3] = rp[0];
-    y[4] = rp[1];
-    y[5] = rp[2];
-    if constexpr (D == 7) {
-        y[0] -= T.t[0] * x[6];
-        y[1] -= T.t[1] * x[6];
-        y[2] -= T.t[2] * x[6];
-        y[6] = x[6];
-    }
-}
 
 template <bool kResidual>
 __device__ __forceinline__ void linearize_sim3(const EdgeTf& T, bool stereo, float fx, float fy, float cx, float cy,
@@ -2913,10 +2865,6 @@ extern "C" int vipe_slam_ba_batch_plan_create(int num_graphs, const int* num_fra
         return VIPE_ERR_GROUP;
     }
     const int dof = group_id == 4 ? 7 : 6;
-    if (with_adjoint && dof != 6) {
-        set_last_error("batched BA: the adjoint is implemented for SE3 graphs");
-        return VIPE_ERR_GROUP;
-    }
     long sumE = 0, sumK = 0;
     for (int g = 0; g < num_graphs; g++) {
         int rc = check_dims(num_frames[g], ht, wd, num_edges[g], num_kx[g], t0[g], t1[g]);

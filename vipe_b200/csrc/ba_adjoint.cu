@@ -56,8 +56,24 @@ __device__ __forceinline__ void cross3(const double* a, const double* b, double*
     c[2] = a[0] * b[1] - a[1] * b[0];
 }
 
-// v <- ad(xi)^T v for xi = (tau, phi): (-phi x v_tau, -tau x v_tau - phi x v_phi)
+// v <- ad(xi)^T v.  SE3, xi = (tau, phi): (-phi x v_tau, -tau x v_tau - phi x v_phi).
+// Sim3, xi = (tau, phi, sigma), ad(xi) = [[phi x + sigma I, tau x, -tau], [0, phi x, 0], [0, 0, 0]]:
+// (-phi x v_tau + sigma v_tau, -tau x v_tau - phi x v_phi, -tau . v_tau).
+template <int D>
 __device__ __forceinline__ void adT_apply(const double* xi, double* v) {
+    if constexpr (D == 7) {
+        const double vs = -(xi[0] * v[0] + xi[1] * v[1] + xi[2] * v[2]);
+        double a[3], b[3], c[3];
+        cross3(xi + 3, v, a);
+        cross3(xi, v, b);
+        cross3(xi + 3, v + 3, c);
+        for (int n = 0; n < 3; n++) {
+            v[3 + n] = -b[n] - c[n];
+            v[n] = -a[n] + xi[6] * v[n];
+        }
+        v[6] = vs;
+        return;
+    }
     double a[3], b[3], c[3];
     cross3(xi + 3, v, a);
     cross3(xi, v, b);
@@ -124,16 +140,25 @@ __device__ __forceinline__ void quat_to_rot(const double* q, double* R) {
     R[8] = 1 - 2 * (x * x + y * y);
 }
 
-// Tij = Tj Ti^-1 as a 4x4 (stereo edges: the fixed baseline (-0.1, 0, 0))
+// Tij = Tj Ti^-1 as a 4x4 [s R | t] (SE3: s = 1; stereo edges: the fixed baseline (-0.1, 0, 0))
+template <int D>
 __device__ M4 edge_matrix(const float* poses, int a, int b) {
-    float tij[3], qij[4];
-    edge_pose(poses, a, b, tij, qij);
+    float tij[3], qij[4], sij = 1.f;
+    if constexpr (D == 6) {
+        edge_pose(poses, a, b, tij, qij);
+    } else {
+        EdgeTf T;
+        edge_tf<7>(poses, a, b, T);
+        for (int n = 0; n < 3; n++) tij[n] = T.t[n];
+        for (int n = 0; n < 4; n++) qij[n] = T.q[n];
+        sij = T.s;
+    }
     const double q[4] = {qij[0], qij[1], qij[2], qij[3]};
     double R[9];
     quat_to_rot(q, R);
     M4 T;
     for (int r = 0; r < 3; r++) {
-        for (int c = 0; c < 3; c++) T.m[4 * r + c] = R[3 * r + c];
+        for (int c = 0; c < 3; c++) T.m[4 * r + c] = (D == 6) ? R[3 * r + c] : (double)sij * R[3 * r + c];
         T.m[4 * r + 3] = tij[r];
     }
     T.m[12] = T.m[13] = T.m[14] = 0.0;
@@ -141,16 +166,39 @@ __device__ M4 edge_matrix(const float* poses, int a, int b) {
     return T;
 }
 
-// the edge's 12-vector [source pose, target pose] of a window-pose field (zero
+// the edge's 2D-vector [source pose, target pose] of a window-pose field (zero
 // for poses outside the window; drop_t0 also zeroes pose t0)
-template <typename Tin>
+template <int D, typename Tin>
 __device__ __forceinline__ void edge_dir(const Tin* field, int ia, int ib, int t0, int P, bool drop_t0, double* v) {
-    for (int n = 0; n < 12; n++) v[n] = 0.0;
+    for (int n = 0; n < 2 * D; n++) v[n] = 0.0;
     const int la = ia - t0, lb = ib - t0;
     if (la >= 0 && la < P && !(drop_t0 && la == 0))
-        for (int n = 0; n < 6; n++) v[n] = (double)field[6 * la + n];
+        for (int n = 0; n < D; n++) v[n] = (double)field[D * la + n];
     if (lb >= 0 && lb < P && !(drop_t0 && lb == 0))
-        for (int n = 0; n < 6; n++) v[6 + n] = (double)field[6 * lb + n];
+        for (int n = 0; n < D; n++) v[D + n] = (double)field[D * lb + n];
+}
+
+// y = Ad(Tij) x in FP64 from the edge's 4x4 [s R | t] (s recovered as |column 0|):
+// SE3 [[R, [t]x R], [0, R]];  Sim3 [[s R, [t]x R, -t], [0, R, 0], [0, 0, 1]]
+template <int D>
+__device__ __forceinline__ void ad_apply_m4(const M4& T, const double* x, double* y) {
+    const double s = (D == 6) ? 1.0 : sqrt(T.m[0] * T.m[0] + T.m[4] * T.m[4] + T.m[8] * T.m[8]);
+    double rt[3], rp[3];
+    for (int r = 0; r < 3; r++) {
+        rt[r] = T.m[4 * r] * x[0] + T.m[4 * r + 1] * x[1] + T.m[4 * r + 2] * x[2];  // s R x_tau
+        rp[r] = (T.m[4 * r] * x[3] + T.m[4 * r + 1] * x[4] + T.m[4 * r + 2] * x[5]) / s;  // R x_phi
+    }
+    const double t[3] = {T.m[3], T.m[7], T.m[11]};
+    double tx[3];
+    cross3(t, rp, tx);
+    for (int r = 0; r < 3; r++) {
+        y[r] = rt[r] + tx[r];
+        y[3 + r] = rp[r];
+    }
+    if constexpr (D == 7) {
+        for (int r = 0; r < 3; r++) y[r] -= t[r] * x[6];
+        y[6] = x[6];
+    }
 }
 
 // row r of the 3x4 matrix M times X = (x, y, 1, d)
@@ -160,40 +208,44 @@ __device__ __forceinline__ float mrow(const float* M, int r, const float* X) {
 
 // ---------------------------------------------------------------- kernels
 
-// gT <- incoming pose gradients (left tangent, lietorch layout (N, 7), [6] unused)
+// gT <- incoming pose gradients (left tangent, lietorch layout: SE3 (N, 7) with [6] unused,
+// Sim3 (N, 8) with [7] unused)
 __global__ void ba_adj_init_kernel(BAPtrs base, Batch B) {
     BA_BIND(B, base);
-    for (int q = threadIdx.x; q < d.N * 6; q += blockDim.x) w.adj_gT[q] = (double)io.g_poses[(q / 6) * 7 + q % 6];
+    const int D = d.dof;
+    for (int q = threadIdx.x; q < d.N * D; q += blockDim.x)
+        w.adj_gT[q] = (double)io.g_poses[(q / D) * (D + 1) + q % D];
 }
 
 // retraction T' = Exp(dxi) T:  g_dxi = J_l(dxi)^T g_T',  g_T = Ad(Exp dxi)^T g_T'
 // with J_l = sum ad^n/(n+1)!, Ad(Exp) = sum ad^n/n! (series in FP64).
+template <int D>
 __global__ void ba_adj_prep_kernel(BAPtrs base, Batch B) {
     BA_BIND(B, base);
     if (w.status[0]) return;
     for (int a = threadIdx.x; a < d.P; a += blockDim.x) {
-        double xi[6], term[6], adacc[6], jl[6];
-        for (int n = 0; n < 6; n++) xi[n] = (double)io.dx[6 * a + n];
-        double* g = w.adj_gT + (size_t)(d.t0 + a) * 6;
-        for (int n = 0; n < 6; n++) {
+        double xi[D], term[D], adacc[D], jl[D];
+        for (int n = 0; n < D; n++) xi[n] = (double)io.dx[D * a + n];
+        double* g = w.adj_gT + (size_t)(d.t0 + a) * D;
+        for (int n = 0; n < D; n++) {
             term[n] = g[n];
             adacc[n] = g[n];
             jl[n] = g[n];
         }
         double c = 1.0;  // 1/k!
         for (int k = 1; k <= 30; k++) {
-            adT_apply(xi, term);
+            adT_apply<D>(xi, term);
             c /= k;
             double mx = 0.0;
-            for (int n = 0; n < 6; n++) {
+            for (int n = 0; n < D; n++) {
                 adacc[n] += c * term[n];
                 jl[n] += c / (k + 1) * term[n];
                 mx = fmax(mx, fabs(term[n]));
             }
             if (mx * c < 1e-30) break;
         }
-        for (int n = 0; n < 6; n++) {
-            w.adj_rhs[6 * a + n] = jl[n];
+        for (int n = 0; n < D; n++) {
+            w.adj_rhs[D * a + n] = jl[n];
             g[n] = adacc[n];
         }
     }
@@ -204,6 +256,53 @@ __global__ void ba_adj_prep_kernel(BAPtrs base, Batch B) {
 // them, and stored for ba_adj_frame_b_kernel), then for each edge leaving the
 // frame the 12 sums  sum_p a_p act wd_c Jz_c [Ji_c, Jj_c],  a_p = Q_p g_d(p).
 // 6 CTAs per SM (40 registers): latency-bound, 8.3 vs 9.0 ms per 256-clip step at 4
+// Sim3 target-pose rows of one pixel (tau: d grad f, phi: P x grad f, sigma: grad f . P) with
+// the forward's mask and weight scale: acc += a act wd Jz Jj per channel
+__device__ __forceinline__ void sim3_target_sums(const EdgeTf& T, float fx, float fy, float cx, float cy, float u,
+                                                 float v, float disp, float w0, float w1, float act, float a,
+                                                 float* acc) {
+    const float X3[3] = {(u - cx) / fx, (v - cy) / fy, 1.0f};
+    float RX[3];
+    qrot(T.q, X3, RX);
+    const float P[3] = {T.s * RX[0] + T.t[0] * disp, T.s * RX[1] + T.t[1] * disp, T.s * RX[2] + T.t[2] * disp};
+    if (P[2] < 0.25f) return;
+    const float iz = 1.0f / P[2];
+    const float wc[2] = {0.001f * w0, 0.001f * w1};
+#pragma unroll
+    for (int ch = 0; ch < 2; ch++) {
+        const float g[3] = {ch == 0 ? fx * iz : 0.f, ch == 0 ? 0.f : fy * iz,
+                            ch == 0 ? -fx * P[0] * iz * iz : -fy * P[1] * iz * iz};
+        const float jz = g[0] * T.t[0] + g[1] * T.t[1] + g[2] * T.t[2];
+        const float c = a * act * (wc[ch] * act) * jz;
+        acc[0] += c * disp * g[0];
+        acc[1] += c * disp * g[1];
+        acc[2] += c * disp * g[2];
+        acc[3] += c * (P[1] * g[2] - P[2] * g[1]);
+        acc[4] += c * (P[2] * g[0] - P[0] * g[2]);
+        acc[5] += c * (P[0] * g[1] - P[1] * g[0]);
+        acc[6] += c * (g[0] * P[0] + g[1] * P[1] + g[2] * P[2]);
+    }
+}
+
+// o = Ad(Tij)^T y (a target-pose row pulled back to the source pose, up to sign):
+// SE3 (R^T y_tau, R^T (y_phi + y_tau x t)); Sim3 adds s to the first and -t . y_tau + y_sigma
+template <int D>
+__device__ __forceinline__ void adT_tf(const EdgeTf& T, const float* y, float* o) {
+    const float qc[4] = {-T.q[0], -T.q[1], -T.q[2], T.q[3]};
+    const float yt[3] = {y[0], y[1], y[2]};
+    const float u[3] = {y[3] + (y[1] * T.t[2] - y[2] * T.t[1]), y[4] + (y[2] * T.t[0] - y[0] * T.t[2]),
+                        y[5] + (y[0] * T.t[1] - y[1] * T.t[0])};
+    qrot(qc, yt, o);
+    qrot(qc, u, o + 3);
+    if constexpr (D == 7) {
+        o[0] *= T.s;
+        o[1] *= T.s;
+        o[2] *= T.s;
+        o[6] = y[6] - (T.t[0] * y[0] + T.t[1] * y[1] + T.t[2] * y[2]);
+    }
+}
+
+template <int D>
 __global__ void __launch_bounds__(kAdjThreads, 6) ba_adj_frame_a_kernel(BAPtrs base, Batch B, float alpha) {
     BA_BIND(B, base);
     if (w.status[0]) return;
@@ -234,48 +333,52 @@ __global__ void __launch_bounds__(kAdjThreads, 6) ba_adj_frame_a_kernel(BAPtrs b
     for (int q = eb; q < ee; q++) {
         const int e = w.fe_list[q];
         const int b = (int)io.jj[e];
-        float tij[3], qij[4];
-        edge_pose(io.poses, k, b, tij, qij);
+        EdgeTf Tf;
+        edge_tf<D>(io.poses, k, b, Tf);
         // source rows are -Ad^T(Tij) of the target rows, so only the target-pose sums
         // are accumulated per pixel; the source half follows once per edge
-        float acc[6];
+        float acc[D];
 #pragma unroll
-        for (int n = 0; n < 6; n++) acc[n] = 0.f;
+        for (int n = 0; n < D; n++) acc[n] = 0.f;
         if (act != 0.f) {
             const float* wp = io.weights + (size_t)e * 2 * HW;
             for (int p = p0 + tid; p < p1; p += kAdjThreads) {
                 const float u = (float)(p % W), v = (float)(p / W);
                 const float disp = io.disps[(size_t)k * HW + p];
                 const float a = pa[p - p0];
-                PixelLin L;
-                linearize<false, false>(tij, qij, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p),
-                                        __ldg(wp + HW + p), 0.f, 0.f, act, 1.f, L);
+                if constexpr (D == 6) {
+                    PixelLin L;
+                    linearize<false, false>(Tf.t, Tf.q, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p),
+                                            __ldg(wp + HW + p), 0.f, 0.f, act, 1.f, L);
 #pragma unroll
-                for (int ch = 0; ch < 2; ch++) {
-                    const float g = a * act * L.wd[ch] * L.Jz[ch];
+                    for (int ch = 0; ch < 2; ch++) {
+                        const float g = a * act * L.wd[ch] * L.Jz[ch];
 #pragma unroll
-                    for (int n = 0; n < 6; n++) acc[n] += g * L.Jj[ch][n];
+                        for (int n = 0; n < 6; n++) acc[n] += g * L.Jj[ch][n];
+                    }
+                } else {
+                    sim3_target_sums(Tf, fx, fy, cx, cy, u, v, disp, __ldg(wp + p), __ldg(wp + HW + p), act, a, acc);
                 }
             }
         }
 #pragma unroll
-        for (int n = 0; n < 6; n++) {
+        for (int n = 0; n < D; n++) {
             const float sv = warp_sum(acc[n]);
             if (lane == 0) red[warp][n] = sv;
         }
         __syncthreads();
         if (tid == 0) {
-            float sj[6], si[6];
-            for (int n = 0; n < 6; n++) {
+            float sj[D], si[D];
+            for (int n = 0; n < D; n++) {
                 float sv = 0.f;
                 for (int r = 0; r < kAdjThreads / 32; r++) sv += red[r][n];
                 sj[n] = sv;
             }
-            adj_t(tij, qij, sj, si);
-            float* o = w.adj_aslot + ((size_t)e * d.CF + c) * 12;
-            for (int n = 0; n < 6; n++) {
+            adT_tf<D>(Tf, sj, si);
+            float* o = w.adj_aslot + ((size_t)e * d.CF + c) * 2 * D;
+            for (int n = 0; n < D; n++) {
                 o[n] = -si[n];
-                o[6 + n] = sj[n];
+                o[D + n] = sj[n];
             }
         }
         __syncthreads();
@@ -286,17 +389,18 @@ __global__ void __launch_bounds__(kAdjThreads, 6) ba_adj_frame_a_kernel(BAPtrs b
 __global__ void ba_adj_rhs_kernel(BAPtrs base, Batch B) {
     BA_BIND(B, base);
     if (w.status[0]) return;
-    for (int q = threadIdx.x; q < 6 * d.P; q += blockDim.x) {
-        const int a = q / 6, n = q % 6;
+    const int D = d.dof;
+    for (int q = threadIdx.x; q < D * d.P; q += blockDim.x) {
+        const int a = q / D, n = q % D;
         if (a == 0) continue;
         double sub = 0.0;
         for (int r = w.pe_ptr[a]; r < w.pe_ptr[a + 1]; r++) {
             const int ent = w.pe_list[r];
             const int e = ent >> 2, fl = ent & 3;
             for (int c = 0; c < d.CF; c++) {
-                const float* src = w.adj_aslot + ((size_t)e * d.CF + c) * 12;
+                const float* src = w.adj_aslot + ((size_t)e * d.CF + c) * 2 * D;
                 if (fl & 1) sub += (double)src[n];
-                if (fl & 2) sub += (double)src[6 + n];
+                if (fl & 2) sub += (double)src[D + n];
             }
         }
         w.adj_rhs[q] -= sub;
@@ -304,19 +408,21 @@ __global__ void ba_adj_rhs_kernel(BAPtrs base, Batch B) {
 }
 
 // Jacobian rows of one pixel of one edge from the edge's 3x4 transform M0 =
-// [R | t] (same values as the reference formulas, geom_kernels.cu:338-350):
-//   target pose:  tau_n: grad f . e_n W        phi_n: e_n . (P x grad f)
-//   source pose:  tau_n: -W (R^T grad f)_n     phi_n: -e_n . (X3 x R^T grad f)
-// with P = M0 X, W = d, grad f the projection gradient on P.
+// [s R | t] (SE3: s = 1; same values as the reference formulas, geom_kernels.cu:338-350):
+//   target pose:  tau_n: grad f . e_n W        phi_n: e_n . (P x grad f)     (Sim3 sigma: grad f . P)
+//   source pose:  tau_n: -W (M^T grad f)_n     phi_n: -e_n . (X3 x M^T grad f) (Sim3 sigma: -X3 . M^T grad f)
+// with P = M0 X, W = d, grad f the projection gradient on P, M the 3x3 part of M0.
+template <int D>
 struct PixJ {
     float P[3];
     float iz;
     float gf[2][3];
-    float J[2][12];  // [source 6 | target 6] per channel
+    float J[2][2 * D];  // [source D | target D] per channel
     float jz[2];
 };
 
-__device__ __forceinline__ bool pix_jac(const float* M0, const float* X, float fx, float fy, PixJ& o) {
+template <int D>
+__device__ __forceinline__ bool pix_jac(const float* M0, const float* X, float fx, float fy, PixJ<D>& o) {
 #pragma unroll
     for (int r = 0; r < 3; r++) o.P[r] = mrow(M0, r, X);
     if (o.P[2] < 0.25f) return false;  // the forward's MIN_DEPTH mask
@@ -328,21 +434,26 @@ __device__ __forceinline__ bool pix_jac(const float* M0, const float* X, float f
 #pragma unroll
     for (int ch = 0; ch < 2; ch++) {
         const float* g = o.gf[ch];
-        float rg[3];  // R^T grad f
+        float rg[3];  // M^T grad f
 #pragma unroll
         for (int n = 0; n < 3; n++) rg[n] = M0[n] * g[0] + M0[4 + n] * g[1] + M0[8 + n] * g[2];
-        o.J[ch][0] = -W * rg[0];
-        o.J[ch][1] = -W * rg[1];
-        o.J[ch][2] = -W * rg[2];
-        o.J[ch][3] = -(X[1] * rg[2] - 1.f * rg[1]);
-        o.J[ch][4] = -(1.f * rg[0] - X[0] * rg[2]);
-        o.J[ch][5] = -(X[0] * rg[1] - X[1] * rg[0]);
-        o.J[ch][6] = g[0] * W;
-        o.J[ch][7] = g[1] * W;
-        o.J[ch][8] = g[2] * W;
-        o.J[ch][9] = o.P[1] * g[2] - o.P[2] * g[1];
-        o.J[ch][10] = o.P[2] * g[0] - o.P[0] * g[2];
-        o.J[ch][11] = o.P[0] * g[1] - o.P[1] * g[0];
+        float* J = o.J[ch];
+        J[0] = -W * rg[0];
+        J[1] = -W * rg[1];
+        J[2] = -W * rg[2];
+        J[3] = -(X[1] * rg[2] - 1.f * rg[1]);
+        J[4] = -(1.f * rg[0] - X[0] * rg[2]);
+        J[5] = -(X[0] * rg[1] - X[1] * rg[0]);
+        J[D + 0] = g[0] * W;
+        J[D + 1] = g[1] * W;
+        J[D + 2] = g[2] * W;
+        J[D + 3] = o.P[1] * g[2] - o.P[2] * g[1];
+        J[D + 4] = o.P[2] * g[0] - o.P[0] * g[2];
+        J[D + 5] = o.P[0] * g[1] - o.P[1] * g[0];
+        if constexpr (D == 7) {
+            J[6] = -(X[0] * rg[0] + X[1] * rg[1] + rg[2]);
+            J[13] = g[0] * o.P[0] + g[1] * o.P[1] + g[2] * o.P[2];
+        }
         o.jz[ch] = g[0] * M0[3] + g[1] * M0[7] + g[2] * M0[11];
     }
     return true;
@@ -354,12 +465,13 @@ __device__ __forceinline__ void cross3f(const float* a, const float* b, float* c
     c[2] = a[0] * b[1] - a[1] * b[0];
 }
 
-// One tangent direction v = [v_i | v_j] (12) at one pixel: Y = R (v_i,tau W + v_i,phi x X3),
-// Pt = M^t_v X = v_j,tau W + v_j,phi x P - Y, and dPt/dW.
+// One tangent direction v = [v_i | v_j] (2D) at one pixel: z = v_i,tau W + v_i,phi x X3 (+ v_i,sigma X3),
+// Y = M z, Pt = M^t_v X = v_j,tau W + v_j,phi x P (+ v_j,sigma P) - Y, and dPt/dW.
 struct DirPix {
     float Y[3], Pt[3], dPt[3];
 };
 
+template <int D>
 __device__ __forceinline__ void dir_pix(const float* M0, const float* X, const float* P, const float* v, DirPix& o) {
     const float W = X[3];
     float z[3], c[3];
@@ -367,44 +479,64 @@ __device__ __forceinline__ void dir_pix(const float* M0, const float* X, const f
     cross3f(v + 3, X3, c);
 #pragma unroll
     for (int n = 0; n < 3; n++) z[n] = v[n] * W + c[n];
+    if constexpr (D == 7) {
+#pragma unroll
+        for (int n = 0; n < 3; n++) z[n] += v[6] * X3[n];
+    }
 #pragma unroll
     for (int r = 0; r < 3; r++) o.Y[r] = M0[4 * r] * z[0] + M0[4 * r + 1] * z[1] + M0[4 * r + 2] * z[2];
+    const float* vj = v + D;
     float cp[3];
-    cross3f(v + 9, P, cp);
+    cross3f(vj + 3, P, cp);
 #pragma unroll
-    for (int r = 0; r < 3; r++) o.Pt[r] = v[6 + r] * W + cp[r] - o.Y[r];
-    // d/dW: v_j,tau + v_j,phi x t - R v_i,tau
+    for (int r = 0; r < 3; r++) o.Pt[r] = vj[r] * W + cp[r] - o.Y[r];
+    // d/dW: v_j,tau + v_j,phi x t (+ v_j,sigma t) - M v_i,tau
     const float t[3] = {M0[3], M0[7], M0[11]};
     float ct[3];
-    cross3f(v + 9, t, ct);
+    cross3f(vj + 3, t, ct);
 #pragma unroll
     for (int r = 0; r < 3; r++)
-        o.dPt[r] = v[6 + r] + ct[r] - (M0[4 * r] * v[0] + M0[4 * r + 1] * v[1] + M0[4 * r + 2] * v[2]);
+        o.dPt[r] = vj[r] + ct[r] - (M0[4 * r] * v[0] + M0[4 * r + 1] * v[1] + M0[4 * r + 2] * v[2]);
+    if constexpr (D == 7) {
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            o.Pt[r] += vj[6] * P[r];
+            o.dPt[r] += vj[6] * t[r];
+        }
+    }
 }
 
 // Mixed second derivative along direction v with coefficient cd, channel ch:
 //   f^{s v}_c = grad f . (M^{sv}_k X) + Ps_k . h,  h = (-f iz^2 Zt, 0, f iz^2 Xt - 2 iz f^v)  (u; v: rows 1, 2)
-// and, for pose directions k, grad f . (M^{sv}_k X) = Ps_k . (grad f x v_j,phi)
-// + e_k,phi . [target: -(Y x grad f); source: R^T (Y x grad f)].
+// and, for pose directions k, grad f . (M^{sv}_k X) = Ps_k . (grad f x v_j,phi + v_j,sigma grad f)
+// + e_k,phi . [target: -(Y x grad f); source: R^T (Y x grad f)]
+// + e_k,sigma [target: -Y . grad f; source: Y . grad f]  (Sim3).
 // Adds to g0h (Ps coefficient valid for every s-direction), g0x (pose-only Ps
-// coefficient), om (rotation-dof vector) and returns the depth s-direction value
-// grad f . dPt/dW (the h part for depth is g0h . t, added by the caller).
-__device__ __forceinline__ float mixed(const PixJ& J, int ch, float fxy, const float* v, const DirPix& D, float fv,
-                                       float cd, float* g0h, float* g0x, float* om) {
+// coefficient), om (rotation-dof vector), os (scale-dof scalar) and returns the depth
+// s-direction value grad f . dPt/dW (the h part for depth is g0h . t, added by the caller).
+template <int D>
+__device__ __forceinline__ float mixed(const PixJ<D>& J, int ch, float fxy, const float* v, const DirPix& Dp, float fv,
+                                       float cd, float* g0h, float* g0x, float* om, float* os) {
     const float* g = J.gf[ch];
     const float iz = J.iz, iz2 = iz * iz;
-    g0h[ch] += cd * (-fxy * iz2 * D.Pt[2]);
-    g0h[2] += cd * (fxy * iz2 * D.Pt[ch] - 2.f * iz * fv);
+    g0h[ch] += cd * (-fxy * iz2 * Dp.Pt[2]);
+    g0h[2] += cd * (fxy * iz2 * Dp.Pt[ch] - 2.f * iz * fv);
     float gx[3];
-    cross3f(g, v + 9, gx);
+    cross3f(g, v + D + 3, gx);
     float yg[3];
-    cross3f(D.Y, g, yg);
+    cross3f(Dp.Y, g, yg);
 #pragma unroll
     for (int r = 0; r < 3; r++) {
         g0x[r] += cd * gx[r];
         om[r] += cd * yg[r];
     }
-    return cd * (g[0] * D.dPt[0] + g[1] * D.dPt[1] + g[2] * D.dPt[2]);
+    if constexpr (D == 7) {
+        const float sj = v[13];
+#pragma unroll
+        for (int r = 0; r < 3; r++) g0x[r] += cd * sj * g[r];
+        *os += cd * (Dp.Y[0] * g[0] + Dp.Y[1] * g[1] + Dp.Y[2] * g[2]);
+    }
+    return cd * (g[0] * Dp.dPt[0] + g[1] * Dp.dPt[1] + g[2] * Dp.dPt[2]);
 }
 
 // n consecutive per-edge constants (16-byte aligned shared memory) into registers
@@ -429,19 +561,31 @@ __device__ __forceinline__ int opaque_zero() {
     return z;
 }
 
-constexpr int kPixF = 14;   // per-pixel floats kept in shared memory by ba_adj_frame_b_kernel
-constexpr int kEdgeF = 80;  // per-edge floats: M0, directions x3, damping weights, the directions in target form
-                            // (78 used; rows stay 16-byte aligned for vector reads)
+// per-pixel floats kept in shared memory by ba_adj_frame_b_kernel: a, dzf, mu, gwz, gC, gd, disp, Q, Es[D]
+__host__ __device__ constexpr int kPixF(int D) { return 8 + D; }
+// per-edge floats: M0 [0, 12), the directions lam, dxi, dxi~ (2D each) from kOffDir, the damping
+// weights lm lam dxi of the edge's two poses (2D) at kOffDmp, the three directions in target form
+// (D each) from kOffTf; rows padded to 16 bytes for vector reads (SE3 78 used of 80, Sim3 89 of 92)
+// (every 2D block starts on a 16-byte boundary: SE3 M0 | 3 x 12 | 12 | 3 x 6 in 80 floats, Sim3
+// M0 | 3 x 16 | 16 | 3 x 7 in 100)
+__host__ __device__ constexpr int kStride2(int D) { return (2 * D + 3) / 4 * 4; }
+__host__ __device__ constexpr int kOffDir(int D) { return 12; }
+__host__ __device__ constexpr int kOffDmp(int D) { return 12 + 3 * kStride2(D); }
+__host__ __device__ constexpr int kOffTf(int D) { return kOffDmp(D) + kStride2(D); }
+__host__ __device__ constexpr int kEdgeF(int D) { return (kOffTf(D) + 3 * D + 3) / 4 * 4; }
+__host__ __device__ constexpr int kMom(int D) { return D == 7 ? 16 : 15; }  // G0, om (, os)
 
 // per (depth frame, pixel chunk): the per-pixel adjoint quantities, then the
 // gradient of phi (with the exact derivative of the LM damping) for every edge
-// leaving the frame.  Dynamic shared memory: kPixF floats per pixel.
+// leaving the frame.  Dynamic shared memory: kPixF(D) floats per pixel.
+template <int D>
 __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs base, Batch B, float alpha, float lm,
                                                                           int first) {
+    constexpr int D2 = 2 * D, S2 = kStride2(D), OD = kOffDir(D), OM = kOffDmp(D), OT = kOffTf(D), NM = kMom(D);
     BA_BIND(B, base);
     if (w.status[0]) return;
-    extern __shared__ float pix[];  // [kPixF][chunk]: a, dzf, mu, gwz, gC, gd, disp, Q, Es[6]
-    __shared__ __align__(16) float Esh[kAdjMaxDeg][kEdgeF];
+    extern __shared__ float pix[];  // [kPixF(D)][chunk]: a, dzf, mu, gwz, gC, gd, disp, Q, Es[D]
+    __shared__ __align__(16) float Esh[kAdjMaxDeg][kEdgeF(D)];
     __shared__ int grp[kAdjMaxDeg];  // -1: unique target; else index of the first edge with the same target
     __shared__ float red[kAdjThreads / 32][16];
     __shared__ int any_dup;
@@ -467,11 +611,10 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
     float* pgd = pix + 5 * CH;
     float* pdisp = pix + 6 * CH;
     float* pQ = pix + 7 * CH;
-    float* pEs = pix + 8 * CH;  // 6 x CH: the frame's own-pose slot of E at each pixel
+    float* pEs = pix + 8 * CH;  // D x CH: the frame's own-pose slot of E at each pixel
     const bool self_in = k >= t0 && k < t0 + P;
 
-    // per-edge data: [0,12) M0 = Tij[0:3], [12,48) the directions lam, dxi, dxi~ (12 each),
-    // [48,60) damping weights lm lam dxi of the edge's two poses
+    // per-edge data (offsets above)
     if (tid == 0) any_dup = 0;
     __syncthreads();
     for (int q = warp; q < deg; q += kAdjThreads / 32) {
@@ -479,43 +622,33 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
         const int b = (int)io.jj[e];
         float* Eq = Esh[q];
         if (lane < 3) {
-            const M4 T = edge_matrix(io.poses, k, b);
+            const M4 T = edge_matrix<D>(io.poses, k, b);
             for (int col = 0; col < 4; col++) Eq[4 * lane + col] = (float)T.m[4 * lane + col];
         } else if (lane < 6) {
             const int dir = lane - 3;
-            double v[12];
+            double v[D2];
             if (dir == 0)
-                edge_dir(w.adj_lam, k, b, t0, P, false, v);
+                edge_dir<D>(w.adj_lam, k, b, t0, P, false, v);
             else
-                edge_dir(io.dx, k, b, t0, P, dir == 2, v);
-            for (int n = 0; n < 12; n++) Eq[12 + 12 * dir + n] = (float)v[n];
+                edge_dir<D>(io.dx, k, b, t0, P, dir == 2, v);
+            for (int n = 0; n < D2; n++) Eq[OD + S2 * dir + n] = (float)v[n];
         } else if (lane == 6) {
-            double vl[12], vd[12];
-            edge_dir(w.adj_lam, k, b, t0, P, false, vl);
-            edge_dir(io.dx, k, b, t0, P, false, vd);
-            for (int n = 0; n < 12; n++) Eq[48 + n] = (float)((double)lm * vl[n] * vd[n]);
+            double vl[D2], vd[D2];
+            edge_dir<D>(w.adj_lam, k, b, t0, P, false, vl);
+            edge_dir<D>(io.dx, k, b, t0, P, false, vd);
+            for (int n = 0; n < D2; n++) Eq[OM + n] = (float)((double)lm * vl[n] * vd[n]);
         } else if (lane >= 8 && lane < 11) {
             // J . v = Jj . (v_j - Ad(Tij) v_i) (source rows are -Ad^T of the target rows):
-            // the three directions as one 6-vector each, Ad v_i = (R v_tau + t x R v_phi, R v_phi)
+            // the three directions as one D-vector each
             const int dir = lane - 8;
-            double v[12];
+            double v[D2], av[D];
             if (dir == 0)
-                edge_dir(w.adj_lam, k, b, t0, P, false, v);
+                edge_dir<D>(w.adj_lam, k, b, t0, P, false, v);
             else
-                edge_dir(io.dx, k, b, t0, P, dir == 2, v);
-            const M4 T = edge_matrix(io.poses, k, b);
-            double rt[3], rp[3];
-            for (int r = 0; r < 3; r++) {
-                rt[r] = T.m[4 * r] * v[0] + T.m[4 * r + 1] * v[1] + T.m[4 * r + 2] * v[2];
-                rp[r] = T.m[4 * r] * v[3] + T.m[4 * r + 1] * v[4] + T.m[4 * r + 2] * v[5];
-            }
-            const double t[3] = {T.m[3], T.m[7], T.m[11]};
-            double tx[3];
-            cross3(t, rp, tx);
-            for (int r = 0; r < 3; r++) {
-                Eq[60 + 6 * dir + r] = (float)(v[6 + r] - (rt[r] + tx[r]));
-                Eq[60 + 6 * dir + 3 + r] = (float)(v[9 + r] - rp[r]);
-            }
+                edge_dir<D>(io.dx, k, b, t0, P, dir == 2, v);
+            const M4 T = edge_matrix<D>(io.poses, k, b);
+            ad_apply_m4<D>(T, v, av);
+            for (int n = 0; n < D; n++) Eq[OT + D * dir + n] = (float)(v[D + n] - av[n]);
         } else if (lane == 7) {
             int g = -1;
             if (b != k)
@@ -538,17 +671,17 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
     // target-slot E contribution of edge q at a pixel (sum over channels)
     auto tvec = [&](int q, const float* X, int p, float* out) {
         const int e = w.fe_list[eb + q];
-        PixJ J;
+        PixJ<D> J;
 #pragma unroll
-        for (int n = 0; n < 6; n++) out[n] = 0.f;
-        if (!pix_jac(Esh[q], X, fx, fy, J)) return;
+        for (int n = 0; n < D; n++) out[n] = 0.f;
+        if (!pix_jac<D>(Esh[q], X, fx, fy, J)) return;
         const float* wp = io.weights + (size_t)e * 2 * HW;
         const float wc[2] = {0.001f * __ldg(wp + p), 0.001f * __ldg(wp + HW + p)};
 #pragma unroll
         for (int ch = 0; ch < 2; ch++) {
             const float g = act * act * wc[ch] * J.jz[ch];
 #pragma unroll
-            for (int n = 0; n < 6; n++) out[n] += g * J.J[ch][6 + n];
+            for (int n = 0; n < D; n++) out[n] += g * J.J[ch][D + n];
         }
     };
 
@@ -559,58 +692,63 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
         const float disp = io.disps[(size_t)k * HW + p];
         const float X[4] = {(u - cx) / fx, (v - cy) / fy, 1.f, disp};
         float eD = 0.f, eDt = 0.f, eL = 0.f, dampC = 0.f;
-        float Es[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float Es[D];
+#pragma unroll
+        for (int n = 0; n < D; n++) Es[n] = 0.f;
         if (act != 0.f) {
             for (int q = 0; q < deg; q++) {
                 const int e = w.fe_list[eb + q];
                 const bool stereo = (int)io.jj[e] == k;
                 const float* Eq = Esh[q];
-                PixJ J;
-                if (!pix_jac(Eq, X, fx, fy, J)) continue;
+                PixJ<D> J;
+                if (!pix_jac<D>(Eq, X, fx, fy, J)) continue;
                 const float* wp = io.weights + (size_t)e * 2 * HW;
                 const float wc[2] = {0.001f * __ldg(wp + p), 0.001f * __ldg(wp + HW + p)};
-                float tv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                float tv[D];
+#pragma unroll
+                for (int n = 0; n < D; n++) tv[n] = 0.f;
 #pragma unroll
                 for (int ch = 0; ch < 2; ch++) {
                     const float g = act * act * wc[ch] * J.jz[ch];
                     float jl = 0.f, jd = 0.f, jdt = 0.f;
 #pragma unroll
-                    for (int n = 0; n < 6; n++) {
-                        const float jn = J.J[ch][6 + n];
-                        jl += jn * Eq[60 + n];
-                        jd += jn * Eq[66 + n];
-                        jdt += jn * Eq[72 + n];
+                    for (int n = 0; n < D; n++) {
+                        const float jn = J.J[ch][D + n];
+                        jl += jn * Eq[OT + n];
+                        jd += jn * Eq[OT + D + n];
+                        jdt += jn * Eq[OT + 2 * D + n];
                     }
                     eL += g * jl;
                     eD += g * jd;
                     eDt += g * jdt;
 #pragma unroll
-                    for (int n = 0; n < 6; n++) {
+                    for (int n = 0; n < D; n++) {
                         Es[n] += g * J.J[ch][n];
-                        if (stereo) Es[n] += g * J.J[ch][6 + n];
-                        else tv[n] += g * J.J[ch][6 + n];
+                        if (stereo) Es[n] += g * J.J[ch][D + n];
+                        else tv[n] += g * J.J[ch][D + n];
                     }
                 }
                 if (!stereo && grp[q] < 0)
 #pragma unroll
-                    for (int n = 0; n < 6; n++) dampC += Eq[54 + n] * tv[n] * tv[n];
+                    for (int n = 0; n < D; n++) dampC += Eq[OM + D + n] * tv[n] * tv[n];
             }
             if (dup) {  // targets shared by several edges: the slot holds their sum
                 for (int q = 0; q < deg; q++) {
                     if (grp[q] != q) continue;
-                    float sum[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, tv[6];
+                    float sum[D], tv[D];
+                    for (int n = 0; n < D; n++) sum[n] = 0.f;
                     for (int q2 = q; q2 < deg; q2++)
                         if (grp[q2] == q) {
                             tvec(q2, X, p, tv);
-                            for (int n = 0; n < 6; n++) sum[n] += tv[n];
+                            for (int n = 0; n < D; n++) sum[n] += tv[n];
                         }
-                    for (int n = 0; n < 6; n++) dampC += Esh[q][54 + n] * sum[n] * sum[n];
+                    for (int n = 0; n < D; n++) dampC += Esh[q][OM + D + n] * sum[n] * sum[n];
                 }
             }
             if (self_in && deg > 0) {
                 // lm lam dxi of the frame's own pose: the source half of any edge's damping weights
 #pragma unroll
-                for (int n = 0; n < 6; n++) dampC += Esh[0][48 + n] * Es[n] * Es[n];
+                for (int n = 0; n < D; n++) dampC += Esh[0][OM + n] * Es[n] * Es[n];
             }
         }
         const float* qw = w.qwf + ((size_t)s * HW + p) * 3;
@@ -634,7 +772,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
         pdisp[i] = disp;
         pQ[i] = Q;
 #pragma unroll
-        for (int n = 0; n < 6; n++) pEs[n * CH + i] = Es[n];
+        for (int n = 0; n < D; n++) pEs[n * CH + i] = Es[n];
     }
     __syncthreads();
 
@@ -652,16 +790,16 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
         const float* wp = io.weights + (size_t)e * 2 * HW;
         float* gtp = io.g_targets + (size_t)e * 2 * HW;
         float* gwp = io.g_weights + (size_t)e * 2 * HW;
-        float mom[15];  // G0 (3x4) and the rotation-dof vector
+        float mom[NM];  // G0 (3x4), the rotation-dof vector (and the scale-dof scalar)
 #pragma unroll
-        for (int m = 0; m < 15; m++) mom[m] = 0.f;
+        for (int m = 0; m < NM; m++) mom[m] = 0.f;
         for (int i = tid; i < np_; i += kAdjThreads) {
             const float* Eqv = Esh[q] + opaque_zero();  // per-pixel re-reads, see opaque_zero
             const int p = p0 + i;
             const float u = (float)(p % W), v = (float)(p / W);
             const float X[4] = {(u - cx) / fx, (v - cy) / fy, 1.f, pdisp[i]};
-            PixJ J;
-            if (!pix_jac(Eqc, X, fx, fy, J)) {  // invalid pixel: zero weight, no gradient
+            PixJ<D> J;
+            if (!pix_jac<D>(Eqc, X, fx, fy, J)) {  // invalid pixel: zero weight, no gradient
                 if (first) {
                     gtp[p] = 0.f;
                     gtp[HW + p] = 0.f;
@@ -675,37 +813,38 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
             const float rr[2] = {__ldg(tp + p) - (fx * J.P[0] * iz + cx), __ldg(tp + HW + p) - (fy * J.P[1] * iz + cy)};
             const float wc[2] = {0.001f * __ldg(wp + p), 0.001f * __ldg(wp + HW + p)};
             // the per-pixel damping direction beta (slot E values of this edge's two poses)
-            float beta[12];
+            float beta[D2];
             {
-                float tv[6];
+                float tv[D];
                 if (!stereo) {
                     if (grp[q] < 0) {
 #pragma unroll
-                        for (int n = 0; n < 6; n++) {
+                        for (int n = 0; n < D; n++) {
                             tv[n] = 0.f;
 #pragma unroll
-                            for (int ch = 0; ch < 2; ch++) tv[n] += act * act * wc[ch] * J.jz[ch] * J.J[ch][6 + n];
+                            for (int ch = 0; ch < 2; ch++) tv[n] += act * act * wc[ch] * J.jz[ch] * J.J[ch][D + n];
                         }
                     } else {
-                        float t2[6];
-                        for (int n = 0; n < 6; n++) tv[n] = 0.f;
+                        float t2[D];
+                        for (int n = 0; n < D; n++) tv[n] = 0.f;
                         for (int q2 = grp[q]; q2 < deg; q2++)
                             if (grp[q2] == grp[q]) {
                                 tvec(q2, X, p, t2);
-                                for (int n = 0; n < 6; n++) tv[n] += t2[n];
+                                for (int n = 0; n < D; n++) tv[n] += t2[n];
                             }
                     }
                 }
-                float dmp[12];  // damping weights lm lam dxi of the edge's two poses
-                lds_row<12>(Eqv + 48, dmp);
+                float dmp[D2];  // damping weights lm lam dxi of the edge's two poses
+                lds_row<D2>(Eqv + OM, dmp);
 #pragma unroll
-                for (int n = 0; n < 6; n++) {
+                for (int n = 0; n < D; n++) {
                     const float es = pEs[n * CH + i];
                     beta[n] = 2.f * Q * dmp[n] * es;
-                    beta[6 + n] = 2.f * Q * dmp[6 + n] * (stereo ? es : tv[n]);
+                    beta[D + n] = 2.f * Q * dmp[D + n] * (stereo ? es : tv[n]);
                 }
             }
             float g0h[3] = {0.f, 0.f, 0.f}, g0x[3] = {0.f, 0.f, 0.f}, om[3] = {0.f, 0.f, 0.f}, g4[3] = {0.f, 0.f, 0.f};
+            float os = 0.f;
             float gdp = 0.f;
 #pragma unroll
             for (int ch = 0; ch < 2; ch++) {
@@ -714,21 +853,21 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                 // J . v for the edge's directions lam, dxi, dxi~, beta and the damping sum lm lam dxi J^2
                 float ft[3] = {0.f, 0.f, 0.f}, fb = 0.f, fg = 0.f;
                 {
-                    float wv[18];
-                    lds_row<18>(Eqv + 60, wv);
+                    float wv[3 * D];
+                    lds_row<3 * D>(Eqv + OT, wv);
 #pragma unroll
-                    for (int n = 0; n < 6; n++) {
-                        const float jn = J.J[ch][6 + n];
+                    for (int n = 0; n < D; n++) {
+                        const float jn = J.J[ch][D + n];
                         ft[0] += jn * wv[n];
-                        ft[1] += jn * wv[6 + n];
-                        ft[2] += jn * wv[12 + n];
+                        ft[1] += jn * wv[D + n];
+                        ft[2] += jn * wv[2 * D + n];
                     }
                 }
                 {
-                    float dmp[12];
-                    lds_row<12>(Eqv + 48, dmp);
+                    float dmp[D2];
+                    lds_row<D2>(Eqv + OM, dmp);
 #pragma unroll
-                    for (int n = 0; n < 12; n++) {
+                    for (int n = 0; n < D2; n++) {
                         const float jn = J.J[ch][n];
                         fb += jn * beta[n];
                         fg += dmp[n] * jn * jn;
@@ -760,27 +899,27 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                 g0h[ch] += c4 * (-fxy * iz2 * Eq[11]);
                 g0h[2] += c4 * (fxy * iz2 * Eq[4 * ch + 3] - 2.f * iz * fjz);
                 // every tangent direction enters linearly: one combined direction
-                float ud[12];
+                float ud[D2];
                 {
-                    float dv[12];
-                    lds_row<12>(Eqv + 48, dv);
+                    float dv[D2];
+                    lds_row<D2>(Eqv + OM, dv);
 #pragma unroll
-                    for (int n = 0; n < 12; n++) ud[n] = cE * beta[n] + cB * dv[n] * J.J[ch][n];
-                    lds_row<12>(Eqv + 12, dv);
+                    for (int n = 0; n < D2; n++) ud[n] = cE * beta[n] + cB * dv[n] * J.J[ch][n];
+                    lds_row<D2>(Eqv + OD, dv);
 #pragma unroll
-                    for (int n = 0; n < 12; n++) ud[n] += c1 * dv[n];
-                    lds_row<12>(Eqv + 24, dv);
+                    for (int n = 0; n < D2; n++) ud[n] += c1 * dv[n];
+                    lds_row<D2>(Eqv + OD + S2, dv);
 #pragma unroll
-                    for (int n = 0; n < 12; n++) ud[n] += c2 * dv[n];
-                    lds_row<12>(Eqv + 36, dv);
+                    for (int n = 0; n < D2; n++) ud[n] += c2 * dv[n];
+                    lds_row<D2>(Eqv + OD + 2 * S2, dv);
 #pragma unroll
-                    for (int n = 0; n < 12; n++) ud[n] += c3 * dv[n];
+                    for (int n = 0; n < D2; n++) ud[n] += c3 * dv[n];
                 }
                 // J . ud from the dot products above (ud is their linear combination)
                 const float fu = c1 * ft[0] + c2 * ft[1] + c3 * ft[2] + cE * fb + cB * fg;
-                DirPix D;
-                dir_pix(Eqc, X, J.P, ud, D);
-                gdp += mixed(J, ch, fxy, ud, D, fu, 1.f, g0h, g0x, om);
+                DirPix Dp;
+                dir_pix<D>(Eqc, X, J.P, ud, Dp);
+                gdp += mixed<D>(J, ch, fxy, ud, Dp, fu, 1.f, g0h, g0x, om, &os);
             }
             // depth s-direction of this pixel: Ps = t (column 3 of M0)
             gdp += g0h[0] * Eq[3] + g0h[1] * Eq[7] + g0h[2] * Eq[11];
@@ -794,14 +933,15 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                 mom[4 * r + 3] += gr * X[3] + g4[r];
                 mom[12 + r] += om[r];
             }
+            if constexpr (D == 7) mom[15] += os;
         }
 #pragma unroll
-        for (int m = 0; m < 15; m++) {
+        for (int m = 0; m < NM; m++) {
             const float sv = warp_sum(mom[m]);
             if (lane == 0) red[warp][m] = sv;
         }
         __syncthreads();
-        if (tid < 15) {
+        if (tid < NM) {
             float sv = 0.f;
             for (int r = 0; r < kAdjThreads / 32; r++) sv += red[r][tid];
             w.adj_gpart[((size_t)e * d.CF + c) * kAdjAcc + tid] = stereo ? 0.f : sv;
@@ -812,70 +952,87 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
     for (int i = tid; i < np_; i += kAdjThreads) io.g_disps[(size_t)k * HW + p0 + i] += pgd[i];
 }
 
-// per edge: the 12 pose gradients from the moments: <M^s_k, G0> plus, for the
-// rotation dofs, -om (target pose) or R^T om (source pose)
-// (k < 6: source pose i, M^s = -T hat(e_k); k >= 6: target pose j, M^s = hat(e_{k-6}) T)
+// per edge: the 2D pose gradients from the moments: <M^s_k, G0> plus, for the
+// rotation dofs, -om (target pose) or R^T om (source pose), and for the Sim3 scale dof
+// -os (target) or +os (source)
+// (k < D: source pose i, M^s = -T hat(e_k); k >= D: target pose j, M^s = hat(e_{k-D}) T,
+// hat of a Sim3 tangent [tau, phi, sigma] = [[phi x + sigma I, tau], [0, 0]])
+template <int D>
 __global__ void ba_adj_edge_reduce_kernel(BAPtrs base, Batch B) {
     BA_BIND(B, base);
     if (w.status[0]) return;
-    __shared__ double G[15];
+    constexpr int NM = kMom(D);
+    __shared__ double G[16];
     const int e = local_, tid = threadIdx.x;
-    for (int m = tid; m < 15; m += blockDim.x) {
+    for (int m = tid; m < NM; m += blockDim.x) {
         double sv = 0.0;
         for (int c = 0; c < d.CF; c++) sv += (double)w.adj_gpart[((size_t)e * d.CF + c) * kAdjAcc + m];
         G[m] = sv;
     }
     __syncthreads();
-    if (tid >= 12) return;
+    if (tid >= 2 * D) return;
     const int ia = (int)io.ii[e], ib = (int)io.jj[e];
     double out = 0.0;
     if (ia != ib) {
-        const M4 T = edge_matrix(io.poses, ia, ib);
-        double unit[6] = {0, 0, 0, 0, 0, 0};
-        unit[tid % 6] = 1.0;
-        const M4 H = hat(unit);
-        const bool src = tid < 6;
+        const M4 T = edge_matrix<D>(io.poses, ia, ib);
+        const bool src = tid < D;
+        const int n = tid % D;
+        M4 H = mzero();
+        if (n < 6) {
+            double unit[6] = {0, 0, 0, 0, 0, 0};
+            unit[n] = 1.0;
+            H = hat(unit);
+        } else {
+            H.m[0] = H.m[5] = H.m[10] = 1.0;  // the scale generator diag(1, 1, 1, 0)
+        }
         const M4 Ms = src ? madd(mzero(), mmul(T, H), -1.0) : mmul(H, T);
         for (int r = 0; r < 3; r++)
             for (int col = 0; col < 4; col++) out += Ms.m[4 * r + col] * G[4 * r + col];
-        const int n = tid % 6;
-        if (n >= 3) {
-            if (src)
-                out += T.m[0 * 4 + (n - 3)] * G[12] + T.m[1 * 4 + (n - 3)] * G[13] + T.m[2 * 4 + (n - 3)] * G[14];
-            else
+        if (n >= 3 && n < 6) {
+            if (src) {
+                // R^T om with R the rotation of Tij (the 3x3 block of T is s R)
+                const double sc = (D == 6) ? 1.0 : sqrt(T.m[0] * T.m[0] + T.m[4] * T.m[4] + T.m[8] * T.m[8]);
+                out += (T.m[0 * 4 + (n - 3)] * G[12] + T.m[1 * 4 + (n - 3)] * G[13] + T.m[2 * 4 + (n - 3)] * G[14]) / sc;
+            } else {
                 out -= G[12 + n - 3];
+            }
+        } else if (n == 6) {
+            out += src ? G[15] : -G[15];
         }
     }
-    w.adj_gedge[(size_t)e * 12 + tid] = out;
+    w.adj_gedge[(size_t)e * 2 * D + tid] = out;
 }
 
 // gT[f] += per-edge pose gradients (every frame of the graph, fixed ones too);
 // one warp per frame, edges in index order, fixed reduction order.
+template <int D>
 __global__ void ba_adj_pose_kernel(BAPtrs base, Batch B) {
     BA_BIND(B, base);
     if (w.status[0]) return;
     const int lane = threadIdx.x & 31;
     for (int f = threadIdx.x >> 5; f < d.N; f += blockDim.x >> 5) {
-        double acc[6] = {0, 0, 0, 0, 0, 0};
+        double acc[D];
+        for (int n = 0; n < D; n++) acc[n] = 0.0;
         for (int e = lane; e < d.E; e += 32) {
             const int ia = (int)io.ii[e], ib = (int)io.jj[e];
             if (ia == f)
-                for (int n = 0; n < 6; n++) acc[n] += w.adj_gedge[(size_t)e * 12 + n];
+                for (int n = 0; n < D; n++) acc[n] += w.adj_gedge[(size_t)e * 2 * D + n];
             if (ib == f)
-                for (int n = 0; n < 6; n++) acc[n] += w.adj_gedge[(size_t)e * 12 + 6 + n];
+                for (int n = 0; n < D; n++) acc[n] += w.adj_gedge[(size_t)e * 2 * D + D + n];
         }
-        for (int n = 0; n < 6; n++) {
+        for (int n = 0; n < D; n++) {
             const double sv = warp_sum(acc[n]);
-            if (lane == 0) w.adj_gT[(size_t)f * 6 + n] += sv;
+            if (lane == 0) w.adj_gT[(size_t)f * D + n] += sv;
         }
     }
 }
 
 __global__ void ba_adj_finish_kernel(BAPtrs base, Batch B) {
     BA_BIND(B, base);
-    for (int q = threadIdx.x; q < d.N * 7; q += blockDim.x) {
-        const int f = q / 7, n = q % 7;
-        io.g_poses[q] = n < 6 ? (float)w.adj_gT[(size_t)f * 6 + n] : 0.f;
+    const int D = d.dof;
+    for (int q = threadIdx.x; q < d.N * (D + 1); q += blockDim.x) {
+        const int f = q / (D + 1), n = q % (D + 1);
+        io.g_poses[q] = n < D ? (float)w.adj_gT[(size_t)f * D + n] : 0.f;
     }
 }
 
@@ -914,8 +1071,10 @@ extern "C" int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const
     if (plan->edges > 0 && (!targets || !weights || !ii || !jj || !grad_targets || !grad_weights))
         return VIPE_ERR_ARG;
     size_t smem_b = 0;
-    for (const auto& gd : plan->gds) smem_b = std::max(smem_b, (size_t)kPixF * gd.d.chunk_f * sizeof(float));
-    if (smem_b > (size_t)kPixF * kAdjMaxChunk * sizeof(float)) {
+    const int dof = plan->geo.dof;
+    const int pixf = kPixF(dof);
+    for (const auto& gd : plan->gds) smem_b = std::max(smem_b, (size_t)pixf * gd.d.chunk_f * sizeof(float));
+    if (smem_b > (size_t)pixf * kAdjMaxChunk * sizeof(float)) {
         set_last_error("vipe_slam_ba_batch_backward: pixel chunk beyond 1536 (use more frame_chunks)");
         return VIPE_ERR_CAPACITY;
     }
@@ -931,8 +1090,12 @@ extern "C" int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const
     }
     VIPE_CUDA_TRY(cudaMemsetAsync(grad_eta, 0, sizeof(float) * plan->kx * HW, st));
     VIPE_CUDA_TRY(cudaMemsetAsync(grad_disps_sens, 0, sizeof(float) * plan->frames * HW, st));
-    VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_adj_frame_b_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(kPixF * kAdjMaxChunk * sizeof(float))));
+    if (dof == 7)
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_adj_frame_b_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)(pixf * kAdjMaxChunk * sizeof(float))));
+    else
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_adj_frame_b_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)(pixf * kAdjMaxChunk * sizeof(float))));
     BAPtrs base{const_cast<float*>(tape_poses), const_cast<float*>(tape_disps), const_cast<float*>(intrinsics),
                 disps_sens, targets, weights, eta, ii, jj, depth_active, const_cast<float*>(tape_dx), nullptr,
                 nullptr, dev_status, 0, 1, grad_poses, grad_disps, grad_targets, grad_weights, grad_eta,
@@ -945,18 +1108,24 @@ extern "C" int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const
     const Batch frames{plan->d_table, plan->d_off + (size_t)kOffFrame * (G + 1), G};
     const Batch edges{plan->d_table, plan->d_off + (size_t)kOffEdgeRed * (G + 1), G};
     for (int itr = iterations - 1; itr >= 0; itr--) {
-        base.poses = const_cast<float*>(tape_poses) + (size_t)itr * plan->frames * 7;
+        base.poses = const_cast<float*>(tape_poses) + (size_t)itr * plan->frames * (dof + 1);
         base.disps = const_cast<float*>(tape_disps) + (size_t)itr * plan->frames * HW;
-        base.dx = const_cast<float*>(tape_dx) + (size_t)itr * plan->poses * 6;
+        base.dx = const_cast<float*>(tape_dx) + (size_t)itr * plan->poses * dof;
         base.ftape = const_cast<double*>(tape_factor) + (size_t)itr * plan->ftape_stride;
         {
             VIPE_PROF("ba_adj_prep", st);
-            ba_adj_prep_kernel<<<G, 128, 0, st>>>(base, per_graph);
+            if (dof == 7)
+                ba_adj_prep_kernel<7><<<G, 128, 0, st>>>(base, per_graph);
+            else
+                ba_adj_prep_kernel<6><<<G, 128, 0, st>>>(base, per_graph);
         }
         VIPE_LAUNCH_CHECK();
         if (grid(kOffFrame) > 0) {
             VIPE_PROF("ba_adj_frame_a", st);
-            ba_adj_frame_a_kernel<<<grid(kOffFrame), kAdjThreads, 0, st>>>(base, frames, alpha);
+            if (dof == 7)
+                ba_adj_frame_a_kernel<7><<<grid(kOffFrame), kAdjThreads, 0, st>>>(base, frames, alpha);
+            else
+                ba_adj_frame_a_kernel<6><<<grid(kOffFrame), kAdjThreads, 0, st>>>(base, frames, alpha);
         }
         VIPE_LAUNCH_CHECK();
         {
@@ -967,18 +1136,25 @@ extern "C" int vipe_slam_ba_batch_backward(const vipe_ba_batch_plan* plan, const
         if ((rc = launch_chol_resolve(geo, plan->d_table, base, st)) != VIPE_OK) return rc;
         if (grid(kOffFrame) > 0) {
             VIPE_PROF("ba_adj_frame_b", st);
-            ba_adj_frame_b_kernel<<<grid(kOffFrame), kAdjThreads, smem_b, st>>>(base, frames, alpha, lm,
+            auto fb = dof == 7 ? ba_adj_frame_b_kernel<7> : ba_adj_frame_b_kernel<6>;
+            fb<<<grid(kOffFrame), kAdjThreads, smem_b, st>>>(base, frames, alpha, lm,
                                                                                  itr == iterations - 1 ? 1 : 0);
         }
         VIPE_LAUNCH_CHECK();
         if (grid(kOffEdgeRed) > 0) {
             VIPE_PROF("ba_adj_edge_reduce", st);
-            ba_adj_edge_reduce_kernel<<<grid(kOffEdgeRed), 32, 0, st>>>(base, edges);
+            if (dof == 7)
+                ba_adj_edge_reduce_kernel<7><<<grid(kOffEdgeRed), 32, 0, st>>>(base, edges);
+            else
+                ba_adj_edge_reduce_kernel<6><<<grid(kOffEdgeRed), 32, 0, st>>>(base, edges);
         }
         VIPE_LAUNCH_CHECK();
         {
             VIPE_PROF("ba_adj_pose", st);
-            ba_adj_pose_kernel<<<G, 256, 0, st>>>(base, per_graph);
+            if (dof == 7)
+                ba_adj_pose_kernel<7><<<G, 256, 0, st>>>(base, per_graph);
+            else
+                ba_adj_pose_kernel<6><<<G, 256, 0, st>>>(base, per_graph);
         }
         VIPE_LAUNCH_CHECK();
     }

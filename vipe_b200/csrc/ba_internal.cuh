@@ -4,6 +4,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "lie_group.cuh"
 #include "se3_device.cuh"
 
 #include <algorithm>
@@ -92,12 +93,12 @@ struct Work {
     int* wtile_off;  // K + 1: first Gram tile of each wide frame in wtile
     float* wtile;    // wtile_cap x 16: wide frames' upper-triangle 4 x 4 Gram tiles, all chunks summed
     // adjoint (carved only when Dims::adj)
-    double* adj_gT;    // N * 6   running left-tangent gradient of every pose
+    double* adj_gT;    // N * dof running left-tangent gradient of every pose
     double* adj_rhs;   // dim     g_dxi, then g_dxi - E~ Q g_dz
     double* adj_lam;   // dim     lambda = S'^-1 rhs
-    float* adj_aslot;  // E * CF * 12  per (edge, pixel chunk): sum a act wd Jz [Ji, Jj]
+    float* adj_aslot;  // E * CF * 2 dof  per (edge, pixel chunk): sum a act wd Jz [Ji, Jj]
     float* adj_gpart;  // E * CF * kAdjAcc  per (edge, pixel chunk) pose-gradient moments
-    double* adj_gedge; // E * 12  per-edge pose gradient [source pose, target pose]
+    double* adj_gedge; // E * 2 dof  per-edge pose gradient [source pose, target pose]
 };
 
 constexpr int kAdjAcc = 48;  // 4 moment matrices of 3 x 4 per edge
@@ -211,12 +212,13 @@ inline void carve(C& c, const Dims& d, Work* w) {
         w->adj_gedge = nullptr;
     }
     if (d.adj) {
-        auto g1 = c.template take<double>(N * 6);
+        const size_t D = d.dof;
+        auto g1 = c.template take<double>(N * D);
         auto g2 = c.template take<double>((size_t)d.dim);
         auto g3 = c.template take<double>((size_t)d.dim);
-        auto g4 = c.template take<float>((size_t)std::max<size_t>(1, E) * d.CF * 12);
+        auto g4 = c.template take<float>((size_t)std::max<size_t>(1, E) * d.CF * 2 * D);
         auto g5 = c.template take<float>((size_t)std::max<size_t>(1, E) * d.CF * kAdjAcc);
-        auto g6 = c.template take<double>((size_t)std::max<size_t>(1, E) * 12);
+        auto g6 = c.template take<double>((size_t)std::max<size_t>(1, E) * 2 * D);
         if (w) {
             w->adj_gT = (double*)g1;
             w->adj_rhs = (double*)g2;
@@ -456,6 +458,59 @@ struct SolveArgs {
     int compute_energy;
     const float* mu_sched = nullptr;  // host: the robust kernel's mu at each iteration (GNC), or none
 };
+
+// ---------------------------------------------------------------- relative pose of an edge
+// SE3 (D = 6, poses (N, 7)) or Sim3 (D = 7, poses (N, 8) [t q s]): Tij = Tj Ti^-1; ii == jj is a
+// stereo edge with the fixed baseline (-0.1, 0, 0)
+
+struct EdgeTf {
+    float t[3], q[4], s;
+};
+
+template <int D>
+__device__ __forceinline__ void edge_tf(const float* poses, int a, int b, EdgeTf& T) {
+    if (D == 6) {
+        edge_pose(poses, a, b, T.t, T.q);
+        T.s = 1.f;
+    } else if (a == b) {
+        T.t[0] = -0.1f; T.t[1] = 0.f; T.t[2] = 0.f;
+        T.q[0] = 0.f; T.q[1] = 0.f; T.q[2] = 0.f; T.q[3] = 1.f;
+        T.s = 1.f;
+    } else {
+        float pi[8], pj[8];
+#pragma unroll
+        for (int n = 0; n < 8; n++) {
+            pi[n] = __ldg(poses + 8 * a + n);
+            pj[n] = __ldg(poses + 8 * b + n);
+        }
+        const lie::Sim3<float> G = lie::Sim3<float>::load(pj) * lie::Sim3<float>::load(pi).inv();
+        T.t[0] = G.t[0]; T.t[1] = G.t[1]; T.t[2] = G.t[2];
+        T.q[0] = G.r.q.x; T.q[1] = G.r.q.y; T.q[2] = G.r.q.z; T.q[3] = G.r.q.w;
+        T.s = G.r.s;
+    }
+}
+
+// y = Ad(Tij) x for a tangent x of the source pose: the source-pose Jacobian rows
+// are -Ad^T(Tij) times the target-pose rows, so Ji . x = -Jj . (Ad x).
+//   SE3:  Ad = [[R, [t]x R], [0, R]];   Sim3: Ad = [[s R, [t]x R, -t], [0, R, 0], [0, 0, 1]]
+template <int D>
+__device__ __forceinline__ void edge_ad_apply(const EdgeTf& T, const float* x, float* y) {
+    float rt[3], rp[3];
+    qrot(T.q, x, rt);
+    qrot(T.q, x + 3, rp);
+    y[0] = T.s * rt[0] + (T.t[1] * rp[2] - T.t[2] * rp[1]);
+    y[1] = T.s * rt[1] + (T.t[2] * rp[0] - T.t[0] * rp[2]);
+    y[2] = T.s * rt[2] + (T.t[0] * rp[1] - T.t[1] * rp[0]);
+    y[3] = rp[0];
+    y[4] = rp[1];
+    y[5] = rp[2];
+    if constexpr (D == 7) {
+        y[0] -= T.t[0] * x[6];
+        y[1] -= T.t[1] * x[6];
+        y[2] -= T.t[2] * x[6];
+        y[6] = x[6];
+    }
+}
 
 // host launchers implemented in ba.cu
 int check_dims(int num_frames, int ht, int wd, int num_edges, int num_kx, int t0, int t1);
