@@ -2884,8 +2884,8 @@ extern "C" int vipe_slam_ba_batch_plan_create(int num_graphs, const int* num_fra
     const int che = edge_chunks > 0 ? edge_chunks : (sumE > 0 ? (int)std::max<long>(1, (target + sumE - 1) / sumE) : 1);
     int cf = frame_chunks > 0 ? frame_chunks : (int)std::max<long>(1, (target + sumK - 1) / sumK);
     // the adjoint keeps a few floats per pixel of a (frame, chunk) block in
-    // shared memory: at most kAdjMaxChunk pixels per chunk
-    if (with_adjoint) cf = std::max(cf, (ht * wd + kAdjMaxChunk - 1) / kAdjMaxChunk);
+    // shared memory: at most adj_plan_chunk(dof) pixels per chunk
+    if (with_adjoint) cf = std::max(cf, (ht * wd + adj_plan_chunk(dof) - 1) / adj_plan_chunk(dof));
     auto* plan = new vipe_ba_batch_plan();
     plan->G = num_graphs;
     plan->adjoint = with_adjoint ? 1 : 0;

@@ -27,6 +27,10 @@ constexpr int kFrameThreads = 128;     // one pixel per thread; 32-pixel blocks 
 constexpr int kIndexThreads = 1024;
 constexpr int kEdgeCache = 64;        // edges of a depth frame whose per-edge constants a CTA caches
 constexpr int kAdjMaxChunk = 1536;    // pixels of one (frame, chunk) block of the adjoint frame kernels
+// the plan's pixel chunk for adjoint plans: SE3 1536; Sim3 1024, so that the second adjoint frame
+// kernel's per-pixel arrays (one more float per pixel) and 100-float edge rows leave room for
+// two CTAs per SM
+__host__ __device__ constexpr int adj_plan_chunk(int dof) { return dof == 7 ? 1024 : kAdjMaxChunk; }
 
 // per-edge term layout
 //   [0,78)   upper triangle (row-major, n >= m) of the 12x12 block [Ji Jj]^T W [Ji Jj]
