@@ -3,12 +3,14 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Workload: 256 clips of the bundle-adjustment generative model with uneven
-sizes (keyframes ~U{8..96} at 48x64, SE3, edges |i-j| <= 3 plus Poisson(4) loop
-pairs, 1% outlier flow), 4 LM iterations, first two poses of each clip fixed;
+sizes (keyframes ~U{8..96} at 48x64, Sim3 poses, edges |i-j| <= 3 plus Poisson(4)
+loop pairs, 1% outlier flow), 4 LM iterations, first two poses of each clip fixed;
 seeded synthetic inputs generated on the GPU (vipe_b200.workloads).  One step =
 one batched forward solve of all 256 clips recording its state tape plus the
 hand-written adjoint for fixed incoming gradients (gradients for poses, depths,
 targets, weights, eta, disps_sens).  The metric counts clip solves per second.
+The same batch in SE3 form is timed beside it (se3_fwd_adjoint), and its forward
+alone (batched).
 
 Reported (one JSON line on rank 0):
   value      device-timed solves/s (fwd+adjoint), inputs resident in HBM
@@ -48,7 +50,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "batched BA solves/s (fwd+adjoint)"
 WORKLOAD = (
-    "batched BA: 256 clips, keyframes ~U{8..96} at 48x64, SE3, edges |i-j|<=3 + Poisson(4) loop pairs "
+    "batched BA: 256 clips, keyframes ~U{8..96} at 48x64, Sim3, edges |i-j|<=3 + Poisson(4) loop pairs "
     "(|i-j|>8, both directions), 1% outlier flow (U(-20,20) px, weight 0.05), 4 LM iterations, t0=2"
 )
 
@@ -70,6 +72,7 @@ def parse():
     ap.add_argument("--clips", type=int, default=32)
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--edges", type=int, default=64)
+    ap.add_argument("--group", choices=["se3", "sim3"], default="se3", help="--case batch: pose group")
     return ap.parse_args()
 
 
@@ -592,9 +595,10 @@ def cpu_baseline(b, sample_s):
         "unit": "solves/s",
         "cores": threads,
         "kind": "port",
-        "sample": f"{n} clips of the 256-clip batch (fixed shuffled order), FORWARD solves only (4 LM iterations; "
-        f"the reference has no BA backward), in {el:.1f} s (oracle/ba_oracle.cpp: the reference's ba_cuda_impl "
-        f"restated, FP32 per-edge math on {threads} threads, dense FP64 Cholesky)",
+        "sample": f"{n} clips of the 256-clip batch in its SE3 form (fixed shuffled order), FORWARD solves only "
+        f"(4 LM iterations; the reference's BA has neither a Sim3 form nor a backward), in {el:.1f} s "
+        f"(oracle/ba_oracle.cpp: the reference's ba_cuda_impl restated, FP32 per-edge math on {threads} threads, "
+        f"dense FP64 Cholesky)",
     }
 
 
@@ -634,14 +638,16 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "global_batch": 256, "parallelism": "host threads"},
+        "config": {"workload": WORKLOAD + "; solved here in its SE3 form (the reference's BA has no Sim3 form)",
+                   "global_batch": 256, "parallelism": "host threads"},
         "cpu_baseline": {
             "value": v,
             "unit": "solves/s",
             "cores": threads,
             "kind": "port",
-            "sample": f"{solves} clips of the 256-clip batch in a fixed shuffled order, FORWARD solves only (the "
-            f"reference has no BA backward; each step solves clips for about {per_step:.0f} s; "
+            "sample": f"{solves} clips of the 256-clip batch (SE3 form) in a fixed shuffled order, FORWARD solves "
+            f"only (the reference has no BA backward and no Sim3 BA; each step solves clips for about "
+            f"{per_step:.0f} s; "
             f"oracle/ba_oracle.cpp, the reference's ba_cuda_impl restated on the CPU: the reference's slam_ext "
             f"needs Eigen 3.4, which is downloaded at build time, and cannot be built here)",
         },
@@ -663,10 +669,15 @@ TRAFFIC_PER_EDGE = {
     "ba_frame": 584.0e6 / 8938,
     "ba_adj_frame_b": (1133.0e6 + 3 * 1573.0e6) / 4 / 8938,
 }
+# the same for the Sim3 batch (`... --case batch --clips 32 --group sim3 --reps 1`, 8872 edges; the first
+# backward iteration writes the target/weight gradients, the other three read-modify-write them)
+TRAFFIC_PER_EDGE_SIM3 = {
+    "ba_adj_frame_b": ((616.0e6 + 498.0e6) + 3 * (1054.0e6 + 498.0e6)) / 4 / 8872,
+}
 
 
-def batch_kernel_traffic(b, name):
-    per_edge = TRAFFIC_PER_EDGE.get(name)
+def batch_kernel_traffic(b, name, group="se3"):
+    per_edge = (TRAFFIC_PER_EDGE_SIM3 if group == "sim3" else TRAFFIC_PER_EDGE).get(name)
     return None if per_edge is None else per_edge * sum(b.num_edges)
 
 
@@ -863,7 +874,7 @@ def batched_leg(dev, args, world, dist, flush, stream):
     return value, e2e_line, extras, b.G, n, b
 
 
-def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
+def adjoint_leg(b, tune, dev, args, world, dist, flush, stream, group="se3", with_e2e=True):
     """Forward + hand-written adjoint of the batched BA on the same batch.
 
     One step: the forward solve recording its state tape, then the backward for
@@ -877,15 +888,16 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
 
     lib = _lib.load()
     iters, lm, ep, alpha = 4, 1e-4, 0.1, 0.001
-    plan = BB.BatchPlan(*b.sizes, b.ht, b.wd, dev, edge_chunks=tune[0], frame_chunks=tune[1], adjoint=True)
+    plan = BB.BatchPlan(*b.sizes, b.ht, b.wd, dev, edge_chunks=tune[0], frame_chunks=tune[1], adjoint=True,
+                        group=group)
     T = b.tensors
     F, H, W = plan.total_frames, plan.ht, plan.wd
     static = {k: v.clone() for k, v in T.items()}
     out = plan.outputs(iters)
     tape = plan.make_tape(iters)
     g = torch.Generator(device=dev).manual_seed(1005)
-    gin_p = torch.randn(F, 7, generator=g, device=dev)
-    gin_p[:, 6] = 0
+    gin_p = torch.randn(F, plan.dof + 1, generator=g, device=dev)
+    gin_p[:, plan.dof] = 0
     gin_d = torch.randn(F, H, W, generator=g, device=dev)
     gp, gd = torch.empty_like(gin_p), torch.empty_like(gin_d)
     gt, gw = torch.empty_like(T["targets"]), torch.empty_like(T["weights"])
@@ -947,11 +959,15 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
         avg_s = kms / cnt / 1e3
         ach = nbytes / avg_s / 1e9
         roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                "traffic": batch_kernel_traffic(b, name), "peak_source": src, "bytes_per_launch": nbytes,
+                "traffic": batch_kernel_traffic(b, name, group), "peak_source": src, "bytes_per_launch": nbytes,
                 "avg_launch_ms": avg_s * 1e3,
                 "note": "FP32-issue bound: HBM is the algorithmic bound, not the limiter (ncu: issue active "
-                        "57%, FMA pipe 40%, DRAM 12% of peak on the 32-clip case)"}
+                        "57%, FMA pipe 40% on the 32-clip SE3 case; 69% of its instructions on the FMA pipe)"}
         break
+    if not with_e2e:
+        del plan, static, tape, gt, gw
+        return {"value": value, "ms_per_step": step_ms, "steps": n, "status_nonzero": status_nonzero,
+                "kernel_breakdown": breakdown, "roofline": roof, "gpu_launches_per_step": launches}
 
     # end to end: pinned host inputs and incoming gradients in, outputs and all gradients out.
     # (1) the public streaming API: the batch in parts on their own streams, copies
@@ -962,7 +978,7 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream):
     host_in = {k: v.cpu().pin_memory() for k, v in T.items()}
     host_g = [gin_p.cpu().pin_memory(), gin_d.cpu().pin_memory()]
     runner = StreamedBundleAdjust(b.sizes, b.ht, b.wd, dev, parts=args.e2e_parts, iterations=iters, lm=lm, ep=ep,
-                                  alpha=alpha, edge_chunks=tune[0], frame_chunks=tune[1])
+                                  alpha=alpha, edge_chunks=tune[0], frame_chunks=tune[1], group=group)
     run_out = runner.host_outputs()
     h2d = runner.h2d_bytes(host_in)
     d2h = runner.d2h_bytes(run_out)
@@ -1195,15 +1211,23 @@ def run_ours(args):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
+    from vipe_b200 import workloads as Wk
+
     with ClockSampler(local) as clk:
         fwd_value, fwd_e2e, extras, G, n_fwd, b = batched_leg(dev, args, world, dist, flush, stream)
         torch.cuda.empty_cache()
-        adj = adjoint_leg(b, extras.pop("tune"), dev, args, world, dist, flush, stream)
+        tune = extras.pop("tune")
+        # the headline: config 4 as written (Sim3), forward + adjoint, end to end
+        b7 = Wk.ba_config4(device=dev)
+        adj = adjoint_leg(b7, tune, dev, args, world, dist, flush, stream, group="sim3")
+        del b7
+        torch.cuda.empty_cache()
+        adj_se3 = adjoint_leg(b, tune, dev, args, world, dist, flush, stream, group="se3", with_e2e=False)
     value, e2e, n = adj["value"], adj.pop("e2e"), adj["steps"]
     extras["forward_only"] = {"value": fwd_value, "unit": "solves/s", "ms_per_batch": extras["batch_ms"],
                               "roofline": extras.pop("roofline"),
                               "steps": n_fwd, "e2e": fwd_e2e, "form": "CUDA graph of the whole LM loop"}
-    extras["speedup_fwd_adj_vs_plain_forward_same_gpu"] = value / extras["plain_same_gpu"]["value"]
+    extras["speedup_se3_fwd_adj_vs_plain_forward_same_gpu"] = adj_se3["value"] / extras["plain_same_gpu"]["value"]
     torch.cuda.empty_cache()
     plain = plain_cfg1_leg(dev, args, flush, stream)
     torch.cuda.empty_cache()
@@ -1250,6 +1274,7 @@ def run_ours(args):
             "clocks": clk.summary(),
             "batched": extras,
             "adjoint": adj,
+            "se3_fwd_adjoint": adj_se3,
             "plain_cfg1": plain,
             "plain_backend_256kf": backend,
             "sim3_batched": sim3,
@@ -1340,13 +1365,13 @@ def case_lookup(edges: int, reps: int) -> None:
     torch.cuda.synchronize()
 
 
-def case_batch(clips: int, reps: int) -> None:
+def case_batch(clips: int, reps: int, group: str = "se3") -> None:
     from vipe_b200 import _lib
     from vipe_b200 import workloads as W
     from vipe_b200.ba_batch import BatchPlan
 
-    b = W.make_ba_batch(clips, seed=1004, device="cuda")
-    plan = BatchPlan(*b.sizes, b.ht, b.wd, "cuda", adjoint=True)
+    b = W.make_ba_batch(clips, seed=1004, device="cuda", group=group)
+    plan = BatchPlan(*b.sizes, b.ht, b.wd, "cuda", adjoint=True, group=group)
     it = 4
     tape = plan.make_tape(it)
     T = b.tensors
@@ -1354,8 +1379,8 @@ def case_batch(clips: int, reps: int) -> None:
     for _ in range(reps):
         s = {k: v.clone() for k, v in T.items()}
         _, _, _, st = plan.solve(**s, iterations=it, lm=1e-4, ep=0.1, tape=tape)
-        gp = torch.randn(plan.total_frames, 7, generator=g, device="cuda")
-        gp[:, 6] = 0
+        gp = torch.randn(plan.total_frames, plan.dof + 1, generator=g, device="cuda")
+        gp[:, plan.dof] = 0
         gd = torch.randn(plan.total_frames, b.ht, b.wd, generator=g, device="cuda")
         out = [torch.empty_like(T[k]) for k in ("targets", "weights", "eta", "disps_sens")]
         st2 = torch.zeros(plan.G, dtype=torch.int32, device="cuda")
@@ -1439,7 +1464,7 @@ def run_case(args):
     elif args.case == "corr_encoder":
         case_corr_encoder(args.edges, args.reps)
     elif args.case == "batch":
-        case_batch(args.clips, args.reps)
+        case_batch(args.clips, args.reps, args.group)
     elif args.case == "lookup":
         case_lookup(args.edges, args.reps)
     else:

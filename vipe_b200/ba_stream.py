@@ -95,8 +95,6 @@ class StreamedBundleAdjust:
         self.total_frames, self.total_edges, self.total_kx = sum(num_frames), sum(num_edges), sum(num_kx)
         self.dof = 7 if group == "sim3" else 6
         self.adjoint = bool(adjoint)
-        if self.adjoint and group != "se3":
-            raise RuntimeError("StreamedBundleAdjust: the adjoint covers SE3 graphs only")
         self.parts: list[_Part] = []
         HW = (self.ht, self.wd)
         f0 = e0 = k0 = 0
