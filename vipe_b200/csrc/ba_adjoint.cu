@@ -35,6 +35,13 @@
 // derivative.  So per edge the pixels only accumulate G0 = sum g X^T (3x4) and
 // one 3-vector for the rotation dofs, contracted with Ps per pose direction
 // once per edge; the per-pixel directions of the damping terms fit the same form.
+//
+// Sim3 (D = 7, tangent [tau, phi, sigma], X' = s R X3 + t d): the generator of sigma moves P by
+// sigma P (target pose) or -s R sigma X3 (source pose), so the directions gain
+// Pt_v += v_j,sigma P and Y_v = s R (v_i,tau W + v_i,phi x X3 + v_i,sigma X3), the Ps
+// coefficient gains v_j,sigma grad f, and the scale dofs take one more per-edge moment,
+// os = sum Y_v . grad f (target: -os, source: +os), beside G0 and the rotation vector (whose
+// source rows use the pure rotation R of s R).  Every kernel below is written for D = 6 and 7.
 
 // Precision: the per-pixel work is FP32 like the forward; the re-solve and every
 // pose-level sum are FP64.
