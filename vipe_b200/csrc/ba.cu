@@ -465,10 +465,11 @@ __device__ __forceinline__ void linearize_d(const EdgeTf& T, bool stereo, float 
 
 template <bool kIntr, int D, bool kExt = false>
 // 4 CTAs per SM for the SE3 form (64 registers; 10.4 vs 11.7 ms per 256-clip step at the
-// 80 registers the compiler picks unbounded); the focal and Sim3 forms are left unbounded.
+// 80 registers the compiler picks unbounded), 3 for the Sim3 form (80 registers; 14.0 vs 16.5
+// ms unbounded at 109); the focal form is left unbounded.
 // kExt: robust reweighting / camera model from io.rb compiled in (single solves that ask for
 // them); without it the plain pinhole linearisation carries none of that code.
-__global__ void __launch_bounds__(kEdgeThreads, (D == 6 && !kIntr) ? 4 : 1) ba_edge_kernel(BAPtrs base, Batch B,
+__global__ void __launch_bounds__(kEdgeThreads, (D == 6 && !kIntr) ? 4 : (D == 7 ? 3 : 1)) ba_edge_kernel(BAPtrs base, Batch B,
                                                                                           float iscale) {
     BA_BIND(B, base);
     if (w.status[0]) return;
@@ -2004,9 +2005,10 @@ __global__ void __launch_bounds__(kCholThreads) ba_chol_resolve_kernel(BAPtrs ba
 
 template <bool kIntr, int D, bool kExt = false>
 // 8 CTAs per SM for the SE3 form (32 registers: latency-bound, more warps in flight beat the
-// spills; 5.5 vs 8.5 ms per 256-clip step at 3 CTAs); the focal and Sim3 forms keep 3.
+// spills; 5.5 vs 8.5 ms per 256-clip step at 3 CTAs), 6 for Sim3 (6.0 vs 8.6 ms at 3; 6.3 at 8);
+// the focal form keeps 3.
 // kExt as for ba_edge_kernel.
-__global__ void __launch_bounds__(256, (D == 6 && !kIntr) ? 8 : 3) ba_backsub_kernel(BAPtrs base, Batch B) {
+__global__ void __launch_bounds__(256, (D == 6 && !kIntr) ? 8 : (D == 7 ? 6 : 3)) ba_backsub_kernel(BAPtrs base, Batch B) {
     BA_BIND(B, base);
     if (w.status[0]) return;
     const FrameArgs A{io.poses, io.disps, io.disps_sens, io.intr, io.targets, io.weights, io.eta, io.depth_active, io.jj,
