@@ -157,6 +157,18 @@ def whole_job_rate(world, units_per_rank, ms):
     return world * units_per_rank / (ms / 1e3)
 
 
+VIPE_WARN_SOLVER = 16  # vipe_status: the reduced camera system was not positive definite, dx = 0
+
+
+def status_counts(words):
+    """Per-graph device status words -> how many graphs ended with the solver warning
+    (Cholesky failure, dx = 0 as the reference's solver returns) and how many with an error."""
+    words = [int(x) for x in (words.tolist() if hasattr(words, "tolist") else words)]
+    warn = sum(1 for x in words if x == VIPE_WARN_SOLVER)
+    return {"status_nonzero": sum(1 for x in words if x), "solver_warnings": warn,
+            "errors": sum(1 for x in words if x and x != VIPE_WARN_SOLVER)}
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -853,7 +865,7 @@ def batched_leg(dev, args, world, dist, flush, stream):
         "batch": {"clips": b.G, "frames": sum(b.num_frames), "edges": sum(b.num_edges), "depth_rows": sum(b.num_kx),
                   "input_bytes": h2d},
         "batch_ms": batch_ms,
-        "status_nonzero": sum(1 for x in status if x),
+        **status_counts(status),
         "autotune": {"edge_chunks": tune.edge_chunks, "frame_chunks": tune.frame_chunks,
                      "table_ms": [[ec, fc, ms] for ec, fc, ms in tune.table]},
         "plain_same_gpu": {"value": b.G / (plain_ms / 1e3), "unit": "solves/s", "ms_per_batch": plain_ms,
@@ -938,7 +950,7 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream, group="se3", wit
     torch.cuda.synchronize(dev)
     step_ms = max_over_ranks(sum(a.elapsed_time(c) for a, c in ev), world, dist, dev) / n
     value = whole_job_rate(world, b.G, step_ms)
-    status_nonzero = int((st != 0).sum().item())
+    status = status_counts(st)  # OR of the words over every run above
 
     # live per-kernel profile of one step
     def once():
@@ -966,7 +978,7 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream, group="se3", wit
         break
     if not with_e2e:
         del plan, static, tape, gt, gw
-        return {"value": value, "ms_per_step": step_ms, "steps": n, "status_nonzero": status_nonzero,
+        return {"value": value, "ms_per_step": step_ms, "steps": n, "status": status,
                 "kernel_breakdown": breakdown, "roofline": roof, "gpu_launches_per_step": launches}
 
     # end to end: pinned host inputs and incoming gradients in, outputs and all gradients out.
@@ -983,6 +995,7 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream, group="se3", wit
     h2d = runner.h2d_bytes(host_in)
     d2h = runner.d2h_bytes(run_out)
     e2e = []
+    words = torch.zeros(b.G, dtype=torch.int32)
     for k in range(max(3, args.warmup) + args.steps):
         a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         flush.fill_(float(k))
@@ -990,9 +1003,10 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream, group="se3", wit
         runner.step(host_in, host_g[0], host_g[1], run_out, stream=stream)
         c.record(stream)
         torch.cuda.synchronize(dev)
+        words |= runner.status().cpu()
         if k >= max(3, args.warmup):
             e2e.append(a.elapsed_time(c))
-    stream_status = int((runner.status() != 0).sum().item())
+    stream_status = status_counts(words)  # graphs whose word was non-zero in any step
     e2e_value = whole_job_rate(world, b.G * len(e2e), max_over_ranks(sum(e2e), world, dist, dev))
     nparts = len(runner.parts)
     del runner
@@ -1021,14 +1035,14 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream, group="se3", wit
         "value": value,
         "ms_per_step": step_ms,
         "steps": n,
-        "status_nonzero": status_nonzero,
+        "status": status,
         "kernel_breakdown": breakdown,
         "roofline": roof,
         "gpu_launches_per_step": launches,
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": f"vipe_b200.ba_stream.StreamedBundleAdjust.step ({nparts} parts on their own streams; pinned "
                        "host tensors in: inputs and incoming gradients; out: poses, depths and every input gradient)",
-                "status_nonzero": stream_status,
+                "status": stream_status,
                 "sequential_copies": {"value": seq_value, "unit": "solves/s",
                                       "api": "one BatchPlan: copies in, solve with tape, backward, copies out, in "
                                              "sequence on one stream"}},
@@ -1090,7 +1104,7 @@ def sim3_leg(dev, args, flush, stream):
         "value": b.G / (batch_ms / 1e3),
         "unit": "solves/s",
         "ms_per_batch": batch_ms,
-        "status_nonzero": sum(1 for x in status if x),
+        **status_counts(status),
         "autotune": [tune.edge_chunks, tune.frame_chunks],
         "max_pose_err_vs_fp64_oracle": max(errs),
         "oracle_clips": [b.num_frames[g] for g in order],

@@ -135,7 +135,9 @@ class BatchPlan:
         energy (G, iterations) or (G, 0), status (G,) int32 device words
         (0, a vipe_status error, or VIPE_WARN_SOLVER when that graph's Cholesky
         failed and its dx is 0).  ``out`` reuses preallocated outputs (for
-        CUDA-graph capture); ``check`` validates shapes on the host; ``tape``
+        CUDA-graph capture; the solve ORs its words into ``out``'s status, so zero
+        it between solves that should report separately); ``check`` validates
+        shapes on the host; ``tape``
         (from make_tape) receives the record the backward pass reads.
         """
         if check:

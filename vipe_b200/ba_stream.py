@@ -182,6 +182,9 @@ class StreamedBundleAdjust:
                     part.dev[key].copy_(host[key][a:b], non_blocking=True)
                 fa, fb = part.f
                 d, gr = part.dev, part.grads
+                # the solve and the backward OR their per-graph words in: clear last step's
+                part.out[3].zero_()
+                part.status.zero_()
                 if self.adjoint:
                     gr["grad_poses"].copy_(host_grad_poses[fa:fb], non_blocking=True)
                     gr["grad_disps"].copy_(host_grad_disps[fa:fb], non_blocking=True)
