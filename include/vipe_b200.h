@@ -160,7 +160,9 @@ int vipe_slam_ba_extended_generic(float* poses_io, float* disps_io, float* intri
  *   disps_io, disps_sens (num_keyframes * n_views, ht, wd), depth_active (num_keyframes * n_views);
  *   ii, jj: source and target depth-frame indices (k * n_views + q) of the num_edges terms,
  *     ii != jj; eta (num_kx, ht*wd) over kx = unique(arange(t0 n_views, t1 n_views) ++ ii);
- *   intrinsics (4): fx fy cx cy at the flow resolution, shared by all views (fixed);
+ *   intrinsics (n_views, 4): fx fy cx cy of each view at the flow resolution (fixed): a term
+ *     unprojects with its source view's row and projects with its target view's (the generic
+ *     solver's per-view intrinsics, terms.py:175-206);
  *   dx_out (t1 - t0, 6) keyframe steps; dz_out (num_kx, ht*wd); energy_out (iterations) or NULL;
  *   robust kernel, mu schedule and camera model as vipe_slam_ba_extended_generic.
  * Generic-solver back-substitution (rows of pose t0 kept).  Limits: n_views * (t1 - t0) <= 1024.

@@ -178,12 +178,19 @@ def _mat(T):
     return M
 
 
-def rig_problem(outliers=False):
+RIG_VIEW1_INTR = (1.07, 0.94, 0.9, -0.6)  # view 1 of the per-view case: fx, fy scale; cx, cy shift
+
+
+def rig_problem(outliers=False, views=False):
     """A two-view rig built from config 0 (deterministic, CPU): keyframe poses, rig (2, 7), depth
     frames k * 2 + q (view 1: 0.9 x view 0), the expanded terms of config 0's edges (edge-major,
     view-minor, as GraphBuffer.expand_edge_multiview orders them), targets = the reprojection at
     the initial state through the rig plus a deterministic +-0.8 px pattern (optionally the
-    outliers of with_outliers), config 0's weights per view, eta for kx, 2 LM iterations."""
+    outliers of with_outliers), config 0's weights per view, eta for kx, 2 LM iterations.
+    views=True: per-view intrinsics (view 1: fx, fy scaled and cx, cy shifted by RIG_VIEW1_INTR;
+    intrinsics (2, 4)) and two keyframe self-pairs (t0, t0) and (t0 + 1, t0 + 1), which expand
+    to cross-view terms (k, q) -> (k, (q + 1) % 2) as GraphBuffer's default cross_view_idx does,
+    so that source and target views (and intrinsics) differ within a term."""
     import types
 
     from vipe_b200 import workloads as W
@@ -197,22 +204,35 @@ def rig_problem(outliers=False):
     rig[1, 3:] = torch.tensor(_quat_of_aa(RIG_AA))
     disps = torch.stack([p.disps, 0.9 * p.disps], 1).reshape(N * V, H, Wd).contiguous()
     sens = torch.stack([p.disps_sens, p.disps_sens], 1).reshape(N * V, H, Wd).contiguous()
-    E = p.ii.shape[0]
-    pi = p.ii.repeat_interleave(V)
-    pj = p.jj.repeat_interleave(V)
+    kii, kjj, kw = p.ii, p.jj, p.weights
+    intr = p.intrinsics.clone()
+    if views:
+        self_pairs = torch.tensor([p.t0, p.t0 + 1], dtype=p.ii.dtype)
+        kii, kjj = torch.cat([p.ii, self_pairs]), torch.cat([p.jj, self_pairs])
+        kw = torch.cat([p.weights, p.weights[:2]])
+        sx, sy, ox, oy = RIG_VIEW1_INTR
+        v1 = torch.tensor([intr[0] * sx, intr[1] * sy, intr[2] + ox, intr[3] + oy], dtype=intr.dtype)
+        intr = torch.stack([intr, v1])
+    E = kii.shape[0]
+    pi = kii.repeat_interleave(V)
+    pj = kjj.repeat_interleave(V)
     q = torch.arange(V).repeat(E)
-    di, dj = pi * V + q, pj * V + q
-    fx, fy, cx, cy = [float(v) for v in p.intrinsics]
+    qj = torch.where(pi == pj, (q + 1) % V, q)
+    di, dj = pi * V + q, pj * V + qj
+    K = (intr if views else intr.reshape(1, 4).expand(V, 4)).double()
     G, Rg = _mat(p.poses), _mat(rig)
-    T = torch.linalg.inv(Rg[q]) @ G[pj] @ torch.linalg.inv(G[pi]) @ Rg[q]
+    T = torch.linalg.inv(Rg[qj]) @ G[pj] @ torch.linalg.inv(G[pi]) @ Rg[q]
     vv, uu = torch.meshgrid(torch.arange(H, dtype=torch.float64), torch.arange(Wd, dtype=torch.float64),
                             indexing="ij")
-    X = torch.stack([(uu - cx) / fx, (vv - cy) / fy, torch.ones_like(uu)], 0).reshape(3, -1)
+    uu, vv = uu.reshape(1, -1), vv.reshape(1, -1)
+    Ki, Kj = K[q], K[qj]  # (E * V, 4): source view unprojects, target view projects
+    X = torch.stack([(uu - Ki[:, 2:3]) / Ki[:, 0:1], (vv - Ki[:, 3:4]) / Ki[:, 1:2], torch.ones_like(uu).expand(
+        E * V, -1)], 1)
     d = disps.double()[di].reshape(E * V, 1, -1)
     Pp = T[:, :3, :3] @ X + T[:, :3, 3:] * d
     z = Pp[:, 2].clamp(min=0.1)
-    tu = fx * Pp[:, 0] / z + cx
-    tv = fy * Pp[:, 1] / z + cy
+    tu = Kj[:, 0:1] * Pp[:, 0] / z + Kj[:, 2:3]
+    tv = Kj[:, 1:2] * Pp[:, 1] / z + Kj[:, 3:4]
     k = torch.arange(E * V, dtype=torch.float64)[:, None]
     pix = torch.arange(H * Wd, dtype=torch.float64)[None]
     tu = tu + 0.8 * torch.sin(0.37 * pix + 1.1 * k)
@@ -220,13 +240,13 @@ def rig_problem(outliers=False):
     targets = torch.stack([tu, tv], 1).reshape(E * V, 2, H, Wd).float()
     if outliers:
         targets = with_outliers(targets)
-    weights = p.weights.repeat_interleave(V, 0).contiguous()
+    weights = kw.repeat_interleave(V, 0).contiguous()
     kx = torch.unique(torch.cat([torch.arange(p.t0 * V, p.t1 * V), di]))
     disp_damping = ((p.eta.double() - 1e-7) / 0.2).float()  # per keyframe; both views share it
     eta_frames = disp_damping.repeat_interleave(V, 0)  # (N * V, H*W) in frame order
     eta = (0.2 * eta_frames[kx] + 1e-7).float().contiguous()
     return types.SimpleNamespace(poses=p.poses.clone(), rig=rig, disps=disps, disps_sens=sens,
-                                 intrinsics=p.intrinsics.clone(), targets=targets.contiguous(), weights=weights,
+                                 intrinsics=intr, targets=targets.contiguous(), weights=weights,
                                  ii=di.contiguous(), jj=dj.contiguous(), eta=eta, kx=kx,
                                  disp_damping=disp_damping, depth_active=torch.ones(N * V), t0=p.t0, t1=p.t1,
                                  iterations=2, lm=float(p.lm), ep=float(p.ep), alpha=float(p.alpha), N=N, V=V,

@@ -329,9 +329,10 @@ def camera_cases():
 
 
 RIG = {
-    # name: (outliers, robust_kernel, threshold, n_iters)
-    "rig": (False, None, 1.0, 2),
-    "rig_huber": (True, "huber", 2.0, 3),
+    # name: (outliers, robust_kernel, threshold, n_iters, per-view intrinsics + cross-view terms)
+    "rig": (False, None, 1.0, 2, False),
+    "rig_huber": (True, "huber", 2.0, 3, False),
+    "rig_views": (False, None, 1.0, 2, True),
 }
 
 
@@ -347,8 +348,8 @@ def rig_cases():
     import _graph_buffer_golden as Gd
 
     out = {}
-    for name, (outl, kernel, thr, n_iters) in RIG.items():
-        r = Gd.rig_problem(outliers=outl)
+    for name, (outl, kernel, thr, n_iters, views) in RIG.items():
+        r = Gd.rig_problem(outliers=outl, views=views)
         N, V = r.N, r.V
         H, Wd = r.disps.shape[1:]
         cfg = _Cfg({"dense_disp_alpha": r.alpha, "fused": False, "intrinsics_damping_scale": 1.0,
@@ -376,6 +377,7 @@ def rig_cases():
                             pose_ep=r.ep, motion_only=False, limited_disp=False, optimize_intrinsics=False,
                             optimize_rig_rotation=False, verbose=False)
         out[name] = {"outliers": outl, "kernel": kernel, "threshold": thr, "iterations": n_iters, "n_frames": N,
+                     "views": views,
                      "generic": {"poses": v.poses.clone(), "disps": v.disps.clone().reshape(-1, H, Wd)},
                      "before": {"poses": r.poses.clone()}}
     return out

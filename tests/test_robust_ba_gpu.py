@@ -121,14 +121,15 @@ def _rig_args(r, dev="cuda"):
                 alpha=r.alpha)
 
 
-@pytest.mark.parametrize("name", ["rig", "rig_huber"])
+@pytest.mark.parametrize("name", ["rig", "rig_huber", "rig_views"])
 def test_rig_matches_reference_generic_solver(name):
     """A two-view rig with non-identity extrinsics (tests/_graph_buffer_golden.rig_problem) through
-    vipe_slam_ba_rig against the reference's generic solver on GraphBuffer(n_views=2)."""
+    vipe_slam_ba_rig against the reference's generic solver on GraphBuffer(n_views=2); rig_views
+    adds per-view intrinsics and cross-view terms (source and target views differ)."""
     from vipe_b200.robust_ba import ba_rig
 
     c = G.rig_cases()[name]
-    r = G.rig_problem(outliers=c["outliers"])
+    r = G.rig_problem(outliers=c["outliers"], views=c.get("views", False))
     a = _rig_args(r)
     ba_rig(**a, iterations=c["iterations"], robust_kernel=c["kernel"], threshold=c["threshold"])
     torch.cuda.synchronize()
@@ -156,10 +157,26 @@ def test_rig_differs_from_ignoring_the_rig():
     assert float((a["poses"][:n].cpu() - c["generic"]["poses"][:n]).abs().max()) > 1e-3
 
 
+def test_rig_per_view_intrinsics_are_used():
+    """The per-view case solved with view 0's intrinsics for both views lands far from the
+    generic solver's result (the second view's intrinsics enter the terms)."""
+    from vipe_b200.robust_ba import ba_rig
+
+    c = G.rig_cases()["rig_views"]
+    r = G.rig_problem(views=True)
+    a = _rig_args(r)
+    a["intrinsics"] = a["intrinsics"][0].contiguous()
+    ba_rig(**a, iterations=c["iterations"])
+    torch.cuda.synchronize()
+    n = c["n_frames"]
+    assert float((a["poses"][:n].cpu() - c["generic"]["poses"][:n]).abs().max()) > 1e-3
+
+
 class _FakeBuffer:
     """The GraphBuffer attributes the drop-in reads (single frame store, views, rig, config),
-    with expand_edge_multiview restated from vipe/slam/components/buffer.py:304-362 (no cross
-    edges: ii != jj)."""
+    with expand_edge_multiview restated from vipe/slam/components/buffer.py:304-362 (ii == jj
+    pairs become the cross-view terms (k, q) -> (k, (q + 1) % n_views) of the default
+    cross_view_idx, buffer.py:63-64)."""
 
     def __init__(self, r, kernel, thr):
         import types
@@ -172,7 +189,8 @@ class _FakeBuffer:
         self.rig = r.rig.cuda()
         self.disps = r.disps.reshape(N, V, H, W).cuda().contiguous()
         self.disps_sens = r.disps_sens.reshape(N, V, H, W).cuda().contiguous()
-        self.intrinsics = (r.intrinsics * 8).repeat(V, 1).cuda()
+        intr = r.intrinsics if r.intrinsics.dim() == 2 else r.intrinsics.reshape(1, 4).repeat(V, 1)
+        self.intrinsics = (intr * 8).cuda()
         self.tstamp = torch.arange(N).cuda()
 
         class Cfg(dict):
@@ -187,18 +205,19 @@ class _FakeBuffer:
         pi = ii.reshape(-1, 1).repeat(1, V)
         qj = torch.arange(V, device=ii.device).repeat(jj.shape[0], 1)
         pj = jj.reshape(-1, 1).repeat(1, V)
+        qj = torch.where(pi == pj, (qj + 1) % V, qj)
         di, dj = pi * V + qi, pj * V + qj
         return pi.reshape(-1), qi.reshape(-1), di.reshape(-1), pj.reshape(-1), qj.reshape(-1), dj.reshape(-1)
 
 
-@pytest.mark.parametrize("name", ["rig", "rig_huber"])
+@pytest.mark.parametrize("name", ["rig", "rig_huber", "rig_views"])
 def test_graph_buffer_drop_in_on_a_rig(name):
     """vipe_b200.graph_buffer_ba.bundle_adjustment called the way GraphBuffer is (keyframe edges,
     expanded targets (E * V, H*W, 2), disp_damping per depth frame) against the same fixtures."""
     from vipe_b200.graph_buffer_ba import bundle_adjustment
 
     c = G.rig_cases()[name]
-    r = G.rig_problem(outliers=c["outliers"])
+    r = G.rig_problem(outliers=c["outliers"], views=c.get("views", False))
     buf = _FakeBuffer(r, c["kernel"], c["threshold"])
     E = r.targets.shape[0]
     H, W = r.disps.shape[1:]

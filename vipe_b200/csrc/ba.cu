@@ -453,10 +453,10 @@ template <int D, bool kIntr, bool kResidual>
 __device__ __forceinline__ void linearize_d(const EdgeTf& T, bool stereo, float fx, float fy, float cx, float cy,
                                             float u, float v, float disp, float wu, float wv, float tu, float tv,
                                             float act, float iscale, typename LinOf<D>::T& L,
-                                            const RobustSpec rb = RobustSpec{}) {
+                                            const RobustSpec rb = RobustSpec{}, const SrcIntr si = SrcIntr{}) {
     if constexpr (D == 6)
         linearize<kIntr, kResidual>(T.t, T.q, stereo, fx, fy, cx, cy, u, v, disp, wu, wv, tu, tv, act, iscale, L,
-                                    rb);
+                                    rb, si);
     else
         linearize_sim3<kResidual>(T, stereo, fx, fy, cx, cy, u, v, disp, wu, wv, tu, tv, act, L);
 }
@@ -482,7 +482,11 @@ __global__ void __launch_bounds__(kEdgeThreads, (D == 6 && !kIntr) ? 4 : (D == 7
     const bool stereo = a == b;
     EdgeTf Tf;
     edge_tf<D>(A.poses, a, b, Tf);
-    const float fx = A.intr[0], fy = A.intr[1], cx = A.intr[2], cy = A.intr[3];
+    float fx = A.intr[0], fy = A.intr[1], cx = A.intr[2], cy = A.intr[3];
+    SrcIntr si;
+    if constexpr (kExt) {
+        if (io.rb.nview > 1) view_intrinsics(A.intr, io.rb.nview, a, b, fx, fy, cx, cy, si);
+    }
 
     float H[NH], vj[D], fj[D];
     float hf = 0.f, vf = 0.f, en = 0.f;
@@ -503,7 +507,7 @@ __global__ void __launch_bounds__(kEdgeThreads, (D == 6 && !kIntr) ? 4 : (D == 7
         typename LinOf<D>::T L;
         linearize_d<D, kIntr, true>(Tf, stereo, fx, fy, cx, cy, u, v, __ldg(dp + p), __ldg(wu + p),
                                     __ldg(wu + HW + p), __ldg(tu + p), __ldg(tu + HW + p), 1.0f, A.iscale, L,
-                                    kExt ? io.rb : RobustSpec{});
+                                    kExt ? io.rb : RobustSpec{}, si);
         en += L.we[0] * L.r[0] * L.r[0] + L.we[1] * L.r[1] * L.r[1];
 #pragma unroll
         for (int ch = 0; ch < 2; ch++) {
@@ -689,8 +693,10 @@ __device__ __forceinline__ uint32_t sw128_off(int q, int i) {
     return (uint32_t)q * 128u + ((uint32_t)(((i >> 2) ^ q) & 7) << 4) + (uint32_t)(i & 3) * 4u;
 }
 
-template <bool kIntr, int D>
+template <bool kIntr, int D, bool kExt = false>
 __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base, Batch B, float alpha, float iscale) {
+    // kExt: robust reweighting, camera model and per-view intrinsics from io.rb compiled in
+    // (single solves that ask for them); the batched solves run without that code
     BA_BIND(B, base);
     if (w.status[0]) return;
     const FrameArgs A{io.poses, io.disps, io.disps_sens, io.intr, io.targets, io.weights, io.eta, io.depth_active, io.jj,
@@ -854,8 +860,16 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
                         sl = w.edge_slot[e];
                     }
                     typename LinOf<D>::T L;
-                    linearize_d<D, kIntr, true>(Tf, stereo, fx, fy, cx, cy, u, v, disp, w0, w1, t0v, t1v, act,
-                                                A.iscale, L, io.rb);
+                    if constexpr (kExt) {
+                        float fxj = fx, fyj = fy, cxj = cx, cyj = cy;
+                        SrcIntr si;
+                        if (io.rb.nview > 1) view_intrinsics(A.intr, io.rb.nview, k, (int)A.jj[e], fxj, fyj, cxj, cyj, si);
+                        linearize_d<D, kIntr, true>(Tf, stereo, fxj, fyj, cxj, cyj, u, v, disp, w0, w1, t0v, t1v, act,
+                                                    A.iscale, L, io.rb, si);
+                    } else {
+                        linearize_d<D, kIntr, true>(Tf, stereo, fx, fy, cx, cy, u, v, disp, w0, w1, t0v, t1v, act,
+                                                    A.iscale, L);
+                    }
                     const float g0 = L.wd[0] * L.Jz[0], g1 = L.wd[1] * L.Jz[1];
                     csum += g0 * L.Jz[0] + g1 * L.Jz[1];
                     bsum += g0 * L.r[0] + g1 * L.r[1];
@@ -1144,9 +1158,12 @@ __global__ void __launch_bounds__(kWideThreads) ba_frame_wide_kernel(BAPtrs base
                     edge_tf<D>(A.poses, k, b, Tf);
                     const int sl = w.edge_slot[e];
                     PixelLin L;
-                    linearize_d<D, kIntr, true>(Tf, b == k, fx, fy, cx, cy, uu, vv, disp, __ldg(A.weights + o),
+                    float fxj = fx, fyj = fy, cxj = cx, cyj = cy;
+                    SrcIntr si;
+                    if (io.rb.nview > 1) view_intrinsics(A.intr, io.rb.nview, k, b, fxj, fyj, cxj, cyj, si);
+                    linearize_d<D, kIntr, true>(Tf, b == k, fxj, fyj, cxj, cyj, uu, vv, disp, __ldg(A.weights + o),
                                                 __ldg(A.weights + o + HW), __ldg(A.targets + o),
-                                                __ldg(A.targets + o + HW), act, A.iscale, L, io.rb);
+                                                __ldg(A.targets + o + HW), act, A.iscale, L, io.rb, si);
                     const float g0 = L.wd[0] * L.Jz[0], g1 = L.wd[1] * L.Jz[1];
                     csum += g0 * L.Jz[0] + g1 * L.Jz[1];
                     bsum += g0 * L.r[0] + g1 * L.r[1];
@@ -2091,8 +2108,14 @@ __global__ void __launch_bounds__(256, (D == 6 && !kIntr) ? 8 : (D == 7 ? 6 : 3)
             const float* tp = A.targets + (size_t)e * 2 * HW;
             const RobustSpec rb = kExt ? io.rb : RobustSpec{};
             const bool rob = rb.kind != 0;
-            linearize_d<D, false, false>(Tf, k == b, fx, fy, cx, cy, u, v, disp, __ldg(wp + p), __ldg(wp + HW + p),
-                                         rob ? __ldg(tp + p) : 0.f, rob ? __ldg(tp + HW + p) : 0.f, act, 1.f, L, rb);
+            float fxj = fx, fyj = fy, cxj = cx, cyj = cy;
+            SrcIntr si;
+            if constexpr (kExt) {
+                if (rb.nview > 1) view_intrinsics(A.intr, rb.nview, k, b, fxj, fyj, cxj, cyj, si);
+            }
+            linearize_d<D, false, false>(Tf, k == b, fxj, fyj, cxj, cyj, u, v, disp, __ldg(wp + p), __ldg(wp + HW + p),
+                                         rob ? __ldg(tp + p) : 0.f, rob ? __ldg(tp + HW + p) : 0.f, act, 1.f, L, rb,
+                                         si);
 #pragma unroll
             for (int ch = 0; ch < 2; ch++) {
                 const float g = L.wd[ch] * L.Jz[ch];
@@ -2192,6 +2215,10 @@ int ensure_attributes() {
         g_wide_grid[dev] = sms * std::max(1, std::min(2, std::min(per_sm_a, per_sm_b)));
         VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<true, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            kFrameSmem));
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<true, 6, true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, kFrameSmem));
+        VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<false, 6, true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, kFrameSmem));
         VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<false, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            kFrameSmem));
         VIPE_CUDA_TRY(cudaFuncSetAttribute(ba_frame_kernel<false, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2229,7 +2256,7 @@ int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const 
     const Batch per_graph{d_table, nullptr, G};
     auto grid = [&](int k) { return (unsigned)geo.off[k][G]; };
     const bool intr = a.intr != 0;
-    const bool ext = base.rb.kind != 0 || base.rb.cam != 0;
+    const bool ext = base.rb.kind != 0 || base.rb.cam != 0 || base.rb.nview > 1;
     const int with_frames = a.motion_only ? 0 : 1;
     if (geo.any_edges) {
         {
@@ -2261,6 +2288,12 @@ int launch_linearize_solve(const Geometry& geo, const GraphDesc* d_table, const 
         VIPE_PROF("ba_frame", st);
         if (geo.dof == 7)
             ba_frame_kernel<false, 7><<<grid(kOffFrame), kFrameThreads, kFrameSmem, st>>>(
+                base, batch_of(geo, d_table, d_off, kOffFrame), a.alpha, a.iscale);
+        else if (ext && intr)
+            ba_frame_kernel<true, 6, true><<<grid(kOffFrame), kFrameThreads, kFrameSmem, st>>>(
+                base, batch_of(geo, d_table, d_off, kOffFrame), a.alpha, a.iscale);
+        else if (ext)
+            ba_frame_kernel<false, 6, true><<<grid(kOffFrame), kFrameThreads, kFrameSmem, st>>>(
                 base, batch_of(geo, d_table, d_off, kOffFrame), a.alpha, a.iscale);
         else if (intr)
             ba_frame_kernel<true, 6><<<grid(kOffFrame), kFrameThreads, kFrameSmem, st>>>(
@@ -2371,7 +2404,7 @@ static int launch_update(const Geometry& geo, const GraphDesc* d_table, const in
     const bool intr = a.intr != 0;
     if (!a.motion_only && grid(kOffFrame) > 0) {
         VIPE_PROF("ba_backsub", st);
-        const bool ext = base.rb.kind != 0 || base.rb.cam != 0;
+        const bool ext = base.rb.kind != 0 || base.rb.cam != 0 || base.rb.nview > 1;
         if (geo.dof == 7)
             ba_backsub_kernel<false, 7><<<grid(kOffFrame), 256, 0, st>>>(base, batch_of(geo, d_table, d_off, kOffFrame));
         else if (ext && intr)
@@ -2813,6 +2846,7 @@ extern "C" int vipe_slam_ba_rig(float* poses_io, const float* rig, int n_views, 
     bv.rb.c = robust_kind ? robust_threshold : 1.f;
     bv.rb.cam = camera_model;
     bv.rb.k1 = camera_model == 1 ? distortion : 0.f;
+    bv.rb.nview = V > 1 ? V : 0;  // intrinsics: one row per view, depth frame k * V + q uses row q
     bv.exact_backsub = 1;
     BAPtrs bk{poses_io, nullptr, const_cast<float*>(intrinsics), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
               nullptr, dx_out, nullptr, nullptr, dev_status, iterations, 0};

@@ -148,14 +148,43 @@ struct PixelLin {
 //                   max(sqrt(c^2 mu (mu+1) / r^2) - mu, 0); mu = +inf: the hard TLS 1{r^2 < c^2}
 // kind 0: no reweighting.
 // Also carried here: the camera model of the frames (cam 0 pinhole; cam 1 the unified
-// (MEI) model of vipe/utils/cameras.py:220-330 with distortion k1, fx fy cx cy as for pinhole).
+// (MEI) model of vipe/utils/cameras.py:220-330 with distortion k1, fx fy cx cy as for pinhole),
+// and per-view intrinsics of a multi-view rig: nview > 1 means the intrinsics array holds
+// nview rows (fx, fy, cx, cy) and depth frame f is seen by view f % nview (the generic
+// solver's intrinsics (Q, 4) indexed by the terms' rig indices, vipe/slam/ba/terms.py:175-206).
 struct RobustSpec {
     int kind = 0;
     float c = 1.0f;
     float mu = 1.0f;
     int cam = 0;
     float k1 = 0.0f;
+    int nview = 0;
 };
+
+// Intrinsics of the source view of a term when they differ from the target view's (per-view
+// intrinsics of a rig): the pixel is unprojected with these, projected with the target's
+// (the fx, fy, cx, cy arguments of the linearisation).  on == 0: one camera for both.
+struct SrcIntr {
+    int on = 0;
+    float fx = 1.0f, fy = 1.0f, cx = 0.0f, cy = 0.0f;
+};
+
+// per-view intrinsics: the target view's row of depth frame b into fx..cy and the source
+// view's row of depth frame a into si
+__device__ __forceinline__ void view_intrinsics(const float* intr, int nview, int a, int b, float& fx, float& fy,
+                                                float& cx, float& cy, SrcIntr& si) {
+    const float* ki = intr + 4 * (a % nview);
+    const float* kj = intr + 4 * (b % nview);
+    fx = kj[0];
+    fy = kj[1];
+    cx = kj[2];
+    cy = kj[3];
+    si.on = 1;
+    si.fx = ki[0];
+    si.fy = ki[1];
+    si.cx = ki[2];
+    si.cy = ki[3];
+}
 
 __device__ __forceinline__ float robust_weight(const RobustSpec& rb, float r) {
     if (rb.kind == 1) {
@@ -188,9 +217,10 @@ template <bool kResidual>
 __device__ __forceinline__ void linearize_mei(const float* tij, const float* qij, bool stereo, float fx, float fy,
                                               float cx, float cy, float u, float v, float disp, float wu_in,
                                               float wv_in, float tu, float tv, float act, PixelLin& L,
-                                              const RobustSpec& rb) {
+                                              const RobustSpec& rb, const SrcIntr& si) {
     const float k1 = rb.k1;
-    const float ub = (u - cx) / fx, vb = (v - cy) / fy;
+    const float ub = si.on ? (u - si.cx) / si.fx : (u - cx) / fx;
+    const float vb = si.on ? (v - si.cy) / si.fy : (v - cy) / fy;
     const float r2 = ub * ub + vb * vb;
     const float qq = sqrtf(1.0f + (1.0f - k1 * k1) * r2);
     const float fac = (k1 + qq) / (1.0f + r2);
@@ -248,12 +278,14 @@ template <bool kIntr, bool kResidual>
 __device__ __forceinline__ void linearize(const float* tij, const float* qij, bool stereo, float fx, float fy,
                                           float cx, float cy, float u, float v, float disp, float wu_in, float wv_in,
                                           float tu, float tv, float act, float iscale, PixelLin& L,
-                                          const RobustSpec rb = RobustSpec{}) {
+                                          const RobustSpec rb = RobustSpec{}, const SrcIntr si = SrcIntr{}) {
     if (rb.cam == 1) {
-        linearize_mei<kResidual>(tij, qij, stereo, fx, fy, cx, cy, u, v, disp, wu_in, wv_in, tu, tv, act, L, rb);
+        linearize_mei<kResidual>(tij, qij, stereo, fx, fy, cx, cy, u, v, disp, wu_in, wv_in, tu, tv, act, L, rb, si);
         return;
     }
-    float Xi[4] = {(u - cx) / fx, (v - cy) / fy, 1.0f, disp};
+    // (the focal derivative below assumes one camera: the rig solve has no intrinsics block)
+    float Xi[4] = {si.on ? (u - si.cx) / si.fx : (u - cx) / fx, si.on ? (v - si.cy) / si.fy : (v - cy) / fy, 1.0f,
+                   disp};
     float Xj[4];
     act_h(tij, qij, Xi, Xj);
     const float x = Xj[0], y = Xj[1], h = Xj[3];

@@ -6,14 +6,14 @@ kernel (buffer.py:387-404, 541-545); everything else goes to the generic torch s
 (vipe/slam/ba/solver.py, terms.py).  `bundle_adjustment` here is a drop-in for that method
 that runs those configurations on this library's fused kernels:
 
-  * multi-view rigs (n_views > 1, fixed rig extrinsics): vipe_slam_ba_rig;
+  * multi-view rigs (n_views > 1, fixed rig extrinsics, per-view intrinsics): vipe_slam_ba_rig;
   * robust kernels (Huber, Tukey, GNC-TLS with its mu schedule) and the MEI camera:
     vipe_slam_ba_extended_generic / vipe_slam_ba_rig;
   * single-view pinhole buffers with focal optimisation as before.
 
-It raises for what it does not cover: optimize_rig_rotation, views whose intrinsics differ,
-focal/distortion optimisation with MEI or with a rig, panorama cameras, and sparse tracks
-together with a robust kernel.  Install with
+It raises for what it does not cover: optimize_rig_rotation, MEI views whose distortion
+differs, focal/distortion optimisation with MEI or with a rig, panorama cameras, and sparse
+tracks together with a robust kernel.  Install with
 
     GraphBuffer.bundle_adjustment = vipe_b200.graph_buffer_ba.bundle_adjustment
 """
@@ -72,8 +72,8 @@ def bundle_adjustment(self, target, weight, disp_damping, ii, jj, t0, t1, n_iter
     target = target.reshape(n_terms, H, W, 2).permute(0, 3, 1, 2).contiguous()
     weight = weight.reshape(n_terms, H, W, 2).permute(0, 3, 1, 2).contiguous()
     intr = self.intrinsics
-    if V > 1 and not torch.allclose(intr[1:], intr[:1].expand_as(intr[1:])):
-        raise RuntimeError("fused BA: the views' intrinsics differ")
+    if cam == "mei" and V > 1 and not torch.allclose(intr[1:, 4], intr[:1, 4].expand_as(intr[1:, 4])):
+        raise RuntimeError("fused BA: the views' MEI distortions differ")
     k1 = float(intr[0, 4]) if cam == "mei" else 0.0
     intr8 = (intr[0, :4] / 8.0).contiguous()
     nv = self.disps.shape[0] * V
@@ -105,7 +105,8 @@ def bundle_adjustment(self, target, weight, disp_damping, ii, jj, t0, t1, n_iter
             raise RuntimeError("fused BA: intrinsics optimisation with a rig is not supported")
         if torch.any(di == dj):
             raise RuntimeError("fused BA: terms within one depth frame are not supported")
-        R.ba_rig(self.poses, self.rig.float().contiguous(), disps, intr8, sens, target, weight, eta, di.contiguous(),
+        intr8v = (intr[:, :4] / 8.0).float().contiguous()  # one row per view
+        R.ba_rig(self.poses, self.rig.float().contiguous(), disps, intr8v, sens, target, weight, eta, di.contiguous(),
                  dj.contiguous(), depth_active, t0, t1, iters, pose_damping, pose_ep, motion_only, alpha, verbose,
                  robust_kernel=kernel, threshold=thr, mu_schedule=sched, camera_type=cam, distortion=k1)
     self.disps.clamp_(min=0.001)

@@ -116,8 +116,10 @@ def ba_rig(poses, rig, disps, intrinsics, disps_sens, targets, weights, eta, ii,
            lm, ep, motion_only, alpha, compute_energy=False, robust_kernel=None, threshold=1.0, mu_schedule=None,
            camera_type=None, distortion=0.0):
     """Fused BA over a multi-view rig (vipe_slam_ba_rig): keyframe poses (N, 7), fixed rig
-    extrinsics (V, 7), depth frames (N * V, H, W) indexed k * V + q, and per-term source/target
-    depth-frame indices ii, jj.  Returns [dx (t1 - t0, 6), dz or None, energy]."""
+    extrinsics (V, 7), depth frames (N * V, H, W) indexed k * V + q, per-term source/target
+    depth-frame indices ii, jj, and intrinsics (4,) shared by the views or (V, 4) per view (a
+    term unprojects with its source view's row and projects with its target view's).
+    Returns [dx (t1 - t0, 6), dz or None, energy]."""
     import ctypes
 
     name = None if robust_kernel is None else str(robust_kernel).lower()
@@ -146,6 +148,10 @@ def ba_rig(poses, rig, disps, intrinsics, disps_sens, targets, weights, eta, ii,
     N, V = poses.shape[0], rig.shape[0]
     if disps.shape[0] != N * V:
         raise RuntimeError("disps must hold num_keyframes * n_views depth frames")
+    if intrinsics.numel() == 4:
+        intrinsics = intrinsics.reshape(1, 4).expand(V, 4).contiguous()
+    elif tuple(intrinsics.shape) != (V, 4):
+        raise RuntimeError("intrinsics must be (4,) or (n_views, 4)")
     t0, t1 = int(t0), int(t1)
     _, ht, wd = disps.shape
     num_edges, num_kx = ii.shape[0], eta.shape[0]
