@@ -424,9 +424,38 @@ struct PixJ {
     float P[3];
     float iz;
     float gf[2][3];
-    float J[2][2 * D];  // [source D | target D] per channel
+    float rg[2][3];     // M^T grad f per channel
+    float x0, x1, w;    // the pixel's ray (x0, x1, 1) and inverse depth
     float jz[2];
 };
+
+// element n of channel ch's Jacobian row [source D | target D], formed from the stored
+// gradient (the rows are cheap to re-form; holding all 4D of them costs registers)
+template <int D>
+__device__ __forceinline__ float jrow(const PixJ<D>& o, int ch, int n) {
+    const float* g = o.gf[ch];
+    const float* rg = o.rg[ch];
+    if (n < D) {
+        switch (n) {
+            case 0: return -o.w * rg[0];
+            case 1: return -o.w * rg[1];
+            case 2: return -o.w * rg[2];
+            case 3: return -(o.x1 * rg[2] - rg[1]);
+            case 4: return -(rg[0] - o.x0 * rg[2]);
+            case 5: return -(o.x0 * rg[1] - o.x1 * rg[0]);
+            default: return -(o.x0 * rg[0] + o.x1 * rg[1] + rg[2]);  // Sim3 scale
+        }
+    }
+    switch (n - D) {
+        case 0: return g[0] * o.w;
+        case 1: return g[1] * o.w;
+        case 2: return g[2] * o.w;
+        case 3: return o.P[1] * g[2] - o.P[2] * g[1];
+        case 4: return o.P[2] * g[0] - o.P[0] * g[2];
+        case 5: return o.P[0] * g[1] - o.P[1] * g[0];
+        default: return g[0] * o.P[0] + g[1] * o.P[1] + g[2] * o.P[2];  // Sim3 scale
+    }
+}
 
 template <int D>
 __device__ __forceinline__ bool pix_jac(const float* M0, const float* X, float fx, float fy, PixJ<D>& o) {
@@ -437,30 +466,14 @@ __device__ __forceinline__ bool pix_jac(const float* M0, const float* X, float f
     o.iz = iz;
     o.gf[0][0] = fx * iz; o.gf[0][1] = 0.f; o.gf[0][2] = -fx * o.P[0] * iz * iz;
     o.gf[1][0] = 0.f; o.gf[1][1] = fy * iz; o.gf[1][2] = -fy * o.P[1] * iz * iz;
-    const float W = X[3];
+    o.x0 = X[0];
+    o.x1 = X[1];
+    o.w = X[3];
 #pragma unroll
     for (int ch = 0; ch < 2; ch++) {
         const float* g = o.gf[ch];
-        float rg[3];  // M^T grad f
 #pragma unroll
-        for (int n = 0; n < 3; n++) rg[n] = M0[n] * g[0] + M0[4 + n] * g[1] + M0[8 + n] * g[2];
-        float* J = o.J[ch];
-        J[0] = -W * rg[0];
-        J[1] = -W * rg[1];
-        J[2] = -W * rg[2];
-        J[3] = -(X[1] * rg[2] - 1.f * rg[1]);
-        J[4] = -(1.f * rg[0] - X[0] * rg[2]);
-        J[5] = -(X[0] * rg[1] - X[1] * rg[0]);
-        J[D + 0] = g[0] * W;
-        J[D + 1] = g[1] * W;
-        J[D + 2] = g[2] * W;
-        J[D + 3] = o.P[1] * g[2] - o.P[2] * g[1];
-        J[D + 4] = o.P[2] * g[0] - o.P[0] * g[2];
-        J[D + 5] = o.P[0] * g[1] - o.P[1] * g[0];
-        if constexpr (D == 7) {
-            J[6] = -(X[0] * rg[0] + X[1] * rg[1] + rg[2]);
-            J[13] = g[0] * o.P[0] + g[1] * o.P[1] + g[2] * o.P[2];
-        }
+        for (int n = 0; n < 3; n++) o.rg[ch][n] = M0[n] * g[0] + M0[4 + n] * g[1] + M0[8 + n] * g[2];
         o.jz[ch] = g[0] * M0[3] + g[1] * M0[7] + g[2] * M0[11];
     }
     return true;
@@ -688,7 +701,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
         for (int ch = 0; ch < 2; ch++) {
             const float g = act * act * wc[ch] * J.jz[ch];
 #pragma unroll
-            for (int n = 0; n < D; n++) out[n] += g * J.J[ch][D + n];
+            for (int n = 0; n < D; n++) out[n] += g * jrow<D>(J, ch, D + n);
         }
     };
 
@@ -720,7 +733,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                     float jl = 0.f, jd = 0.f, jdt = 0.f;
 #pragma unroll
                     for (int n = 0; n < D; n++) {
-                        const float jn = J.J[ch][D + n];
+                        const float jn = jrow<D>(J, ch, D + n);
                         jl += jn * Eq[OT + n];
                         jd += jn * Eq[OT + D + n];
                         jdt += jn * Eq[OT + 2 * D + n];
@@ -730,9 +743,9 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                     eDt += g * jdt;
 #pragma unroll
                     for (int n = 0; n < D; n++) {
-                        Es[n] += g * J.J[ch][n];
-                        if (stereo) Es[n] += g * J.J[ch][D + n];
-                        else tv[n] += g * J.J[ch][D + n];
+                        Es[n] += g * jrow<D>(J, ch, n);
+                        if (stereo) Es[n] += g * jrow<D>(J, ch, D + n);
+                        else tv[n] += g * jrow<D>(J, ch, D + n);
                     }
                 }
                 if (!stereo && grp[q] < 0)
@@ -854,7 +867,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                         for (int n = 0; n < D; n++) {
                             tv[n] = 0.f;
 #pragma unroll
-                            for (int ch = 0; ch < 2; ch++) tv[n] += act * act * wc[ch] * J.jz[ch] * J.J[ch][D + n];
+                            for (int ch = 0; ch < 2; ch++) tv[n] += act * act * wc[ch] * J.jz[ch] * jrow<D>(J, ch, D + n);
                         }
                     } else {
                         float t2[D];
@@ -889,7 +902,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                     lds_row<3 * D>(Eqv + OT, wv);
 #pragma unroll
                     for (int n = 0; n < D; n++) {
-                        const float jn = J.J[ch][D + n];
+                        const float jn = jrow<D>(J, ch, D + n);
                         ft[0] += jn * wv[n];
                         ft[1] += jn * wv[D + n];
                         ft[2] += jn * wv[2 * D + n];
@@ -900,7 +913,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                     lds_row<D2>(Eqv + OM, dmp);
 #pragma unroll
                     for (int n = 0; n < D2; n++) {
-                        const float jn = J.J[ch][n];
+                        const float jn = jrow<D>(J, ch, n);
                         fb += jn * beta[n];
                         fg += dmp[n] * jn * jn;
                     }
@@ -938,7 +951,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                     float dv[D2];
                     lds_row<D2>(Eqv + OM, dv);
 #pragma unroll
-                    for (int n = 0; n < D2; n++) ud[n] = cE * beta[n] + cB * dv[n] * J.J[ch][n];
+                    for (int n = 0; n < D2; n++) ud[n] = cE * beta[n] + cB * dv[n] * jrow<D>(J, ch, n);
                     lds_row<D2>(Eqv + OD, dv);
 #pragma unroll
                     for (int n = 0; n < D2; n++) ud[n] += c1 * dv[n];
