@@ -156,7 +156,12 @@ int vipe_slam_ba_extended_generic(float* poses_io, float* disps_io, float* intri
  * d_i = p_i * n_views + q_i into frame (p_j, q_j) through R_qj^-1 G_pj G_pi^-1 R_qi); the
  * reference's fused path refuses n_views > 1 and non-identity rigs (buffer.py:387-404).
  *   poses_io (num_keyframes, 7) keyframe poses G (updated in the window [t0, t1));
- *   rig (n_views, 7) fixed extrinsics R_q (cam-to-central, [tx ty tz qx qy qz qw]);
+ *   rig (n_views, 7) extrinsics R_q (cam-to-central, [tx ty tz qx qy qz qw]); fixed, or with
+ *     optimize_rig_rotation the rotations of views 1..n_views-1 are optimised and written back
+ *     (the generic solver's rig group: 6-DoF rig steps, minus the pose Jacobians, damping
+ *     rig_lm * diag + rig_ep, view 0 fixed, only the rotation of a step applied,
+ *     buffer.py:668-673 and retractor.py:34-38; every (keyframe, view) is then an unknown of
+ *     the virtual solve, so num_keyframes * n_views <= 1024);
  *   disps_io, disps_sens (num_keyframes * n_views, ht, wd), depth_active (num_keyframes * n_views);
  *   ii, jj: source and target depth-frame indices (k * n_views + q) of the num_edges terms,
  *     ii != jj; eta (num_kx, ht*wd) over kx = unique(arange(t0 n_views, t1 n_views) ++ ii);
@@ -168,15 +173,15 @@ int vipe_slam_ba_extended_generic(float* poses_io, float* disps_io, float* intri
  * Generic-solver back-substitution (rows of pose t0 kept).  Limits: n_views * (t1 - t0) <= 1024.
  * Workspace: vipe_slam_ba_rig_workspace_size. */
 size_t vipe_slam_ba_rig_workspace_size(int num_keyframes, int n_views, int ht, int wd, int num_edges, int num_kx,
-                                       int t0, int t1);
-int vipe_slam_ba_rig(float* poses_io, const float* rig, int n_views, float* disps_io, const float* intrinsics,
+                                       int t0, int t1, int optimize_rig_rotation);
+int vipe_slam_ba_rig(float* poses_io, float* rig, int n_views, float* disps_io, const float* intrinsics,
                      const float* disps_sens, const float* targets, const float* weights, const float* eta,
                      const int64_t* ii, const int64_t* jj, const float* depth_active, int num_keyframes, int ht,
                      int wd, int num_edges, int num_kx, int t0, int t1, int iterations, float lm, float ep,
                      int motion_only, float alpha, int compute_energy, float* dx_out, float* dz_out,
                      float* energy_out, int robust_kind, float robust_threshold, const float* mu_schedule,
-                     int camera_model, float distortion, void* workspace, size_t workspace_bytes,
-                     int32_t* dev_status, void* stream);
+                     int camera_model, float distortion, int optimize_rig_rotation, float rig_lm, float rig_ep,
+                     void* workspace, size_t workspace_bytes, int32_t* dev_status, void* stream);
 
 /* Replaces slam_ext.ba (reference: csrc/slam_ext/slam.cpp:42-45,
  * geom_kernels.cu:1826-1834): ba_extended with depth_active = 1, no focal

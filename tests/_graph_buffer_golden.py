@@ -179,9 +179,10 @@ def _mat(T):
 
 
 RIG_VIEW1_INTR = (1.07, 0.94, 0.9, -0.6)  # view 1 of the per-view case: fx, fy scale; cx, cy shift
+RIG_ROT_ERR = (0.006, -0.004, 0.005)  # rig-rotation case: view 1's initial rotation error (axis-angle)
 
 
-def rig_problem(outliers=False, views=False):
+def rig_problem(outliers=False, views=False, rig_error=False):
     """A two-view rig built from config 0 (deterministic, CPU): keyframe poses, rig (2, 7), depth
     frames k * 2 + q (view 1: 0.9 x view 0), the expanded terms of config 0's edges (edge-major,
     view-minor, as GraphBuffer.expand_edge_multiview orders them), targets = the reprojection at
@@ -190,7 +191,10 @@ def rig_problem(outliers=False, views=False):
     views=True: per-view intrinsics (view 1: fx, fy scaled and cx, cy shifted by RIG_VIEW1_INTR;
     intrinsics (2, 4)) and two keyframe self-pairs (t0, t0) and (t0 + 1, t0 + 1), which expand
     to cross-view terms (k, q) -> (k, (q + 1) % 2) as GraphBuffer's default cross_view_idx does,
-    so that source and target views (and intrinsics) differ within a term."""
+    so that source and target views (and intrinsics) differ within a term.
+    rig_error=True: the returned rig (the solve's initial value) has view 1 rotated by
+    RIG_ROT_ERR away from the rig the targets were made with (rig_true), for the solves that
+    optimise the rig rotation."""
     import types
 
     from vipe_b200 import workloads as W
@@ -245,7 +249,18 @@ def rig_problem(outliers=False, views=False):
     disp_damping = ((p.eta.double() - 1e-7) / 0.2).float()  # per keyframe; both views share it
     eta_frames = disp_damping.repeat_interleave(V, 0)  # (N * V, H*W) in frame order
     eta = (0.2 * eta_frames[kx] + 1e-7).float().contiguous()
-    return types.SimpleNamespace(poses=p.poses.clone(), rig=rig, disps=disps, disps_sens=sens,
+    rig_true = rig
+    if rig_error:
+        rig = rig.clone()
+        e = _quat_of_aa(RIG_ROT_ERR)
+        q1 = rig[1, 3:].double()
+        # quaternion product e (x) q1: view 1's rotation with the error applied on the left
+        x1, y1, z1, w1 = q1.tolist()
+        x0, y0, z0, w0 = e
+        rig[1, 3:] = torch.tensor([w0 * x1 + x0 * w1 + y0 * z1 - z0 * y1, w0 * y1 - x0 * z1 + y0 * w1 + z0 * x1,
+                                   w0 * z1 + x0 * y1 - y0 * x1 + z0 * w1, w0 * w1 - x0 * x1 - y0 * y1 - z0 * z1],
+                                  dtype=rig.dtype)
+    return types.SimpleNamespace(poses=p.poses.clone(), rig=rig, rig_true=rig_true, disps=disps, disps_sens=sens,
                                  intrinsics=intr, targets=targets.contiguous(), weights=weights,
                                  ii=di.contiguous(), jj=dj.contiguous(), eta=eta, kx=kx,
                                  disp_damping=disp_damping, depth_active=torch.ones(N * V), t0=p.t0, t1=p.t1,

@@ -329,10 +329,12 @@ def camera_cases():
 
 
 RIG = {
-    # name: (outliers, robust_kernel, threshold, n_iters, per-view intrinsics + cross-view terms)
-    "rig": (False, None, 1.0, 2, False),
-    "rig_huber": (True, "huber", 2.0, 3, False),
-    "rig_views": (False, None, 1.0, 2, True),
+    # name: (outliers, robust_kernel, threshold, n_iters, per-view intrinsics + cross-view terms,
+    #        rig rotation optimised from a perturbed initial rig)
+    "rig": (False, None, 1.0, 2, False, False),
+    "rig_huber": (True, "huber", 2.0, 3, False, False),
+    "rig_views": (False, None, 1.0, 2, True, False),
+    "rig_rot": (False, None, 1.0, 3, False, True),
 }
 
 
@@ -348,8 +350,8 @@ def rig_cases():
     import _graph_buffer_golden as Gd
 
     out = {}
-    for name, (outl, kernel, thr, n_iters, views) in RIG.items():
-        r = Gd.rig_problem(outliers=outl, views=views)
+    for name, (outl, kernel, thr, n_iters, views, rig_rot) in RIG.items():
+        r = Gd.rig_problem(outliers=outl, views=views, rig_error=rig_rot)
         N, V = r.N, r.V
         H, Wd = r.disps.shape[1:]
         cfg = _Cfg({"dense_disp_alpha": r.alpha, "fused": False, "intrinsics_damping_scale": 1.0,
@@ -375,9 +377,9 @@ def rig_cases():
         v.bundle_adjustment(target=target, weight=weight, disp_damping=disp_damping, ii=r.pi[::V].clone(),
                             jj=r.pj[::V].clone(), t0=r.t0, t1=r.t1, n_iters=n_iters, pose_damping=r.lm,
                             pose_ep=r.ep, motion_only=False, limited_disp=False, optimize_intrinsics=False,
-                            optimize_rig_rotation=False, verbose=False)
+                            optimize_rig_rotation=rig_rot, verbose=False)
         out[name] = {"outliers": outl, "kernel": kernel, "threshold": thr, "iterations": n_iters, "n_frames": N,
-                     "views": views,
+                     "views": views, "rig_rot": rig_rot, "rig": v.rig.clone(), "rig_before": r.rig.clone(),
                      "generic": {"poses": v.poses.clone(), "disps": v.disps.clone().reshape(-1, H, Wd)},
                      "before": {"poses": r.poses.clone()}}
     return out

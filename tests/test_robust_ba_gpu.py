@@ -121,18 +121,27 @@ def _rig_args(r, dev="cuda"):
                 alpha=r.alpha)
 
 
-@pytest.mark.parametrize("name", ["rig", "rig_huber", "rig_views"])
+@pytest.mark.parametrize("name", ["rig", "rig_huber", "rig_views", "rig_rot"])
 def test_rig_matches_reference_generic_solver(name):
     """A two-view rig with non-identity extrinsics (tests/_graph_buffer_golden.rig_problem) through
     vipe_slam_ba_rig against the reference's generic solver on GraphBuffer(n_views=2); rig_views
-    adds per-view intrinsics and cross-view terms (source and target views differ)."""
+    adds per-view intrinsics and cross-view terms (source and target views differ); rig_rot
+    starts from a rotated view-1 rig and optimises the rig rotation (optimize_rig_rotation)."""
     from vipe_b200.robust_ba import ba_rig
 
     c = G.rig_cases()[name]
-    r = G.rig_problem(outliers=c["outliers"], views=c.get("views", False))
+    rot = c.get("rig_rot", False)
+    r = G.rig_problem(outliers=c["outliers"], views=c.get("views", False), rig_error=rot)
     a = _rig_args(r)
-    ba_rig(**a, iterations=c["iterations"], robust_kernel=c["kernel"], threshold=c["threshold"])
+    ba_rig(**a, iterations=c["iterations"], robust_kernel=c["kernel"], threshold=c["threshold"],
+           optimize_rig_rotation=rot)
     torch.cuda.synchronize()
+    if rot:
+        dr = float((a["rig"].cpu() - c["rig"]).abs().max())
+        moved_r = float((c["rig"] - c["rig_before"]).abs().max())
+        print(f"{name}: rig {dr:.2e} (moved {moved_r:.2e})")
+        assert dr <= 2e-4 < moved_r
+        assert float((a["rig"][0].cpu() - c["rig"][0]).abs().max()) == 0.0  # view 0 fixed
     n = c["n_frames"]
     g = c["generic"]
     dp = float((a["poses"][:n].cpu() - g["poses"][:n]).abs().max())
@@ -210,14 +219,15 @@ class _FakeBuffer:
         return pi.reshape(-1), qi.reshape(-1), di.reshape(-1), pj.reshape(-1), qj.reshape(-1), dj.reshape(-1)
 
 
-@pytest.mark.parametrize("name", ["rig", "rig_huber", "rig_views"])
+@pytest.mark.parametrize("name", ["rig", "rig_huber", "rig_views", "rig_rot"])
 def test_graph_buffer_drop_in_on_a_rig(name):
     """vipe_b200.graph_buffer_ba.bundle_adjustment called the way GraphBuffer is (keyframe edges,
     expanded targets (E * V, H*W, 2), disp_damping per depth frame) against the same fixtures."""
     from vipe_b200.graph_buffer_ba import bundle_adjustment
 
     c = G.rig_cases()[name]
-    r = G.rig_problem(outliers=c["outliers"], views=c.get("views", False))
+    rot = c.get("rig_rot", False)
+    r = G.rig_problem(outliers=c["outliers"], views=c.get("views", False), rig_error=rot)
     buf = _FakeBuffer(r, c["kernel"], c["threshold"])
     E = r.targets.shape[0]
     H, W = r.disps.shape[1:]
@@ -225,7 +235,9 @@ def test_graph_buffer_drop_in_on_a_rig(name):
     weight = r.weights.permute(0, 2, 3, 1).reshape(E, H * W, 2).cuda()
     dd = r.disp_damping.repeat_interleave(r.V, 0).reshape(r.N * r.V, H, W).cuda()
     bundle_adjustment(buf, target, weight, dd, r.pi[::r.V].cuda(), r.pj[::r.V].cuda(), r.t0, r.t1, c["iterations"],
-                      r.lm, r.ep, False, False, False, False)
+                      r.lm, r.ep, False, False, False, rot)
+    if rot:
+        assert float((buf.rig.cpu() - c["rig"]).abs().max()) <= 2e-4
     torch.cuda.synchronize()
     n = c["n_frames"]
     g = c["generic"]

@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(kIndexThreads)
     }
     for (int f = tid; f < N; f += kIndexThreads) w.flag[f] = 0;
     __syncthreads();
-    for (int t = t0 + tid; t < t1; t += kIndexThreads) w.flag[t] = 1;
+    for (int t = d.kx0 + tid; t < d.kx1; t += kIndexThreads) w.flag[t] = 1;
     for (int e = tid; e < E; e += kIndexThreads) {
         const int64_t a = ii[e], b = jj[e];
         if (a < 0 || a >= N || b < 0 || b >= N) {
@@ -2698,28 +2698,63 @@ __global__ void ba_rig_adjoint_kernel(const float* __restrict__ rig, int V, doub
         }
 }
 
-// S_k = A^T S_v A and b_k = A^T b_v over the window (P keyframes, V views); the focal
-// row and column of S_k are zero (the rig solve keeps the intrinsics fixed)
-__global__ void ba_rig_project_kernel(const double* __restrict__ Hv, const double* __restrict__ bv, int ldv, int P,
-                                      int V, const double* __restrict__ A, double* __restrict__ Hk,
+// S_k = A^T S_v A and b_k = A^T b_v.  Columns of the keyframe system: the P window keyframes
+// (a left step of G_k moves Tv(k, q) by A_q eps_k), then, when the rig is optimised, views
+// 1..V-1 (a left step of R_q moves Tv(k, q) by -A_q delta_q for every keyframe k: the rig
+// Jacobian is minus the pose one, vipe/slam/maths/geom.py:292-294); the last row and column
+// (the fixed intrinsics) stay zero.  Virtual unknowns are the frames [v0, v0 + Pv) of the
+// virtual window (v0 = t0 V without the rig, 0 with it).
+struct RigCols {
+    int P, V, N, t0, v0, Pv, rig;
+    // virtual unknown, sign and view of the c-th contribution to column block cb (-1: none)
+    __device__ int count(int cb) const { return cb < P ? V : N; }
+    __device__ int at(int cb, int c, int& q, double& sg) const {
+        int k;
+        if (cb < P) {
+            k = t0 + cb;
+            q = c;
+            sg = 1.0;
+        } else {
+            k = c;
+            q = cb - P + 1;
+            sg = -1.0;
+        }
+        const int u = k * V + q - v0;
+        return (u >= 0 && u < Pv) ? u : -1;
+    }
+};
+
+__global__ void ba_rig_project_kernel(const double* __restrict__ Hv, const double* __restrict__ bv, int ldv,
+                                      RigCols rc, const double* __restrict__ A, double* __restrict__ Hk,
                                       double* __restrict__ bk, int ldk) {
-    const long n = 6L * P;
+    const long n = 6L * (rc.P + (rc.rig ? rc.V - 1 : 0));
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < (long)ldk * ldk) {
         const long r = i / ldk, c = i % ldk;
         double s = 0.0;
         if (r < n && c < n) {
-            const int a = (int)(r / 6), ir = (int)(r % 6), b = (int)(c / 6), jc = (int)(c % 6);
-            for (int q = 0; q < V; q++) {
-                const double* Aq = A + (size_t)q * 36;
-                for (int q2 = 0; q2 < V; q2++) {
+            const int cb1 = (int)(r / 6), ir = (int)(r % 6), cb2 = (int)(c / 6), jc = (int)(c % 6);
+            const int n1 = rc.count(cb1), n2 = rc.count(cb2);
+            for (int c1 = 0; c1 < n1; c1++) {
+                int q1;
+                double s1;
+                const int u1 = rc.at(cb1, c1, q1, s1);
+                if (u1 < 0) continue;
+                const double* Aq = A + (size_t)q1 * 36;
+                for (int c2 = 0; c2 < n2; c2++) {
+                    int q2;
+                    double s2;
+                    const int u2 = rc.at(cb2, c2, q2, s2);
+                    if (u2 < 0) continue;
                     const double* Aq2 = A + (size_t)q2 * 36;
-                    const double* blk = Hv + (size_t)((a * V + q) * 6) * ldv + (size_t)(b * V + q2) * 6;
+                    const double* blk = Hv + (size_t)(u1 * 6) * ldv + (size_t)u2 * 6;
+                    double acc = 0.0;
                     for (int m = 0; m < 6; m++) {
                         double t = 0.0;
                         for (int nn = 0; nn < 6; nn++) t += blk[(size_t)m * ldv + nn] * Aq2[6 * nn + jc];
-                        s += Aq[6 * m + ir] * t;
+                        acc += Aq[6 * m + ir] * t;
                     }
+                    s += s1 * s2 * acc;
                 }
             }
         }
@@ -2728,23 +2763,52 @@ __global__ void ba_rig_project_kernel(const double* __restrict__ Hv, const doubl
     if (i < ldk) {
         double s = 0.0;
         if (i < n) {
-            const int a = (int)(i / 6), ir = (int)(i % 6);
-            for (int q = 0; q < V; q++)
-                for (int m = 0; m < 6; m++) s += A[(size_t)q * 36 + 6 * m + ir] * bv[(a * V + q) * 6 + m];
+            const int cb = (int)(i / 6), ir = (int)(i % 6);
+            for (int c1 = 0; c1 < rc.count(cb); c1++) {
+                int q;
+                double sg;
+                const int u = rc.at(cb, c1, q, sg);
+                if (u < 0) continue;
+                for (int m = 0; m < 6; m++) s += sg * A[(size_t)q * 36 + 6 * m + ir] * bv[u * 6 + m];
+            }
         }
         bk[i] = s;
     }
 }
 
-// dx_v(a V + q) = A_q dx_k(a)
-__global__ void ba_rig_expand_kernel(const float* __restrict__ dxk, const double* __restrict__ A, int P, int V,
+// dx_v(k V + q) = A_q (dx_k(k) [k in the window] - delta_q [q >= 1, rig optimised]) over the
+// virtual unknowns; delta from the keyframe solve's solution (rows 6P..), zero if it failed
+__global__ void ba_rig_expand_kernel(const float* __restrict__ dxk, const double* __restrict__ xk,
+                                     const int* __restrict__ fail_k, const double* __restrict__ A, RigCols rc,
                                      float* __restrict__ dxv) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P * V * 6) return;
-    const int av = i / 6, m = i % 6, a = av / V, q = av % V;
+    if (i >= rc.Pv * 6) return;
+    const int u = i / 6, m = i % 6;
+    const int f = u + rc.v0, k = f / rc.V, q = f % rc.V, a = k - rc.t0;
+    const bool rig = rc.rig && q >= 1 && fail_k[0] == 0;
     double s = 0.0;
-    for (int n = 0; n < 6; n++) s += A[(size_t)q * 36 + 6 * m + n] * (double)dxk[6 * a + n];
+    for (int n = 0; n < 6; n++) {
+        double x = (a >= 0 && a < rc.P) ? (double)dxk[6 * a + n] : 0.0;
+        if (rig) x -= xk[6 * rc.P + 6 * (q - 1) + n];
+        s += A[(size_t)q * 36 + 6 * m + n] * x;
+    }
     dxv[i] = (float)s;
+}
+
+// R_q <- Exp([0, delta_q rotation]) R_q for views 1..V-1: the reference's rig retraction keeps the
+// rotation of the step only (RigRotationOnlyRetractor, vipe/slam/maths/retractor.py:34-38)
+__global__ void ba_rig_rotation_retract_kernel(float* __restrict__ rig, const double* __restrict__ xk, int P, int V,
+                                               const int* __restrict__ fail_k, const int* __restrict__ status_v,
+                                               const int* __restrict__ status_k) {
+    const int q = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= V || fail_k[0] || status_v[0] || status_k[0]) return;
+    float xi[6], T[7];
+    for (int n = 0; n < 3; n++) xi[n] = 0.f;
+    for (int n = 3; n < 6; n++) xi[n] = (float)xk[6 * P + 6 * (q - 1) + n];
+    float* pz = rig + (size_t)q * 7;
+    for (int n = 0; n < 7; n++) T[n] = pz[n];
+    retract_pose(xi, T);
+    for (int n = 0; n < 7; n++) pz[n] = T[n];
 }
 
 // G_k <- Exp(dx_k) G_k over the keyframe window
@@ -2768,9 +2832,15 @@ __global__ void ba_rig_desc_kernel(GraphDesc* table, GraphDesc gd) {
     }
 }
 
-static void rig_dims(int N, int V, int ht, int wd, int E, int K, int t0, int t1, Dims& dv, Dims& dk) {
-    dv = make_dims(N * V, ht, wd, E, K, t0 * V, t1 * V, 0, 0, 6, true);
+// Virtual solve: the window's virtual poses, or every virtual pose when the rig is optimised
+// (a rig step moves the virtual poses of fixed keyframes too); kx stays the window's frames plus
+// the edges' sources.  Keyframe solve: 6 rows per window keyframe, then 6 per optimised view.
+static void rig_dims(int N, int V, int ht, int wd, int E, int K, int t0, int t1, int rig_opt, Dims& dv, Dims& dk) {
+    dv = make_dims(N * V, ht, wd, E, K, rig_opt ? 0 : t0 * V, rig_opt ? N * V : t1 * V, 0, 0, 6, true);
+    dv.kx0 = t0 * V;
+    dv.kx1 = t1 * V;
     dk = make_dims(N, ht, wd, 0, 0, t0, t1, 0, 0, 6, true);
+    if (rig_opt) dk.dim += 6 * (V - 1);
 }
 
 template <typename C>
@@ -2784,12 +2854,13 @@ static void rig_carve(C& cv, const Dims& dv, const Dims& dk, GraphDesc& gv, Grap
 }
 
 extern "C" size_t vipe_slam_ba_rig_workspace_size(int num_keyframes, int n_views, int ht, int wd, int num_edges,
-                                                  int num_kx, int t0, int t1) {
+                                                  int num_kx, int t0, int t1, int optimize_rig_rotation) {
     if (n_views < 1 || num_keyframes < 1 || (long)num_keyframes * n_views > (1 << 30)) return 0;
     if (check_dims(num_keyframes * n_views, ht, wd, num_edges, num_kx, t0 * n_views, t1 * n_views) != VIPE_OK)
         return 0;
+    if (optimize_rig_rotation && n_views > 1 && num_keyframes * n_views > kMaxPoses) return 0;
     Dims dv, dk;
-    rig_dims(num_keyframes, n_views, ht, wd, num_edges, num_kx, t0, t1, dv, dk);
+    rig_dims(num_keyframes, n_views, ht, wd, num_edges, num_kx, t0, t1, optimize_rig_rotation ? 1 : 0, dv, dk);
     Sizer c;
     GraphDesc gv{}, gk{};
     GraphDesc *tv, *tk;
@@ -2799,15 +2870,15 @@ extern "C" size_t vipe_slam_ba_rig_workspace_size(int num_keyframes, int n_views
     return c.used + 256;
 }
 
-extern "C" int vipe_slam_ba_rig(float* poses_io, const float* rig, int n_views, float* disps_io,
+extern "C" int vipe_slam_ba_rig(float* poses_io, float* rig, int n_views, float* disps_io,
                                 const float* intrinsics, const float* disps_sens, const float* targets,
                                 const float* weights, const float* eta, const int64_t* ii, const int64_t* jj,
                                 const float* depth_active, int num_keyframes, int ht, int wd, int num_edges,
                                 int num_kx, int t0, int t1, int iterations, float lm, float ep, int motion_only,
                                 float alpha, int compute_energy, float* dx_out, float* dz_out, float* energy_out,
                                 int robust_kind, float robust_threshold, const float* mu_schedule, int camera_model,
-                                float distortion, void* workspace, size_t workspace_bytes, int32_t* dev_status,
-                                void* stream) {
+                                float distortion, int optimize_rig_rotation, float rig_lm, float rig_ep,
+                                void* workspace, size_t workspace_bytes, int32_t* dev_status, void* stream) {
     if (n_views < 1 || !rig) {
         set_last_error("rig BA: n_views >= 1 and the rig extrinsics (n_views, 7) are required");
         return VIPE_ERR_ARG;
@@ -2821,14 +2892,21 @@ extern "C" int vipe_slam_ba_rig(float* poses_io, const float* rig, int n_views, 
             if (!(mu_schedule[k] > 0.f)) return VIPE_ERR_ARG;
     }
     const int V = n_views, Nv = num_keyframes * V;
+    const int rig_opt = (optimize_rig_rotation && V > 1) ? 1 : 0;
     int rc = check_dims(Nv, ht, wd, num_edges, num_kx, t0 * V, t1 * V);
     if (rc != VIPE_OK) return rc;
+    if (rig_opt && Nv > kMaxPoses) {
+        set_last_error("rig BA: optimising the rig makes every (keyframe, view) an unknown: n_views * num_keyframes "
+                       "exceeds the solver's window");
+        return VIPE_ERR_CAPACITY;
+    }
+    if (rig_opt && !(rig_lm >= 0.f && rig_ep >= 0.f)) return VIPE_ERR_ARG;
     rc = check_ba_args(poses_io, disps_io, intrinsics, disps_sens, targets, weights, eta, ii, jj, depth_active,
                        num_edges, iterations, motion_only, compute_energy, dx_out, dz_out, energy_out);
     if (rc != VIPE_OK) return rc;
     cudaStream_t st = as_stream(stream);
     GraphDesc gv{}, gk{};
-    rig_dims(num_keyframes, V, ht, wd, num_edges, num_kx, t0, t1, gv.d, gk.d);
+    rig_dims(num_keyframes, V, ht, wd, num_edges, num_kx, t0, t1, rig_opt, gv.d, gk.d);
     Carver cv(workspace, workspace_bytes);
     GraphDesc *tv, *tk;
     float *vposes, *vdx;
@@ -2851,31 +2929,46 @@ extern "C" int vipe_slam_ba_rig(float* poses_io, const float* rig, int n_views, 
     BAPtrs bk{poses_io, nullptr, const_cast<float*>(intrinsics), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
               nullptr, dx_out, nullptr, nullptr, dev_status, iterations, 0};
     SolveArgs a{iterations, lm, ep, alpha, motion_only, 0, 1e-6f, 1e-6f, 1.f, compute_energy};
+    // the keyframe solve damps rows past the poses (the rig rows) with the scalar pair
+    SolveArgs ak = a;
+    if (rig_opt) {
+        ak.ilm = rig_lm;
+        ak.iep = rig_ep;
+    }
     const int P = t1 - t0;
+    const RigCols cols{P, V, num_keyframes, t0, gv.d.t0, gv.d.P, rig_opt};
     if ((rc = launch_index(geo_v, tv, bv, &gv, st)) != VIPE_OK) return rc;
     ba_rig_desc_kernel<<<1, 32, 0, st>>>(tk, gk);
-    VIPE_LAUNCH_CHECK();
-    ba_rig_adjoint_kernel<<<1, 32 * ((V + 31) / 32), 0, st>>>(rig, V, A);
     VIPE_LAUNCH_CHECK();
     const int ldv = gv.d.dim, ldk = gk.d.dim;
     for (int itr = 0; itr < iterations; itr++) {
         BAPtrs b = bv;
         if (robust_kind == 3) b.rb.mu = mu_schedule[itr];
+        if (itr == 0 || rig_opt) {
+            ba_rig_adjoint_kernel<<<1, 32 * ((V + 31) / 32), 0, st>>>(rig, V, A);
+            VIPE_LAUNCH_CHECK();
+        }
         ba_rig_virtual_kernel<<<ceil_div(Nv, 128), 128, 0, st>>>(poses_io, rig, num_keyframes, V, vposes);
         VIPE_LAUNCH_CHECK();
         if ((rc = launch_linearize_solve(geo_v, tv, nullptr, b, a, itr, st, false)) != VIPE_OK) return rc;
         {
             VIPE_PROF("ba_rig_project", st);
-            ba_rig_project_kernel<<<ceil_div((long)ldk * ldk, 256), 256, 0, st>>>(gv.w.Hm, gv.w.bv, ldv, P, V, A,
+            ba_rig_project_kernel<<<ceil_div((long)ldk * ldk, 256), 256, 0, st>>>(gv.w.Hm, gv.w.bv, ldv, cols, A,
                                                                                  gk.w.Hm, gk.w.bv, ldk);
         }
         VIPE_LAUNCH_CHECK();
-        if ((rc = launch_cholesky(geo_k, tk, nullptr, bk, a, st)) != VIPE_OK) return rc;
-        ba_rig_expand_kernel<<<ceil_div(P * V * 6, 128), 128, 0, st>>>(dx_out, A, P, V, vdx);
+        if ((rc = launch_cholesky(geo_k, tk, nullptr, bk, ak, st)) != VIPE_OK) return rc;
+        ba_rig_expand_kernel<<<ceil_div(gv.d.P * 6, 128), 128, 0, st>>>(dx_out, gk.w.bv, gk.w.meta + 4, A, cols,
+                                                                         vdx);
         VIPE_LAUNCH_CHECK();
         if ((rc = launch_update(geo_v, tv, nullptr, b, a, st)) != VIPE_OK) return rc;
         ba_rig_retract_kernel<<<ceil_div(P, 128), 128, 0, st>>>(poses_io, dx_out, t0, P, gv.w.status, gk.w.status);
         VIPE_LAUNCH_CHECK();
+        if (rig_opt) {
+            ba_rig_rotation_retract_kernel<<<1, 32 * ((V + 31) / 32), 0, st>>>(rig, gk.w.bv, P, V, gk.w.meta + 4,
+                                                                             gv.w.status, gk.w.status);
+            VIPE_LAUNCH_CHECK();
+        }
     }
     if (dev_status) {
         ba_status_kernel<<<1, 1, 0, st>>>(bv, Batch{tv, nullptr, 1});

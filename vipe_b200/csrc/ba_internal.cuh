@@ -42,6 +42,8 @@ __host__ __device__ inline int tri12(int r, int c) { return r >= c ? r * (r + 1)
 
 struct Dims {
     int N, H, W, HW, E, K, t0, t1, P, dim;
+    int kx0, kx1;      // frames [kx0, kx1) join kx with the edges' sources (= [t0, t1) except for
+                       // a rig solve that optimises the rig, whose pose window spans every frame)
     int CHe, chunk_e;  // edge kernel pixel chunks
     int CF, chunk_f;   // frame kernel pixel chunks
     long tile_cap;     // capacity of frame SYRK tiles (tensor-core frames, per pixel chunk)
@@ -127,6 +129,7 @@ inline Dims make_dims(int N, int H, int W, int E, int K, int t0, int t1, int che
                       bool single = false) {
     Dims d;
     d.N = N; d.H = H; d.W = W; d.HW = H * W; d.E = E; d.K = K; d.t0 = t0; d.t1 = t1;
+    d.kx0 = t0; d.kx1 = t1;
     d.P = t1 - t0;
     d.dof = dof;
     d.dim = dof * d.P + 1;

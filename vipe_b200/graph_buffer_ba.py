@@ -6,13 +6,14 @@ kernel (buffer.py:387-404, 541-545); everything else goes to the generic torch s
 (vipe/slam/ba/solver.py, terms.py).  `bundle_adjustment` here is a drop-in for that method
 that runs those configurations on this library's fused kernels:
 
-  * multi-view rigs (n_views > 1, fixed rig extrinsics, per-view intrinsics): vipe_slam_ba_rig;
+  * multi-view rigs (n_views > 1, per-view intrinsics, rig extrinsics fixed or with their
+    rotations optimised as the generic solver's rig group): vipe_slam_ba_rig;
   * robust kernels (Huber, Tukey, GNC-TLS with its mu schedule) and the MEI camera:
     vipe_slam_ba_extended_generic / vipe_slam_ba_rig;
   * single-view pinhole buffers with focal optimisation as before.
 
-It raises for what it does not cover: optimize_rig_rotation, MEI views whose distortion
-differs, focal/distortion optimisation with MEI or with a rig, panorama cameras, and sparse
+(With one view optimize_rig_rotation changes nothing: the generic solver fixes rig 0.) It raises
+for what it does not cover: MEI views whose distortion differs, focal/distortion optimisation with MEI or with a rig, panorama cameras, and sparse
 tracks together with a robust kernel.  Install with
 
     GraphBuffer.bundle_adjustment = vipe_b200.graph_buffer_ba.bundle_adjustment
@@ -46,8 +47,6 @@ def robust_settings(ba_config, n_iters):
 def bundle_adjustment(self, target, weight, disp_damping, ii, jj, t0, t1, n_iters, pose_damping, pose_ep,
                       motion_only, limited_disp, optimize_intrinsics, optimize_rig_rotation, verbose=False):
     """Drop-in for GraphBuffer.bundle_adjustment (same arguments) on the fused GPU solver."""
-    if optimize_rig_rotation:
-        raise RuntimeError("fused BA: optimize_rig_rotation is not supported")
     cam = getattr(self.camera_type, "value", self.camera_type)
     cam = str(cam).lower()
     if cam not in ("pinhole", "mei"):
@@ -106,7 +105,11 @@ def bundle_adjustment(self, target, weight, disp_damping, ii, jj, t0, t1, n_iter
         if torch.any(di == dj):
             raise RuntimeError("fused BA: terms within one depth frame are not supported")
         intr8v = (intr[:, :4] / 8.0).float().contiguous()  # one row per view
-        R.ba_rig(self.poses, self.rig.float().contiguous(), disps, intr8v, sens, target, weight, eta, di.contiguous(),
+        rig = self.rig.float().contiguous()
+        R.ba_rig(self.poses, rig, disps, intr8v, sens, target, weight, eta, di.contiguous(),
                  dj.contiguous(), depth_active, t0, t1, iters, pose_damping, pose_ep, motion_only, alpha, verbose,
-                 robust_kernel=kernel, threshold=thr, mu_schedule=sched, camera_type=cam, distortion=k1)
+                 robust_kernel=kernel, threshold=thr, mu_schedule=sched, camera_type=cam, distortion=k1,
+                 optimize_rig_rotation=optimize_rig_rotation)
+        if optimize_rig_rotation:
+            self.rig.copy_(rig)
     self.disps.clamp_(min=0.001)

@@ -114,12 +114,14 @@ def ba_extended_robust(poses, disps, intrinsics, disps_sens, targets, weights, e
 
 def ba_rig(poses, rig, disps, intrinsics, disps_sens, targets, weights, eta, ii, jj, depth_active, t0, t1, iterations,
            lm, ep, motion_only, alpha, compute_energy=False, robust_kernel=None, threshold=1.0, mu_schedule=None,
-           camera_type=None, distortion=0.0):
+           camera_type=None, distortion=0.0, optimize_rig_rotation=False, rig_damping=1e-4, rig_ep=1e-4):
     """Fused BA over a multi-view rig (vipe_slam_ba_rig): keyframe poses (N, 7), fixed rig
     extrinsics (V, 7), depth frames (N * V, H, W) indexed k * V + q, per-term source/target
     depth-frame indices ii, jj, and intrinsics (4,) shared by the views or (V, 4) per view (a
     term unprojects with its source view's row and projects with its target view's).
-    Returns [dx (t1 - t0, 6), dz or None, energy]."""
+    optimize_rig_rotation: the rotations of rig views 1..V-1 join the solve (the generic
+    solver's rig group, buffer.py:668-673; rig_damping and rig_ep its damping) and are written
+    back into ``rig``.  Returns [dx (t1 - t0, 6), dz or None, energy]."""
     import ctypes
 
     name = None if robust_kernel is None else str(robust_kernel).lower()
@@ -157,7 +159,8 @@ def ba_rig(poses, rig, disps, intrinsics, disps_sens, targets, weights, eta, ii,
     num_edges, num_kx = ii.shape[0], eta.shape[0]
     dev = poses.device
     lib = _lib.load()
-    ws_bytes = lib.vipe_slam_ba_rig_workspace_size(N, V, ht, wd, num_edges, num_kx, t0, t1)
+    opt = int(bool(optimize_rig_rotation))
+    ws_bytes = lib.vipe_slam_ba_rig_workspace_size(N, V, ht, wd, num_edges, num_kx, t0, t1, opt)
     if ws_bytes == 0:
         raise RuntimeError("rig bundle adjustment: unsupported sizes or window")
     with torch.cuda.device(dev):
@@ -172,8 +175,8 @@ def ba_rig(poses, rig, disps, intrinsics, disps_sens, targets, weights, eta, ii,
             N, ht, wd, num_edges, num_kx, t0, t1, iterations, float(lm), float(ep), int(bool(motion_only)),
             float(alpha), int(bool(compute_energy)), dx.data_ptr(), _lib.ptr(dz),
             energy.data_ptr() if compute_energy else None, kind, float(threshold),
-            None if sched is None else ctypes.cast(sched, ctypes.c_void_p), cam, float(distortion), ws.data_ptr(),
-            ws_bytes, status.data_ptr(), _lib.stream_of(poses))
+            None if sched is None else ctypes.cast(sched, ctypes.c_void_p), cam, float(distortion), opt,
+            float(rig_damping), float(rig_ep), ws.data_ptr(), ws_bytes, status.data_ptr(), _lib.stream_of(poses))
         _lib.check(rc, "ba_rig")
         _se._raise_device_status(int(status.item()), "ba_rig")
     return [dx, dz, energy]
