@@ -169,7 +169,9 @@ int vipe_slam_ba_extended_generic(float* poses_io, float* disps_io, float* intri
  *     unprojects with its source view's row and projects with its target view's (the generic
  *     solver's per-view intrinsics, terms.py:175-206);
  *   dx_out (t1 - t0, 6) keyframe steps; dz_out (num_kx, ht*wd); energy_out (iterations) or NULL;
- *   robust kernel, mu schedule and camera model as vipe_slam_ba_extended_generic.
+ *   robust kernel, mu schedule and camera model as vipe_slam_ba_extended_generic; with the MEI
+ *     camera view_distortion (device, n_views floats in [0, 1], or NULL for `distortion` in
+ *     every view) gives each view its k1, used as its intrinsics rows are;
  * Generic-solver back-substitution (rows of pose t0 kept).  Limits: n_views * (t1 - t0) <= 1024.
  * Workspace: vipe_slam_ba_rig_workspace_size. */
 size_t vipe_slam_ba_rig_workspace_size(int num_keyframes, int n_views, int ht, int wd, int num_edges, int num_kx,
@@ -180,8 +182,9 @@ int vipe_slam_ba_rig(float* poses_io, float* rig, int n_views, float* disps_io, 
                      int wd, int num_edges, int num_kx, int t0, int t1, int iterations, float lm, float ep,
                      int motion_only, float alpha, int compute_energy, float* dx_out, float* dz_out,
                      float* energy_out, int robust_kind, float robust_threshold, const float* mu_schedule,
-                     int camera_model, float distortion, int optimize_rig_rotation, float rig_lm, float rig_ep,
-                     void* workspace, size_t workspace_bytes, int32_t* dev_status, void* stream);
+                     int camera_model, float distortion, const float* view_distortion, int optimize_rig_rotation,
+                     float rig_lm, float rig_ep, void* workspace, size_t workspace_bytes, int32_t* dev_status,
+                     void* stream);
 
 /* Replaces slam_ext.ba (reference: csrc/slam_ext/slam.cpp:42-45,
  * geom_kernels.cu:1826-1834): ba_extended with depth_active = 1, no focal

@@ -330,11 +330,12 @@ def camera_cases():
 
 RIG = {
     # name: (outliers, robust_kernel, threshold, n_iters, per-view intrinsics + cross-view terms,
-    #        rig rotation optimised from a perturbed initial rig)
-    "rig": (False, None, 1.0, 2, False, False),
-    "rig_huber": (True, "huber", 2.0, 3, False, False),
-    "rig_views": (False, None, 1.0, 2, True, False),
-    "rig_rot": (False, None, 1.0, 3, False, True),
+    #        rig rotation optimised from a perturbed initial rig, MEI k1 per view or None: pinhole)
+    "rig": (False, None, 1.0, 2, False, False, None),
+    "rig_huber": (True, "huber", 2.0, 3, False, False, None),
+    "rig_views": (False, None, 1.0, 2, True, False, None),
+    "rig_rot": (False, None, 1.0, 3, False, True, None),
+    "rig_mei_views": (False, None, 1.0, 4, True, False, (0.15, 0.3)),
 }
 
 
@@ -350,7 +351,7 @@ def rig_cases():
     import _graph_buffer_golden as Gd
 
     out = {}
-    for name, (outl, kernel, thr, n_iters, views, rig_rot) in RIG.items():
+    for name, (outl, kernel, thr, n_iters, views, rig_rot, mei_k1) in RIG.items():
         r = Gd.rig_problem(outliers=outl, views=views, rig_error=rig_rot)
         N, V = r.N, r.V
         H, Wd = r.disps.shape[1:]
@@ -358,11 +359,13 @@ def rig_cases():
                     "robust_kernel": kernel, "robust_kernel_threshold": thr, "gnc_mu_init": 1.0, "gnc_mu_step": 3.0,
                     "gnc_mu_max": 1.0e6, "gnc_n_mu_steps": 4, "gnc_gn_iters_per_mu": 6})
         v = GraphBuffer(height=8 * H, width=8 * Wd, n_views=V, buffer_size=N, init_disp=1.0, cross_view_idx=None,
-                        ba_config=cfg, sparse_tracks=DummySparseTracks(n_views=V), camera_type=CameraType.PINHOLE,
-                        device=torch.device("cpu"))
+                        ba_config=cfg, sparse_tracks=DummySparseTracks(n_views=V),
+                        camera_type=CameraType.MEI if mei_k1 else CameraType.PINHOLE, device=torch.device("cpu"))
         v.n_frames = N
         v.tstamp[:N] = torch.arange(N)
         v.intrinsics[:, :4] = r.intrinsics * 8
+        if mei_k1:
+            v.intrinsics[:, 4] = torch.tensor(mei_k1)
         v.rig[:] = r.rig
         v.poses[:N] = r.poses
         v.disps[:N] = r.disps.reshape(N, V, H, Wd)
@@ -380,6 +383,7 @@ def rig_cases():
                             optimize_rig_rotation=rig_rot, verbose=False)
         out[name] = {"outliers": outl, "kernel": kernel, "threshold": thr, "iterations": n_iters, "n_frames": N,
                      "views": views, "rig_rot": rig_rot, "rig": v.rig.clone(), "rig_before": r.rig.clone(),
+                     "mei_k1": mei_k1,
                      "generic": {"poses": v.poses.clone(), "disps": v.disps.clone().reshape(-1, H, Wd)},
                      "before": {"poses": r.poses.clone()}}
     return out

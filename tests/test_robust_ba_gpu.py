@@ -121,20 +121,23 @@ def _rig_args(r, dev="cuda"):
                 alpha=r.alpha)
 
 
-@pytest.mark.parametrize("name", ["rig", "rig_huber", "rig_views", "rig_rot"])
+@pytest.mark.parametrize("name", ["rig", "rig_huber", "rig_views", "rig_rot", "rig_mei_views"])
 def test_rig_matches_reference_generic_solver(name):
     """A two-view rig with non-identity extrinsics (tests/_graph_buffer_golden.rig_problem) through
     vipe_slam_ba_rig against the reference's generic solver on GraphBuffer(n_views=2); rig_views
     adds per-view intrinsics and cross-view terms (source and target views differ); rig_rot
-    starts from a rotated view-1 rig and optimises the rig rotation (optimize_rig_rotation)."""
+    starts from a rotated view-1 rig and optimises the rig rotation (optimize_rig_rotation);
+    rig_mei_views is the per-view case on MEI cameras with a different k1 per view."""
     from vipe_b200.robust_ba import ba_rig
 
     c = G.rig_cases()[name]
     rot = c.get("rig_rot", False)
     r = G.rig_problem(outliers=c["outliers"], views=c.get("views", False), rig_error=rot)
     a = _rig_args(r)
+    mei = c.get("mei_k1")
+    cam = dict(camera_type="mei", distortion=torch.tensor(mei)) if mei else {}
     ba_rig(**a, iterations=c["iterations"], robust_kernel=c["kernel"], threshold=c["threshold"],
-           optimize_rig_rotation=rot)
+           optimize_rig_rotation=rot, **cam)
     torch.cuda.synchronize()
     if rot:
         dr = float((a["rig"].cpu() - c["rig"]).abs().max())
@@ -187,19 +190,21 @@ class _FakeBuffer:
     pairs become the cross-view terms (k, q) -> (k, (q + 1) % n_views) of the default
     cross_view_idx, buffer.py:63-64)."""
 
-    def __init__(self, r, kernel, thr):
+    def __init__(self, r, kernel, thr, mei_k1=None):
         import types
 
         N, V = r.N, r.V
         H, W = r.disps.shape[1:]
         self.n_views, self.height, self.width = V, 8 * H, 8 * W
-        self.camera_type = "pinhole"
+        self.camera_type = "mei" if mei_k1 else "pinhole"
         self.poses = r.poses.cuda().contiguous()
         self.rig = r.rig.cuda()
         self.disps = r.disps.reshape(N, V, H, W).cuda().contiguous()
         self.disps_sens = r.disps_sens.reshape(N, V, H, W).cuda().contiguous()
         intr = r.intrinsics if r.intrinsics.dim() == 2 else r.intrinsics.reshape(1, 4).repeat(V, 1)
         self.intrinsics = (intr * 8).cuda()
+        if mei_k1:
+            self.intrinsics = torch.cat([self.intrinsics, torch.tensor(mei_k1).reshape(V, 1).cuda()], 1)
         self.tstamp = torch.arange(N).cuda()
 
         class Cfg(dict):
@@ -219,7 +224,7 @@ class _FakeBuffer:
         return pi.reshape(-1), qi.reshape(-1), di.reshape(-1), pj.reshape(-1), qj.reshape(-1), dj.reshape(-1)
 
 
-@pytest.mark.parametrize("name", ["rig", "rig_huber", "rig_views", "rig_rot"])
+@pytest.mark.parametrize("name", ["rig", "rig_huber", "rig_views", "rig_rot", "rig_mei_views"])
 def test_graph_buffer_drop_in_on_a_rig(name):
     """vipe_b200.graph_buffer_ba.bundle_adjustment called the way GraphBuffer is (keyframe edges,
     expanded targets (E * V, H*W, 2), disp_damping per depth frame) against the same fixtures."""
@@ -228,7 +233,7 @@ def test_graph_buffer_drop_in_on_a_rig(name):
     c = G.rig_cases()[name]
     rot = c.get("rig_rot", False)
     r = G.rig_problem(outliers=c["outliers"], views=c.get("views", False), rig_error=rot)
-    buf = _FakeBuffer(r, c["kernel"], c["threshold"])
+    buf = _FakeBuffer(r, c["kernel"], c["threshold"], c.get("mei_k1"))
     E = r.targets.shape[0]
     H, W = r.disps.shape[1:]
     target = r.targets.permute(0, 2, 3, 1).reshape(E, H * W, 2).cuda()

@@ -45,8 +45,8 @@ _SIGS: dict[str, tuple] = {
     "vipe_slam_ba_rig_workspace_size": (SZ, [I, I, I, I, I, I, I, I, I]),
     "vipe_slam_ba_rig": (
         I,
-        [P, P, I, P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, F, I, F, I, P, P, P, I, F, P, I, F, I, F, F,
-         P, SZ, P, P],
+        [P, P, I, P, P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, I, F, F, I, F, I, P, P, P, I, F, P, I, F, P, I, F,
+         F, P, SZ, P, P],
     ),
     "vipe_slam_ba_extended_generic": (
         I,

@@ -484,8 +484,9 @@ __global__ void __launch_bounds__(kEdgeThreads, (D == 6 && !kIntr) ? 4 : (D == 7
     edge_tf<D>(A.poses, a, b, Tf);
     float fx = A.intr[0], fy = A.intr[1], cx = A.intr[2], cy = A.intr[3];
     SrcIntr si;
+    RobustSpec rbt = kExt ? io.rb : RobustSpec{};
     if constexpr (kExt) {
-        if (io.rb.nview > 1) view_intrinsics(A.intr, io.rb.nview, a, b, fx, fy, cx, cy, si);
+        if (rbt.nview > 1) view_camera(A.intr, rbt, a, b, fx, fy, cx, cy, si);
     }
 
     float H[NH], vj[D], fj[D];
@@ -507,7 +508,7 @@ __global__ void __launch_bounds__(kEdgeThreads, (D == 6 && !kIntr) ? 4 : (D == 7
         typename LinOf<D>::T L;
         linearize_d<D, kIntr, true>(Tf, stereo, fx, fy, cx, cy, u, v, __ldg(dp + p), __ldg(wu + p),
                                     __ldg(wu + HW + p), __ldg(tu + p), __ldg(tu + HW + p), 1.0f, A.iscale, L,
-                                    kExt ? io.rb : RobustSpec{}, si);
+                                    rbt, si);
         en += L.we[0] * L.r[0] * L.r[0] + L.we[1] * L.r[1] * L.r[1];
 #pragma unroll
         for (int ch = 0; ch < 2; ch++) {
@@ -863,9 +864,10 @@ __global__ void __launch_bounds__(kFrameThreads, 3) ba_frame_kernel(BAPtrs base,
                     if constexpr (kExt) {
                         float fxj = fx, fyj = fy, cxj = cx, cyj = cy;
                         SrcIntr si;
-                        if (io.rb.nview > 1) view_intrinsics(A.intr, io.rb.nview, k, (int)A.jj[e], fxj, fyj, cxj, cyj, si);
+                        RobustSpec rbt = io.rb;
+                        if (rbt.nview > 1) view_camera(A.intr, rbt, k, (int)A.jj[e], fxj, fyj, cxj, cyj, si);
                         linearize_d<D, kIntr, true>(Tf, stereo, fxj, fyj, cxj, cyj, u, v, disp, w0, w1, t0v, t1v, act,
-                                                    A.iscale, L, io.rb, si);
+                                                    A.iscale, L, rbt, si);
                     } else {
                         linearize_d<D, kIntr, true>(Tf, stereo, fx, fy, cx, cy, u, v, disp, w0, w1, t0v, t1v, act,
                                                     A.iscale, L);
@@ -1160,10 +1162,11 @@ __global__ void __launch_bounds__(kWideThreads) ba_frame_wide_kernel(BAPtrs base
                     PixelLin L;
                     float fxj = fx, fyj = fy, cxj = cx, cyj = cy;
                     SrcIntr si;
-                    if (io.rb.nview > 1) view_intrinsics(A.intr, io.rb.nview, k, b, fxj, fyj, cxj, cyj, si);
+                    RobustSpec rbt = io.rb;
+                    if (rbt.nview > 1) view_camera(A.intr, rbt, k, b, fxj, fyj, cxj, cyj, si);
                     linearize_d<D, kIntr, true>(Tf, b == k, fxj, fyj, cxj, cyj, uu, vv, disp, __ldg(A.weights + o),
                                                 __ldg(A.weights + o + HW), __ldg(A.targets + o),
-                                                __ldg(A.targets + o + HW), act, A.iscale, L, io.rb, si);
+                                                __ldg(A.targets + o + HW), act, A.iscale, L, rbt, si);
                     const float g0 = L.wd[0] * L.Jz[0], g1 = L.wd[1] * L.Jz[1];
                     csum += g0 * L.Jz[0] + g1 * L.Jz[1];
                     bsum += g0 * L.r[0] + g1 * L.r[1];
@@ -2106,12 +2109,12 @@ __global__ void __launch_bounds__(256, (D == 6 && !kIntr) ? 8 : (D == 7 ? 6 : 3)
             typename LinOf<D>::T L;
             // robust reweighting needs the residual, hence the targets
             const float* tp = A.targets + (size_t)e * 2 * HW;
-            const RobustSpec rb = kExt ? io.rb : RobustSpec{};
+            RobustSpec rb = kExt ? io.rb : RobustSpec{};
             const bool rob = rb.kind != 0;
             float fxj = fx, fyj = fy, cxj = cx, cyj = cy;
             SrcIntr si;
             if constexpr (kExt) {
-                if (rb.nview > 1) view_intrinsics(A.intr, rb.nview, k, b, fxj, fyj, cxj, cyj, si);
+                if (rb.nview > 1) view_camera(A.intr, rb, k, b, fxj, fyj, cxj, cyj, si);
             }
             linearize_d<D, false, false>(Tf, k == b, fxj, fyj, cxj, cyj, u, v, disp, __ldg(wp + p), __ldg(wp + HW + p),
                                          rob ? __ldg(tp + p) : 0.f, rob ? __ldg(tp + HW + p) : 0.f, act, 1.f, L, rb,
@@ -2877,8 +2880,9 @@ extern "C" int vipe_slam_ba_rig(float* poses_io, float* rig, int n_views, float*
                                 int num_kx, int t0, int t1, int iterations, float lm, float ep, int motion_only,
                                 float alpha, int compute_energy, float* dx_out, float* dz_out, float* energy_out,
                                 int robust_kind, float robust_threshold, const float* mu_schedule, int camera_model,
-                                float distortion, int optimize_rig_rotation, float rig_lm, float rig_ep,
-                                void* workspace, size_t workspace_bytes, int32_t* dev_status, void* stream) {
+                                float distortion, const float* view_distortion, int optimize_rig_rotation,
+                                float rig_lm, float rig_ep, void* workspace, size_t workspace_bytes,
+                                int32_t* dev_status, void* stream) {
     if (n_views < 1 || !rig) {
         set_last_error("rig BA: n_views >= 1 and the rig extrinsics (n_views, 7) are required");
         return VIPE_ERR_ARG;
@@ -2925,6 +2929,7 @@ extern "C" int vipe_slam_ba_rig(float* poses_io, float* rig, int n_views, float*
     bv.rb.cam = camera_model;
     bv.rb.k1 = camera_model == 1 ? distortion : 0.f;
     bv.rb.nview = V > 1 ? V : 0;  // intrinsics: one row per view, depth frame k * V + q uses row q
+    bv.rb.k1v = (camera_model == 1 && V > 1) ? view_distortion : nullptr;  // MEI: per-view k1
     bv.exact_backsub = 1;
     BAPtrs bk{poses_io, nullptr, const_cast<float*>(intrinsics), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
               nullptr, dx_out, nullptr, nullptr, dev_status, iterations, 0};

@@ -159,6 +159,7 @@ struct RobustSpec {
     int cam = 0;
     float k1 = 0.0f;
     int nview = 0;
+    const float* k1v = nullptr;  // per-view MEI distortion (nview entries), or one k1 for all
 };
 
 // Intrinsics of the source view of a term when they differ from the target view's (per-view
@@ -167,6 +168,7 @@ struct RobustSpec {
 struct SrcIntr {
     int on = 0;
     float fx = 1.0f, fy = 1.0f, cx = 0.0f, cy = 0.0f;
+    float k1 = 0.0f;  // the source view's MEI distortion
 };
 
 // per-view intrinsics: the target view's row of depth frame b into fx..cy and the source
@@ -184,6 +186,19 @@ __device__ __forceinline__ void view_intrinsics(const float* intr, int nview, in
     si.fy = ki[1];
     si.cx = ki[2];
     si.cy = ki[3];
+}
+
+// the per-view camera of a term from source frame a into target frame b: the target's
+// intrinsics into fx..cy and its MEI distortion into rb.k1, the source's into si
+__device__ __forceinline__ void view_camera(const float* intr, RobustSpec& rb, int a, int b, float& fx, float& fy,
+                                            float& cx, float& cy, SrcIntr& si) {
+    view_intrinsics(intr, rb.nview, a, b, fx, fy, cx, cy, si);
+    if (rb.k1v) {
+        si.k1 = rb.k1v[a % rb.nview];
+        rb.k1 = rb.k1v[b % rb.nview];
+    } else {
+        si.k1 = rb.k1;
+    }
 }
 
 __device__ __forceinline__ float robust_weight(const RobustSpec& rb, float r) {
@@ -218,13 +233,14 @@ __device__ __forceinline__ void linearize_mei(const float* tij, const float* qij
                                               float cx, float cy, float u, float v, float disp, float wu_in,
                                               float wv_in, float tu, float tv, float act, PixelLin& L,
                                               const RobustSpec& rb, const SrcIntr& si) {
-    const float k1 = rb.k1;
+    const float k1 = rb.k1;                 // the target view's (projection)
+    const float k1s = si.on ? si.k1 : k1;   // the source view's (unprojection)
     const float ub = si.on ? (u - si.cx) / si.fx : (u - cx) / fx;
     const float vb = si.on ? (v - si.cy) / si.fy : (v - cy) / fy;
     const float r2 = ub * ub + vb * vb;
-    const float qq = sqrtf(1.0f + (1.0f - k1 * k1) * r2);
-    const float fac = (k1 + qq) / (1.0f + r2);
-    const float Xi[4] = {ub * fac / (fac - k1), vb * fac / (fac - k1), 1.0f, disp};
+    const float qq = sqrtf(1.0f + (1.0f - k1s * k1s) * r2);
+    const float fac = (k1s + qq) / (1.0f + r2);
+    const float Xi[4] = {ub * fac / (fac - k1s), vb * fac / (fac - k1s), 1.0f, disp};
     float Xj[4];
     act_h(tij, qij, Xi, Xj);
     const float P0 = Xj[0], P1 = Xj[1], P2 = Xj[2], h = Xj[3];

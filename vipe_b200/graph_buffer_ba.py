@@ -6,15 +6,15 @@ kernel (buffer.py:387-404, 541-545); everything else goes to the generic torch s
 (vipe/slam/ba/solver.py, terms.py).  `bundle_adjustment` here is a drop-in for that method
 that runs those configurations on this library's fused kernels:
 
-  * multi-view rigs (n_views > 1, per-view intrinsics, rig extrinsics fixed or with their
-    rotations optimised as the generic solver's rig group): vipe_slam_ba_rig;
+  * multi-view rigs (n_views > 1, per-view intrinsics and MEI distortion, rig extrinsics fixed
+    or with their rotations optimised as the generic solver's rig group): vipe_slam_ba_rig;
   * robust kernels (Huber, Tukey, GNC-TLS with its mu schedule) and the MEI camera:
     vipe_slam_ba_extended_generic / vipe_slam_ba_rig;
   * single-view pinhole buffers with focal optimisation as before.
 
 (With one view optimize_rig_rotation changes nothing: the generic solver fixes rig 0.) It raises
-for what it does not cover: MEI views whose distortion differs, focal/distortion optimisation with MEI or with a rig, panorama cameras, and sparse
-tracks together with a robust kernel.  Install with
+for what it does not cover: focal/distortion optimisation with MEI or with a rig, panorama
+cameras, and sparse tracks together with a robust kernel.  Install with
 
     GraphBuffer.bundle_adjustment = vipe_b200.graph_buffer_ba.bundle_adjustment
 """
@@ -71,8 +71,6 @@ def bundle_adjustment(self, target, weight, disp_damping, ii, jj, t0, t1, n_iter
     target = target.reshape(n_terms, H, W, 2).permute(0, 3, 1, 2).contiguous()
     weight = weight.reshape(n_terms, H, W, 2).permute(0, 3, 1, 2).contiguous()
     intr = self.intrinsics
-    if cam == "mei" and V > 1 and not torch.allclose(intr[1:, 4], intr[:1, 4].expand_as(intr[1:, 4])):
-        raise RuntimeError("fused BA: the views' MEI distortions differ")
     k1 = float(intr[0, 4]) if cam == "mei" else 0.0
     intr8 = (intr[0, :4] / 8.0).contiguous()
     nv = self.disps.shape[0] * V
@@ -108,7 +106,8 @@ def bundle_adjustment(self, target, weight, disp_damping, ii, jj, t0, t1, n_iter
         rig = self.rig.float().contiguous()
         R.ba_rig(self.poses, rig, disps, intr8v, sens, target, weight, eta, di.contiguous(),
                  dj.contiguous(), depth_active, t0, t1, iters, pose_damping, pose_ep, motion_only, alpha, verbose,
-                 robust_kernel=kernel, threshold=thr, mu_schedule=sched, camera_type=cam, distortion=k1,
+                 robust_kernel=kernel, threshold=thr, mu_schedule=sched, camera_type=cam,
+                 distortion=intr[:, 4].float().contiguous() if cam == "mei" else 0.0,
                  optimize_rig_rotation=optimize_rig_rotation)
         if optimize_rig_rotation:
             self.rig.copy_(rig)

@@ -119,6 +119,7 @@ def ba_rig(poses, rig, disps, intrinsics, disps_sens, targets, weights, eta, ii,
     extrinsics (V, 7), depth frames (N * V, H, W) indexed k * V + q, per-term source/target
     depth-frame indices ii, jj, and intrinsics (4,) shared by the views or (V, 4) per view (a
     term unprojects with its source view's row and projects with its target view's).
+    distortion: the MEI k1 of every view, or a (V,) tensor with one per view.
     optimize_rig_rotation: the rotations of rig views 1..V-1 join the solve (the generic
     solver's rig group, buffer.py:668-673; rig_damping and rig_ep its damping) and are written
     back into ``rig``.  Returns [dx (t1 - t0, 6), dz or None, energy]."""
@@ -160,6 +161,14 @@ def ba_rig(poses, rig, disps, intrinsics, disps_sens, targets, weights, eta, ii,
     dev = poses.device
     lib = _lib.load()
     opt = int(bool(optimize_rig_rotation))
+    k1v = None
+    if isinstance(distortion, torch.Tensor):
+        k1v = distortion.to(device=poses.device, dtype=torch.float32).reshape(-1).contiguous()
+        if k1v.numel() != V:
+            raise RuntimeError("distortion must be a float or one value per view")
+        if cam == 1 and not bool(((k1v >= 0) & (k1v <= 1)).all()):
+            raise RuntimeError("MEI distortion must lie in [0, 1]")
+        distortion = float(k1v[0])
     ws_bytes = lib.vipe_slam_ba_rig_workspace_size(N, V, ht, wd, num_edges, num_kx, t0, t1, opt)
     if ws_bytes == 0:
         raise RuntimeError("rig bundle adjustment: unsupported sizes or window")
@@ -175,7 +184,7 @@ def ba_rig(poses, rig, disps, intrinsics, disps_sens, targets, weights, eta, ii,
             N, ht, wd, num_edges, num_kx, t0, t1, iterations, float(lm), float(ep), int(bool(motion_only)),
             float(alpha), int(bool(compute_energy)), dx.data_ptr(), _lib.ptr(dz),
             energy.data_ptr() if compute_energy else None, kind, float(threshold),
-            None if sched is None else ctypes.cast(sched, ctypes.c_void_p), cam, float(distortion), opt,
+            None if sched is None else ctypes.cast(sched, ctypes.c_void_p), cam, float(distortion), _lib.ptr(k1v), opt,
             float(rig_damping), float(rig_ep), ws.data_ptr(), ws_bytes, status.data_ptr(), _lib.stream_of(poses))
         _lib.check(rc, "ba_rig")
         _se._raise_device_status(int(status.item()), "ba_rig")
