@@ -80,12 +80,18 @@ struct Params {
 using namespace ::vipe::tc;
 
 // TMA tensor store of a staged box (3-D map: target columns, source pixels, target
-// rows); completion is tracked per thread with bulk groups
+// rows); completion is tracked per thread with bulk groups.  The volume is written once and
+// never re-read by this kernel: its lines carry the L2 evict-first policy, so the write stream
+// leaves L2 in the order it arrives and the re-read B tiles stay resident (640 edges: 3.95 ->
+// 3.73 ms per build, the minimum of alternating runs)
 __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int x, int y, int z) {
-    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
-                     reinterpret_cast<uint64_t>(map)),
-                 "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
-                 : "memory");
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    asm volatile(
+        "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group.L2::cache_hint [%0, {%2, %3, %4}], [%1], %5;" ::"l"(
+            reinterpret_cast<uint64_t>(map)),
+        "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z), "l"(pol)
+        : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 // the staged boxes of every committed store have been read (the buffer may be rewritten)
