@@ -820,21 +820,23 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
             const float X[4] = {(u - cx) / fx, (v - cy) / fy, 1.f, pdisp[i]};
             // Sim3: this pixel's targets, weights and (after the first iteration) the gradients so
             // far are issued before the Jacobian so that their latency hides under it (74 vs 81
-            // ms per 256-clip step); the SE3 form keeps them at their uses (70.5 vs 69.7 ms: the
-            // earlier loads cost it spills at 128 registers)
+            // ms per 256-clip step), and the read-once targets and the gradients go through L2
+            // with the streaming (evict-first) hint, which keeps the weights the two passes share
+            // and the spilled registers resident (68.2 vs 72.8 ms); the SE3 form keeps plain
+            // accesses at their uses (the earlier loads cost it spills, the hints 1.5 %)
             constexpr bool kHoist = D == 7;
             float tg0 = 0.f, tg1 = 0.f, wg0 = 0.f, wg1 = 0.f;
             float ogt0 = 0.f, ogt1 = 0.f, ogw0 = 0.f, ogw1 = 0.f;
             if constexpr (kHoist) {
-                tg0 = __ldg(tp + p);
-                tg1 = __ldg(tp + HW + p);
+                tg0 = __ldcs(tp + p);
+                tg1 = __ldcs(tp + HW + p);
                 wg0 = __ldg(wp + p);
                 wg1 = __ldg(wp + HW + p);
                 if (!first) {
-                    ogt0 = gtp[p];
-                    ogt1 = gtp[HW + p];
-                    ogw0 = gwp[p];
-                    ogw1 = gwp[HW + p];
+                    ogt0 = __ldcs(gtp + p);
+                    ogt1 = __ldcs(gtp + HW + p);
+                    ogw0 = __ldcs(gwp + p);
+                    ogw1 = __ldcs(gwp + HW + p);
                 }
             }
             PixJ<D> J;
@@ -933,10 +935,18 @@ __global__ void __launch_bounds__(kAdjThreads, 2) ba_adj_frame_b_kernel(BAPtrs b
                 const size_t pc = (size_t)ch * HW + p;
                 const float ogt = kHoist ? (ch == 0 ? ogt0 : ogt1) : (first ? 0.f : gtp[pc]);
                 const float ogw = kHoist ? (ch == 0 ? ogw0 : ogw1) : (first ? 0.f : gwp[pc]);
-                gtp[pc] = ogt + wpc * ft[0] + A * gwz * fjz;
-                gwp[pc] = ogw +
+                const float ngt = ogt + wpc * ft[0] + A * gwz * fjz;
+                if constexpr (kHoist)
+                    __stcs(gtp + pc, ngt);
+                else
+                    gtp[pc] = ngt;
+                const float ngw = ogw +
                           0.001f * ((stereo ? 0.f : ft[0] * (rr[ch] - ft[1]) - fg) +
                                     act * act * (gwz * fjz * rr[ch] + gC * fjz * fjz + fjz * (G3 + fb)));
+                if constexpr (kHoist)
+                    __stcs(gwp + pc, ngw);
+                else
+                    gwp[pc] = ngw;
                 // first derivatives (s part) and the depth t-direction (column 3 of G0)
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
