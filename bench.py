@@ -974,7 +974,7 @@ def adjoint_leg(b, tune, dev, args, world, dist, flush, stream, group="se3", wit
                 "traffic": batch_kernel_traffic(b, name, group), "peak_source": src, "bytes_per_launch": nbytes,
                 "avg_launch_ms": avg_s * 1e3,
                 "note": "FP32-issue bound: HBM is the algorithmic bound, not the limiter (ncu, 32-clip "
-                        "cases: issue active 58% / 57%, FMA pipe 40% / 39% for SE3 / Sim3)"}
+                        "cases: issue active 58% / 59%, FMA pipe 40% / 41% for SE3 / Sim3)"}
         break
     if not with_e2e:
         del plan, static, tape, gt, gw
