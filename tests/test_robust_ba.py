@@ -48,3 +48,23 @@ def test_cpu_tensors_are_refused():
 def test_unknown_camera_raises():
     with pytest.raises(ValueError, match="camera_type"):
         R.ba_extended_robust(*_dummy(), camera_type="panorama")
+
+
+def test_rig_workspace_covers_the_rig_rotation_solve():
+    """Host-only sizing of the rig solve: optimising the rig rotation makes every (keyframe, view)
+    a virtual unknown and adds six rows per optimised view, so its workspace is larger; a rig
+    whose keyframes x views exceed the solver's 1024 window poses is refused (size 0)."""
+    from vipe_b200 import _lib
+
+    lib = _lib.load()
+    N, V, H, W, E, K, t0, t1 = 40, 3, 48, 64, 300, 120, 30, 40
+    fixed = lib.vipe_slam_ba_rig_workspace_size(N, V, H, W, E, K, t0, t1, 0)
+    rot = lib.vipe_slam_ba_rig_workspace_size(N, V, H, W, E, K, t0, t1, 1)
+    assert fixed > 0 and rot > fixed
+    # 400 keyframes x 3 views = 1200 virtual unknowns: fine with a fixed rig (window 30 x 3), not
+    # when the rig rotation is optimised
+    assert lib.vipe_slam_ba_rig_workspace_size(400, V, H, W, E, K, t0, t1, 0) > 0
+    assert lib.vipe_slam_ba_rig_workspace_size(400, V, H, W, E, K, t0, t1, 1) == 0
+    # one view: the rig has nothing to optimise (view 0 is fixed), so the flag changes nothing
+    assert lib.vipe_slam_ba_rig_workspace_size(N, 1, H, W, E, 40, t0, t1, 1) == \
+        lib.vipe_slam_ba_rig_workspace_size(N, 1, H, W, E, 40, t0, t1, 0)

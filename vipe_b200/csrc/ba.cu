@@ -2861,9 +2861,11 @@ extern "C" size_t vipe_slam_ba_rig_workspace_size(int num_keyframes, int n_views
     if (n_views < 1 || num_keyframes < 1 || (long)num_keyframes * n_views > (1 << 30)) return 0;
     if (check_dims(num_keyframes * n_views, ht, wd, num_edges, num_kx, t0 * n_views, t1 * n_views) != VIPE_OK)
         return 0;
-    if (optimize_rig_rotation && n_views > 1 && num_keyframes * n_views > kMaxPoses) return 0;
+    // (as in vipe_slam_ba_rig: with one view there is no rig to optimise, view 0 being fixed)
+    const int rig_opt = (optimize_rig_rotation && n_views > 1) ? 1 : 0;
+    if (rig_opt && num_keyframes * n_views > kMaxPoses) return 0;
     Dims dv, dk;
-    rig_dims(num_keyframes, n_views, ht, wd, num_edges, num_kx, t0, t1, optimize_rig_rotation ? 1 : 0, dv, dk);
+    rig_dims(num_keyframes, n_views, ht, wd, num_edges, num_kx, t0, t1, rig_opt, dv, dk);
     Sizer c;
     GraphDesc gv{}, gk{};
     GraphDesc *tv, *tk;
